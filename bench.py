@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the Wyckoff-search trial evaluation (trial structures evaluated/s).
+
+Workload (one "step"): one complete Wyckoff search of the PbSO4-like Pnma
+problem -- 4096 replicas x 5000 generations, 75 % single-site / 25 %
+collective moves, replica ladders of 8, exchange every 10 generations, the
+resolution and penalty ramps of the reference -- run on the device as one
+launch.  Every step starts from fresh random coordinates (uploaded before the
+timed region) and the L2 cache is flushed before each step.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Rank 0 prints one JSON line.  With N > 1 (torchrun), each rank runs its own
+4096-replica search (weak scaling; replicas and ladders are independent, so
+there is no collective on the data path) and the time is the maximum over
+ranks.  ``--impl reference`` times the CPU implementation (the FP64 oracle
+port of the reference's trial evaluation, OpenMP over replicas) on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PARTICLES = 4096
+GENERATIONS = 5000
+SWAP_EVERY = 10
+MUFU_PER_CLK_PER_SM = 16   # SFU transcendental rate of an sm_100 SM (4 per sub-partition)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--particles', type=int, default=PARTICLES)
+    ap.add_argument('--generations', type=int, default=GENERATIONS)
+    ap.add_argument('--cos-mode', type=int, default=0)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.dev), f'--query-gpu={self.Q}',
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': float(max(mx)), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def algorithmic_cos(P, groups, n_particles):
+    """Cosines a search evaluates: per generation, every active reflection times
+    the atoms entering |F|^2 (centring translates excluded), for every replica,
+    plus one re-measurement of the current state at each resolution step."""
+    gm = P.refl.group_meta.reshape(-1, 4)
+    n_f = int((P.tables.gen_skip[:P.n_tot] == 0).sum())
+    refl_act = np.array([int(gm[g - 1, 0] + gm[g - 1, 1]) for g in groups])
+    steps = 1 + int((np.diff(groups) != 0).sum())
+    reeval = sum(int(gm[g - 1, 0] + gm[g - 1, 1]) for g in np.unique(groups))
+    per_particle = int(refl_act.sum()) + reeval
+    factor = 1 if P.centro else 2
+    return per_particle * n_f * n_particles * factor, steps
+
+
+def cpu_baseline(P, groups, pen, n_particles, seconds=10.0):
+    from oracle import oracle as O
+    r = O.WyckoffCpuRunner(P, n_particles, seed=7)
+    gens = np.linspace(0, len(groups) - 1, 64).astype(int)
+    t0 = time.perf_counter()
+    trials = 0
+    used = 0
+    for g in gens:
+        trials += r.generation(int(groups[g]), float(pen[g]))
+        used += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {'value': trials / dt, 'unit': 'trials/s', 'cores': O.num_threads(), 'kind': 'port',
+            'sample': f'{n_particles} replicas x {used} generations spread evenly over the 5000-generation '
+                      f'schedule ({trials} trials, {dt:.1f} s, FP64, OpenMP over replicas)'}
+
+
+def dist_setup(args):
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from powder6_b200.swarm_wyckoff import schedule
+    from powder6_b200.workloads import wyckoff_problem
+    from oracle import oracle as O
+    P = wyckoff_problem(seed=1)
+    groups, pen = schedule(args.generations, P.refl.n_groups)
+    r = O.WyckoffCpuRunner(P, args.particles, seed=7)
+    gens = np.linspace(0, args.generations - 1, 4 * (args.steps + args.warmup)).astype(int)
+    it = iter(gens)
+    per_step = 4
+
+    def step():
+        n = 0
+        for _ in range(per_step):
+            g = next(it)
+            n += r.generation(int(groups[g]), float(pen[g]))
+        return n
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    trials = sum(step() for _ in range(args.steps))
+    dt = time.perf_counter() - t0
+    v = trials / dt
+    sample = (f'{args.particles} replicas x {per_step} generations per step, generations spread evenly over the '
+              f'{args.generations}-generation schedule; FP64 oracle port, OpenMP over replicas')
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'trial structures evaluated/s', 'value': v, 'unit': 'trials/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000 * dt / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': f'wyckoff-search Pnma PbSO4-like, {args.particles} replicas x {args.generations} '
+                               f'generations (sampled), d_min 1.2 A'},
+        'cpu_baseline': {'value': v, 'unit': 'trials/s', 'cores': O.num_threads(), 'kind': 'port', 'sample': sample},
+        'e2e': {'value': v, 'unit': 'trials/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == 'reference':
+        run_reference(args, world, rank)
+        return
+    import torch
+    from powder6_b200.swarm_wyckoff import (WyckoffSession, build_ladders, initial_state, project_all,
+                                            schedule)
+    from powder6_b200.workloads import mulberry32, wyckoff_problem
+    torch.cuda.set_device(local)
+    P = wyckoff_problem(seed=1)
+    n = args.particles
+    G = args.generations
+    groups, pen = schedule(G, P.refl.n_groups)
+    sess = WyckoffSession(P, n, run_key=1000 + rank, cos_mode=args.cos_mode, device=local)
+    assign = np.zeros(n, dtype=np.uint32)
+    sess.set_assign(assign)
+    ladders, temps = build_ladders(assign)
+    sess.set_ladders(ladders, 8)
+    sess.set_schedule(groups, pen)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    rnd = mulberry32(20261026 + rank)
+
+    def fresh_inputs():
+        pos = project_all(P, np.array([rnd() for _ in range(n * sess.coords_per_particle)], dtype=np.float32), assign)
+        st = initial_state(n, temps, rnd)
+        return pos, st
+
+    def device_step(pos, st):
+        sess.sync_state(pos, st)           # inputs resident before the timed kernel
+        flush.zero_()
+        torch.cuda.synchronize()
+        sess.run(0, G, SWAP_EVERY, True)
+        sess.synchronize(600)
+        return sess.last_kernel_ms()
+
+    inputs = [fresh_inputs() for _ in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        device_step(*inputs[i])
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = sess.launch_count()
+    with ClockSampler(local) as clk:
+        times = [device_step(*inputs[args.warmup + i]) for i in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = sess.launch_count() - l0
+    total_ms = max_over_ranks(float(sum(times)), world)
+    trials_per_step = n * G
+    value = world * trials_per_step * args.steps / (total_ms / 1000.0)
+    # end to end through the host-buffer C-ABI call: upload, search, read back
+    pos, st = inputs[-1]
+    torch.cuda.synchronize()
+    e2e_times = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        sess.run_host(pos, st, 0, G, SWAP_EVERY, True)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = max_over_ranks(float(sum(e2e_times)), world)
+    e2e_value = world * trials_per_step * args.steps / e2e_total
+    h2d = n * sess.coords_per_particle * 4 + n * 48
+    d2h = 2 * n * sess.coords_per_particle * 4 + n * 48
+    if rank == 0:
+        clocks = clk.summary()
+        cos_total, nsteps = algorithmic_cos(P, groups, n)
+        ms = float(np.mean(times))
+        achieved = cos_total / (ms / 1000.0) / 1e9
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clocks['sm_mhz'] or 1965.0
+        peak = MUFU_PER_CLK_PER_SM * nsm * mhz * 1e6 / 1e9
+        traffic = None
+        tf = ROOT / 'profiles' / 'wy_kernel_traffic.json'
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get('bytes_per_launch')
+        line = {
+            'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp32', 'data': 'synthetic',
+            'config': {'workload': f'wyckoff-search Pnma PbSO4-like (Pb 4c, S 4c, O 4c, O 4c, O 8d; 24 atoms/cell), '
+                                   f'{n} replicas x {G} generations per GPU, d_min 1.2 A '
+                                   f'({P.refl.n_refl} reflections, {P.refl.n_groups} groups)',
+                       'replicas_per_gpu': n, 'generations': G, 'step': 'one full search, one launch',
+                       'l2': 'flushed before every step (256 MB write)', 'cos': ['sfu', 'poly'][args.cos_mode],
+                       'parallelism': f'replicas only x{world}'},
+            'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak, 'unit': 'Gcos/s',
+                         'frac': achieved / peak, 'traffic': traffic,
+                         'note': f'{cos_total:.4g} algorithmic cosines per launch; peak = {MUFU_PER_CLK_PER_SM} '
+                                 f'SFU ops/clk/SM x {nsm} SMs x {mhz:.0f} MHz (median SM clock under load)'},
+            'e2e': {'value': e2e_value, 'unit': 'trials/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line['cpu_baseline'] = cpu_baseline(P, groups, pen, n)
+        print(json.dumps(line), flush=True)
+    sess.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

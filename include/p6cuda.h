@@ -1,0 +1,194 @@
+/*
+ * libp6cuda -- C ABI of the B200 trial-evaluation backend for Powder 6.
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary.  Every
+ * function returns a p6_status; on failure p6_last_error() returns a message
+ * for the calling thread.  Sessions are opaque, own their device memory and one
+ * CUDA stream, and are safe to use from one thread at a time.
+ *
+ * Reference interfaces replaced (paths inside nitad54448/powder6):
+ *   Wyckoff search device layer   js/swarm_wyckoff.js:1293-1720
+ *                                 (buffers, dispatchCoords, evaluateCoordsSync,
+ *                                  readStateFromGPU, syncStateToGPU) and the
+ *                                 kernel swarm_reflection.wgsl:601-1270
+ *   Parallel-tempering backend    js/pt_gpu.js:371-423 (RVPTGPU.create / costs /
+ *                                 batch / run)
+ */
+#ifndef P6CUDA_H
+#define P6CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes.  The JS/Python host maps every non-OK code to the reference's
+ * fallback behaviour (throw -> CPU PT; Wyckoff -> 'wy-error'). */
+typedef enum {
+  P6_OK = 0,
+  P6_ERR_INVALID_ARG = 1,
+  P6_ERR_CAPACITY = 2,
+  P6_ERR_DEVICE_LOST = 3,
+  P6_ERR_TIMEOUT = 4,
+  P6_ERR_NOT_CONVERGED = 5,
+  P6_ERR_VALIDATION = 6,
+  P6_ERR_CUDA = 7
+} p6_status;
+
+/* Message of the last failure on this thread ("" when none). */
+const char *p6_last_error(void);
+/* ABI version, bumped whenever a struct below changes layout. */
+int p6_abi_version(void);
+/* Host-side fault injection for failure-path tests: after `after_calls` more
+ * entry-point calls, return `code` once (0 disables).  Never touches a GPU. */
+void p6_debug_inject_failure(int code, int after_calls);
+
+/* ======================================================================== */
+/* Wyckoff search                                                            */
+/* ======================================================================== */
+
+/* Per-particle Metropolis state, 48 bytes, the layout of ParticleState in
+ * swarm_reflection.wgsl:65-87 and SW_STATE_STRIDE (js/swarm_wyckoff.js:45). */
+typedef struct {
+  float fit;       /* cc - pen * penScale at the scale it was measured */
+  float cc;        /* 1 - wR2 */
+  float pen;       /* raw penalty, at weight 1 */
+  float step_size; /* proposal width, fractional coordinates */
+  float temp;      /* rung temperature */
+  uint32_t seed;   /* per-chain key of the counter-based generator */
+  uint32_t accepted;
+  uint32_t pad;
+  float best_fit;  /* -1e30: nothing recorded yet */
+  float best_cc;
+  float best_pen;
+  float best_pad;
+} p6_wy_particle_state;
+
+/* Static problem description: the packed arrays js/swarm_wyckoff.js:1293-1548
+ * uploads, in the reference layouts, plus the kernel constants swInject
+ * (js/swarm_wyckoff.js:201-282) compiles in. */
+typedef struct {
+  int num_particles;
+  /* genPack: site | op << 8 | type << 20 | skip << 24, n_assign * n_tot */
+  const uint32_t *gen_pack;
+  int n_assign;
+  int n_tot;
+  /* symmetry operators, 12 floats each: r[9] row-major then t[3] */
+  const float *sym_packed;
+  int n_ops;
+  /* per (assignment, site): P[9], T[3]; max_sites is the row stride */
+  const float *site_proj;
+  int max_sites;
+  /* reflections: packed hkl (10 bits each, +512 bias), multiplicity */
+  const uint32_t *refl_pack;
+  int n_refl;
+  /* groups: start, count, Iobs[, weight]; stride 3 or 4 */
+  const float *group_meta;
+  int n_groups;
+  int group_stride;
+  /* scattering factors f(s) exp(-B s^2/4), n_refl * n_elem */
+  const float *f_tab;
+  int n_elem;
+  /* restraint table [zByType | rMin (n_elem^2) | rules (7 floats each)] */
+  const float *restraint_tables;
+  int n_restraint_floats;
+  int r_min_off;
+  int rule_off;
+  int n_rules;
+  int max_coord_slots; /* slot capacity (>= the slots the rules claim), <= 256 */
+  int geom_slots;      /* == max_coord_slots when any rule has a shape, else 1 */
+  /* contact geometry: reduced-basis orth (fractional -> Cartesian) and the
+   * integer change of basis, both row-major; inv_orth is Cartesian ->
+   * fractional of the cell's own basis (polyhedron moves) */
+  double orth[9];
+  double xform[9];
+  double inv_orth[9];
+  int min_image_shell; /* 0 or 1 */
+  int count_shell;     /* 0 or 1 */
+  int centro;          /* (-I|0) in the group: F is real */
+  float pen_clash, pen_bond, pen_coord, pen_geom, poly_prob;
+  /* Robbins-Monro step adaptation (exp(a(1-t)), exp(-a t)) and bounds */
+  float step_up, step_down, step_min, step_max;
+  /* fitness arithmetic: 0 = SFU cosine on the integer-reduced phase,
+   * 1 = FMA-pipe polynomial (slower, closer to FP64) */
+  int cos_mode;
+  uint32_t run_key; /* key of the counter-based generator for this session */
+} p6_wy_problem;
+
+typedef struct p6_wy_session p6_wy_session;
+
+/* Creates the device buffers and uploads the static tables
+ * (js/swarm_wyckoff.js:1293-1548).  `device` is a CUDA ordinal. */
+p6_status p6_wy_create(const p6_wy_problem *problem, int device, p6_wy_session **out);
+/* Frees everything the session owns (the finally of js/swarm_wyckoff.js:2637-2645). */
+p6_status p6_wy_destroy(p6_wy_session *s);
+
+/* bufAssign write (js/swarm_wyckoff.js:1767, 2005, 2324). */
+p6_status p6_wy_set_assign(p6_wy_session *s, const uint32_t *assign_of);
+/* Params.nGroupsActive / penScale (js/swarm_wyckoff.js:2223-2230). */
+p6_status p6_wy_set_params(p6_wy_session *s, int n_groups_active, float pen_scale);
+/* syncStateToGPU (js/swarm_wyckoff.js:2160-2185): current coordinates
+ * (num_particles * max_sites * 3 floats) and per-particle state.  Resets the
+ * best-ever half to the current coordinates. */
+p6_status p6_wy_sync_state(p6_wy_session *s, const float *positions, const p6_wy_particle_state *state);
+/* readStateFromGPU (js/swarm_wyckoff.js:1676-1720): current and best-ever
+ * coordinates and the state array.  Any pointer may be NULL. */
+p6_status p6_wy_read_state(p6_wy_session *s, float *positions, float *best_positions, p6_wy_particle_state *state);
+/* dispatchCoords(coords, isMCMC) (js/swarm_wyckoff.js:1558-1571): one
+ * generation for every particle; coords (may be NULL) replaces the current
+ * coordinates first.  Asynchronous. */
+p6_status p6_wy_dispatch(p6_wy_session *s, const float *coords, int mcmc);
+/* evaluateCoordsSync (js/swarm_wyckoff.js:1643-1667): dispatch then read fit
+ * (first num_particles floats) and cc (next num_particles floats). */
+p6_status p6_wy_evaluate_sync(p6_wy_session *s, const float *coords, int mcmc, float *fit_cc);
+
+/* B200 path: run generations [gen0, gen0 + n_gen) of a schedule entirely on
+ * the device.  Each CTA owns one replica ladder (rungs consecutive entries
+ * of `ladders`, -1 for an empty rung), so the exchange sweep every
+ * `swap_every` generations (js/swarm_wyckoff.js:1825-1851) runs inside the CTA
+ * without a host round trip.  sched_groups/sched_pen hold nGroupsActive and
+ * penScale per generation (length >= gen0 + n_gen); a change of nGroupsActive
+ * re-measures the current state first (js/swarm_wyckoff.js:2226-2256), and
+ * reeval_first != 0 does so before generation gen0 as well (the first
+ * generation of a restart, or a chunk that starts on a ramp step). */
+p6_status p6_wy_set_ladders(p6_wy_session *s, const int32_t *ladders, int n_ladders, int rungs);
+p6_status p6_wy_set_schedule(p6_wy_session *s, const int32_t *sched_groups, const float *sched_pen, int n_gen);
+p6_status p6_wy_run(p6_wy_session *s, int gen0, int n_gen, int swap_every, int reeval_first);
+/* Host-buffer form of p6_wy_run: uploads positions/state, runs, reads them back
+ * (copies inside the call). */
+p6_status p6_wy_run_host(p6_wy_session *s, const float *positions_in, const p6_wy_particle_state *state_in,
+                         int gen0, int n_gen, int swap_every, int reeval_first, float *positions_out,
+                         float *best_out, p6_wy_particle_state *state_out);
+
+/* Waits for the session's stream, polling with a deadline (P6_ERR_TIMEOUT). */
+p6_status p6_wy_synchronize(p6_wy_session *s, double timeout_seconds);
+/* Exact coordinate access in the kernel's 32-bit fixed point (x * 2^32). */
+p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current);
+p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best);
+/* Parity support: record, for the next dispatch, each particle's proposal
+ * (max_sites * 3 fixed-point words) and a record of 8 floats
+ * {f_new, cc, pen_scaled, u, accepted, f_old, temp, step_before}. */
+p6_status p6_wy_set_trace(p6_wy_session *s, int enable);
+p6_status p6_wy_read_trace(p6_wy_session *s, uint32_t *proposals, float *records);
+/* mult * |F|^2 of every reflection of each particle's last traced evaluation
+ * (num_particles * n_refl floats; reflections past the active groups untouched). */
+p6_status p6_wy_read_trace_ic(p6_wy_session *s, float *ic);
+/* The generated cell of one particle's current coordinates, in genPack order,
+ * fixed point (n_tot * 3 words). */
+p6_status p6_wy_debug_expand(p6_wy_session *s, int particle, uint32_t *atoms);
+/* Milliseconds of the last p6_wy_run / p6_wy_dispatch kernel (CUDA events on
+ * the session stream). */
+p6_status p6_wy_last_kernel_ms(p6_wy_session *s, float *ms);
+/* Kernel launches made by this session so far. */
+p6_status p6_wy_launch_count(p6_wy_session *s, long long *count);
+
+/* Philox4x32-10 of one (counter, key) on the device: known-answer check. */
+p6_status p6_philox_device(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* P6CUDA_H */

@@ -1,0 +1,204 @@
+"""ORACLE -- test infrastructure, not product code.
+
+ctypes access to libp6oracle.so, the FP64 CPU restatement of the reference's
+trial evaluation (see p6_oracle_wyckoff.c for the functions and the reference
+lines each follows).  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg import this module; the product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / 'libp6oracle.so'
+
+
+class Geom(C.Structure):
+    _fields_ = [('o', C.c_double * 9), ('r', C.c_double * 9), ('minImageShell', C.c_int), ('countShell', C.c_int),
+                ('penClash', C.c_double), ('penBond', C.c_double), ('penCoord', C.c_double),
+                ('penGeom', C.c_double), ('penScale', C.c_double)]
+
+
+class Problem(C.Structure):
+    _fields_ = [('genPack', C.c_void_p), ('symPacked', C.c_void_p), ('siteProj', C.c_void_p),
+                ('reflPack', C.c_void_p), ('groupMeta', C.c_void_p), ('fTab', C.c_void_p), ('tables', C.c_void_p),
+                ('nTot', C.c_int), ('maxSites', C.c_int), ('nElem', C.c_int), ('nGroupsActive', C.c_int),
+                ('stride', C.c_int), ('rMinOff', C.c_int), ('ruleOff', C.c_int), ('nRules', C.c_int),
+                ('maxCoordSlots', C.c_int), ('geomSlots', C.c_int), ('centro', C.c_int),
+                ('stepUp', C.c_double), ('stepDown', C.c_double), ('stepMin', C.c_double), ('stepMax', C.c_double)]
+
+
+_lib = None
+
+
+def build():
+    if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in HERE.glob('*.c')):
+        subprocess.run(['make', '-s', '-C', str(HERE)], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = C.CDLL(str(LIB))
+        P = C.c_void_p
+        lib.p6o_wy_fitness.restype = C.c_double
+        lib.p6o_wy_fitness.argtypes = [P, C.c_int, P, P, C.c_int, P, P, C.c_int, C.c_int, P, P, C.c_int, C.c_int, P]
+        lib.p6o_wy_fitness_projected.restype = C.c_double
+        lib.p6o_wy_fitness_projected.argtypes = [P, P, C.c_int, P, P, C.c_int, C.c_int, P, P, C.c_int, C.c_int, P]
+        lib.p6o_wy_expand_fixed.restype = None
+        lib.p6o_wy_expand_fixed.argtypes = [P, P, C.c_int, P, P, P]
+        lib.p6o_wy_penalty_sites.restype = C.c_double
+        lib.p6o_wy_penalty_sites.argtypes = [P, P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, C.POINTER(Geom)]
+        lib.p6o_wy_accept.restype = C.c_int
+        lib.p6o_wy_accept.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.POINTER(C.c_int)]
+        lib.p6o_wy_generation.restype = C.c_long
+        lib.p6o_wy_generation.argtypes = [C.POINTER(Problem), C.POINTER(Geom), C.c_int, P, P, P, P, C.c_int]
+        lib.p6o_num_threads.restype = C.c_int
+        lib.p6o_num_threads.argtypes = []
+        if hasattr(lib, 'p6o_philox'):
+            lib.p6o_philox.restype = None
+            lib.p6o_philox.argtypes = [P, P, P]
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def wy_fitness(coords, site_proj_row, gen_pack_row, sym_packed, group_meta, n_groups, stride, refl_pack, f_tab,
+               n_elem, centro):
+    """swFitnessOnCpu: returns (cc, (scc, soo, sco))."""
+    lib = load()
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    sp = np.ascontiguousarray(site_proj_row, dtype=np.float32)
+    gp = np.ascontiguousarray(gen_pack_row, dtype=np.uint32)
+    sums = np.zeros(3)
+    cc = lib.p6o_wy_fitness(_p(coords), len(coords) // 3, _p(sp), _p(gp), len(gp), _p(sym_packed),
+                            _p(group_meta), n_groups, stride, _p(refl_pack), _p(f_tab), n_elem, int(centro),
+                            _p(sums))
+    return cc, tuple(sums)
+
+
+def wy_fitness_projected(proj, gen_pack_row, sym_packed, group_meta, n_groups, stride, refl_pack, f_tab, n_elem,
+                         centro):
+    lib = load()
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    gp = np.ascontiguousarray(gen_pack_row, dtype=np.uint32)
+    sums = np.zeros(3)
+    cc = lib.p6o_wy_fitness_projected(_p(proj), _p(gp), len(gp), _p(sym_packed), _p(group_meta), n_groups, stride,
+                                      _p(refl_pack), _p(f_tab), n_elem, int(centro), _p(sums))
+    return cc, tuple(sums)
+
+
+def expand_fixed(site_x, gen_pack_row, rint, tfix):
+    lib = load()
+    site_x = np.ascontiguousarray(site_x, dtype=np.uint32)
+    gp = np.ascontiguousarray(gen_pack_row, dtype=np.uint32)
+    rint = np.ascontiguousarray(rint, dtype=np.int32)
+    tfix = np.ascontiguousarray(tfix, dtype=np.uint32)
+    out = np.zeros(len(gp) * 3, dtype=np.uint32)
+    lib.p6o_wy_expand_fixed(_p(site_x), _p(gp), len(gp), _p(rint), _p(tfix), _p(out))
+    return out
+
+
+def make_geom(orth, xform, min_image_shell, count_shell, pen_clash, pen_bond, pen_coord, pen_geom, pen_scale):
+    g = Geom()
+    for i in range(9):
+        g.o[i] = float(orth[i])
+        g.r[i] = float(xform[i])
+    g.minImageShell = int(min_image_shell)
+    g.countShell = int(count_shell)
+    g.penClash, g.penBond, g.penCoord, g.penGeom, g.penScale = (float(pen_clash), float(pen_bond),
+                                                                  float(pen_coord), float(pen_geom), float(pen_scale))
+    return g
+
+
+def wy_penalty(proj, gen_pack_row, sym_packed, n_elem, tables, r_min_off, rule_off, n_rules, max_coord_slots,
+               geom_slots, geom):
+    lib = load()
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    gp = np.ascontiguousarray(gen_pack_row, dtype=np.uint32)
+    tables = np.ascontiguousarray(tables, dtype=np.float32)
+    return lib.p6o_wy_penalty_sites(_p(proj), _p(gp), len(gp), _p(sym_packed), n_elem, _p(tables), r_min_off,
+                                    rule_off, n_rules, max_coord_slots, geom_slots, C.byref(geom))
+
+
+def wy_accept(state8, cc, pen, pen_scale, u, step_up, step_down, step_min, step_max):
+    lib = load()
+    st = np.ascontiguousarray(state8, dtype=np.float64).copy()
+    bu = C.c_int(0)
+    acc = lib.p6o_wy_accept(_p(st), cc, pen, pen_scale, u, step_up, step_down, step_min, step_max, C.byref(bu))
+    return acc, st, bu.value
+
+
+def num_threads():
+    return load().p6o_num_threads()
+
+
+class WyckoffCpuRunner:
+    """Whole generations of the Wyckoff search on the host cores (FP64, OpenMP
+    over replicas): the timed CPU baseline.  Holds the packed arrays alive."""
+
+    def __init__(self, P, n_particles, seed=1, n_threads=0, step_up=None, step_down=None):
+        import math as _m
+        self.lib = load()
+        self.P = P
+        self.n = int(n_particles)
+        self.keep = []
+
+        def k(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self.keep.append(a)
+            return a.ctypes.data
+
+        pr = Problem()
+        pr.genPack = k(P.tables.gen_pack, np.uint32)
+        pr.symPacked = k(P.sym_packed, np.float32)
+        pr.siteProj = k(P.tables.site_proj, np.float32)
+        pr.reflPack = k(P.refl.refl_pack, np.uint32)
+        pr.groupMeta = k(P.refl.group_meta, np.float32)
+        pr.fTab = k(P.f_tab, np.float32)
+        pr.tables = k(P.restraints.tables, np.float32)
+        pr.nTot, pr.maxSites, pr.nElem = P.n_tot, P.max_sites, P.n_elem
+        pr.nGroupsActive, pr.stride = P.refl.n_groups, P.refl.group_stride
+        pr.rMinOff, pr.ruleOff, pr.nRules = P.restraints.r_min_off, P.restraints.rule_off, P.restraints.n_rules
+        pr.maxCoordSlots = max(64, P.restraints.slots_needed)
+        pr.geomSlots = pr.maxCoordSlots if P.restraints.geometry else 1
+        pr.centro = 1 if P.centro else 0
+        pr.stepUp = step_up if step_up is not None else _m.exp(0.08 * 0.7)
+        pr.stepDown = step_down if step_down is not None else _m.exp(-0.08 * 0.3)
+        pr.stepMin, pr.stepMax = 2e-4, 0.5
+        self.pr = pr
+        rng = np.random.default_rng(seed)
+        ms = P.max_sites
+        sp = P.tables.site_proj[:ms * 12].astype(np.float64).reshape(ms, 12)
+        raw = rng.random((self.n, ms, 3))
+        pos = np.einsum('sij,nsj->nsi', sp[:, :9].reshape(ms, 3, 3), raw) + sp[:, 9:]
+        self.pos = np.ascontiguousarray((pos - np.floor(pos)).reshape(-1))
+        self.assign = np.zeros(self.n, dtype=np.uint32)
+        R = 8
+        ratio = (0.05 / 5e-4) ** (1 / (R - 1))
+        st = np.zeros((self.n, 8))
+        st[:, 0] = -1e30
+        st[:, 3] = 0.08
+        st[:, 4] = [5e-4 * ratio ** (i % R) for i in range(self.n)]
+        st[:, 5] = -1e30
+        self.st = np.ascontiguousarray(st.reshape(-1))
+        self.seeds = rng.integers(1, 2 ** 32 - 1, size=self.n, dtype=np.uint64).astype(np.uint32)
+        self.n_threads = int(n_threads)
+
+    def generation(self, n_groups_active, pen_scale):
+        self.pr.nGroupsActive = int(n_groups_active)
+        P = self.P
+        g = make_geom(P.orth, P.xform, P.min_image_shell, 1, P.pen_clash, P.pen_bond, P.pen_coord, P.pen_geom,
+                      pen_scale)
+        return self.lib.p6o_wy_generation(C.byref(self.pr), C.byref(g), self.n, _p(self.pos), _p(self.assign),
+                                          _p(self.st), _p(self.seeds), self.n_threads)

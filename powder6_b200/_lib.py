@@ -1,0 +1,121 @@
+"""ctypes binding of libp6cuda.so (declared in include/p6cuda.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+the shared library is missing or cannot be loaded, every product entry point
+raises P6Error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / 'libp6cuda.so'
+
+P6_OK = 0
+STATUS_NAMES = {0: 'OK', 1: 'INVALID_ARG', 2: 'CAPACITY', 3: 'DEVICE_LOST', 4: 'TIMEOUT', 5: 'NOT_CONVERGED',
+                6: 'VALIDATION', 7: 'CUDA'}
+
+
+class P6Error(RuntimeError):
+    def __init__(self, code: int, message: str):
+        self.code = code
+        self.status = STATUS_NAMES.get(code, str(code))
+        super().__init__(f'p6 {self.status}: {message}')
+
+
+class P6WyParticleState(C.Structure):
+    _fields_ = [('fit', C.c_float), ('cc', C.c_float), ('pen', C.c_float), ('step_size', C.c_float),
+                ('temp', C.c_float), ('seed', C.c_uint32), ('accepted', C.c_uint32), ('pad', C.c_uint32),
+                ('best_fit', C.c_float), ('best_cc', C.c_float), ('best_pen', C.c_float), ('best_pad', C.c_float)]
+
+
+class P6WyProblem(C.Structure):
+    _fields_ = [('num_particles', C.c_int),
+                ('gen_pack', C.POINTER(C.c_uint32)), ('n_assign', C.c_int), ('n_tot', C.c_int),
+                ('sym_packed', C.POINTER(C.c_float)), ('n_ops', C.c_int),
+                ('site_proj', C.POINTER(C.c_float)), ('max_sites', C.c_int),
+                ('refl_pack', C.POINTER(C.c_uint32)), ('n_refl', C.c_int),
+                ('group_meta', C.POINTER(C.c_float)), ('n_groups', C.c_int), ('group_stride', C.c_int),
+                ('f_tab', C.POINTER(C.c_float)), ('n_elem', C.c_int),
+                ('restraint_tables', C.POINTER(C.c_float)), ('n_restraint_floats', C.c_int),
+                ('r_min_off', C.c_int), ('rule_off', C.c_int), ('n_rules', C.c_int),
+                ('max_coord_slots', C.c_int), ('geom_slots', C.c_int),
+                ('orth', C.c_double * 9), ('xform', C.c_double * 9), ('inv_orth', C.c_double * 9),
+                ('min_image_shell', C.c_int), ('count_shell', C.c_int), ('centro', C.c_int),
+                ('pen_clash', C.c_float), ('pen_bond', C.c_float), ('pen_coord', C.c_float),
+                ('pen_geom', C.c_float), ('poly_prob', C.c_float),
+                ('step_up', C.c_float), ('step_down', C.c_float), ('step_min', C.c_float), ('step_max', C.c_float),
+                ('cos_mode', C.c_int), ('run_key', C.c_uint32)]
+
+
+_P = C.c_void_p
+_SIGS = {
+    'p6_last_error': (C.c_char_p, []),
+    'p6_abi_version': (C.c_int, []),
+    'p6_debug_inject_failure': (None, [C.c_int, C.c_int]),
+    'p6_philox_device': (C.c_int, [_P, _P, _P]),
+    'p6_wy_create': (C.c_int, [C.POINTER(P6WyProblem), C.c_int, C.POINTER(C.c_void_p)]),
+    'p6_wy_destroy': (C.c_int, [_P]),
+    'p6_wy_set_assign': (C.c_int, [_P, _P]),
+    'p6_wy_set_params': (C.c_int, [_P, C.c_int, C.c_float]),
+    'p6_wy_sync_state': (C.c_int, [_P, _P, _P]),
+    'p6_wy_read_state': (C.c_int, [_P, _P, _P, _P]),
+    'p6_wy_dispatch': (C.c_int, [_P, _P, C.c_int]),
+    'p6_wy_evaluate_sync': (C.c_int, [_P, _P, C.c_int, _P]),
+    'p6_wy_set_ladders': (C.c_int, [_P, _P, C.c_int, C.c_int]),
+    'p6_wy_set_schedule': (C.c_int, [_P, _P, _P, C.c_int]),
+    'p6_wy_run': (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
+    'p6_wy_run_host': (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P]),
+    'p6_wy_synchronize': (C.c_int, [_P, C.c_double]),
+    'p6_wy_write_positions_fixed': (C.c_int, [_P, _P]),
+    'p6_wy_read_positions_fixed': (C.c_int, [_P, _P, _P]),
+    'p6_wy_set_trace': (C.c_int, [_P, C.c_int]),
+    'p6_wy_read_trace': (C.c_int, [_P, _P, _P]),
+    'p6_wy_read_trace_ic': (C.c_int, [_P, _P]),
+    'p6_wy_debug_expand': (C.c_int, [_P, C.c_int, _P]),
+    'p6_wy_last_kernel_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
+    'p6_wy_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+}
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Load libp6cuda.so; builds it in-tree when missing and nvcc is present."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists() and build_if_missing:
+        from . import build as _build
+        try:
+            _build.build()
+        except Exception as e:  # no toolchain on this machine
+            raise P6Error(7, f'libp6cuda.so is missing and could not be built: {e}') from e
+    if not LIB_PATH.exists():
+        raise P6Error(7, f'libp6cuda.so not found at {LIB_PATH}')
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols():
+    return list(_SIGS)
+
+
+def check(status: int):
+    if status != P6_OK:
+        msg = load().p6_last_error()
+        raise P6Error(status, msg.decode() if msg else '')
+
+
+def ptr(a):
+    """numpy array -> void* (None passes NULL)."""
+    if a is None:
+        return None
+    return C.c_void_p(a.ctypes.data)

@@ -1,0 +1,1527 @@
+// Wyckoff-search trial evaluation on sm_100a.
+//
+// One generation of the reference kernel (swarm_reflection.wgsl:601-1270) per
+// replica: proposal (one free site with p = 3/4, else every site), projection
+// onto the Wyckoff subspace, symmetry expansion, grouped |F|^2 against the
+// observed group intensities, the scale-free weighted wR2, clash and
+// restraint penalties, Metropolis acceptance, Robbins-Monro step adaptation
+// and the best-ever cache.  The layout is B200-first rather than a
+// translation:
+//
+//  * one warp owns one replica; one CTA owns one replica ladder (the rungs of
+//    one assignment, js/swarm_wyckoff.js:1784-1808), so the exchange sweep
+//    (js/swarm_wyckoff.js:1825-1851) is a CTA barrier plus a shared-memory
+//    swap, and a whole block of generations -- or a whole search -- is one
+//    launch with no host round trip;
+//  * coordinates are 32-bit fixed point (x * 2^32).  The orbit image
+//    R x + t, the phase h.x mod 1 and the minimum-image separation are exact
+//    integer arithmetic; only the final cosine is floating point (the SFU's
+//    cos.approx on the exactly reduced turn, or an FMA-pipe polynomial);
+//  * the static reflection, scattering-factor and group tables are staged
+//    into shared memory once per CTA with the bulk-copy engine;
+//  * the group sums scc, soo, sco are accumulated and reduced in FP64;
+//  * random numbers are Philox4x32-10 keyed by (chain seed, session key) and
+//    counted by (generation, replica, lane, purpose): no generator state.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "p6_common.cuh"
+
+namespace p6 {
+namespace wy {
+
+constexpr int kMaxSites = 32;
+constexpr int kMaxElem = 8;
+constexpr int kMaxRules = 32;
+constexpr int kMaxRungs = 32;
+constexpr float kNoNeighbour = 1.0e9f;
+constexpr float kNoPartnerCharge = 5.0f;
+constexpr float kCoordSoftA = 0.25f;
+constexpr double kTwoPow32 = 4294967296.0;
+constexpr float kTurnToRad = 1.46291807926715968e-09f;  // 2 pi / 2^32
+constexpr uint32_t kStageWaitLimit = 1u << 24;
+
+struct OpFix {
+  int r[9];
+  uint32_t t[3];
+};
+
+struct ProjFix {
+  int num[9];
+  int den;
+  uint32_t t[3];
+  int pad[2];
+};
+
+struct RuleDev {
+  int a, b;
+  float dmin, dmax, count;
+  int mode, geom, pad;
+};
+
+struct ReflRec {  // 8 bytes
+  short h, k, l;
+  unsigned short mult;
+};
+
+struct PState {  // mirror of p6_wy_particle_state
+  float fit, cc, pen, step, temp;
+  uint32_t seed, accepted, pad;
+  float bestFit, bestCC, bestPen, bestPad;
+};
+static_assert(sizeof(PState) == 48, "state stride");
+
+struct Params {
+  const uint32_t *gen;     // reordered genPack per assignment: F atoms (site runs) first
+  const int4 *runs;        // per assignment, kMaxSites runs {start, end, type, site}
+  const int *nRuns;        // per assignment
+  const int *nF;           // per assignment: atoms entering |F|^2
+  const uint32_t *freeMask;
+  const OpFix *ops;
+  const ProjFix *proj;     // per (assignment, site)
+  const unsigned char *blob;  // staged static tables
+  int blobBytes, offRefl, offF, offGroup, offRmin;
+  const RuleDev *rules;
+  int nRules;
+  int numParticles, nTot, maxSites, nRefl, nGroups, nElem, nAssign;
+  float orth[9];
+  int xf[9];
+  int minImageShell, countShell, centro, maxCoordSlots, geomSlots;
+  float penClash, penBond, penCoord, penGeom;
+  float stepUp, stepDown, stepMin, stepMax;
+  uint32_t runKey;
+  uint32_t *pos;           // [2][numParticles][maxSites*3]
+  PState *st;
+  const uint32_t *assign;
+  const int *ladders;      // nLadders * rungs, -1 empty; null: consecutive particles
+  int rungs, nLadders;
+  const int *schedGroups;  // per generation; null: use ngaArg/penArg
+  const float *schedPen;
+  int ngaArg;
+  float penArg;
+  uint32_t *tracePos;
+  float *traceRec;
+  float *traceIc;          // per particle, nRefl: mult |F|^2 of the last evaluation
+  unsigned long long *swapStats;  // [tried, taken]
+  int *errFlag;
+  int warpSmemBytes;       // per-warp shared-memory slice
+  int atomsOff, icOff;     // offsets inside the slice
+};
+
+// ---------------------------------------------------------------------------
+// Cosine / sine of a 32-bit turn.
+// ---------------------------------------------------------------------------
+// cos(2 pi t) and sin(2 pi t) with the SFU: the turn is already reduced
+// exactly, so the hardware sees an argument in [-pi, pi).
+__device__ __forceinline__ float cos_turn_sfu(uint32_t ph) {
+  return __cosf((float)(int)ph * kTurnToRad);
+}
+__device__ __forceinline__ void sincos_turn_sfu(uint32_t ph, float *s, float *c) {
+  __sincosf((float)(int)ph * kTurnToRad, s, c);
+}
+
+// Polynomial form: quarter-turn reduction in integers, then Taylor series of
+// sin and cos of phi = x pi / 2, |x| <= 1/2 (truncation below 2e-9).
+constexpr double kHalfPi = 1.57079632679489661923;
+__device__ __forceinline__ void sincos_turn_poly(uint32_t ph, float *s_out, float *c_out) {
+  uint32_t q = (ph + 0x20000000u) >> 30;
+  int r = (int)(ph - (q << 30));
+  float x = (float)r * (1.0f / 1073741824.0f);
+  float x2 = x * x;
+  constexpr double a = kHalfPi;
+  constexpr float S0 = (float)a, S1 = (float)(-a * a * a / 6.0), S2 = (float)(a * a * a * a * a / 120.0),
+                  S3 = (float)(-a * a * a * a * a * a * a / 5040.0),
+                  S4 = (float)(a * a * a * a * a * a * a * a * a / 362880.0);
+  constexpr float C1 = (float)(-a * a / 2.0), C2 = (float)(a * a * a * a / 24.0),
+                  C3 = (float)(-a * a * a * a * a * a / 720.0),
+                  C4 = (float)(a * a * a * a * a * a * a * a / 40320.0),
+                  C5 = (float)(-a * a * a * a * a * a * a * a * a * a / 3628800.0);
+  float sp = x * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, S4, S3), S2), S1), S0);
+  float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, C5, C4), C3), C2), C1), 1.0f);
+  float cs = (q & 1u) ? sp : cp;
+  float sn = (q & 1u) ? cp : sp;
+  if ((q + 1u) & 2u) cs = -cs;   // q = 1, 2
+  if (q & 2u) sn = -sn;          // q = 2, 3
+  *s_out = sn;
+  *c_out = cs;
+}
+
+template <int COSMODE>
+__device__ __forceinline__ float cos_turn(uint32_t ph) {
+  if (COSMODE == 0) return cos_turn_sfu(ph);
+  float s, c;
+  sincos_turn_poly(ph, &s, &c);
+  return c;
+}
+template <int COSMODE>
+__device__ __forceinline__ void sincos_turn(uint32_t ph, float *s, float *c) {
+  if (COSMODE == 0)
+    sincos_turn_sfu(ph, s, c);
+  else
+    sincos_turn_poly(ph, s, c);
+}
+
+// ---------------------------------------------------------------------------
+// Geometry helpers (fixed point).
+// ---------------------------------------------------------------------------
+// Exact separation i - j in the reduced basis, nearest image, as fractions.
+__device__ __forceinline__ void frac_delta(const Params &P, uint4 a, uint4 b, float q[3]) {
+  int d0 = (int)(a.x - b.x), d1 = (int)(a.y - b.y), d2 = (int)(a.z - b.z);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    uint32_t v = (uint32_t)P.xf[3 * i] * (uint32_t)d0 + (uint32_t)P.xf[3 * i + 1] * (uint32_t)d1 +
+                 (uint32_t)P.xf[3 * i + 2] * (uint32_t)d2;
+    q[i] = (float)(int)v * (1.0f / 4294967296.0f);
+  }
+}
+__device__ __forceinline__ void cart_vec(const Params &P, const float t[3], float c[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) c[i] = P.orth[3 * i] * t[0] + P.orth[3 * i + 1] * t[1] + P.orth[3 * i + 2] * t[2];
+}
+__device__ __forceinline__ float cart_len(const Params &P, const float t[3]) {
+  float c[3];
+  cart_vec(P, t, c);
+  return sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+}
+__device__ __forceinline__ float cart_dist(const Params &P, uint4 a, uint4 b) {
+  float q[3];
+  frac_delta(P, a, b, q);
+  float best = 1e30f;
+  const int S = P.minImageShell;
+  for (int i = -S; i <= S; ++i)
+    for (int j = -S; j <= S; ++j)
+      for (int k = -S; k <= S; ++k) {
+        float t[3] = {q[0] + i, q[1] + j, q[2] + k}, c[3];
+        cart_vec(P, t, c);
+        best = fminf(best, c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      }
+  return sqrtf(best);
+}
+
+__device__ __forceinline__ float geom_cos_error(int code, float c) {
+  switch (code) {
+    case 1: return c + 1.0f;
+    case 2: return c + 0.5f;
+    case 3: return c + 0.3333333f;
+    case 4:
+    case 5: return fminf(fabsf(c), fabsf(c + 1.0f));
+    default: return 0.0f;
+  }
+}
+
+__device__ __forceinline__ int64_t floor_div(int64_t a, int d) {
+  int64_t q = a / d;
+  if ((a % d) != 0 && a < 0) --q;
+  return q;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-level pieces of one trial.
+// ---------------------------------------------------------------------------
+struct WarpSmem {
+  uint32_t cur[kMaxSites * 3];
+  uint32_t prop[kMaxSites * 3];
+  int4 runs[kMaxSites];
+  PState st;
+  int meta[8];  // A, nRuns, nF, nSites, freeMask, particle
+};
+
+// Symmetry expansion of `sites` into atoms[0..nTot) (reordered genPack).
+__device__ __forceinline__ void expand(const Params &P, int A, const uint32_t *sites, uint4 *atoms, int lane) {
+  const uint32_t *gen = P.gen + (size_t)A * P.nTot;
+  const int maxT = max(min(P.nElem, kMaxElem), 1) - 1;
+  for (int i = lane; i < P.nTot; i += 32) {
+    uint32_t w = __ldg(gen + i);
+    int s = w & 0xFF, o = (w >> 8) & 0xFFF, t = min((int)((w >> 20) & 0xF), maxT);
+    const OpFix &op = P.ops[o];
+    uint32_t x = sites[s * 3], y = sites[s * 3 + 1], z = sites[s * 3 + 2];
+    uint4 a;
+    a.x = (uint32_t)op.r[0] * x + (uint32_t)op.r[1] * y + (uint32_t)op.r[2] * z + op.t[0];
+    a.y = (uint32_t)op.r[3] * x + (uint32_t)op.r[4] * y + (uint32_t)op.r[5] * z + op.t[1];
+    a.z = (uint32_t)op.r[6] * x + (uint32_t)op.r[7] * y + (uint32_t)op.r[8] * z + op.t[2];
+    a.w = (uint32_t)t;
+    atoms[i] = a;
+  }
+}
+
+// |F|^2 per reflection into ic[], then group sums (FP64), warp-reduced.
+template <int COSMODE>
+__device__ __forceinline__ void fitness(const Params &P, const WarpSmem &ws, const uint4 *atoms, float *ic,
+                                        const ReflRec *refl, const float *ftab, const float4 *groups, int nga,
+                                        int lane, double sums[3], float *traceIc) {
+  const int nRuns = ws.meta[1];
+  const int nReflAct = nga > 0 ? (int)(groups[nga - 1].x + groups[nga - 1].y) : 0;
+  const bool centro = P.centro != 0;
+  const int nElem = P.nElem;
+  for (int r0 = lane; r0 < nReflAct; r0 += 64) {
+    const int r1 = r0 + 32;
+    const bool has1 = r1 < nReflAct;
+    const ReflRec a0 = refl[r0];
+    const ReflRec a1 = refl[has1 ? r1 : r0];
+    const uint32_t h0 = (uint32_t)(int)a0.h, k0 = (uint32_t)(int)a0.k, l0 = (uint32_t)(int)a0.l;
+    const uint32_t h1 = (uint32_t)(int)a1.h, k1 = (uint32_t)(int)a1.k, l1 = (uint32_t)(int)a1.l;
+    const float *f0 = ftab + (size_t)r0 * nElem;
+    const float *f1 = ftab + (size_t)(has1 ? r1 : r0) * nElem;
+    float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
+    for (int k = 0; k < nRuns; ++k) {
+      const int4 run = ws.runs[k];
+      float c0 = 0.f, s0 = 0.f, c1 = 0.f, s1 = 0.f;
+      if (centro) {
+        for (int a = run.x; a < run.y; ++a) {
+          const uint4 at = atoms[a];
+          c0 += cos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z);
+          c1 += cos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z);
+        }
+      } else {
+        for (int a = run.x; a < run.y; ++a) {
+          const uint4 at = atoms[a];
+          float sa, ca, sb, cb;
+          sincos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z, &sa, &ca);
+          sincos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z, &sb, &cb);
+          c0 += ca; s0 += sa; c1 += cb; s1 += sb;
+        }
+      }
+      const float w0 = f0[run.z], w1 = f1[run.z];
+      fr0 = fmaf(w0, c0, fr0); fi0 = fmaf(w0, s0, fi0);
+      fr1 = fmaf(w1, c1, fr1); fi1 = fmaf(w1, s1, fi1);
+    }
+    ic[r0] = (float)a0.mult * (fr0 * fr0 + fi0 * fi0);
+    if (has1) ic[r1] = (float)a1.mult * (fr1 * fr1 + fi1 * fi1);
+  }
+  __syncwarp();
+  if (traceIc)
+    for (int r = lane; r < nReflAct; r += 32) traceIc[r] = ic[r];
+  double scc = 0.0, soo = 0.0, sco = 0.0;
+  for (int g = lane; g < nga; g += 32) {
+    const float4 gm = groups[g];
+    if (!(gm.w > 0.f)) continue;
+    const int start = (int)gm.x, cnt = (int)gm.y;
+    float iCalc = 0.f;
+    for (int m = 0; m < cnt; ++m) iCalc += ic[start + m];
+    const double w = gm.w, io = gm.z, c = iCalc;
+    scc += w * c * c;
+    soo += w * io * io;
+    sco += w * c * io;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    scc += __shfl_xor_sync(0xffffffffu, scc, o);
+    soo += __shfl_xor_sync(0xffffffffu, soo, o);
+    sco += __shfl_xor_sync(0xffffffffu, sco, o);
+  }
+  sums[0] = scc;
+  sums[1] = soo;
+  sums[2] = sco;
+  __syncwarp();
+}
+
+__device__ __forceinline__ float cc_of(const double sums[3]) {
+  const double den = sums[0] * sums[1];
+  if (!(den > 1e-20) || !(sums[2] > 0.0)) return 0.0f;
+  double ex = fmin(1.0, fmax(0.0, sums[2] * sums[2] / den));
+  double cc = 1.0 - sqrt(fmax(0.0, 1.0 - ex));
+  return (float)fmin(1.0, fmax(0.0, cc));
+}
+
+// Clash penalty only (no distance rules): sum over pairs j > i.
+__device__ __forceinline__ float clash_penalty(const Params &P, const uint4 *atoms, const float *rmin, int lane) {
+  float pen = 0.f;
+  const int n = P.nTot, ne = P.nElem;
+  for (int i = lane; i < n; i += 32) {
+    const uint4 ai = atoms[i];
+    for (int j = i + 1; j < n; ++j) {
+      const uint4 aj = atoms[j];
+      const float dmin = rmin[ai.w * ne + aj.w];
+      const float d = cart_dist(P, ai, aj);
+      if (d < dmin) pen += P.penClash * (1.0f + 9.0f * ((dmin - d) / fmaxf(dmin, 1e-3f)));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pen += __shfl_xor_sync(0xffffffffu, pen, o);
+  return pen;
+}
+
+// Full penalty with distance rules (swarm_reflection.wgsl:913-1128), per-lane
+// slot lists in local memory.  SLOTS is the compiled slot capacity.
+template <int SLOTS>
+__device__ float rule_penalty(const Params &P, const uint4 *atoms, const float *rmin, const float *shellLen,
+                              int lane) {
+  const int nRules = min(P.nRules, kMaxRules);
+  int slotOff[kMaxRules], slotN[kMaxRules];
+  int acc = 0;
+  for (int k = 0; k < nRules; ++k) {
+    slotOff[k] = acc;
+    int nk = 0;
+    if (P.rules[k].mode != 0) nk = min((int)P.rules[k].count, min(P.maxCoordSlots, SLOTS) - acc);
+    nk = max(nk, 0);
+    slotN[k] = nk;
+    acc += nk;
+  }
+  const int slotTotal = acc;
+  const bool shapes = P.geomSlots >= P.maxCoordSlots;
+  float pen = 0.f;
+  const int n = P.nTot, ne = P.nElem;
+  for (int i = lane; i < n; i += 32) {
+    const uint4 ai = atoms[i];
+    const int ti = (int)ai.w;
+    uint32_t myRules = 0;
+    for (int k = 0; k < nRules; ++k)
+      if (P.rules[k].a == ti) myRules |= 1u << k;
+    float nearest[kMaxRules], inWindow[kMaxRules];
+    for (int k = 0; k < kMaxRules; ++k) { nearest[k] = kNoNeighbour; inWindow[k] = 0.f; }
+    float slot[SLOTS];
+    float slotV[SLOTS][3];
+    for (int m = 0; m < slotTotal; ++m) slot[m] = kNoNeighbour;
+    for (int j = 0; j < n; ++j) {
+      const uint4 aj = atoms[j];
+      const int tj = (int)aj.w;
+      const float d = cart_dist(P, ai, aj);
+      if (j != i) {
+        const float dmin = rmin[ti * ne + tj];
+        if (j > i && d < dmin) pen += P.penClash * (1.0f + 9.0f * ((dmin - d) / fmaxf(dmin, 1e-3f)));
+      }
+      if (myRules == 0) continue;
+      float qf[3];
+      frac_delta(P, ai, aj, qf);
+      const float dq = cart_len(P, qf);
+      for (int k = 0; k < nRules; ++k) {
+        if (!(myRules & (1u << k))) continue;
+        const RuleDev &R = P.rules[k];
+        if (R.b != tj) continue;
+        const int nk = slotN[k];
+        const bool counted = nk > 0;
+        if (j != i) nearest[k] = fminf(nearest[k], d);
+        float cutoff = R.dmax;
+        if (counted) cutoff = fmaxf(cutoff, slot[slotOff[k] + nk - 1]);
+        const int S = P.countShell;
+        for (int sa = -S; sa <= S; ++sa)
+          for (int sb = -S; sb <= S; ++sb)
+            for (int sc = -S; sc <= S; ++sc) {
+              const int si = (sa + 1) * 9 + (sb + 1) * 3 + (sc + 1);
+              if (S == 1 && shellLen[si] - dq > cutoff) continue;
+              const float t[3] = {qf[0] + sa, qf[1] + sb, qf[2] + sc};
+              float dv[3];
+              cart_vec(P, t, dv);
+              const float dd = sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+              if (dd < 1.0e-4f && j == i) continue;
+              if (dd >= R.dmin && dd <= R.dmax) inWindow[k] += 1.0f;
+              if (counted) {
+                const int lo = slotOff[k], hi = lo + nk;
+                const bool shaped = shapes && R.geom != 0;
+                if (dd < slot[hi - 1]) {
+                  int m = hi - 1;
+                  while (m > lo && slot[m - 1] > dd) {
+                    slot[m] = slot[m - 1];
+                    if (shaped) { slotV[m][0] = slotV[m - 1][0]; slotV[m][1] = slotV[m - 1][1]; slotV[m][2] = slotV[m - 1][2]; }
+                    --m;
+                  }
+                  slot[m] = dd;
+                  if (shaped) { slotV[m][0] = dv[0]; slotV[m][1] = dv[1]; slotV[m][2] = dv[2]; }
+                  cutoff = fmaxf(R.dmax, slot[hi - 1]);
+                }
+              }
+            }
+      }
+    }
+    for (int k = 0; k < nRules; ++k) {
+      if (!(myRules & (1u << k))) continue;
+      const RuleDev &R = P.rules[k];
+      if (R.mode == 0) {
+        const float nk = nearest[k];
+        if (nk < kNoNeighbour && nk > R.dmax) pen += P.penBond * (nk - R.dmax);
+      } else {
+        const int nk = slotN[k];
+        float deficit = 0.f;
+        for (int m = 0; m < nk; ++m) {
+          const float dm = slot[slotOff[k] + m];
+          if (dm >= kNoNeighbour) deficit += kNoPartnerCharge;
+          else {
+            const float miss = fmaxf(0.f, dm - R.dmax) + fmaxf(0.f, R.dmin - dm);
+            deficit += miss * (1.0f + miss / kCoordSoftA);
+          }
+        }
+        pen += P.penBond * deficit;
+        if (shapes && R.geom != 0 && nk >= 2) {
+          const int lo = slotOff[k];
+          float g = 0.f;
+          for (int m = 0; m + 1 < nk; ++m) {
+            const float dm = slot[lo + m];
+            if (dm >= kNoNeighbour) continue;
+            for (int q = m + 1; q < nk; ++q) {
+              const float dn = slot[lo + q];
+              if (dn >= kNoNeighbour) continue;
+              const float c = (slotV[lo + m][0] * slotV[lo + q][0] + slotV[lo + m][1] * slotV[lo + q][1] +
+                               slotV[lo + m][2] * slotV[lo + q][2]) / fmaxf(dm * dn, 1e-6f);
+              const float e = geom_cos_error(R.geom, c);
+              g += e * e;
+            }
+          }
+          pen += P.penBond * P.penGeom * g;
+        }
+        if (R.mode == 1) pen += P.penCoord * fmaxf(0.f, inWindow[k] - R.count);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pen += __shfl_xor_sync(0xffffffffu, pen, o);
+  return pen;
+}
+
+template <int SLOTS>
+__device__ __forceinline__ float penalty(const Params &P, const uint4 *atoms, const float *rmin,
+                                         const float *shellLen, int lane) {
+  if (SLOTS == 0) return clash_penalty(P, atoms, rmin, lane);
+  return rule_penalty<(SLOTS > 0 ? SLOTS : 1)>(P, atoms, rmin, shellLen, lane);
+}
+
+// Proposal into ws.prop: lane 0 picks the move, lanes < maxSites move and project.
+__device__ __forceinline__ void propose(const Params &P, WarpSmem &ws, int g, int p, int lane, float sd,
+                                        float *uMetro) {
+  const uint2 key = make_uint2(ws.st.seed, P.runKey);
+  int pick = -1;
+  float um = 0.f;
+  if (lane == 0) {
+    const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xFFFFu, 1u), key);
+    const uint32_t free = (uint32_t)ws.meta[4];
+    const int nFree = __popc(free);
+    if (u01(c.x) < 0.75f && nFree > 0) {
+      int k = min(nFree - 1, (int)(u01(c.y) * (float)nFree));
+      uint32_t m = free;
+      for (int i = 0; i < k; ++i) m &= m - 1;
+      pick = __ffs(m) - 1;
+    }
+    um = u01(c.z);
+  }
+  pick = __shfl_sync(0xffffffffu, pick, 0);
+  *uMetro = __shfl_sync(0xffffffffu, um, 0);
+  const int A = ws.meta[0];
+  if (lane < P.maxSites) {
+    const int s = lane;
+    const bool moving = (pick < 0) || (pick == s);
+    if (moving) {
+      const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, (uint32_t)s, 2u), key);
+      const float2 n01 = gauss2(c.x, c.y);
+      const float2 n23 = gauss2(c.z, c.w);
+      const float gz[3] = {n01.x, n01.y, n23.x};
+      int64_t pos[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        pos[i] = (int64_t)ws.cur[s * 3 + i] + (int64_t)llrint((double)gz[i] * (double)sd * kTwoPow32);
+      const ProjFix &pr = P.proj[(size_t)A * P.maxSites + s];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        int64_t acc = (int64_t)pr.num[3 * i] * pos[0] + (int64_t)pr.num[3 * i + 1] * pos[1] +
+                      (int64_t)pr.num[3 * i + 2] * pos[2];
+        if (pr.den != 1) acc = floor_div(acc, pr.den);
+        ws.prop[s * 3 + i] = (uint32_t)(acc + (int64_t)pr.t[i]);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) ws.prop[s * 3 + i] = ws.cur[s * 3 + i];
+    }
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// The kernel.
+// ---------------------------------------------------------------------------
+template <int COSMODE, int SLOTS>
+__global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int nGen, int mcmc, int swapEvery,
+                                                 int reevalFirst) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t stageBar;
+  __shared__ float shellLen[27];
+  __shared__ float exE[kMaxRungs];
+  __shared__ int exSwap[kMaxRungs];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nWarps = blockDim.x >> 5;
+
+  // Stage the static tables (reflections, f table, groups, rMin) once per CTA.
+  unsigned char *stat = smem;
+  const int blobPad = (P.blobBytes + 127) & ~127;
+  if (threadIdx.x == 0) {
+    mbar_init(&stageBar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(&stageBar, (uint32_t)P.blobBytes);
+    // chunks of at most 64 KB, 16-byte multiples (blobBytes is padded on the host)
+    for (int off = 0; off < P.blobBytes; off += 65536) {
+      const int n = min(65536, P.blobBytes - off);
+      bulk_g2s(stat + off, P.blob + off, (uint32_t)n, &stageBar);
+    }
+  }
+  if (threadIdx.x < 27) {
+    const float t[3] = {(float)((int)threadIdx.x / 9 - 1), (float)(((int)threadIdx.x / 3) % 3 - 1),
+                        (float)((int)threadIdx.x % 3 - 1)};
+    shellLen[threadIdx.x] = cart_len(P, t);
+  }
+  if (!mbar_wait_bounded(&stageBar, 0, kStageWaitLimit)) {
+    raise_flag(P.errFlag, DEV_STAGE_TIMEOUT);
+    // give the copy in flight a second bounded chance before leaving
+    mbar_wait_bounded(&stageBar, 0, kStageWaitLimit);
+    return;
+  }
+  __syncthreads();
+  const ReflRec *refl = reinterpret_cast<const ReflRec *>(stat + P.offRefl);
+  const float *ftab = reinterpret_cast<const float *>(stat + P.offF);
+  const float4 *groups = reinterpret_cast<const float4 *>(stat + P.offGroup);
+  const float *rmin = reinterpret_cast<const float *>(stat + P.offRmin);
+
+  unsigned char *wbase = smem + blobPad + (size_t)warp * P.warpSmemBytes;
+  WarpSmem &ws = *reinterpret_cast<WarpSmem *>(wbase);
+  uint4 *atoms = reinterpret_cast<uint4 *>(wbase + P.atomsOff);
+  float *ic = reinterpret_cast<float *>(wbase + P.icOff);
+
+  const int rungs = P.rungs;
+  const int nLadders = P.nLadders;
+  const size_t curStride = (size_t)P.maxSites * 3;
+  uint32_t *bestBase = P.pos + (size_t)P.numParticles * curStride;
+
+  for (int L = blockIdx.x; L < nLadders; L += gridDim.x) {
+    int p = -1;
+    if (warp < rungs) {
+      if (P.ladders)
+        p = P.ladders[(size_t)L * rungs + warp];
+      else {
+        const int q = L * rungs + warp;
+        p = q < P.numParticles ? q : -1;
+      }
+    }
+    const bool active = p >= 0;
+    if (active) {
+      const int A = (int)P.assign[p];
+      if (lane == 0) {
+        ws.meta[0] = A;
+        ws.meta[1] = P.nRuns[A];
+        ws.meta[2] = P.nF[A];
+        ws.meta[4] = (int)P.freeMask[A];
+        ws.meta[5] = p;
+        ws.st = P.st[p];
+      }
+      if (lane < kMaxSites) ws.runs[lane] = P.runs[(size_t)A * kMaxSites + lane];
+      for (int j = lane; j < (int)curStride; j += 32) ws.cur[j] = P.pos[(size_t)p * curStride + j];
+    }
+    __syncwarp();
+    int prevNga = -1;
+    for (int gi = 0; gi < nGen; ++gi) {
+      const int g = gen0 + gi;
+      const int nga = P.schedGroups ? P.schedGroups[g] : P.ngaArg;
+      const float penScale = P.schedGroups ? P.schedPen[g] : P.penArg;
+      const int ngaC = max(0, min(nga, P.nGroups));
+      if (active) {
+        const bool reeval = mcmc && ((gi == 0 && reevalFirst) || (gi > 0 && nga != prevNga));
+        if (reeval || !mcmc) {
+          // evaluate the current state (dispatchCoords(null, false))
+          expand(P, ws.meta[0], ws.cur, atoms, lane);
+          __syncwarp();
+          double sums[3];
+          fitness<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, ngaC, lane, sums,
+                           P.traceIc ? P.traceIc + (size_t)p * P.nRefl : nullptr);
+          const float cc = cc_of(sums);
+          const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, lane) * penScale;
+          if (lane == 0) {
+            ws.st.fit = cc - pen;
+            ws.st.cc = cc;
+            ws.st.pen = pen / fmaxf(penScale, 1e-9f);
+          }
+          __syncwarp();
+        }
+        if (mcmc) {
+          float uMetro;
+          const float sd = __shfl_sync(0xffffffffu, lane == 0 ? ws.st.step : 0.f, 0);
+          propose(P, ws, g, p, lane, sd, &uMetro);
+          expand(P, ws.meta[0], ws.prop, atoms, lane);
+          __syncwarp();
+          double sums[3];
+          fitness<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, ngaC, lane, sums,
+                           P.traceIc ? P.traceIc + (size_t)p * P.nRefl : nullptr);
+          const float cc = cc_of(sums);
+          const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, lane) * penScale;
+          int acc = 0, best = 0;
+          if (lane == 0) {
+            PState &st = ws.st;
+            const float fNew = cc - pen;
+            float fOld = st.fit;
+            if (fOld > -1.0e29f) fOld = st.cc - st.pen * penScale;
+            const float stepBefore = st.step;
+            if (fNew >= fOld)
+              acc = 1;
+            else if (uMetro < expf((fNew - fOld) / fmaxf(st.temp, 1e-9f)))
+              acc = 1;
+            if (acc) {
+              st.fit = fNew;
+              st.cc = cc;
+              st.pen = pen / fmaxf(penScale, 1e-9f);
+              st.accepted += 1u;
+              const bool hasBest = st.bestFit > -1.0e29f;
+              const float bestR = hasBest ? st.bestCC - st.bestPen * penScale : -1.0e30f;
+              if (fNew > bestR) {
+                st.bestFit = fNew;
+                st.bestCC = cc;
+                st.bestPen = pen / fmaxf(penScale, 1e-9f);
+                best = 1;
+              }
+            }
+            st.step = fminf(fmaxf(st.step * (acc ? P.stepUp : P.stepDown), P.stepMin), P.stepMax);
+            if (P.traceRec) {
+              float *rec = P.traceRec + (size_t)p * 8;
+              rec[0] = fNew; rec[1] = cc; rec[2] = pen; rec[3] = uMetro;
+              rec[4] = (float)acc; rec[5] = fOld; rec[6] = st.temp; rec[7] = stepBefore;
+            }
+          }
+          acc = __shfl_sync(0xffffffffu, acc, 0);
+          best = __shfl_sync(0xffffffffu, best, 0);
+          if (P.tracePos)
+            for (int j = lane; j < (int)curStride; j += 32) P.tracePos[(size_t)p * curStride + j] = ws.prop[j];
+          if (acc)
+            for (int j = lane; j < (int)curStride; j += 32) ws.cur[j] = ws.prop[j];
+          if (best)
+            for (int j = lane; j < (int)curStride; j += 32) bestBase[(size_t)p * curStride + j] = ws.prop[j];
+          __syncwarp();
+        }
+      }
+      prevNga = nga;
+      // replica exchange inside the ladder (js/swarm_wyckoff.js:1825-1851)
+      if (swapEvery > 0 && mcmc && P.ladders && ((g + 1) % swapEvery) == 0) {
+        if (active && lane == 0) {
+          const PState &st = ws.st;
+          exE[warp] = isfinite(st.cc) ? st.cc - st.pen * penScale : st.fit;
+        }
+        if (threadIdx.x < kMaxRungs) exSwap[threadIdx.x] = -1;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          const int parity = ((g + 1) / swapEvery) & 1;
+          unsigned long long tried = 0, taken = 0;
+          for (int r = parity; r + 1 < rungs; r += 2) {
+            const int a = P.ladders[(size_t)L * rungs + r], b = P.ladders[(size_t)L * rungs + r + 1];
+            if (a < 0 || b < 0) continue;
+            const float fa = exE[r], fb = exE[r + 1];
+            if (!isfinite(fa) || !isfinite(fb)) continue;
+            ++tried;
+            WarpSmem &wa = *reinterpret_cast<WarpSmem *>(smem + blobPad + (size_t)r * P.warpSmemBytes);
+            WarpSmem &wb = *reinterpret_cast<WarpSmem *>(smem + blobPad + (size_t)(r + 1) * P.warpSmemBytes);
+            const float d = (1.0f / wa.st.temp - 1.0f / wb.st.temp) * (fb - fa);
+            if (d < 0.f) {
+              const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)L, (uint32_t)r, 7u),
+                                            make_uint2(P.runKey, 0x45584348u));
+              if (u01(c.x) >= expf(d)) continue;
+            }
+            ++taken;
+            exSwap[r] = r + 1;
+          }
+          if (P.swapStats && tried) {
+            atomicAdd(P.swapStats, tried);
+            atomicAdd(P.swapStats + 1, taken);
+          }
+        }
+        __syncthreads();
+        // each pair (r, r+1) swaps coordinates and energies; rungs keep temp and step
+        for (int r = warp; r < rungs; r += nWarps) {
+          if (exSwap[r] < 0) continue;
+          WarpSmem &wa = *reinterpret_cast<WarpSmem *>(smem + blobPad + (size_t)r * P.warpSmemBytes);
+          WarpSmem &wb = *reinterpret_cast<WarpSmem *>(smem + blobPad + (size_t)(r + 1) * P.warpSmemBytes);
+          for (int j = lane; j < (int)curStride; j += 32) {
+            const uint32_t t = wa.cur[j];
+            wa.cur[j] = wb.cur[j];
+            wb.cur[j] = t;
+          }
+          if (lane == 0) {
+            float t = wa.st.fit; wa.st.fit = wb.st.fit; wb.st.fit = t;
+            t = wa.st.cc; wa.st.cc = wb.st.cc; wb.st.cc = t;
+            t = wa.st.pen; wa.st.pen = wb.st.pen; wb.st.pen = t;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (active) {
+      for (int j = lane; j < (int)curStride; j += 32) P.pos[(size_t)p * curStride + j] = ws.cur[j];
+      if (lane == 0) P.st[p] = ws.st;
+    }
+    __syncthreads();
+  }
+}
+
+// Generated cell of one particle in genPack order (parity support).
+__global__ void wy_expand_one(const Params P, const uint32_t *genOrig, int particle, uint32_t *out) {
+  const int i = threadIdx.x + blockIdx.x * blockDim.x;
+  if (i >= P.nTot) return;
+  const int A = (int)P.assign[particle];
+  const uint32_t w = genOrig[(size_t)A * P.nTot + i];
+  const int s = w & 0xFF, o = (w >> 8) & 0xFFF;
+  const OpFix &op = P.ops[o];
+  const uint32_t *x = P.pos + (size_t)particle * P.maxSites * 3 + s * 3;
+  for (int c = 0; c < 3; ++c)
+    out[i * 3 + c] = (uint32_t)op.r[3 * c] * x[0] + (uint32_t)op.r[3 * c + 1] * x[1] +
+                     (uint32_t)op.r[3 * c + 2] * x[2] + op.t[c];
+}
+
+__global__ void philox_one(uint4 c, uint2 k, uint4 *out) { *out = philox4x32_10(c, k); }
+
+}  // namespace wy
+}  // namespace p6
+
+// ===========================================================================
+// Host side: the session.
+// ===========================================================================
+using namespace p6;
+using namespace p6::wy;
+
+struct p6_wy_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Params P{};
+  int cosMode = 0;
+  int slots = 0;  // 0: clash only; 64 / 256: rule variants
+  uint32_t *dGen = nullptr, *dGenOrig = nullptr, *dFree = nullptr, *dPos = nullptr, *dAssign = nullptr;
+  int4 *dRuns = nullptr;
+  int *dNRuns = nullptr, *dNF = nullptr, *dLadders = nullptr, *dSchedG = nullptr, *dErr = nullptr;
+  float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr;
+  uint32_t *dTracePos = nullptr;
+  OpFix *dOps = nullptr;
+  ProjFix *dProj = nullptr;
+  unsigned char *dBlob = nullptr;
+  RuleDev *dRules = nullptr;
+  PState *dSt = nullptr;
+  unsigned long long *dSwap = nullptr;
+  int nLadders = 0, rungs = 8, schedLen = 0;
+  int nga = 0;
+  float penScale = 1.0f;
+  bool trace = false;
+  long long launches = 0;
+  std::vector<uint32_t> hostAssign;
+  std::vector<uint32_t> siteCountOfAssign;
+  int smemBytes = 0;
+  int maxGrid = 0;
+};
+
+namespace {
+
+thread_local std::string g_err;
+int g_inject_code = 0, g_inject_after = -1;
+
+}  // namespace
+
+namespace p6 {
+p6_status set_error(p6_status code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+p6_status cuda_error(cudaError_t e, const char *what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorIllegalAddress || e == cudaErrorLaunchFailure || e == cudaErrorDevicesUnavailable ||
+      e == cudaErrorHardwareStackError || e == cudaErrorIllegalInstruction || e == cudaErrorMisalignedAddress)
+    return P6_ERR_DEVICE_LOST;
+  return P6_ERR_CUDA;
+}
+void clear_error() { g_err.clear(); }
+}  // namespace p6
+
+static p6_status injected() {
+  if (g_inject_after < 0 || g_inject_code == 0) return P6_OK;
+  if (g_inject_after-- == 0) {
+    const int c = g_inject_code;
+    g_inject_code = 0;
+    g_inject_after = -1;
+    return set_error((p6_status)c, "injected failure (host-side fault injection)");
+  }
+  return P6_OK;
+}
+
+#define P6_ENTRY()                      \
+  do {                                  \
+    clear_error();                      \
+    p6_status _inj = injected();        \
+    if (_inj != P6_OK) return _inj;     \
+  } while (0)
+
+static uint32_t to_fixed(double x) {
+  double f = x - std::floor(x);
+  double v = std::floor(f * kTwoPow32 + 0.5);
+  if (v >= kTwoPow32) v -= kTwoPow32;
+  return (uint32_t)(uint64_t)v;
+}
+static float from_fixed(uint32_t x) {
+  float f = (float)((double)x / kTwoPow32);
+  return f >= 1.0f ? 0.0f : f;
+}
+// Translation snapped to a multiple of 1/24 when it is one, then fixed point.
+static uint32_t trans_fixed(double t) {
+  double s = t * 24.0, r = std::floor(s + 0.5);
+  if (std::fabs(s - r) < 1e-4) {
+    long long n = ((long long)r % 24 + 24) % 24;
+    return (uint32_t)((n * 4294967296LL + 12) / 24);
+  }
+  return to_fixed(t);
+}
+// Smallest denominator (<= 24) making every entry of P an integer.
+static bool rationalise(const float *p, int n, int *num, int *den) {
+  static const int dens[] = {1, 2, 3, 4, 6, 8, 12, 24};
+  for (int d : dens) {
+    bool ok = true;
+    for (int i = 0; i < n && ok; ++i) {
+      double v = (double)p[i] * d;
+      if (std::fabs(v - std::floor(v + 0.5)) > 1e-4) ok = false;
+    }
+    if (ok) {
+      for (int i = 0; i < n; ++i) num[i] = (int)std::floor((double)p[i] * d + 0.5);
+      *den = d;
+      return true;
+    }
+  }
+  return false;
+}
+
+template <typename T>
+static p6_status upload(T **dst, const T *src, size_t n, cudaStream_t s) {
+  P6_CUDA(cudaMalloc((void **)dst, std::max<size_t>(n, 1) * sizeof(T)));
+  if (n) P6_CUDA(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  return P6_OK;
+}
+
+static void free_session(p6_wy_session *s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
+                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dTraceRec, s->dTraceIc, s->dTracePos, s->dOps,
+                  s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+template <int C, int S>
+static cudaError_t launch_variant(p6_wy_session *s, int grid, int block, int gen0, int nGen, int mcmc,
+                                  int swapEvery, int reevalFirst) {
+  auto k = wy_kernel<C, S>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemBytes);
+  if (e != cudaSuccess) return e;
+  k<<<grid, block, s->smemBytes, s->stream>>>(s->P, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch(p6_wy_session *s, int gen0, int nGen, int mcmc, int swapEvery, int reevalFirst) {
+  Params &P = s->P;
+  const int rungs = P.rungs;
+  const int block = 32 * rungs;
+  int grid = std::min(P.nLadders, s->maxGrid > 0 ? s->maxGrid : P.nLadders);
+  grid = std::max(grid, 1);
+  cudaError_t e;
+  const int C = s->cosMode, S = s->slots;
+  if (C == 0 && S == 0) e = launch_variant<0, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  else if (C == 1 && S == 0) e = launch_variant<1, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  else if (C == 0 && S == 64) e = launch_variant<0, 64>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  else if (C == 1 && S == 64) e = launch_variant<1, 64>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  else if (C == 0) e = launch_variant<0, 256>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  else e = launch_variant<1, 256>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  if (e == cudaSuccess) s->launches++;
+  return e;
+}
+
+static p6_status check_device_flag(p6_wy_session *s) {
+  int flag = 0;
+  P6_CUDA(cudaMemcpyAsync(&flag, s->dErr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  if (flag == DEV_STAGE_TIMEOUT) return set_error(P6_ERR_TIMEOUT, "static-table staging did not complete in time");
+  if (flag) return set_error(P6_ERR_CAPACITY, "device reported a capacity error");
+  return P6_OK;
+}
+
+extern "C" {
+
+const char *p6_last_error(void) { return g_err.c_str(); }
+int p6_abi_version(void) { return 1; }
+void p6_debug_inject_failure(int code, int after_calls) {
+  g_inject_code = code;
+  g_inject_after = code ? after_calls : -1;
+}
+
+p6_status p6_philox_device(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  clear_error();
+  uint4 *d = nullptr;
+  P6_CUDA(cudaMalloc(&d, sizeof(uint4)));
+  philox_one<<<1, 1>>>(make_uint4(ctr[0], ctr[1], ctr[2], ctr[3]), make_uint2(key[0], key[1]), d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(uint4), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_error(e, "philox_one");
+  return P6_OK;
+}
+
+p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out) {
+  P6_ENTRY();
+  if (!pr || !out) return set_error(P6_ERR_INVALID_ARG, "null problem or output pointer");
+  *out = nullptr;
+  if (pr->num_particles <= 0 || pr->n_assign <= 0 || pr->n_tot <= 0 || pr->n_ops <= 0 || pr->max_sites <= 0)
+    return set_error(P6_ERR_INVALID_ARG, "empty problem");
+  if (!pr->gen_pack || !pr->sym_packed || !pr->site_proj || !pr->refl_pack || !pr->group_meta || !pr->f_tab ||
+      !pr->restraint_tables)
+    return set_error(P6_ERR_INVALID_ARG, "null table pointer");
+  if (pr->max_sites > kMaxSites)
+    return set_error(P6_ERR_CAPACITY, "more than 32 independent sites per assignment");
+  if (pr->n_elem < 1 || pr->n_elem > kMaxElem) return set_error(P6_ERR_CAPACITY, "1 to 8 elements are supported");
+  if (pr->n_ops > 4096) return set_error(P6_ERR_CAPACITY, "more than 4096 operators");
+  if (pr->n_rules > kMaxRules) return set_error(P6_ERR_CAPACITY, "more than 32 distance rules");
+  if (pr->max_coord_slots > 256) return set_error(P6_ERR_CAPACITY, "more than 256 neighbour slots");
+  if (pr->group_stride != 3 && pr->group_stride != 4) return set_error(P6_ERR_INVALID_ARG, "group stride must be 3 or 4");
+  if (pr->poly_prob > 0.f)
+    return set_error(P6_ERR_INVALID_ARG, "polyhedron moves are not available in this build (poly_prob must be 0)");
+  if (pr->n_tot > 4096) return set_error(P6_ERR_CAPACITY, "more than 4096 generated atoms");
+  if (pr->cos_mode != 0 && pr->cos_mode != 1) return set_error(P6_ERR_INVALID_ARG, "cos_mode must be 0 or 1");
+
+  const int nA = pr->n_assign, nTot = pr->n_tot, ms = pr->max_sites, nE = pr->n_elem;
+  // --- validate and convert host tables -----------------------------------
+  std::vector<uint32_t> genR((size_t)nA * nTot);
+  std::vector<int4> runs((size_t)nA * kMaxSites, make_int4(0, 0, 0, 0));
+  std::vector<int> nRuns(nA), nF(nA);
+  for (int A = 0; A < nA; ++A) {
+    const uint32_t *g = pr->gen_pack + (size_t)A * nTot;
+    int w = 0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int i = 0; i < nTot; ++i) {
+        const uint32_t word = g[i];
+        const int site = word & 0xFF, op = (word >> 8) & 0xFFF, skip = (word >> 24) & 1;
+        if (site >= ms || op >= pr->n_ops)
+          return set_error(P6_ERR_INVALID_ARG, "genPack entry names a site or operator out of range");
+        if ((skip != 0) == (pass == 0)) continue;
+        genR[(size_t)A * nTot + w++] = word;
+      }
+    int nf = 0, nr = 0;
+    for (int i = 0; i < nTot; ++i)
+      if (!((g[i] >> 24) & 1)) ++nf;
+    for (int i = 0; i < nf; ++i) {
+      const uint32_t word = genR[(size_t)A * nTot + i];
+      const int site = word & 0xFF, ty = std::min<int>((word >> 20) & 0xF, nE - 1);
+      if (nr > 0 && runs[(size_t)A * kMaxSites + nr - 1].w == site && runs[(size_t)A * kMaxSites + nr - 1].y == i) {
+        runs[(size_t)A * kMaxSites + nr - 1].y = i + 1;
+      } else {
+        if (nr >= kMaxSites) return set_error(P6_ERR_CAPACITY, "a site's images are not contiguous in genPack");
+        runs[(size_t)A * kMaxSites + nr++] = make_int4(i, i + 1, ty, site);
+      }
+    }
+    nRuns[A] = nr;
+    nF[A] = nf;
+  }
+  std::vector<OpFix> ops(pr->n_ops);
+  for (int o = 0; o < pr->n_ops; ++o) {
+    const float *b = pr->sym_packed + o * 12;
+    for (int k = 0; k < 9; ++k) {
+      const double v = b[k];
+      if (std::fabs(v - std::floor(v + 0.5)) > 1e-6)
+        return set_error(P6_ERR_INVALID_ARG, "operator with a non-integer rotation part");
+      ops[o].r[k] = (int)std::floor(v + 0.5);
+    }
+    for (int k = 0; k < 3; ++k) ops[o].t[k] = trans_fixed(b[9 + k]);
+  }
+  std::vector<ProjFix> proj((size_t)nA * ms);
+  std::vector<uint32_t> freeMask(nA, 0);
+  for (int A = 0; A < nA; ++A)
+    for (int si = 0; si < ms; ++si) {
+      const float *b = pr->site_proj + ((size_t)A * ms + si) * 12;
+      ProjFix &f = proj[(size_t)A * ms + si];
+      if (!rationalise(b, 9, f.num, &f.den))
+        return set_error(P6_ERR_INVALID_ARG, "a Wyckoff projector is not a rational matrix with denominator <= 24");
+      for (int k = 0; k < 3; ++k) f.t[k] = trans_fixed(b[9 + k]);
+      double norm = 0;
+      for (int k = 0; k < 9; ++k) norm += std::fabs(b[k]);
+      if (norm > 1e-6) freeMask[A] |= 1u << si;
+    }
+  // --- static blob: reflections | f table | groups | rMin ---------------------
+  auto pad16 = [](size_t n) { return (n + 15) & ~(size_t)15; };
+  const size_t offRefl = 0, szRefl = pad16((size_t)pr->n_refl * sizeof(ReflRec));
+  const size_t offF = offRefl + szRefl, szF = pad16((size_t)pr->n_refl * nE * sizeof(float));
+  const size_t offG = offF + szF, szG = pad16((size_t)pr->n_groups * sizeof(float4));
+  const size_t offR = offG + szG, szR = pad16((size_t)nE * nE * sizeof(float));
+  const size_t blobBytes = offR + szR;
+  std::vector<unsigned char> blob(blobBytes, 0);
+  for (int r = 0; r < pr->n_refl; ++r) {
+    const uint32_t pk = pr->refl_pack[2 * r];
+    ReflRec rec;
+    rec.h = (short)((int)(pk & 0x3FF) - 512);
+    rec.k = (short)((int)((pk >> 10) & 0x3FF) - 512);
+    rec.l = (short)((int)((pk >> 20) & 0x3FF) - 512);
+    const uint32_t m = pr->refl_pack[2 * r + 1];
+    if (m > 65535) return set_error(P6_ERR_INVALID_ARG, "multiplicity out of range");
+    rec.mult = (unsigned short)m;
+    std::memcpy(&blob[offRefl + r * sizeof(ReflRec)], &rec, sizeof(rec));
+  }
+  std::memcpy(&blob[offF], pr->f_tab, (size_t)pr->n_refl * nE * sizeof(float));
+  for (int gI = 0; gI < pr->n_groups; ++gI) {
+    const float *gm = pr->group_meta + (size_t)gI * pr->group_stride;
+    float4 v = make_float4(gm[0], gm[1], gm[2], pr->group_stride >= 4 ? gm[3] : 1.0f);
+    if (v.x < 0 || v.y < 0 || (int)v.x + (int)v.y > pr->n_refl)
+      return set_error(P6_ERR_INVALID_ARG, "group range outside the reflection list");
+    if (gI > 0) {
+      const float *pg = pr->group_meta + (size_t)(gI - 1) * pr->group_stride;
+      if ((int)v.x != (int)pg[0] + (int)pg[1])
+        return set_error(P6_ERR_INVALID_ARG, "groups must be contiguous and in order");
+    }
+    std::memcpy(&blob[offG + gI * sizeof(float4)], &v, sizeof(v));
+  }
+  for (int i = 0; i < nE * nE; ++i) {
+    const float v = pr->restraint_tables[pr->r_min_off + i];
+    std::memcpy(&blob[offR + i * sizeof(float)], &v, sizeof(float));
+  }
+  std::vector<RuleDev> rules(std::max(pr->n_rules, 1));
+  for (int k = 0; k < pr->n_rules; ++k) {
+    const float *rb = pr->restraint_tables + pr->rule_off + 7 * k;
+    rules[k] = RuleDev{(int)rb[0], (int)rb[1], rb[2], rb[3], rb[4], (int)rb[5], (int)rb[6], 0};
+  }
+  // --- shared memory plan ----------------------------------------------------
+  const int rungs = 8;
+  const size_t atomsOff = (sizeof(WarpSmem) + 15) & ~(size_t)15;
+  const size_t icOff = atomsOff + (size_t)nTot * sizeof(uint4);
+  const size_t warpBytes = (icOff + (size_t)pr->n_refl * sizeof(float) + 127) & ~(size_t)127;
+  const size_t smem = ((blobBytes + 127) & ~(size_t)127) + warpBytes * rungs;
+
+  p6_wy_session *s = new p6_wy_session();
+  s->device = device;
+  s->cosMode = pr->cos_mode;
+  const int slotsNeeded = pr->n_rules > 0 ? (pr->max_coord_slots <= 64 ? 64 : 256) : 0;
+  s->slots = slotsNeeded;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "cudaSetDevice"); }
+  int smemOptin = 0, nSM = 0;
+  cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, device);
+  // Shared memory: the staged tables once, plus one slice per rung (8 warps).
+  if ((int)smem > smemOptin - 1024) {
+    free_session(s);
+    return set_error(P6_ERR_CAPACITY, "the reflection table and generated cell do not fit in shared memory");
+  }
+  s->smemBytes = (int)smem;
+  p6_status st;
+#define P6_TRY(x)                   \
+  do {                              \
+    st = (x);                       \
+    if (st != P6_OK) {              \
+      free_session(s);              \
+      return st;                    \
+    }                               \
+  } while (0)
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "cudaStreamCreate"); }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  P6_TRY(upload(&s->dGen, genR.data(), genR.size(), s->stream));
+  P6_TRY(upload(&s->dGenOrig, pr->gen_pack, (size_t)nA * nTot, s->stream));
+  P6_TRY(upload(&s->dRuns, runs.data(), runs.size(), s->stream));
+  P6_TRY(upload(&s->dNRuns, nRuns.data(), nRuns.size(), s->stream));
+  P6_TRY(upload(&s->dNF, nF.data(), nF.size(), s->stream));
+  P6_TRY(upload(&s->dFree, freeMask.data(), freeMask.size(), s->stream));
+  P6_TRY(upload(&s->dOps, ops.data(), ops.size(), s->stream));
+  P6_TRY(upload(&s->dProj, proj.data(), proj.size(), s->stream));
+  P6_TRY(upload(&s->dBlob, blob.data(), blob.size(), s->stream));
+  P6_TRY(upload(&s->dRules, rules.data(), rules.size(), s->stream));
+  const size_t posWords = (size_t)2 * pr->num_particles * ms * 3;
+  e = cudaMalloc(&s->dPos, posWords * sizeof(uint32_t));
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "cudaMalloc positions"); }
+  cudaMemsetAsync(s->dPos, 0, posWords * sizeof(uint32_t), s->stream);
+  e = cudaMalloc(&s->dSt, (size_t)pr->num_particles * sizeof(PState));
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "cudaMalloc state"); }
+  cudaMemsetAsync(s->dSt, 0, (size_t)pr->num_particles * sizeof(PState), s->stream);
+  std::vector<uint32_t> assign0(pr->num_particles, 0);
+  P6_TRY(upload(&s->dAssign, assign0.data(), assign0.size(), s->stream));
+  s->hostAssign = assign0;
+  e = cudaMalloc(&s->dErr, sizeof(int));
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "cudaMalloc flag"); }
+  cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
+  e = cudaMalloc(&s->dSwap, 2 * sizeof(unsigned long long));
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "cudaMalloc swap stats"); }
+  cudaMemsetAsync(s->dSwap, 0, 2 * sizeof(unsigned long long), s->stream);
+
+  Params &P = s->P;
+  P.gen = s->dGen;
+  P.runs = s->dRuns;
+  P.nRuns = s->dNRuns;
+  P.nF = s->dNF;
+  P.freeMask = s->dFree;
+  P.ops = s->dOps;
+  P.proj = s->dProj;
+  P.blob = s->dBlob;
+  P.blobBytes = (int)blobBytes;
+  P.offRefl = (int)offRefl;
+  P.offF = (int)offF;
+  P.offGroup = (int)offG;
+  P.offRmin = (int)offR;
+  P.rules = s->dRules;
+  P.nRules = pr->n_rules;
+  P.numParticles = pr->num_particles;
+  P.nTot = nTot;
+  P.maxSites = ms;
+  P.nRefl = pr->n_refl;
+  P.nGroups = pr->n_groups;
+  P.nElem = nE;
+  P.nAssign = nA;
+  for (int i = 0; i < 9; ++i) {
+    P.orth[i] = (float)pr->orth[i];
+    const double x = pr->xform[i];
+    if (std::fabs(x - std::floor(x + 0.5)) > 1e-9) {
+      free_session(s);
+      return set_error(P6_ERR_INVALID_ARG, "xform must be an integer matrix");
+    }
+    P.xf[i] = (int)std::floor(x + 0.5);
+  }
+  P.minImageShell = pr->min_image_shell ? 1 : 0;
+  P.countShell = pr->count_shell ? 1 : 0;
+  P.centro = pr->centro;
+  P.maxCoordSlots = pr->max_coord_slots;
+  P.geomSlots = pr->geom_slots;
+  P.penClash = pr->pen_clash;
+  P.penBond = pr->pen_bond;
+  P.penCoord = pr->pen_coord;
+  P.penGeom = pr->pen_geom;
+  P.stepUp = pr->step_up;
+  P.stepDown = pr->step_down;
+  P.stepMin = pr->step_min;
+  P.stepMax = pr->step_max;
+  P.runKey = pr->run_key;
+  P.pos = s->dPos;
+  P.st = s->dSt;
+  P.assign = s->dAssign;
+  P.ladders = nullptr;
+  P.rungs = 8;
+  P.nLadders = (pr->num_particles + 7) / 8;
+  P.schedGroups = nullptr;
+  P.schedPen = nullptr;
+  P.ngaArg = pr->n_groups;
+  P.penArg = 1.0f;
+  P.swapStats = s->dSwap;
+  P.errFlag = s->dErr;
+  P.warpSmemBytes = (int)warpBytes;
+  P.atomsOff = (int)atomsOff;
+  P.icOff = (int)icOff;
+  s->nga = pr->n_groups;
+  // Resident CTAs: the persistent grid covers the GPU once.
+  int occ = 0;
+  cudaFuncSetAttribute(wy_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemBytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wy_kernel<0, 0>, 256, s->smemBytes);
+  s->maxGrid = std::max(1, occ) * std::max(1, nSM);
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) { free_session(s); return cuda_error(e, "session upload"); }
+  *out = s;
+  return P6_OK;
+#undef P6_TRY
+}
+
+p6_status p6_wy_destroy(p6_wy_session *s) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  free_session(s);
+  return P6_OK;
+}
+
+p6_status p6_wy_set_assign(p6_wy_session *s, const uint32_t *assign_of) {
+  P6_ENTRY();
+  if (!s || !assign_of) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  for (int i = 0; i < s->P.numParticles; ++i)
+    if ((int)assign_of[i] >= s->P.nAssign) return set_error(P6_ERR_INVALID_ARG, "assignment index out of range");
+  P6_CUDA(cudaSetDevice(s->device));
+  s->hostAssign.assign(assign_of, assign_of + s->P.numParticles);
+  P6_CUDA(cudaMemcpyAsync(s->dAssign, s->hostAssign.data(), s->hostAssign.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_set_params(p6_wy_session *s, int n_groups_active, float pen_scale) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  s->nga = n_groups_active;
+  s->penScale = pen_scale;
+  return P6_OK;
+}
+
+static p6_status write_positions_f32(p6_wy_session *s, const float *positions, bool resetBest) {
+  const size_t n = (size_t)s->P.numParticles * s->P.maxSites * 3;
+  std::vector<uint32_t> fx(resetBest ? 2 * n : n);
+  for (size_t i = 0; i < n; ++i) fx[i] = to_fixed(positions[i]);
+  if (resetBest)
+    for (size_t i = 0; i < n; ++i) fx[n + i] = fx[i];
+  P6_CUDA(cudaMemcpyAsync(s->dPos, fx.data(), fx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_sync_state(p6_wy_session *s, const float *positions, const p6_wy_particle_state *state) {
+  P6_ENTRY();
+  if (!s || !positions || !state) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaSetDevice(s->device));
+  p6_status st = write_positions_f32(s, positions, true);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaMemcpyAsync(s->dSt, state, (size_t)s->P.numParticles * sizeof(PState), cudaMemcpyHostToDevice,
+                          s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_read_state(p6_wy_session *s, float *positions, float *best_positions, p6_wy_particle_state *state) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t n = (size_t)s->P.numParticles * s->P.maxSites * 3;
+  std::vector<uint32_t> fx(2 * n);
+  P6_CUDA(cudaMemcpyAsync(fx.data(), s->dPos, fx.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  if (state)
+    P6_CUDA(cudaMemcpyAsync(state, s->dSt, (size_t)s->P.numParticles * sizeof(PState), cudaMemcpyDeviceToHost,
+                            s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  if (positions)
+    for (size_t i = 0; i < n; ++i) positions[i] = from_fixed(fx[i]);
+  if (best_positions)
+    for (size_t i = 0; i < n; ++i) best_positions[i] = from_fixed(fx[n + i]);
+  return P6_OK;
+}
+
+p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current) {
+  P6_ENTRY();
+  if (!s || !current) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  const size_t n = (size_t)s->P.numParticles * s->P.maxSites * 3;
+  P6_CUDA(cudaMemcpyAsync(s->dPos, current, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaMemcpyAsync(s->dPos + n, current, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  const size_t n = (size_t)s->P.numParticles * s->P.maxSites * 3;
+  if (current) P6_CUDA(cudaMemcpyAsync(current, s->dPos, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  if (best) P6_CUDA(cudaMemcpyAsync(best, s->dPos + n, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_set_trace(p6_wy_session *s, int enable) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (enable && !s->dTracePos) {
+    P6_CUDA(cudaMalloc(&s->dTracePos, (size_t)s->P.numParticles * s->P.maxSites * 3 * sizeof(uint32_t)));
+    P6_CUDA(cudaMalloc(&s->dTraceRec, (size_t)s->P.numParticles * 8 * sizeof(float)));
+    P6_CUDA(cudaMalloc(&s->dTraceIc, (size_t)s->P.numParticles * std::max(s->P.nRefl, 1) * sizeof(float)));
+    P6_CUDA(cudaMemsetAsync(s->dTraceIc, 0, (size_t)s->P.numParticles * std::max(s->P.nRefl, 1) * sizeof(float),
+                            s->stream));
+  }
+  s->trace = enable != 0;
+  return P6_OK;
+}
+
+p6_status p6_wy_read_trace(p6_wy_session *s, uint32_t *proposals, float *records) {
+  P6_ENTRY();
+  if (!s || !s->dTracePos) return set_error(P6_ERR_INVALID_ARG, "tracing was not enabled");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (proposals)
+    P6_CUDA(cudaMemcpyAsync(proposals, s->dTracePos, (size_t)s->P.numParticles * s->P.maxSites * 3 * 4,
+                            cudaMemcpyDeviceToHost, s->stream));
+  if (records)
+    P6_CUDA(cudaMemcpyAsync(records, s->dTraceRec, (size_t)s->P.numParticles * 8 * 4, cudaMemcpyDeviceToHost,
+                            s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+static p6_status dispatch_impl(p6_wy_session *s, int mcmc) {
+  Params &P = s->P;
+  Params saved = P;
+  P.ladders = nullptr;
+  P.rungs = 8;
+  P.nLadders = (P.numParticles + 7) / 8;
+  P.schedGroups = nullptr;
+  P.schedPen = nullptr;
+  P.ngaArg = s->nga;
+  P.penArg = s->penScale;
+  P.tracePos = s->trace ? s->dTracePos : nullptr;
+  P.traceRec = s->trace ? s->dTraceRec : nullptr;
+  P.traceIc = s->trace ? s->dTraceIc : nullptr;
+  P6_CUDA(cudaEventRecord(s->ev0, s->stream));
+  cudaError_t e = launch(s, 0, 1, mcmc, 0, 0);
+  P = saved;
+  if (e != cudaSuccess) return cuda_error(e, "wy_kernel launch");
+  P6_CUDA(cudaEventRecord(s->ev1, s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_dispatch(p6_wy_session *s, const float *coords, int mcmc) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (coords) {
+    const size_t n = (size_t)s->P.numParticles * s->P.maxSites * 3;
+    std::vector<uint32_t> fx(n);
+    for (size_t i = 0; i < n; ++i) fx[i] = to_fixed(coords[i]);
+    P6_CUDA(cudaMemcpyAsync(s->dPos, fx.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    P6_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return dispatch_impl(s, mcmc);
+}
+
+p6_status p6_wy_evaluate_sync(p6_wy_session *s, const float *coords, int mcmc, float *fit_cc) {
+  P6_ENTRY();
+  if (!s || !fit_cc) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  p6_status st = p6_wy_dispatch(s, coords, mcmc);
+  if (st != P6_OK) return st;
+  std::vector<PState> h(s->P.numParticles);
+  P6_CUDA(cudaMemcpyAsync(h.data(), s->dSt, h.size() * sizeof(PState), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < s->P.numParticles; ++i) {
+    fit_cc[i] = h[i].fit;
+    fit_cc[s->P.numParticles + i] = h[i].cc;
+  }
+  return check_device_flag(s);
+}
+
+p6_status p6_wy_set_ladders(p6_wy_session *s, const int32_t *ladders, int n_ladders, int rungs) {
+  P6_ENTRY();
+  if (!s || !ladders || n_ladders <= 0) return set_error(P6_ERR_INVALID_ARG, "null or empty ladder table");
+  if (rungs < 1 || rungs > 8) return set_error(P6_ERR_INVALID_ARG, "rungs must be 1..8 (one warp per rung)");
+  std::vector<int> seen(s->P.numParticles, 0);
+  for (int i = 0; i < n_ladders * rungs; ++i) {
+    const int p = ladders[i];
+    if (p < -1 || p >= s->P.numParticles) return set_error(P6_ERR_INVALID_ARG, "ladder entry out of range");
+    if (p >= 0 && seen[p]++) return set_error(P6_ERR_INVALID_ARG, "a particle appears in two ladder slots");
+  }
+  P6_CUDA(cudaSetDevice(s->device));
+  if (s->dLadders) cudaFree(s->dLadders);
+  s->dLadders = nullptr;
+  p6_status st = upload(&s->dLadders, ladders, (size_t)n_ladders * rungs, s->stream);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  s->nLadders = n_ladders;
+  s->rungs = rungs;
+  return P6_OK;
+}
+
+p6_status p6_wy_set_schedule(p6_wy_session *s, const int32_t *sched_groups, const float *sched_pen, int n_gen) {
+  P6_ENTRY();
+  if (!s || !sched_groups || !sched_pen || n_gen <= 0) return set_error(P6_ERR_INVALID_ARG, "empty schedule");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (s->dSchedG) cudaFree(s->dSchedG);
+  if (s->dSchedP) cudaFree(s->dSchedP);
+  s->dSchedG = nullptr;
+  s->dSchedP = nullptr;
+  p6_status st = upload(&s->dSchedG, sched_groups, (size_t)n_gen, s->stream);
+  if (st != P6_OK) return st;
+  st = upload(&s->dSchedP, sched_pen, (size_t)n_gen, s->stream);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  s->schedLen = n_gen;
+  return P6_OK;
+}
+
+p6_status p6_wy_run(p6_wy_session *s, int gen0, int n_gen, int swap_every, int reeval_first) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  if (!s->dLadders) return set_error(P6_ERR_INVALID_ARG, "no ladders set (p6_wy_set_ladders)");
+  if (!s->dSchedG || gen0 < 0 || n_gen <= 0 || gen0 + n_gen > s->schedLen)
+    return set_error(P6_ERR_INVALID_ARG, "generation range outside the schedule");
+  P6_CUDA(cudaSetDevice(s->device));
+  Params &P = s->P;
+  Params saved = P;
+  P.ladders = s->dLadders;
+  P.rungs = s->rungs;
+  P.nLadders = s->nLadders;
+  P.schedGroups = s->dSchedG;
+  P.schedPen = s->dSchedP;
+  P.tracePos = nullptr;
+  P.traceRec = nullptr;
+  P.traceIc = nullptr;
+  P6_CUDA(cudaEventRecord(s->ev0, s->stream));
+  cudaError_t e = launch(s, gen0, n_gen, 1, swap_every, reeval_first ? 1 : 0);
+  P = saved;
+  if (e != cudaSuccess) return cuda_error(e, "wy_kernel launch");
+  P6_CUDA(cudaEventRecord(s->ev1, s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_run_host(p6_wy_session *s, const float *positions_in, const p6_wy_particle_state *state_in, int gen0,
+                         int n_gen, int swap_every, int reeval_first, float *positions_out, float *best_out,
+                         p6_wy_particle_state *state_out) {
+  P6_ENTRY();
+  if (!s || !positions_in || !state_in) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  p6_status st = p6_wy_sync_state(s, positions_in, state_in);
+  if (st != P6_OK) return st;
+  st = p6_wy_run(s, gen0, n_gen, swap_every, reeval_first);
+  if (st != P6_OK) return st;
+  st = p6_wy_read_state(s, positions_out, best_out, state_out);
+  if (st != P6_OK) return st;
+  return check_device_flag(s);
+}
+
+p6_status p6_wy_synchronize(p6_wy_session *s, double timeout_seconds) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(s->stream);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) return cuda_error(e, "cudaStreamQuery");
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > timeout_seconds) return set_error(P6_ERR_TIMEOUT, "the device did not finish within the deadline");
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  return check_device_flag(s);
+}
+
+p6_status p6_wy_read_trace_ic(p6_wy_session *s, float *ic) {
+  P6_ENTRY();
+  if (!s || !s->dTraceIc || !ic) return set_error(P6_ERR_INVALID_ARG, "tracing was not enabled");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaMemcpyAsync(ic, s->dTraceIc, (size_t)s->P.numParticles * s->P.nRefl * sizeof(float),
+                          cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_debug_expand(p6_wy_session *s, int particle, uint32_t *atoms) {
+  P6_ENTRY();
+  if (!s || !atoms || particle < 0 || particle >= s->P.numParticles)
+    return set_error(P6_ERR_INVALID_ARG, "bad particle or output");
+  P6_CUDA(cudaSetDevice(s->device));
+  uint32_t *d = nullptr;
+  P6_CUDA(cudaMalloc(&d, (size_t)s->P.nTot * 3 * sizeof(uint32_t)));
+  wy_expand_one<<<(s->P.nTot + 127) / 128, 128, 0, s->stream>>>(s->P, s->dGenOrig, particle, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(atoms, d, (size_t)s->P.nTot * 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_error(e, "wy_expand_one");
+  return P6_OK;
+}
+
+p6_status p6_wy_last_kernel_ms(p6_wy_session *s, float *ms) {
+  P6_ENTRY();
+  if (!s || !ms) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaEventSynchronize(s->ev1));
+  P6_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
+  return P6_OK;
+}
+
+p6_status p6_wy_launch_count(p6_wy_session *s, long long *count) {
+  P6_ENTRY();
+  if (!s || !count) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  *count = s->launches;
+  return P6_OK;
+}
+
+}  // extern "C"

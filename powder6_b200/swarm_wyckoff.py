@@ -1,0 +1,438 @@
+"""Host side of the Wyckoff search on the B200 backend.
+
+Mirrors the device layer of ``runWyckoffSearch`` (js/swarm_wyckoff.js:964-2646):
+the same packed buffers, the same per-particle state record, the same
+dispatch / evaluate / read / sync operations (``WyckoffSession``), and the
+same search schedule -- replica ladders of ``rungs`` chains per assignment
+(:1784-1808), exchange every ``swapEvery`` generations (:1825-1851), the
+resolution ramp (``rampedGroupCount``, :934-938, :2218-2226) and the penalty
+ramp (:2228-2230).  ``run_wyckoff_search`` keeps the whole generation loop on
+the device: each CUDA block owns a ladder, so the exchange sweep needs no host
+round trip.
+
+``cpu_cross_check`` is the product's FP64 re-score of the winner, the role
+``swFitnessOnCpu`` plays in the reference report (js/swarm_wyckoff.js:2524-2563).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import P6WyParticleState, P6WyProblem, check, ptr
+from .reflections import ramped_group_count
+from .workloads import WyckoffProblem, mulberry32
+
+SW_DEFAULTS = dict(
+    penClash=0.05, penBond=0.10, penCoord=0.03, penRampStart=0.2, penRampEnd=4.0, polyProb=0.0,
+    tempHot=0.05, tempCold=5e-4, rungs=8, swapEvery=10, stepInit=0.08, stepMin=2e-4, stepMax=0.5,
+    targetAccept=0.3, stepAdapt=0.08, rampSteps=24, rampStart=0.25, rampFull=0.6,
+    quenchSteps=600, quenchStep0=0.02, quenchStep1=5e-5, topN=20, numParticles=512, generations=2000,
+)
+
+STATE_DTYPE = np.dtype([('fit', '<f4'), ('cc', '<f4'), ('pen', '<f4'), ('step_size', '<f4'), ('temp', '<f4'),
+                        ('seed', '<u4'), ('accepted', '<u4'), ('pad', '<u4'), ('best_fit', '<f4'),
+                        ('best_cc', '<f4'), ('best_pen', '<f4'), ('best_pad', '<f4')])
+assert STATE_DTYPE.itemsize == 48
+
+
+def adaptation(settings: Optional[dict] = None) -> Dict[str, float]:
+    """STEP_UP/STEP_DOWN/STEP_MIN/STEP_MAX as swInject computes and validates them
+    (js/swarm_wyckoff.js:201-216)."""
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    vals = [d['stepMin'], d['stepMax'], d['stepInit'], d['targetAccept'], d['stepAdapt']]
+    if (not all(math.isfinite(v) for v in vals) or d['stepMin'] <= 0 or d['stepMax'] < d['stepMin']
+            or d['stepInit'] < d['stepMin'] or d['stepInit'] > d['stepMax'] or d['targetAccept'] <= 0
+            or d['targetAccept'] >= 1 or d['stepAdapt'] <= 0):
+        raise ValueError('Invalid Wyckoff step adaptation settings.')
+    out = {'STEP_MIN': d['stepMin'], 'STEP_MAX': d['stepMax'],
+           'STEP_UP': math.exp(min(700.0, d['stepAdapt'] * (1 - d['targetAccept']))),
+           'STEP_DOWN': math.exp(-d['stepAdapt'] * d['targetAccept'])}
+    for k, v in out.items():
+        with np.errstate(over='ignore'):
+            f = np.float32(v)
+        if not np.isfinite(f) or f <= 0:
+            raise ValueError('Wyckoff adaptation exceeds GPU float limits.')
+    return out
+
+
+class WyckoffSession:
+    """One device session: the buffers and kernel of one search (swarm_wyckoff.js:1293-1720)."""
+
+    def __init__(self, problem: WyckoffProblem, num_particles: int, run_key: int = 1, cos_mode: int = 0,
+                 device: int = 0, settings: Optional[dict] = None, max_coord_slots: Optional[int] = None):
+        self.lib = _lib.load()
+        self.problem = problem
+        self.num_particles = int(num_particles)
+        T = problem.tables
+        R = problem.restraints
+        ad = adaptation(settings)
+        self._keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.POINTER(np.ctypeslib.as_ctypes_type(dt)))
+
+        pr = P6WyProblem()
+        pr.num_particles = self.num_particles
+        pr.gen_pack = arr(T.gen_pack, np.uint32)
+        pr.n_assign = len(problem.assignments)
+        pr.n_tot = T.n_tot
+        pr.sym_packed = arr(problem.sym_packed, np.float32)
+        pr.n_ops = len(problem.group.ops)
+        pr.site_proj = arr(T.site_proj, np.float32)
+        pr.max_sites = T.max_sites
+        pr.refl_pack = arr(problem.refl.refl_pack, np.uint32)
+        pr.n_refl = problem.refl.n_refl
+        pr.group_meta = arr(problem.refl.group_meta, np.float32)
+        pr.n_groups = problem.refl.n_groups
+        pr.group_stride = problem.refl.group_stride
+        pr.f_tab = arr(problem.f_tab, np.float32)
+        pr.n_elem = problem.n_elem
+        pr.restraint_tables = arr(R.tables, np.float32)
+        pr.n_restraint_floats = len(R.tables)
+        pr.r_min_off = R.r_min_off
+        pr.rule_off = R.rule_off
+        pr.n_rules = R.n_rules
+        slots = max(64, R.slots_needed) if max_coord_slots is None else max_coord_slots
+        pr.max_coord_slots = slots
+        pr.geom_slots = slots if R.geometry else 1
+        for i in range(9):
+            pr.orth[i] = float(problem.orth[i])
+            pr.xform[i] = float(problem.xform[i])
+            pr.inv_orth[i] = float(problem.inv_orth[i])
+        pr.min_image_shell = problem.min_image_shell
+        pr.count_shell = 1
+        pr.centro = 1 if problem.centro else 0
+        pr.pen_clash = problem.pen_clash
+        pr.pen_bond = problem.pen_bond
+        pr.pen_coord = problem.pen_coord
+        pr.pen_geom = problem.pen_geom
+        pr.poly_prob = 0.0
+        pr.step_up, pr.step_down = ad['STEP_UP'], ad['STEP_DOWN']
+        pr.step_min, pr.step_max = ad['STEP_MIN'], ad['STEP_MAX']
+        pr.cos_mode = int(cos_mode)
+        pr.run_key = int(run_key) & 0xFFFFFFFF
+        self.adapt = ad
+        h = C.c_void_p()
+        check(self.lib.p6_wy_create(C.byref(pr), int(device), C.byref(h)))
+        self.h = h
+        self.coords_per_particle = T.max_sites * 3
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.p6_wy_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference device operations -------------------------------------------
+    def set_assign(self, assign_of: np.ndarray):
+        a = np.ascontiguousarray(assign_of, dtype=np.uint32)
+        check(self.lib.p6_wy_set_assign(self.h, ptr(a)))
+
+    def set_params(self, n_groups_active: int, pen_scale: float):
+        check(self.lib.p6_wy_set_params(self.h, int(n_groups_active), float(pen_scale)))
+
+    def sync_state(self, positions: np.ndarray, state: np.ndarray):
+        p = np.ascontiguousarray(positions, dtype=np.float32)
+        s = np.ascontiguousarray(state, dtype=STATE_DTYPE)
+        check(self.lib.p6_wy_sync_state(self.h, ptr(p), ptr(s)))
+
+    def read_state(self):
+        n = self.num_particles * self.coords_per_particle
+        pos = np.zeros(n, dtype=np.float32)
+        best = np.zeros(n, dtype=np.float32)
+        st = np.zeros(self.num_particles, dtype=STATE_DTYPE)
+        check(self.lib.p6_wy_read_state(self.h, ptr(pos), ptr(best), ptr(st)))
+        return pos, best, st
+
+    def dispatch(self, coords: Optional[np.ndarray] = None, mcmc: bool = False):
+        c = None if coords is None else np.ascontiguousarray(coords, dtype=np.float32)
+        check(self.lib.p6_wy_dispatch(self.h, ptr(c), 1 if mcmc else 0))
+
+    def evaluate_sync(self, coords: Optional[np.ndarray] = None, mcmc: bool = False):
+        c = None if coords is None else np.ascontiguousarray(coords, dtype=np.float32)
+        out = np.zeros(2 * self.num_particles, dtype=np.float32)
+        check(self.lib.p6_wy_evaluate_sync(self.h, ptr(c), 1 if mcmc else 0, ptr(out)))
+        return out[:self.num_particles], out[self.num_particles:]
+
+    # -- fused device path -----------------------------------------------------
+    def set_ladders(self, ladders: np.ndarray, rungs: int):
+        l = np.ascontiguousarray(ladders, dtype=np.int32)
+        check(self.lib.p6_wy_set_ladders(self.h, ptr(l), len(l) // rungs, int(rungs)))
+
+    def set_schedule(self, groups: np.ndarray, pen: np.ndarray):
+        g = np.ascontiguousarray(groups, dtype=np.int32)
+        p = np.ascontiguousarray(pen, dtype=np.float32)
+        check(self.lib.p6_wy_set_schedule(self.h, ptr(g), ptr(p), len(g)))
+
+    def run(self, gen0: int, n_gen: int, swap_every: int, reeval_first: bool = True):
+        check(self.lib.p6_wy_run(self.h, int(gen0), int(n_gen), int(swap_every), 1 if reeval_first else 0))
+
+    def run_host(self, positions: np.ndarray, state: np.ndarray, gen0: int, n_gen: int, swap_every: int,
+                 reeval_first: bool = True):
+        n = self.num_particles * self.coords_per_particle
+        p = np.ascontiguousarray(positions, dtype=np.float32)
+        s = np.ascontiguousarray(state, dtype=STATE_DTYPE)
+        pos = np.zeros(n, dtype=np.float32)
+        best = np.zeros(n, dtype=np.float32)
+        st = np.zeros(self.num_particles, dtype=STATE_DTYPE)
+        check(self.lib.p6_wy_run_host(self.h, ptr(p), ptr(s), int(gen0), int(n_gen), int(swap_every),
+                                      1 if reeval_first else 0, ptr(pos), ptr(best), ptr(st)))
+        return pos, best, st
+
+    def synchronize(self, timeout: float = 60.0):
+        check(self.lib.p6_wy_synchronize(self.h, float(timeout)))
+
+    # -- parity support --------------------------------------------------------
+    def write_positions_fixed(self, x: np.ndarray):
+        a = np.ascontiguousarray(x, dtype=np.uint32)
+        check(self.lib.p6_wy_write_positions_fixed(self.h, ptr(a)))
+
+    def read_positions_fixed(self):
+        n = self.num_particles * self.coords_per_particle
+        cur = np.zeros(n, dtype=np.uint32)
+        best = np.zeros(n, dtype=np.uint32)
+        check(self.lib.p6_wy_read_positions_fixed(self.h, ptr(cur), ptr(best)))
+        return cur, best
+
+    def set_trace(self, on: bool):
+        check(self.lib.p6_wy_set_trace(self.h, 1 if on else 0))
+
+    def read_trace(self):
+        props = np.zeros(self.num_particles * self.coords_per_particle, dtype=np.uint32)
+        rec = np.zeros(self.num_particles * 8, dtype=np.float32)
+        check(self.lib.p6_wy_read_trace(self.h, ptr(props), ptr(rec)))
+        return props, rec.reshape(-1, 8)
+
+    def read_trace_ic(self):
+        ic = np.zeros(self.num_particles * self.problem.refl.n_refl, dtype=np.float32)
+        check(self.lib.p6_wy_read_trace_ic(self.h, ptr(ic)))
+        return ic.reshape(self.num_particles, -1)
+
+    def debug_expand(self, particle: int):
+        out = np.zeros(self.problem.n_tot * 3, dtype=np.uint32)
+        check(self.lib.p6_wy_debug_expand(self.h, int(particle), ptr(out)))
+        return out
+
+    def last_kernel_ms(self) -> float:
+        v = C.c_float()
+        check(self.lib.p6_wy_last_kernel_ms(self.h, C.byref(v)))
+        return v.value
+
+    def launch_count(self) -> int:
+        v = C.c_longlong()
+        check(self.lib.p6_wy_launch_count(self.h, C.byref(v)))
+        return v.value
+
+
+# ---------------------------------------------------------------------------
+# Search schedule
+# ---------------------------------------------------------------------------
+def build_ladders(assign_of: np.ndarray, rungs: int = 8, temp_cold: float = 5e-4, temp_hot: float = 0.05):
+    """Ladders of ``rungs`` chains of one assignment, geometric temperatures from
+    cold to hot; leftover chains sit on the cold rung as singleton ladders
+    (js/swarm_wyckoff.js:1784-1808).  Returns (ladder table, temperature per chain)."""
+    R = max(2, rungs)
+    ratio = (temp_hot / temp_cold) ** (1 / (R - 1))
+    rung_temp = [temp_cold * ratio ** r for r in range(R)]
+    temp = np.zeros(len(assign_of), dtype=np.float32)
+    by = {}
+    for i, A in enumerate(assign_of):
+        by.setdefault(int(A), []).append(i)
+    table = []
+    for chains in by.values():
+        c = 0
+        while c + R <= len(chains):
+            lad = chains[c:c + R]
+            for r, ci in enumerate(lad):
+                temp[ci] = rung_temp[r]
+            table.extend(lad)
+            c += R
+        for ci in chains[c:]:
+            temp[ci] = rung_temp[0]
+            table.extend([ci] + [-1] * (R - 1))
+    return np.array(table, dtype=np.int32), temp
+
+
+def schedule(generations: int, n_groups: int, settings: Optional[dict] = None):
+    """nGroupsActive and penScale per generation (js/swarm_wyckoff.js:2218-2230)."""
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    groups = np.zeros(generations, dtype=np.int32)
+    pen = np.zeros(generations, dtype=np.float32)
+    for gen in range(generations):
+        t = gen / (generations - 1) if generations > 1 else 1.0
+        level = min(d['rampSteps'] - 1, int(math.floor(t * d['rampSteps'])))
+        groups[gen] = ramped_group_count(n_groups, level, d['rampSteps'] - 1, d['rampStart'], d['rampFull'])
+        pen[gen] = d['penRampStart'] + t * (d['penRampEnd'] - d['penRampStart'])
+    return groups, pen
+
+
+def project_all(problem: WyckoffProblem, positions: np.ndarray, assign_of: np.ndarray):
+    """projectSites for every particle, vectorised (js/wyckoff_assign.js:1155-1187)."""
+    T = problem.tables
+    ms = T.max_sites
+    P = positions.reshape(len(assign_of), ms, 3).astype(np.float64)
+    sp = T.site_proj.reshape(-1, ms, 12).astype(np.float64)[assign_of]        # (n, ms, 12)
+    out = np.einsum('nsij,nsj->nsi', sp[:, :, :9].reshape(len(assign_of), ms, 3, 3), P) + sp[:, :, 9:]
+    out -= np.floor(out)
+    nS = T.site_count[assign_of]
+    mask = np.arange(ms)[None, :] < nS[:, None]
+    out[~mask] = 0
+    return out.reshape(-1).astype(np.float32)
+
+
+def initial_state(n: int, temps: np.ndarray, rnd: Callable[[], float], settings: Optional[dict] = None):
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    st = np.zeros(n, dtype=STATE_DTYPE)
+    st['fit'] = -np.inf
+    st['cc'] = np.nan
+    st['pen'] = 0
+    st['step_size'] = d['stepInit']
+    st['temp'] = temps
+    st['seed'] = [int(rnd() * 4294967296) & 0xFFFFFFFF for _ in range(n)]
+    st['best_fit'] = -1e30
+    return st
+
+
+def cpu_cross_check(problem: WyckoffProblem, coords: np.ndarray, assign: int = 0) -> float:
+    """FP64 re-score of one structure from the packed arrays (the report's
+    cross-check, js/swarm_wyckoff.js:2524-2563)."""
+    T = problem.tables
+    ms = T.max_sites
+    sp = T.site_proj[assign * ms * 12:(assign + 1) * ms * 12].astype(np.float64).reshape(ms, 12)
+    x = np.asarray(coords, dtype=np.float64).reshape(ms, 3)
+    proj = np.einsum('sij,sj->si', sp[:, :9].reshape(ms, 3, 3), x) + sp[:, 9:]
+    proj -= np.floor(proj)
+    gp = T.gen_pack[assign * T.n_tot:(assign + 1) * T.n_tot].astype(np.int64)
+    site, op, ty, skip = gp & 0xFF, (gp >> 8) & 0xFFF, (gp >> 20) & 0xF, (gp >> 24) & 1
+    sym = problem.sym_packed.astype(np.float64).reshape(-1, 12)
+    R = sym[op, :9].reshape(-1, 3, 3)
+    t = sym[op, 9:]
+    g = np.einsum('aij,aj->ai', R, proj[site]) + t
+    g -= np.floor(g)
+    keep = skip == 0
+    g, ty = g[keep], np.minimum(ty[keep], problem.n_elem - 1)
+    pk = problem.refl.refl_pack[0::2].astype(np.int64)
+    hkl = np.stack([(pk & 0x3FF) - 512, ((pk >> 10) & 0x3FF) - 512, ((pk >> 20) & 0x3FF) - 512], 1).astype(np.float64)
+    mult = problem.refl.refl_pack[1::2].astype(np.float64)
+    q = hkl @ g.T
+    ph = 2 * np.pi * (q - np.floor(q))
+    f = problem.f_tab.astype(np.float64).reshape(-1, problem.n_elem)[:, ty]
+    fr = (f * np.cos(ph)).sum(1)
+    fi = (f * np.sin(ph)).sum(1)
+    ic = mult * (fr * fr + fi * fi)
+    gm = problem.refl.group_meta.astype(np.float64).reshape(-1, problem.refl.group_stride)
+    scc = soo = sco = 0.0
+    for row in gm:
+        w = row[3] if problem.refl.group_stride >= 4 else 1.0
+        if not w > 0:
+            continue
+        c = ic[int(row[0]):int(row[0]) + int(row[1])].sum()
+        scc += w * c * c
+        soo += w * row[2] * row[2]
+        sco += w * c * row[2]
+    den = scc * soo
+    if not den > 1e-20 or not sco > 0:
+        return 0.0
+    ex = min(1.0, max(0.0, sco * sco / den))
+    return min(1.0, max(0.0, 1 - math.sqrt(max(0.0, 1 - ex))))
+
+
+@dataclass
+class SearchResult:
+    best_cc: float
+    best_pen: float
+    best_coords: np.ndarray
+    trials: int
+    kernel_ms: float
+    accept_rate: float
+    swap_rate: float
+    launches: int
+    seed: int
+    cpu_check: Dict[str, float] = field(default_factory=dict)
+
+
+def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
+                       restarts: int = 1, seed: int = 20261026, cos_mode: int = 0, chunk: Optional[int] = None,
+                       settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
+                       on_progress: Optional[Callable[[dict], None]] = None,
+                       should_stop: Optional[Callable[[], bool]] = None) -> SearchResult:
+    """One assignment list, ``restarts`` independent restarts, all generations on
+    the device.  The per-assignment best is re-scored at full resolution and the
+    final penalty weight and cross-checked on the CPU, as the reference reports."""
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    rnd = mulberry32(seed)
+    own = session is None
+    sess = session or WyckoffSession(problem, num_particles, run_key=seed, cos_mode=cos_mode, settings=settings)
+    n = sess.num_particles
+    nA = len(problem.assignments)
+    assign_of = (np.arange(n) % nA).astype(np.uint32) if nA > 1 else np.zeros(n, dtype=np.uint32)
+    assign_of.sort()
+    sess.set_assign(assign_of)
+    ladders, temps = build_ladders(assign_of, int(d['rungs']), d['tempCold'], d['tempHot'])
+    sess.set_ladders(ladders, max(2, int(d['rungs'])))
+    groups, pen = schedule(generations, problem.refl.n_groups, d)
+    sess.set_schedule(groups, pen)
+    chunk = chunk or generations
+    best = {'cc': -np.inf, 'pen': 0.0, 'coords': None, 'A': 0}
+    total_ms = 0.0
+    acc_total = 0
+    swaps0 = None
+    for restart in range(restarts):
+        pos = np.array([rnd() for _ in range(n * sess.coords_per_particle)], dtype=np.float32)
+        pos = project_all(problem, pos, assign_of)
+        st = initial_state(n, temps, rnd, d)
+        sess.sync_state(pos, st)
+        g0 = 0
+        while g0 < generations:
+            if should_stop and should_stop():
+                break
+            ng = min(chunk, generations - g0)
+            reeval = g0 == 0 or groups[g0] != groups[g0 - 1]
+            sess.run(g0, ng, int(d['swapEvery']), reeval)
+            sess.synchronize(600.0)
+            total_ms += sess.last_kernel_ms()
+            g0 += ng
+            if on_progress:
+                on_progress({'restart': restart + 1, 'restarts': restarts, 'generation': g0 - 1,
+                             'generations': generations})
+        cur, bestpos, st = sess.read_state()
+        acc_total += int(st['accepted'].sum())
+        scale = float(pen[-1])
+        score = np.where(st['best_fit'] > -1e29, st['best_cc'] - st['best_pen'] * scale, -np.inf)
+        i = int(np.argmax(score))
+        if score[i] > best['cc'] - best['pen'] * scale:
+            cpp = sess.coords_per_particle
+            best = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
+                    'coords': bestpos[i * cpp:(i + 1) * cpp].copy(), 'A': int(assign_of[i])}
+    trials = n * generations * restarts
+    res = SearchResult(best['cc'], best['pen'], best['coords'], trials, total_ms,
+                       acc_total / max(1, trials), float('nan'), sess.launch_count(), seed)
+    if best['coords'] is not None:
+        cpu = cpu_cross_check(problem, best['coords'], best['A'])
+        res.cpu_check = {'gpu': best['cc'], 'cpu': cpu, 'delta': abs(best['cc'] - cpu)}
+    if own:
+        sess.close()
+    return res

@@ -1,0 +1,184 @@
+"""Seeded synthetic problems with the shapes of the benchmark configurations.
+
+The reference measures no public dataset for this path; these generators stand
+in for real extracted intensities with the stated cells, sites, resolution and
+noise.
+
+* ``wyckoff_problem``: a Wyckoff search problem.  Default: Pnma, a = 8.48,
+  b = 5.40, c = 6.96 A, sites Pb 4c, S 4c, O 4c, O 4c, O 8d (PbSO4-like),
+  seeded random true coordinates, |F|^2 of every unique reflection to
+  d_min = 1.2 A with X-ray f(s) (Waasmaier-Kirfel) and overall B = 0, 2 %
+  Gaussian noise and sigma = 2 % of the noiseless value.
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .crystal import inverse3, orth_matrix, reduced_cell
+from .reflections import (PackedReflections, gaussian_form_factor, generate_reflections, pack_reflections,
+                          scattering_table)
+from .symmetry import SpaceGroup, has_inversion_at_origin, space_group
+from .wyckoff_tables import (Assignment, AssignmentTables, RestraintTables, build_assignment_tables,
+                             build_restraint_tables, make_assignment, pack_sym_ops)
+
+DATA = Path(__file__).resolve().parent / 'data'
+
+
+def load_form_factor_table() -> Dict[str, dict]:
+    return json.loads((DATA / 'xray_wk1995_subset.json').read_text())['table']
+
+
+def mulberry32(seed: int):
+    """The reference's seeded host stream (js/swarm_wyckoff.js:354-363)."""
+    s = seed & 0xFFFFFFFF
+
+    def rnd():
+        nonlocal s
+        s = (s + 0x6D2B79F5) & 0xFFFFFFFF
+        t = s
+        t = ((t ^ (t >> 15)) * (t | 1)) & 0xFFFFFFFF
+        t ^= (t + ((t ^ (t >> 7)) * (t | 61) & 0xFFFFFFFF)) & 0xFFFFFFFF
+        return ((t ^ (t >> 14)) & 0xFFFFFFFF) / 4294967296.0
+    return rnd
+
+
+@dataclass
+class WyckoffProblem:
+    group: SpaceGroup
+    cell: Dict[str, float]
+    demand: List[dict]
+    assignments: List[Assignment]
+    tables: AssignmentTables
+    refl: PackedReflections
+    f_tab: np.ndarray
+    n_elem: int
+    restraints: RestraintTables
+    sym_packed: np.ndarray
+    centro: bool
+    orth: np.ndarray
+    xform: np.ndarray
+    inv_orth: np.ndarray
+    min_image_shell: int
+    true_coords: Optional[np.ndarray] = None
+    rows: List[dict] = field(default_factory=list)
+    pen_clash: float = 0.05
+    pen_bond: float = 0.10
+    pen_coord: float = 0.03
+    pen_geom: float = 1.0
+
+    @property
+    def n_tot(self) -> int:
+        return self.tables.n_tot
+
+    @property
+    def max_sites(self) -> int:
+        return self.tables.max_sites
+
+
+def structure_factors_fp64(group: SpaceGroup, assignment: Assignment, coords: np.ndarray,
+                           hkl: np.ndarray, f_of: np.ndarray) -> np.ndarray:
+    """|F|^2 of the full cell (every image, both sine and cosine), FP64.
+    hkl (n, 3) ints; f_of (n, nElem) scattering factors per reflection."""
+    F = np.zeros(len(hkl), dtype=np.complex128)
+    h = hkl.astype(np.float64)
+    for si, s in enumerate(assignment.sites):
+        p = s.w.project(*coords[si * 3:si * 3 + 3])
+        for oi in s.w.coset_ops:
+            o = group.ops[oi]
+            x = np.array([sum(o.r[3 * i + k] * p[k] for k in range(3)) + o.t_frac[i] for i in range(3)])
+            x -= np.floor(x)
+            F += f_of[:, s.element_idx] * np.exp(2j * np.pi * (h @ x))
+    return np.abs(F) ** 2
+
+
+def _min_contact(group: SpaceGroup, assignment: Assignment, coords: np.ndarray, red) -> float:
+    """Shortest nearest-image distance between any two atoms of the generated cell."""
+    pts = []
+    for si, s in enumerate(assignment.sites):
+        p = s.w.project(*coords[si * 3:si * 3 + 3])
+        for oi in s.w.coset_ops:
+            o = group.ops[oi]
+            pts.append([sum(o.r[3 * i + k] * p[k] for k in range(3)) + o.t_frac[i] for i in range(3)])
+    x = np.array(pts) % 1.0
+    d = x[:, None, :] - x[None, :, :]
+    q = np.einsum('ij,abj->abi', red.xform.reshape(3, 3), d)
+    q -= np.round(q)
+    c = np.einsum('ij,abj->abi', red.orth.reshape(3, 3), q)
+    r = np.sqrt((c ** 2).sum(-1))
+    np.fill_diagonal(r, np.inf)
+    return float(r.min()) if len(x) > 1 else np.inf
+
+
+def wyckoff_problem(seed: int = 1, group_number: int = 62,
+                    cell: Optional[Dict[str, float]] = None,
+                    composition: Sequence[Tuple[str, int]] = (('Pb', 4), ('S', 4), ('O', 16)),
+                    sites: Sequence[Tuple[str, str]] = (('Pb', '4c'), ('S', '4c'), ('O', '4c'), ('O', '4c'),
+                                                        ('O', '8d')),
+                    dmin: float = 1.2, wavelength: float = 1.5406, noise: float = 0.02,
+                    windows: Sequence[dict] = (), min_contact: Optional[float] = None,
+                    extra_assignments: Sequence[Sequence[Tuple[str, str]]] = (),
+                    true_min_contact: float = 1.6) -> WyckoffProblem:
+    cell = dict(cell or {'a': 8.48, 'b': 5.40, 'c': 6.96, 'alpha': 90.0, 'beta': 90.0, 'gamma': 90.0})
+    group = space_group(group_number)
+    ff_table = load_form_factor_table()
+    demand = [{'element': el, 'count': n, 'z': ff_table[el]['Z'] if el in ff_table else 1} for el, n in composition]
+    assignment = make_assignment(group, demand, sites)
+    assignments = [assignment] + [make_assignment(group, demand, a) for a in extra_assignments]
+    tables = build_assignment_tables(assignments, group, demand)
+    rng = np.random.default_rng(seed)
+    red0 = reduced_cell(cell)
+    true = np.zeros(tables.max_sites * 3)
+    for _attempt in range(2000):
+        for si, s in enumerate(assignment.sites):
+            true[si * 3:si * 3 + 3] = np.array(s.w.project(*rng.random(3))) % 1.0
+        if _min_contact(group, assignment, true, red0) >= true_min_contact:
+            break
+    refs = generate_reflections(cell, group.ops, dmin, with_eq=False)
+    if tables.centring:
+        refs = [r for r in refs if all(abs((r.h * c[0] + r.k * c[1] + r.l * c[2]) -
+                                           round(r.h * c[0] + r.k * c[1] + r.l * c[2])) < 1e-6
+                                       for c in tables.centring)]
+    hkl = np.array([[r.h, r.k, r.l] for r in refs], dtype=np.int64)
+    ff = gaussian_form_factor(ff_table)
+    s_arr = np.array([1.0 / r.d0 for r in refs])
+    f_of = np.array([[ff(d['element'], s) for d in demand] for s in s_arr])
+    I = structure_factors_fp64(group, assignment, true, hkl, f_of)
+    floor_ = 1e-3 * float(np.mean(I)) if len(I) else 1.0
+    rows = []
+    for r, i_true in zip(refs, I):
+        sigma = noise * max(i_true, floor_)
+        fo2 = i_true + rng.normal() * sigma
+        tth = 2 * math.degrees(math.asin(min(1.0, wavelength / (2 * r.d0))))
+        rows.append({'h': r.h, 'k': r.k, 'l': r.l, 'mult': r.m, 'Fo2': fo2, 'sigma': sigma, 'd': r.d0, 'tth': tth})
+    refl = pack_reflections(rows)
+    f_tab, n_elem, _missing = scattering_table(refl, demand, ff, 0.0)
+    restraints = build_restraint_tables(demand, list(windows), min_contact)
+    red = reduced_cell(cell)
+    orth0 = orth_matrix(cell).astype(np.float64)
+    prob = WyckoffProblem(group, cell, demand, assignments, tables, refl, f_tab, n_elem, restraints,
+                          pack_sym_ops(group.ops), has_inversion_at_origin(group.ops), red.orth, red.xform,
+                          inverse3(orth0), 1 if restraints.max_distance > red.safe_radius else 0, true, rows)
+    # penBond / penCoord per charged slot (js/swarm_wyckoff.js:1482-1506)
+    n_of = {d['element'].upper(): d['count'] for d in demand}
+    bond_slots, coord_centres = 0, 0
+    for w in windows:
+        nA = n_of.get(str(w['a']).upper(), 0)
+        if not nA:
+            continue
+        has_count = w.get('count') is not None and w['count'] > 0
+        if has_count:
+            bond_slots += nA * w['count']
+            coord_centres += nA
+        elif w.get('dmax') is not None:
+            bond_slots += nA
+            if w.get('bothWays', True) is not False and str(w['a']).upper() != str(w['b']).upper():
+                bond_slots += n_of.get(str(w['b']).upper(), 0)
+    prob.pen_bond = 0.10 / max(1, bond_slots)
+    prob.pen_coord = 0.03 / max(1, coord_centres)
+    return prob

@@ -1,0 +1,304 @@
+"""Wyckoff trial kernel on the GPU, through the C ABI, against the FP64 oracle.
+
+Tolerances (stated per test): the fitness cc = 1 - wR2 and the per-reflection
+mult |F|^2 are FP32 arithmetic on exactly reduced integer phases; the oracle
+is FP64.  Orbit expansion and proposals on the Wyckoff subspace are integer
+arithmetic and are compared bit for bit."""
+import math
+
+import numpy as np
+import pytest
+
+from powder6_b200 import _lib
+from powder6_b200.swarm_wyckoff import (STATE_DTYPE, WyckoffSession, build_ladders, initial_state, project_all,
+                                        run_wyckoff_search, schedule)
+from powder6_b200.workloads import mulberry32, wyckoff_problem
+
+pytestmark = pytest.mark.gpu
+
+TWO32 = 2.0 ** 32
+
+
+def to_fixed(x):
+    f = np.asarray(x, dtype=np.float64)
+    f = f - np.floor(f)
+    v = np.floor(f * TWO32 + 0.5)
+    v[v >= TWO32] -= TWO32
+    return v.astype(np.uint64).astype(np.uint32)
+
+
+def trans_fixed(t):
+    s = t * 24.0
+    r = math.floor(s + 0.5)
+    assert abs(s - r) < 1e-4
+    n = int(r) % 24
+    return (n * 2 ** 32 + 12) // 24
+
+
+def random_positions(P, n, seed):
+    rng = np.random.default_rng(seed)
+    assign = np.zeros(n, dtype=np.uint32)
+    pos = project_all(P, rng.random(n * P.max_sites * 3).astype(np.float32), assign)
+    return to_fixed(pos.astype(np.float64)), assign
+
+
+def oracle_cc_pen(O, P, X_sites, n_groups, pen_scale, n_rules=0, slots=64, geom_slots=1):
+    """FP64 fitness and penalty of already-projected fixed-point site coordinates."""
+    x = X_sites.astype(np.float64) / TWO32
+    gp = P.tables.gen_pack[:P.n_tot]
+    cc, sums = O.wy_fitness_projected(x, gp, P.sym_packed, P.refl.group_meta, n_groups, 4, P.refl.refl_pack,
+                                      P.f_tab, P.n_elem, P.centro)
+    geom = O.make_geom(P.orth, P.xform, P.min_image_shell, 1, P.pen_clash, P.pen_bond, P.pen_coord, P.pen_geom,
+                       pen_scale)
+    pen = O.wy_penalty(x, gp, P.sym_packed, P.n_elem, P.restraints.tables, P.restraints.r_min_off,
+                       P.restraints.rule_off, P.restraints.n_rules, slots, geom_slots, geom)
+    return cc, pen, sums
+
+
+def icalc_fp64(P, X_sites):
+    """mult |F|^2 per reflection, FP64, from fixed-point sites (the oracle's arithmetic)."""
+    x = X_sites.astype(np.float64) / TWO32
+    ms = P.max_sites
+    gp = P.tables.gen_pack[:P.n_tot].astype(np.int64)
+    site, op, ty, skip = gp & 0xFF, (gp >> 8) & 0xFFF, (gp >> 20) & 0xF, (gp >> 24) & 1
+    sym = P.sym_packed.astype(np.float64).reshape(-1, 12)
+    g = np.einsum('aij,aj->ai', sym[op, :9].reshape(-1, 3, 3), x.reshape(ms, 3)[site]) + sym[op, 9:]
+    g = g[skip == 0]
+    ty = ty[skip == 0]
+    pk = P.refl.refl_pack[0::2].astype(np.int64)
+    hkl = np.stack([(pk & 0x3FF) - 512, ((pk >> 10) & 0x3FF) - 512, ((pk >> 20) & 0x3FF) - 512], 1)
+    q = hkl @ g.T
+    f = P.f_tab.astype(np.float64).reshape(-1, P.n_elem)[:, ty]
+    F = (f * np.exp(2j * np.pi * (q - np.floor(q)))).sum(1)
+    return P.refl.refl_pack[1::2] * np.abs(F) ** 2
+
+
+@pytest.fixture(scope='module')
+def prob():
+    return wyckoff_problem(seed=1)
+
+
+def test_philox_device_known_answer():
+    lib = _lib.load()
+    for ctr, key, exp in [([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+                          ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+                           [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1])]:
+        c = np.array(ctr, dtype=np.uint32)
+        k = np.array(key, dtype=np.uint32)
+        o = np.zeros(4, dtype=np.uint32)
+        _lib.check(lib.p6_philox_device(_lib.ptr(c), _lib.ptr(k), _lib.ptr(o)))
+        assert list(o) == exp
+
+
+def test_orbit_expansion_bit_exact(prob, oracle):
+    P = prob
+    n = 64
+    X, assign = random_positions(P, n, 3)
+    with WyckoffSession(P, n) as s:
+        s.write_positions_fixed(X)
+        rint = np.array([o.r for o in P.group.ops], dtype=np.int32).reshape(-1)
+        tf = np.array([[trans_fixed(float(v)) for v in P.sym_packed.reshape(-1, 12)[o, 9:]]
+                       for o in range(len(P.group.ops))], dtype=np.uint64).astype(np.uint32).reshape(-1)
+        for p in (0, 17, 63):
+            got = s.debug_expand(p)
+            sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
+            want = oracle.expand_fixed(sites, P.tables.gen_pack[:P.n_tot], rint, tf)
+            assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize('cos_mode,cc_tol,ic_tol', [(0, 2e-6, 2e-4), (1, 5e-7, 5e-6)])
+def test_evaluation_parity(prob, oracle, cos_mode, cc_tol, ic_tol):
+    """cc within cc_tol (absolute, on a [0, 1] fitness), penalty within 1e-5
+    relative, and mult |F|^2 within ic_tol relative to the largest reflection
+    of each structure (FP32 sum of FP32 cosines vs FP64)."""
+    P = prob
+    n = 256
+    X, assign = random_positions(P, n, 5 + cos_mode)
+    # put the first particles on the true structure and close to it
+    tx = to_fixed(P.true_coords)
+    X[:P.max_sites * 3] = tx
+    with WyckoffSession(P, n, cos_mode=cos_mode) as s:
+        s.write_positions_fixed(X)
+        s.set_trace(True)
+        worst_cc = worst_ic = worst_pen = 0.0
+        for nga, scale in ((P.refl.n_groups, 1.0), (max(8, P.refl.n_groups // 4), 2.5)):
+            s.set_params(nga, scale)
+            s.dispatch(None, mcmc=False)
+            s.synchronize(60)
+            _, _, st = s.read_state()
+            ic = s.read_trace_ic()
+            for p in range(n):
+                sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
+                cc, pen, _ = oracle_cc_pen(oracle, P, sites, nga, scale)
+                worst_cc = max(worst_cc, abs(float(st['cc'][p]) - cc))
+                worst_pen = max(worst_pen, abs(float(st['pen'][p]) * scale - pen) / max(1.0, pen))
+                assert abs(float(st['fit'][p]) - (cc - pen)) < cc_tol + 1e-5 * max(1.0, pen)
+                if nga == P.refl.n_groups and p < 32:
+                    ref = icalc_fp64(P, sites)
+                    worst_ic = max(worst_ic, float(np.max(np.abs(ic[p] - ref)) / ref.max()))
+        print(f'cos_mode {cos_mode}: max |dcc| {worst_cc:.3e}, max rel |d mult F^2| {worst_ic:.3e}, '
+              f'max rel dpen {worst_pen:.3e}')
+        assert worst_cc <= cc_tol
+        assert worst_ic <= ic_tol
+        assert worst_pen <= 1e-5
+        assert float(st['cc'][0]) > 0.95
+
+
+def test_mcmc_step_parity_and_proposals(prob, oracle):
+    """One generation with tracing: each proposal is re-scored by the oracle,
+    the acceptance follows the kernel's own rule, unmoved sites are bit-identical,
+    moved sites lie on their Wyckoff subspace, and the state update matches."""
+    P = prob
+    n = 512
+    X, assign = random_positions(P, n, 9)
+    rnd = mulberry32(4)
+    temps = np.full(n, 0.01, dtype=np.float32)
+    st0 = initial_state(n, temps, rnd)
+    with WyckoffSession(P, n, run_key=77) as s:
+        s.write_positions_fixed(X)
+        s.set_params(P.refl.n_groups, 1.0)
+        s.dispatch(None, mcmc=False)                       # measure the current state first
+        s.synchronize(60)
+        _, _, st = s.read_state()
+        st['step_size'] = 0.05
+        st['temp'] = temps
+        st['seed'] = st0['seed']
+        st['best_fit'] = -1e30
+        cur_f = np.zeros(n * P.max_sites * 3, dtype=np.float32)
+        # restore exact coordinates after sync_state (which takes float32) by rewriting fixed point
+        s.sync_state(cur_f, st)
+        s.write_positions_fixed(X)
+        s.set_trace(True)
+        s.set_params(P.refl.n_groups, 1.0)
+        s.dispatch(None, mcmc=True)
+        s.synchronize(60)
+        props, rec = s.read_trace()
+        after, best = s.read_positions_fixed()
+        _, _, st1 = s.read_state()
+    ms3 = P.max_sites * 3
+    n_single = n_coll = 0
+    worst = 0.0
+    for p in range(n):
+        x0 = X[p * ms3:(p + 1) * ms3].reshape(-1, 3)
+        x1 = props[p * ms3:(p + 1) * ms3].reshape(-1, 3)
+        moved = [i for i in range(P.max_sites) if not np.array_equal(x0[i], x1[i])]
+        if len(moved) == 1:
+            n_single += 1
+        elif len(moved) > 1:
+            n_coll += 1
+        for i in range(P.max_sites):
+            w = P.assignments[0].sites[i].w
+            if w.triplet == 'x,1/4,z':
+                assert x1[i][1] == 2 ** 30                   # y pinned exactly to 1/4
+        cc, pen, _ = oracle_cc_pen(oracle, P, props[p * ms3:(p + 1) * ms3], P.refl.n_groups, 1.0)
+        f_new, cc_g, pen_g, u, acc, f_old, temp, step_before = rec[p]
+        worst = max(worst, abs(cc_g - cc))
+        assert abs(pen_g - pen) <= 1e-5 * max(1.0, pen)
+        prob_acc = math.exp(min(0.0, f_new - f_old) / max(temp, 1e-9))
+        rule = f_new >= f_old or u < prob_acc
+        if abs(u - prob_acc) > 1e-5:                          # float vs double exp at the boundary
+            assert bool(acc) == rule
+        state_x = after[p * ms3:(p + 1) * ms3]
+        assert np.array_equal(state_x, props[p * ms3:(p + 1) * ms3] if acc else X[p * ms3:(p + 1) * ms3])
+        want_step = step_before * (s.adapt['STEP_UP'] if acc else s.adapt['STEP_DOWN'])
+        want_step = min(max(want_step, s.adapt['STEP_MIN']), s.adapt['STEP_MAX'])
+        assert abs(float(st1['step_size'][p]) - want_step) < 1e-6 * want_step
+        assert int(st1['accepted'][p]) == int(st['accepted'][p]) + int(acc)
+    assert worst <= 2e-6
+    # 3/4 single-site proposals, binomial tolerance
+    frac = n_single / max(1, n_single + n_coll)
+    assert 0.65 < frac < 0.85, frac
+
+
+def test_fused_run_is_deterministic_and_exchanges(prob):
+    P = prob
+    n = 512
+    results = []
+    for _ in range(2):
+        rnd = mulberry32(99)
+        assign = np.zeros(n, dtype=np.uint32)
+        with WyckoffSession(P, n, run_key=12345) as s:
+            s.set_assign(assign)
+            lad, temps = build_ladders(assign)
+            s.set_ladders(lad, 8)
+            g, pen = schedule(300, P.refl.n_groups)
+            s.set_schedule(g, pen)
+            pos = project_all(P, np.array([rnd() for _ in range(n * P.max_sites * 3)], dtype=np.float32), assign)
+            st = initial_state(n, temps, rnd)
+            s.sync_state(pos, st)
+            s.run(0, 150, 10, True)
+            s.run(150, 150, 10, bool(g[150] != g[149]))
+            s.synchronize(120)
+            cur, best = s.read_positions_fixed()
+            _, _, st1 = s.read_state()
+            results.append((cur.copy(), best.copy(), st1.copy()))
+    (c0, b0, s0), (c1, b1, s1) = results
+    assert np.array_equal(c0, c1) and np.array_equal(b0, b1)
+    assert np.array_equal(s0.view(np.uint32), s1.view(np.uint32))
+    assert np.all((s0['cc'] >= 0) & (s0['cc'] <= 1))
+    assert np.all(s0['best_fit'] > -1e29)
+    acc = s0['accepted'].sum() / (n * 300)
+    assert 0.02 < acc < 0.9
+
+
+def test_search_recovers_the_true_structure(prob):
+    """wyckoff-search.js:82-84: the winner's GPU fitness agrees with the CPU
+    re-score to 1e-3; and on this synthetic problem the search finds the truth."""
+    P = prob
+    res = run_wyckoff_search(P, num_particles=1024, generations=1500, restarts=1, seed=20261026, chunk=500)
+    assert res.cpu_check['delta'] <= 1e-3
+    assert res.best_cc >= 0.95, res.best_cc
+    assert res.launches >= 3
+
+
+def test_restraint_rules_parity(oracle):
+    """Counted shells, shapes and nearest-neighbour rules (the 64-slot variant)."""
+    P = wyckoff_problem(seed=2, windows=[{'a': 'S', 'b': 'O', 'count': 4, 'dmin': 1.35, 'dmax': 1.65,
+                                          'geometry': 'tetrahedron'},
+                                         {'a': 'Pb', 'b': 'O', 'dmax': 3.2}])
+    n = 128
+    X, assign = random_positions(P, n, 21)
+    with WyckoffSession(P, n) as s:
+        s.write_positions_fixed(X)
+        s.set_params(P.refl.n_groups, 1.7)
+        s.dispatch(None, mcmc=False)
+        s.synchronize(60)
+        _, _, st = s.read_state()
+    worst = 0.0
+    for p in range(n):
+        sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
+        cc, pen, _ = oracle_cc_pen(oracle, P, sites, P.refl.n_groups, 1.7, P.restraints.n_rules, 64, 64)
+        worst = max(worst, abs(float(st['pen'][p]) * 1.7 - pen) / max(1.0, pen))
+    assert worst <= 2e-5, worst
+
+
+def test_synchronize_deadline_and_recovery(prob):
+    """A host wait that runs out returns TIMEOUT and leaves the session usable."""
+    P = prob
+    n = 4096
+    with WyckoffSession(P, n) as s:
+        assign = np.zeros(n, dtype=np.uint32)
+        lad, temps = build_ladders(assign)
+        s.set_ladders(lad, 8)
+        g, pen = schedule(2000, P.refl.n_groups)
+        s.set_schedule(g, pen)
+        s.run(0, 2000, 10, True)
+        with pytest.raises(_lib.P6Error) as e:
+            s.synchronize(1e-6)
+        assert e.value.status == 'TIMEOUT'
+        s.synchronize(120)
+        _, _, st = s.read_state()
+        assert np.isfinite(st['fit']).all()
+
+
+def test_argument_errors_are_reported():
+    P = wyckoff_problem(seed=1)
+    with pytest.raises(_lib.P6Error) as e:
+        WyckoffSession(P, 0)
+    assert e.value.status == 'INVALID_ARG'
+    with WyckoffSession(P, 16) as s:
+        with pytest.raises(_lib.P6Error) as e:
+            s.set_assign(np.full(16, 3, dtype=np.uint32))
+        assert e.value.status == 'INVALID_ARG'
+        with pytest.raises(_lib.P6Error):
+            s.run(0, 10, 10)                                  # no ladders yet
