@@ -8,7 +8,7 @@
 
 #include <string>
 
-#include "../../include/p6cuda.h"
+#include "p6cuda.h"
 
 namespace p6 {
 

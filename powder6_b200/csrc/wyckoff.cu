@@ -58,7 +58,7 @@ struct ProjFix {
   int num[9];
   int den;
   uint32_t t[3];
-  int pad[2];
+  int pad[2];  // pad[0] = 1: diagonal 0/1 projector with den 1 (keep or drop each coordinate)
 };
 
 struct RuleDev {
@@ -88,7 +88,7 @@ struct Params {
   const OpFix *ops;
   const ProjFix *proj;     // per (assignment, site)
   const unsigned char *blob;  // staged static tables
-  int blobBytes, offRefl, offF, offGroup, offRmin;
+  int blobBytes, offRefl, offF, offGroup, offRmin, offSoo, offOps, offPairs, nPairs;
   const RuleDev *rules;
   int nRules;
   int numParticles, nTot, maxSites, nRefl, nGroups, nElem, nAssign;
@@ -113,7 +113,7 @@ struct Params {
   unsigned long long *swapStats;  // [tried, taken]
   int *errFlag;
   int warpSmemBytes;       // per-warp shared-memory slice
-  int atomsOff, icOff;     // offsets inside the slice
+  int genOff, projOff, atomsOff, icOff;  // offsets inside the slice
 };
 
 // ---------------------------------------------------------------------------
@@ -225,24 +225,33 @@ __device__ __forceinline__ int64_t floor_div(int64_t a, int d) {
 
 // ---------------------------------------------------------------------------
 // Warp-level pieces of one trial.
+//
+// Work is issue-bound (every replica generation is a few thousand warp
+// instructions for a hundred or so warp-wide cosines), so the layout below
+// is chosen to minimise instructions per cosine: four reflections per lane
+// share each broadcast atom load, the phase is three integer multiply-adds,
+// the clash loop walks a balanced pair list on squared distances, the
+// constant sum of w Iobs^2 comes from a prefix table, and the chain state
+// lives in registers of lane 0.
 // ---------------------------------------------------------------------------
+constexpr int kReflPerLane = 4;
+
 struct WarpSmem {
   uint32_t cur[kMaxSites * 3];
   uint32_t prop[kMaxSites * 3];
   int4 runs[kMaxSites];
-  PState st;
   int meta[8];  // A, nRuns, nF, nSites, freeMask, particle
 };
 
-// Symmetry expansion of `sites` into atoms[0..nTot) (reordered genPack).
-__device__ __forceinline__ void expand(const Params &P, int A, const uint32_t *sites, uint4 *atoms, int lane) {
-  const uint32_t *gen = P.gen + (size_t)A * P.nTot;
+// Symmetry expansion of `sites` into atoms[0..nTot) (reordered genPack, ops in smem).
+__device__ __forceinline__ void expand(const Params &P, const uint32_t *gen, const OpFix *ops,
+                                       const uint32_t *sites, uint4 *atoms, int lane) {
   const int maxT = max(min(P.nElem, kMaxElem), 1) - 1;
   for (int i = lane; i < P.nTot; i += 32) {
-    uint32_t w = __ldg(gen + i);
-    int s = w & 0xFF, o = (w >> 8) & 0xFFF, t = min((int)((w >> 20) & 0xF), maxT);
-    const OpFix &op = P.ops[o];
-    uint32_t x = sites[s * 3], y = sites[s * 3 + 1], z = sites[s * 3 + 2];
+    const uint32_t w = gen[i];
+    const int s = w & 0xFF, o = (w >> 8) & 0xFFF, t = min((int)((w >> 20) & 0xF), maxT);
+    const OpFix &op = ops[o];
+    const uint32_t x = sites[s * 3], y = sites[s * 3 + 1], z = sites[s * 3 + 2];
     uint4 a;
     a.x = (uint32_t)op.r[0] * x + (uint32_t)op.r[1] * y + (uint32_t)op.r[2] * z + op.t[0];
     a.y = (uint32_t)op.r[3] * x + (uint32_t)op.r[4] * y + (uint32_t)op.r[5] * z + op.t[1];
@@ -252,74 +261,92 @@ __device__ __forceinline__ void expand(const Params &P, int A, const uint32_t *s
   }
 }
 
-// |F|^2 per reflection into ic[], then group sums (FP64), warp-reduced.
+// mult |F|^2 per active reflection into ic[], then the group sums scc and sco
+// (FP64).  soo, the sum of w Iobs^2, comes from the prefix table.
 template <int COSMODE>
 __device__ __forceinline__ void fitness(const Params &P, const WarpSmem &ws, const uint4 *atoms, float *ic,
-                                        const ReflRec *refl, const float *ftab, const float4 *groups, int nga,
-                                        int lane, double sums[3], float *traceIc) {
+                                        const ReflRec *refl, const float *ftab, const float4 *groups,
+                                        const double *sooPrefix, int nga, int lane, double sums[3],
+                                        float *traceIc) {
   const int nRuns = ws.meta[1];
   const int nReflAct = nga > 0 ? (int)(groups[nga - 1].x + groups[nga - 1].y) : 0;
   const bool centro = P.centro != 0;
   const int nElem = P.nElem;
-  for (int r0 = lane; r0 < nReflAct; r0 += 64) {
-    const int r1 = r0 + 32;
-    const bool has1 = r1 < nReflAct;
-    const ReflRec a0 = refl[r0];
-    const ReflRec a1 = refl[has1 ? r1 : r0];
-    const uint32_t h0 = (uint32_t)(int)a0.h, k0 = (uint32_t)(int)a0.k, l0 = (uint32_t)(int)a0.l;
-    const uint32_t h1 = (uint32_t)(int)a1.h, k1 = (uint32_t)(int)a1.k, l1 = (uint32_t)(int)a1.l;
-    const float *f0 = ftab + (size_t)r0 * nElem;
-    const float *f1 = ftab + (size_t)(has1 ? r1 : r0) * nElem;
-    float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
-    for (int k = 0; k < nRuns; ++k) {
-      const int4 run = ws.runs[k];
-      float c0 = 0.f, s0 = 0.f, c1 = 0.f, s1 = 0.f;
+  for (int base = 0; base < nReflAct; base += 32 * kReflPerLane) {
+    uint32_t h[kReflPerLane], k[kReflPerLane], l[kReflPerLane];
+    int rr[kReflPerLane];
+    float fr[kReflPerLane], fi[kReflPerLane];
+#pragma unroll
+    for (int j = 0; j < kReflPerLane; ++j) {
+      const int r = base + lane + 32 * j;
+      rr[j] = r;
+      const ReflRec a = refl[r < nReflAct ? r : 0];
+      const bool ok = r < nReflAct;
+      h[j] = ok ? (uint32_t)(int)a.h : 0u;
+      k[j] = ok ? (uint32_t)(int)a.k : 0u;
+      l[j] = ok ? (uint32_t)(int)a.l : 0u;
+      fr[j] = 0.f;
+      fi[j] = 0.f;
+    }
+    for (int q = 0; q < nRuns; ++q) {
+      const int4 run = ws.runs[q];
+      float c[kReflPerLane], sn[kReflPerLane];
+#pragma unroll
+      for (int j = 0; j < kReflPerLane; ++j) { c[j] = 0.f; sn[j] = 0.f; }
       if (centro) {
         for (int a = run.x; a < run.y; ++a) {
           const uint4 at = atoms[a];
-          c0 += cos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z);
-          c1 += cos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z);
+#pragma unroll
+          for (int j = 0; j < kReflPerLane; ++j) c[j] += cos_turn<COSMODE>(h[j] * at.x + k[j] * at.y + l[j] * at.z);
         }
       } else {
         for (int a = run.x; a < run.y; ++a) {
           const uint4 at = atoms[a];
-          float sa, ca, sb, cb;
-          sincos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z, &sa, &ca);
-          sincos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z, &sb, &cb);
-          c0 += ca; s0 += sa; c1 += cb; s1 += sb;
+#pragma unroll
+          for (int j = 0; j < kReflPerLane; ++j) {
+            float sa, ca;
+            sincos_turn<COSMODE>(h[j] * at.x + k[j] * at.y + l[j] * at.z, &sa, &ca);
+            c[j] += ca;
+            sn[j] += sa;
+          }
         }
       }
-      const float w0 = f0[run.z], w1 = f1[run.z];
-      fr0 = fmaf(w0, c0, fr0); fi0 = fmaf(w0, s0, fi0);
-      fr1 = fmaf(w1, c1, fr1); fi1 = fmaf(w1, s1, fi1);
+#pragma unroll
+      for (int j = 0; j < kReflPerLane; ++j) {
+        const int r = rr[j] < nReflAct ? rr[j] : 0;
+        const float w = ftab[r * nElem + run.z];
+        fr[j] = fmaf(w, c[j], fr[j]);
+        fi[j] = fmaf(w, sn[j], fi[j]);
+      }
     }
-    ic[r0] = (float)a0.mult * (fr0 * fr0 + fi0 * fi0);
-    if (has1) ic[r1] = (float)a1.mult * (fr1 * fr1 + fi1 * fi1);
+#pragma unroll
+    for (int j = 0; j < kReflPerLane; ++j)
+      if (rr[j] < nReflAct) {
+        const float v = (float)refl[rr[j]].mult * (fr[j] * fr[j] + fi[j] * fi[j]);
+        ic[rr[j]] = v;
+        if (traceIc) traceIc[rr[j]] = v;
+      }
   }
   __syncwarp();
-  if (traceIc)
-    for (int r = lane; r < nReflAct; r += 32) traceIc[r] = ic[r];
-  double scc = 0.0, soo = 0.0, sco = 0.0;
+  double dcc = 0.0, dco = 0.0;
   for (int g = lane; g < nga; g += 32) {
     const float4 gm = groups[g];
     if (!(gm.w > 0.f)) continue;
     const int start = (int)gm.x, cnt = (int)gm.y;
     float iCalc = 0.f;
     for (int m = 0; m < cnt; ++m) iCalc += ic[start + m];
-    const double w = gm.w, io = gm.z, c = iCalc;
-    scc += w * c * c;
-    soo += w * io * io;
-    sco += w * c * io;
+    const double wc = (double)gm.w * (double)iCalc;
+    dcc = fma(wc, (double)iCalc, dcc);
+    dco = fma(wc, (double)gm.z, dco);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    scc += __shfl_xor_sync(0xffffffffu, scc, o);
-    soo += __shfl_xor_sync(0xffffffffu, soo, o);
-    sco += __shfl_xor_sync(0xffffffffu, sco, o);
+    dcc += __shfl_xor_sync(0xffffffffu, dcc, o);
+    dco += __shfl_xor_sync(0xffffffffu, dco, o);
   }
-  sums[0] = scc;
-  sums[1] = soo;
-  sums[2] = sco;
+  sums[0] = dcc;
+  sums[1] = sooPrefix[nga];
+  sums[2] = dco;
   __syncwarp();
 }
 
@@ -331,17 +358,42 @@ __device__ __forceinline__ float cc_of(const double sums[3]) {
   return (float)fmin(1.0, fmax(0.0, cc));
 }
 
-// Clash penalty only (no distance rules): sum over pairs j > i.
-__device__ __forceinline__ float clash_penalty(const Params &P, const uint4 *atoms, const float *rmin, int lane) {
+// Squared nearest-image distance in the reduced basis (minimum-image shell 0).
+__device__ __forceinline__ float dist2_near(const Params &P, uint4 a, uint4 b) {
+  float q[3];
+  frac_delta(P, a, b, q);
+  float c[3];
+  cart_vec(P, q, c);
+  return c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+}
+
+__device__ __forceinline__ float clash_term(const Params &P, float d, float dmin) {
+  return P.penClash * (1.0f + 9.0f * ((dmin - d) / fmaxf(dmin, 1e-3f)));
+}
+
+// Clash penalty only (no distance rules): sum over pairs i < j.  Small cells
+// walk a precomputed, balanced pair list; large ones stripe j over the lanes.
+__device__ __forceinline__ float clash_penalty(const Params &P, const uint4 *atoms, const float *rmin,
+                                               const uint32_t *pairs, int lane) {
   float pen = 0.f;
   const int n = P.nTot, ne = P.nElem;
-  for (int i = lane; i < n; i += 32) {
-    const uint4 ai = atoms[i];
-    for (int j = i + 1; j < n; ++j) {
-      const uint4 aj = atoms[j];
+  if (pairs && P.minImageShell == 0) {
+    for (int idx = lane; idx < P.nPairs; idx += 32) {
+      const uint32_t pr = pairs[idx];
+      const uint4 ai = atoms[pr & 0xFFFF], aj = atoms[pr >> 16];
       const float dmin = rmin[ai.w * ne + aj.w];
-      const float d = cart_dist(P, ai, aj);
-      if (d < dmin) pen += P.penClash * (1.0f + 9.0f * ((dmin - d) / fmaxf(dmin, 1e-3f)));
+      const float d2 = dist2_near(P, ai, aj);
+      if (d2 < dmin * dmin) pen += clash_term(P, sqrtf(d2), dmin);
+    }
+  } else {
+    for (int i = 0; i < n - 1; ++i) {
+      const uint4 ai = atoms[i];
+      for (int j = i + 1 + lane; j < n; j += 32) {
+        const uint4 aj = atoms[j];
+        const float dmin = rmin[ai.w * ne + aj.w];
+        const float d = P.minImageShell ? cart_dist(P, ai, aj) : sqrtf(dist2_near(P, ai, aj));
+        if (d < dmin) pen += clash_term(P, d, dmin);
+      }
     }
   }
 #pragma unroll
@@ -386,7 +438,7 @@ __device__ float rule_penalty(const Params &P, const uint4 *atoms, const float *
       const float d = cart_dist(P, ai, aj);
       if (j != i) {
         const float dmin = rmin[ti * ne + tj];
-        if (j > i && d < dmin) pen += P.penClash * (1.0f + 9.0f * ((dmin - d) / fmaxf(dmin, 1e-3f)));
+        if (j > i && d < dmin) pen += clash_term(P, d, dmin);
       }
       if (myRules == 0) continue;
       float qf[3];
@@ -477,51 +529,54 @@ __device__ float rule_penalty(const Params &P, const uint4 *atoms, const float *
 
 template <int SLOTS>
 __device__ __forceinline__ float penalty(const Params &P, const uint4 *atoms, const float *rmin,
-                                         const float *shellLen, int lane) {
-  if (SLOTS == 0) return clash_penalty(P, atoms, rmin, lane);
+                                         const float *shellLen, const uint32_t *pairs, int lane) {
+  if (SLOTS == 0) return clash_penalty(P, atoms, rmin, pairs, lane);
   return rule_penalty<(SLOTS > 0 ? SLOTS : 1)>(P, atoms, rmin, shellLen, lane);
 }
 
-// Proposal into ws.prop: lane 0 picks the move, lanes < maxSites move and project.
-__device__ __forceinline__ void propose(const Params &P, WarpSmem &ws, int g, int p, int lane, float sd,
-                                        float *uMetro) {
-  const uint2 key = make_uint2(ws.st.seed, P.runKey);
+// Proposal into ws.prop.  Every lane draws one Philox block in lock-step:
+// lanes < maxSites turn theirs into three normal deviates for their site; the
+// move choice and the Metropolis deviate come from the block of lane 31
+// (a lane no site uses when maxSites <= 31), or from a second block.
+__device__ __forceinline__ void propose(const Params &P, WarpSmem &ws, const ProjFix *proj, int g, int p,
+                                        int lane, float sd, uint32_t seed, float *uMetro) {
+  const uint2 key = make_uint2(seed, P.runKey);
+  const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, (uint32_t)lane, 2u), key);
+  uint4 cc = make_uint4(__shfl_sync(0xffffffffu, c.x, 31), __shfl_sync(0xffffffffu, c.y, 31),
+                        __shfl_sync(0xffffffffu, c.z, 31), __shfl_sync(0xffffffffu, c.w, 31));
+  if (P.maxSites >= 32) cc = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xFFFFu, 1u), key);
+  const uint32_t free = (uint32_t)ws.meta[4];
+  const int nFree = __popc(free);
   int pick = -1;
-  float um = 0.f;
-  if (lane == 0) {
-    const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xFFFFu, 1u), key);
-    const uint32_t free = (uint32_t)ws.meta[4];
-    const int nFree = __popc(free);
-    if (u01(c.x) < 0.75f && nFree > 0) {
-      int k = min(nFree - 1, (int)(u01(c.y) * (float)nFree));
-      uint32_t m = free;
-      for (int i = 0; i < k; ++i) m &= m - 1;
-      pick = __ffs(m) - 1;
-    }
-    um = u01(c.z);
+  if (u01(cc.x) < 0.75f && nFree > 0) {
+    const int kth = min(nFree - 1, (int)(u01(cc.y) * (float)nFree));
+    pick = __fns(free, 0, kth + 1);
   }
-  pick = __shfl_sync(0xffffffffu, pick, 0);
-  *uMetro = __shfl_sync(0xffffffffu, um, 0);
-  const int A = ws.meta[0];
+  *uMetro = u01(cc.z);
   if (lane < P.maxSites) {
     const int s = lane;
     const bool moving = (pick < 0) || (pick == s);
     if (moving) {
-      const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, (uint32_t)s, 2u), key);
       const float2 n01 = gauss2(c.x, c.y);
       const float2 n23 = gauss2(c.z, c.w);
       const float gz[3] = {n01.x, n01.y, n23.x};
+      const float scale = sd * 4294967296.0f;
       int64_t pos[3];
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-        pos[i] = (int64_t)ws.cur[s * 3 + i] + (int64_t)llrint((double)gz[i] * (double)sd * kTwoPow32);
-      const ProjFix &pr = P.proj[(size_t)A * P.maxSites + s];
+      for (int i = 0; i < 3; ++i) pos[i] = (int64_t)ws.cur[s * 3 + i] + __float2ll_rn(gz[i] * scale);
+      const ProjFix &pr = proj[s];
+      if (pr.pad[0]) {  // diagonal 0/1 projector: keep or drop each coordinate
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        int64_t acc = (int64_t)pr.num[3 * i] * pos[0] + (int64_t)pr.num[3 * i + 1] * pos[1] +
-                      (int64_t)pr.num[3 * i + 2] * pos[2];
-        if (pr.den != 1) acc = floor_div(acc, pr.den);
-        ws.prop[s * 3 + i] = (uint32_t)(acc + (int64_t)pr.t[i]);
+        for (int i = 0; i < 3; ++i)
+          ws.prop[s * 3 + i] = (pr.num[4 * i] ? (uint32_t)pos[i] : 0u) + pr.t[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          int64_t acc = (int64_t)pr.num[3 * i] * pos[0] + (int64_t)pr.num[3 * i + 1] * pos[1] +
+                        (int64_t)pr.num[3 * i + 2] * pos[2];
+          if (pr.den != 1) acc = floor_div(acc, pr.den);
+          ws.prop[s * 3 + i] = (uint32_t)(acc + (int64_t)pr.t[i]);
+        }
       }
     } else {
 #pragma unroll
@@ -535,18 +590,18 @@ __device__ __forceinline__ void propose(const Params &P, WarpSmem &ws, int g, in
 // The kernel.
 // ---------------------------------------------------------------------------
 template <int COSMODE, int SLOTS>
-__global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int nGen, int mcmc, int swapEvery,
+__global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, int nGen, int mcmc, int swapEvery,
                                                  int reevalFirst) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t stageBar;
   __shared__ float shellLen[27];
-  __shared__ float exE[kMaxRungs];
+  __shared__ float exFit[kMaxRungs], exCC[kMaxRungs], exPen[kMaxRungs], exTemp[kMaxRungs], exE[kMaxRungs];
   __shared__ int exSwap[kMaxRungs];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nWarps = blockDim.x >> 5;
 
-  // Stage the static tables (reflections, f table, groups, rMin) once per CTA.
+  // Stage the static tables once per CTA with the bulk-copy engine.
   unsigned char *stat = smem;
   const int blobPad = (P.blobBytes + 127) & ~127;
   if (threadIdx.x == 0) {
@@ -556,7 +611,6 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
   __syncthreads();
   if (threadIdx.x == 0) {
     mbar_arrive_expect_tx(&stageBar, (uint32_t)P.blobBytes);
-    // chunks of at most 64 KB, 16-byte multiples (blobBytes is padded on the host)
     for (int off = 0; off < P.blobBytes; off += 65536) {
       const int n = min(65536, P.blobBytes - off);
       bulk_g2s(stat + off, P.blob + off, (uint32_t)n, &stageBar);
@@ -569,7 +623,6 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
   }
   if (!mbar_wait_bounded(&stageBar, 0, kStageWaitLimit)) {
     raise_flag(P.errFlag, DEV_STAGE_TIMEOUT);
-    // give the copy in flight a second bounded chance before leaving
     mbar_wait_bounded(&stageBar, 0, kStageWaitLimit);
     return;
   }
@@ -578,11 +631,16 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
   const float *ftab = reinterpret_cast<const float *>(stat + P.offF);
   const float4 *groups = reinterpret_cast<const float4 *>(stat + P.offGroup);
   const float *rmin = reinterpret_cast<const float *>(stat + P.offRmin);
+  const double *sooPrefix = reinterpret_cast<const double *>(stat + P.offSoo);
+  const OpFix *ops = reinterpret_cast<const OpFix *>(stat + P.offOps);
+  const uint32_t *pairs = P.nPairs > 0 ? reinterpret_cast<const uint32_t *>(stat + P.offPairs) : nullptr;
 
   unsigned char *wbase = smem + blobPad + (size_t)warp * P.warpSmemBytes;
   WarpSmem &ws = *reinterpret_cast<WarpSmem *>(wbase);
   uint4 *atoms = reinterpret_cast<uint4 *>(wbase + P.atomsOff);
   float *ic = reinterpret_cast<float *>(wbase + P.icOff);
+  uint32_t *gen = reinterpret_cast<uint32_t *>(wbase + P.genOff);
+  ProjFix *proj = reinterpret_cast<ProjFix *>(wbase + P.projOff);
 
   const int rungs = P.rungs;
   const int nLadders = P.nLadders;
@@ -600,6 +658,9 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
       }
     }
     const bool active = p >= 0;
+    // chain state in registers (meaningful on lane 0)
+    float fit = 0.f, cc0 = 0.f, pen0 = 0.f, step = 0.f, temp = 0.f, bestFit = -1e30f, bestCC = 0.f, bestPen = 0.f;
+    uint32_t seed = 0, accepted = 0;
     if (active) {
       const int A = (int)P.assign[p];
       if (lane == 0) {
@@ -608,10 +669,16 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
         ws.meta[2] = P.nF[A];
         ws.meta[4] = (int)P.freeMask[A];
         ws.meta[5] = p;
-        ws.st = P.st[p];
+        const PState st = P.st[p];
+        fit = st.fit; cc0 = st.cc; pen0 = st.pen; step = st.step; temp = st.temp;
+        seed = st.seed; accepted = st.accepted;
+        bestFit = st.bestFit; bestCC = st.bestCC; bestPen = st.bestPen;
       }
+      seed = __shfl_sync(0xffffffffu, seed, 0);
       if (lane < kMaxSites) ws.runs[lane] = P.runs[(size_t)A * kMaxSites + lane];
       for (int j = lane; j < (int)curStride; j += 32) ws.cur[j] = P.pos[(size_t)p * curStride + j];
+      for (int j = lane; j < P.nTot; j += 32) gen[j] = __ldg(P.gen + (size_t)A * P.nTot + j);
+      for (int j = lane; j < P.maxSites; j += 32) proj[j] = P.proj[(size_t)A * P.maxSites + j];
     }
     __syncwarp();
     int prevNga = -1;
@@ -621,64 +688,59 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
       const float penScale = P.schedGroups ? P.schedPen[g] : P.penArg;
       const int ngaC = max(0, min(nga, P.nGroups));
       if (active) {
+        float *tIc = P.traceIc ? P.traceIc + (size_t)p * P.nRefl : nullptr;
         const bool reeval = mcmc && ((gi == 0 && reevalFirst) || (gi > 0 && nga != prevNga));
         if (reeval || !mcmc) {
           // evaluate the current state (dispatchCoords(null, false))
-          expand(P, ws.meta[0], ws.cur, atoms, lane);
+          expand(P, gen, ops, ws.cur, atoms, lane);
           __syncwarp();
           double sums[3];
-          fitness<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, ngaC, lane, sums,
-                           P.traceIc ? P.traceIc + (size_t)p * P.nRefl : nullptr);
+          fitness<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
           const float cc = cc_of(sums);
-          const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, lane) * penScale;
-          if (lane == 0) {
-            ws.st.fit = cc - pen;
-            ws.st.cc = cc;
-            ws.st.pen = pen / fmaxf(penScale, 1e-9f);
-          }
-          __syncwarp();
+          const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, pairs, lane) * penScale;
+          fit = cc - pen;
+          cc0 = cc;
+          pen0 = pen / fmaxf(penScale, 1e-9f);
         }
         if (mcmc) {
           float uMetro;
-          const float sd = __shfl_sync(0xffffffffu, lane == 0 ? ws.st.step : 0.f, 0);
-          propose(P, ws, g, p, lane, sd, &uMetro);
-          expand(P, ws.meta[0], ws.prop, atoms, lane);
+          const float sd = __shfl_sync(0xffffffffu, step, 0);
+          propose(P, ws, proj, g, p, lane, sd, seed, &uMetro);
+          expand(P, gen, ops, ws.prop, atoms, lane);
           __syncwarp();
           double sums[3];
-          fitness<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, ngaC, lane, sums,
-                           P.traceIc ? P.traceIc + (size_t)p * P.nRefl : nullptr);
+          fitness<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
           const float cc = cc_of(sums);
-          const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, lane) * penScale;
+          const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, pairs, lane) * penScale;
           int acc = 0, best = 0;
           if (lane == 0) {
-            PState &st = ws.st;
             const float fNew = cc - pen;
-            float fOld = st.fit;
-            if (fOld > -1.0e29f) fOld = st.cc - st.pen * penScale;
-            const float stepBefore = st.step;
+            float fOld = fit;
+            if (fOld > -1.0e29f) fOld = cc0 - pen0 * penScale;
+            const float stepBefore = step;
             if (fNew >= fOld)
               acc = 1;
-            else if (uMetro < expf((fNew - fOld) / fmaxf(st.temp, 1e-9f)))
+            else if (uMetro < expf((fNew - fOld) / fmaxf(temp, 1e-9f)))
               acc = 1;
             if (acc) {
-              st.fit = fNew;
-              st.cc = cc;
-              st.pen = pen / fmaxf(penScale, 1e-9f);
-              st.accepted += 1u;
-              const bool hasBest = st.bestFit > -1.0e29f;
-              const float bestR = hasBest ? st.bestCC - st.bestPen * penScale : -1.0e30f;
+              fit = fNew;
+              cc0 = cc;
+              pen0 = pen / fmaxf(penScale, 1e-9f);
+              accepted += 1u;
+              const bool hasBest = bestFit > -1.0e29f;
+              const float bestR = hasBest ? bestCC - bestPen * penScale : -1.0e30f;
               if (fNew > bestR) {
-                st.bestFit = fNew;
-                st.bestCC = cc;
-                st.bestPen = pen / fmaxf(penScale, 1e-9f);
+                bestFit = fNew;
+                bestCC = cc;
+                bestPen = pen / fmaxf(penScale, 1e-9f);
                 best = 1;
               }
             }
-            st.step = fminf(fmaxf(st.step * (acc ? P.stepUp : P.stepDown), P.stepMin), P.stepMax);
+            step = fminf(fmaxf(step * (acc ? P.stepUp : P.stepDown), P.stepMin), P.stepMax);
             if (P.traceRec) {
               float *rec = P.traceRec + (size_t)p * 8;
               rec[0] = fNew; rec[1] = cc; rec[2] = pen; rec[3] = uMetro;
-              rec[4] = (float)acc; rec[5] = fOld; rec[6] = st.temp; rec[7] = stepBefore;
+              rec[4] = (float)acc; rec[5] = fOld; rec[6] = temp; rec[7] = stepBefore;
             }
           }
           acc = __shfl_sync(0xffffffffu, acc, 0);
@@ -690,14 +752,17 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
           if (best)
             for (int j = lane; j < (int)curStride; j += 32) bestBase[(size_t)p * curStride + j] = ws.prop[j];
           __syncwarp();
+        } else if (lane == 0 && P.traceRec) {
+          float *rec = P.traceRec + (size_t)p * 8;
+          rec[0] = fit; rec[1] = cc0; rec[2] = pen0 * penScale;
         }
       }
       prevNga = nga;
       // replica exchange inside the ladder (js/swarm_wyckoff.js:1825-1851)
       if (swapEvery > 0 && mcmc && P.ladders && ((g + 1) % swapEvery) == 0) {
         if (active && lane == 0) {
-          const PState &st = ws.st;
-          exE[warp] = isfinite(st.cc) ? st.cc - st.pen * penScale : st.fit;
+          exFit[warp] = fit; exCC[warp] = cc0; exPen[warp] = pen0; exTemp[warp] = temp;
+          exE[warp] = isfinite(cc0) ? cc0 - pen0 * penScale : fit;
         }
         if (threadIdx.x < kMaxRungs) exSwap[threadIdx.x] = -1;
         __syncthreads();
@@ -710,9 +775,7 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
             const float fa = exE[r], fb = exE[r + 1];
             if (!isfinite(fa) || !isfinite(fb)) continue;
             ++tried;
-            WarpSmem &wa = *reinterpret_cast<WarpSmem *>(smem + blobPad + (size_t)r * P.warpSmemBytes);
-            WarpSmem &wb = *reinterpret_cast<WarpSmem *>(smem + blobPad + (size_t)(r + 1) * P.warpSmemBytes);
-            const float d = (1.0f / wa.st.temp - 1.0f / wb.st.temp) * (fb - fa);
+            const float d = (1.0f / exTemp[r] - 1.0f / exTemp[r + 1]) * (fb - fa);
             if (d < 0.f) {
               const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)L, (uint32_t)r, 7u),
                                             make_uint2(P.runKey, 0x45584348u));
@@ -720,6 +783,9 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
             }
             ++taken;
             exSwap[r] = r + 1;
+            float t = exFit[r]; exFit[r] = exFit[r + 1]; exFit[r + 1] = t;
+            t = exCC[r]; exCC[r] = exCC[r + 1]; exCC[r + 1] = t;
+            t = exPen[r]; exPen[r] = exPen[r + 1]; exPen[r + 1] = t;
           }
           if (P.swapStats && tried) {
             atomicAdd(P.swapStats, tried);
@@ -737,18 +803,20 @@ __global__ void __launch_bounds__(256) wy_kernel(const Params P, int gen0, int n
             wa.cur[j] = wb.cur[j];
             wb.cur[j] = t;
           }
-          if (lane == 0) {
-            float t = wa.st.fit; wa.st.fit = wb.st.fit; wb.st.fit = t;
-            t = wa.st.cc; wa.st.cc = wb.st.cc; wb.st.cc = t;
-            t = wa.st.pen; wa.st.pen = wb.st.pen; wb.st.pen = t;
-          }
         }
         __syncthreads();
+        if (active && lane == 0) { fit = exFit[warp]; cc0 = exCC[warp]; pen0 = exPen[warp]; }
       }
     }
     if (active) {
       for (int j = lane; j < (int)curStride; j += 32) P.pos[(size_t)p * curStride + j] = ws.cur[j];
-      if (lane == 0) P.st[p] = ws.st;
+      if (lane == 0) {
+        PState st;
+        st.fit = fit; st.cc = cc0; st.pen = pen0; st.step = step; st.temp = temp;
+        st.seed = seed; st.accepted = accepted; st.pad = 0;
+        st.bestFit = bestFit; st.bestCC = bestCC; st.bestPen = bestPen; st.bestPad = 0.f;
+        P.st[p] = st;
+      }
     }
     __syncthreads();
   }
@@ -1039,17 +1107,28 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
       if (!rationalise(b, 9, f.num, &f.den))
         return set_error(P6_ERR_INVALID_ARG, "a Wyckoff projector is not a rational matrix with denominator <= 24");
       for (int k = 0; k < 3; ++k) f.t[k] = trans_fixed(b[9 + k]);
+      f.pad[0] = f.pad[1] = 0;
+      if (f.den == 1) {
+        bool diag = true;
+        for (int k = 0; k < 9 && diag; ++k)
+          diag = (k % 4 == 0) ? (f.num[k] == 0 || f.num[k] == 1) : f.num[k] == 0;
+        f.pad[0] = diag ? 1 : 0;
+      }
       double norm = 0;
       for (int k = 0; k < 9; ++k) norm += std::fabs(b[k]);
       if (norm > 1e-6) freeMask[A] |= 1u << si;
     }
-  // --- static blob: reflections | f table | groups | rMin ---------------------
+  // --- static blob: reflections | f table | groups | rMin | soo prefix | ops | pairs ---
   auto pad16 = [](size_t n) { return (n + 15) & ~(size_t)15; };
+  const int nPairs = nTot <= 96 ? nTot * (nTot - 1) / 2 : 0;
   const size_t offRefl = 0, szRefl = pad16((size_t)pr->n_refl * sizeof(ReflRec));
   const size_t offF = offRefl + szRefl, szF = pad16((size_t)pr->n_refl * nE * sizeof(float));
   const size_t offG = offF + szF, szG = pad16((size_t)pr->n_groups * sizeof(float4));
   const size_t offR = offG + szG, szR = pad16((size_t)nE * nE * sizeof(float));
-  const size_t blobBytes = offR + szR;
+  const size_t offS = offR + szR, szS = pad16((size_t)(pr->n_groups + 1) * sizeof(double));
+  const size_t offO = offS + szS, szO = pad16((size_t)pr->n_ops * sizeof(OpFix));
+  const size_t offP = offO + szO, szP = pad16((size_t)nPairs * sizeof(uint32_t));
+  const size_t blobBytes = offP + szP;
   std::vector<unsigned char> blob(blobBytes, 0);
   for (int r = 0; r < pr->n_refl; ++r) {
     const uint32_t pk = pr->refl_pack[2 * r];
@@ -1063,6 +1142,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
     std::memcpy(&blob[offRefl + r * sizeof(ReflRec)], &rec, sizeof(rec));
   }
   std::memcpy(&blob[offF], pr->f_tab, (size_t)pr->n_refl * nE * sizeof(float));
+  std::vector<double> soo(pr->n_groups + 1, 0.0);
   for (int gI = 0; gI < pr->n_groups; ++gI) {
     const float *gm = pr->group_meta + (size_t)gI * pr->group_stride;
     float4 v = make_float4(gm[0], gm[1], gm[2], pr->group_stride >= 4 ? gm[3] : 1.0f);
@@ -1074,10 +1154,22 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
         return set_error(P6_ERR_INVALID_ARG, "groups must be contiguous and in order");
     }
     std::memcpy(&blob[offG + gI * sizeof(float4)], &v, sizeof(v));
+    // sum of w Iobs^2 over the first gI+1 groups: constant for a given number of active groups
+    soo[gI + 1] = soo[gI] + ((v.w > 0.f) ? (double)v.w * (double)v.z * (double)v.z : 0.0);
   }
+  std::memcpy(&blob[offS], soo.data(), soo.size() * sizeof(double));
   for (int i = 0; i < nE * nE; ++i) {
     const float v = pr->restraint_tables[pr->r_min_off + i];
     std::memcpy(&blob[offR + i * sizeof(float)], &v, sizeof(float));
+  }
+  std::memcpy(&blob[offO], ops.data(), ops.size() * sizeof(OpFix));
+  {
+    int q = 0;
+    for (int i = 0; i < nTot && nPairs; ++i)
+      for (int j = i + 1; j < nTot; ++j) {
+        const uint32_t v = (uint32_t)i | ((uint32_t)j << 16);
+        std::memcpy(&blob[offP + (size_t)(q++) * sizeof(uint32_t)], &v, sizeof(v));
+      }
   }
   std::vector<RuleDev> rules(std::max(pr->n_rules, 1));
   for (int k = 0; k < pr->n_rules; ++k) {
@@ -1086,7 +1178,9 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   }
   // --- shared memory plan ----------------------------------------------------
   const int rungs = 8;
-  const size_t atomsOff = (sizeof(WarpSmem) + 15) & ~(size_t)15;
+  const size_t genOff = (sizeof(WarpSmem) + 15) & ~(size_t)15;
+  const size_t projOff = (genOff + (size_t)nTot * sizeof(uint32_t) + 15) & ~(size_t)15;
+  const size_t atomsOff = (projOff + (size_t)ms * sizeof(ProjFix) + 15) & ~(size_t)15;
   const size_t icOff = atomsOff + (size_t)nTot * sizeof(uint4);
   const size_t warpBytes = (icOff + (size_t)pr->n_refl * sizeof(float) + 127) & ~(size_t)127;
   const size_t smem = ((blobBytes + 127) & ~(size_t)127) + warpBytes * rungs;
@@ -1161,6 +1255,10 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.offF = (int)offF;
   P.offGroup = (int)offG;
   P.offRmin = (int)offR;
+  P.offSoo = (int)offS;
+  P.offOps = (int)offO;
+  P.offPairs = (int)offP;
+  P.nPairs = nPairs;
   P.rules = s->dRules;
   P.nRules = pr->n_rules;
   P.numParticles = pr->num_particles;
@@ -1206,6 +1304,8 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.swapStats = s->dSwap;
   P.errFlag = s->dErr;
   P.warpSmemBytes = (int)warpBytes;
+  P.genOff = (int)genOff;
+  P.projOff = (int)projOff;
   P.atomsOff = (int)atomsOff;
   P.icOff = (int)icOff;
   s->nga = pr->n_groups;
