@@ -115,6 +115,10 @@ typedef struct {
    * 1 = FMA-pipe polynomial (slower, closer to FP64) */
   int cos_mode;
   uint32_t run_key; /* key of the counter-based generator for this session */
+  /* per-replica site sums of |F| kept in shared memory so a proposal
+   * recomputes only the site it moved (bit-identical results): 1 on; 0 or -1
+   * (auto) evaluate every image, which measured faster on the PbSO4 search */
+  int incremental;
 } p6_wy_problem;
 
 typedef struct p6_wy_session p6_wy_session;
@@ -181,6 +185,9 @@ p6_status p6_wy_debug_expand(p6_wy_session *s, int particle, uint32_t *atoms);
 /* Milliseconds of the last p6_wy_run / p6_wy_dispatch kernel (CUDA events on
  * the session stream). */
 p6_status p6_wy_last_kernel_ms(p6_wy_session *s, float *ms);
+/* Session layout: whether site sums are incremental, shared memory per CTA,
+ * and the resident grid (any pointer may be NULL). */
+p6_status p6_wy_query(p6_wy_session *s, int *incremental, int *smem_bytes, int *max_grid);
 /* Kernel launches made by this session so far. */
 p6_status p6_wy_launch_count(p6_wy_session *s, long long *count);
 

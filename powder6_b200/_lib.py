@@ -47,7 +47,7 @@ class P6WyProblem(C.Structure):
                 ('pen_clash', C.c_float), ('pen_bond', C.c_float), ('pen_coord', C.c_float),
                 ('pen_geom', C.c_float), ('poly_prob', C.c_float),
                 ('step_up', C.c_float), ('step_down', C.c_float), ('step_min', C.c_float), ('step_max', C.c_float),
-                ('cos_mode', C.c_int), ('run_key', C.c_uint32)]
+                ('cos_mode', C.c_int), ('run_key', C.c_uint32), ('incremental', C.c_int)]
 
 
 _P = C.c_void_p
@@ -77,6 +77,7 @@ _SIGS = {
     'p6_wy_debug_expand': (C.c_int, [_P, C.c_int, _P]),
     'p6_wy_last_kernel_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_wy_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    'p6_wy_query': (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
 }
 
 _lib = None

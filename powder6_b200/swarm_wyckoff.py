@@ -65,7 +65,8 @@ class WyckoffSession:
     """One device session: the buffers and kernel of one search (swarm_wyckoff.js:1293-1720)."""
 
     def __init__(self, problem: WyckoffProblem, num_particles: int, run_key: int = 1, cos_mode: int = 0,
-                 device: int = 0, settings: Optional[dict] = None, max_coord_slots: Optional[int] = None):
+                 device: int = 0, settings: Optional[dict] = None, max_coord_slots: Optional[int] = None,
+                 incremental: int = -1):
         self.lib = _lib.load()
         self.problem = problem
         self.num_particles = int(num_particles)
@@ -119,6 +120,7 @@ class WyckoffSession:
         pr.step_min, pr.step_max = ad['STEP_MIN'], ad['STEP_MAX']
         pr.cos_mode = int(cos_mode)
         pr.run_key = int(run_key) & 0xFFFFFFFF
+        pr.incremental = int(incremental)
         self.adapt = ad
         h = C.c_void_p()
         check(self.lib.p6_wy_create(C.byref(pr), int(device), C.byref(h)))
@@ -237,6 +239,11 @@ class WyckoffSession:
         v = C.c_float()
         check(self.lib.p6_wy_last_kernel_ms(self.h, C.byref(v)))
         return v.value
+
+    def query(self) -> dict:
+        inc, smem, grid = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.p6_wy_query(self.h, C.byref(inc), C.byref(smem), C.byref(grid)))
+        return {'incremental': bool(inc.value), 'smem_bytes': smem.value, 'max_grid': grid.value}
 
     def launch_count(self) -> int:
         v = C.c_longlong()

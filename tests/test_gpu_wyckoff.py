@@ -302,3 +302,36 @@ def test_argument_errors_are_reported():
         assert e.value.status == 'INVALID_ARG'
         with pytest.raises(_lib.P6Error):
             s.run(0, 10, 10)                                  # no ladders yet
+
+
+def _fused(P, n, gens, incremental, cos_mode=0):
+    rnd = mulberry32(314)
+    assign = np.zeros(n, dtype=np.uint32)
+    with WyckoffSession(P, n, run_key=2718, cos_mode=cos_mode, incremental=incremental) as s:
+        assert s.query()['incremental'] == bool(incremental)
+        s.set_assign(assign)
+        lad, temps = build_ladders(assign)
+        s.set_ladders(lad, 8)
+        g, pen = schedule(gens, P.refl.n_groups)
+        s.set_schedule(g, pen)
+        pos = project_all(P, np.array([rnd() for _ in range(n * P.max_sites * 3)], dtype=np.float32), assign)
+        s.sync_state(pos, initial_state(n, temps, rnd))
+        half = gens // 2
+        s.run(0, half, 10, True)
+        s.run(half, gens - half, 10, bool(g[half] != g[half - 1]))
+        s.synchronize(120)
+        cur, best = s.read_positions_fixed()
+        _, _, st = s.read_state()
+    return cur, best, st
+
+
+@pytest.mark.parametrize('cos_mode', [0, 1])
+def test_incremental_site_sums_are_bit_identical_to_full_evaluation(prob, cos_mode):
+    """The cached per-site sums are re-summed in site order, so a search with
+    them follows exactly the trajectory of full re-evaluation, through the
+    resolution ramp and the ladder exchanges."""
+    P = prob
+    a = _fused(P, 512, 400, 1, cos_mode)
+    b = _fused(P, 512, 400, 0, cos_mode)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32))
