@@ -191,6 +191,70 @@ p6_status p6_wy_query(p6_wy_session *s, int *incremental, int *smem_bytes, int *
 /* Kernel launches made by this session so far. */
 p6_status p6_wy_launch_count(p6_wy_session *s, long long *count);
 
+
+/* ======================================================================== */
+/* Parallel tempering (Rietveld)                                             */
+/* ======================================================================== */
+
+/* One phase and one dataset, X-rays, TCH profile: the arrays RVPTGPU.compile
+ * packs (js/pt_gpu.js:20-227) in plain form.  The full parameter vector is
+ * [scale, a, b, c, alpha, beta, gamma, U, V, W, X, Y, zero, Biso, bkg0, ...]
+ * (GSAS units for U..Y); `index` maps the nv refined parameters into it, and
+ * lo/hi/scales are ctx.info[j].lo/hi and ctx.setup.scales
+ * (js/rietveld_core.js:2147-2170). */
+typedef struct {
+  int n_refl;              /* reflections over the cell envelope (generateReflections, :247-276) */
+  const int32_t *hkl;      /* 3 per reflection */
+  const int32_t *mult;
+  int n_reps;              /* coset representatives modulo centring (cosets, :164-180) */
+  const int32_t *rep_rot;  /* 9 per representative, row-major */
+  const double *rep_trans; /* 3 per representative */
+  int n_atoms;
+  const double *atom_pos;  /* 3 per atom, fractional */
+  const double *atom_wmult;/* site multiplicity / n_reps */
+  const double *atom_occ;
+  const double *ff_a, *ff_b, *ff_c; /* 5, 5, 1 per atom: f0(s) = c + sum a exp(-b (s/2)^2) */
+  int n_points;
+  const double *tth;       /* ascending */
+  const double *y, *w;
+  double lambda1, lambda2, ratio, pol_k, min_fwhm, dmin;
+  int n_bkg;               /* Chebyshev terms */
+  int n_full;
+  const double *full_values;
+  int nv;
+  const int32_t *index;
+  const double *lo, *hi, *scales;
+  int cubic;               /* b = c = a */
+  int chains;
+  double max_temp;
+  uint32_t seed;
+} p6_pt_problem;
+
+typedef struct p6_pt_session p6_pt_session;
+
+/* RVPTGPU.create (js/pt_gpu.js:371-406): device buffers for the plan. */
+p6_status p6_pt_create(const p6_pt_problem *problem, int device, p6_pt_session **out);
+p6_status p6_pt_destroy(p6_pt_session *s);
+/* create().costs (js/pt_gpu.js:402): chi^2 of n_vectors refined-parameter
+ * vectors (nv each); ycalc (may be NULL) receives n_vectors * n_points floats. */
+p6_status p6_pt_costs(p6_pt_session *s, const double *vectors, int n_vectors, double *costs, float *ycalc);
+/* create().initial (js/pt_gpu.js:400): chain c starts from vectors[c % n]. */
+p6_status p6_pt_initial(p6_pt_session *s, const double *vectors, int n_vectors);
+/* create().batch (js/pt_gpu.js:403): `count` sweeps of nv proposals per
+ * chain with even/odd exchanges, or one evaluation of the start (bootstrap).
+ * Asynchronous; read the state to wait. */
+p6_status p6_pt_batch(p6_pt_session *s, int count, int bootstrap);
+/* State after the last batch: `state` in the reference layout
+ * (chains x (3 nv + 12) floats: x, proposal, best, cost, bestCost, sweep,
+ * accepted, proposals, swaps, swapAttempts, valid, log u, unsolved,
+ * proposalCost, feasible), and exactly: x, best (chains x nv doubles),
+ * costs (cost, bestCost per chain), counters (accepted, proposals, swaps,
+ * swapAttempts per chain).  Any pointer may be NULL. */
+p6_status p6_pt_read_state(p6_pt_session *s, float *state, double *x, double *best, double *costs, double *counters);
+p6_status p6_pt_synchronize(p6_pt_session *s, double timeout_seconds);
+p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms);
+p6_status p6_pt_launch_count(p6_pt_session *s, long long *count);
+
 /* Philox4x32-10 of one (counter, key) on the device: known-answer check. */
 p6_status p6_philox_device(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

@@ -202,3 +202,103 @@ class WyckoffCpuRunner:
                       pen_scale)
         return self.lib.p6o_wy_generation(C.byref(self.pr), C.byref(g), self.n, _p(self.pos), _p(self.assign),
                                           _p(self.st), _p(self.seeds), self.n_threads)
+
+
+# ---------------------------------------------------------------------------
+# Parallel-tempering Rietveld cost (p6_oracle_pt.c)
+# ---------------------------------------------------------------------------
+class PtProblem(C.Structure):
+    _fields_ = [('nOps', C.c_int), ('rot', C.c_void_p), ('trans', C.c_void_p),
+                ('nReps', C.c_int), ('repRot', C.c_void_p), ('repTrans', C.c_void_p),
+                ('nAtoms', C.c_int), ('pos', C.c_void_p), ('wMult', C.c_void_p), ('occ', C.c_void_p),
+                ('ffA', C.c_void_p), ('ffB', C.c_void_p), ('ffC', C.c_void_p),
+                ('n', C.c_int), ('tth', C.c_void_p), ('y', C.c_void_p), ('w', C.c_void_p),
+                ('lambda1', C.c_double), ('lambda2', C.c_double), ('ratio', C.c_double), ('polK', C.c_double),
+                ('minFwhm', C.c_double), ('nBkg', C.c_int), ('dmin', C.c_double)]
+
+
+class PtSetup(C.Structure):
+    _fields_ = [('nv', C.c_int), ('index', C.c_void_p), ('lo', C.c_void_p), ('hi', C.c_void_p),
+                ('scales', C.c_void_p), ('cubic', C.c_int), ('chains', C.c_int), ('sweeps', C.c_int),
+                ('maxTemp', C.c_double), ('seed', C.c_uint32)]
+
+
+class PtModel:
+    """FP64 reference cost of a powder6_b200.pt_gpu.PTProblem (the same inputs the kernel gets)."""
+
+    def __init__(self, prob, dmin=None):
+        from powder6_b200.symmetry import cosets, space_group
+        lib = load()
+        lib.p6o_pt_cost.restype = C.c_double
+        lib.p6o_pt_cost.argtypes = [C.POINTER(PtProblem), C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.p6o_pt_temper.restype = C.c_double
+        lib.p6o_pt_temper.argtypes = [C.POINTER(PtProblem), C.POINTER(PtSetup), C.c_void_p, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int]
+        self.lib = lib
+        self.prob = prob
+        g = space_group(prob.group_number)
+        reps, _ = cosets(g.ops)
+        self.keep = []
+
+        def a(x, dt):
+            x = np.ascontiguousarray(x, dtype=dt)
+            self.keep.append(x)
+            return x.ctypes.data
+
+        p = PtProblem()
+        p.nOps = len(g.ops)
+        p.rot = a([o.r for o in g.ops], np.int32)
+        p.trans = a([o.t_frac for o in g.ops], np.float64)
+        p.nReps = len(reps)
+        p.repRot = a([o.r for o in reps], np.int32)
+        p.repTrans = a([o.t_frac for o in reps], np.float64)
+        p.nAtoms = len(prob.atoms)
+        p.pos = a([at['pos'] for at in prob.atoms], np.float64)
+        p.wMult = a([at['mult'] / len(reps) for at in prob.atoms], np.float64)
+        p.occ = a([at.get('occ', 1.0) for at in prob.atoms], np.float64)
+        p.ffA = a([at['a'] for at in prob.atoms], np.float64)
+        p.ffB = a([at['b'] for at in prob.atoms], np.float64)
+        p.ffC = a([at['c'] for at in prob.atoms], np.float64)
+        p.n = len(prob.tth)
+        p.tth = a(prob.tth, np.float64)
+        p.y = a(prob.y, np.float64)
+        p.w = a(prob.w, np.float64)
+        p.lambda1, p.lambda2, p.ratio, p.polK = prob.lambda1, prob.lambda2, prob.ratio, prob.pol_k
+        p.minFwhm = prob.min_fwhm
+        p.nBkg = prob.n_bkg
+        p.dmin = 0.0 if dmin is None else float(dmin)
+        self.p = p
+
+    def cost_full(self, v, with_pattern=False):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        y = np.zeros(len(self.prob.tth)) if with_pattern else None
+        nr = C.c_int(0)
+        c = self.lib.p6o_pt_cost(C.byref(self.p), v.ctypes.data, None if y is None else y.ctypes.data, C.byref(nr))
+        return (c, y, nr.value) if with_pattern else c
+
+    def cost(self, x):
+        return self.cost_full(self.prob.apply(x))
+
+    def pattern(self, prob, v):
+        return self.cost_full(v, with_pattern=True)[1]
+
+    def temper(self, x0, scales, chains=16, sweeps=50, max_temp=100.0, seed=12345, max_sweeps=0):
+        prob = self.prob
+        s = PtSetup()
+        s.nv = len(x0)
+        idx = np.ascontiguousarray(prob.index, dtype=np.int32)
+        lo = np.ascontiguousarray(prob.lo, dtype=np.float64)
+        hi = np.ascontiguousarray(prob.hi, dtype=np.float64)
+        sc = np.ascontiguousarray(scales, dtype=np.float64)
+        self.keep += [idx, lo, hi, sc]
+        s.index, s.lo, s.hi, s.scales = idx.ctypes.data, lo.ctypes.data, hi.ctypes.data, sc.ctypes.data
+        s.cubic = 1 if prob.system == 'cubic' else 0
+        s.chains, s.sweeps, s.maxTemp, s.seed = chains, sweeps, max_temp, seed
+        base = np.ascontiguousarray(prob.values, dtype=np.float64)
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        best = np.zeros(len(x0))
+        stats = np.zeros(6)
+        self.lib.p6o_pt_temper(C.byref(self.p), C.byref(s), base.ctypes.data, len(base), x0.ctypes.data,
+                               best.ctypes.data, stats.ctypes.data, int(max_sweeps))
+        return best, {'proposals': stats[0], 'accepted': stats[1], 'swapAttempts': stats[2], 'swaps': stats[3],
+                      'bestChi2': stats[4], 'initialChi2': stats[5]}

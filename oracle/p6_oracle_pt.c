@@ -1,0 +1,472 @@
+/*
+ * ORACLE -- test infrastructure, not product code.
+ *
+ * FP64 CPU restatement of the reference's Rietveld cost for parallel
+ * tempering, and of its CPU parallel tempering.
+ *
+ *   p6o_pt_cost      chi^2 = sum_{w>0} w (y - ycalc)^2 of one parameter vector:
+ *                    js/rietveld_core.js:1878-1889 (cost), 1152-1165
+ *                    (evalDataset), 855-917 (evalPhase, render), 920-931 and
+ *                    640-646 (Chebyshev background), 719-747 (geometry),
+ *                    749-822 (structure, no anomalous terms), 247-276
+ *                    (generateReflections via p6o_generate_reflections),
+ *                    238-245 (reflectionDmin); js/profile.js:108-131
+ *                    (calculatePeakShift), 149-219 (width floors), 426-550
+ *                    (TCH widths, calculateProfileWidths), 552-567
+ *                    (getPeakFWHM), 603-760 (prepareVoigt, evalVoigt),
+ *                    1013-1090 (buildPeakContributions: all K-alpha-1, then
+ *                    all K-alpha-2), 1131-1159 (intensityDerivativeColumn);
+ *                    js/constants.js:138-145 (softPositive), 155-201
+ *                    (pseudo-Voigt constants, pvMixCoeffs), 248-251 (GSAS
+ *                    units); js/crystal.js:480-497 (Lp).
+ *   p6o_pt_temper    js/rietveld_core.js:2171-2241 (temper): one xorshift32
+ *                    stream, nv single-coordinate proposals per replica per
+ *                    sweep, reflecting bounds, Metropolis on chi^2/2, even/odd
+ *                    adjacent exchanges.
+ *
+ * Scope of the restatement: one phase, one dataset, X-rays, TCH profile
+ * without Stephens terms or SL/HL asymmetry, no preferred orientation, no
+ * displacement or transparency, Chebyshev background -- the model of the
+ * parallel-tempering benchmark configuration.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PI_ 3.14159265358979323846
+#define DEG2RAD (PI_ / 180.0)
+#define R2D (180.0 / PI_)
+
+int p6o_generate_reflections(const double *cell, const int *rot, const double *trans, int nOps, double dmin,
+                             const int *box, int *oh, int *ok, int *ol, int *om, double *od0, int maxOut);
+
+/* Full parameter vector layout (the values apply() produces). */
+enum {
+    PT_SCALE = 0, PT_A, PT_B, PT_C, PT_AL, PT_BE, PT_GA, PT_U, PT_V, PT_W, PT_X, PT_Y, PT_ZERO, PT_BISO, PT_BKG0
+};
+
+typedef struct {
+    /* phase */
+    int nOps;
+    const int *rot;        /* nOps*9 */
+    const double *trans;   /* nOps*3 */
+    int nReps;
+    const int *repRot;     /* nReps*9 */
+    const double *repTrans;/* nReps*3 */
+    int nAtoms;
+    const double *pos;     /* nAtoms*3 fractional */
+    const double *wMult;   /* site multiplicity / nReps, per atom */
+    const double *occ;     /* per atom */
+    const double *ffA, *ffB, *ffC; /* 5, 5, 1 per atom */
+    /* dataset */
+    int n;
+    const double *tth, *y, *w;
+    double lambda1, lambda2, ratio, polK, minFwhm;
+    int nBkg;
+    double dmin;           /* > 0: use this; <= 0: reflectionDmin of the parameters */
+} p6o_pt_problem;
+
+static const double GCONV = 0.023548200450309493;   /* sqrt(8 ln 2) / 100 */
+static const double LCONV = 0.01;
+static const double CG = 2.772588722239781;         /* 4 ln 2 */
+static const double WIN_G = 8.0, WIN_L = 25.0, WIN_MAX = 10.0;
+
+static double pv_g0(void) { return 2.0 * sqrt(log(2.0) / PI_); }
+static double pv_l0(void) { return 2.0 / PI_; }
+
+static double soft_positive(double x, double f)
+{
+    if (!isfinite(x)) return f;
+    double h = hypot(x, 2 * f);
+    return x < 0 ? f * (f / (0.5 * h - 0.5 * x)) : 0.5 * x + 0.5 * h;
+}
+
+static double soft_floor(double x, double f)
+{
+    if (!isfinite(x) || !(x > 0)) return f;
+    if (!(f > 0)) return x;
+    double r = x / f;
+    if (r > 20) return x;
+    return f * pow(pow(r, 4) + 1, 0.25);
+}
+
+static double peak_fwhm(double gG0, double gL0)
+{
+    double gG = fmax(1e-9, gG0 != 0 ? gG0 : 1e-9), gL = fmax(1e-9, gL0 != 0 ? gL0 : 1e-9);
+    double s = pow(gG, 5) + 2.69269 * pow(gG, 4) * gL + 2.42843 * pow(gG, 3) * pow(gL, 2) +
+               4.47163 * pow(gG, 2) * pow(gL, 3) + 0.07842 * gG * pow(gL, 4) + pow(gL, 5);
+    if (s < 0 || !isfinite(s)) return fmax(fmax(gG, gL), 1e-6);
+    return fmax(1e-6, pow(s, 0.2));
+}
+
+typedef struct {
+    double x0, inv, cL, cG, pedestal, maxd, area;
+} voigt_t;
+
+static double eval_voigt(double x, const voigt_t *p, double maxd, double pedestal)
+{
+    double delta = x - p->x0;
+    if (delta > maxd || delta < -maxd) return 0.0;
+    double dg = (delta * p->inv) * (delta * p->inv);
+    double g = exp(-CG * dg);
+    double l = 1.0 / (1.0 + 4.0 * dg);
+    double v = p->cL * l + p->cG * g - pedestal;
+    return v > 0 ? v : 0.0;
+}
+
+/* prepareVoigt, TCH branch (profile.js:603-722), no asymmetry. */
+static void prepare_tch(double tthPeak, double x0, const double *v, double fwhmMin, voigt_t *p)
+{
+    double gG = fwhmMin, gL = fwhmMin;
+    double thetaRad = tthPeak * (PI_ / 180) / 2;
+    double safe = fmin(thetaRad, PI_ / 2.0 - 1e-6);
+    if (!(safe < 1e-6)) {
+        double tanT = tan(safe), cosT = cos(safe), cosTs = fmax(cosT, 1e-9);
+        double sig2 = v[PT_U] * tanT * tanT + v[PT_V] * tanT + v[PT_W];
+        double floorSq = pow(0.25 * fwhmMin / GCONV, 2);
+        gG = sqrt(soft_positive(sig2, floorSq)) * GCONV;
+        double gLc = v[PT_X] / cosTs + v[PT_Y] * tanT;
+        gL = soft_positive(gLc, 0.25 * fwhmMin / LCONV) * LCONV;
+    }
+    gG = soft_floor(gG, fwhmMin);
+    gL = soft_floor(gL, fwhmMin);
+    double HG = fmax(1e-9, gG), HL = fmax(1e-9, gL);
+    double fwhm = fmax(1e-9, peak_fwhm(HG, HL));
+    double eta = 0;
+    if (fwhm > 1e-9) {
+        double r = HL / fwhm;
+        eta = fmax(0, fmin(1, 1.36603 * r - 0.47719 * (r * r) + 0.11116 * pow(r, 3)));
+    }
+    /* pvMixCoeffs(eta, fwhm, fwhm) */
+    double e = fmax(0, fmin(1, eta));
+    double wL = e * pv_l0() / fmax(1e-12, fwhm), wG = (1 - e) * pv_g0() / fmax(1e-12, fwhm), s = wL + wG;
+    double cL = e, cG = 1 - e;
+    if (s > 0 && isfinite(s)) { cL = wL / s; cG = wG / s; }
+    p->x0 = x0;
+    p->inv = 1 / fwhm;
+    p->cL = cL;
+    p->cG = cG;
+    p->area = (cL * (1 / pv_l0()) + cG * (1 / pv_g0())) * fwhm;
+    double winFwhm = fmax(1e-6, fwhm);
+    double etaWin = fmax(0, fmin(1, eta));
+    double mult = WIN_G + (WIN_L - WIN_G) * etaWin;
+    double R = fmin(WIN_MAX, mult * fmax(0.01, winFwhm));
+    p->pedestal = fmax(eval_voigt(x0 + R, p, INFINITY, 0.0), eval_voigt(x0 - R, p, INFINITY, 0.0));
+    p->maxd = R;
+}
+
+static double lp_factor(double tth, double K)
+{
+    if (!isfinite(tth) || tth <= 0 || tth >= 180) return 1;
+    double th = 0.5 * tth * DEG2RAD, s = sin(th), c = cos(th);
+    if (s < 1e-6 || c < 1e-6) return 1;
+    double L = 1 / (s * s * c);
+    double k = (isfinite(K) && K >= 0) ? K : 1;
+    double c2 = cos(tth * DEG2RAD);
+    double P = (1 + k * c2 * c2) / (1 + k);
+    return L * P;
+}
+
+static int lower_bound(const double *a, int n, double t)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < t) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+static double inv_dsq_cell(const double *c6, double h, double k, double l, int *ok)
+{
+    double a = c6[0], b = c6[1], c = c6[2];
+    double al = c6[3] * DEG2RAD, be = c6[4] * DEG2RAD, ga = c6[5] * DEG2RAD;
+    double cA = cos(al), cB = cos(be), cG = cos(ga), sA = sin(al), sB = sin(be), sG = sin(ga);
+    double vf = 1 - cA * cA - cB * cB - cG * cG + 2 * cA * cB * cG;
+    *ok = 0;
+    if (!(a > 0 && b > 0 && c > 0) || vf <= 1e-9 || fabs(sA) < 1e-9 || fabs(sB) < 1e-9 || fabs(sG) < 1e-9) return NAN;
+    *ok = 1;
+    double V = a * b * c * sqrt(vf);
+    double as = b * c * sA / V, bs = a * c * sB / V, cs = a * b * sG / V;
+    double cAs = (cB * cG - cA) / (sB * sG), cBs = (cA * cG - cB) / (sA * sG), cGs = (cA * cB - cG) / (sA * sB);
+    return h * h * (as * as) + k * k * (bs * bs) + l * l * (cs * cs) + h * k * (2 * as * bs * cGs) +
+           k * l * (2 * bs * cs * cAs) + h * l * (2 * as * cs * cBs);
+}
+
+/*
+ * chi^2 of the full parameter vector v.  ycalc (may be NULL) receives the
+ * calculated pattern; nRefl (may be NULL) the reflection count used.
+ */
+double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int *nReflOut)
+{
+    const int n = P->n;
+    double c6[6] = {v[PT_A], v[PT_B], v[PT_C], v[PT_AL], v[PT_BE], v[PT_GA]};
+    int okc;
+    inv_dsq_cell(c6, 1, 0, 0, &okc);
+    if (!okc) return INFINITY;
+    double dmin = P->dmin;
+    if (!(dmin > 0)) {
+        double lambda = P->lambda1;
+        if (P->ratio > 1e-6 && P->lambda2 > 0) lambda = fmin(lambda, P->lambda2);
+        double margin = WIN_MAX + fabs(v[PT_ZERO]);
+        double upper = fmin(179.999999, P->tth[n - 1] + margin + .001);
+        dmin = lambda / (2 * sin(upper * DEG2RAD / 2));
+    }
+    int cap = 200000;
+    int *h = malloc(sizeof(int) * cap), *k = malloc(sizeof(int) * cap), *l = malloc(sizeof(int) * cap),
+        *m = malloc(sizeof(int) * cap);
+    double *d0 = malloc(sizeof(double) * cap);
+    int nr = p6o_generate_reflections(c6, P->rot, P->trans, P->nOps, dmin, NULL, h, k, l, m, d0, cap);
+    if (nr > cap) nr = cap;
+    if (nReflOut) *nReflOut = nr;
+    double *tthR = malloc(sizeof(double) * (nr + 1)), *F2 = malloc(sizeof(double) * (nr + 1));
+    voigt_t *p1 = malloc(sizeof(voigt_t) * (nr + 1)), *p2 = malloc(sizeof(voigt_t) * (nr + 1));
+    int *st1 = malloc(sizeof(int) * (nr + 1) * 4);
+    double *w2 = malloc(sizeof(double) * (nr + 1));
+    int *has1 = calloc(nr + 1, sizeof(int)), *has2 = calloc(nr + 1, sizeof(int));
+    const double lam = P->lambda1;
+    const int doublet = P->ratio > 1e-6 && P->lambda2 > 1e-6 && fabs(P->lambda1 - P->lambda2) > 1e-6;
+    /* geometry and structure */
+    for (int r = 0; r < nr; r++) {
+        int okq;
+        double q = inv_dsq_cell(c6, h[r], k[r], l[r], &okq), s = sqrt(q), sinT = lam * s / 2, tth = NAN;
+        if (q > 0 && sinT < 1) tth = 2 * asin(sinT) * R2D;
+        tthR[r] = tth;
+        double Ar = 0, Br = 0, s2 = s * s;
+        if (isfinite(tth)) {
+            for (int j = 0; j < P->nAtoms; j++) {
+                double dw = exp(-v[PT_BISO] * s2 / 4);
+                const double *a = P->ffA + 5 * j, *b = P->ffB + 5 * j;
+                double qq = (s / 2) * (s / 2), f0 = P->ffC[j];
+                for (int i = 0; i < 5; i++) f0 += a[i] * exp(-b[i] * qq);
+                double wj = P->occ[j] * f0 * dw * P->wMult[j], c = 0, sn = 0;
+                const double *pos = P->pos + 3 * j;
+                for (int qn = 0; qn < P->nReps; qn++) {
+                    const int *R = P->repRot + 9 * qn;
+                    const double *t = P->repTrans + 3 * qn;
+                    double H0 = h[r] * R[0] + k[r] * R[3] + l[r] * R[6], H1 = h[r] * R[1] + k[r] * R[4] + l[r] * R[7],
+                           H2 = h[r] * R[2] + k[r] * R[5] + l[r] * R[8];
+                    double ph = 2 * PI_ * (H0 * pos[0] + H1 * pos[1] + H2 * pos[2] + h[r] * t[0] + k[r] * t[1] + l[r] * t[2]);
+                    c += cos(ph);
+                    sn += sin(ph);
+                }
+                Ar += wj * c;
+                Br += wj * sn;
+            }
+        }
+        F2[r] = Ar * Ar + Br * Br;
+    }
+    /* contributions: all K-alpha-1, then all K-alpha-2 */
+    for (int r = 0; r < nr; r++) {
+        double bragg = tthR[r];
+        if (!(isfinite(bragg) && bragg > 0 && bragg < 180)) continue;
+        double base = bragg + v[PT_ZERO];
+        prepare_tch(base, base, v, P->minFwhm, &p1[r]);
+        double lo = base - p1[r].maxd, hi = base + p1[r].maxd;
+        int start = lower_bound(P->tth, n, lo), stop = start;
+        if (start >= n) continue;
+        while (stop < n && P->tth[stop] <= hi) stop++;
+        if (stop <= start) continue;
+        has1[r] = 1;
+        st1[4 * r] = start;
+        st1[4 * r + 1] = stop;
+    }
+    if (doublet) {
+        for (int r = 0; r < nr; r++) {
+            double bragg = tthR[r];
+            if (!(isfinite(bragg) && bragg > 0 && bragg < 180)) continue;
+            double sin2 = sin(bragg * DEG2RAD / 2.0) * (P->lambda2 / P->lambda1);
+            if (fabs(sin2) >= 1) continue;
+            double tth2 = 2 * asin(sin2) / DEG2RAD;
+            double base2 = tth2 + v[PT_ZERO];
+            prepare_tch(base2, base2, v, P->minFwhm, &p2[r]);
+            /* prep1 of this reflection (built in the first pass even if its window missed the axis) */
+            voigt_t ref1;
+            prepare_tch(bragg + v[PT_ZERO], bragg + v[PT_ZERO], v, P->minFwhm, &ref1);
+            double lpr = lp_factor(base2, P->polK) / lp_factor(ref1.x0, P->polK);
+            w2[r] = P->ratio * ref1.area / p2[r].area * lpr;
+            double lo = base2 - p2[r].maxd, hi = base2 + p2[r].maxd;
+            int start = lower_bound(P->tth, n, lo), stop = start;
+            if (start >= n) continue;
+            while (stop < n && P->tth[stop] <= hi) stop++;
+            if (stop <= start) continue;
+            has2[r] = 1;
+            st1[4 * r + 2] = start;
+            st1[4 * r + 3] = stop;
+        }
+    }
+    /* heights and the pattern (evalPhase + render): column = Ka1 + w2 Ka2 */
+    double *y = calloc(n, sizeof(double));
+    double *col = malloc(sizeof(double) * n);
+    for (int r = 0; r < nr; r++) {
+        if (!has1[r] && !has2[r]) continue;
+        if (!isfinite(tthR[r])) continue;
+        double tc = tthR[r] + v[PT_ZERO];
+        voigt_t ref1;
+        prepare_tch(tc, tc, v, P->minFwhm, &ref1);
+        double K = ref1.area;
+        if (!(K > 0)) continue;
+        double lp = lp_factor(tc, P->polK);
+        double factor = m[r] * lp * 1.0 / K;          /* height per unit S |F|^2 */
+        double height = v[PT_SCALE] * (factor * F2[r]);
+        int s0 = n, s1 = 0;
+        if (has1[r]) { if (st1[4 * r] < s0) s0 = st1[4 * r]; if (st1[4 * r + 1] > s1) s1 = st1[4 * r + 1]; }
+        if (has2[r]) { if (st1[4 * r + 2] < s0) s0 = st1[4 * r + 2]; if (st1[4 * r + 3] > s1) s1 = st1[4 * r + 3]; }
+        for (int i = s0; i < s1; i++) col[i] = 0;
+        if (has1[r])
+            for (int i = st1[4 * r]; i < st1[4 * r + 1]; i++) col[i] += 1.0 * eval_voigt(P->tth[i], &p1[r], p1[r].maxd, p1[r].pedestal);
+        if (has2[r])
+            for (int i = st1[4 * r + 2]; i < st1[4 * r + 3]; i++)
+                col[i] += w2[r] * eval_voigt(P->tth[i], &p2[r], p2[r].maxd, p2[r].pedestal);
+        if (!height) continue;
+        for (int i = s0; i < s1; i++) y[i] += height * col[i];
+    }
+    /* background (Chebyshev over the fitted range) and chi^2 */
+    double lo = P->tth[0], hi = P->tth[n - 1], chi2 = 0;
+    for (int i = 0; i < n; i++) {
+        double x = hi > lo ? 2 * (P->tth[i] - lo) / (hi - lo) - 1 : 0;
+        double Tm2 = 1, Tm1 = x, bk = 0;
+        for (int kk = 0; kk < P->nBkg; kk++) {
+            double T = kk == 0 ? 1 : kk == 1 ? x : 2 * x * Tm1 - Tm2;
+            if (kk >= 2) { Tm2 = Tm1; Tm1 = T; }
+            double b = v[PT_BKG0 + kk];
+            if (b) bk += b * T;
+        }
+        double yc = bk + y[i];
+        if (ycalc) ycalc[i] = yc;
+        if (!(P->w[i] > 0)) continue;
+        double res = P->y[i] - yc;
+        chi2 += P->w[i] * res * res;
+    }
+    free(h); free(k); free(l); free(m); free(d0); free(tthR); free(F2); free(p1); free(p2); free(st1); free(w2);
+    free(has1); free(has2); free(y); free(col);
+    return chi2;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CPU parallel tempering (temper), refined parameters mapped into v.        */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int nv;
+    const int *index;     /* refined parameter j -> full vector index */
+    const double *lo, *hi, *scales;
+    int cubic;            /* b = c = a, angles fixed */
+    int chains, sweeps;
+    double maxTemp;
+    uint32_t seed;
+} p6o_pt_setup;
+
+static void apply_params(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *base, const double *x,
+                         double *v, int nFull)
+{
+    (void)P;
+    memcpy(v, base, sizeof(double) * nFull);
+    for (int j = 0; j < S->nv; j++) v[S->index[j]] = x[j];
+    if (S->cubic) { v[PT_B] = v[PT_A]; v[PT_C] = v[PT_A]; }
+}
+
+static double reflect(double value, double low, double high)
+{
+    if (!isfinite(value)) return NAN;
+    if (isfinite(low) && isfinite(high)) {
+        double span = high - low;
+        if (!(span > 0)) return low;
+        double folded = fmod(fmod(value - low, 2 * span) + 2 * span, 2 * span);
+        return low + (folded <= span ? folded : 2 * span - folded);
+    }
+    if (value < low) return low + (low - value);
+    if (value > high) return high - (value - high);
+    return value;
+}
+
+/* temper's random(): xorshift32, (state + 0.5) / 2^32 (rietveld_core.js:2174-2177) */
+static double xorshift_uniform(uint32_t *s)
+{
+    *s ^= *s << 13;
+    *s ^= *s >> 17;
+    *s ^= *s << 5;
+    return ((double)*s + 0.5) / 4294967296.0;
+}
+
+/*
+ * Runs temper() from x0 (nv refined values).  best (nv) receives the best
+ * vector; stats: proposals, accepted, swapAttempts, swaps, bestCost,
+ * initialCost.  maxSweeps < sweeps stops early (bounded samples).
+ */
+double p6o_pt_temper(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *baseFull, int nFull,
+                     const double *x0, double *best, double *stats, int maxSweeps)
+{
+    uint32_t rs = S->seed;
+#define RND() xorshift_uniform(&rs)
+    const int nv = S->nv, C = S->chains;
+    double *v = malloc(sizeof(double) * nFull);
+    double *X = malloc(sizeof(double) * nv * C), *cost = malloc(sizeof(double) * C), *T = malloc(sizeof(double) * C);
+    double *prop = malloc(sizeof(double) * nv);
+    int *order = malloc(sizeof(int) * C);
+    apply_params(P, S, baseFull, x0, v, nFull);
+    double initial = p6o_pt_cost(P, v, NULL, NULL), bestCost = initial;
+    memcpy(best, x0, sizeof(double) * nv);
+    for (int r = 0; r < C; r++) {
+        T[r] = pow(S->maxTemp, (double)r / (C - 1));
+        memcpy(X + r * nv, x0, sizeof(double) * nv);
+        cost[r] = initial;
+        order[r] = r;
+    }
+    double proposals = 0, accepted = 0, attempts = 0, swaps = 0;
+    int sweeps = maxSweeps > 0 && maxSweeps < S->sweeps ? maxSweeps : S->sweeps;
+    for (int sweep = 0; sweep < sweeps; sweep++) {
+        for (int r = 0; r < C; r++) {
+            int slot = order[r];
+            double *x = X + slot * nv;
+            for (int move = 0; move < nv; move++) {
+                int coord = (int)floor(RND() * nv);
+                memcpy(prop, x, sizeof(double) * nv);
+                double u1 = RND();                 /* JavaScript evaluates left to right */
+                double u2 = RND();
+                double g = sqrt(-2 * log(u1)) * cos(2 * PI_ * u2);
+                prop[coord] = reflect(prop[coord] + g * S->scales[coord] * sqrt(T[r]), S->lo[coord], S->hi[coord]);
+                if (!isfinite(prop[coord])) continue;
+                apply_params(P, S, baseFull, prop, v, nFull);
+                double c = p6o_pt_cost(P, v, NULL, NULL);
+                proposals++;
+                if (isfinite(c) && (c <= cost[slot] || log(RND()) < (cost[slot] - c) / (2 * T[r]))) {
+                    memcpy(x, prop, sizeof(double) * nv);
+                    cost[slot] = c;
+                    accepted++;
+                    if (c < bestCost) { bestCost = c; memcpy(best, prop, sizeof(double) * nv); }
+                }
+            }
+        }
+        for (int r = sweep % 2; r < C - 1; r += 2) {
+            int a = order[r], b = order[r + 1];
+            double la = 0.5 * (1 / T[r] - 1 / T[r + 1]) * (cost[a] - cost[b]);
+            attempts++;
+            if (la >= 0 || log(RND()) < la) { order[r] = b; order[r + 1] = a; swaps++; }
+        }
+    }
+#undef RND
+    stats[0] = proposals; stats[1] = accepted; stats[2] = attempts; stats[3] = swaps;
+    stats[4] = bestCost; stats[5] = initial;
+    free(v); free(X); free(cost); free(T); free(prop); free(order);
+    return bestCost;
+}
+
+/* Test hooks: closed forms of the profile model. */
+double p6o_lp(double tth, double K) { return lp_factor(tth, K); }
+double p6o_peak_fwhm(double gG, double gL) { return peak_fwhm(gG, gL); }
+double p6o_soft_positive(double x, double f) { return soft_positive(x, f); }
+double p6o_soft_floor(double x, double f) { return soft_floor(x, f); }
+/* prepareVoigt (TCH) of the widths in v at tthPeak: out = x0, 1/fwhm, cL, cG, pedestal, maxd, area */
+void p6o_prepare_tch(const double *v, double minFwhm, double tthPeak, double *out)
+{
+    voigt_t p;
+    prepare_tch(tthPeak, tthPeak, v, minFwhm, &p);
+    out[0] = p.x0; out[1] = p.inv; out[2] = p.cL; out[3] = p.cG; out[4] = p.pedestal; out[5] = p.maxd; out[6] = p.area;
+}
+/* evalVoigt without truncation or pedestal, for area checks */
+double p6o_voigt_raw(double delta, double inv, double cL, double cG)
+{
+    voigt_t p = {0, inv, cL, cG, 0, INFINITY, 0};
+    return eval_voigt(delta, &p, INFINITY, 0.0);
+}

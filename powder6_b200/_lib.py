@@ -50,6 +50,19 @@ class P6WyProblem(C.Structure):
                 ('cos_mode', C.c_int), ('run_key', C.c_uint32), ('incremental', C.c_int)]
 
 
+class P6PtProblem(C.Structure):
+    _fields_ = [('n_refl', C.c_int), ('hkl', C.c_void_p), ('mult', C.c_void_p),
+                ('n_reps', C.c_int), ('rep_rot', C.c_void_p), ('rep_trans', C.c_void_p),
+                ('n_atoms', C.c_int), ('atom_pos', C.c_void_p), ('atom_wmult', C.c_void_p), ('atom_occ', C.c_void_p),
+                ('ff_a', C.c_void_p), ('ff_b', C.c_void_p), ('ff_c', C.c_void_p),
+                ('n_points', C.c_int), ('tth', C.c_void_p), ('y', C.c_void_p), ('w', C.c_void_p),
+                ('lambda1', C.c_double), ('lambda2', C.c_double), ('ratio', C.c_double), ('pol_k', C.c_double),
+                ('min_fwhm', C.c_double), ('dmin', C.c_double), ('n_bkg', C.c_int),
+                ('n_full', C.c_int), ('full_values', C.c_void_p),
+                ('nv', C.c_int), ('index', C.c_void_p), ('lo', C.c_void_p), ('hi', C.c_void_p), ('scales', C.c_void_p),
+                ('cubic', C.c_int), ('chains', C.c_int), ('max_temp', C.c_double), ('seed', C.c_uint32)]
+
+
 _P = C.c_void_p
 _SIGS = {
     'p6_last_error': (C.c_char_p, []),
@@ -78,6 +91,15 @@ _SIGS = {
     'p6_wy_last_kernel_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_wy_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     'p6_wy_query': (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    'p6_pt_create': (C.c_int, [C.POINTER(P6PtProblem), C.c_int, C.POINTER(C.c_void_p)]),
+    'p6_pt_destroy': (C.c_int, [_P]),
+    'p6_pt_costs': (C.c_int, [_P, _P, C.c_int, _P, _P]),
+    'p6_pt_initial': (C.c_int, [_P, _P, C.c_int]),
+    'p6_pt_batch': (C.c_int, [_P, C.c_int, C.c_int]),
+    'p6_pt_read_state': (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    'p6_pt_synchronize': (C.c_int, [_P, C.c_double]),
+    'p6_pt_last_batch_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
+    'p6_pt_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
 }
 
 _lib = None

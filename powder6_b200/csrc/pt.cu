@@ -1,0 +1,782 @@
+// Parallel-tempering Rietveld trial evaluation on sm_100a.
+//
+// Replaces the WebGPU backend of js/pt_gpu.js (compile / create / costs /
+// batch / run, :20-423): per chain, propose one coordinate (Gaussian step x
+// scale x sqrt(T), reflected into the bounds), evaluate the full powder
+// pattern -- reflections of the trial cell, |F|^2 over the coset
+// representatives, TCH pseudo-Voigt profiles with the K-alpha-2 doublet and
+// pedestal, Lorentz-polarisation, Chebyshev background -- and the weighted
+// chi^2, then the Metropolis test on chi^2/2 (js/rietveld_core.js:2171-2241).
+//
+// B200 layout:
+//  * one CTA per chain, one launch per sweep (nv proposals).  The adjacent
+//    exchange of the previous sweep runs at the start of the launch: both
+//    chains of a pair read the previous state (double-buffered) and derive
+//    the same decision from the same counter-based draw, so nothing is
+//    synchronised across CTAs and a sequence of sweeps can be captured in a
+//    CUDA graph;
+//  * the observed pattern is staged once per launch into shared memory;
+//  * per-reflection work (geometry, widths, areas, pedestals, Lp, weights) is
+//    FP64 -- a few dozen peaks per trial, and peak positions need it; the
+//    per-point profile shape is FP32 on an FP64 offset from the peak, and the
+//    chi^2 is accumulated and reduced in FP64;
+//  * |F|^2 takes a warp per reflection with the lanes over the coset
+//    representatives; the phase is reduced to one turn in FP64 before the
+//    FP32 sine and cosine.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "p6_common.cuh"
+
+namespace p6 {
+namespace pt {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxNv = 32;
+constexpr int kMaxFull = 64;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kD2R = kPi / 180.0;
+constexpr double kR2D = 180.0 / kPi;
+constexpr double kGconv = 0.023548200450309493;   // sqrt(8 ln 2) / 100
+constexpr double kLconv = 0.01;
+constexpr double kCg = 2.772588722239781;         // 4 ln 2
+constexpr double kWinG = 8.0, kWinL = 25.0, kWinMax = 10.0;
+
+enum { SCALE = 0, PA, PB, PC, PAL, PBE, PGA, PU, PV, PW, PX, PY, PZERO, PBISO, PBKG0 };
+
+// Chain state (device, FP64); the reference layout is produced on read-back.
+struct Chain {
+  double x[kMaxNv];
+  double best[kMaxNv];
+  double cost, bestCost;
+  double sweep, accepted, proposals, swaps, swapAttempts, valid, logu, unsolved, proposalCost, feasible;
+};
+
+struct Peak {            // one contribution (K-alpha-1 or K-alpha-2) of a reflection
+  double x0, maxd;       // centre and truncation radius, degrees
+  float inv, cL, cG, pedestal;
+  int lo, hi;            // window [lo, hi) in point indices
+};
+
+struct Params {
+  int nRefl, nReps, nAtoms, n, nBkg, nFull, nv, chains, cubic;
+  const int *hkl;        // nRefl * 3 (envelope)
+  const int *mult;
+  const int *repRot;     // nReps * 9
+  const double *repTrans;// nReps * 3
+  const double *atomPos, *atomW, *atomOcc, *ffA, *ffB, *ffC;
+  const double *tth, *y;
+  const float *w;
+  double lambda1, lambda2, ratio, polK, minFwhm, qmax;
+  const double *full;    // base full parameter vector
+  const int *index;      // nv -> full index
+  const double *lo, *hi, *scales;
+  double maxTemp;
+  uint32_t seed;
+  int stageObs;          // observed pattern staged in shared memory
+  int *errFlag;
+};
+
+// ---------------------------------------------------------------------------
+// Profile model (FP64 per peak).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double soft_positive(double x, double f) {
+  if (!isfinite(x)) return f;
+  const double h = hypot(x, 2 * f);
+  return x < 0 ? f * (f / (0.5 * h - 0.5 * x)) : 0.5 * x + 0.5 * h;
+}
+__device__ __forceinline__ double soft_floor(double x, double f) {
+  if (!isfinite(x) || !(x > 0)) return f;
+  if (!(f > 0)) return x;
+  const double r = x / f;
+  if (r > 20) return x;
+  return f * pow(pow(r, 4.0) + 1, 0.25);
+}
+__device__ __forceinline__ double peak_fwhm(double gG, double gL) {
+  gG = fmax(1e-9, gG != 0 ? gG : 1e-9);
+  gL = fmax(1e-9, gL != 0 ? gL : 1e-9);
+  const double s = pow(gG, 5.0) + 2.69269 * pow(gG, 4.0) * gL + 2.42843 * pow(gG, 3.0) * pow(gL, 2.0) +
+                   4.47163 * pow(gG, 2.0) * pow(gL, 3.0) + 0.07842 * gG * pow(gL, 4.0) + pow(gL, 5.0);
+  if (s < 0 || !isfinite(s)) return fmax(fmax(gG, gL), 1e-6);
+  return fmax(1e-6, pow(s, 0.2));
+}
+__device__ __forceinline__ double voigt64(double delta, double inv, double cL, double cG, double pedestal) {
+  const double dg = (delta * inv) * (delta * inv);
+  const double v = cL * (1.0 / (1.0 + 4.0 * dg)) + cG * exp(-kCg * dg) - pedestal;
+  return v > 0 ? v : 0.0;
+}
+// prepareVoigt, TCH branch: widths at tthPeak, centre x0.  Returns the analytic area.
+__device__ double prepare(const double *v, double minFwhm, double tthPeak, double x0, Peak &p) {
+  double gG = minFwhm, gL = minFwhm;
+  const double theta = tthPeak * (kPi / 180) / 2;
+  const double safe = fmin(theta, kPi / 2.0 - 1e-6);
+  if (!(safe < 1e-6)) {
+    const double t = tan(safe), c = cos(safe), cs = fmax(c, 1e-9);
+    const double sig2 = v[PU] * t * t + v[PV] * t + v[PW];
+    const double floorSq = pow(0.25 * minFwhm / kGconv, 2.0);
+    gG = sqrt(soft_positive(sig2, floorSq)) * kGconv;
+    gL = soft_positive(v[PX] / cs + v[PY] * t, 0.25 * minFwhm / kLconv) * kLconv;
+  }
+  gG = soft_floor(gG, minFwhm);
+  gL = soft_floor(gL, minFwhm);
+  const double HG = fmax(1e-9, gG), HL = fmax(1e-9, gL);
+  const double fwhm = fmax(1e-9, peak_fwhm(HG, HL));
+  double eta = 0;
+  if (fwhm > 1e-9) {
+    const double r = HL / fwhm;
+    eta = fmax(0.0, fmin(1.0, 1.36603 * r - 0.47719 * (r * r) + 0.11116 * pow(r, 3.0)));
+  }
+  const double g0 = 2.0 * sqrt(log(2.0) / kPi), l0 = 2.0 / kPi;
+  const double e = fmax(0.0, fmin(1.0, eta));
+  const double wL = e * l0 / fmax(1e-12, fwhm), wG = (1 - e) * g0 / fmax(1e-12, fwhm), s = wL + wG;
+  double cL = e, cG = 1 - e;
+  if (s > 0 && isfinite(s)) { cL = wL / s; cG = wG / s; }
+  const double inv = 1 / fwhm;
+  const double mult = kWinG + (kWinL - kWinG) * fmax(0.0, fmin(1.0, eta));
+  const double R = fmin(kWinMax, mult * fmax(0.01, fmax(1e-6, fwhm)));
+  const double ped = fmax(voigt64(R, inv, cL, cG, 0.0), voigt64(-R, inv, cL, cG, 0.0));
+  p.x0 = x0;
+  p.maxd = R;
+  p.inv = (float)inv;
+  p.cL = (float)cL;
+  p.cG = (float)cG;
+  p.pedestal = (float)ped;
+  return (cL * (1 / l0) + cG * (1 / g0)) * fwhm;
+}
+__device__ __forceinline__ double lp_factor(double tth, double K) {
+  if (!isfinite(tth) || tth <= 0 || tth >= 180) return 1;
+  const double th = 0.5 * tth * kD2R, s = sin(th), c = cos(th);
+  if (s < 1e-6 || c < 1e-6) return 1;
+  const double k = (isfinite(K) && K >= 0) ? K : 1;
+  const double c2 = cos(tth * kD2R);
+  return (1 / (s * s * c)) * ((1 + k * c2 * c2) / (1 + k));
+}
+__device__ __forceinline__ int lower_bound(const double *a, int n, double t) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Reciprocal metric of the cell (buildInvDsq): aa bb cc ab bc ac; false if degenerate.
+__device__ bool inv_dsq_form(const double *v, double f[6]) {
+  const double a = v[PA], b = v[PB], c = v[PC];
+  const double al = v[PAL] * kD2R, be = v[PBE] * kD2R, ga = v[PGA] * kD2R;
+  const double cA = cos(al), cB = cos(be), cG = cos(ga), sA = sin(al), sB = sin(be), sG = sin(ga);
+  const double vf = 1 - cA * cA - cB * cB - cG * cG + 2 * cA * cB * cG;
+  if (!(a > 0 && b > 0 && c > 0) || vf <= 1e-9 || fabs(sA) < 1e-9 || fabs(sB) < 1e-9 || fabs(sG) < 1e-9) return false;
+  const double V = a * b * c * sqrt(vf);
+  const double as = b * c * sA / V, bs = a * c * sB / V, cs = a * b * sG / V;
+  const double cAs = (cB * cG - cA) / (sB * sG), cBs = (cA * cG - cB) / (sA * sG), cGs = (cA * cB - cG) / (sA * sB);
+  f[0] = as * as; f[1] = bs * bs; f[2] = cs * cs;
+  f[3] = 2 * as * bs * cGs; f[4] = 2 * bs * cs * cAs; f[5] = 2 * as * cs * cBs;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// One full cost evaluation of the parameter vector in shared memory `v`.
+// All threads call it; returns chi^2 on every thread (INF if invalid).
+// ---------------------------------------------------------------------------
+struct Shared {
+  double v[kMaxFull];
+  double f[6];
+  int valid;
+  double warpChi[kWarps];
+  double chi;
+};
+
+__device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, float *h1, float *w2, int *act,
+                           const double *tth, const double *yobs, const float *wobs, float *ycalc) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
+  __syncthreads();
+  if (!sh.valid) return INFINITY;
+  const double *v = sh.v;
+  const int nR = P.nRefl;
+  const bool doublet = P.ratio > 1e-6 && P.lambda2 > 1e-6 && fabs(P.lambda1 - P.lambda2) > 1e-6;
+  // --- reflections: warp per reflection (|F|^2 over the coset representatives), lane 0 prepares the peaks
+  for (int k = warp; k < nR; k += kWarps) {
+    const int hh = P.hkl[3 * k], kk = P.hkl[3 * k + 1], ll = P.hkl[3 * k + 2];
+    const double q = hh * hh * sh.f[0] + kk * kk * sh.f[1] + ll * ll * sh.f[2] + hh * kk * sh.f[3] +
+                     kk * ll * sh.f[4] + hh * ll * sh.f[5];
+    const double s = sqrt(q), sinT = P.lambda1 * s / 2;
+    const bool live = q > 0 && q <= P.qmax && sinT < 1;
+    float A = 0.f, B = 0.f;
+    if (live) {
+      const double s2 = s * s, qq = (s / 2) * (s / 2);
+      for (int j = 0; j < P.nAtoms; ++j) {
+        double f0 = P.ffC[j];
+        for (int i = 0; i < 5; ++i) f0 += P.ffA[5 * j + i] * exp(-P.ffB[5 * j + i] * qq);
+        const double wj = P.atomOcc[j] * f0 * exp(-v[PBISO] * s2 / 4) * P.atomW[j];
+        const double *pos = P.atomPos + 3 * j;
+        float c = 0.f, sn = 0.f;
+        for (int r = lane; r < P.nReps; r += 32) {
+          const int *R = P.repRot + 9 * r;
+          const double *t = P.repTrans + 3 * r;
+          const double H0 = hh * R[0] + kk * R[3] + ll * R[6], H1 = hh * R[1] + kk * R[4] + ll * R[7],
+                       H2 = hh * R[2] + kk * R[5] + ll * R[8];
+          double turn = H0 * pos[0] + H1 * pos[1] + H2 * pos[2] + hh * t[0] + kk * t[1] + ll * t[2];
+          turn -= floor(turn);
+          float sv, cv;
+          sincospif((float)(2.0 * turn), &sv, &cv);
+          c += cv;
+          sn += sv;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          c += __shfl_xor_sync(0xffffffffu, c, o);
+          sn += __shfl_xor_sync(0xffffffffu, sn, o);
+        }
+        A += (float)wj * c;
+        B += (float)wj * sn;
+      }
+    }
+    if (lane == 0) {
+      act[k] = 0;
+      if (live) {
+        const double bragg = 2 * asin(sinT) * kR2D;
+        const double base = bragg + v[PZERO];
+        const double area1 = prepare(v, P.minFwhm, base, base, pk1[k]);
+        const double lp = lp_factor(base, P.polK);
+        const double F2 = (double)A * A + (double)B * B;
+        const double factor = P.mult[k] * lp * 1.0 / area1;
+        h1[k] = (float)(v[SCALE] * (factor * F2));
+        int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = lo;
+        while (hi < P.n && tth[hi] <= base + pk1[k].maxd) ++hi;
+        pk1[k].lo = lo;
+        pk1[k].hi = hi;
+        int flag = (hi > lo && lo < P.n) ? 1 : 0;
+        pk2[k].lo = pk2[k].hi = 0;
+        w2[k] = 0.f;
+        if (doublet) {
+          const double sin2 = sin(bragg * kD2R / 2.0) * (P.lambda2 / P.lambda1);
+          if (fabs(sin2) < 1) {
+            const double base2 = 2 * asin(sin2) / kD2R + v[PZERO];
+            const double area2 = prepare(v, P.minFwhm, base2, base2, pk2[k]);
+            const double lpr = lp_factor(base2, P.polK) / lp_factor(base, P.polK);
+            w2[k] = (float)(P.ratio * area1 / area2 * lpr);
+            int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd), hi2 = lo2;
+            while (hi2 < P.n && tth[hi2] <= base2 + pk2[k].maxd) ++hi2;
+            pk2[k].lo = lo2;
+            pk2[k].hi = hi2;
+            if (hi2 > lo2 && lo2 < P.n) flag |= 2;
+          }
+        }
+        if (!(area1 > 0)) flag = 0;
+        act[k] = flag;
+      }
+    }
+  }
+  __syncthreads();
+  // --- pattern in warp tiles of 32 points, then chi^2 (FP64)
+  double chi = 0.0;
+  const double x0 = tth[0], x1 = tth[P.n - 1];
+  for (int base = warp * 32; base < P.n; base += kThreads) {
+    const int i = base + lane;
+    const bool in = i < P.n;
+    const double x = in ? tth[i] : 0.0;
+    float yp = 0.f;
+    const int tLo = base, tHi = min(base + 32, P.n);
+    for (int k = 0; k < nR; ++k) {
+      const int a = act[k];
+      if (!a) continue;
+      const bool o1 = (a & 1) && pk1[k].lo < tHi && pk1[k].hi > tLo;
+      const bool o2 = (a & 2) && pk2[k].lo < tHi && pk2[k].hi > tLo;
+      if (!o1 && !o2) continue;
+      float col = 0.f;
+      if (o1 && in && i >= pk1[k].lo && i < pk1[k].hi) {
+        const Peak &p = pk1[k];
+        const float d = (float)(x - p.x0) * p.inv, dg = d * d;
+        const float val = p.cL * (1.0f / (1.0f + 4.0f * dg)) + p.cG * expf(-(float)kCg * dg) - p.pedestal;
+        col += val > 0.f ? val : 0.f;
+      }
+      if (o2 && in && i >= pk2[k].lo && i < pk2[k].hi) {
+        const Peak &p = pk2[k];
+        const float d = (float)(x - p.x0) * p.inv, dg = d * d;
+        const float val = p.cL * (1.0f / (1.0f + 4.0f * dg)) + p.cG * expf(-(float)kCg * dg) - p.pedestal;
+        col += w2[k] * (val > 0.f ? val : 0.f);
+      }
+      yp = fmaf(h1[k], col, yp);
+    }
+    if (in) {
+      const double z = x1 > x0 ? 2 * (x - x0) / (x1 - x0) - 1 : 0;
+      double Tm2 = 1, Tm1 = z, bk = 0;
+      for (int kk = 0; kk < P.nBkg; ++kk) {
+        const double T = kk == 0 ? 1 : kk == 1 ? z : 2 * z * Tm1 - Tm2;
+        if (kk >= 2) { Tm2 = Tm1; Tm1 = T; }
+        const double b = v[PBKG0 + kk];
+        if (b != 0) bk += b * T;
+      }
+      const double yc = bk + (double)yp;
+      if (ycalc) ycalc[i] = (float)yc;
+      const float w = wobs[i];
+      if (w > 0.f) {
+        const double r = yobs[i] - yc;
+        chi += (double)w * r * r;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) chi += __shfl_xor_sync(0xffffffffu, chi, o);
+  if (lane == 0) sh.warpChi[warp] = chi;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0;
+    for (int w = 0; w < kWarps; ++w) t += sh.warpChi[w];
+    sh.chi = isfinite(t) ? t : INFINITY;
+  }
+  __syncthreads();
+  return sh.chi;
+}
+
+__device__ __forceinline__ void apply(const Params &P, const double *x, double *v) {
+  for (int i = 0; i < P.nFull; ++i) v[i] = P.full[i];
+  for (int j = 0; j < P.nv; ++j) v[P.index[j]] = x[j];
+  if (P.cubic) { v[PB] = v[PA]; v[PC] = v[PA]; }
+}
+
+__device__ __forceinline__ double reflect(double value, double low, double high) {
+  if (!isfinite(value)) return NAN;
+  if (low > -1e300 && high < 1e300) {
+    const double span = high - low;
+    if (!(span > 0)) return low;
+    const double folded = fmod(fmod(value - low, 2 * span) + 2 * span, 2 * span);
+    return low + (folded <= span ? folded : 2 * span - folded);
+  }
+  if (value < low) return low + (low - value);
+  if (value > high) return high - (value - high);
+  return value;
+}
+
+__device__ __forceinline__ double uniform_open(uint32_t x) { return ((double)x + 0.5) / 4294967296.0; }
+
+// ---------------------------------------------------------------------------
+// Kernels.
+// ---------------------------------------------------------------------------
+struct SmemLayout {
+  int pk1, pk2, h1, w2, act, tth, y, w, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int nRefl, int n, int stage) {
+  SmemLayout L;
+  int o = 0;
+  auto take = [&](int bytes) { const int at = o; o += (bytes + 15) & ~15; return at; };
+  L.pk1 = take(nRefl * (int)sizeof(Peak));
+  L.pk2 = take(nRefl * (int)sizeof(Peak));
+  L.h1 = take(nRefl * 4);
+  L.w2 = take(nRefl * 4);
+  L.act = take(nRefl * 4);
+  L.tth = stage ? take(n * 8) : 0;
+  L.y = stage ? take(n * 8) : 0;
+  L.w = stage ? take(n * 4) : 0;
+  L.total = o;
+  return L;
+}
+
+// Cost of one parameter vector per CTA (create().costs / pattern).
+__global__ void __launch_bounds__(kThreads) pt_cost_kernel(const Params P, const double *vectors, double *costs,
+                                                           float *ycalc) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Shared sh;
+  const SmemLayout L = smem_layout(P.nRefl, P.n, 0);
+  const int c = blockIdx.x;
+  if (threadIdx.x == 0) apply(P, vectors + (size_t)c * P.nv, sh.v);
+  __syncthreads();
+  const double chi = evaluate(P, sh, reinterpret_cast<Peak *>(smem + L.pk1), reinterpret_cast<Peak *>(smem + L.pk2),
+                              reinterpret_cast<float *>(smem + L.h1), reinterpret_cast<float *>(smem + L.w2),
+                              reinterpret_cast<int *>(smem + L.act), P.tth, P.y, P.w,
+                              ycalc ? ycalc + (size_t)c * P.n : nullptr);
+  if (threadIdx.x == 0) costs[c] = chi;
+}
+
+// One sweep: the exchange of the previous sweep (if any), then `moves`
+// proposals with Metropolis.  in/out are the double-buffered chain states.
+__global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, const Chain *in, Chain *out, int moves,
+                                                            int exchangeParity, int bootstrap) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Shared sh;
+  __shared__ double xs[kMaxNv], cur;
+  __shared__ Chain st;
+  const SmemLayout L = smem_layout(P.nRefl, P.n, P.stageObs);
+  Peak *pk1 = reinterpret_cast<Peak *>(smem + L.pk1), *pk2 = reinterpret_cast<Peak *>(smem + L.pk2);
+  float *h1 = reinterpret_cast<float *>(smem + L.h1), *w2 = reinterpret_cast<float *>(smem + L.w2);
+  int *act = reinterpret_cast<int *>(smem + L.act);
+  const double *tth = P.tth, *yobs = P.y;
+  const float *wobs = P.w;
+  if (P.stageObs) {
+    double *t = reinterpret_cast<double *>(smem + L.tth), *y = reinterpret_cast<double *>(smem + L.y);
+    float *w = reinterpret_cast<float *>(smem + L.w);
+    for (int i = threadIdx.x; i < P.n; i += kThreads) { t[i] = P.tth[i]; y[i] = P.y[i]; w[i] = P.w[i]; }
+    tth = t; yobs = y; wobs = w;
+  }
+  const int c = blockIdx.x, C = P.chains;
+  const double T = pow(P.maxTemp, (double)c / (double)(C - 1));
+  if (threadIdx.x == 0) {
+    st = in[c];
+    // adjacent exchange of the previous sweep, even/odd pairs alternating
+    if (exchangeParity >= 0) {
+      const int left = ((c - exchangeParity) % 2 == 0) ? c : c - 1;
+      const int right = left + 1;
+      if (left >= exchangeParity && right < C) {
+        const Chain &a = in[left], &b = in[right];
+        const double Ta = pow(P.maxTemp, (double)left / (C - 1)), Tb = pow(P.maxTemp, (double)right / (C - 1));
+        const double la = 0.5 * (1 / Ta - 1 / Tb) * (a.cost - b.cost);
+        const uint4 r = philox4x32_10(make_uint4((uint32_t)a.sweep, (uint32_t)left, 0x45584348u, 3u),
+                                      make_uint2(P.seed, 0x9E3779B9u));
+        const bool swap = la >= 0 || log(uniform_open(r.x)) < la;
+        if (c == left) st.swapAttempts += 1;
+        if (swap) {
+          const Chain &o = (c == left) ? b : a;
+          for (int j = 0; j < P.nv; ++j) st.x[j] = o.x[j];
+          st.cost = o.cost;
+          st.feasible = o.feasible;
+          if (c == left) st.swaps += 1;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int m = 0; m < moves; ++m) {
+    if (threadIdx.x == 0) {
+      for (int j = 0; j < P.nv; ++j) xs[j] = st.x[j];
+      if (!bootstrap) {
+        const uint4 r = philox4x32_10(make_uint4((uint32_t)st.sweep, (uint32_t)c, (uint32_t)m, 1u),
+                                      make_uint2(P.seed, 0x2545F491u));
+        const int j = min(P.nv - 1, (int)(uniform_open(r.x) * P.nv));
+        const double z = sqrt(-2.0 * log(uniform_open(r.y))) * cos(2.0 * kPi * uniform_open(r.z));
+        xs[j] = reflect(st.x[j] + z * P.scales[j] * sqrt(T), P.lo[j], P.hi[j]);
+        st.logu = log(uniform_open(r.w));
+      }
+      apply(P, xs, sh.v);
+    }
+    __syncthreads();
+    const double cost = evaluate(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nullptr);
+    if (threadIdx.x == 0) {
+      st.proposalCost = cost;
+      if (bootstrap) {
+        st.cost = cost;
+        st.bestCost = cost;
+        for (int j = 0; j < P.nv; ++j) st.best[j] = st.x[j];
+      } else {
+        st.proposals += 1;
+        if (isfinite(cost) && (cost <= st.cost || st.logu < (st.cost - cost) / (2 * T))) {
+          for (int j = 0; j < P.nv; ++j) st.x[j] = xs[j];
+          st.cost = cost;
+          st.accepted += 1;
+          if (cost < st.bestCost) {
+            st.bestCost = cost;
+            for (int j = 0; j < P.nv; ++j) st.best[j] = xs[j];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (!bootstrap && moves > 0) st.sweep += 1;
+    out[c] = st;
+  }
+}
+
+}  // namespace pt
+}  // namespace p6
+
+// ===========================================================================
+// Host side.
+// ===========================================================================
+using namespace p6;
+using namespace p6::pt;
+
+struct p6_pt_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Params P{};
+  int smemSweep = 0, smemCost = 0;
+  Chain *dChain[2] = {nullptr, nullptr};
+  int curBuf = 0;
+  int pendingParity = -1;   // exchange owed by the last sweep, applied at the start of the next
+  long long sweepsDone = 0;
+  void *dAlloc[32] = {};
+  int nAlloc = 0;
+  double *dVec = nullptr, *dCost = nullptr;
+  float *dY = nullptr;
+  int vecCap = 0;
+  long long launches = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  int graphCount = 0;
+};
+
+template <typename T>
+static p6_status pt_upload(p6_pt_session *s, const T *src, size_t n, const T **dst) {
+  T *d = nullptr;
+  P6_CUDA(cudaMalloc((void **)&d, std::max<size_t>(n, 1) * sizeof(T)));
+  if (n && src) P6_CUDA(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, s->stream));
+  s->dAlloc[s->nAlloc++] = d;
+  *dst = d;
+  return P6_OK;
+}
+
+static void pt_free(p6_pt_session *s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->graphExec) cudaGraphExecDestroy(s->graphExec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  for (int i = 0; i < s->nAlloc; ++i) cudaFree(s->dAlloc[i]);
+  for (void *p : {(void *)s->dChain[0], (void *)s->dChain[1], (void *)s->dVec, (void *)s->dCost, (void *)s->dY})
+    if (p) cudaFree(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+static p6_status pt_ensure_vectors(p6_pt_session *s, int n) {
+  if (n <= s->vecCap) return P6_OK;
+  if (s->dVec) cudaFree(s->dVec);
+  if (s->dCost) cudaFree(s->dCost);
+  if (s->dY) cudaFree(s->dY);
+  s->dVec = nullptr; s->dCost = nullptr; s->dY = nullptr;
+  P6_CUDA(cudaMalloc(&s->dVec, (size_t)n * s->P.nv * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dCost, (size_t)n * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dY, (size_t)n * s->P.n * sizeof(float)));
+  s->vecCap = n;
+  return P6_OK;
+}
+
+extern "C" {
+
+p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out) {
+  clear_error();
+  if (!pr || !out) return set_error(P6_ERR_INVALID_ARG, "null problem or output pointer");
+  *out = nullptr;
+  if (pr->n_refl <= 0 || pr->n_reps <= 0 || pr->n_atoms <= 0 || pr->n_points < 2)
+    return set_error(P6_ERR_INVALID_ARG, "empty problem");
+  if (pr->nv < 1 || pr->nv > kMaxNv) return set_error(P6_ERR_CAPACITY, "1 to 32 refined parameters");
+  if (pr->n_full < PBKG0 + pr->n_bkg || pr->n_full > kMaxFull)
+    return set_error(P6_ERR_INVALID_ARG, "full parameter vector too short or too long");
+  if (pr->chains < 2 || pr->chains > 65535) return set_error(P6_ERR_INVALID_ARG, "at least 2 chains");
+  if (!(pr->max_temp > 1)) return set_error(P6_ERR_INVALID_ARG, "max_temp must exceed 1");
+  if (!pr->hkl || !pr->mult || !pr->rep_rot || !pr->rep_trans || !pr->atom_pos || !pr->atom_wmult ||
+      !pr->atom_occ || !pr->ff_a || !pr->ff_b || !pr->ff_c || !pr->tth || !pr->y || !pr->w || !pr->full_values ||
+      !pr->index || !pr->lo || !pr->hi || !pr->scales)
+    return set_error(P6_ERR_INVALID_ARG, "null table pointer");
+  for (int j = 0; j < pr->nv; ++j)
+    if (pr->index[j] < 0 || pr->index[j] >= pr->n_full) return set_error(P6_ERR_INVALID_ARG, "parameter index out of range");
+  for (int i = 1; i < pr->n_points; ++i)
+    if (!(pr->tth[i] > pr->tth[i - 1])) return set_error(P6_ERR_INVALID_ARG, "the 2-theta axis must be ascending");
+  p6_pt_session *s = new p6_pt_session();
+  s->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaSetDevice"); }
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaStreamCreate"); }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  Params &P = s->P;
+  P.nRefl = pr->n_refl; P.nReps = pr->n_reps; P.nAtoms = pr->n_atoms; P.n = pr->n_points; P.nBkg = pr->n_bkg;
+  P.nFull = pr->n_full; P.nv = pr->nv; P.chains = pr->chains; P.cubic = pr->cubic;
+  P.lambda1 = pr->lambda1; P.lambda2 = pr->lambda2; P.ratio = pr->ratio; P.polK = pr->pol_k;
+  P.minFwhm = pr->min_fwhm > 0 ? pr->min_fwhm : 1e-3;
+  P.qmax = 1.0 / (pr->dmin * pr->dmin) * (1 + 1e-9);
+  P.maxTemp = pr->max_temp;
+  P.seed = pr->seed;
+  std::vector<float> wf(pr->n_points);
+  for (int i = 0; i < pr->n_points; ++i) wf[i] = (float)pr->w[i];
+  p6_status st;
+#define PT_TRY(x) do { st = (x); if (st != P6_OK) { pt_free(s); return st; } } while (0)
+  PT_TRY(pt_upload(s, pr->hkl, (size_t)3 * pr->n_refl, &P.hkl));
+  PT_TRY(pt_upload(s, pr->mult, (size_t)pr->n_refl, &P.mult));
+  PT_TRY(pt_upload(s, pr->rep_rot, (size_t)9 * pr->n_reps, &P.repRot));
+  PT_TRY(pt_upload(s, pr->rep_trans, (size_t)3 * pr->n_reps, &P.repTrans));
+  PT_TRY(pt_upload(s, pr->atom_pos, (size_t)3 * pr->n_atoms, &P.atomPos));
+  PT_TRY(pt_upload(s, pr->atom_wmult, (size_t)pr->n_atoms, &P.atomW));
+  PT_TRY(pt_upload(s, pr->atom_occ, (size_t)pr->n_atoms, &P.atomOcc));
+  PT_TRY(pt_upload(s, pr->ff_a, (size_t)5 * pr->n_atoms, &P.ffA));
+  PT_TRY(pt_upload(s, pr->ff_b, (size_t)5 * pr->n_atoms, &P.ffB));
+  PT_TRY(pt_upload(s, pr->ff_c, (size_t)pr->n_atoms, &P.ffC));
+  PT_TRY(pt_upload(s, pr->tth, (size_t)pr->n_points, &P.tth));
+  PT_TRY(pt_upload(s, pr->y, (size_t)pr->n_points, &P.y));
+  PT_TRY(pt_upload(s, (const float *)wf.data(), (size_t)pr->n_points, &P.w));
+  PT_TRY(pt_upload(s, pr->full_values, (size_t)pr->n_full, &P.full));
+  PT_TRY(pt_upload(s, pr->index, (size_t)pr->nv, &P.index));
+  PT_TRY(pt_upload(s, pr->lo, (size_t)pr->nv, &P.lo));
+  PT_TRY(pt_upload(s, pr->hi, (size_t)pr->nv, &P.hi));
+  PT_TRY(pt_upload(s, pr->scales, (size_t)pr->nv, &P.scales));
+  int smemOptin = 0;
+  cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  const int staticBytes = 4096;
+  P.stageObs = smem_layout(P.nRefl, P.n, 1).total + staticBytes <= smemOptin ? 1 : 0;
+  s->smemSweep = smem_layout(P.nRefl, P.n, P.stageObs).total;
+  s->smemCost = smem_layout(P.nRefl, P.n, 0).total;
+  if (s->smemCost + staticBytes > smemOptin) {
+    pt_free(s);
+    return set_error(P6_ERR_CAPACITY, "too many reflections for the shared-memory peak table");
+  }
+  e = cudaFuncSetAttribute(pt_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemSweep);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(pt_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemCost);
+  if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaFuncSetAttribute"); }
+  for (int b = 0; b < 2; ++b) {
+    e = cudaMalloc(&s->dChain[b], (size_t)pr->chains * sizeof(Chain));
+    if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaMalloc chains"); }
+    cudaMemsetAsync(s->dChain[b], 0, (size_t)pr->chains * sizeof(Chain), s->stream);
+  }
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "upload"); }
+#undef PT_TRY
+  *out = s;
+  return P6_OK;
+}
+
+p6_status p6_pt_destroy(p6_pt_session *s) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  pt_free(s);
+  return P6_OK;
+}
+
+p6_status p6_pt_costs(p6_pt_session *s, const double *vectors, int n_vectors, double *costs, float *ycalc) {
+  clear_error();
+  if (!s || !vectors || !costs || n_vectors <= 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  P6_CUDA(cudaSetDevice(s->device));
+  p6_status st = pt_ensure_vectors(s, n_vectors);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaMemcpyAsync(s->dVec, vectors, (size_t)n_vectors * s->P.nv * sizeof(double), cudaMemcpyHostToDevice,
+                          s->stream));
+  pt_cost_kernel<<<n_vectors, kThreads, s->smemCost, s->stream>>>(s->P, s->dVec, s->dCost, ycalc ? s->dY : nullptr);
+  P6_CUDA(cudaGetLastError());
+  s->launches++;
+  P6_CUDA(cudaMemcpyAsync(costs, s->dCost, (size_t)n_vectors * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if (ycalc)
+    P6_CUDA(cudaMemcpyAsync(ycalc, s->dY, (size_t)n_vectors * s->P.n * sizeof(float), cudaMemcpyDeviceToHost,
+                            s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_pt_initial(p6_pt_session *s, const double *vectors, int n_vectors) {
+  clear_error();
+  if (!s || !vectors || n_vectors <= 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  P6_CUDA(cudaSetDevice(s->device));
+  std::vector<Chain> h(s->P.chains);
+  for (int c = 0; c < s->P.chains; ++c) {
+    Chain &ch = h[c];
+    std::memset(&ch, 0, sizeof(Chain));
+    const double *v = vectors + (size_t)(c % n_vectors) * s->P.nv;
+    for (int j = 0; j < s->P.nv; ++j) ch.x[j] = ch.best[j] = v[j];
+    ch.cost = ch.bestCost = 3e38;
+    ch.valid = 1;
+  }
+  P6_CUDA(cudaMemcpyAsync(s->dChain[s->curBuf], h.data(), h.size() * sizeof(Chain), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  s->pendingParity = -1;
+  s->sweepsDone = 0;
+  return P6_OK;
+}
+
+// One sweep launch: exchange owed by the previous sweep, then `moves` proposals.
+static cudaError_t pt_launch_sweep(p6_pt_session *s, int moves, int parity, int bootstrap) {
+  Chain *in = s->dChain[s->curBuf], *out = s->dChain[s->curBuf ^ 1];
+  pt_sweep_kernel<<<s->P.chains, kThreads, s->smemSweep, s->stream>>>(s->P, in, out, moves, parity, bootstrap);
+  s->curBuf ^= 1;
+  s->launches++;
+  return cudaGetLastError();
+}
+
+p6_status p6_pt_batch(p6_pt_session *s, int count, int bootstrap) {
+  clear_error();
+  if (!s || count <= 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaEventRecord(s->ev0, s->stream));
+  if (bootstrap) {
+    P6_CUDA(pt_launch_sweep(s, 1, -1, 1));
+  } else {
+    for (int j = 0; j < count; ++j) {
+      P6_CUDA(pt_launch_sweep(s, s->P.nv, s->pendingParity, 0));
+      s->pendingParity = (int)(s->sweepsDone % 2);
+      s->sweepsDone++;
+    }
+  }
+  P6_CUDA(cudaEventRecord(s->ev1, s->stream));
+  return P6_OK;
+}
+
+p6_status p6_pt_read_state(p6_pt_session *s, float *state, double *x, double *best, double *costs, double *counters) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  const int C = s->P.chains, nv = s->P.nv;
+  std::vector<Chain> h(C);
+  // the exchange owed by the last sweep is applied (exchange only, no moves) before reading
+  if (s->pendingParity >= 0) {
+    P6_CUDA(pt_launch_sweep(s, 0, s->pendingParity, 0));
+    s->pendingParity = -1;
+  }
+  P6_CUDA(cudaMemcpyAsync(h.data(), s->dChain[s->curBuf], C * sizeof(Chain), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  const int stride = 3 * nv + 12;
+  for (int c = 0; c < C; ++c) {
+    const Chain &ch = h[c];
+    if (state) {
+      float *b = state + (size_t)c * stride;
+      for (int j = 0; j < nv; ++j) { b[j] = (float)ch.x[j]; b[nv + j] = (float)ch.x[j]; b[2 * nv + j] = (float)ch.best[j]; }
+      const double tail[12] = {ch.cost, ch.bestCost, (double)s->sweepsDone, ch.accepted, ch.proposals, ch.swaps,
+                               ch.swapAttempts, ch.valid, ch.logu, ch.unsolved, ch.proposalCost, ch.feasible};
+      for (int k = 0; k < 12; ++k) b[3 * nv + k] = (float)std::min(tail[k], 3e38);
+    }
+    for (int j = 0; j < nv; ++j) {
+      if (x) x[(size_t)c * nv + j] = ch.x[j];
+      if (best) best[(size_t)c * nv + j] = ch.best[j];
+    }
+    if (costs) { costs[2 * c] = ch.cost; costs[2 * c + 1] = ch.bestCost; }
+    if (counters) {
+      counters[4 * c] = ch.accepted; counters[4 * c + 1] = ch.proposals;
+      counters[4 * c + 2] = ch.swaps; counters[4 * c + 3] = ch.swapAttempts;
+    }
+  }
+  return P6_OK;
+}
+
+p6_status p6_pt_synchronize(p6_pt_session *s, double timeout_seconds) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaStreamQuery(s->stream);
+    if (e == cudaSuccess) return P6_OK;
+    if (e != cudaErrorNotReady) return cuda_error(e, "cudaStreamQuery");
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_seconds)
+      return set_error(P6_ERR_TIMEOUT, "the device did not finish within the deadline");
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms) {
+  clear_error();
+  if (!s || !ms) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaEventSynchronize(s->ev1));
+  P6_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
+  return P6_OK;
+}
+
+p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
+  clear_error();
+  if (!s || !count) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  *count = s->launches;
+  return P6_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,439 @@
+"""Parallel-tempering backend on the B200, mirroring RVPTGPU (js/pt_gpu.js).
+
+``compile(ctx)``, ``create(ctx)`` and ``run(ctx)`` keep the reference's call
+surface (js/pt_gpu.js:20-227, 371-406, 409-423):
+
+* ``compile`` builds the plan -- the reflections of the phase over the cell
+  envelope (the upper bounds of the refined cell), the coset representatives,
+  the atoms and the observed pattern;
+* ``create`` returns an object with ``plan``, ``close()``, ``initial(vectors)``,
+  ``costs(vectors)`` and ``batch(count, bootstrap)`` (the state in the
+  reference layout, chains x (3 nv + 12) floats);
+* ``run`` validates two probes against ``ctx.cost`` (relative error 1e-3, a
+  disagreement raises with "disagrees" in the message, as js/pt_gpu.js:413-415),
+  runs ``ctx.setup.sweeps`` sweeps in batches of ceil(8 / nv), re-scores every
+  new per-chain best with ``ctx.cost`` and returns ``{x, stopped, pt}``.
+
+Any failure raises; the caller falls back to its CPU tempering, as
+RVCore.refineAsync does (js/rietveld_core.js:2450-2467).
+
+``ctx`` is a ``PTContext``: the problem (``PTProblem``), the start ``x``, the
+per-parameter bounds ``info``, ``setup`` {sweeps, chains, maxTemp, seed,
+initialCost, scales}, and the callables ``cost``, ``feasible``, ``should_stop``,
+``on_iter``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import P6PtProblem, check
+from .reflections import generate_reflections
+from .symmetry import cosets, space_group
+
+# Full parameter vector layout shared with the kernel.
+FULL_NAMES = ['scale', 'a', 'b', 'c', 'alpha', 'beta', 'gamma', 'U', 'V', 'W', 'X', 'Y', 'zero', 'Biso']
+PROFILE_WINDOW_MAX_DEG = 10.0
+
+
+@dataclass
+class PTProblem:
+    group_number: int
+    system: str
+    atoms: List[dict]                 # {element, pos (3), mult, occ, a (5), b (5), c}
+    tth: np.ndarray
+    y: np.ndarray
+    w: np.ndarray
+    lambda1: float
+    lambda2: float
+    ratio: float
+    pol_k: float
+    min_fwhm: float
+    n_bkg: int
+    values: np.ndarray                # full parameter vector
+    refined: List[str]                # names of the refined parameters
+    lo: np.ndarray
+    hi: np.ndarray
+
+    @property
+    def index(self) -> np.ndarray:
+        return np.array([self.full_index(n) for n in self.refined], dtype=np.int32)
+
+    def full_index(self, name: str) -> int:
+        if name.startswith('bkg'):
+            return len(FULL_NAMES) + int(name[3:])
+        return FULL_NAMES.index(name)
+
+    def apply(self, x: Sequence[float]) -> np.ndarray:
+        v = self.values.astype(np.float64).copy()
+        for j, i in enumerate(self.index):
+            v[i] = x[j]
+        if self.system == 'cubic':
+            v[2] = v[3] = v[1]
+        return v
+
+
+@dataclass
+class PTContext:
+    problem: PTProblem
+    x: np.ndarray
+    setup: dict
+    cost: Optional[Callable[[np.ndarray], float]] = None
+    feasible: Optional[Callable[[np.ndarray], bool]] = None
+    should_stop: Optional[Callable[[], bool]] = None
+    on_iter: Optional[Callable[[dict], None]] = None
+    max_iter: int = 0
+
+
+def reflection_dmin(problem: PTProblem) -> float:
+    """reflectionDmin with the envelope of the zero-point range (js/rietveld_core.js:238-245)."""
+    lam = problem.lambda1
+    if problem.ratio > 1e-6 and problem.lambda2 > 0:
+        lam = min(lam, problem.lambda2)
+    zi = problem.full_index('zero')
+    zmax = abs(problem.values[zi])
+    if 'zero' in problem.refined:
+        j = problem.refined.index('zero')
+        zmax = max(abs(problem.lo[j]), abs(problem.hi[j]))
+    upper = min(179.999999, float(problem.tth[-1]) + PROFILE_WINDOW_MAX_DEG + zmax + .001)
+    return lam / (2 * math.sin(math.radians(upper) / 2))
+
+
+@dataclass
+class Plan:
+    hkl: np.ndarray
+    mult: np.ndarray
+    rep_rot: np.ndarray
+    rep_trans: np.ndarray
+    dmin: float
+    nv: int
+    chains: int
+    stride: int
+    point_count: int
+    reflection_count: int
+
+
+def compile(ctx: PTContext) -> Plan:
+    """The packed plan (js/pt_gpu.js:20-227): envelope reflections, cosets."""
+    P = ctx.problem
+    g = space_group(P.group_number)
+    dmin = reflection_dmin(P)
+    v = P.values.copy()
+    # envelope: the largest cell the bounds allow (monotone for the orthogonal and cubic metrics)
+    for name in ('a', 'b', 'c'):
+        if name in P.refined:
+            v[P.full_index(name)] = P.hi[P.refined.index(name)]
+    if P.system == 'cubic':
+        v[2] = v[3] = v[1]
+    cell = {'a': v[1], 'b': v[2], 'c': v[3], 'alpha': v[4], 'beta': v[5], 'gamma': v[6]}
+    refl = generate_reflections(cell, g.ops, dmin, with_eq=False)
+    if not refl:
+        raise RuntimeError('No reflections for the PT backend.')
+    reps, _nc = cosets(g.ops)
+    hkl = np.array([[r.h, r.k, r.l] for r in refl], dtype=np.int32)
+    mult = np.array([r.m for r in refl], dtype=np.int32)
+    rep_rot = np.array([o.r for o in reps], dtype=np.int32)
+    rep_trans = np.array([o.t_frac for o in reps], dtype=np.float64)
+    nv = len(P.refined)
+    return Plan(hkl, mult, rep_rot, rep_trans, dmin, nv, int(ctx.setup['chains']), 3 * nv + 12, len(P.tth), len(refl))
+
+
+class PTSession:
+    """create(ctx) (js/pt_gpu.js:371-406): device state of one PT run."""
+
+    def __init__(self, ctx: PTContext, device: int = 0, plan: Optional[Plan] = None):
+        self.lib = _lib.load()
+        self.ctx = ctx
+        self.plan = plan or compile(ctx)
+        P = ctx.problem
+        self._keep = []
+
+        def a(x, dt):
+            x = np.ascontiguousarray(x, dtype=dt)
+            self._keep.append(x)
+            return x.ctypes.data
+
+        n_reps = len(self.plan.rep_rot)
+        pr = P6PtProblem()
+        pr.n_refl = self.plan.reflection_count
+        pr.hkl = a(self.plan.hkl, np.int32)
+        pr.mult = a(self.plan.mult, np.int32)
+        pr.n_reps = n_reps
+        pr.rep_rot = a(self.plan.rep_rot, np.int32)
+        pr.rep_trans = a(self.plan.rep_trans, np.float64)
+        pr.n_atoms = len(P.atoms)
+        pr.atom_pos = a([at['pos'] for at in P.atoms], np.float64)
+        pr.atom_wmult = a([at['mult'] / n_reps for at in P.atoms], np.float64)
+        pr.atom_occ = a([at.get('occ', 1.0) for at in P.atoms], np.float64)
+        pr.ff_a = a([at['a'] for at in P.atoms], np.float64)
+        pr.ff_b = a([at['b'] for at in P.atoms], np.float64)
+        pr.ff_c = a([at['c'] for at in P.atoms], np.float64)
+        pr.n_points = len(P.tth)
+        pr.tth = a(P.tth, np.float64)
+        pr.y = a(P.y, np.float64)
+        pr.w = a(P.w, np.float64)
+        pr.lambda1, pr.lambda2, pr.ratio, pr.pol_k = P.lambda1, P.lambda2, P.ratio, P.pol_k
+        pr.min_fwhm = P.min_fwhm
+        pr.dmin = self.plan.dmin
+        pr.n_bkg = P.n_bkg
+        pr.n_full = len(P.values)
+        pr.full_values = a(P.values, np.float64)
+        pr.nv = self.plan.nv
+        pr.index = a(P.index, np.int32)
+        pr.lo = a(P.lo, np.float64)
+        pr.hi = a(P.hi, np.float64)
+        pr.scales = a(ctx.setup['scales'], np.float64)
+        pr.cubic = 1 if P.system == 'cubic' else 0
+        pr.chains = self.plan.chains
+        pr.max_temp = float(ctx.setup['maxTemp'])
+        pr.seed = int(ctx.setup['seed']) & 0xFFFFFFFF
+        h = C.c_void_p()
+        check(self.lib.p6_pt_create(C.byref(pr), int(device), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.p6_pt_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def costs(self, vectors: Sequence[Sequence[float]], with_pattern: bool = False):
+        v = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(-1, self.plan.nv))
+        out = np.zeros(len(v), dtype=np.float64)
+        y = np.zeros((len(v), self.plan.point_count), dtype=np.float32) if with_pattern else None
+        check(self.lib.p6_pt_costs(self.h, v.ctypes.data, len(v), out.ctypes.data,
+                                   None if y is None else y.ctypes.data))
+        return (out, y) if with_pattern else out
+
+    def initial(self, vectors: Sequence[Sequence[float]]):
+        v = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(-1, self.plan.nv))
+        check(self.lib.p6_pt_initial(self.h, v.ctypes.data, len(v)))
+
+    def batch(self, count: int, bootstrap: bool = False) -> np.ndarray:
+        check(self.lib.p6_pt_batch(self.h, int(count), 1 if bootstrap else 0))
+        return self.state()
+
+    def launch(self, count: int, bootstrap: bool = False):
+        check(self.lib.p6_pt_batch(self.h, int(count), 1 if bootstrap else 0))
+
+    def state(self) -> np.ndarray:
+        st = np.zeros(self.plan.chains * self.plan.stride, dtype=np.float32)
+        check(self.lib.p6_pt_read_state(self.h, st.ctypes.data, None, None, None, None))
+        return st
+
+    def exact_state(self):
+        c, nv = self.plan.chains, self.plan.nv
+        x = np.zeros((c, nv))
+        best = np.zeros((c, nv))
+        costs = np.zeros((c, 2))
+        counters = np.zeros((c, 4))
+        check(self.lib.p6_pt_read_state(self.h, None, x.ctypes.data, best.ctypes.data, costs.ctypes.data,
+                                        counters.ctypes.data))
+        return x, best, costs, counters
+
+    def synchronize(self, timeout: float = 60.0):
+        check(self.lib.p6_pt_synchronize(self.h, float(timeout)))
+
+    def last_batch_ms(self) -> float:
+        v = C.c_float()
+        check(self.lib.p6_pt_last_batch_ms(self.h, C.byref(v)))
+        return v.value
+
+    def launch_count(self) -> int:
+        v = C.c_longlong()
+        check(self.lib.p6_pt_launch_count(self.h, C.byref(v)))
+        return v.value
+
+
+def create(ctx: PTContext, device: int = 0) -> PTSession:
+    return PTSession(ctx, device)
+
+
+def _reflected(value, lo, hi):
+    if math.isfinite(lo) and math.isfinite(hi):
+        span = hi - lo
+        if span <= 0:
+            return lo
+        folded = ((value - lo) % (2 * span) + 2 * span) % (2 * span)
+        return lo + (folded if folded <= span else 2 * span - folded)
+    return 2 * lo - value if value < lo else (2 * hi - value if value > hi else value)
+
+
+def run(ctx: PTContext, device: int = 0) -> dict:
+    """RVPTGPU.run (js/pt_gpu.js:409-423)."""
+    P = ctx.problem
+    gpu = create(ctx, device)
+    try:
+        x0 = np.asarray(ctx.x, dtype=np.float64)
+        scales = np.asarray(ctx.setup['scales'], dtype=np.float64)
+        probes = [x0, np.array([_reflected(v + s * 0.25, lo, hi) for v, s, lo, hi in zip(x0, scales, P.lo, P.hi)])]
+        chains = int(ctx.setup['chains'])
+        gc = gpu.costs([probes[c % 2] for c in range(chains)])
+        validation = 0.0
+        for c in range(chains):
+            cpu = ctx.cost(probes[c % 2]) if ctx.cost else float('nan')
+            if not math.isfinite(cpu):
+                continue
+            err = abs(gc[c] - cpu) / max(1.0, cpu)
+            validation = max(validation, err)
+            if not math.isfinite(gc[c]) or err > 1e-3:
+                raise RuntimeError(f'B200 PT cost disagrees with the double-precision model (relative error {err:.3g}).')
+        gpu.initial([x0])
+        gpu.batch(1, True)
+        best = x0.copy()
+        best_cost = float(ctx.setup.get('initialCost', ctx.cost(x0) if ctx.cost else gc[0]))
+        seen = set()
+        sweeps = int(ctx.setup['sweeps'])
+        count = max(1, math.ceil(8 / len(x0)))
+        completed = 0
+        stopped = False
+        while completed < sweeps:
+            if ctx.should_stop and ctx.should_stop():
+                stopped = True
+                break
+            n = min(count, sweeps - completed)
+            gpu.launch(n)
+            completed += n
+            _, bests, costs, _ = gpu.exact_state()
+            for c in range(chains):
+                cand = bests[c]
+                key = cand.tobytes()
+                if key in seen:
+                    continue
+                seen.add(key)
+                if not all(lo <= v <= hi for v, lo, hi in zip(cand, P.lo, P.hi)):
+                    continue
+                if ctx.feasible and not ctx.feasible(cand):
+                    continue
+                value = ctx.cost(cand) if ctx.cost else costs[c, 1]
+                if value < best_cost:
+                    best, best_cost = cand.copy(), value
+            if ctx.on_iter:
+                ctx.on_iter({'it': completed, 'chi2': best_cost, 'maxIter': ctx.max_iter, 'stage': 'pt',
+                             'backend': 'cuda'})
+        _, _, _, counters = gpu.exact_state()
+        stats = {'accepted': float(counters[:, 0].sum()), 'proposals': float(counters[:, 1].sum()),
+                 'swaps': float(counters[:, 2].sum()), 'swapAttempts': float(counters[:, 3].sum())}
+        pt = {'backend': 'cuda', 'chains': chains, 'sweeps': completed, 'requestedSweeps': sweeps,
+              'maxTemp': ctx.setup['maxTemp'], 'seed': ctx.setup['seed'],
+              'initialChi2': ctx.setup.get('initialCost'), 'bestChi2': best_cost, 'validationError': validation}
+        pt.update(stats)
+        return {'x': best, 'stopped': stopped, 'pt': pt}
+    finally:
+        gpu.close()
+
+
+# ---------------------------------------------------------------------------
+# The NaCl parallel-tempering workload (seeded, synthetic).
+# ---------------------------------------------------------------------------
+FULLPROF_TO_GSAS_U = 1803.4     # 100^2 / (8 ln 2), Kaduk & Reid (2011)
+
+
+def nacl_problem(seed: int = 1, tth0: float = 10.0, tth1: float = 120.0, step: float = 0.02,
+                 peak_counts: float = 1e4, n_bkg: int = 6) -> PTProblem:
+    """Fm-3m NaCl, a = 5.640 A, Na 4a, Cl 4b, Biso 1.0; Cu K-alpha-1/2 1.5406/1.5444,
+    ratio 0.5; TCH U, V, W = 0.004, -0.002, 0.003 deg^2 and X (strain), Y (size)
+    = 0.02, 0.01 deg in FullProf units, converted to the reference's GSAS units
+    (GU = 1803.4 U; size -> X = 100 Y_FP; strain -> Y = 100 X_FP).  The observed
+    pattern is left empty: ``synthesise`` fills it (Poisson counts, w = 1/max(1, y))."""
+    from .workloads import load_form_factor_table
+    ff = load_form_factor_table()
+    n = int(round((tth1 - tth0) / step)) + 1
+    tth = tth0 + step * np.arange(n, dtype=np.float64)
+    atoms = []
+    for el, pos in (('Na', (0.0, 0.0, 0.0)), ('Cl', (0.5, 0.5, 0.5))):
+        e = ff[el]
+        atoms.append({'element': el, 'pos': pos, 'mult': 4, 'occ': 1.0, 'a': e['a'], 'b': e['b'], 'c': e['c']})
+    vals = np.zeros(len(FULL_NAMES) + n_bkg)
+    vals[:len(FULL_NAMES)] = [1.0, 5.640, 5.640, 5.640, 90, 90, 90,
+                              FULLPROF_TO_GSAS_U * 0.004, FULLPROF_TO_GSAS_U * -0.002, FULLPROF_TO_GSAS_U * 0.003,
+                              100 * 0.01, 100 * 0.02, 0.0, 1.0]
+    vals[len(FULL_NAMES):] = [300.0, -80.0, 40.0, -15.0, 8.0, -3.0][:n_bkg]
+    refined = ['scale', 'a', 'Biso', 'U', 'V', 'W', 'zero']
+    prob = PTProblem(225, 'cubic', atoms, tth, np.zeros(n), np.ones(n), 1.5406, 1.5444, 0.5, 1.0,
+                     max(1e-4, 2 * step), n_bkg, vals, refined, np.zeros(7), np.zeros(7))
+    prob.peak_counts = peak_counts
+    prob.seed = seed
+    return prob
+
+
+def set_bounds(prob: PTProblem, truth: np.ndarray):
+    t = {n: truth[prob.full_index(n)] for n in prob.refined}
+    lo = {'scale': 0.5 * t['scale'], 'a': 0.98 * t['a'], 'Biso': 0.0, 'U': 0.0, 'V': -20.0, 'W': 0.0, 'zero': -0.1}
+    hi = {'scale': 1.5 * t['scale'], 'a': 1.02 * t['a'], 'Biso': 4.0, 'U': 40.0, 'V': 20.0, 'W': 30.0, 'zero': 0.1}
+    prob.lo = np.array([lo[n] for n in prob.refined])
+    prob.hi = np.array([hi[n] for n in prob.refined])
+
+
+def synthesise(prob: PTProblem, pattern: Callable[[PTProblem, np.ndarray], np.ndarray], seed: int = 1):
+    """Fill y, w with Poisson counts of the model at the true values, scaled so the
+    strongest point is ~prob.peak_counts; returns the true refined vector."""
+    rng = np.random.default_rng(seed)
+    truth = prob.values.copy()
+    bk = truth.copy()
+    bk[0] = 0.0
+    y_bkg = pattern(prob, bk)
+    y1 = pattern(prob, truth)
+    peak = float(np.max(y1 - y_bkg))
+    truth[0] = (getattr(prob, 'peak_counts', 1e4) - float(np.max(y_bkg))) / max(peak, 1e-30)
+    yc = pattern(prob, truth)
+    y = rng.poisson(np.maximum(yc, 0)).astype(np.float64)
+    prob.values = truth
+    prob.y = y
+    prob.w = 1.0 / np.maximum(1.0, y)
+    set_bounds(prob, truth)
+    return np.array([truth[prob.full_index(n)] for n in prob.refined])
+
+
+def start_vectors(prob: PTProblem, truth_x: np.ndarray, n: int, seed: int = 1) -> List[np.ndarray]:
+    """Uniform +/-5 % starts around the truth (the zero point, true value 0, by +/-0.01 deg)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        x = truth_x.copy()
+        for j, name in enumerate(prob.refined):
+            x[j] = truth_x[j] + (rng.uniform(-0.01, 0.01) if name == 'zero' else truth_x[j] * rng.uniform(-0.05, 0.05))
+            x[j] = min(max(x[j], prob.lo[j]), prob.hi[j])
+        out.append(x)
+    return out
+
+
+STEP_CAP = {'scale': None, 'a': 'cell', 'Biso': 2.0, 'U': 'profile', 'V': 'profile', 'W': 'profile', 'zero': 0.1}
+
+
+def natural_scales(prob: PTProblem, x: np.ndarray) -> np.ndarray:
+    """The 'natural' step of preparePT (0.15 stepCap, js/rietveld_core.js:2158-2164 and
+    :511-524); with the curvature term the caller's J'WJ diagonal may shrink it."""
+    out = np.zeros(len(x))
+    for j, name in enumerate(prob.refined):
+        cap = STEP_CAP.get(name)
+        if cap == 'cell':
+            cap = 0.02 * abs(x[j]) + 1e-6
+        elif cap == 'profile':
+            cap = 0.5 * max(abs(x[j]), 5)
+        out[j] = 0.15 * cap if cap is not None else 0.1 * max(1.0, abs(x[j]))
+    return out
+
+
+def pt_scales(prob: PTProblem, x: np.ndarray, jtwj_diag: Optional[np.ndarray] = None) -> np.ndarray:
+    nat = natural_scales(prob, x)
+    if jtwj_diag is None:
+        return nat
+    sens = np.where(jtwj_diag > 0, 1 / np.sqrt(np.maximum(jtwj_diag, 1e-300)), nat)
+    return np.maximum(np.maximum(nat, np.minimum(4 * nat, sens)), 1e-8)

@@ -1,0 +1,126 @@
+"""Parallel-tempering backend on the B200 against the FP64 oracle.
+
+The kernel computes the per-reflection work (|F|^2, TCH widths, areas, Lp,
+doublet weight) and the chi^2 accumulation in FP64 and the per-point profile
+shape in FP32, as the reference's WGSL kernel does in FP32 throughout
+(js/pt_gpu.js:229-369).  Tolerances: chi^2 relative 2e-6, calculated
+pattern absolute 2e-5 of the pattern maximum.  run() itself applies the
+reference's 1e-3 validation gate (js/pt_gpu.js:413-415)."""
+import math
+
+import numpy as np
+import pytest
+
+from powder6_b200.pt_gpu import (PTContext, PTSession, nacl_problem, pt_scales, reflection_dmin, run, start_vectors,
+                                 synthesise)
+
+pytestmark = pytest.mark.gpu
+
+CHI2_RTOL = 2e-6
+PATTERN_ATOL_FRAC = 2e-5
+
+
+@pytest.fixture(scope='module')
+def nacl(oracle):
+    P = nacl_problem(seed=1)
+    truth = synthesise(P, oracle.PtModel(P).pattern, seed=1)
+    return P, oracle.PtModel(P, dmin=reflection_dmin(P)), truth
+
+
+def ctx_of(P, x0, chains=16, sweeps=20, seed=7, max_temp=100.0, cost=None):
+    return PTContext(P, x0, {'chains': chains, 'sweeps': sweeps, 'maxTemp': max_temp, 'seed': seed,
+                             'scales': pt_scales(P, x0)}, cost=cost)
+
+
+def test_costs_match_oracle(nacl):
+    P, M, truth = nacl
+    xs = [truth] + start_vectors(P, truth, 7, seed=11)
+    with PTSession(ctx_of(P, truth, chains=len(xs))) as s:
+        g = s.costs(xs)
+    for x, gc in zip(xs, g):
+        c = M.cost(x)
+        assert abs(gc - c) <= CHI2_RTOL * c, (gc, c)
+
+
+def test_pattern_matches_oracle(nacl):
+    P, M, truth = nacl
+    xs = [truth] + start_vectors(P, truth, 3, seed=12)
+    with PTSession(ctx_of(P, truth, chains=4)) as s:
+        _, ys = s.costs(xs, with_pattern=True)
+    for x, y in zip(xs, ys):
+        _, yo, _ = M.cost_full(P.apply(x), True)
+        assert np.max(np.abs(y - yo)) <= PATTERN_ATOL_FRAC * np.max(np.abs(yo))
+
+
+def test_out_of_envelope_cell_is_infinite_or_consistent(nacl):
+    """A cell inside the bounds always scores finitely; a degenerate one (a = 0) is +inf."""
+    P, M, truth = nacl
+    x = truth.copy()
+    x[1] = P.hi[1]
+    bad = truth.copy()
+    bad[1] = 0.0
+    with PTSession(ctx_of(P, truth, chains=2)) as s:
+        g = s.costs([x, bad])
+    assert abs(g[0] - M.cost(x)) <= CHI2_RTOL * M.cost(x)
+    assert math.isinf(g[1])
+
+
+def test_batch_counters_and_monotone_best(nacl):
+    P, M, truth = nacl
+    x0 = start_vectors(P, truth, 1, seed=5)[0]
+    chains, sweeps = 16, 12
+    with PTSession(ctx_of(P, x0, chains=chains)) as s:
+        s.initial([x0])
+        s.batch(1, True)
+        _, _, c0, _ = s.exact_state()
+        s.batch(sweeps)
+        x, best, costs, counters = s.exact_state()
+        st = s.state()
+        launches = s.launch_count()
+    nv = len(x0)
+    assert counters[:, 1].sum() == chains * sweeps * nv                 # proposals; the bootstrap sweep counts none
+    assert np.all(counters[:, 0] <= counters[:, 1])                    # accepted <= proposals
+    assert np.all(counters[:, 2] <= counters[:, 3])                    # swaps <= attempts
+    assert np.all(costs[:, 1] <= c0[:, 1] + 1e-9)                       # best never worsens
+    for c in range(chains):                                             # each best re-scores to its cost
+        assert abs(M.cost(best[c]) - costs[c, 1]) <= CHI2_RTOL * costs[c, 1]
+        assert np.all(best[c] >= P.lo - 1e-12) and np.all(best[c] <= P.hi + 1e-12)
+    stride = 3 * nv + 12
+    assert st.shape == (chains * stride,)
+    assert np.allclose(st.reshape(chains, stride)[:, :nv], x, rtol=1e-6, atol=1e-6)
+    assert launches >= sweeps + 1
+
+
+def test_determinism(nacl):
+    P, M, truth = nacl
+    x0 = start_vectors(P, truth, 1, seed=6)[0]
+    out = []
+    for _ in range(2):
+        with PTSession(ctx_of(P, x0, chains=8, seed=3)) as s:
+            s.initial([x0])
+            s.batch(1, True)
+            s.batch(5)
+            out.append(s.exact_state())
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+def test_run_reduces_chi2_and_validates(nacl):
+    P, M, truth = nacl
+    x0 = start_vectors(P, truth, 1, seed=8)[0]
+    c0 = M.cost(x0)
+    ctx = ctx_of(P, x0, chains=32, sweeps=40, cost=M.cost)
+    ctx.setup['initialCost'] = c0
+    r = run(ctx)
+    assert r['pt']['validationError'] < 1e-5
+    assert r['pt']['bestChi2'] < 0.5 * c0
+    assert abs(M.cost(r['x']) - r['pt']['bestChi2']) <= 1e-12 * c0
+    assert r['pt']['proposals'] == 32 * 40 * len(x0)
+
+
+def test_run_rejects_a_disagreeing_cost(nacl):
+    P, M, truth = nacl
+    x0 = start_vectors(P, truth, 1, seed=9)[0]
+    ctx = ctx_of(P, x0, chains=4, sweeps=2, cost=lambda x: 1.01 * M.cost(x))
+    with pytest.raises(RuntimeError, match='disagrees'):
+        run(ctx)

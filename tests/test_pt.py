@@ -1,0 +1,110 @@
+"""Parallel-tempering Rietveld model: the FP64 oracle against closed forms
+restated from the reference's tests (tests/numerics.test.cjs:41-61,
+186-200; tests/regressions.test.cjs:1583-1592), the synthetic NaCl workload,
+and the CPU tempering schedule (js/rietveld_core.js:2171-2241)."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from powder6_b200.pt_gpu import (PTContext, compile, nacl_problem, natural_scales, pt_scales, reflection_dmin,
+                                 start_vectors, synthesise)
+
+
+@pytest.fixture(scope='module')
+def nacl(oracle):
+    P = nacl_problem(seed=1)
+    M = oracle.PtModel(P)
+    truth = synthesise(P, M.pattern, seed=1)
+    return P, oracle.PtModel(P, dmin=reflection_dmin(P)), truth
+
+
+def hooks(oracle):
+    lib = oracle.load()
+    for name in ('p6o_lp', 'p6o_peak_fwhm', 'p6o_soft_positive', 'p6o_soft_floor'):
+        getattr(lib, name).restype = C.c_double
+        getattr(lib, name).argtypes = [C.c_double, C.c_double]
+    lib.p6o_voigt_raw.restype = C.c_double
+    lib.p6o_voigt_raw.argtypes = [C.c_double] * 4
+    lib.p6o_prepare_tch.restype = None
+    lib.p6o_prepare_tch.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    return lib
+
+
+def test_lorentz_polarisation_closed_forms(oracle):
+    lib = hooks(oracle)
+    assert abs(lib.p6o_lp(90, 1) - 0.5 / (0.5 * math.sqrt(0.5))) < 1e-12
+    assert lib.p6o_lp(0, 1) == 1 and lib.p6o_lp(180, 1) == 1          # degenerate geometry leaves intensity alone
+    t = 60.0
+    L = 1 / (math.sin(math.radians(30)) ** 2 * math.cos(math.radians(30)))
+    assert abs(lib.p6o_lp(t, 0) - L) < 1e-12                           # K = 0: no polarisation
+    assert abs(lib.p6o_lp(t, 1) - L * (1 + 0.25) / 2) < 1e-12
+
+
+def test_width_helpers(oracle):
+    lib = hooks(oracle)
+    assert abs(lib.p6o_peak_fwhm(0.1, 1e-12) - 0.1) < 1e-9              # pure Gaussian
+    assert abs(lib.p6o_peak_fwhm(1e-12, 0.1) - 0.1) < 1e-9              # pure Lorentzian
+    assert lib.p6o_peak_fwhm(0.1, 0.1) > 0.1
+    assert lib.p6o_soft_positive(0.0, 0.3) == pytest.approx(0.3)        # f at x = 0
+    assert lib.p6o_soft_positive(1e6, 0.3) == pytest.approx(1e6)
+    assert lib.p6o_soft_positive(-1e6, 0.3) == pytest.approx(0.09 / 1e6, rel=1e-6)
+    assert lib.p6o_soft_floor(0.0, 0.04) == 0.04 and lib.p6o_soft_floor(2.0, 0.04) == 2.0
+    assert abs(lib.p6o_soft_floor(0.1, 0.04) - 0.1) / 0.1 < 0.01      # within 1 % of x by 2.5 f
+
+
+def test_area_normaliser_matches_the_integral(oracle):
+    """The analytic area of the unit-height pseudo-Voigt equals its integral
+    (the regressions.test.cjs:1583-1592 check, without asymmetry)."""
+    lib = hooks(oracle)
+    v = np.zeros(14)
+    v[7:12] = [7.2136, -3.6068, 5.4102, 1.0, 2.0]
+    out = np.zeros(7)
+    lib.p6o_prepare_tch(v.ctypes.data, 0.04, 60.0, out.ctypes.data)
+    inv, cL, cG, area = out[1], out[2], out[3], out[6]
+    fwhm = 1 / inv
+    L, n = 3000 * fwhm, 400000
+    u = -1 + (np.arange(n) + 0.5) * 2 / n
+    x = L * u ** 3
+    dx = 3 * L * u * u * 2 / n
+    vals = np.array([lib.p6o_voigt_raw(float(d), inv, cL, cG) for d in x[::50]])
+    integral = float((vals * dx[::50] * 50).sum())
+    assert abs(integral - area) < 2e-4 * area
+    # unit height at the centre, and the pedestal is the edge value
+    assert abs(lib.p6o_voigt_raw(0.0, inv, cL, cG) - 1.0) < 1e-12
+    assert abs(out[4] - lib.p6o_voigt_raw(out[5], inv, cL, cG)) < 1e-15
+
+
+def test_synthetic_nacl_and_chi2_at_truth(nacl):
+    P, M, truth = nacl
+    assert len(P.tth) == 5501 and P.tth[0] == 10.0 and abs(P.tth[-1] - 120.0) < 1e-9
+    c, y, nr = M.cost_full(P.values, True)
+    assert nr == 18
+    n = len(P.tth)
+    assert abs(c - n) < 6 * math.sqrt(2 * n)            # Poisson counts, w = 1/y: chi^2 ~ n
+    assert 0.9e4 < P.y.max() < 1.1e4
+    for x in start_vectors(P, truth, 4, seed=3):
+        assert M.cost(x) > 2 * c                         # +/-5 % starts are far off
+
+
+def test_plan_envelope_and_dmin(nacl):
+    P, M, truth = nacl
+    plan = compile(PTContext(P, truth, {'chains': 64, 'sweeps': 10, 'maxTemp': 100.0, 'seed': 1,
+                                        'scales': natural_scales(P, truth)}))
+    assert plan.reflection_count >= 18 and plan.stride == 3 * 7 + 12
+    # dmin from 2theta_max 120 + the 10 deg window + |zero| bound (0.1)
+    assert abs(plan.dmin - 1.5406 / (2 * math.sin(math.radians(130.101) / 2))) < 1e-9
+
+
+def test_cpu_tempering_schedule_and_determinism(nacl):
+    """Proposals = chains x sweeps x nv (webgpu-pt.js:131-136); same seed, same run."""
+    P, M, truth = nacl
+    x0 = start_vectors(P, truth, 1, seed=5)[0]
+    sc = pt_scales(P, x0)
+    b1, s1 = M.temper(x0, sc, chains=4, sweeps=10, seed=99)
+    b2, s2 = M.temper(x0, sc, chains=4, sweeps=10, seed=99)
+    assert np.array_equal(b1, b2) and s1 == s2
+    assert s1['proposals'] == 4 * 10 * 7
+    assert s1['swapAttempts'] == 5 * 2 + 5 * 1                # even sweeps 2 pairs, odd sweeps 1 pair
+    assert s1['bestChi2'] <= s1['initialChi2']
