@@ -255,6 +255,31 @@ p6_status p6_pt_synchronize(p6_pt_session *s, double timeout_seconds);
 p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms);
 p6_status p6_pt_launch_count(p6_pt_session *s, long long *count);
 
+/* p6_pt_costs without any device allocation.  No reference counterpart: the
+ * WebGPU backend has no caller that must avoid allocating.
+ *
+ * Same arguments, kernel and results as p6_pt_costs, but the scratch (the
+ * uploaded vectors, the costs and the optional patterns) lives in one
+ * file-scope device array of P6_PT_STATIC_SCRATCH_BYTES per device instead of
+ * buffers that p6_pt_costs grows with cudaMalloc.  For callers that cannot
+ * allocate: cudaMalloc/cudaFree synchronise the whole device, which stalls a
+ * host that keeps tempering sweeps in flight on other streams while it
+ * validates probe costs, and a host that has handed all free HBM to its own
+ * pool has nothing left for a lazy allocation to take.
+ *
+ * Limit: align256(n_vectors * nv * 8) + align256(n_vectors * 8)
+ * + (ycalc ? n_vectors * n_points * 4 : 0) <= P6_PT_STATIC_SCRATCH_BYTES;
+ * larger requests return P6_ERR_CAPACITY (split them, or use p6_pt_costs).
+ * Nothing in the scratch has to start at zero: each call writes every byte it
+ * reads.  All sessions on a device share the one array, so calls that overlap
+ * in time (two host threads, on the same or different sessions) race; a
+ * single thread never overlaps itself because the call returns only after its
+ * stream has finished.  The first call on each device looks up the array's
+ * address (cudaGetSymbolAddress); make that first call outside any stream
+ * capture. */
+#define P6_PT_STATIC_SCRATCH_BYTES (4u << 20)
+p6_status p6_pt_costs_static(p6_pt_session *s, const double *vectors, int n_vectors, double *costs, float *ycalc);
+
 /* Philox4x32-10 of one (counter, key) on the device: known-answer check. */
 p6_status p6_philox_device(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

@@ -100,6 +100,7 @@ _SIGS = {
     'p6_pt_synchronize': (C.c_int, [_P, C.c_double]),
     'p6_pt_last_batch_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_pt_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    'p6_pt_costs_static': (C.c_int, [_P, _P, C.c_int, _P, _P]),
 }
 
 _lib = None

@@ -29,6 +29,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -780,3 +781,64 @@ p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// p6_pt_costs_static: the cost kernel on a file-scope scratch array, so the
+// call allocates no device memory.
+// ===========================================================================
+static __device__ __align__(256) unsigned char g_pt_static_scratch[P6_PT_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_scratch_mu;
+unsigned char *g_static_scratch_addr[kMaxDevices] = {};
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Address of the scratch array on `device` (the current device), looked up once.
+p6_status static_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= kMaxDevices) return set_error(P6_ERR_INVALID_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+  if (!g_static_scratch_addr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_pt_static_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_pt_static_scratch)");
+    g_static_scratch_addr[device] = static_cast<unsigned char *>(p);
+  }
+  *out = g_static_scratch_addr[device];
+  return P6_OK;
+}
+}  // namespace
+
+extern "C" p6_status p6_pt_costs_static(p6_pt_session *s, const double *vectors, int n_vectors, double *costs,
+                                        float *ycalc) {
+  clear_error();
+  if (!s || !vectors || !costs || n_vectors <= 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  const size_t vecBytes = align256((size_t)n_vectors * s->P.nv * sizeof(double));
+  const size_t costBytes = align256((size_t)n_vectors * sizeof(double));
+  const size_t yBytes = ycalc ? (size_t)n_vectors * s->P.n * sizeof(float) : 0;
+  const size_t need = vecBytes + costBytes + yBytes;
+  if (need > P6_PT_STATIC_SCRATCH_BYTES)
+    return set_error(P6_ERR_CAPACITY, "p6_pt_costs_static: " + std::to_string(n_vectors) + " vectors need " +
+                                          std::to_string(need) + " bytes of scratch, more than the " +
+                                          std::to_string(P6_PT_STATIC_SCRATCH_BYTES) +
+                                          "-byte static scratch; pass fewer vectors per call or use p6_pt_costs");
+  P6_CUDA(cudaSetDevice(s->device));
+  unsigned char *base = nullptr;
+  const p6_status st = static_scratch(s->device, &base);
+  if (st != P6_OK) return st;
+  double *dVec = reinterpret_cast<double *>(base);
+  double *dCost = reinterpret_cast<double *>(base + vecBytes);
+  float *dY = ycalc ? reinterpret_cast<float *>(base + vecBytes + costBytes) : nullptr;
+  P6_CUDA(cudaMemcpyAsync(dVec, vectors, (size_t)n_vectors * s->P.nv * sizeof(double), cudaMemcpyHostToDevice,
+                          s->stream));
+  pt_cost_kernel<<<n_vectors, kThreads, s->smemCost, s->stream>>>(s->P, dVec, dCost, dY);
+  P6_CUDA(cudaGetLastError());
+  s->launches++;
+  P6_CUDA(cudaMemcpyAsync(costs, dCost, (size_t)n_vectors * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if (ycalc)
+    P6_CUDA(cudaMemcpyAsync(ycalc, dY, (size_t)n_vectors * s->P.n * sizeof(float), cudaMemcpyDeviceToHost,
+                            s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}

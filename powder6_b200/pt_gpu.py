@@ -221,6 +221,16 @@ class PTSession:
                                    None if y is None else y.ctypes.data))
         return (out, y) if with_pattern else out
 
+    def costs_static(self, vectors: Sequence[Sequence[float]], with_pattern: bool = False):
+        """costs() through p6_pt_costs_static: no device allocation, at most
+        P6_PT_STATIC_SCRATCH_BYTES (4 MiB) of vectors, costs and patterns per call."""
+        v = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(-1, self.plan.nv))
+        out = np.zeros(len(v), dtype=np.float64)
+        y = np.zeros((len(v), self.plan.point_count), dtype=np.float32) if with_pattern else None
+        check(self.lib.p6_pt_costs_static(self.h, v.ctypes.data, len(v), out.ctypes.data,
+                                          None if y is None else y.ctypes.data))
+        return (out, y) if with_pattern else out
+
     def initial(self, vectors: Sequence[Sequence[float]]):
         v = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(-1, self.plan.nv))
         check(self.lib.p6_pt_initial(self.h, v.ctypes.data, len(v)))
