@@ -280,9 +280,11 @@ def main():
         mhz = clocks['sm_mhz'] or 1965.0
         peak = MUFU_PER_CLK_PER_SM * nsm * mhz * 1e6 / 1e9
         traffic = None
-        tf = ROOT / 'profiles' / 'wy_kernel_traffic.json'
+        tf = ROOT / 'profiles' / 'wy_kernel_traffic.txt'
         if tf.exists():
-            traffic = json.loads(tf.read_text()).get('bytes_per_launch')
+            for ln in tf.read_text().splitlines():
+                if ln.startswith('bytes_per_launch:'):
+                    traffic = int(ln.split(':', 1)[1])
         line = {
             'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
