@@ -302,3 +302,79 @@ class PtModel:
                                best.ctypes.data, stats.ctypes.data, int(max_sweeps))
         return best, {'proposals': stats[0], 'accepted': stats[1], 'swapAttempts': stats[2], 'swaps': stats[3],
                       'bestChi2': stats[4], 'initialChi2': stats[5]}
+
+    def _setup(self, scales=None):
+        prob = self.prob
+        s = PtSetup()
+        s.nv = len(prob.refined)
+        idx = np.ascontiguousarray(prob.index, dtype=np.int32)
+        lo = np.ascontiguousarray(prob.lo, dtype=np.float64)
+        hi = np.ascontiguousarray(prob.hi, dtype=np.float64)
+        sc = np.ascontiguousarray(np.ones(s.nv) if scales is None else scales, dtype=np.float64)
+        self.keep += [idx, lo, hi, sc]
+        s.index, s.lo, s.hi, s.scales = idx.ctypes.data, lo.ctypes.data, hi.ctypes.data, sc.ctypes.data
+        s.cubic = 1 if prob.system == 'cubic' else 0
+        base = np.ascontiguousarray(prob.values, dtype=np.float64)
+        self.keep.append(base)
+        return s, base
+
+    def normal(self, x):
+        """normal() of the least-squares finish: (A = J'WJ, g = J'W r, f = chi^2) at x."""
+        lib = self.lib
+        lib.p6o_pt_normal.restype = C.c_int
+        lib.p6o_pt_normal.argtypes = [C.POINTER(PtProblem), C.POINTER(PtSetup), C.c_void_p, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]
+        s, base = self._setup()
+        nv = s.nv
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        A = np.zeros((nv, nv))
+        g = np.zeros(nv)
+        f = C.c_double(0)
+        ok = lib.p6o_pt_normal(C.byref(self.p), C.byref(s), base.ctypes.data, len(base), x.ctypes.data,
+                               A.ctypes.data, g.ctypes.data, C.byref(f))
+        if not ok:
+            raise ValueError('the model is not finite at x')
+        return A, g, f.value
+
+    def lm(self, x0, max_iter=20, tol=1e-5):
+        """lm() from x0: returns (x, {'chi2', 'iterations', 'accepted', 'code'})."""
+        lib = self.lib
+        lib.p6o_pt_lm.restype = C.c_int
+        lib.p6o_pt_lm.argtypes = [C.POINTER(PtProblem), C.POINTER(PtSetup), C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_int, C.c_double, C.c_void_p]
+        s, base = self._setup()
+        x = np.ascontiguousarray(np.array(x0, dtype=np.float64))
+        out = np.zeros(4)
+        lib.p6o_pt_lm(C.byref(self.p), C.byref(s), base.ctypes.data, len(base), x.ctypes.data, int(max_iter),
+                      float(tol), out.ctypes.data)
+        return x, {'chi2': out[0], 'iterations': int(out[1]), 'accepted': int(out[2]), 'code': int(out[3])}
+
+    def linear_start(self, x):
+        """One Gauss-Newton step on the scale and background parameters, kept if it
+        lowers chi^2 (js/rietveld_core.js:2252-2263)."""
+        prob = self.prob
+        lin = [j for j, n in enumerate(prob.refined) if n == 'scale' or n.startswith('bkg')]
+        A, g, f = self.normal(x)
+        x = np.array(x, dtype=np.float64)
+        if not lin:
+            return x, f
+        lib = self.lib
+        lib.p6o_solve_spd.restype = C.c_int
+        lib.p6o_solve_spd.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        M = np.ascontiguousarray(A[np.ix_(lin, lin)])
+        rhs = np.ascontiguousarray(g[lin])
+        d = np.zeros(len(lin))
+        if lib.p6o_solve_spd(M.ctypes.data, rhs.ctypes.data, len(lin), d.ctypes.data):
+            xt = x.copy()
+            for a, q in enumerate(lin):
+                xt[q] = min(prob.hi[q], max(prob.lo[q], x[q] + d[a]))
+            ft = self.cost(xt)
+            if ft < f:
+                return xt, ft
+        return x, f
+
+    def rwp(self, chi2):
+        """Rwp = sqrt(chi^2 / sum w y^2) over the points with w > 0 (datasetStats)."""
+        w, y = self.prob.w, self.prob.y
+        m = w > 0
+        return float(np.sqrt(chi2 / np.sum(w[m] * y[m] ** 2)))

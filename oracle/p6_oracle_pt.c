@@ -470,3 +470,338 @@ double p6o_voigt_raw(double delta, double inv, double cL, double cG)
     voigt_t p = {0, inv, cL, cG, 0, INFINITY, 0};
     return eval_voigt(delta, &p, INFINITY, 0.0);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Least-squares finish: normal equations and Levenberg-Marquardt            */
+/* (js/rietveld_core.js:1953-2140), finite-difference steps and limits       */
+/* (fdStep :526-538, defaultLimits :486-508, stepCap :511-524), Cholesky and */
+/* solveSPD (:1304-1335).  Parameters are identified by their full index.    */
+/* ------------------------------------------------------------------------ */
+enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG };
+
+static int kind_of(int fi)
+{
+    if (fi == PT_SCALE) return K_SCALE;
+    if (fi >= PT_A && fi <= PT_C) return K_CELL;
+    if (fi >= PT_AL && fi <= PT_GA) return K_ANGLE;
+    if (fi >= PT_U && fi <= PT_W) return K_PROFILE;
+    if (fi == PT_X || fi == PT_Y) return K_LORENTZ;
+    if (fi == PT_ZERO) return K_ZERO;
+    if (fi == PT_BISO) return K_BISO;
+    return K_BKG;
+}
+
+/* fdStep: cell a, b, c max(1e-6|v|, 1e-6); angles, zero 1e-4; others max(1e-4|v|, 1e-5) */
+static double fd_step(int kind, double v)
+{
+    double a = fabs(v);
+    switch (kind) {
+    case K_CELL: return fmax(1e-6 * a, 1e-6);
+    case K_ANGLE: return 1e-4;
+    case K_ZERO: return 1e-4;
+    default: return fmax(1e-4 * a, 1e-5);
+    }
+}
+
+/* defaultLimits: the physical range a finite-difference probe may use */
+static void default_limits(int kind, double v, double *lo, double *hi)
+{
+    switch (kind) {
+    case K_SCALE: *lo = 0; *hi = INFINITY; return;
+    case K_CELL: *lo = 0.5 * v; *hi = 2 * v; return;
+    case K_ANGLE: *lo = 30; *hi = 150; return;
+    case K_BISO: *lo = -2; *hi = 30; return;
+    case K_ZERO: *lo = -2; *hi = 2; return;
+    case K_LORENTZ: *lo = 0; *hi = INFINITY; return;
+    default: *lo = -INFINITY; *hi = INFINITY; return;
+    }
+}
+
+/* stepCap: the largest change of one iteration */
+static double step_cap(int kind, double v)
+{
+    switch (kind) {
+    case K_CELL: return 0.02 * fabs(v) + 1e-6;
+    case K_ANGLE: return 1;
+    case K_BISO: return 2;
+    case K_ZERO: return 0.1;
+    case K_PROFILE: case K_LORENTZ: return 0.5 * fmax(fabs(v), 5);
+    default: return INFINITY;
+    }
+}
+
+static int cholesky(const double *A, int n, double *L)
+{
+    memset(L, 0, sizeof(double) * n * n);
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j <= i; j++) {
+            double s = A[i * n + j];
+            for (int k = 0; k < j; k++) s -= L[i * n + k] * L[j * n + k];
+            if (i == j) {
+                if (!(s > 0) || !isfinite(s)) return 0;
+                L[i * n + i] = sqrt(s);
+            } else
+                L[i * n + j] = s / L[j * n + j];
+        }
+    return 1;
+}
+
+static void chol_solve(const double *L, const double *b, int n, double *x)
+{
+    for (int i = 0; i < n; i++) {
+        double s = b[i];
+        for (int k = 0; k < i; k++) s -= L[i * n + k] * x[k];
+        x[i] = s / L[i * n + i];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double s = x[i];
+        for (int k = i + 1; k < n; k++) s -= L[k * n + i] * x[k];
+        x[i] = s / L[i * n + i];
+    }
+}
+
+/* solveSPD with the growing ridge; returns 0 when it fails */
+int p6o_solve_spd(const double *A, const double *b, int n, double *x)
+{
+    double *L = malloc(sizeof(double) * n * n), *B = malloc(sizeof(double) * n * n);
+    int ok = cholesky(A, n, L);
+    if (!ok) {
+        double tr = 0;
+        for (int i = 0; i < n; i++) tr += fabs(A[i * n + i]);
+        double ridge = (tr / (n > 1 ? n : 1)) * 1e-12;
+        if (!(ridge > 0 || ridge < 0)) ridge = 1e-300;
+        for (int a = 0; a < 10 && !ok; a++, ridge *= 100) {
+            memcpy(B, A, sizeof(double) * n * n);
+            for (int i = 0; i < n; i++) B[i * n + i] += ridge;
+            ok = cholesky(B, n, L);
+        }
+    }
+    if (ok) chol_solve(L, b, n, x);
+    free(L); free(B);
+    return ok;
+}
+
+/* Gaussian-variance minimum of U t^2 + V t + W over t = tan(theta) of the fitted range */
+static double variance_minimum(const p6o_pt_problem *P, const double *v)
+{
+    double t0 = tan(P->tth[0] * DEG2RAD / 2), t1 = tan(P->tth[P->n - 1] * DEG2RAD / 2);
+    double U = v[PT_U], V = v[PT_V], W = v[PT_W];
+    double m = fmin(U * t0 * t0 + V * t0 + W, U * t1 * t1 + V * t1 + W);
+    if (U > 0) {
+        double ts = -V / (2 * U);
+        if (ts > t0 && ts < t1) m = fmin(m, U * ts * ts + V * ts + W);
+    }
+    return m;
+}
+static double violation_of(const p6o_pt_problem *P, const double *v)
+{
+    double m = variance_minimum(P, v);
+    return m < 0 ? -m : 0;
+}
+
+/*
+ * normal(): A = J'WJ, g = J'W r and f = chi^2 at the refined vector x.
+ * Scale and background columns are analytic, the others symmetric finite
+ * differences of the phase pattern (one-sided at a physical limit).
+ */
+int p6o_pt_normal(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *baseFull, int nFull, const double *x,
+                  double *A, double *g, double *f)
+{
+    const int n = P->n, nv = S->nv;
+    double *v = malloc(sizeof(double) * nFull), *vp = malloc(sizeof(double) * nFull);
+    double *y0 = malloc(sizeof(double) * n), *ya = malloc(sizeof(double) * n), *yb = malloc(sizeof(double) * n);
+    double *J = calloc((size_t)nv * n, sizeof(double)), *r = calloc(n, sizeof(double));
+    apply_params(P, S, baseFull, x, v, nFull);
+    double chi = p6o_pt_cost(P, v, y0, NULL);
+    if (!isfinite(chi)) { free(v); free(vp); free(y0); free(ya); free(yb); free(J); free(r); return 0; }
+    for (int j = 0; j < nv; j++) {
+        const int fi = S->index[j], kind = kind_of(fi);
+        double *col = J + (size_t)j * n;
+        if (kind == K_SCALE) {
+            memcpy(vp, v, sizeof(double) * nFull);
+            vp[PT_SCALE] = 1;
+            p6o_pt_cost(P, vp, ya, NULL);
+            vp[PT_SCALE] = 0;
+            p6o_pt_cost(P, vp, yb, NULL);
+            for (int i = 0; i < n; i++) col[i] = ya[i] - yb[i];
+        } else if (kind == K_BKG) {
+            const int kk = fi - PT_BKG0;
+            double lo = P->tth[0], hi = P->tth[n - 1];
+            for (int i = 0; i < n; i++) {
+                double z = hi > lo ? 2 * (P->tth[i] - lo) / (hi - lo) - 1 : 0, Tm2 = 1, Tm1 = z, T = 1;
+                for (int q = 0; q <= kk; q++) {
+                    T = q == 0 ? 1 : q == 1 ? z : 2 * z * Tm1 - Tm2;
+                    if (q >= 2) { Tm2 = Tm1; Tm1 = T; }
+                }
+                col[i] = T;
+            }
+        } else {
+            const double val = x[j], h = fd_step(kind, val);
+            double llo, lhi;
+            default_limits(kind, val, &llo, &lhi);
+            const int plus = val + h <= lhi, minus = val - h >= llo;
+            double xp[64], xm[64];
+            memcpy(xp, x, sizeof(double) * nv);
+            memcpy(xm, x, sizeof(double) * nv);
+            xp[j] = plus ? val + h : val;
+            xm[j] = minus ? val - h : val;
+            const double d = xp[j] - xm[j];
+            if (d != 0) {
+                if (plus) {
+                    apply_params(P, S, baseFull, xp, vp, nFull);
+                    p6o_pt_cost(P, vp, ya, NULL);
+                }
+                if (minus) {
+                    apply_params(P, S, baseFull, xm, vp, nFull);
+                    p6o_pt_cost(P, vp, yb, NULL);
+                }
+                for (int i = 0; i < n; i++) col[i] = ((plus ? ya[i] : y0[i]) - (minus ? yb[i] : y0[i])) / d;
+            }
+        }
+    }
+    double ff = 0;
+    for (int i = 0; i < n; i++) {
+        if (!(P->w[i] > 0)) continue;
+        r[i] = P->y[i] - y0[i];
+        ff += P->w[i] * r[i] * r[i];
+    }
+    for (int a = 0; a < nv; a++) {
+        const double *Ja = J + (size_t)a * n;
+        double ga = 0;
+        for (int i = 0; i < n; i++) ga += P->w[i] * Ja[i] * r[i];
+        g[a] = ga;
+        for (int b = 0; b <= a; b++) {
+            const double *Jb = J + (size_t)b * n;
+            double s = 0;
+            for (int i = 0; i < n; i++) s += P->w[i] * Ja[i] * Jb[i];
+            A[a * nv + b] = s;
+            A[b * nv + a] = s;
+        }
+    }
+    *f = ff;
+    free(v); free(vp); free(y0); free(ya); free(yb); free(J); free(r);
+    return 1;
+}
+
+static double cost_at(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *baseFull, int nFull, const double *x)
+{
+    double v[128];
+    apply_params(P, S, baseFull, x, v, nFull);
+    return p6o_pt_cost(P, v, NULL, NULL);
+}
+
+/*
+ * lm() of one stage without constraints: x (nv) in/out, bounds S->lo/hi.
+ * out[0] = chi^2, out[1] = iterations tried, out[2] = accepted steps,
+ * out[3] = exit code (0 iteration limit, 1 chi^2 change below tol,
+ * 2 projected gradient below tolerance, 3 singular, 4 stalled,
+ * 5 all parameters at limits, 6 stopped at the variance limit).
+ * The variance guard cuts a step that would make U tan^2 + V tan + W
+ * negative back to the boundary by bisection (the second of the
+ * reference's two remedies; its projection onto the face is not restated).
+ */
+int p6o_pt_lm(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *baseFull, int nFull, double *x,
+              int maxIter, double tol, double *out)
+{
+    const int nv = S->nv, nPts = P->n;
+    double *A = malloc(sizeof(double) * nv * nv), *g = malloc(sizeof(double) * nv);
+    double *Mx = malloc(sizeof(double) * nv * nv), *bx = malloc(sizeof(double) * nv), *dx = malloc(sizeof(double) * nv);
+    double xn[64], step[64], sc[64], v[128], cand[64];
+    int F[64];
+    double f = cost_at(P, S, baseFull, nFull, x), mu = 1e-3, nu = 2;
+    int conv = 0, have = 0, it, code = 0, accepted = 0;
+    if (!(tol > 0)) tol = 1e-5;
+    apply_params(P, S, baseFull, x, v, nFull);
+    double curViolation = violation_of(P, v);
+    for (it = 0; it < maxIter; it++) {
+        double fNE;
+        if (!have) {
+            if (!p6o_pt_normal(P, S, baseFull, nFull, x, A, g, &fNE)) { code = 3; break; }
+            have = 1;
+        }
+        int nF = 0;
+        for (int j = 0; j < nv; j++) {
+            const double lo = S->lo[j], hi = S->hi[j];
+            const int atLo = x[j] <= lo + 1e-12 * (1 + fabs(lo)), atHi = x[j] >= hi - 1e-12 * (1 + fabs(hi));
+            if (!((atLo && g[j] < 0) || (atHi && g[j] > 0)) && A[j * nv + j] > 0) F[nF++] = j;
+        }
+        if (!nF) { code = 5; break; }
+        double grad = 0, noise = sqrt(fmax(f / fmax(1, nPts - nv), 1e-30));
+        for (int a = 0; a < nF; a++) {
+            sc[a] = 1 / sqrt(A[F[a] * nv + F[a]]);
+            grad = fmax(grad, fabs(g[F[a]]) * sc[a] / noise);
+        }
+        if (f < 1e-24 || grad < 1e-4) { code = 2; break; }
+        for (int a = 0; a < nF; a++) {
+            bx[a] = g[F[a]] * sc[a];
+            for (int b = 0; b < nF; b++) Mx[a * nF + b] = A[F[a] * nv + F[b]] * sc[a] * sc[b];
+            Mx[a * nF + a] += mu;
+        }
+        if (!p6o_solve_spd(Mx, bx, nF, dx)) {
+            mu *= nu; nu *= 2;
+            if (mu > 1e30) { code = 3; break; }
+            continue;
+        }
+        memcpy(xn, x, sizeof(double) * nv);
+        memset(step, 0, sizeof(double) * nv);
+        for (int a = 0; a < nF; a++) {
+            const int q = F[a];
+            const double cap = step_cap(kind_of(S->index[q]), x[q]);
+            const double sh = fmax(-cap, fmin(cap, dx[a] * sc[a]));
+            xn[q] = fmin(S->hi[q], fmax(S->lo[q], x[q] + sh));
+            step[q] = xn[q] - x[q];
+        }
+        apply_params(P, S, baseFull, xn, v, nFull);
+        double violation = violation_of(P, v);
+        int blocked = 0;
+        if (curViolation == 0 && violation > 0) {
+            double loA = 0, hiA = 1;
+            for (int bi = 0; bi < 24; bi++) {
+                double mid = 0.5 * (loA + hiA);
+                for (int a = 0; a < nv; a++) cand[a] = x[a] + mid * step[a];
+                apply_params(P, S, baseFull, cand, v, nFull);
+                if (violation_of(P, v) == 0) loA = mid; else hiA = mid;
+            }
+            for (int a = 0; a < nv; a++) { xn[a] = x[a] + loA * step[a]; step[a] = xn[a] - x[a]; }
+            apply_params(P, S, baseFull, xn, v, nFull);
+            violation = violation_of(P, v);
+            blocked = 1;
+        }
+        double pred = 0, sAs = 0;
+        for (int a = 0; a < nv; a++) {
+            if (!step[a]) continue;
+            pred += 2 * g[a] * step[a];
+            double tt = 0;
+            for (int b = 0; b < nv; b++) tt += A[a * nv + b] * step[b];
+            sAs += step[a] * tt;
+        }
+        pred -= sAs;
+        const double fn = p6o_pt_cost(P, v, NULL, NULL);
+        if (fn < f) {
+            const double rho = pred > 0 ? (f - fn) / pred : 0.5, rel = (f - fn) / f;
+            int small = 1;
+            const double s2 = fmax(f, 1e-30) / fmax(1, nPts - nv);
+            for (int a = 0; a < nF; a++) {
+                const int q = F[a];
+                if (fabs(step[q]) * sqrt(A[q * nv + q] / s2) > 0.1) { small = 0; break; }
+            }
+            memcpy(x, xn, sizeof(double) * nv);
+            f = fn;
+            have = 0;
+            curViolation = violation;
+            mu *= fmax(1.0 / 3, 1 - pow(2 * rho - 1, 3));
+            nu = 2;
+            accepted++;
+            if (!blocked && rel < tol && small) {
+                if (++conv >= 2) { code = 1; it++; break; }
+            } else
+                conv = 0;
+        } else {
+            mu *= nu; nu *= 2;
+            if (mu > 1e20) { code = blocked ? 6 : (grad < 1e-3 ? 2 : 4); break; }
+        }
+    }
+    out[0] = f; out[1] = it; out[2] = accepted; out[3] = code;
+    free(A); free(g); free(Mx); free(bx); free(dx);
+    return 1;
+}

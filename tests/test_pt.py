@@ -108,3 +108,45 @@ def test_cpu_tempering_schedule_and_determinism(nacl):
     assert s1['proposals'] == 4 * 10 * 7
     assert s1['swapAttempts'] == 5 * 2 + 5 * 1                # even sweeps 2 pairs, odd sweeps 1 pair
     assert s1['bestChi2'] <= s1['initialChi2']
+
+
+def test_normal_equations_are_consistent(nacl):
+    """A = J'WJ is symmetric positive semi-definite; f is the chi^2; g = J'W r
+    is minus half the gradient of chi^2 (checked along the Gauss-Newton direction)."""
+    P, M, truth = nacl
+    x = truth.copy()
+    x[1] *= 1.0005
+    A, g, f = M.normal(x)
+    assert np.allclose(A, A.T, rtol=0, atol=0)
+    assert abs(f - M.cost(x)) <= 1e-12 * f
+    assert np.all(np.linalg.eigvalsh(A / np.sqrt(np.outer(np.diag(A), np.diag(A)))) > -1e-9)
+    d = np.linalg.solve(A, g)
+    t = 1e-4
+    slope = (M.cost(x + t * d) - M.cost(x - t * d)) / (2 * t)
+    assert abs(slope + 2 * g @ d) < 1e-4 * abs(2 * g @ d)
+
+
+def test_lm_converges_from_near_the_truth(nacl):
+    """The least-squares finish from a start inside the basin reaches chi^2 ~ n
+    (Poisson counts, w = 1/y) and stops on the chi^2-change criterion."""
+    P, M, truth = nacl
+    x0 = truth.copy()
+    x0[1] *= 1.001
+    x0[3] *= 1.2
+    x, info = M.lm(x0, 30)
+    n = len(P.tth)
+    assert info['code'] in (1, 2)
+    assert abs(info['chi2'] - n) < 6 * math.sqrt(2 * n)
+    assert info['chi2'] <= M.cost(truth) + 1e-9
+    assert abs(x[1] - truth[1]) < 1e-4
+
+
+def test_linear_start_solves_the_scale(nacl):
+    """With every other parameter at the truth, one Gauss-Newton step on the
+    (linear) scale recovers it."""
+    P, M, truth = nacl
+    x0 = truth.copy()
+    x0[0] *= 1.3
+    x, f = M.linear_start(x0)
+    assert abs(x[0] - truth[0]) < 1e-3 * truth[0]
+    assert f < M.cost(x0)
