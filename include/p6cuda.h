@@ -255,6 +255,27 @@ p6_status p6_pt_synchronize(p6_pt_session *s, double timeout_seconds);
 p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms);
 p6_status p6_pt_launch_count(p6_pt_session *s, long long *count);
 
+/* Least-squares finish after tempering (js/rietveld_core.js:1953-2140), in
+ * FP64 on the device: patterns, the finite-difference Jacobian (fdStep
+ * :526-538, central where defaultLimits :486-508 allow), the normal
+ * equations and the damped Cholesky solve (solveSPD :1304-1335).
+ *
+ * p6_pt_model_costs: chi^2 of n refined vectors (n x nv) with the FP64 model
+ *   (the re-score of new per-chain bests, js/pt_gpu.js:419-421).
+ * p6_pt_normal: A = J'WJ (nv x nv, row-major), g = J'W r, f = chi^2 at x.
+ * p6_pt_linear_start: one Gauss-Newton step on the scale and background
+ *   parameters from x, kept if it lowers chi^2 (:2252-2263); chi2 may be NULL.
+ * p6_pt_lm: lm() from x (in/out) within the session's bounds, at most
+ *   max_iter iterations, relative chi^2 tolerance tol (<= 0: 1e-5).
+ *   out (may be NULL): chi^2, iterations, accepted steps, exit code
+ *   (0 iteration limit, 1 chi^2 change below tol, 2 projected gradient below
+ *   tolerance, 3 singular system, 4 stalled, 5 all parameters at limits,
+ *   6 stopped at the Gaussian-variance limit). */
+p6_status p6_pt_model_costs(p6_pt_session *s, const double *x, int n, double *chi2);
+p6_status p6_pt_normal(p6_pt_session *s, const double *x, double *A, double *g, double *f);
+p6_status p6_pt_linear_start(p6_pt_session *s, double *x, double *chi2);
+p6_status p6_pt_lm(p6_pt_session *s, double *x, int max_iter, double tol, double *out);
+
 /* p6_pt_costs without any device allocation.  No reference counterpart: the
  * WebGPU backend has no caller that must avoid allocating.
  *

@@ -29,9 +29,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "p6_common.cuh"
@@ -67,6 +69,12 @@ struct Peak {            // one contribution (K-alpha-1 or K-alpha-2) of a refle
   int lo, hi;            // window [lo, hi) in point indices
 };
 
+struct PeakD {           // the same in FP64 throughout (least-squares finish)
+  double x0, maxd;
+  double inv, cL, cG, pedestal;
+  int lo, hi;
+};
+
 struct Params {
   int nRefl, nReps, nAtoms, n, nBkg, nFull, nv, chains, cubic;
   const int *hkl;        // nRefl * 3 (envelope)
@@ -76,6 +84,7 @@ struct Params {
   const double *atomPos, *atomW, *atomOcc, *ffA, *ffB, *ffC;
   const double *tth, *y;
   const float *w;
+  const double *wd;      // the weights in FP64 (least-squares finish)
   double lambda1, lambda2, ratio, polK, minFwhm, qmax;
   const double *full;    // base full parameter vector
   const int *index;      // nv -> full index
@@ -115,7 +124,8 @@ __device__ __forceinline__ double voigt64(double delta, double inv, double cL, d
   return v > 0 ? v : 0.0;
 }
 // prepareVoigt, TCH branch: widths at tthPeak, centre x0.  Returns the analytic area.
-__device__ double prepare(const double *v, double minFwhm, double tthPeak, double x0, Peak &p) {
+template <class PK>
+__device__ double prepare(const double *v, double minFwhm, double tthPeak, double x0, PK &p) {
   double gG = minFwhm, gL = minFwhm;
   const double theta = tthPeak * (kPi / 180) / 2;
   const double safe = fmin(theta, kPi / 2.0 - 1e-6);
@@ -146,10 +156,11 @@ __device__ double prepare(const double *v, double minFwhm, double tthPeak, doubl
   const double ped = fmax(voigt64(R, inv, cL, cG, 0.0), voigt64(-R, inv, cL, cG, 0.0));
   p.x0 = x0;
   p.maxd = R;
-  p.inv = (float)inv;
-  p.cL = (float)cL;
-  p.cG = (float)cG;
-  p.pedestal = (float)ped;
+  using T = decltype(p.inv);
+  p.inv = (T)inv;
+  p.cL = (T)cL;
+  p.cG = (T)cG;
+  p.pedestal = (T)ped;
   return (cL * (1 / l0) + cG * (1 / g0)) * fwhm;
 }
 __device__ __forceinline__ double lp_factor(double tth, double K) {
@@ -165,6 +176,16 @@ __device__ __forceinline__ int lower_bound(const double *a, int n, double t) {
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     if (a[mid] < t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// First index >= from with a[i] > t (the end of a window that starts at from).
+__device__ __forceinline__ int upper_bound(const double *a, int n, double t, int from) {
+  int lo = from, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] <= t) lo = mid + 1; else hi = mid;
   }
   return lo;
 }
@@ -196,12 +217,16 @@ struct Shared {
   double chi;
 };
 
-__device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, float *h1, float *w2, int *act,
-                           const double *tth, const double *yobs, const float *wobs, float *ycalc) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0) sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
-  __syncthreads();
-  if (!sh.valid) return INFINITY;
+// Per-reflection stage of one evaluation: |F|^2 (warp per reflection, lanes
+// over the coset representatives) and, on lane 0, the K-alpha-1/2 peaks,
+// heights and windows.  F64 = false: FP32 structure-factor sums and FP32
+// peak shapes (the tempering cost); F64 = true: FP64 throughout, with the
+// unit-scale heights u1 for the scale column of the least-squares finish.
+template <bool F64, class PK, class H>
+__device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK *pk2, H *h1, H *w2, double *u1,
+                                 int *act, const double *tth) {
+  using A_t = typename std::conditional<F64, double, float>::type;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double *v = sh.v;
   const int nR = P.nRefl;
   const bool doublet = P.ratio > 1e-6 && P.lambda2 > 1e-6 && fabs(P.lambda1 - P.lambda2) > 1e-6;
@@ -212,7 +237,7 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
                      kk * ll * sh.f[4] + hh * ll * sh.f[5];
     const double s = sqrt(q), sinT = P.lambda1 * s / 2;
     const bool live = q > 0 && q <= P.qmax && sinT < 1;
-    float A = 0.f, B = 0.f;
+    A_t A = 0, B = 0;
     if (live) {
       const double s2 = s * s, qq = (s / 2) * (s / 2);
       for (int j = 0; j < P.nAtoms; ++j) {
@@ -220,7 +245,7 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
         for (int i = 0; i < 5; ++i) f0 += P.ffA[5 * j + i] * exp(-P.ffB[5 * j + i] * qq);
         const double wj = P.atomOcc[j] * f0 * exp(-v[PBISO] * s2 / 4) * P.atomW[j];
         const double *pos = P.atomPos + 3 * j;
-        float c = 0.f, sn = 0.f;
+        A_t c = 0, sn = 0;
         for (int r = lane; r < P.nReps; r += 32) {
           const int *R = P.repRot + 9 * r;
           const double *t = P.repTrans + 3 * r;
@@ -228,8 +253,11 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
                        H2 = hh * R[2] + kk * R[5] + ll * R[8];
           double turn = H0 * pos[0] + H1 * pos[1] + H2 * pos[2] + hh * t[0] + kk * t[1] + ll * t[2];
           turn -= floor(turn);
-          float sv, cv;
-          sincospif((float)(2.0 * turn), &sv, &cv);
+          A_t sv, cv;
+          if constexpr (F64)
+            sincospi(2.0 * turn, &sv, &cv);
+          else
+            sincospif((float)(2.0 * turn), &sv, &cv);
           c += cv;
           sn += sv;
         }
@@ -238,8 +266,8 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
           c += __shfl_xor_sync(0xffffffffu, c, o);
           sn += __shfl_xor_sync(0xffffffffu, sn, o);
         }
-        A += (float)wj * c;
-        B += (float)wj * sn;
+        A += (A_t)wj * c;
+        B += (A_t)wj * sn;
       }
     }
     if (lane == 0) {
@@ -251,23 +279,23 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
         const double lp = lp_factor(base, P.polK);
         const double F2 = (double)A * A + (double)B * B;
         const double factor = P.mult[k] * lp * 1.0 / area1;
-        h1[k] = (float)(v[SCALE] * (factor * F2));
-        int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = lo;
-        while (hi < P.n && tth[hi] <= base + pk1[k].maxd) ++hi;
+        h1[k] = (H)(v[SCALE] * (factor * F2));
+        if (u1) u1[k] = factor * F2;
+        const int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = upper_bound(tth, P.n, base + pk1[k].maxd, lo);
         pk1[k].lo = lo;
         pk1[k].hi = hi;
         int flag = (hi > lo && lo < P.n) ? 1 : 0;
         pk2[k].lo = pk2[k].hi = 0;
-        w2[k] = 0.f;
+        w2[k] = 0;
         if (doublet) {
           const double sin2 = sin(bragg * kD2R / 2.0) * (P.lambda2 / P.lambda1);
           if (fabs(sin2) < 1) {
             const double base2 = 2 * asin(sin2) / kD2R + v[PZERO];
             const double area2 = prepare(v, P.minFwhm, base2, base2, pk2[k]);
             const double lpr = lp_factor(base2, P.polK) / lp_factor(base, P.polK);
-            w2[k] = (float)(P.ratio * area1 / area2 * lpr);
-            int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd), hi2 = lo2;
-            while (hi2 < P.n && tth[hi2] <= base2 + pk2[k].maxd) ++hi2;
+            w2[k] = (H)(P.ratio * area1 / area2 * lpr);
+            const int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd),
+                      hi2 = upper_bound(tth, P.n, base2 + pk2[k].maxd, lo2);
             pk2[k].lo = lo2;
             pk2[k].hi = hi2;
             if (hi2 > lo2 && lo2 < P.n) flag |= 2;
@@ -278,6 +306,17 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
       }
     }
   }
+}
+
+__device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, float *h1, float *w2, int *act,
+                           const double *tth, const double *yobs, const float *wobs, float *ycalc) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
+  __syncthreads();
+  if (!sh.valid) return INFINITY;
+  const double *v = sh.v;
+  const int nR = P.nRefl;
+  reflection_stage<false>(P, sh, pk1, pk2, h1, w2, nullptr, act, tth);
   __syncthreads();
   // --- pattern in warp tiles of 32 points, then chi^2 (FP64)
   double chi = 0.0;
@@ -489,6 +528,243 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Least-squares finish (FP64): patterns for the finite-difference Jacobian,
+// the normal equations J'WJ, J'W r, chi^2, and the damped Cholesky solve
+// (js/rietveld_core.js:1953-2140, :1304-1335).
+// ---------------------------------------------------------------------------
+struct Smem64 {
+  int pk1, pk2, h1, w2, u1, act, total;
+};
+__host__ __device__ inline Smem64 smem64_layout(int nRefl) {
+  Smem64 L;
+  int o = 0;
+  auto take = [&](int bytes) { const int at = o; o += (bytes + 15) & ~15; return at; };
+  L.pk1 = take(nRefl * (int)sizeof(PeakD));
+  L.pk2 = take(nRefl * (int)sizeof(PeakD));
+  L.h1 = take(nRefl * 8);
+  L.w2 = take(nRefl * 8);
+  L.u1 = take(nRefl * 8);
+  L.act = take(nRefl * 4);
+  L.total = o;
+  return L;
+}
+
+// FP64 pattern of refined vector c (one CTA each): y = background + peaks,
+// yu (when given; vector 0 only) = the peaks at unit scale (the scale
+// column), chiOut[c] = chi^2.
+__global__ void __launch_bounds__(kThreads) pt_pattern64_kernel(const Params P, const double *vectors, double *y,
+                                                                double *yu, double *chiOut) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Shared sh;
+  const Smem64 L = smem64_layout(P.nRefl);
+  PeakD *pk1 = reinterpret_cast<PeakD *>(smem + L.pk1), *pk2 = reinterpret_cast<PeakD *>(smem + L.pk2);
+  double *h1 = reinterpret_cast<double *>(smem + L.h1), *w2 = reinterpret_cast<double *>(smem + L.w2);
+  double *u1 = reinterpret_cast<double *>(smem + L.u1);
+  int *act = reinterpret_cast<int *>(smem + L.act);
+  const int c = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double *yc = y + (size_t)c * P.n, *yq = yu ? yu + (size_t)c * P.n : nullptr;
+  if (tid == 0) {
+    apply(P, vectors + (size_t)c * P.nv, sh.v);
+    sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!sh.valid) {
+    for (int i = tid; i < P.n; i += kThreads) {
+      yc[i] = NAN;
+      if (yq) yq[i] = NAN;
+    }
+    if (tid == 0) chiOut[c] = INFINITY;
+    return;
+  }
+  reflection_stage<true>(P, sh, pk1, pk2, h1, w2, u1, act, P.tth);
+  __syncthreads();
+  const double *v = sh.v;
+  const int nR = P.nRefl;
+  const double x0 = P.tth[0], x1 = P.tth[P.n - 1];
+  double chi = 0.0;
+  for (int base = warp * 32; base < P.n; base += kThreads) {
+    const int i = base + lane;
+    const bool in = i < P.n;
+    const double x = in ? P.tth[i] : 0.0;
+    double yp = 0.0, yu1 = 0.0;
+    const int tLo = base, tHi = min(base + 32, P.n);
+    for (int k = 0; k < nR; ++k) {
+      const int a = act[k];
+      if (!a) continue;
+      const bool o1 = (a & 1) && pk1[k].lo < tHi && pk1[k].hi > tLo;
+      const bool o2 = (a & 2) && pk2[k].lo < tHi && pk2[k].hi > tLo;
+      if (!o1 && !o2) continue;
+      double col = 0.0;
+      if (o1 && in && i >= pk1[k].lo && i < pk1[k].hi) {
+        const PeakD &p = pk1[k];
+        col += voigt64(x - p.x0, p.inv, p.cL, p.cG, p.pedestal);
+      }
+      if (o2 && in && i >= pk2[k].lo && i < pk2[k].hi) {
+        const PeakD &p = pk2[k];
+        col += w2[k] * voigt64(x - p.x0, p.inv, p.cL, p.cG, p.pedestal);
+      }
+      yp += h1[k] * col;
+      yu1 += u1[k] * col;
+    }
+    if (in) {
+      const double z = x1 > x0 ? 2 * (x - x0) / (x1 - x0) - 1 : 0;
+      double Tm2 = 1, Tm1 = z, bk = 0;
+      for (int kk = 0; kk < P.nBkg; ++kk) {
+        const double T = kk == 0 ? 1 : kk == 1 ? z : 2 * z * Tm1 - Tm2;
+        if (kk >= 2) { Tm2 = Tm1; Tm1 = T; }
+        const double b = v[PBKG0 + kk];
+        if (b != 0) bk += b * T;
+      }
+      const double ycal = bk + yp;
+      yc[i] = ycal;
+      if (yq) yq[i] = yu1;
+      const double w = P.wd[i];
+      if (w > 0) {
+        const double r = P.y[i] - ycal;
+        chi += w * r * r;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) chi += __shfl_xor_sync(0xffffffffu, chi, o);
+  if (lane == 0) sh.warpChi[warp] = chi;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0;
+    for (int w = 0; w < kWarps; ++w) t += sh.warpChi[w];
+    chiOut[c] = isfinite(t) ? t : INFINITY;
+  }
+}
+
+// Jacobian column descriptors: 0 scale (unit-scale peaks of vector 0),
+// 1 Chebyshev T_k, 2 finite difference (y[plus] - y[minus]) / step, 3 zero.
+struct LmCols {
+  int kind[kMaxNv];
+  int plus[kMaxNv], minus[kMaxNv], bkg[kMaxNv];
+  double step[kMaxNv];
+};
+
+__device__ __forceinline__ double cheb_t(int k, double z) {
+  double Tm2 = 1, Tm1 = z, T = 1;
+  for (int q = 0; q <= k; ++q) {
+    T = q == 0 ? 1 : q == 1 ? z : 2 * z * Tm1 - Tm2;
+    if (q >= 2) { Tm2 = Tm1; Tm1 = T; }
+  }
+  return T;
+}
+
+__device__ __forceinline__ double jcol(const Params &P, const LmCols &L, int j, int i, const double *y,
+                                       const double *yu, double z) {
+  switch (L.kind[j]) {
+    case 0: return yu[i];
+    case 1: return cheb_t(L.bkg[j], z);
+    case 2: return (y[(size_t)L.plus[j] * P.n + i] - y[(size_t)L.minus[j] * P.n + i]) / L.step[j];
+    default: return 0.0;
+  }
+}
+
+// Normal equations: block b < nv(nv+1)/2 -> A[a][b'] (a >= b'), then nv blocks
+// of g, then one block of f.  Strided FP64 sums, reduced in a fixed order.
+__global__ void __launch_bounds__(kThreads) pt_normal_kernel(const Params P, const LmCols L, const double *y,
+                                                             const double *yu, double *out) {
+  __shared__ double part[kWarps];
+  const int nv = P.nv, nPairs = nv * (nv + 1) / 2, b = blockIdx.x, tid = threadIdx.x;
+  int ja = -1, jb = -1, mode;
+  if (b < nPairs) {
+    mode = 0;
+    int a = 0, rem = b;
+    while (rem > a) { rem -= a + 1; ++a; }
+    ja = a; jb = rem;
+  } else if (b < nPairs + nv) {
+    mode = 1;
+    ja = b - nPairs;
+  } else {
+    mode = 2;
+  }
+  const double x0 = P.tth[0], x1 = P.tth[P.n - 1];
+  double acc = 0.0;
+  for (int i = tid; i < P.n; i += kThreads) {
+    const double w = P.wd[i];
+    const double z = x1 > x0 ? 2 * (P.tth[i] - x0) / (x1 - x0) - 1 : 0;
+    const double r = w > 0 ? P.y[i] - y[i] : 0.0;
+    if (mode == 0)
+      acc += w * jcol(P, L, ja, i, y, yu, z) * jcol(P, L, jb, i, y, yu, z);
+    else if (mode == 1)
+      acc += w * jcol(P, L, ja, i, y, yu, z) * r;
+    else if (w > 0)
+      acc += w * r * r;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((tid & 31) == 0) part[tid >> 5] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0;
+    for (int w = 0; w < kWarps; ++w) t += part[w];
+    if (mode == 0) {
+      out[ja * nv + jb] = t;
+      out[jb * nv + ja] = t;
+    } else if (mode == 1) {
+      out[nv * nv + ja] = t;
+    } else {
+      out[nv * nv + nv] = t;
+    }
+  }
+}
+
+// solveSPD on the free set F (nF indices into A, g).  mode 0: the scaled,
+// damped LM system (D A_FF D + mu I) d = D g_F, result D d; mode 1: A_FF d = g_F.
+// One thread; FP64 Cholesky with the growing ridge.  out[nF] = 1 on success.
+__global__ void pt_lm_solve_kernel(const double *A, const double *g, int nv, const int *F, int nF, double mu, int mode,
+                                   double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double M[kMaxNv * kMaxNv], Lc[kMaxNv * kMaxNv], rhs[kMaxNv], sc[kMaxNv], x[kMaxNv];
+  for (int a = 0; a < nF; ++a) sc[a] = mode == 0 ? 1.0 / sqrt(A[F[a] * nv + F[a]]) : 1.0;
+  for (int a = 0; a < nF; ++a) {
+    rhs[a] = g[F[a]] * sc[a];
+    for (int b = 0; b < nF; ++b) M[a * nF + b] = A[F[a] * nv + F[b]] * sc[a] * sc[b];
+    if (mode == 0) M[a * nF + a] += mu;
+  }
+  auto chol = [&](double ridge) -> bool {
+    for (int i = 0; i < nF; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double s = M[i * nF + j] + (i == j ? ridge : 0.0);
+        for (int k = 0; k < j; ++k) s -= Lc[i * nF + k] * Lc[j * nF + k];
+        if (i == j) {
+          if (!(s > 0) || !isfinite(s)) return false;
+          Lc[i * nF + i] = sqrt(s);
+        } else {
+          Lc[i * nF + j] = s / Lc[j * nF + j];
+        }
+      }
+    return true;
+  };
+  bool ok = chol(0.0);
+  if (!ok) {
+    double tr = 0;
+    for (int i = 0; i < nF; ++i) tr += fabs(M[i * nF + i]);
+    double ridge = (tr / (nF > 1 ? nF : 1)) * 1e-12;
+    if (!(ridge > 0 || ridge < 0)) ridge = 1e-300;
+    for (int a = 0; a < 10 && !ok; ++a, ridge *= 100) ok = chol(ridge);
+  }
+  if (ok) {
+    for (int i = 0; i < nF; ++i) {
+      double s = rhs[i];
+      for (int k = 0; k < i; ++k) s -= Lc[i * nF + k] * x[k];
+      x[i] = s / Lc[i * nF + i];
+    }
+    for (int i = nF - 1; i >= 0; --i) {
+      double s = x[i];
+      for (int k = i + 1; k < nF; ++k) s -= Lc[k * nF + i] * x[k];
+      x[i] = s / Lc[i * nF + i];
+    }
+    for (int a = 0; a < nF; ++a) out[a] = x[a] * sc[a];
+  }
+  out[nF] = ok ? 1.0 : 0.0;
+}
+
 }  // namespace pt
 }  // namespace p6
 
@@ -517,6 +793,14 @@ struct p6_pt_session {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graphExec = nullptr;
   int graphCount = 0;
+  // least-squares finish: host copies of the parameter description and FP64 scratch
+  std::vector<double> fullHost, loHost, hiHost;
+  std::vector<int> indexHost;
+  double tthFirst = 0, tthLast = 0;
+  int smem64 = 0;
+  double *dLmVec = nullptr, *dLmY = nullptr, *dLmYu = nullptr, *dLmChi = nullptr, *dLmOut = nullptr;
+  int *dLmF = nullptr;
+  int lmCap = 0;
 };
 
 template <typename T>
@@ -536,7 +820,9 @@ static void pt_free(p6_pt_session *s) {
   if (s->graphExec) cudaGraphExecDestroy(s->graphExec);
   if (s->graph) cudaGraphDestroy(s->graph);
   for (int i = 0; i < s->nAlloc; ++i) cudaFree(s->dAlloc[i]);
-  for (void *p : {(void *)s->dChain[0], (void *)s->dChain[1], (void *)s->dVec, (void *)s->dCost, (void *)s->dY})
+  for (void *p : {(void *)s->dChain[0], (void *)s->dChain[1], (void *)s->dVec, (void *)s->dCost, (void *)s->dY,
+                  (void *)s->dLmVec, (void *)s->dLmY, (void *)s->dLmYu, (void *)s->dLmChi, (void *)s->dLmOut,
+                  (void *)s->dLmF})
     if (p) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -611,6 +897,7 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
   PT_TRY(pt_upload(s, pr->tth, (size_t)pr->n_points, &P.tth));
   PT_TRY(pt_upload(s, pr->y, (size_t)pr->n_points, &P.y));
   PT_TRY(pt_upload(s, (const float *)wf.data(), (size_t)pr->n_points, &P.w));
+  PT_TRY(pt_upload(s, pr->w, (size_t)pr->n_points, &P.wd));
   PT_TRY(pt_upload(s, pr->full_values, (size_t)pr->n_full, &P.full));
   PT_TRY(pt_upload(s, pr->index, (size_t)pr->nv, &P.index));
   PT_TRY(pt_upload(s, pr->lo, (size_t)pr->nv, &P.lo));
@@ -626,7 +913,17 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
     pt_free(s);
     return set_error(P6_ERR_CAPACITY, "too many reflections for the shared-memory peak table");
   }
+  // the FP64 peak table of the least-squares finish; 0 when it does not fit (the finish then reports CAPACITY)
+  s->smem64 = smem64_layout(P.nRefl).total + staticBytes <= smemOptin ? smem64_layout(P.nRefl).total : 0;
+  s->fullHost.assign(pr->full_values, pr->full_values + pr->n_full);
+  s->indexHost.assign(pr->index, pr->index + pr->nv);
+  s->loHost.assign(pr->lo, pr->lo + pr->nv);
+  s->hiHost.assign(pr->hi, pr->hi + pr->nv);
+  s->tthFirst = pr->tth[0];
+  s->tthLast = pr->tth[pr->n_points - 1];
   e = cudaFuncSetAttribute(pt_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemSweep);
+  if (e == cudaSuccess && s->smem64 > 0)
+    e = cudaFuncSetAttribute(pt_pattern64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smem64);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(pt_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemCost);
   if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaFuncSetAttribute"); }
   for (int b = 0; b < 2; ++b) {
@@ -781,6 +1078,342 @@ p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
 }
 
 }  // extern "C"
+
+
+// ===========================================================================
+// Least-squares finish (js/rietveld_core.js:1953-2140): FP64 patterns and
+// normal equations on the device, the damped Cholesky solve on the device,
+// the scalar control of lm() on the host.
+// ===========================================================================
+namespace {
+enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG };
+
+int lm_kind(int fi) {
+  if (fi == SCALE) return K_SCALE;
+  if (fi >= PA && fi <= PC) return K_CELL;
+  if (fi >= PAL && fi <= PGA) return K_ANGLE;
+  if (fi >= PU && fi <= PW) return K_PROFILE;
+  if (fi == PX || fi == PY) return K_LORENTZ;
+  if (fi == PZERO) return K_ZERO;
+  if (fi == PBISO) return K_BISO;
+  return K_BKG;
+}
+// fdStep (js/rietveld_core.js:526-538)
+double lm_fd_step(int kind, double v) {
+  const double a = std::fabs(v);
+  switch (kind) {
+    case K_CELL: return std::max(1e-6 * a, 1e-6);
+    case K_ANGLE: case K_ZERO: return 1e-4;
+    default: return std::max(1e-4 * a, 1e-5);
+  }
+}
+// defaultLimits (js/rietveld_core.js:486-508): the range a finite-difference probe may use
+void lm_limits(int kind, double v, double *lo, double *hi) {
+  const double inf = std::numeric_limits<double>::infinity();
+  switch (kind) {
+    case K_SCALE: *lo = 0; *hi = inf; return;
+    case K_CELL: *lo = 0.5 * v; *hi = 2 * v; return;
+    case K_ANGLE: *lo = 30; *hi = 150; return;
+    case K_BISO: *lo = -2; *hi = 30; return;
+    case K_ZERO: *lo = -2; *hi = 2; return;
+    case K_LORENTZ: *lo = 0; *hi = inf; return;
+    default: *lo = -inf; *hi = inf; return;
+  }
+}
+// stepCap (js/rietveld_core.js:511-524)
+double lm_step_cap(int kind, double v) {
+  switch (kind) {
+    case K_CELL: return 0.02 * std::fabs(v) + 1e-6;
+    case K_ANGLE: return 1;
+    case K_BISO: return 2;
+    case K_ZERO: return 0.1;
+    case K_PROFILE: case K_LORENTZ: return 0.5 * std::max(std::fabs(v), 5.0);
+    default: return std::numeric_limits<double>::infinity();
+  }
+}
+
+// How far the Gaussian variance U tan^2 + V tan + W falls below zero over the fitted range.
+double lm_violation(const p6_pt_session *s, const double *x) {
+  std::vector<double> v = s->fullHost;
+  for (size_t j = 0; j < s->indexHost.size(); ++j) v[s->indexHost[j]] = x[j];
+  const double t0 = std::tan(s->tthFirst * kD2R / 2), t1 = std::tan(s->tthLast * kD2R / 2);
+  const double U = v[PU], V = v[PV], W = v[PW];
+  double m = std::min(U * t0 * t0 + V * t0 + W, U * t1 * t1 + V * t1 + W);
+  if (U > 0) {
+    const double ts = -V / (2 * U);
+    if (ts > t0 && ts < t1) m = std::min(m, U * ts * ts + V * ts + W);
+  }
+  return m < 0 ? -m : 0;
+}
+
+p6_status lm_ensure(p6_pt_session *s, int m) {
+  if (s->smem64 <= 0)
+    return set_error(P6_ERR_CAPACITY, "too many reflections for the FP64 peak table of the least-squares finish");
+  if (m <= s->lmCap) return P6_OK;
+  for (void *p : {(void *)s->dLmVec, (void *)s->dLmY, (void *)s->dLmYu, (void *)s->dLmChi, (void *)s->dLmOut,
+                  (void *)s->dLmF})
+    if (p) cudaFree(p);
+  s->dLmVec = s->dLmY = s->dLmYu = s->dLmChi = s->dLmOut = nullptr;
+  s->dLmF = nullptr;
+  s->lmCap = 0;
+  const int nv = s->P.nv, n = s->P.n;
+  P6_CUDA(cudaMalloc(&s->dLmVec, (size_t)m * nv * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dLmY, (size_t)m * n * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dLmYu, (size_t)n * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dLmChi, (size_t)m * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dLmOut, (size_t)(nv * nv + nv + 1 + kMaxNv + 1) * sizeof(double)));
+  P6_CUDA(cudaMalloc(&s->dLmF, (size_t)kMaxNv * sizeof(int)));
+  s->lmCap = m;
+  return P6_OK;
+}
+
+// chi^2 of n refined vectors with the FP64 model (one CTA each).
+p6_status lm_costs(p6_pt_session *s, const double *x, int n, double *f) {
+  p6_status st = lm_ensure(s, n);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaMemcpyAsync(s->dLmVec, x, (size_t)n * s->P.nv * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  pt_pattern64_kernel<<<n, kThreads, s->smem64, s->stream>>>(s->P, s->dLmVec, s->dLmY, nullptr, s->dLmChi);
+  P6_CUDA(cudaGetLastError());
+  s->launches++;
+  P6_CUDA(cudaMemcpyAsync(f, s->dLmChi, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+p6_status lm_cost(p6_pt_session *s, const double *x, double *f) { return lm_costs(s, x, 1, f); }
+
+// normal() at x: A (nv x nv), g (nv), f, left on the device in dLmOut and copied to the host.
+p6_status lm_normal(p6_pt_session *s, const double *x, double *A, double *g, double *f) {
+  const int nv = s->P.nv;
+  std::vector<double> vecs((size_t)(1 + 2 * nv) * nv);
+  std::copy(x, x + nv, vecs.begin());
+  LmCols L{};
+  int m = 1;
+  for (int j = 0; j < nv; ++j) {
+    const int fi = s->indexHost[j], kind = lm_kind(fi);
+    L.plus[j] = L.minus[j] = 0;
+    L.step[j] = 1;
+    if (kind == K_SCALE) { L.kind[j] = 0; continue; }
+    if (kind == K_BKG) { L.kind[j] = 1; L.bkg[j] = fi - PBKG0; continue; }
+    const double val = x[j], h = lm_fd_step(kind, val);
+    double llo, lhi;
+    lm_limits(kind, val, &llo, &lhi);
+    const bool plus = val + h <= lhi, minus = val - h >= llo;
+    const double vp = plus ? val + h : val, vm = minus ? val - h : val, d = vp - vm;
+    if (!(d != 0)) { L.kind[j] = 3; continue; }
+    L.kind[j] = 2;
+    L.step[j] = d;
+    if (plus) {
+      std::copy(x, x + nv, vecs.begin() + (size_t)m * nv);
+      vecs[(size_t)m * nv + j] = vp;
+      L.plus[j] = m++;
+    }
+    if (minus) {
+      std::copy(x, x + nv, vecs.begin() + (size_t)m * nv);
+      vecs[(size_t)m * nv + j] = vm;
+      L.minus[j] = m++;
+    }
+  }
+  p6_status st = lm_ensure(s, m);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaMemcpyAsync(s->dLmVec, vecs.data(), (size_t)m * nv * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  // vector 0 (with its unit-scale column), then the finite-difference probes
+  pt_pattern64_kernel<<<1, kThreads, s->smem64, s->stream>>>(s->P, s->dLmVec, s->dLmY, s->dLmYu, s->dLmChi);
+  P6_CUDA(cudaGetLastError());
+  if (m > 1) {
+    pt_pattern64_kernel<<<m - 1, kThreads, s->smem64, s->stream>>>(s->P, s->dLmVec + nv, s->dLmY + s->P.n, nullptr,
+                                                                    s->dLmChi + 1);
+    P6_CUDA(cudaGetLastError());
+  }
+  const int blocks = nv * (nv + 1) / 2 + nv + 1;
+  pt_normal_kernel<<<blocks, kThreads, 0, s->stream>>>(s->P, L, s->dLmY, s->dLmYu, s->dLmOut);
+  P6_CUDA(cudaGetLastError());
+  s->launches += m > 1 ? 3 : 2;
+  std::vector<double> h((size_t)nv * nv + nv + 1);
+  double chi0 = 0;
+  P6_CUDA(cudaMemcpyAsync(h.data(), s->dLmOut, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaMemcpyAsync(&chi0, s->dLmChi, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  if (!std::isfinite(chi0))
+    return set_error(P6_ERR_VALIDATION, "the model is not finite at the point of the normal equations");
+  std::copy(h.begin(), h.begin() + (size_t)nv * nv, A);
+  std::copy(h.begin() + (size_t)nv * nv, h.begin() + (size_t)nv * nv + nv, g);
+  *f = h[(size_t)nv * nv + nv];
+  return P6_OK;
+}
+
+// solveSPD of the free set on the device (A, g already in dLmOut).
+p6_status lm_solve(p6_pt_session *s, const int *F, int nF, double mu, int mode, double *d, bool *ok) {
+  const int nv = s->P.nv;
+  P6_CUDA(cudaMemcpyAsync(s->dLmF, F, nF * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+  double *out = s->dLmOut + nv * nv + nv + 1;
+  pt_lm_solve_kernel<<<1, 32, 0, s->stream>>>(s->dLmOut, s->dLmOut + nv * nv, nv, s->dLmF, nF, mu, mode, out);
+  P6_CUDA(cudaGetLastError());
+  s->launches++;
+  std::vector<double> h(nF + 1);
+  P6_CUDA(cudaMemcpyAsync(h.data(), out, (nF + 1) * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  *ok = h[nF] != 0;
+  std::copy(h.begin(), h.begin() + nF, d);
+  return P6_OK;
+}
+}  // namespace
+
+extern "C" p6_status p6_pt_normal(p6_pt_session *s, const double *x, double *A, double *g, double *f) {
+  clear_error();
+  if (!s || !x || !A || !g || !f) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaSetDevice(s->device));
+  return lm_normal(s, x, A, g, f);
+}
+
+extern "C" p6_status p6_pt_model_costs(p6_pt_session *s, const double *x, int n, double *chi2) {
+  clear_error();
+  if (!s || !x || !chi2 || n <= 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  P6_CUDA(cudaSetDevice(s->device));
+  return lm_costs(s, x, n, chi2);
+}
+
+extern "C" p6_status p6_pt_linear_start(p6_pt_session *s, double *x, double *chi2) {
+  clear_error();
+  if (!s || !x) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaSetDevice(s->device));
+  const int nv = s->P.nv;
+  std::vector<int> lin;
+  for (int j = 0; j < nv; ++j) {
+    const int k = lm_kind(s->indexHost[j]);
+    if (k == K_SCALE || k == K_BKG) lin.push_back(j);
+  }
+  std::vector<double> A((size_t)nv * nv), g(nv), d(nv + 1), xt(x, x + nv);
+  double f = 0;
+  p6_status st = lm_normal(s, x, A.data(), g.data(), &f);
+  if (st != P6_OK) return st;
+  if (!lin.empty()) {
+    bool ok = false;
+    st = lm_solve(s, lin.data(), (int)lin.size(), 0.0, 1, d.data(), &ok);
+    if (st != P6_OK) return st;
+    if (ok) {
+      for (size_t a = 0; a < lin.size(); ++a) {
+        const int q = lin[a];
+        xt[q] = std::min(s->hiHost[q], std::max(s->loHost[q], x[q] + d[a]));
+      }
+      double ft = 0;
+      st = lm_cost(s, xt.data(), &ft);
+      if (st != P6_OK) return st;
+      if (ft < f) {
+        std::copy(xt.begin(), xt.end(), x);
+        f = ft;
+      }
+    }
+  }
+  if (chi2) *chi2 = f;
+  return P6_OK;
+}
+
+extern "C" p6_status p6_pt_lm(p6_pt_session *s, double *x, int max_iter, double tol, double *out) {
+  clear_error();
+  if (!s || !x || max_iter < 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  P6_CUDA(cudaSetDevice(s->device));
+  const int nv = s->P.nv, nPts = s->P.n;
+  if (!(tol > 0)) tol = 1e-5;
+  std::vector<double> A((size_t)nv * nv), g(nv), dx(nv + 1), xn(nv), step(nv), sc(nv), cand(nv);
+  std::vector<int> F(nv);
+  double f = 0;
+  p6_status st = lm_cost(s, x, &f);
+  if (st != P6_OK) return st;
+  if (!std::isfinite(f)) return set_error(P6_ERR_VALIDATION, "the model gives non-finite values at the start values");
+  double mu = 1e-3, nu = 2, curViolation = lm_violation(s, x);
+  int conv = 0, it, code = 0, accepted = 0;
+  bool have = false;
+  for (it = 0; it < max_iter; ++it) {
+    if (!have) {
+      double fNE = 0;
+      st = lm_normal(s, x, A.data(), g.data(), &fNE);
+      if (st != P6_OK) return st;
+      have = true;
+    }
+    int nF = 0;
+    for (int j = 0; j < nv; ++j) {
+      const double lo = s->loHost[j], hi = s->hiHost[j];
+      const bool atLo = x[j] <= lo + 1e-12 * (1 + std::fabs(lo)), atHi = x[j] >= hi - 1e-12 * (1 + std::fabs(hi));
+      if (!((atLo && g[j] < 0) || (atHi && g[j] > 0)) && A[j * nv + j] > 0) F[nF++] = j;
+    }
+    if (!nF) { code = 5; break; }
+    double grad = 0;
+    const double noise = std::sqrt(std::max(f / std::max(1, nPts - nv), 1e-30));
+    for (int a = 0; a < nF; ++a) {
+      sc[a] = 1 / std::sqrt(A[F[a] * nv + F[a]]);
+      grad = std::max(grad, std::fabs(g[F[a]]) * sc[a] / noise);
+    }
+    if (f < 1e-24 || grad < 1e-4) { code = 2; break; }
+    bool ok = false;
+    st = lm_solve(s, F.data(), nF, mu, 0, dx.data(), &ok);
+    if (st != P6_OK) return st;
+    if (!ok) {
+      mu *= nu; nu *= 2;
+      if (mu > 1e30) { code = 3; break; }
+      continue;
+    }
+    std::copy(x, x + nv, xn.begin());
+    std::fill(step.begin(), step.end(), 0.0);
+    for (int a = 0; a < nF; ++a) {
+      const int q = F[a];
+      const double cap = lm_step_cap(lm_kind(s->indexHost[q]), x[q]);
+      const double sh = std::max(-cap, std::min(cap, dx[a]));
+      xn[q] = std::min(s->hiHost[q], std::max(s->loHost[q], x[q] + sh));
+      step[q] = xn[q] - x[q];
+    }
+    double violation = lm_violation(s, xn.data());
+    bool blocked = false;
+    if (curViolation == 0 && violation > 0) {
+      double loA = 0, hiA = 1;
+      for (int bi = 0; bi < 24; ++bi) {
+        const double mid = 0.5 * (loA + hiA);
+        for (int a = 0; a < nv; ++a) cand[a] = x[a] + mid * step[a];
+        if (lm_violation(s, cand.data()) == 0) loA = mid; else hiA = mid;
+      }
+      for (int a = 0; a < nv; ++a) { xn[a] = x[a] + loA * step[a]; step[a] = xn[a] - x[a]; }
+      violation = lm_violation(s, xn.data());
+      blocked = true;
+    }
+    double pred = 0, sAs = 0;
+    for (int a = 0; a < nv; ++a) {
+      if (!step[a]) continue;
+      pred += 2 * g[a] * step[a];
+      double tt = 0;
+      for (int b = 0; b < nv; ++b) tt += A[a * nv + b] * step[b];
+      sAs += step[a] * tt;
+    }
+    pred -= sAs;
+    double fn = 0;
+    st = lm_cost(s, xn.data(), &fn);
+    if (st != P6_OK) return st;
+    if (fn < f) {
+      const double rho = pred > 0 ? (f - fn) / pred : 0.5, rel = (f - fn) / f;
+      bool small = true;
+      const double s2 = std::max(f, 1e-30) / std::max(1, nPts - nv);
+      for (int a = 0; a < nF; ++a) {
+        const int q = F[a];
+        if (std::fabs(step[q]) * std::sqrt(A[q * nv + q] / s2) > 0.1) { small = false; break; }
+      }
+      std::copy(xn.begin(), xn.end(), x);
+      f = fn;
+      have = false;
+      curViolation = violation;
+      mu *= std::max(1.0 / 3, 1 - std::pow(2 * rho - 1, 3));
+      nu = 2;
+      ++accepted;
+      if (!blocked && rel < tol && small) {
+        if (++conv >= 2) { code = 1; ++it; break; }
+      } else {
+        conv = 0;
+      }
+    } else {
+      mu *= nu; nu *= 2;
+      if (mu > 1e20) { code = blocked ? 6 : (grad < 1e-3 ? 2 : 4); break; }
+    }
+  }
+  if (out) { out[0] = f; out[1] = it; out[2] = accepted; out[3] = code; }
+  return P6_OK;
+}
 
 // ===========================================================================
 // p6_pt_costs_static: the cost kernel on a file-scope scratch array, so the

@@ -260,6 +260,39 @@ class PTSession:
     def synchronize(self, timeout: float = 60.0):
         check(self.lib.p6_pt_synchronize(self.h, float(timeout)))
 
+    # --- least-squares finish (FP64 on the device)
+    def model_costs(self, vectors) -> np.ndarray:
+        """chi^2 of each refined vector with the FP64 model (one launch)."""
+        v = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(-1, self.plan.nv))
+        out = np.zeros(len(v))
+        check(self.lib.p6_pt_model_costs(self.h, v.ctypes.data, len(v), out.ctypes.data))
+        return out
+
+    def model_cost(self, x) -> float:
+        return float(self.model_costs([x])[0])
+
+    def normal(self, x):
+        """(A = J'WJ, g = J'W r, f = chi^2) at x, FP64 on the device."""
+        nv = self.plan.nv
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        A = np.zeros((nv, nv))
+        g = np.zeros(nv)
+        f = C.c_double()
+        check(self.lib.p6_pt_normal(self.h, x.ctypes.data, A.ctypes.data, g.ctypes.data, C.byref(f)))
+        return A, g, f.value
+
+    def linear_start(self, x):
+        x = np.ascontiguousarray(np.array(x, dtype=np.float64))
+        f = C.c_double()
+        check(self.lib.p6_pt_linear_start(self.h, x.ctypes.data, C.byref(f)))
+        return x, f.value
+
+    def lm(self, x, max_iter: int = 20, tol: float = 1e-5):
+        x = np.ascontiguousarray(np.array(x, dtype=np.float64))
+        out = np.zeros(4)
+        check(self.lib.p6_pt_lm(self.h, x.ctypes.data, int(max_iter), float(tol), out.ctypes.data))
+        return x, {'chi2': out[0], 'iterations': int(out[1]), 'accepted': int(out[2]), 'code': int(out[3])}
+
     def last_batch_ms(self) -> float:
         v = C.c_float()
         check(self.lib.p6_pt_last_batch_ms(self.h, C.byref(v)))
@@ -285,19 +318,25 @@ def _reflected(value, lo, hi):
     return 2 * lo - value if value < lo else (2 * hi - value if value > hi else value)
 
 
-def run(ctx: PTContext, device: int = 0) -> dict:
-    """RVPTGPU.run (js/pt_gpu.js:409-423)."""
+def run(ctx: PTContext, device: int = 0, session: Optional[PTSession] = None) -> dict:
+    """RVPTGPU.run (js/pt_gpu.js:409-423).
+
+    ``ctx.cost`` re-scores the probes and each new per-chain best, as the
+    reference does with its CPU model; when it is None, the session's FP64
+    device model does both, with all the new bests of a batch in one launch.
+    ``session`` reuses an open session (it is left open)."""
     P = ctx.problem
-    gpu = create(ctx, device)
+    gpu = session or create(ctx, device)
     try:
         x0 = np.asarray(ctx.x, dtype=np.float64)
         scales = np.asarray(ctx.setup['scales'], dtype=np.float64)
         probes = [x0, np.array([_reflected(v + s * 0.25, lo, hi) for v, s, lo, hi in zip(x0, scales, P.lo, P.hi)])]
         chains = int(ctx.setup['chains'])
         gc = gpu.costs([probes[c % 2] for c in range(chains)])
+        ref = [ctx.cost(probes[0]), ctx.cost(probes[1])] if ctx.cost else list(gpu.model_costs(probes))
         validation = 0.0
         for c in range(chains):
-            cpu = ctx.cost(probes[c % 2]) if ctx.cost else float('nan')
+            cpu = ref[c % 2]
             if not math.isfinite(cpu):
                 continue
             err = abs(gc[c] - cpu) / max(1.0, cpu)
@@ -307,7 +346,7 @@ def run(ctx: PTContext, device: int = 0) -> dict:
         gpu.initial([x0])
         gpu.batch(1, True)
         best = x0.copy()
-        best_cost = float(ctx.setup.get('initialCost', ctx.cost(x0) if ctx.cost else gc[0]))
+        best_cost = float(ctx.setup.get('initialCost', ref[0]))
         seen = set()
         sweeps = int(ctx.setup['sweeps'])
         count = max(1, math.ceil(8 / len(x0)))
@@ -321,6 +360,7 @@ def run(ctx: PTContext, device: int = 0) -> dict:
             gpu.launch(n)
             completed += n
             _, bests, costs, _ = gpu.exact_state()
+            fresh = []
             for c in range(chains):
                 cand = bests[c]
                 key = cand.tobytes()
@@ -331,9 +371,12 @@ def run(ctx: PTContext, device: int = 0) -> dict:
                     continue
                 if ctx.feasible and not ctx.feasible(cand):
                     continue
-                value = ctx.cost(cand) if ctx.cost else costs[c, 1]
-                if value < best_cost:
-                    best, best_cost = cand.copy(), value
+                fresh.append(cand)
+            if fresh:
+                values = [ctx.cost(c) for c in fresh] if ctx.cost else gpu.model_costs(fresh)
+                for cand, value in zip(fresh, values):
+                    if value < best_cost:
+                        best, best_cost = cand.copy(), float(value)
             if ctx.on_iter:
                 ctx.on_iter({'it': completed, 'chi2': best_cost, 'maxIter': ctx.max_iter, 'stage': 'pt',
                              'backend': 'cuda'})
@@ -346,7 +389,58 @@ def run(ctx: PTContext, device: int = 0) -> dict:
         pt.update(stats)
         return {'x': best, 'stopped': stopped, 'pt': pt}
     finally:
-        gpu.close()
+        if session is None:
+            gpu.close()
+
+
+def rwp(problem: PTProblem, chi2: float) -> float:
+    """Rwp = sqrt(chi^2 / sum w y^2) over the points with w > 0 (js/rietveld_core.js:1578-1608)."""
+    m = problem.w > 0
+    return float(np.sqrt(chi2 / np.sum(problem.w[m] * problem.y[m] ** 2)))
+
+
+def refine(ctx: PTContext, device: int = 0, max_iter: int = 20, tol: float = 1e-5,
+           target_chi2: Optional[float] = None) -> dict:
+    """refine() with algorithm 'pt' (js/rietveld_core.js:2242-2300) on the device:
+    one Gauss-Newton step on the scale and background, tempering from there
+    (``run``), the tempering's best kept if it is no worse than the start,
+    then the least-squares finish.  Returns x, chi2, Rwp, the PT record, the
+    LM record, the wall time at the end of each stage and, with
+    ``target_chi2``, the wall time at which the best chi^2 so far first
+    reached it (checked after the linear start, after every batch of sweeps
+    and after the finish)."""
+    import time
+    t0 = time.perf_counter()
+    hit = {'t': None}
+
+    def note(chi2):
+        if target_chi2 is not None and hit['t'] is None and chi2 <= target_chi2:
+            hit['t'] = time.perf_counter() - t0
+
+    with PTSession(ctx, device) as gpu:
+        x, f = gpu.linear_start(ctx.x)
+        note(f)
+        t_lin = time.perf_counter() - t0
+        user_iter = ctx.on_iter
+
+        def on_iter(p):
+            note(p['chi2'])
+            if user_iter:
+                user_iter(p)
+        setup = dict(ctx.setup)
+        setup['initialCost'] = f
+        sub = PTContext(ctx.problem, x, setup, cost=ctx.cost, feasible=ctx.feasible, should_stop=ctx.should_stop,
+                        on_iter=on_iter, max_iter=ctx.max_iter)
+        r = run(sub, device, session=gpu)
+        t_pt = time.perf_counter() - t0
+        if r['pt']['bestChi2'] <= f:
+            x = r['x']
+        xf, lm = gpu.lm(x, max_iter, tol)
+        note(lm['chi2'])
+        t_lm = time.perf_counter() - t0
+    return {'x': xf, 'chi2': lm['chi2'], 'rwp': rwp(ctx.problem, lm['chi2']), 'pt': r['pt'], 'lm': lm,
+            'stopped': r['stopped'], 'seconds': {'linear': t_lin, 'pt': t_pt, 'lm': t_lm},
+            'time_to_target': hit['t']}
 
 
 # ---------------------------------------------------------------------------

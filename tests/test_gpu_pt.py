@@ -124,3 +124,64 @@ def test_run_rejects_a_disagreeing_cost(nacl):
     ctx = ctx_of(P, x0, chains=4, sweeps=2, cost=lambda x: 1.01 * M.cost(x))
     with pytest.raises(RuntimeError, match='disagrees'):
         run(ctx)
+
+
+def near_truth(truth):
+    x0 = truth.copy()
+    x0[1] *= 1.001
+    x0[3] *= 1.2
+    return x0
+
+
+def test_fp64_model_and_normal_equations_match_oracle(nacl):
+    """FP64 model cost, A = J'WJ, g = J'W r and f against the oracle.  A and g
+    are compared on their natural scales sqrt(A_ii A_jj) and sqrt(A_ii f)."""
+    P, M, truth = nacl
+    x = near_truth(truth)
+    with PTSession(ctx_of(P, truth, chains=2)) as s:
+        c = s.model_costs([x, truth])
+        A, g, f = s.normal(x)
+    assert abs(c[0] - M.cost(x)) <= 1e-10 * c[0]
+    assert abs(c[1] - M.cost(truth)) <= 1e-10 * c[1]
+    Ao, go, fo = M.normal(x)
+    assert abs(f - fo) <= 1e-10 * fo
+    d = np.sqrt(np.diag(Ao))
+    assert np.max(np.abs(A - Ao) / np.outer(d, d)) < 1e-7
+    assert np.max(np.abs(g - go) / (d * math.sqrt(fo))) < 1e-7
+
+
+def test_linear_start_matches_oracle(nacl):
+    P, M, truth = nacl
+    x0 = truth.copy()
+    x0[0] *= 1.3
+    with PTSession(ctx_of(P, truth, chains=2)) as s:
+        xg, fg = s.linear_start(x0)
+    xo, fo = M.linear_start(x0)
+    assert np.allclose(xg, xo, rtol=1e-9, atol=0)
+    assert abs(fg - fo) <= 1e-9 * fo
+
+
+def test_lm_finish_matches_oracle(nacl):
+    P, M, truth = nacl
+    x0 = near_truth(truth)
+    with PTSession(ctx_of(P, truth, chains=2)) as s:
+        xg, ig = s.lm(x0, 30)
+    xo, io = M.lm(x0, 30)
+    assert ig['code'] == io['code'] and ig['accepted'] == io['accepted']
+    assert abs(ig['chi2'] - io['chi2']) <= 1e-9 * io['chi2']
+    assert np.allclose(xg, xo, rtol=1e-7, atol=1e-9)
+
+
+def test_refine_reaches_the_target_rwp(nacl):
+    """Linear start, tempering and the least-squares finish on the device from a
+    +/-5 % start reach Rwp <= 1.05 x the Rwp of the finish started at the truth."""
+    from powder6_b200.pt_gpu import refine, rwp
+    P, M, truth = nacl
+    _, ref = M.lm(truth, 30)
+    target = 1.05 * rwp(P, ref['chi2'])
+    x0 = start_vectors(P, truth, 1, seed=8)[0]
+    ctx = ctx_of(P, x0, chains=64, sweeps=300)
+    r = refine(ctx, target_chi2=target ** 2 * float(np.sum(P.w * P.y ** 2)))
+    assert r['rwp'] <= target
+    assert r['time_to_target'] is not None and r['time_to_target'] <= r['seconds']['lm']
+    assert abs(M.cost(r['x']) - r['chi2']) <= 1e-9 * r['chi2']
