@@ -50,6 +50,10 @@ def parse():
     ap.add_argument('--generations', type=int, default=GENERATIONS)
     ap.add_argument('--cos-mode', type=int, default=0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt'],
+                    help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit')
+    ap.add_argument('--chains', type=int, default=64)
+    ap.add_argument('--sweeps', type=int, default=2000)
     return ap.parse_args()
 
 
@@ -208,11 +212,166 @@ def run_reference(args, world, rank):
     }), flush=True)
 
 
+PT_WORKLOAD = ('pt-rietveld NaCl Fm-3m a=5.640 (Na 4a, Cl 4b, Biso 1.0), Cu Ka1/Ka2 1.5406/1.5444 ratio 0.5, '
+               '2theta 10-120 step 0.02 (5501 points), TCH U,V,W,X,Y = 0.004,-0.002,0.003,0.02,0.01 (FullProf '
+               'units, converted), 6-term Chebyshev, Poisson counts peak ~1e4; refined scale, a, Biso, U, V, W, zero '
+               'from +/-5 % starts')
+
+
+def pt_setup(seed):
+    from oracle import oracle as O
+    from powder6_b200.pt_gpu import nacl_problem, start_vectors, synthesise
+    P = nacl_problem(seed=1)
+    truth = synthesise(P, O.PtModel(P).pattern, seed=1)
+    x0 = start_vectors(P, truth, 1, seed=seed)[0]
+    return P, truth, x0
+
+
+def pt_target(P, truth):
+    """Target: 1.05 x the Rwp the least-squares finish converges to from the truth (FP64 oracle)."""
+    from oracle import oracle as O
+    from powder6_b200.pt_gpu import reflection_dmin, rwp
+    _, ref = O.PtModel(P, dmin=reflection_dmin(P)).lm(truth, 30)
+    target_rwp = 1.05 * rwp(P, ref['chi2'])
+    return target_rwp, target_rwp ** 2 * float(np.sum(P.w * P.y ** 2))
+
+
+def run_reference_pt(args, world, rank):
+    """The CPU tempering (temper at 16 chains, the reference's cap) of the FP64 oracle port on one host thread."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from powder6_b200.pt_gpu import pt_scales, reflection_dmin
+    P, truth, x0 = pt_setup(5)
+    M = O.PtModel(P, dmin=reflection_dmin(P))
+    sc = pt_scales(P, x0)
+    chains, per_step = 16, 2
+
+    def step(seed):
+        _, st = M.temper(x0, sc, chains=chains, sweeps=per_step, seed=seed)
+        return st['proposals']
+    for i in range(args.warmup):
+        step(100 + i)
+    t0 = time.perf_counter()
+    trials = sum(step(200 + i) for i in range(args.steps))
+    dt = time.perf_counter() - t0
+    v = trials / dt
+    sample = (f'{chains} chains x {per_step} sweeps x {len(x0)} proposals per step (FP64 oracle port of temper, '
+              f'one host thread)')
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'trial structures evaluated/s', 'value': v, 'unit': 'trials/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000 * dt / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': PT_WORKLOAD + ' (sampled)'},
+        'cpu_baseline': {'value': v, 'unit': 'trials/s', 'cores': 1, 'kind': 'port', 'sample': sample},
+        'e2e': {'value': v, 'unit': 'trials/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+
+
+def pt_cpu_baseline(P, x0, seconds=10.0):
+    from oracle import oracle as O
+    from powder6_b200.pt_gpu import pt_scales, reflection_dmin
+    M = O.PtModel(P, dmin=reflection_dmin(P))
+    sc = pt_scales(P, x0)
+    t0 = time.perf_counter()
+    trials, runs = 0, 0
+    while time.perf_counter() - t0 < seconds:
+        _, st = M.temper(x0, sc, chains=16, sweeps=2, seed=300 + runs)
+        trials += st['proposals']
+        runs += 1
+    dt = time.perf_counter() - t0
+    return {'value': trials / dt, 'unit': 'trials/s', 'cores': 1, 'kind': 'port',
+            'sample': f'{runs} runs of 16 chains x 2 sweeps x {len(x0)} proposals ({int(trials)} trials, {dt:.1f} s, '
+                      f'FP64 oracle port of temper, one host thread)'}
+
+
+def main_pt(args, world, rank, local):
+    """One step = one tempering run of the NaCl fit: args.sweeps sweeps of
+    args.chains chains from a +/-5 % start.  value: proposals per second of
+    the sweeps (CUDA events around one batch of all the sweeps, state
+    resident); e2e: proposals per second of refine() through the public API
+    (linear start, the same sweeps with the reference's batching and FP64
+    re-scores, least-squares finish; host start vector in, result out);
+    time_to_target_rwp: wall seconds from the start of refine() to a best
+    Rwp <= 1.05 x the converged Rwp, median over the steps."""
+    import torch
+    from powder6_b200.pt_gpu import PTContext, PTSession, pt_scales, refine
+    torch.cuda.set_device(local)
+    P, truth, _ = pt_setup(5)
+    target_rwp, target_chi2 = pt_target(P, truth)
+    starts = [pt_setup(10 + i + 100 * rank)[2] for i in range(args.warmup + args.steps)]
+
+    def ctx_for(x0, seed):
+        return PTContext(P, x0, {'chains': args.chains, 'sweeps': args.sweeps, 'maxTemp': 100.0, 'seed': seed,
+                                 'scales': pt_scales(P, x0)})
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    dev_ms, launches = [], 0
+    with PTSession(ctx_for(starts[0], 1), local) as s:
+        for i, x0 in enumerate(starts):
+            s.initial([x0])
+            s.batch(1, True)
+            flush.zero_()
+            torch.cuda.synchronize()
+            l0 = s.launch_count()
+            s.launch(args.sweeps)
+            s.synchronize(600)
+            if i >= args.warmup:
+                dev_ms.append(s.last_batch_ms())
+                launches += s.launch_count() - l0
+    barrier(world)
+    trials = args.chains * args.sweeps * len(starts[0])
+    total_ms = max_over_ranks(float(sum(dev_ms)), world)
+    value = world * trials * args.steps / (total_ms / 1000.0)
+    e2e_s, ttt, rwps = [], [], []
+    with ClockSampler(local) as clk:
+        for i, x0 in enumerate(starts):
+            t0 = time.perf_counter()
+            r = refine(ctx_for(x0, 7 + i), local, target_chi2=target_chi2)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                e2e_s.append(dt)
+                ttt.append(r['time_to_target'])
+                rwps.append(r['rwp'])
+    e2e_total = max_over_ranks(float(sum(e2e_s)), world)
+    e2e_value = world * trials * args.steps / e2e_total
+    if rank == 0:
+        clocks = clk.summary()
+        ms = float(np.mean(dev_ms))
+        reached = [t for t in ttt if t is not None]
+        line = {
+            'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp32 profile, fp64 peaks and chi2', 'data': 'synthetic',
+            'config': {'workload': PT_WORKLOAD, 'chains': args.chains, 'sweeps': args.sweeps,
+                       'step': 'one tempering run (all sweeps) for value; one refine() for e2e',
+                       'l2': 'flushed before every step (256 MB write)', 'parallelism': f'replicas only x{world}'},
+            'time_to_target_rwp': {'median_s': float(np.median(reached)) if reached else None,
+                                   'reached': f'{len(reached)}/{len(ttt)}', 'target_rwp': target_rwp,
+                                   'final_rwp_median': float(np.median(rwps))},
+            'e2e': {'value': e2e_value, 'unit': 'trials/s', 'h2d_bytes_per_step': len(starts[0]) * 8,
+                    'd2h_bytes_per_step': len(starts[0]) * 8},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line['cpu_baseline'] = pt_cpu_baseline(P, starts[0])
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == 'reference':
-        run_reference(args, world, rank)
+        if args.workload == 'pt':
+            run_reference_pt(args, world, rank)
+        else:
+            run_reference(args, world, rank)
+        return
+    if args.workload == 'pt':
+        main_pt(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     import torch
     from powder6_b200.swarm_wyckoff import (WyckoffSession, build_ladders, initial_state, project_all,
