@@ -50,8 +50,11 @@ def parse():
     ap.add_argument('--generations', type=int, default=GENERATIONS)
     ap.add_argument('--cos-mode', type=int, default=0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt'],
-                    help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit')
+    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt', 'contract'],
+                    help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit; '
+                         'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000)')
+    ap.add_argument('--method', default='split', choices=['split', 'fp32'],
+                    help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
     ap.add_argument('--chains', type=int, default=64)
     ap.add_argument('--sweeps', type=int, default=2000)
     return ap.parse_args()
@@ -358,17 +361,152 @@ def main_pt(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+CT_WORKLOAD = ('fixed-profile contraction Y = I . P: 16384 replicas x 3000 reflections (lognormal sigma 1.5) x 12000 '
+               'points (2theta 5-125 step 0.01), pseudo-Voigt columns FWHM U(0.05, 0.3) deg truncated at +/-20 FWHM, '
+               'per-replica weighted chi^2 against a Poisson observed pattern')
+
+
+def ct_cpu_rows(p, seconds):
+    """FP64 oracle product on a sample of replica rows, host BLAS threads."""
+    from oracle import oracle as O
+    rows = 256
+    t0 = time.perf_counter()
+    done = 0
+    while time.perf_counter() - t0 < seconds:
+        lo = (done * rows) % (len(p.intensities) - rows)
+        O.contract_fp64(p.intensities[lo:lo + rows], p.profile_t, p.yobs, p.w)
+        done += rows
+    dt = time.perf_counter() - t0
+    return done, dt
+
+
+def run_reference_ct(args, world, rank):
+    if rank != 0:
+        return
+    from powder6_b200.contraction import banded_problem
+    p = banded_problem(seed=1)
+    for _ in range(args.warmup):
+        ct_cpu_rows(p, 0.5)
+    trials, dt = ct_cpu_rows(p, 2.0 * args.steps)
+    v = trials / dt
+    cores = os.cpu_count()
+    sample = f'{trials} replicas in blocks of 256 rows (FP64 product over the full profile matrix, host BLAS)'
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'trial structures evaluated/s', 'value': v, 'unit': 'trials/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000 * dt / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': CT_WORKLOAD + ' (sampled rows)'},
+        'cpu_baseline': {'value': v, 'unit': 'trials/s', 'cores': cores, 'kind': 'port', 'sample': sample},
+        'e2e': {'value': v, 'unit': 'trials/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+
+
+def main_ct(args, world, rank, local):
+    """One step = one evaluation of all 16384 replicas: split of I into bf16
+    parts, the banded product, FP64 chi^2 per replica.  value: replicas per
+    second from CUDA events, I resident (196 MB, larger than L2); e2e: the
+    same through p6_ct_run_host from pinned host memory (I in, chi^2 out)."""
+    import torch
+    from powder6_b200.contraction import FP32, SPLIT_BF16, ContractionSession, banded_problem
+    torch.cuda.set_device(local)
+    p = banded_problem(seed=1 + rank)
+    method = SPLIT_BF16 if args.method == 'split' else FP32
+    M, K = p.intensities.shape
+    N = p.profile_t.shape[0]
+    pinned = torch.empty((M, K), dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[:] = p.intensities
+    host = pinned.numpy()
+    with ContractionSession(p, device=local) as s:
+        s.set_intensities(host)
+        q = s.query()
+        for _ in range(args.warmup):
+            s.evaluate(method)
+            s.synchronize()
+        barrier(world)
+        l0 = s.query()['launches']
+        times = []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                s.evaluate(method)
+                s.synchronize()
+                times.append(s.last_ms())
+        launches = s.query()['launches'] - l0
+        total_ms = max_over_ranks(float(sum(times)), world)
+        value = world * M * args.steps / (total_ms / 1000.0)
+        e2e = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            s.run_host(host, method)
+            e2e.append(time.perf_counter() - t0)
+        e2e_total = max_over_ranks(float(sum(e2e)), world)
+        e2e_value = world * M * args.steps / e2e_total
+    if rank == 0:
+        clocks = clk.summary()
+        ms = float(np.mean(times))
+        n_mt = (M + 127) // 128
+        if method == SPLIT_BF16:
+            flops = 3 * 2.0 * 128 * 256 * 64 * q['band_kblocks'] * n_mt
+            note = 'executed tcgen05 MMA flops (3 bf16 products per K step over each tile band)'
+            peak = measured_peak('bf16_tflops')
+        else:
+            flops = 2.0 * 128 * 128 * q['band_cols128'] * n_mt
+            note = 'executed FP32 FMA flops over each tile band'
+            peak = (None, None)
+        useful = 2.0 * M * float(np.count_nonzero(p.profile_t))
+        achieved = flops / (ms / 1000.0) / 1e12
+        line = {
+            'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'bf16x3 split, fp32 accumulate, fp64 chi2' if method == SPLIT_BF16 else 'fp32, fp64 chi2',
+            'data': 'synthetic',
+            'config': {'workload': CT_WORKLOAD, 'method': args.method, 'replicas': M, 'reflections': K, 'points': N,
+                       'l2': 'inputs larger than L2 (I is 196 MB)', 'parallelism': f'replicas only x{world}'},
+            'roofline': {'bound': 'tensor' if method == SPLIT_BF16 else 'fp32', 'achieved': achieved,
+                         'peak': peak[0], 'unit': 'TFLOP/s',
+                         'frac': achieved / peak[0] if peak[0] else None, 'traffic': None,
+                         'note': f'{note}: {flops:.4g} per launch; useful banded flops {useful:.4g}; '
+                                 f'dense-equivalent {2.0 * M * K * N:.4g}; peak {peak[1]}'},
+            'e2e': {'value': e2e_value, 'unit': 'trials/s', 'h2d_bytes_per_step': M * K * 4,
+                    'd2h_bytes_per_step': M * 8},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            trials, dt = ct_cpu_rows(p, 10.0)
+            line['cpu_baseline'] = {'value': trials / dt, 'unit': 'trials/s', 'cores': os.cpu_count(),
+                                    'kind': 'port',
+                                    'sample': f'{trials} replicas in blocks of 256 rows, FP64 product with the full '
+                                              f'profile matrix (host BLAS), {dt:.1f} s'}
+        print(json.dumps(line), flush=True)
+
+
+def measured_peak(key):
+    f = ROOT / 'MEASURED_PEAKS.json'
+    if f.exists():
+        try:
+            v = json.loads(f.read_text()).get(key)
+            if v:
+                return float(v), 'of measured (MEASURED_PEAKS.json ' + key + ')'
+        except (ValueError, OSError):
+            pass
+    fallback = {'bf16_tflops': 1590.0, 'hbm_gbs': 6650.0}
+    return fallback.get(key), 'of fallback'
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == 'reference':
         if args.workload == 'pt':
             run_reference_pt(args, world, rank)
+        elif args.workload == 'contract':
+            run_reference_ct(args, world, rank)
         else:
             run_reference(args, world, rank)
         return
-    if args.workload == 'pt':
-        main_pt(args, world, rank, local)
+    if args.workload in ('pt', 'contract'):
+        (main_pt if args.workload == 'pt' else main_ct)(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

@@ -301,6 +301,53 @@ p6_status p6_pt_lm(p6_pt_session *s, double *x, int max_iter, double tol, double
 #define P6_PT_STATIC_SCRATCH_BYTES (4u << 20)
 p6_status p6_pt_costs_static(p6_pt_session *s, const double *vectors, int n_vectors, double *costs, float *ycalc);
 
+/* ======================================================================== */
+/* Profile contraction with the cell and profile fixed                       */
+/* ======================================================================== */
+
+/* With the cell and profile fixed, the calculated patterns of all replicas
+ * are Y = I . P: intensities I (replicas x reflections, the per-reflection
+ * heights mult Lp |F|^2 / area each replica's structure gives, as
+ * js/rietveld_core.js:881-886 forms them) times the banded profile matrix P
+ * (reflections x points, the unit-height Ka1 + Ka2 columns of
+ * js/profile.js:1013-1090).  The reference renders every trial pattern peak
+ * by peak; here the product runs on the tensor cores (split-BF16, FP32
+ * accumulation) or on the CUDA cores in FP32, and the weighted chi^2 of each
+ * replica against the observed pattern is reduced in FP64. */
+typedef struct {
+  int n_refl;              /* K: reflections, sorted by 2-theta */
+  int n_points;            /* N: pattern points */
+  int max_replicas;        /* M capacity */
+  const float *profile_t;  /* P transposed: n_points x n_refl, row j = the profile values at point j */
+  const float *yobs;       /* n_points observed counts */
+  const float *w;          /* n_points weights (w <= 0 excludes a point) */
+} p6_ct_problem;
+
+enum { P6_CT_SPLIT_BF16 = 0, P6_CT_FP32 = 1 };
+
+typedef struct p6_ct_session p6_ct_session;
+
+p6_status p6_ct_create(const p6_ct_problem *problem, int device, p6_ct_session **out);
+p6_status p6_ct_destroy(p6_ct_session *s);
+/* Uploads I (n_replicas x n_refl, row-major, host memory). */
+p6_status p6_ct_set_intensities(p6_ct_session *s, const float *intensities, int n_replicas);
+/* Asynchronous: Y = I . P with `method` and chi^2 per replica; store_pattern
+ * != 0 also keeps Y (n_replicas x n_points) on the device. */
+p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern);
+/* Waits, then copies chi^2 (n_replicas doubles) and, if stored and
+ * requested, Y.  Either pointer may be NULL. */
+p6_status p6_ct_read(p6_ct_session *s, double *chi2, float *pattern);
+/* Upload, evaluate, read chi^2: the end-to-end call. */
+p6_status p6_ct_run_host(p6_ct_session *s, const float *intensities, int n_replicas, int method, double *chi2);
+p6_status p6_ct_synchronize(p6_ct_session *s);
+/* Device time of the last p6_ct_evaluate. */
+p6_status p6_ct_last_ms(p6_ct_session *s, float *ms);
+/* Band statistics: K-blocks (64 reflections) summed over the 256-point tiles
+ * the tensor-core path runs, reflections summed over the 128-point tiles of
+ * the FP32 path, the number of 256-point tiles, kernels launched. */
+p6_status p6_ct_query(p6_ct_session *s, long long *band_kblocks, long long *band_cols128, int *n_tiles,
+                      long long *launches);
+
 /* Philox4x32-10 of one (counter, key) on the device: known-answer check. */
 p6_status p6_philox_device(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

@@ -378,3 +378,19 @@ class PtModel:
         w, y = self.prob.w, self.prob.y
         m = w > 0
         return float(np.sqrt(chi2 / np.sum(w[m] * y[m] ** 2)))
+
+
+def contract_fp64(intensities, profile_t, yobs, w):
+    """FP64 restatement of the fixed-profile pattern and its chi^2: y_calc =
+    sum_k height_k col_k (evalPhase/render, js/rietveld_core.js:855-917) with
+    the heights as the rows of ``intensities`` and the columns of the profile
+    matrix (``profile_t`` is its transpose, points x reflections), and
+    chi^2 = sum over w > 0 of w (y - y_calc)^2 (js/rietveld_core.js:1878-1889).
+    Returns (Y, chi2)."""
+    I = np.asarray(intensities, dtype=np.float64)
+    Y = I @ np.asarray(profile_t, dtype=np.float64).T
+    w = np.asarray(w, dtype=np.float64)
+    m = w > 0
+    r = np.asarray(yobs, dtype=np.float64)[None, :] - Y
+    chi2 = (w[None, m] * r[:, m] ** 2).sum(axis=1)
+    return Y, chi2

@@ -64,6 +64,11 @@ class P6PtProblem(C.Structure):
 
 
 _P = C.c_void_p
+class P6CtProblem(C.Structure):
+    _fields_ = [('n_refl', C.c_int), ('n_points', C.c_int), ('max_replicas', C.c_int),
+                ('profile_t', C.c_void_p), ('yobs', C.c_void_p), ('w', C.c_void_p)]
+
+
 _SIGS = {
     'p6_last_error': (C.c_char_p, []),
     'p6_abi_version': (C.c_int, []),
@@ -105,6 +110,16 @@ _SIGS = {
     'p6_pt_normal': (C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double)]),
     'p6_pt_linear_start': (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
     'p6_pt_lm': (C.c_int, [_P, _P, C.c_int, C.c_double, _P]),
+    'p6_ct_create': (C.c_int, [C.POINTER(P6CtProblem), C.c_int, C.POINTER(C.c_void_p)]),
+    'p6_ct_destroy': (C.c_int, [_P]),
+    'p6_ct_set_intensities': (C.c_int, [_P, _P, C.c_int]),
+    'p6_ct_evaluate': (C.c_int, [_P, C.c_int, C.c_int]),
+    'p6_ct_read': (C.c_int, [_P, _P, _P]),
+    'p6_ct_run_host': (C.c_int, [_P, _P, C.c_int, C.c_int, _P]),
+    'p6_ct_synchronize': (C.c_int, [_P]),
+    'p6_ct_last_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
+    'p6_ct_query': (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                              C.POINTER(C.c_longlong)]),
 }
 
 _lib = None

@@ -1,0 +1,650 @@
+// Profile contraction Y = I . P with the cell and profile fixed.
+//
+// When a Wyckoff search holds the cell and the profile fixed, the calculated
+// pattern of every replica is the product of its reflection intensities I
+// (replicas x reflections) and one banded profile matrix P (reflections x
+// points): column j of P is nonzero only for the reflections whose window
+// covers point j, and with the reflections sorted by 2-theta the nonzero
+// rows of a run of columns form one contiguous range.
+//
+// The split-BF16 path runs on the 5th-generation tensor cores:
+//  * I = I_hi + I_lo and P = P_hi + P_lo with bf16 parts (I_hi = bf16(I),
+//    I_lo = bf16(I - I_hi)); Y = I_hi P_hi + I_hi P_lo + I_lo P_hi with FP32
+//    accumulation (the dropped I_lo P_lo term is ~2^-16 relative);
+//  * one CTA per 128 x 256 output tile; its K loop covers only the K-blocks
+//    (64 reflections) the tile's band touches;
+//  * warp 0 issues TMA loads (128B-swizzled, K-major tiles of the four bf16
+//    operands) into a two-stage shared-memory ring; warp 1 issues
+//    tcgen05.mma (M 128, N 256, K 16) into a TMEM accumulator and commits
+//    each stage back to the producer; warps 2-5 read the accumulator with
+//    tcgen05.ld and reduce the weighted residual against the observed
+//    pattern in FP64 (the only FP64 on this path), optionally storing Y;
+//  * per-tile chi^2 partials are summed per replica in a fixed order.
+// A plain FP32 CUDA-core kernel over the same bands is the comparison
+// method.  Every device wait is bounded; a wait that runs out records an
+// error the host reports as P6_ERR_TIMEOUT.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "p6_common.cuh"
+
+namespace p6 {
+namespace ct {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+constexpr int A_TILE = BM * BK * 2;                       // 16 KB per bf16 operand tile
+constexpr int B_TILE = BN * BK * 2;                       // 32 KB
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;      // 96 KB: A_hi, A_lo, B_hi, B_lo
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack (1024-B swizzle atoms)
+constexpr int kThreads = 192;                             // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t TMEM_COLS = 256;
+constexpr unsigned long long kWaitNs = 2000000000ull;     // 2 s per wait
+
+// SIMT comparison kernel tiles
+constexpr int FM = 128, FN = 128, FK = 16;
+
+enum CtError : int { CT_OK = 0, CT_WAIT_FULL = 11, CT_WAIT_EMPTY = 12, CT_WAIT_ACC = 13, CT_WAIT_DRAIN = 14 };
+
+struct Params {
+  int M, N, Kp, nTilesN;
+  const int2 *kRange;     // per BN tile: K-blocks [x, y)
+  const float *yobs, *w;  // N
+  float *Y;               // optional, M x N
+  double *chiPart;        // M x nTilesN
+  int *errFlag;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for phase `parity` of `bar` for at most kWaitNs.
+__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > kWaitNs) return false;
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major, 128B-swizzled bf16 tile:
+// 8-row x 128-byte swizzle atoms stacked every 1024 bytes (SBO), LBO unused (1),
+// descriptor version 1, layout SWIZZLE_128B (2).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator, bf16 A and B, both
+// K-major, N = BN, M = BM.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 32 columns of FP32 from TMEM: thread t gets row t of its warp's lane quarter.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    contract_tc_kernel(const __grid_constant__ CUtensorMap tmAhi, const __grid_constant__ CUtensorMap tmAlo,
+                       const __grid_constant__ CUtensorMap tmBhi, const __grid_constant__ CUtensorMap tmBlo,
+                       const Params P) {
+  extern __shared__ unsigned char smemRaw[];
+  __shared__ __align__(8) uint64_t fullBar[STAGES], emptyBar[STAGES], accBar;
+  __shared__ uint32_t tmemBase;
+  unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nt = blockIdx.x, mt = blockIdx.y;
+  const int2 kr = P.kRange[nt];
+  const int nkb = kr.y - kr.x;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&fullBar[s], 1);
+      mbar_init(&emptyBar[s], 1);
+    }
+    mbar_init(&accBar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmemBase)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmemBase;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // producer: TMA loads of the four operand tiles of each K-block
+      int issued = 0;
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % STAGES;
+        if (i >= STAGES && !wait_phase(&emptyBar[s], ((i / STAGES) - 1) & 1)) {
+          raise_flag(P.errFlag, CT_WAIT_EMPTY);
+          break;
+        }
+        unsigned char *st = smem + s * STAGE_BYTES;
+        mbar_arrive_expect_tx(&fullBar[s], STAGE_BYTES);
+        const int kx = (kr.x + i) * BK;
+        tma_load_2d(st, &tmAhi, kx, mt * BM, &fullBar[s]);
+        tma_load_2d(st + A_TILE, &tmAlo, kx, mt * BM, &fullBar[s]);
+        tma_load_2d(st + 2 * A_TILE, &tmBhi, kx, nt * BN, &fullBar[s]);
+        tma_load_2d(st + 2 * A_TILE + B_TILE, &tmBlo, kx, nt * BN, &fullBar[s]);
+        ++issued;
+      }
+      // every copy issued has landed before the CTA may exit
+      for (int i = max(0, issued - STAGES); i < issued; ++i)
+        if (!wait_phase(&fullBar[i % STAGES], (i / STAGES) & 1)) raise_flag(P.errFlag, CT_WAIT_DRAIN);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer: three bf16 products per K step into one FP32 accumulator
+      int done = 0;
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % STAGES;
+        if (!wait_phase(&fullBar[s], (i / STAGES) & 1)) {
+          raise_flag(P.errFlag, CT_WAIT_FULL);
+          break;
+        }
+        fence_after_sync();
+        const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+#pragma unroll
+        for (int k = 0; k < BK / 16; ++k) {
+          const uint32_t off = k * 32;   // 16 bf16 along K inside the 128-byte swizzle row
+          const uint64_t aHi = smem_desc(base + off), aLo = smem_desc(base + A_TILE + off);
+          const uint64_t bHi = smem_desc(base + 2 * A_TILE + off), bLo = smem_desc(base + 2 * A_TILE + B_TILE + off);
+          umma_bf16(tmem, aHi, bHi, (i > 0 || k > 0) ? 1u : 0u);
+          umma_bf16(tmem, aHi, bLo, 1u);
+          umma_bf16(tmem, aLo, bHi, 1u);
+        }
+        umma_commit(&emptyBar[s]);
+        ++done;
+      }
+      if (done > 0) {
+        umma_commit(&accBar);        // arrives once every MMA above has completed
+        // the accumulator is freed below only after the MMAs that write it are done
+        if (!wait_phase(&accBar, 0)) raise_flag(P.errFlag, CT_WAIT_ACC);
+      } else {
+        mbar_arrive(&accBar);        // empty band: nothing in flight
+      }
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, one replica row per thread
+    const int q = warp & 3, row = q * 32 + lane, grow = mt * BM + row;
+    const bool ok = __all_sync(0xffffffffu, wait_phase(&accBar, 0));
+    if (!ok && lane == 0) raise_flag(P.errFlag, CT_WAIT_ACC);
+    fence_after_sync();
+    double chi = 0.0;
+    float v[32];
+    for (int c = 0; c < BN; c += 32) {
+      if (nkb > 0 && ok) {
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = 0.f;
+      }
+      if (grow < P.M) {
+        const int col0 = nt * BN + c;
+        const bool vecStore = P.Y && col0 + 32 <= P.N && (P.N & 3) == 0;
+        if (vecStore) {
+          float4 *dst = reinterpret_cast<float4 *>(P.Y + (size_t)grow * P.N + col0);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int col = col0 + j;
+          if (col < P.N) {
+            if (P.Y && !vecStore) P.Y[(size_t)grow * P.N + col] = v[j];
+            const double d = (double)P.yobs[col] - (double)v[j];
+            chi += (double)P.w[col] * d * d;
+          }
+        }
+      }
+    }
+    if (grow < P.M) P.chiPart[(size_t)grow * P.nTilesN + nt] = chi;
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 1) {
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+// Split of an FP32 matrix (rows x cols, leading dimension ld) into bf16 hi/lo
+// parts (rows x Kp, zero padded to Kp columns).
+__global__ void split_kernel(const float *src, int rows, int cols, int ld, int Kp, __nv_bfloat16 *hi,
+                             __nv_bfloat16 *lo) {
+  const size_t total = (size_t)rows * Kp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / Kp;
+    const int k = (int)(i - r * Kp);
+    const float x = k < cols ? src[r * ld + k] : 0.f;
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi[i] = h;
+    lo[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+// Plain FP32 comparison: 128 x 128 tile, 16 x 16 threads x (8 x 8) outputs, K steps of 16
+// over the tile's band; FP64 chi^2 partials per 128-column tile.
+__global__ void __launch_bounds__(256) contract_fp32_kernel(const float *I, int ldI, const float *PT, int ldP,
+                                                            const int2 *kRange128, int M, int N, int nTiles128,
+                                                            const float *yobs, const float *w, float *Y,
+                                                            double *chiPart) {
+  __shared__ float As[FK][FM + 4], Bs[FK][FN + 4];
+  __shared__ double rowChi[FM][17];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int nt = blockIdx.x, mt = blockIdx.y;
+  const int2 kr = kRange128[nt];
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+  for (int k0 = kr.x; k0 < kr.y; k0 += FK) {
+    for (int e = threadIdx.x; e < FM * FK; e += 256) {
+      const int r = e / FK, k = e % FK;
+      const int gm = mt * FM + r, gn = nt * FN + r, gk = k0 + k;
+      As[k][r] = (gm < M && gk < kr.y) ? I[(size_t)gm * ldI + gk] : 0.f;
+      Bs[k][r] = (gn < N && gk < kr.y) ? PT[(size_t)gn * ldP + gk] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < FK; ++k) {
+      float a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = As[k][ty * 8 + i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Bs[k][tx * 8 + j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gm = mt * FM + ty * 8 + i;
+    double c = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int gn = nt * FN + tx * 8 + j;
+      if (gm < M && gn < N) {
+        if (Y) Y[(size_t)gm * N + gn] = acc[i][j];
+        const double d = (double)yobs[gn] - (double)acc[i][j];
+        c += (double)w[gn] * d * d;
+      }
+    }
+    rowChi[ty * 8 + i][tx] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x < FM) {
+    const int gm = mt * FM + threadIdx.x;
+    double c = 0.0;
+    for (int t = 0; t < 16; ++t) c += rowChi[threadIdx.x][t];
+    if (gm < M) chiPart[(size_t)gm * nTiles128 + nt] = c;
+  }
+}
+
+// chi2[r] = sum of the row's tile partials, in tile order.
+__global__ void chi_reduce_kernel(const double *part, int M, int nTiles, double *chi2) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= M) return;
+  double s = 0.0;
+  for (int t = 0; t < nTiles; ++t) s += part[(size_t)r * nTiles + t];
+  chi2[r] = s;
+}
+
+}  // namespace ct
+}  // namespace p6
+
+// ===========================================================================
+// Host side.
+// ===========================================================================
+using namespace p6;
+using namespace p6::ct;
+
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// 2-D bf16 tensor map: rows x Kp elements, K contiguous, box 64 x boxRows, 128B swizzle.
+p6_status make_map(CUtensorMap *m, void *base, int rows, int Kp, int boxRows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(P6_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)boxRows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(P6_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return P6_OK;
+}
+
+// K-ranges of each column tile of width `tile`: the smallest and largest
+// reflection with a nonzero profile value in the tile, rounded out to `align`.
+std::vector<int2> bands(const float *PT, int N, int K, int tile, int align, int Kp) {
+  const int nt = (N + tile - 1) / tile;
+  std::vector<int2> out(nt);
+  for (int t = 0; t < nt; ++t) {
+    int lo = K, hi = -1;
+    for (int j = t * tile; j < std::min(N, (t + 1) * tile); ++j) {
+      const float *row = PT + (size_t)j * K;
+      int a = 0;
+      while (a < K && row[a] == 0.f) ++a;
+      if (a == K) continue;
+      int b = K - 1;
+      while (b > a && row[b] == 0.f) --b;
+      lo = std::min(lo, a);
+      hi = std::max(hi, b);
+    }
+    if (hi < lo) {
+      out[t] = make_int2(0, 0);
+    } else {
+      const int kLo = lo / align * align, kHi = std::min(Kp, (hi + 1 + align - 1) / align * align);
+      out[t] = make_int2(kLo, kHi);
+    }
+  }
+  return out;
+}
+}  // namespace
+
+struct p6_ct_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int K = 0, Kp = 0, N = 0, Np = 0, maxM = 0, M = 0;
+  int nTilesN = 0, nTiles128 = 0;
+  float *dPT = nullptr;                 // N x K (FP32, the comparison path)
+  __nv_bfloat16 *dBhi = nullptr, *dBlo = nullptr, *dAhi = nullptr, *dAlo = nullptr;
+  float *dI = nullptr;                  // maxM x K (FP32 intensities)
+  float *dY = nullptr;                  // maxM x N, allocated on first request
+  float *dYobs = nullptr, *dW = nullptr;
+  double *dPart = nullptr, *dChi = nullptr;
+  int2 *dRange = nullptr, *dRange128 = nullptr;
+  int *dErr = nullptr;
+  long long bandBlocks = 0, bandCols128 = 0;   // sum of K-blocks over BN tiles; sum of K over 128-col tiles
+  CUtensorMap mapAhi, mapAlo, mapBhi, mapBlo;
+  long long launches = 0;
+};
+
+static void ct_free(p6_ct_session *s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (void *p : {(void *)s->dPT, (void *)s->dBhi, (void *)s->dBlo, (void *)s->dAhi, (void *)s->dAlo, (void *)s->dI,
+                  (void *)s->dY, (void *)s->dYobs, (void *)s->dW, (void *)s->dPart, (void *)s->dChi,
+                  (void *)s->dRange, (void *)s->dRange128, (void *)s->dErr})
+    if (p) cudaFree(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+static p6_status ct_check_flag(p6_ct_session *s) {
+  int flag = 0;
+  P6_CUDA(cudaMemcpyAsync(&flag, s->dErr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  if (flag) {
+    cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
+    return set_error(P6_ERR_TIMEOUT, "a tensor-core pipeline wait did not complete in time (code " +
+                                         std::to_string(flag) + ")");
+  }
+  return P6_OK;
+}
+
+extern "C" {
+
+p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out) {
+  clear_error();
+  if (!pr || !out) return set_error(P6_ERR_INVALID_ARG, "null problem or output pointer");
+  *out = nullptr;
+  if (pr->n_refl <= 0 || pr->n_points <= 0 || pr->max_replicas <= 0 || !pr->profile_t || !pr->yobs || !pr->w)
+    return set_error(P6_ERR_INVALID_ARG, "empty problem");
+  p6_ct_session *s = new p6_ct_session();
+  s->device = device;
+  s->K = pr->n_refl;
+  s->Kp = (pr->n_refl + BK - 1) / BK * BK;
+  s->N = pr->n_points;
+  s->Np = (pr->n_points + BN - 1) / BN * BN;
+  s->maxM = pr->max_replicas;
+  s->nTilesN = s->Np / BN;
+  s->nTiles128 = (s->N + FN - 1) / FN;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "cudaSetDevice"); }
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "cudaStreamCreate"); }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  const std::vector<int2> rBN = bands(pr->profile_t, s->N, s->K, BN, BK, s->Kp);
+  const std::vector<int2> r128 = bands(pr->profile_t, s->N, s->K, FN, 1, s->K);
+  std::vector<int2> kb(rBN.size());
+  for (size_t t = 0; t < rBN.size(); ++t) {
+    kb[t] = make_int2(rBN[t].x / BK, rBN[t].y / BK);
+    s->bandBlocks += kb[t].y - kb[t].x;
+  }
+  for (const int2 &r : r128) s->bandCols128 += r.y - r.x;
+  const size_t K = s->K, Kp = s->Kp, N = s->N, Np = s->Np, M = s->maxM;
+  p6_status st = P6_OK;
+#define CT_ALLOC(ptr, bytes)                                   \
+  do {                                                         \
+    e = cudaMalloc((void **)&(ptr), (bytes));                  \
+    if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "cudaMalloc"); } \
+  } while (0)
+  CT_ALLOC(s->dPT, N * K * sizeof(float));
+  CT_ALLOC(s->dBhi, Np * Kp * 2);
+  CT_ALLOC(s->dBlo, Np * Kp * 2);
+  CT_ALLOC(s->dAhi, M * Kp * 2);
+  CT_ALLOC(s->dAlo, M * Kp * 2);
+  CT_ALLOC(s->dI, M * K * sizeof(float));
+  CT_ALLOC(s->dYobs, N * sizeof(float));
+  CT_ALLOC(s->dW, N * sizeof(float));
+  CT_ALLOC(s->dPart, M * std::max(s->nTilesN, s->nTiles128) * sizeof(double));
+  CT_ALLOC(s->dChi, M * sizeof(double));
+  CT_ALLOC(s->dRange, kb.size() * sizeof(int2));
+  CT_ALLOC(s->dRange128, r128.size() * sizeof(int2));
+  CT_ALLOC(s->dErr, sizeof(int));
+#undef CT_ALLOC
+  cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
+  cudaMemsetAsync(s->dBhi, 0, Np * Kp * 2, s->stream);
+  cudaMemsetAsync(s->dBlo, 0, Np * Kp * 2, s->stream);
+  cudaMemcpyAsync(s->dPT, pr->profile_t, N * K * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+  cudaMemcpyAsync(s->dYobs, pr->yobs, N * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+  cudaMemcpyAsync(s->dW, pr->w, N * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+  cudaMemcpyAsync(s->dRange, kb.data(), kb.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
+  cudaMemcpyAsync(s->dRange128, r128.data(), r128.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
+  split_kernel<<<1184, 256, 0, s->stream>>>(s->dPT, s->N, s->K, s->K, s->Kp, s->dBhi, s->dBlo);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "profile upload"); }
+  if ((st = make_map(&s->mapAhi, s->dAhi, s->maxM, s->Kp, BM)) != P6_OK ||
+      (st = make_map(&s->mapAlo, s->dAlo, s->maxM, s->Kp, BM)) != P6_OK ||
+      (st = make_map(&s->mapBhi, s->dBhi, s->Np, s->Kp, BN)) != P6_OK ||
+      (st = make_map(&s->mapBlo, s->dBlo, s->Np, s->Kp, BN)) != P6_OK) {
+    ct_free(s);
+    return st;
+  }
+  e = cudaFuncSetAttribute(contract_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "cudaFuncSetAttribute"); }
+  *out = s;
+  return P6_OK;
+}
+
+p6_status p6_ct_destroy(p6_ct_session *s) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  ct_free(s);
+  return P6_OK;
+}
+
+p6_status p6_ct_set_intensities(p6_ct_session *s, const float *intensities, int n_replicas) {
+  clear_error();
+  if (!s || !intensities || n_replicas <= 0) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  if (n_replicas > s->maxM) return set_error(P6_ERR_CAPACITY, "more replicas than the session was created for");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaMemcpyAsync(s->dI, intensities, (size_t)n_replicas * s->K * sizeof(float), cudaMemcpyHostToDevice,
+                          s->stream));
+  s->M = n_replicas;
+  return P6_OK;
+}
+
+p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern) {
+  clear_error();
+  if (!s || s->M <= 0) return set_error(P6_ERR_INVALID_ARG, "no intensities set");
+  if (method != P6_CT_SPLIT_BF16 && method != P6_CT_FP32) return set_error(P6_ERR_INVALID_ARG, "unknown method");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (store_pattern && !s->dY) P6_CUDA(cudaMalloc(&s->dY, (size_t)s->maxM * s->N * sizeof(float)));
+  float *Y = store_pattern ? s->dY : nullptr;
+  P6_CUDA(cudaEventRecord(s->ev0, s->stream));
+  int nTiles;
+  if (method == P6_CT_SPLIT_BF16) {
+    split_kernel<<<1184, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo);
+    P6_CUDA(cudaGetLastError());
+    Params P;
+    P.M = s->M; P.N = s->N; P.Kp = s->Kp; P.nTilesN = s->nTilesN;
+    P.kRange = s->dRange; P.yobs = s->dYobs; P.w = s->dW; P.Y = Y; P.chiPart = s->dPart; P.errFlag = s->dErr;
+    const dim3 grid(s->nTilesN, (s->M + BM - 1) / BM);
+    contract_tc_kernel<<<grid, kThreads, SMEM_BYTES, s->stream>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo, P);
+    P6_CUDA(cudaGetLastError());
+    nTiles = s->nTilesN;
+    s->launches += 2;
+  } else {
+    const dim3 grid(s->nTiles128, (s->M + FM - 1) / FM);
+    contract_fp32_kernel<<<grid, 256, 0, s->stream>>>(s->dI, s->K, s->dPT, s->K, s->dRange128, s->M, s->N,
+                                                       s->nTiles128, s->dYobs, s->dW, Y, s->dPart);
+    P6_CUDA(cudaGetLastError());
+    nTiles = s->nTiles128;
+    s->launches += 1;
+  }
+  chi_reduce_kernel<<<(s->M + 255) / 256, 256, 0, s->stream>>>(s->dPart, s->M, nTiles, s->dChi);
+  P6_CUDA(cudaGetLastError());
+  s->launches += 1;
+  P6_CUDA(cudaEventRecord(s->ev1, s->stream));
+  return P6_OK;
+}
+
+p6_status p6_ct_read(p6_ct_session *s, double *chi2, float *pattern) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (pattern && !s->dY) return set_error(P6_ERR_INVALID_ARG, "no pattern was stored");
+  if (chi2) P6_CUDA(cudaMemcpyAsync(chi2, s->dChi, (size_t)s->M * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if (pattern)
+    P6_CUDA(cudaMemcpyAsync(pattern, s->dY, (size_t)s->M * s->N * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return ct_check_flag(s);
+}
+
+p6_status p6_ct_run_host(p6_ct_session *s, const float *intensities, int n_replicas, int method, double *chi2) {
+  p6_status st = p6_ct_set_intensities(s, intensities, n_replicas);
+  if (st != P6_OK) return st;
+  st = p6_ct_evaluate(s, method, 0);
+  if (st != P6_OK) return st;
+  return p6_ct_read(s, chi2, nullptr);
+}
+
+p6_status p6_ct_synchronize(p6_ct_session *s) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return ct_check_flag(s);
+}
+
+p6_status p6_ct_last_ms(p6_ct_session *s, float *ms) {
+  clear_error();
+  if (!s || !ms) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaEventSynchronize(s->ev1));
+  P6_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
+  return P6_OK;
+}
+
+p6_status p6_ct_query(p6_ct_session *s, long long *band_kblocks, long long *band_cols128, int *n_tiles,
+                      long long *launches) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  if (band_kblocks) *band_kblocks = s->bandBlocks;
+  if (band_cols128) *band_cols128 = s->bandCols128;
+  if (n_tiles) *n_tiles = s->nTilesN;
+  if (launches) *launches = s->launches;
+  return P6_OK;
+}
+
+}  // extern "C"

@@ -108,13 +108,14 @@ __device__ __forceinline__ double soft_floor(double x, double f) {
   if (!(f > 0)) return x;
   const double r = x / f;
   if (r > 20) return x;
-  return f * pow(pow(r, 4.0) + 1, 0.25);
+  const double r2 = r * r;
+  return f * sqrt(sqrt(r2 * r2 + 1));   // f (r^4 + 1)^(1/4)
 }
 __device__ __forceinline__ double peak_fwhm(double gG, double gL) {
   gG = fmax(1e-9, gG != 0 ? gG : 1e-9);
   gL = fmax(1e-9, gL != 0 ? gL : 1e-9);
-  const double s = pow(gG, 5.0) + 2.69269 * pow(gG, 4.0) * gL + 2.42843 * pow(gG, 3.0) * pow(gL, 2.0) +
-                   4.47163 * pow(gG, 2.0) * pow(gL, 3.0) + 0.07842 * gG * pow(gL, 4.0) + pow(gL, 5.0);
+  const double g2 = gG * gG, g3 = g2 * gG, g4 = g2 * g2, l2 = gL * gL, l3 = l2 * gL, l4 = l2 * l2;
+  const double s = g4 * gG + 2.69269 * g4 * gL + 2.42843 * g3 * l2 + 4.47163 * g2 * l3 + 0.07842 * gG * l4 + l4 * gL;
   if (s < 0 || !isfinite(s)) return fmax(fmax(gG, gL), 1e-6);
   return fmax(1e-6, pow(s, 0.2));
 }
@@ -132,7 +133,7 @@ __device__ double prepare(const double *v, double minFwhm, double tthPeak, doubl
   if (!(safe < 1e-6)) {
     const double t = tan(safe), c = cos(safe), cs = fmax(c, 1e-9);
     const double sig2 = v[PU] * t * t + v[PV] * t + v[PW];
-    const double floorSq = pow(0.25 * minFwhm / kGconv, 2.0);
+    const double fq = 0.25 * minFwhm / kGconv, floorSq = fq * fq;
     gG = sqrt(soft_positive(sig2, floorSq)) * kGconv;
     gL = soft_positive(v[PX] / cs + v[PY] * t, 0.25 * minFwhm / kLconv) * kLconv;
   }
@@ -143,7 +144,7 @@ __device__ double prepare(const double *v, double minFwhm, double tthPeak, doubl
   double eta = 0;
   if (fwhm > 1e-9) {
     const double r = HL / fwhm;
-    eta = fmax(0.0, fmin(1.0, 1.36603 * r - 0.47719 * (r * r) + 0.11116 * pow(r, 3.0)));
+    eta = fmax(0.0, fmin(1.0, 1.36603 * r - 0.47719 * (r * r) + 0.11116 * (r * r * r)));
   }
   const double g0 = 2.0 * sqrt(log(2.0) / kPi), l0 = 2.0 / kPi;
   const double e = fmax(0.0, fmin(1.0, eta));
@@ -230,7 +231,7 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
   const double *v = sh.v;
   const int nR = P.nRefl;
   const bool doublet = P.ratio > 1e-6 && P.lambda2 > 1e-6 && fabs(P.lambda1 - P.lambda2) > 1e-6;
-  // --- reflections: warp per reflection (|F|^2 over the coset representatives), lane 0 prepares the peaks
+  // |F|^2: warp per reflection, lanes over the coset representatives
   for (int k = warp; k < nR; k += kWarps) {
     const int hh = P.hkl[3 * k], kk = P.hkl[3 * k + 1], ll = P.hkl[3 * k + 2];
     const double q = hh * hh * sh.f[0] + kk * kk * sh.f[1] + ll * ll * sh.f[2] + hh * kk * sh.f[3] +
@@ -270,39 +271,65 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
         B += (A_t)wj * sn;
       }
     }
-    if (lane == 0) {
-      act[k] = 0;
+    if (lane == 0) h1[k] = (H)((double)A * A + (double)B * B);   // F^2, parked until the heights
+  }
+  __syncwarp();
+  // Peaks: lane pairs over this warp's reflections, the even lane preparing
+  // K-alpha-1 and the odd lane K-alpha-2 of the same reflection at once.
+  const int cnt = nR > warp ? (nR - 1 - warp) / kWarps + 1 : 0;
+  for (int b = 0; b < 2 * cnt; b += 32) {
+    const int idx = b + lane, line = idx & 1;
+    const bool mine = idx < 2 * cnt;
+    const int k = warp + (idx >> 1) * kWarps;
+    double area = 0.0, lp = 1.0;
+    int flag = 0;
+    bool live = false;
+    if (mine) {
+      const int hh = P.hkl[3 * k], kk = P.hkl[3 * k + 1], ll = P.hkl[3 * k + 2];
+      const double q = hh * hh * sh.f[0] + kk * kk * sh.f[1] + ll * ll * sh.f[2] + hh * kk * sh.f[3] +
+                       kk * ll * sh.f[4] + hh * ll * sh.f[5];
+      const double sinT = P.lambda1 * sqrt(q) / 2;
+      live = q > 0 && q <= P.qmax && sinT < 1;
       if (live) {
         const double bragg = 2 * asin(sinT) * kR2D;
-        const double base = bragg + v[PZERO];
-        const double area1 = prepare(v, P.minFwhm, base, base, pk1[k]);
-        const double lp = lp_factor(base, P.polK);
-        const double F2 = (double)A * A + (double)B * B;
-        const double factor = P.mult[k] * lp * 1.0 / area1;
-        h1[k] = (H)(v[SCALE] * (factor * F2));
-        if (u1) u1[k] = factor * F2;
-        const int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = upper_bound(tth, P.n, base + pk1[k].maxd, lo);
-        pk1[k].lo = lo;
-        pk1[k].hi = hi;
-        int flag = (hi > lo && lo < P.n) ? 1 : 0;
-        pk2[k].lo = pk2[k].hi = 0;
-        w2[k] = 0;
-        if (doublet) {
-          const double sin2 = sin(bragg * kD2R / 2.0) * (P.lambda2 / P.lambda1);
-          if (fabs(sin2) < 1) {
-            const double base2 = 2 * asin(sin2) / kD2R + v[PZERO];
-            const double area2 = prepare(v, P.minFwhm, base2, base2, pk2[k]);
-            const double lpr = lp_factor(base2, P.polK) / lp_factor(base, P.polK);
-            w2[k] = (H)(P.ratio * area1 / area2 * lpr);
-            const int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd),
-                      hi2 = upper_bound(tth, P.n, base2 + pk2[k].maxd, lo2);
-            pk2[k].lo = lo2;
-            pk2[k].hi = hi2;
-            if (hi2 > lo2 && lo2 < P.n) flag |= 2;
+        if (line == 0) {
+          const double base = bragg + v[PZERO];
+          area = prepare(v, P.minFwhm, base, base, pk1[k]);
+          lp = lp_factor(base, P.polK);
+          const int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = upper_bound(tth, P.n, base + pk1[k].maxd, lo);
+          pk1[k].lo = lo;
+          pk1[k].hi = hi;
+          flag = (hi > lo && lo < P.n) ? 1 : 0;
+        } else {
+          pk2[k].lo = pk2[k].hi = 0;
+          if (doublet) {
+            const double sin2 = sin(bragg * kD2R / 2.0) * (P.lambda2 / P.lambda1);
+            if (fabs(sin2) < 1) {
+              const double base2 = 2 * asin(sin2) / kD2R + v[PZERO];
+              area = prepare(v, P.minFwhm, base2, base2, pk2[k]);
+              lp = lp_factor(base2, P.polK);
+              const int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd),
+                        hi2 = upper_bound(tth, P.n, base2 + pk2[k].maxd, lo2);
+              pk2[k].lo = lo2;
+              pk2[k].hi = hi2;
+              flag = (hi2 > lo2 && lo2 < P.n) ? 2 : 0;
+            }
           }
         }
-        if (!(area1 > 0)) flag = 0;
-        act[k] = flag;
+      }
+    }
+    const double area2 = __shfl_xor_sync(0xffffffffu, area, 1), lp2 = __shfl_xor_sync(0xffffffffu, lp, 1);
+    const int flag2 = __shfl_xor_sync(0xffffffffu, flag, 1);
+    if (mine && line == 0) {
+      act[k] = 0;
+      w2[k] = 0;
+      if (live) {
+        const double F2 = (double)h1[k];
+        const double factor = P.mult[k] * lp * 1.0 / area;
+        h1[k] = (H)(v[SCALE] * (factor * F2));
+        if (u1) u1[k] = factor * F2;
+        if (area2 > 0) w2[k] = (H)(P.ratio * area / area2 * (lp2 / lp));
+        act[k] = area > 0 ? (flag | flag2) : 0;
       }
     }
   }
@@ -320,7 +347,7 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
   __syncthreads();
   // --- pattern in warp tiles of 32 points, then chi^2 (FP64)
   double chi = 0.0;
-  const double x0 = tth[0], x1 = tth[P.n - 1];
+  const double x0 = tth[0], x1 = tth[P.n - 1], zs = x1 > x0 ? 2.0 / (x1 - x0) : 0.0;
   for (int base = warp * 32; base < P.n; base += kThreads) {
     const int i = base + lane;
     const bool in = i < P.n;
@@ -349,7 +376,7 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
       yp = fmaf(h1[k], col, yp);
     }
     if (in) {
-      const double z = x1 > x0 ? 2 * (x - x0) / (x1 - x0) - 1 : 0;
+      const double z = x1 > x0 ? (x - x0) * zs - 1 : 0;
       double Tm2 = 1, Tm1 = z, bk = 0;
       for (int kk = 0; kk < P.nBkg; ++kk) {
         const double T = kk == 0 ? 1 : kk == 1 ? z : 2 * z * Tm1 - Tm2;
@@ -582,7 +609,7 @@ __global__ void __launch_bounds__(kThreads) pt_pattern64_kernel(const Params P, 
   __syncthreads();
   const double *v = sh.v;
   const int nR = P.nRefl;
-  const double x0 = P.tth[0], x1 = P.tth[P.n - 1];
+  const double x0 = P.tth[0], x1 = P.tth[P.n - 1], zs = x1 > x0 ? 2.0 / (x1 - x0) : 0.0;
   double chi = 0.0;
   for (int base = warp * 32; base < P.n; base += kThreads) {
     const int i = base + lane;
@@ -609,7 +636,7 @@ __global__ void __launch_bounds__(kThreads) pt_pattern64_kernel(const Params P, 
       yu1 += u1[k] * col;
     }
     if (in) {
-      const double z = x1 > x0 ? 2 * (x - x0) / (x1 - x0) - 1 : 0;
+      const double z = x1 > x0 ? (x - x0) * zs - 1 : 0;
       double Tm2 = 1, Tm1 = z, bk = 0;
       for (int kk = 0; kk < P.nBkg; ++kk) {
         const double T = kk == 0 ? 1 : kk == 1 ? z : 2 * z * Tm1 - Tm2;
@@ -683,11 +710,11 @@ __global__ void __launch_bounds__(kThreads) pt_normal_kernel(const Params P, con
   } else {
     mode = 2;
   }
-  const double x0 = P.tth[0], x1 = P.tth[P.n - 1];
+  const double x0 = P.tth[0], x1 = P.tth[P.n - 1], zs = x1 > x0 ? 2.0 / (x1 - x0) : 0.0;
   double acc = 0.0;
   for (int i = tid; i < P.n; i += kThreads) {
     const double w = P.wd[i];
-    const double z = x1 > x0 ? 2 * (P.tth[i] - x0) / (x1 - x0) - 1 : 0;
+    const double z = x1 > x0 ? (P.tth[i] - x0) * zs - 1 : 0;
     const double r = w > 0 ? P.y[i] - y[i] : 0.0;
     if (mode == 0)
       acc += w * jcol(P, L, ja, i, y, yu, z) * jcol(P, L, jb, i, y, yu, z);
