@@ -160,6 +160,11 @@ p6_status p6_wy_evaluate_sync(p6_wy_session *s, const float *coords, int mcmc, f
 p6_status p6_wy_set_ladders(p6_wy_session *s, const int32_t *ladders, int n_ladders, int rungs);
 p6_status p6_wy_set_schedule(p6_wy_session *s, const int32_t *sched_groups, const float *sched_pen, int n_gen);
 p6_status p6_wy_run(p6_wy_session *s, int gen0, int n_gen, int swap_every, int reeval_first);
+/* quench (js/swarm_wyckoff.js:2013-2090): with a schedule of step widths set
+ * (step_sd[g] for generations g < n_gen), p6_wy_run takes greedy steps --
+ * a proposal is kept only if it raises the fitness, the step width is the
+ * schedule's, not the adapted one.  step_sd = NULL restores the search. */
+p6_status p6_wy_set_quench(p6_wy_session *s, const float *step_sd, int n_gen);
 /* Host-buffer form of p6_wy_run: uploads positions/state, runs, reads them back
  * (copies inside the call). */
 p6_status p6_wy_run_host(p6_wy_session *s, const float *positions_in, const p6_wy_particle_state *state_in,

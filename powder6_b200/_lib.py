@@ -84,6 +84,7 @@ _SIGS = {
     'p6_wy_evaluate_sync': (C.c_int, [_P, _P, C.c_int, _P]),
     'p6_wy_set_ladders': (C.c_int, [_P, _P, C.c_int, C.c_int]),
     'p6_wy_set_schedule': (C.c_int, [_P, _P, _P, C.c_int]),
+    'p6_wy_set_quench': (C.c_int, [_P, _P, C.c_int]),
     'p6_wy_run': (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     'p6_wy_run_host': (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P]),
     'p6_wy_synchronize': (C.c_int, [_P, C.c_double]),

@@ -105,6 +105,7 @@ struct Params {
   int rungs, nLadders;
   const int *schedGroups;  // per generation; null: use ngaArg/penArg
   const float *schedPen;
+  const float *quenchSd;   // per generation: greedy quench with this step; null: Metropolis with adapted steps
   int ngaArg;
   float penArg;
   uint32_t *tracePos;
@@ -855,7 +856,7 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, in
         }
         if (mcmc) {
           float uMetro;
-          const float sd = __shfl_sync(0xffffffffu, step, 0);
+          const float sd = P.quenchSd ? P.quenchSd[g] : __shfl_sync(0xffffffffu, step, 0);
           propose(P, ws, proj, g, p, lane, sd, seed, &uMetro);
           double sums[3];
           uint32_t moved = 0;
@@ -892,7 +893,9 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, in
             float fOld = fit;
             if (fOld > -1.0e29f) fOld = cc0 - pen0 * penScale;
             const float stepBefore = step;
-            if (fNew >= fOld)
+            if (P.quenchSd)
+              acc = fNew > fOld ? 1 : 0;   // quench: only improvements (js/swarm_wyckoff.js:2069-2075)
+            else if (fNew >= fOld)
               acc = 1;
             else if (uMetro < expf((fNew - fOld) / fmaxf(temp, 1e-9f)))
               acc = 1;
@@ -910,7 +913,7 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, in
                 best = 1;
               }
             }
-            step = fminf(fmaxf(step * (acc ? P.stepUp : P.stepDown), P.stepMin), P.stepMax);
+            if (!P.quenchSd) step = fminf(fmaxf(step * (acc ? P.stepUp : P.stepDown), P.stepMin), P.stepMax);
             if (P.traceRec) {
               float *rec = P.traceRec + (size_t)p * 8;
               rec[0] = fNew; rec[1] = cc; rec[2] = pen; rec[3] = uMetro;
@@ -1050,7 +1053,8 @@ struct p6_wy_session {
   uint32_t *dGen = nullptr, *dGenOrig = nullptr, *dFree = nullptr, *dPos = nullptr, *dAssign = nullptr;
   int4 *dRuns = nullptr;
   int *dNRuns = nullptr, *dNF = nullptr, *dLadders = nullptr, *dSchedG = nullptr, *dErr = nullptr;
-  float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr;
+  float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr, *dQuench = nullptr;
+  int quenchLen = 0;
   uint32_t *dTracePos = nullptr;
   OpFix *dOps = nullptr;
   ProjFix *dProj = nullptr;
@@ -1158,7 +1162,7 @@ static void free_session(p6_wy_session *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
-                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dTraceRec, s->dTraceIc, s->dTracePos, s->dOps,
+                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTracePos, s->dOps,
                   s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1764,6 +1768,22 @@ p6_status p6_wy_set_schedule(p6_wy_session *s, const int32_t *sched_groups, cons
   return P6_OK;
 }
 
+p6_status p6_wy_set_quench(p6_wy_session *s, const float *step_sd, int n_gen) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (s->dQuench) cudaFree(s->dQuench);
+  s->dQuench = nullptr;
+  s->quenchLen = 0;
+  if (!step_sd) return P6_OK;
+  if (n_gen <= 0) return set_error(P6_ERR_INVALID_ARG, "empty quench schedule");
+  p6_status st = upload(&s->dQuench, step_sd, (size_t)n_gen, s->stream);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  s->quenchLen = n_gen;
+  return P6_OK;
+}
+
 p6_status p6_wy_run(p6_wy_session *s, int gen0, int n_gen, int swap_every, int reeval_first) {
   P6_ENTRY();
   if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
@@ -1778,9 +1798,18 @@ p6_status p6_wy_run(p6_wy_session *s, int gen0, int n_gen, int swap_every, int r
   P.nLadders = s->nLadders;
   P.schedGroups = s->dSchedG;
   P.schedPen = s->dSchedP;
-  P.tracePos = nullptr;
-  P.traceRec = nullptr;
-  P.traceIc = nullptr;
+  P.quenchSd = nullptr;
+  if (s->dQuench) {
+    if (gen0 + n_gen > s->quenchLen) {
+      P = saved;
+      return set_error(P6_ERR_INVALID_ARG, "generation range outside the quench schedule");
+    }
+    P.quenchSd = s->dQuench;
+  }
+  // with tracing on, the records hold the last generation of the run
+  P.tracePos = s->trace ? s->dTracePos : nullptr;
+  P.traceRec = s->trace ? s->dTraceRec : nullptr;
+  P.traceIc = s->trace ? s->dTraceIc : nullptr;
   P6_CUDA(cudaEventRecord(s->ev0, s->stream));
   cudaError_t e = launch(s, gen0, n_gen, 1, swap_every, reeval_first ? 1 : 0);
   P = saved;

@@ -186,6 +186,16 @@ class WyckoffSession:
         p = np.ascontiguousarray(pen, dtype=np.float32)
         check(self.lib.p6_wy_set_schedule(self.h, ptr(g), ptr(p), len(g)))
 
+    def set_quench(self, step_sd: Optional[np.ndarray]):
+        """Greedy quench mode (js/swarm_wyckoff.js:2013-2090): per generation step
+        width, only improvements accepted, no step adaptation; None restores
+        the Metropolis search."""
+        if step_sd is None:
+            check(self.lib.p6_wy_set_quench(self.h, None, 0))
+        else:
+            a = np.ascontiguousarray(step_sd, dtype=np.float32)
+            check(self.lib.p6_wy_set_quench(self.h, ptr(a), len(a)))
+
     def run(self, gen0: int, n_gen: int, swap_every: int, reeval_first: bool = True):
         check(self.lib.p6_wy_run(self.h, int(gen0), int(n_gen), int(swap_every), 1 if reeval_first else 0))
 
@@ -378,16 +388,81 @@ class SearchResult:
     launches: int
     seed: int
     cpu_check: Dict[str, float] = field(default_factory=dict)
+    quench: Dict[str, float] = field(default_factory=dict)
+    time_to_target: Optional[float] = None
+    wall_s: float = 0.0
+
+
+def quench_schedule(settings: Optional[dict] = None) -> np.ndarray:
+    """Step widths of the quench: geometric from quenchStep0 to quenchStep1 over quenchSteps."""
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    steps = int(d['quenchSteps'])
+    t = np.arange(steps) / max(1, steps - 1) if steps > 1 else np.ones(1)
+    return (d['quenchStep0'] * (d['quenchStep1'] / d['quenchStep0']) ** t).astype(np.float32)
+
+
+def quench(problem: WyckoffProblem, sess: 'WyckoffSession', best: Dict[int, dict], rnd: Callable[[], float],
+           settings: Optional[dict] = None) -> Dict[int, dict]:
+    """quench (js/swarm_wyckoff.js:2013-2100) on the device: every chain starts
+    from its assignment's best, is re-measured at full resolution and the
+    final penalty weight, and takes quenchSteps greedy steps of shrinking
+    width.  ``best`` maps assignment -> {'cc', 'pen', 'coords'}; returns the
+    same map re-scored and improved."""
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    live = sorted(A for A, b in best.items() if b.get('coords') is not None)
+    if not live:
+        return best
+    n, cpp = sess.num_particles, sess.coords_per_particle
+    assign_of = np.array([live[i % len(live)] for i in range(n)], dtype=np.uint32)
+    sess.set_assign(assign_of)
+    pos = np.concatenate([best[int(A)]['coords'] for A in assign_of]).astype(np.float32)
+    st = initial_state(n, np.full(n, d['tempCold'], dtype=np.float32), rnd, d)
+    sess.sync_state(pos, st)
+    sd = quench_schedule(d)
+    steps = len(sd)
+    scale = float(d['penRampEnd'])
+    sess.set_schedule(np.full(steps, problem.refl.n_groups, dtype=np.int32), np.full(steps, scale, dtype=np.float32))
+    sess.set_quench(sd)
+    try:
+        sess.run(0, steps, 0, True)
+        sess.synchronize(600.0)
+        ms = sess.last_kernel_ms()
+    finally:
+        sess.set_quench(None)
+    cur, bestpos, st = sess.read_state()
+    out = {}
+    for A in live:
+        idx = np.nonzero(assign_of == A)[0]
+        # the start, re-measured at full resolution, is the first candidate
+        i0 = int(idx[0])
+        rec = [(float(st['best_cc'][i] - st['best_pen'][i] * scale), int(i)) for i in idx if st['best_fit'][i] > -1e29]
+        if rec:
+            _, i = max(rec)
+            out[A] = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
+                      'coords': bestpos[i * cpp:(i + 1) * cpp].copy(), 'improved': True}
+        else:
+            out[A] = {'cc': float(st['cc'][i0]), 'pen': float(st['pen'][i0]), 'coords': best[A]['coords'],
+                      'improved': False}
+    out['_ms'] = ms
+    return out
 
 
 def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
                        restarts: int = 1, seed: int = 20261026, cos_mode: int = 0, chunk: Optional[int] = None,
                        settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
                        on_progress: Optional[Callable[[dict], None]] = None,
-                       should_stop: Optional[Callable[[], bool]] = None) -> SearchResult:
+                       should_stop: Optional[Callable[[], bool]] = None, do_quench: bool = True,
+                       target_cc: Optional[float] = None) -> SearchResult:
     """One assignment list, ``restarts`` independent restarts, all generations on
-    the device.  The per-assignment best is re-scored at full resolution and the
-    final penalty weight and cross-checked on the CPU, as the reference reports."""
+    the device, then the quench of the per-assignment bests.  The winner is
+    re-scored at full resolution and the final penalty weight and
+    cross-checked on the CPU, as the reference reports.  With ``target_cc``,
+    ``time_to_target`` is the wall time from the start to the first chunk
+    boundary (or the end of the quench) at which the best cc reached it."""
+    import time
+    t_start = time.perf_counter()
     d = dict(SW_DEFAULTS)
     d.update(settings or {})
     rnd = mulberry32(seed)
@@ -403,12 +478,14 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     groups, pen = schedule(generations, problem.refl.n_groups, d)
     sess.set_schedule(groups, pen)
     chunk = chunk or generations
-    best = {'cc': -np.inf, 'pen': 0.0, 'coords': None, 'A': 0}
+    scale = float(pen[-1])
+    per_a: Dict[int, dict] = {}
     total_ms = 0.0
     acc_total = 0
-    swaps0 = None
+    hit = None
+    cpp = sess.coords_per_particle
     for restart in range(restarts):
-        pos = np.array([rnd() for _ in range(n * sess.coords_per_particle)], dtype=np.float32)
+        pos = np.array([rnd() for _ in range(n * cpp)], dtype=np.float32)
         pos = project_all(problem, pos, assign_of)
         st = initial_state(n, temps, rnd, d)
         sess.sync_state(pos, st)
@@ -422,21 +499,46 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
             sess.synchronize(600.0)
             total_ms += sess.last_kernel_ms()
             g0 += ng
+            if target_cc is not None and hit is None and g0 < generations:
+                _, _, stc = sess.read_state()
+                ok = stc['best_fit'] > -1e29
+                if np.any(ok) and float(np.max(stc['best_cc'][ok])) >= target_cc:
+                    hit = time.perf_counter() - t_start
             if on_progress:
                 on_progress({'restart': restart + 1, 'restarts': restarts, 'generation': g0 - 1,
                              'generations': generations})
         cur, bestpos, st = sess.read_state()
         acc_total += int(st['accepted'].sum())
-        scale = float(pen[-1])
-        score = np.where(st['best_fit'] > -1e29, st['best_cc'] - st['best_pen'] * scale, -np.inf)
-        i = int(np.argmax(score))
-        if score[i] > best['cc'] - best['pen'] * scale:
-            cpp = sess.coords_per_particle
-            best = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
-                    'coords': bestpos[i * cpp:(i + 1) * cpp].copy(), 'A': int(assign_of[i])}
+        for i in range(n):
+            if not st['best_fit'][i] > -1e29:
+                continue
+            A = int(assign_of[i])
+            f = float(st['best_cc'][i] - st['best_pen'][i] * scale)
+            if A not in per_a or f > per_a[A]['cc'] - per_a[A]['pen'] * scale:
+                per_a[A] = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
+                            'coords': bestpos[i * cpp:(i + 1) * cpp].copy()}
+    qinfo = {}
+    if do_quench and per_a and not (should_stop and should_stop()):
+        before = {A: v['cc'] for A, v in per_a.items()}
+        q = quench(problem, sess, per_a, rnd, d)
+        qinfo = {'ms': q.pop('_ms'), 'improved': int(sum(1 for A in q if q[A].get('improved'))),
+                 'best_before': max(before.values())}
+        total_ms += qinfo['ms']
+        per_a = q
+        sess.set_assign(assign_of)
+        sess.set_schedule(groups, pen)
+    best = {'cc': -np.inf, 'pen': 0.0, 'coords': None, 'A': 0}
+    for A, v in per_a.items():
+        if v['cc'] - v['pen'] * scale > best['cc'] - best['pen'] * scale:
+            best = dict(v, A=A)
+    if target_cc is not None and hit is None and best['coords'] is not None and best['cc'] >= target_cc:
+        hit = time.perf_counter() - t_start
+    if qinfo:
+        qinfo['best_after'] = best['cc']
     trials = n * generations * restarts
     res = SearchResult(best['cc'], best['pen'], best['coords'], trials, total_ms,
-                       acc_total / max(1, trials), float('nan'), sess.launch_count(), seed)
+                       acc_total / max(1, trials), float('nan'), sess.launch_count(), seed, quench=qinfo,
+                       time_to_target=hit, wall_s=time.perf_counter() - t_start)
     if best['coords'] is not None:
         cpu = cpu_cross_check(problem, best['coords'], best['A'])
         res.cpu_check = {'gpu': best['cc'], 'cpu': cpu, 'delta': abs(best['cc'] - cpu)}

@@ -251,6 +251,53 @@ def test_search_recovers_the_true_structure(prob):
     assert res.launches >= 3
 
 
+def test_quench_only_improves_and_reports_time_to_target(prob):
+    """quench (js/swarm_wyckoff.js:2013-2100): from a short search, the greedy
+    quench at full resolution never loses the re-measured start, its winner
+    re-scores on the CPU, and time_to_target is reported when reached."""
+    P = prob
+    short = run_wyckoff_search(P, num_particles=512, generations=300, seed=7, chunk=100, do_quench=False)
+    res = run_wyckoff_search(P, num_particles=512, generations=300, seed=7, chunk=100, do_quench=True,
+                             target_cc=short.best_cc - 0.05)
+    q = res.quench
+    assert q and q['ms'] > 0
+    assert res.best_cc >= q['best_before'] - 2e-3       # the start is re-measured at full resolution
+    assert res.cpu_check['delta'] <= 1e-3
+    assert res.time_to_target is not None and res.time_to_target <= res.wall_s
+
+
+def test_quench_accepts_improvements_only(prob):
+    """In quench mode every accepted proposal raised the fitness, and the step
+    widths stay where the search left them (no adaptation)."""
+    from powder6_b200.swarm_wyckoff import build_ladders, initial_state, project_all, quench_schedule
+    from powder6_b200.workloads import mulberry32
+    P = prob
+    n = 256
+    rnd = mulberry32(5)
+    with WyckoffSession(P, n) as s:
+        assign = np.zeros(n, dtype=np.uint32)
+        s.set_assign(assign)
+        ladders, temps = build_ladders(assign)
+        s.set_ladders(ladders, 8)
+        pos = project_all(P, np.array([rnd() for _ in range(n * s.coords_per_particle)], dtype=np.float32), assign)
+        st0 = initial_state(n, temps, rnd)
+        s.sync_state(pos, st0)
+        sd = quench_schedule()[:50]
+        s.set_schedule(np.full(50, P.refl.n_groups, dtype=np.int32), np.full(50, 4.0, dtype=np.float32))
+        s.set_quench(sd)
+        s.set_trace(True)
+        s.run(0, 50, 0, True)
+        s.synchronize(60)
+        _, rec = s.read_trace()
+        _, _, st = s.read_state()
+        s.set_quench(None)
+    rec = rec.reshape(n, 8)
+    acc = rec[:, 4] > 0.5
+    assert np.all(rec[acc, 0] > rec[acc, 5])
+    assert np.all(st['step_size'] == st0['step_size'])
+    assert st['accepted'].sum() > 0
+
+
 def test_restraint_rules_parity(oracle):
     """Counted shells, shapes and nearest-neighbour rules (the 64-slot variant)."""
     P = wyckoff_problem(seed=2, windows=[{'a': 'S', 'b': 'O', 'count': 4, 'dmin': 1.35, 'dmax': 1.65,
