@@ -306,6 +306,31 @@ p6_status p6_pt_lm(p6_pt_session *s, double *x, int max_iter, double tol, double
 #define P6_PT_STATIC_SCRATCH_BYTES (4u << 20)
 p6_status p6_pt_costs_static(p6_pt_session *s, const double *vectors, int n_vectors, double *costs, float *ycalc);
 
+/* Many searches in one persistent launch.  The sessions (same device and
+ * cos_mode, incremental evaluation off, at most 8 rungs, ladders and
+ * schedules set) keep their own tables and state; the batch runs all their
+ * ladders in one launch of persistent CTAs that take (search, ladder) items
+ * from a list -- longest estimated ladder first (order 0) or in search order
+ * (1) -- each CTA staging the tables of the search it is working on.  The
+ * dynamic shared memory of the launch is the largest search's.  No
+ * reference counterpart: the reference runs one search per worker
+ * (js/wyckoff_worker.js); each search's results are those of p6_wy_run. */
+typedef struct p6_wy_batch p6_wy_batch;
+p6_status p6_wy_batch_create(p6_wy_session *const *sessions, int n_sessions, p6_wy_batch **out);
+p6_status p6_wy_batch_destroy(p6_wy_batch *b);
+/* Launch shape: ctas_per_sm persistent CTAs per SM (0: the occupancy limit,
+ * at most the value p6_wy_batch_query reports) and the item order. */
+p6_status p6_wy_batch_set_launch(p6_wy_batch *b, int ctas_per_sm, int order);
+p6_status p6_wy_batch_query(p6_wy_batch *b, int *max_ctas_per_sm, int *smem_bytes, int *n_items, long long *launches);
+/* Generations [gen0[i], gen0[i] + n_gen[i]) of session i, exchange every
+ * swap_every generations; use_graph != 0 replays the launch from a CUDA
+ * graph captured on first use.  Asynchronous; the sessions' later calls
+ * wait for it. */
+p6_status p6_wy_batch_run(p6_wy_batch *b, const int32_t *gen0, const int32_t *n_gen, int swap_every, int reeval_first,
+                          int use_graph);
+p6_status p6_wy_batch_synchronize(p6_wy_batch *b, double timeout_seconds);
+p6_status p6_wy_batch_last_ms(p6_wy_batch *b, float *ms);
+
 /* ======================================================================== */
 /* Profile contraction with the cell and profile fixed                       */
 /* ======================================================================== */

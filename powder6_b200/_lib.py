@@ -111,6 +111,14 @@ _SIGS = {
     'p6_pt_normal': (C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double)]),
     'p6_pt_linear_start': (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
     'p6_pt_lm': (C.c_int, [_P, _P, C.c_int, C.c_double, _P]),
+    'p6_wy_batch_create': (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p)]),
+    'p6_wy_batch_destroy': (C.c_int, [_P]),
+    'p6_wy_batch_set_launch': (C.c_int, [_P, C.c_int, C.c_int]),
+    'p6_wy_batch_query': (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_longlong)]),
+    'p6_wy_batch_run': (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
+    'p6_wy_batch_synchronize': (C.c_int, [_P, C.c_double]),
+    'p6_wy_batch_last_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_ct_create': (C.c_int, [C.POINTER(P6CtProblem), C.c_int, C.POINTER(C.c_void_p)]),
     'p6_ct_destroy': (C.c_int, [_P]),
     'p6_ct_set_intensities': (C.c_int, [_P, _P, C.c_int]),

@@ -11,12 +11,15 @@
 //  * I = I_hi + I_lo and P = P_hi + P_lo with bf16 parts (I_hi = bf16(I),
 //    I_lo = bf16(I - I_hi)); Y = I_hi P_hi + I_hi P_lo + I_lo P_hi with FP32
 //    accumulation (the dropped I_lo P_lo term is ~2^-16 relative);
-//  * one CTA per 128 x 256 output tile; its K loop covers only the K-blocks
-//    (64 reflections) the tile's band touches;
+//  * 128 x 256 output tiles, handed round-robin to one persistent CTA per
+//    SM; a tile's K loop covers only the K-blocks (64 reflections) its band
+//    touches;
 //  * warp 0 issues TMA loads (128B-swizzled, K-major tiles of the four bf16
 //    operands) into a two-stage shared-memory ring; warp 1 issues
-//    tcgen05.mma (M 128, N 256, K 16) into a TMEM accumulator and commits
-//    each stage back to the producer; warps 2-5 read the accumulator with
+//    tcgen05.mma (M 128, N 256, K 16) into one of two TMEM accumulators
+//    (alternating per tile, so one tile's epilogue overlaps the next tile's
+//    MMAs) and commits each stage back to the producer; warps 2-5 read the
+//    accumulator with
 //    tcgen05.ld and reduce the weighted residual against the observed
 //    pattern in FP64 (the only FP64 on this path), optionally storing Y;
 //  * per-tile chi^2 partials are summed per replica in a fixed order.
@@ -45,7 +48,7 @@ constexpr int B_TILE = BN * BK * 2;                       // 32 KB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;      // 96 KB: A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack (1024-B swizzle atoms)
 constexpr int kThreads = 192;                             // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
-constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t TMEM_COLS = 2 * BN;                    // two accumulator buffers
 constexpr unsigned long long kWaitNs = 2000000000ull;     // 2 s per wait
 
 // SIMT comparison kernel tiles
@@ -54,7 +57,7 @@ constexpr int FM = 128, FN = 128, FK = 16;
 enum CtError : int { CT_OK = 0, CT_WAIT_FULL = 11, CT_WAIT_EMPTY = 12, CT_WAIT_ACC = 13, CT_WAIT_DRAIN = 14 };
 
 struct Params {
-  int M, N, Kp, nTilesN;
+  int M, N, Kp, nTilesN, nTilesM;
   const int2 *kRange;     // per BN tile: K-blocks [x, y)
   const float *yobs, *w;  // N
   float *Y;               // optional, M x N
@@ -143,20 +146,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                        const __grid_constant__ CUtensorMap tmBhi, const __grid_constant__ CUtensorMap tmBlo,
                        const Params P) {
   extern __shared__ unsigned char smemRaw[];
-  __shared__ __align__(8) uint64_t fullBar[STAGES], emptyBar[STAGES], accBar;
+  __shared__ __align__(8) uint64_t fullBar[STAGES], emptyBar[STAGES], accFull[2], accEmpty[2];
   __shared__ uint32_t tmemBase;
   unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nt = blockIdx.x, mt = blockIdx.y;
-  const int2 kr = P.kRange[nt];
-  const int nkb = kr.y - kr.x;
+  const int nTiles = P.nTilesN * P.nTilesM;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&fullBar[s], 1);
       mbar_init(&emptyBar[s], 1);
     }
-    mbar_init(&accBar, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&accFull[a], 1);
+      mbar_init(&accEmpty[a], 4);     // one arrival per epilogue warp
+    }
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -170,96 +174,127 @@ __global__ void __launch_bounds__(kThreads, 1)
   fence_after_sync();
   const uint32_t tmem = tmemBase;
 
+  // Tiles t = blockIdx.x, + gridDim.x, ...: column tile t % nTilesN of row tile
+  // t / nTilesN, so the CTAs at work share the rows of I in L2.
   if (warp == 0) {
     if (lane == 0) {
       // producer: TMA loads of the four operand tiles of each K-block
-      int issued = 0;
-      for (int i = 0; i < nkb; ++i) {
-        const int s = i % STAGES;
-        if (i >= STAGES && !wait_phase(&emptyBar[s], ((i / STAGES) - 1) & 1)) {
-          raise_flag(P.errFlag, CT_WAIT_EMPTY);
-          break;
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x) {
+        const int nt = t % P.nTilesN, mt = t / P.nTilesN;
+        const int2 kr = P.kRange[nt];
+        for (int i = kr.x; i < kr.y; ++i, ++it) {
+          const int s = it % STAGES;
+          if (it >= STAGES && !wait_phase(&emptyBar[s], ((it / STAGES) - 1) & 1)) {
+            raise_flag(P.errFlag, CT_WAIT_EMPTY);
+            ok = false;
+            break;
+          }
+          unsigned char *st = smem + s * STAGE_BYTES;
+          mbar_arrive_expect_tx(&fullBar[s], STAGE_BYTES);
+          const int kx = i * BK;
+          tma_load_2d(st, &tmAhi, kx, mt * BM, &fullBar[s]);
+          tma_load_2d(st + A_TILE, &tmAlo, kx, mt * BM, &fullBar[s]);
+          tma_load_2d(st + 2 * A_TILE, &tmBhi, kx, nt * BN, &fullBar[s]);
+          tma_load_2d(st + 2 * A_TILE + B_TILE, &tmBlo, kx, nt * BN, &fullBar[s]);
         }
-        unsigned char *st = smem + s * STAGE_BYTES;
-        mbar_arrive_expect_tx(&fullBar[s], STAGE_BYTES);
-        const int kx = (kr.x + i) * BK;
-        tma_load_2d(st, &tmAhi, kx, mt * BM, &fullBar[s]);
-        tma_load_2d(st + A_TILE, &tmAlo, kx, mt * BM, &fullBar[s]);
-        tma_load_2d(st + 2 * A_TILE, &tmBhi, kx, nt * BN, &fullBar[s]);
-        tma_load_2d(st + 2 * A_TILE + B_TILE, &tmBlo, kx, nt * BN, &fullBar[s]);
-        ++issued;
       }
       // every copy issued has landed before the CTA may exit
-      for (int i = max(0, issued - STAGES); i < issued; ++i)
+      for (int i = max(0, it - STAGES); i < it; ++i)
         if (!wait_phase(&fullBar[i % STAGES], (i / STAGES) & 1)) raise_flag(P.errFlag, CT_WAIT_DRAIN);
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      // MMA issuer: three bf16 products per K step into one FP32 accumulator
-      int done = 0;
-      for (int i = 0; i < nkb; ++i) {
-        const int s = i % STAGES;
-        if (!wait_phase(&fullBar[s], (i / STAGES) & 1)) {
-          raise_flag(P.errFlag, CT_WAIT_FULL);
+      // MMA issuer: three bf16 products per K step, accumulators alternating
+      // between two TMEM buffers so the epilogue of one tile overlaps the next
+      int it = 0, j = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x, ++j) {
+        const int nt = t % P.nTilesN, acc = j & 1;
+        const int2 kr = P.kRange[nt];
+        if (j >= 2 && !wait_phase(&accEmpty[acc], ((j >> 1) - 1) & 1)) {
+          raise_flag(P.errFlag, CT_WAIT_ACC);
           break;
         }
         fence_after_sync();
-        const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t d = tmem + (uint32_t)(acc * BN);
+        int done = 0;
+        for (int i = kr.x; i < kr.y; ++i, ++it) {
+          const int s = it % STAGES;
+          if (!wait_phase(&fullBar[s], (it / STAGES) & 1)) {
+            raise_flag(P.errFlag, CT_WAIT_FULL);
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+          const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
 #pragma unroll
-        for (int k = 0; k < BK / 16; ++k) {
-          const uint32_t off = k * 32;   // 16 bf16 along K inside the 128-byte swizzle row
-          const uint64_t aHi = smem_desc(base + off), aLo = smem_desc(base + A_TILE + off);
-          const uint64_t bHi = smem_desc(base + 2 * A_TILE + off), bLo = smem_desc(base + 2 * A_TILE + B_TILE + off);
-          umma_bf16(tmem, aHi, bHi, (i > 0 || k > 0) ? 1u : 0u);
-          umma_bf16(tmem, aHi, bLo, 1u);
-          umma_bf16(tmem, aLo, bHi, 1u);
+          for (int k = 0; k < BK / 16; ++k) {
+            const uint32_t off = k * 32;   // 16 bf16 along K inside the 128-byte swizzle row
+            const uint64_t aHi = smem_desc(base + off), aLo = smem_desc(base + A_TILE + off);
+            const uint64_t bHi = smem_desc(base + 2 * A_TILE + off), bLo = smem_desc(base + 2 * A_TILE + B_TILE + off);
+            umma_bf16(d, aHi, bHi, (done > 0 || k > 0) ? 1u : 0u);
+            umma_bf16(d, aHi, bLo, 1u);
+            umma_bf16(d, aLo, bHi, 1u);
+          }
+          umma_commit(&emptyBar[s]);
+          ++done;
         }
-        umma_commit(&emptyBar[s]);
-        ++done;
-      }
-      if (done > 0) {
-        umma_commit(&accBar);        // arrives once every MMA above has completed
-        // the accumulator is freed below only after the MMAs that write it are done
-        if (!wait_phase(&accBar, 0)) raise_flag(P.errFlag, CT_WAIT_ACC);
-      } else {
-        mbar_arrive(&accBar);        // empty band: nothing in flight
+        if (done > 0)
+          umma_commit(&accFull[acc]);   // arrives once every MMA of the tile has completed
+        else
+          mbar_arrive(&accFull[acc]);   // empty band (or a failed wait): nothing in flight
       }
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, one replica row per thread
-    const int q = warp & 3, row = q * 32 + lane, grow = mt * BM + row;
-    const bool ok = __all_sync(0xffffffffu, wait_phase(&accBar, 0));
-    if (!ok && lane == 0) raise_flag(P.errFlag, CT_WAIT_ACC);
-    fence_after_sync();
-    double chi = 0.0;
-    float v[32];
-    for (int c = 0; c < BN; c += 32) {
-      if (nkb > 0 && ok) {
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] = 0.f;
+    const int q = warp & 3;
+    int j = 0;
+    for (int t = blockIdx.x; t < nTiles; t += gridDim.x, ++j) {
+      const int nt = t % P.nTilesN, mt = t / P.nTilesN, acc = j & 1;
+      const int2 kr = P.kRange[nt];
+      const int row = q * 32 + lane, grow = mt * BM + row;
+      const bool ok = __all_sync(0xffffffffu, wait_phase(&accFull[acc], (j >> 1) & 1));
+      if (!ok) {
+        if (lane == 0) raise_flag(P.errFlag, CT_WAIT_ACC);
+        break;
       }
-      if (grow < P.M) {
-        const int col0 = nt * BN + c;
-        const bool vecStore = P.Y && col0 + 32 <= P.N && (P.N & 3) == 0;
-        if (vecStore) {
-          float4 *dst = reinterpret_cast<float4 *>(P.Y + (size_t)grow * P.N + col0);
+      fence_after_sync();
+      double chi = 0.0;
+      float v[32];
+      for (int c = 0; c < BN; c += 32) {
+        if (kr.y > kr.x) {
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
+        } else {
 #pragma unroll
-          for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+          for (int jj = 0; jj < 32; ++jj) v[jj] = 0.f;
         }
+        if (grow < P.M) {
+          const int col0 = nt * BN + c;
+          const bool vecStore = P.Y && col0 + 32 <= P.N && (P.N & 3) == 0;
+          if (vecStore) {
+            float4 *dst = reinterpret_cast<float4 *>(P.Y + (size_t)grow * P.N + col0);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = col0 + j;
-          if (col < P.N) {
-            if (P.Y && !vecStore) P.Y[(size_t)grow * P.N + col] = v[j];
-            const double d = (double)P.yobs[col] - (double)v[j];
-            chi += (double)P.w[col] * d * d;
+            for (int jj = 0; jj < 8; ++jj) dst[jj] = make_float4(v[4 * jj], v[4 * jj + 1], v[4 * jj + 2], v[4 * jj + 3]);
+          }
+#pragma unroll
+          for (int jj = 0; jj < 32; ++jj) {
+            const int col = col0 + jj;
+            if (col < P.N) {
+              if (P.Y && !vecStore) P.Y[(size_t)grow * P.N + col] = v[jj];
+              const double dd = (double)__ldg(P.yobs + col) - (double)v[jj];
+              chi += (double)__ldg(P.w + col) * dd * dd;
+            }
           }
         }
       }
+      if (grow < P.M) P.chiPart[(size_t)grow * P.nTilesN + nt] = chi;
+      // the accumulator buffer is free for the tile after next
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accEmpty[acc]);
     }
-    if (grow < P.M) P.chiPart[(size_t)grow * P.nTilesN + nt] = chi;
   }
   fence_before_sync();
   __syncthreads();
@@ -442,6 +477,7 @@ struct p6_ct_session {
   long long bandBlocks = 0, bandCols128 = 0;   // sum of K-blocks over BN tiles; sum of K over 128-col tiles
   CUtensorMap mapAhi, mapAlo, mapBhi, mapBlo;
   long long launches = 0;
+  int numSMs = 148;
 };
 
 static void ct_free(p6_ct_session *s) {
@@ -541,6 +577,7 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
     ct_free(s);
     return st;
   }
+  cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, device);
   e = cudaFuncSetAttribute(contract_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "cudaFuncSetAttribute"); }
   *out = s;
@@ -578,9 +615,10 @@ p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern) {
     split_kernel<<<1184, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo);
     P6_CUDA(cudaGetLastError());
     Params P;
-    P.M = s->M; P.N = s->N; P.Kp = s->Kp; P.nTilesN = s->nTilesN;
+    P.M = s->M; P.N = s->N; P.Kp = s->Kp; P.nTilesN = s->nTilesN; P.nTilesM = (s->M + BM - 1) / BM;
     P.kRange = s->dRange; P.yobs = s->dYobs; P.w = s->dW; P.Y = Y; P.chiPart = s->dPart; P.errFlag = s->dErr;
-    const dim3 grid(s->nTilesN, (s->M + BM - 1) / BM);
+    // persistent: one CTA per SM, tiles handed out round-robin
+    const int grid = std::min(P.nTilesN * P.nTilesM, s->numSMs);
     contract_tc_kernel<<<grid, kThreads, SMEM_BYTES, s->stream>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo, P);
     P6_CUDA(cudaGetLastError());
     nTiles = s->nTilesN;

@@ -714,9 +714,12 @@ __device__ __forceinline__ void propose(const Params &P, WarpView &ws, const Pro
 // ---------------------------------------------------------------------------
 // The kernel.
 // ---------------------------------------------------------------------------
+// One CTA's share of a search: ladders L0, L0 + Lstep, ... of the problem P,
+// generations [gen0, gen0 + nGen).  Returns false (on every thread) when the
+// static tables could not be staged in time.
 template <int COSMODE, int SLOTS, int INCR>
-__global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, int nGen, int mcmc, int swapEvery,
-                                                    int reevalFirst) {
+__device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int gen0, int nGen, int mcmc,
+                                       int swapEvery, int reevalFirst) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t stageBar;
   __shared__ float shellLen[27];
@@ -746,12 +749,12 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, in
                         (float)((int)threadIdx.x % 3 - 1)};
     shellLen[threadIdx.x] = cart_len(P, t);
   }
-  if (!mbar_wait_bounded(&stageBar, 0, kStageWaitLimit)) {
-    raise_flag(P.errFlag, DEV_STAGE_TIMEOUT);
-    mbar_wait_bounded(&stageBar, 0, kStageWaitLimit);
-    return;
+  const bool staged = __syncthreads_and(mbar_wait_bounded(&stageBar, 0, kStageWaitLimit) ? 1 : 0) != 0;
+  if (!staged) {
+    if (threadIdx.x == 0) raise_flag(P.errFlag, DEV_STAGE_TIMEOUT);
+    mbar_wait_bounded(&stageBar, 0, kStageWaitLimit);   // copies still in flight land before the CTA moves on
+    return false;
   }
-  __syncthreads();
   const ReflRec *refl = reinterpret_cast<const ReflRec *>(stat + P.offRefl);
   const float *ftab = reinterpret_cast<const float *>(stat + P.offF);
   const float4 *groups = reinterpret_cast<const float4 *>(stat + P.offGroup);
@@ -775,7 +778,7 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, in
   float *Cb = INCR ? reinterpret_cast<float *>(wbase + P.cbOff) : nullptr;
   uint4 *atomsB[2] = {atoms, INCR ? reinterpret_cast<uint4 *>(wbase + P.atoms2Off) : atoms};
 
-  for (int L = blockIdx.x; L < nLadders; L += gridDim.x) {
+  for (int L = L0; L < nLadders; L += Lstep) {
     int p = -1;
     if (warp < rungs) {
       if (P.ladders)
@@ -1013,6 +1016,47 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const Params P, int gen0, in
         P.st[p] = st;
       }
     }
+    __syncthreads();
+  }
+  // the staging barrier is set up afresh by the next call on this CTA
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&stageBar)) : "memory");
+  __syncthreads();
+  return true;
+}
+
+template <int COSMODE, int SLOTS, int INCR>
+__global__ void __launch_bounds__(256, 4) wy_kernel(const __grid_constant__ Params P, int gen0, int nGen, int mcmc,
+                                                    int swapEvery, int reevalFirst) {
+  wy_cta<COSMODE, SLOTS, INCR>(P, blockIdx.x, gridDim.x, gen0, nGen, mcmc, swapEvery, reevalFirst);
+}
+
+// Per-problem generation range of a batched launch.
+struct RunArgs {
+  int gen0, nGen, mcmc, swapEvery, reevalFirst, pad[3];
+};
+
+// Many independent searches in one persistent launch: each CTA takes the
+// next (problem, ladder) item from a list ordered by estimated cost, copies
+// that problem's parameters into shared memory, stages its tables and runs
+// the ladder through its generations.
+template <int COSMODE, int SLOTS, int INCR>
+__global__ void __launch_bounds__(256, 4) wy_batch_kernel(const Params *probs, const RunArgs *args, const int2 *items,
+                                                          int nItems, int *counter) {
+  __shared__ __align__(16) Params Ps;
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = item;
+    if (it >= nItems) break;
+    const int2 w = items[it];
+    const int *src = reinterpret_cast<const int *>(probs + w.x);
+    int *dst = reinterpret_cast<int *>(&Ps);
+    for (int i = threadIdx.x; i < (int)(sizeof(Params) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    const RunArgs a = args[w.x];
+    // Lstep = nLadders: this ladder only
+    if (!wy_cta<COSMODE, SLOTS, INCR>(Ps, w.y, Ps.nLadders, a.gen0, a.nGen, a.mcmc, a.swapEvery, a.reevalFirst)) break;
     __syncthreads();
   }
 }
@@ -1896,6 +1940,260 @@ p6_status p6_wy_launch_count(p6_wy_session *s, long long *count) {
   P6_ENTRY();
   if (!s || !count) return set_error(P6_ERR_INVALID_ARG, "null argument");
   *count = s->launches;
+  return P6_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched searches: many sessions' ladders in one persistent launch.
+// ===========================================================================
+struct p6_wy_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<p6_wy_session *> sessions;
+  std::vector<cudaEvent_t> evSess;   // one per session: its queued work before the batch
+  std::vector<Params> hProbs;
+  std::vector<RunArgs> hArgs;
+  std::vector<int2> hItems;
+  Params *dProbs = nullptr;
+  RunArgs *dArgs = nullptr;
+  int2 *dItems = nullptr;
+  int *dCounter = nullptr;
+  int itemsCap = 0, nItems = 0;
+  int smemBytes = 0, cosMode = 0, slots = 0, numSMs = 0, maxPerSM = 1;
+  int perSM = 0;   // persistent CTAs per SM (0: the occupancy limit)
+  int order = 0;   // 0: longest estimated ladder first; 1: problem order
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graphGrid = -1;
+  long long launches = 0;
+};
+
+namespace {
+template <int C, int S>
+cudaError_t batch_attr(int smem, int *occ) {
+  auto k = wy_batch_kernel<C, S, 0>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, 256, smem);
+}
+template <int C, int S>
+void batch_launch(p6_wy_batch *b, int grid) {
+  wy_batch_kernel<C, S, 0><<<grid, 256, b->smemBytes, b->stream>>>(b->dProbs, b->dArgs, b->dItems, b->nItems,
+                                                                   b->dCounter);
+}
+cudaError_t batch_variant_attr(p6_wy_batch *b, int *occ) {
+  const int C = b->cosMode, S = b->slots;
+  if (S == 0) return C ? batch_attr<1, 0>(b->smemBytes, occ) : batch_attr<0, 0>(b->smemBytes, occ);
+  if (S == 64) return C ? batch_attr<1, 64>(b->smemBytes, occ) : batch_attr<0, 64>(b->smemBytes, occ);
+  return C ? batch_attr<1, 256>(b->smemBytes, occ) : batch_attr<0, 256>(b->smemBytes, occ);
+}
+void batch_variant_launch(p6_wy_batch *b, int grid) {
+  const int C = b->cosMode, S = b->slots;
+  if (S == 0) C ? batch_launch<1, 0>(b, grid) : batch_launch<0, 0>(b, grid);
+  else if (S == 64) C ? batch_launch<1, 64>(b, grid) : batch_launch<0, 64>(b, grid);
+  else C ? batch_launch<1, 256>(b, grid) : batch_launch<0, 256>(b, grid);
+}
+void batch_free(p6_wy_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (void *p : {(void *)b->dProbs, (void *)b->dArgs, (void *)b->dItems, (void *)b->dCounter})
+    if (p) cudaFree(p);
+  for (cudaEvent_t ev : b->evSess)
+    if (ev) cudaEventDestroy(ev);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+}  // namespace
+
+extern "C" {
+
+p6_status p6_wy_batch_create(p6_wy_session *const *sessions, int n_sessions, p6_wy_batch **out) {
+  P6_ENTRY();
+  if (!sessions || n_sessions <= 0 || !out) return set_error(P6_ERR_INVALID_ARG, "no sessions");
+  *out = nullptr;
+  for (int i = 0; i < n_sessions; ++i) {
+    const p6_wy_session *s = sessions[i];
+    if (!s) return set_error(P6_ERR_INVALID_ARG, "null session in the batch");
+    if (s->device != sessions[0]->device) return set_error(P6_ERR_INVALID_ARG, "sessions on different devices");
+    if (s->cosMode != sessions[0]->cosMode) return set_error(P6_ERR_INVALID_ARG, "sessions with different cos_mode");
+    if (s->incremental) return set_error(P6_ERR_INVALID_ARG, "batched searches use the full evaluation (incremental = 0)");
+    if (s->P.rungs > 8) return set_error(P6_ERR_CAPACITY, "batched ladders hold at most 8 rungs");
+  }
+  p6_wy_batch *b = new p6_wy_batch();
+  b->device = sessions[0]->device;
+  b->sessions.assign(sessions, sessions + n_sessions);
+  b->cosMode = sessions[0]->cosMode;
+  for (p6_wy_session *s : b->sessions) {
+    b->smemBytes = std::max(b->smemBytes, s->smemBytes);
+    b->slots = std::max(b->slots, s->slots);
+  }
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+  b->evSess.assign(n_sessions, nullptr);
+  for (int i = 0; i < n_sessions && e == cudaSuccess; ++i)
+    e = cudaEventCreateWithFlags(&b->evSess[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dProbs, sizeof(Params) * n_sessions);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dArgs, sizeof(RunArgs) * n_sessions);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dCounter, sizeof(int));
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->numSMs, cudaDevAttrMultiProcessorCount, b->device);
+  int occ = 0;
+  if (e == cudaSuccess) e = batch_variant_attr(b, &occ);
+  if (e != cudaSuccess) {
+    batch_free(b);
+    return cuda_error(e, "batch set-up");
+  }
+  if (occ < 1) {
+    batch_free(b);
+    return set_error(P6_ERR_CAPACITY, "the largest problem of the batch does not fit one CTA per SM");
+  }
+  b->maxPerSM = occ;
+  *out = b;
+  return P6_OK;
+}
+
+p6_status p6_wy_batch_destroy(p6_wy_batch *b) {
+  P6_ENTRY();
+  if (!b) return set_error(P6_ERR_INVALID_ARG, "null batch");
+  batch_free(b);
+  return P6_OK;
+}
+
+p6_status p6_wy_batch_set_launch(p6_wy_batch *b, int ctas_per_sm, int order) {
+  P6_ENTRY();
+  if (!b || ctas_per_sm < 0 || ctas_per_sm > b->maxPerSM || order < 0 || order > 1)
+    return set_error(P6_ERR_INVALID_ARG, "bad launch shape");
+  b->perSM = ctas_per_sm;
+  b->order = order;
+  return P6_OK;
+}
+
+p6_status p6_wy_batch_query(p6_wy_batch *b, int *max_ctas_per_sm, int *smem_bytes, int *n_items, long long *launches) {
+  P6_ENTRY();
+  if (!b) return set_error(P6_ERR_INVALID_ARG, "null batch");
+  if (max_ctas_per_sm) *max_ctas_per_sm = b->maxPerSM;
+  if (smem_bytes) *smem_bytes = b->smemBytes;
+  if (n_items) *n_items = b->nItems;
+  if (launches) *launches = b->launches;
+  return P6_OK;
+}
+
+p6_status p6_wy_batch_run(p6_wy_batch *b, const int32_t *gen0, const int32_t *n_gen, int swap_every, int reeval_first,
+                          int use_graph) {
+  P6_ENTRY();
+  if (!b || !gen0 || !n_gen) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaSetDevice(b->device));
+  const int n = (int)b->sessions.size();
+  b->hProbs.resize(n);
+  b->hArgs.resize(n);
+  std::vector<std::pair<double, int2>> items;
+  for (int i = 0; i < n; ++i) {
+    p6_wy_session *s = b->sessions[i];
+    if (!s->dLadders) return set_error(P6_ERR_INVALID_ARG, "a session of the batch has no ladders");
+    if (!s->dSchedG || gen0[i] < 0 || n_gen[i] <= 0 || gen0[i] + n_gen[i] > s->schedLen)
+      return set_error(P6_ERR_INVALID_ARG, "a generation range lies outside its schedule");
+    Params P = s->P;
+    P.ladders = s->dLadders;
+    P.rungs = s->rungs;
+    P.nLadders = s->nLadders;
+    P.schedGroups = s->dSchedG;
+    P.schedPen = s->dSchedP;
+    P.quenchSd = nullptr;
+    P.tracePos = nullptr;
+    P.traceRec = nullptr;
+    P.traceIc = nullptr;
+    b->hProbs[i] = P;
+    b->hArgs[i] = RunArgs{gen0[i], n_gen[i], 1, swap_every, reeval_first ? 1 : 0, {0, 0, 0}};
+    // cost of one ladder: generations x reflections x atoms entering |F|^2 x rungs
+    const double cost = (double)n_gen[i] * (double)(P.nRefl + 16) * (double)(P.nTot + 4) * (double)P.rungs;
+    for (int L = 0; L < s->nLadders; ++L) items.push_back({cost, make_int2(i, L)});
+  }
+  if (b->order == 0)
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::pair<double, int2> &x, const std::pair<double, int2> &y) { return x.first > y.first; });
+  b->hItems.resize(items.size());
+  for (size_t k = 0; k < items.size(); ++k) b->hItems[k] = items[k].second;
+  if ((int)items.size() > b->itemsCap) {
+    if (b->dItems) cudaFree(b->dItems);
+    b->dItems = nullptr;
+    b->itemsCap = 0;
+    P6_CUDA(cudaMalloc(&b->dItems, sizeof(int2) * items.size()));
+    b->itemsCap = (int)items.size();
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    b->graphGrid = -1;
+  }
+  b->nItems = (int)items.size();
+  // the batch starts after each session's queued work (state uploads) is done
+  for (int i = 0; i < n; ++i) {
+    P6_CUDA(cudaEventRecord(b->evSess[i], b->sessions[i]->stream));
+    P6_CUDA(cudaStreamWaitEvent(b->stream, b->evSess[i], 0));
+  }
+  P6_CUDA(cudaMemcpyAsync(b->dProbs, b->hProbs.data(), sizeof(Params) * n, cudaMemcpyHostToDevice, b->stream));
+  P6_CUDA(cudaMemcpyAsync(b->dArgs, b->hArgs.data(), sizeof(RunArgs) * n, cudaMemcpyHostToDevice, b->stream));
+  P6_CUDA(cudaMemcpyAsync(b->dItems, b->hItems.data(), sizeof(int2) * b->nItems, cudaMemcpyHostToDevice, b->stream));
+  const int perSM = b->perSM > 0 ? b->perSM : b->maxPerSM;
+  const int grid = std::max(1, std::min(b->nItems, perSM * b->numSMs));
+  P6_CUDA(cudaEventRecord(b->ev0, b->stream));
+  if (use_graph) {
+    if (!b->exec || b->graphGrid != grid) {
+      if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+      if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+      P6_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      cudaMemsetAsync(b->dCounter, 0, sizeof(int), b->stream);
+      batch_variant_launch(b, grid);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+      if (e != cudaSuccess) return cuda_error(e, "batch graph capture");
+      P6_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+      b->graphGrid = grid;
+    }
+    P6_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  } else {
+    P6_CUDA(cudaMemsetAsync(b->dCounter, 0, sizeof(int), b->stream));
+    batch_variant_launch(b, grid);
+    P6_CUDA(cudaGetLastError());
+  }
+  b->launches++;
+  P6_CUDA(cudaEventRecord(b->ev1, b->stream));
+  // later work on each session (state reads) waits for the batch
+  for (p6_wy_session *s : b->sessions) P6_CUDA(cudaStreamWaitEvent(s->stream, b->ev1, 0));
+  return P6_OK;
+}
+
+p6_status p6_wy_batch_synchronize(p6_wy_batch *b, double timeout_seconds) {
+  P6_ENTRY();
+  if (!b) return set_error(P6_ERR_INVALID_ARG, "null batch");
+  P6_CUDA(cudaSetDevice(b->device));
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(b->stream);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) return cuda_error(e, "cudaStreamQuery");
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > timeout_seconds) return set_error(P6_ERR_TIMEOUT, "the batch did not finish within the deadline");
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  for (p6_wy_session *s : b->sessions) {
+    const p6_status st = check_device_flag(s);
+    if (st != P6_OK) return st;
+  }
+  return P6_OK;
+}
+
+p6_status p6_wy_batch_last_ms(p6_wy_batch *b, float *ms) {
+  P6_ENTRY();
+  if (!b || !ms) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaEventSynchronize(b->ev1));
+  P6_CUDA(cudaEventElapsedTime(ms, b->ev0, b->ev1));
   return P6_OK;
 }
 

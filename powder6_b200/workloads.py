@@ -123,7 +123,7 @@ def wyckoff_problem(seed: int = 1, group_number: int = 62,
                     dmin: float = 1.2, wavelength: float = 1.5406, noise: float = 0.02,
                     windows: Sequence[dict] = (), min_contact: Optional[float] = None,
                     extra_assignments: Sequence[Sequence[Tuple[str, str]]] = (),
-                    true_min_contact: float = 1.6) -> WyckoffProblem:
+                    true_min_contact: float = 1.6, contact_attempts: int = 2000) -> WyckoffProblem:
     cell = dict(cell or {'a': 8.48, 'b': 5.40, 'c': 6.96, 'alpha': 90.0, 'beta': 90.0, 'gamma': 90.0})
     group = space_group(group_number)
     ff_table = load_form_factor_table()
@@ -134,7 +134,7 @@ def wyckoff_problem(seed: int = 1, group_number: int = 62,
     rng = np.random.default_rng(seed)
     red0 = reduced_cell(cell)
     true = np.zeros(tables.max_sites * 3)
-    for _attempt in range(2000):
+    for _attempt in range(contact_attempts):
         for si, s in enumerate(assignment.sites):
             true[si * 3:si * 3 + 3] = np.array(s.w.project(*rng.random(3))) % 1.0
         if _min_contact(group, assignment, true, red0) >= true_min_contact:
@@ -182,3 +182,88 @@ def wyckoff_problem(seed: int = 1, group_number: int = 62,
     prob.pen_bond = 0.10 / max(1, bond_slots)
     prob.pen_coord = 0.03 / max(1, coord_centres)
     return prob
+
+
+# ---------------------------------------------------------------------------
+# Batched uneven Wyckoff searches (many independent problems in one launch).
+# ---------------------------------------------------------------------------
+BATCH_GROUPS = (2, 14, 15, 62, 176, 225)       # P-1, P2_1/c, C2/c, Pnma, P6_3/m, Fm-3m
+BATCH_ELEMENTS = ('C', 'N', 'O', 'S', 'Na', 'Cl', 'Ti', 'Fe', 'Pb')
+
+
+@dataclass
+class BatchItem:
+    problem: 'WyckoffProblem'
+    replicas: int
+    points: int
+    target_reflections: int
+
+
+def _log_uniform(rng, lo, hi):
+    return float(np.exp(rng.uniform(math.log(lo), math.log(hi))))
+
+
+def _random_cell(rng, system: str) -> Dict[str, float]:
+    a, b, c = (rng.uniform(4.0, 20.0) for _ in range(3))
+    if system == 'triclinic':
+        return {'a': a, 'b': b, 'c': c, 'alpha': rng.uniform(75, 105), 'beta': rng.uniform(75, 105),
+                'gamma': rng.uniform(75, 105)}
+    if system == 'monoclinic':
+        return {'a': a, 'b': b, 'c': c, 'alpha': 90.0, 'beta': rng.uniform(92, 118), 'gamma': 90.0}
+    if system == 'orthorhombic':
+        return {'a': a, 'b': b, 'c': c, 'alpha': 90.0, 'beta': 90.0, 'gamma': 90.0}
+    if system == 'hexagonal':
+        return {'a': a, 'b': a, 'c': c, 'alpha': 90.0, 'beta': 90.0, 'gamma': 120.0}
+    return {'a': a, 'b': a, 'c': a, 'alpha': 90.0, 'beta': 90.0, 'gamma': 90.0}
+
+
+def _cell_volume(cell) -> float:
+    al, be, ga = (math.radians(cell[k]) for k in ('alpha', 'beta', 'gamma'))
+    return cell['a'] * cell['b'] * cell['c'] * math.sqrt(
+        max(1e-12, 1 - math.cos(al) ** 2 - math.cos(be) ** 2 - math.cos(ga) ** 2
+            + 2 * math.cos(al) * math.cos(be) * math.cos(ga)))
+
+
+def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelength: float = 1.5406):
+    """Seeded uneven problems: space groups from BATCH_GROUPS, 1-24 sites and
+    50-3000 reflections and 2000-12000 points and 256-2048 replicas (all
+    log-uniform), cells uniform in 4-20 A, at most ``max_atoms`` atoms per
+    cell (resampled otherwise).  The reflection count sets d_min through the
+    volume of the reciprocal sphere; the point count is recorded only (the
+    search's fitness works on integrated intensities)."""
+    from .symmetry import space_group
+    rng = np.random.default_rng(seed)
+    out: List[BatchItem] = []
+    while len(out) < n:
+        g = space_group(int(rng.choice(BATCH_GROUPS)))
+        cell = _random_cell(rng, g.system)
+        n_sites = max(1, min(24, int(round(_log_uniform(rng, 1, 24)))))
+        free = [w for w in g.wyckoff if w.n_free > 0]
+        weights = np.array([1.0 / w.multiplicity ** 0.5 for w in free])
+        labels, atoms = [], 0
+        palette = list(rng.choice(BATCH_ELEMENTS, size=int(rng.integers(1, 5)), replace=False))
+        for _ in range(n_sites):
+            w = free[int(rng.choice(len(free), p=weights / weights.sum()))]
+            el = str(rng.choice(palette))
+            labels.append((el, f'{w.multiplicity}{w.letter}'))
+            atoms += w.multiplicity
+        if atoms > max_atoms:
+            continue
+        comp: Dict[str, int] = {}
+        for el, lab in labels:
+            comp[el] = comp.get(el, 0) + int(lab[:-1])
+        target = int(round(_log_uniform(rng, 50, 3000)))
+        n_pg = len({o.r for o in g.ops})
+        n_c = len(g.ops) // n_pg
+        vol = _cell_volume(cell)
+        dmin = (4 * math.pi * vol / (3 * 2 * n_pg * n_c * target)) ** (1.0 / 3.0)
+        dmin = max(dmin, wavelength / 2 * 1.0001)
+        prob = wyckoff_problem(seed=int(rng.integers(1 << 30)), group_number=g.number, cell=cell,
+                               composition=tuple(comp.items()), sites=tuple(labels), dmin=dmin,
+                               wavelength=wavelength, true_min_contact=1.0, contact_attempts=40)
+        if prob.refl.n_refl < 8:
+            continue
+        replicas = int(round(_log_uniform(rng, 256, 2048) / 8)) * 8
+        points = int(round(_log_uniform(rng, 2000, 12000)))
+        out.append(BatchItem(prob, replicas, points, target))
+    return out

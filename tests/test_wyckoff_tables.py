@@ -139,3 +139,19 @@ def test_ladders_and_schedule():
     g, p = schedule(5000, 87)
     assert g[0] == 22 and g[-1] == 87 and p[0] == np.float32(0.2) and p[-1] == np.float32(4.0)
     assert np.all(np.diff(g) >= 0) and len(set(g.tolist())) <= 24
+
+
+def test_batched_problem_generator():
+    """Uneven batch: the six space groups, 1-24 sites, at most 512 atoms per cell,
+    replicas 256-2048 in multiples of 8, points 2000-12000."""
+    from powder6_b200.workloads import BATCH_GROUPS, batched_problems
+    items = batched_problems(12, seed=4)
+    assert len(items) == 12
+    for it in items:
+        P = it.problem
+        assert P.group.number in BATCH_GROUPS
+        assert 1 <= P.max_sites <= 24
+        assert sum(d['count'] for d in P.demand) <= 512
+        assert 256 <= it.replicas <= 2048 and it.replicas % 8 == 0
+        assert 2000 <= it.points <= 12000
+        assert P.refl.n_refl >= 8
