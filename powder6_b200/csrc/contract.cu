@@ -18,10 +18,11 @@
 //    operands) into a two-stage shared-memory ring; warp 1 issues
 //    tcgen05.mma (M 128, N 256, K 16) into one of two TMEM accumulators
 //    (alternating per tile, so one tile's epilogue overlaps the next tile's
-//    MMAs) and commits each stage back to the producer; warps 2-5 read the
-//    accumulator with
-//    tcgen05.ld and reduce the weighted residual against the observed
-//    pattern in FP64 (the only FP64 on this path), optionally storing Y;
+//    MMAs) and commits each stage back to the producer; warps 2-17 (four
+//    per TMEM lane quarter, 64 of the tile's columns each) read the
+//    accumulator with tcgen05.ld and reduce the weighted residual against
+//    the observed pattern (terms in FP32, sums in FP64, the only FP64 on
+//    this path), optionally storing Y;
 //  * per-tile chi^2 partials are summed per replica in a fixed order.
 // A plain FP32 CUDA-core kernel over the same bands is the comparison
 // method.  Every device wait is bounded; a wait that runs out records an
@@ -47,7 +48,9 @@ constexpr int A_TILE = BM * BK * 2;                       // 16 KB per bf16 oper
 constexpr int B_TILE = BN * BK * 2;                       // 32 KB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;      // 96 KB: A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack (1024-B swizzle atoms)
-constexpr int kThreads = 192;                             // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kEpiWarps = 16;                             // four per TMEM lane quarter
+constexpr int kEpiSpan = BN / (kEpiWarps / 4);              // columns per epilogue warp (64)
+constexpr int kThreads = 64 + 32 * kEpiWarps;               // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
 constexpr uint32_t TMEM_COLS = 2 * BN;                    // two accumulator buffers
 constexpr unsigned long long kWaitNs = 2000000000ull;     // 2 s per wait
 
@@ -61,7 +64,7 @@ struct Params {
   const int2 *kRange;     // per BN tile: K-blocks [x, y)
   const float *yobs, *w;  // N
   float *Y;               // optional, M x N
-  double *chiPart;        // M x nTilesN
+  double *chiPart;        // M x nTilesN x (epilogue warps per lane quarter)
   int *errFlag;
 };
 
@@ -141,6 +144,28 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 64 columns: one load, one wait.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, "
+      "%38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, "
+      "%60, %61, %62, %63}, [%64];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
+        "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
+        "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]),
+        "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
+        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     contract_tc_kernel(const __grid_constant__ CUtensorMap tmAhi, const __grid_constant__ CUtensorMap tmAlo,
                        const __grid_constant__ CUtensorMap tmBhi, const __grid_constant__ CUtensorMap tmBlo,
@@ -159,7 +184,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&accFull[a], 1);
-      mbar_init(&accEmpty[a], 4);     // one arrival per epilogue warp
+      mbar_init(&accEmpty[a], kEpiWarps);   // one arrival per epilogue warp
     }
     fence_mbar_init();
   }
@@ -248,8 +273,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, one replica row per thread
-    const int q = warp & 3;
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (one replica row per
+    // thread) and columns kEpiSpan * part .. + kEpiSpan of the tile; the terms
+    // w (y - y_calc)^2 are formed in FP32 and summed in FP64
+    const int q = warp & 3, part = (warp - 2) >> 2, cBeg = part * kEpiSpan;
+    const int slots = kEpiWarps / 4;
     int j = 0;
     for (int t = blockIdx.x; t < nTiles; t += gridDim.x, ++j) {
       const int nt = t % P.nTilesN, mt = t / P.nTilesN, acc = j & 1;
@@ -261,35 +289,49 @@ __global__ void __launch_bounds__(kThreads, 1)
         break;
       }
       fence_after_sync();
-      double chi = 0.0;
-      float v[32];
-      for (int c = 0; c < BN; c += 32) {
-        if (kr.y > kr.x) {
-          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
-        } else {
+      float v[kEpiSpan];
+      if (kr.y > kr.x) {
+        tmem_ld64(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + cBeg), v);
+      } else {
 #pragma unroll
-          for (int jj = 0; jj < 32; ++jj) v[jj] = 0.f;
-        }
-        if (grow < P.M) {
-          const int col0 = nt * BN + c;
-          const bool vecStore = P.Y && col0 + 32 <= P.N && (P.N & 3) == 0;
-          if (vecStore) {
+        for (int jj = 0; jj < kEpiSpan; ++jj) v[jj] = 0.f;
+      }
+      double chi0 = 0.0, chi1 = 0.0;
+      if (grow < P.M) {
+        const int col0 = nt * BN + cBeg;
+        if (col0 + kEpiSpan <= P.N) {
+          // whole span inside the pattern: vector loads of the observed counts and weights
+          const float4 *yo4 = reinterpret_cast<const float4 *>(P.yobs + col0);
+          const float4 *w4 = reinterpret_cast<const float4 *>(P.w + col0);
+#pragma unroll
+          for (int g = 0; g < kEpiSpan / 4; ++g) {
+            const float4 yo = __ldg(yo4 + g), ww = __ldg(w4 + g);
+            const float d0 = yo.x - v[4 * g], d1 = yo.y - v[4 * g + 1], d2 = yo.z - v[4 * g + 2], d3 = yo.w - v[4 * g + 3];
+            chi0 += (double)(ww.x * d0 * d0) + (double)(ww.y * d1 * d1);
+            chi1 += (double)(ww.z * d2 * d2) + (double)(ww.w * d3 * d3);
+          }
+          if (P.Y && (P.N & 3) == 0) {
             float4 *dst = reinterpret_cast<float4 *>(P.Y + (size_t)grow * P.N + col0);
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) dst[jj] = make_float4(v[4 * jj], v[4 * jj + 1], v[4 * jj + 2], v[4 * jj + 3]);
-          }
+            for (int g = 0; g < kEpiSpan / 4; ++g)
+              dst[g] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+          } else if (P.Y) {
 #pragma unroll
-          for (int jj = 0; jj < 32; ++jj) {
+            for (int jj = 0; jj < kEpiSpan; ++jj) P.Y[(size_t)grow * P.N + col0 + jj] = v[jj];
+          }
+        } else {
+#pragma unroll
+          for (int jj = 0; jj < kEpiSpan; ++jj) {
             const int col = col0 + jj;
             if (col < P.N) {
-              if (P.Y && !vecStore) P.Y[(size_t)grow * P.N + col] = v[jj];
-              const double dd = (double)__ldg(P.yobs + col) - (double)v[jj];
-              chi += (double)__ldg(P.w + col) * dd * dd;
+              if (P.Y) P.Y[(size_t)grow * P.N + col] = v[jj];
+              const float dd = __ldg(P.yobs + col) - v[jj];
+              chi0 += (double)(__ldg(P.w + col) * dd * dd);
             }
           }
         }
+        P.chiPart[((size_t)grow * P.nTilesN + nt) * slots + part] = chi0 + chi1;
       }
-      if (grow < P.M) P.chiPart[(size_t)grow * P.nTilesN + nt] = chi;
       // the accumulator buffer is free for the tile after next
       fence_before_sync();
       __syncwarp();
@@ -552,7 +594,7 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
   CT_ALLOC(s->dI, M * K * sizeof(float));
   CT_ALLOC(s->dYobs, N * sizeof(float));
   CT_ALLOC(s->dW, N * sizeof(float));
-  CT_ALLOC(s->dPart, M * std::max(s->nTilesN, s->nTiles128) * sizeof(double));
+  CT_ALLOC(s->dPart, M * std::max((size_t)s->nTilesN * (kEpiWarps / 4), (size_t)s->nTiles128) * sizeof(double));
   CT_ALLOC(s->dChi, M * sizeof(double));
   CT_ALLOC(s->dRange, kb.size() * sizeof(int2));
   CT_ALLOC(s->dRange128, r128.size() * sizeof(int2));
@@ -621,7 +663,7 @@ p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern) {
     const int grid = std::min(P.nTilesN * P.nTilesM, s->numSMs);
     contract_tc_kernel<<<grid, kThreads, SMEM_BYTES, s->stream>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo, P);
     P6_CUDA(cudaGetLastError());
-    nTiles = s->nTilesN;
+    nTiles = s->nTilesN * (kEpiWarps / 4);   // per replica: tiles x epilogue slots, in order
     s->launches += 2;
   } else {
     const dim3 grid(s->nTiles128, (s->M + FM - 1) / FM);
