@@ -347,17 +347,36 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // Split of an FP32 matrix (rows x cols, leading dimension ld) into bf16 hi/lo
-// parts (rows x Kp, zero padded to Kp columns).
+// parts (rows x Kp, zero padded to Kp columns, Kp a multiple of 4): four
+// columns per thread, 16-byte loads where the row stride allows, 8-byte stores.
+__device__ __forceinline__ void split4(const float x[4], __nv_bfloat16 *hi, __nv_bfloat16 *lo, size_t at) {
+  __align__(8) __nv_bfloat16 h[4], l[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    h[i] = __float2bfloat16_rn(x[i]);
+    l[i] = __float2bfloat16_rn(x[i] - __bfloat162float(h[i]));
+  }
+  *reinterpret_cast<uint2 *>(hi + at) = *reinterpret_cast<const uint2 *>(h);
+  *reinterpret_cast<uint2 *>(lo + at) = *reinterpret_cast<const uint2 *>(l);
+}
+
 __global__ void split_kernel(const float *src, int rows, int cols, int ld, int Kp, __nv_bfloat16 *hi,
                              __nv_bfloat16 *lo) {
-  const size_t total = (size_t)rows * Kp;
+  const int q = Kp / 4;
+  const size_t total = (size_t)rows * q;
+  const bool vec = (ld & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const size_t r = i / Kp;
-    const int k = (int)(i - r * Kp);
-    const float x = k < cols ? src[r * ld + k] : 0.f;
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    hi[i] = h;
-    lo[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+    const size_t r = i / q;
+    const int k = (int)(i - r * q) * 4;
+    float x[4];
+    if (vec && k + 3 < cols) {
+      const float4 f = __ldg(reinterpret_cast<const float4 *>(src + r * ld + k));
+      x[0] = f.x; x[1] = f.y; x[2] = f.z; x[3] = f.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[j] = k + j < cols ? src[r * ld + k + j] : 0.f;
+    }
+    split4(x, hi, lo, r * Kp + k);
   }
 }
 
@@ -608,7 +627,7 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
   cudaMemcpyAsync(s->dW, pr->w, N * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dRange, kb.data(), kb.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dRange128, r128.data(), r128.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
-  split_kernel<<<1184, 256, 0, s->stream>>>(s->dPT, s->N, s->K, s->K, s->Kp, s->dBhi, s->dBlo);
+  split_kernel<<<2368, 256, 0, s->stream>>>(s->dPT, s->N, s->K, s->K, s->Kp, s->dBhi, s->dBlo);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "profile upload"); }
@@ -654,7 +673,7 @@ p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern) {
   P6_CUDA(cudaEventRecord(s->ev0, s->stream));
   int nTiles;
   if (method == P6_CT_SPLIT_BF16) {
-    split_kernel<<<1184, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo);
+    split_kernel<<<2368, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo);
     P6_CUDA(cudaGetLastError());
     Params P;
     P.M = s->M; P.N = s->N; P.Kp = s->Kp; P.nTilesN = s->nTilesN; P.nTilesM = (s->M + BM - 1) / BM;
