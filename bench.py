@@ -50,9 +50,10 @@ def parse():
     ap.add_argument('--generations', type=int, default=GENERATIONS)
     ap.add_argument('--cos-mode', type=int, default=0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt', 'contract'],
+    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt', 'contract', 'batch'],
                     help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit; '
-                         'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000)')
+                         'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000); '
+                         'batch: 64 uneven Wyckoff searches in one persistent launch')
     ap.add_argument('--method', default='split', choices=['split', 'fp32'],
                     help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
     ap.add_argument('--chains', type=int, default=64)
@@ -146,6 +147,60 @@ def cpu_baseline(P, groups, pen, n_particles, seconds=10.0):
     return {'value': trials / dt, 'unit': 'trials/s', 'cores': O.num_threads(), 'kind': 'port',
             'sample': f'{n_particles} replicas x {used} generations spread evenly over the 5000-generation '
                       f'schedule ({trials} trials, {dt:.1f} s, FP64, OpenMP over replicas)'}
+
+
+def wyckoff_time_to_target(P, n, sess):
+    """Time to target wR2 (outside the timed region): the converged wR2 is the
+    quenched winner of a full 5000-generation search; the target is 1.05 x
+    that wR2; the clock runs from the start of run_wyckoff_search (random
+    start, generations in chunks of 250 so the best can be read between
+    launches) to the first chunk boundary, or the end of the quench, at
+    which the best wR2 is within the target."""
+    from powder6_b200.swarm_wyckoff import run_wyckoff_search
+    conv = run_wyckoff_search(P, num_particles=n, generations=GENERATIONS, seed=11, session=sess)
+    wr2 = 1.0 - conv.best_cc
+    target = 1.0 - 1.05 * wr2
+    runs = [run_wyckoff_search(P, num_particles=n, generations=GENERATIONS, seed=101 + k, chunk=250, session=sess,
+                               target_cc=target) for k in range(3)]
+    hits = [r.time_to_target for r in runs if r.time_to_target is not None]
+    return {'median_s': float(np.median(hits)) if hits else None, 'reached': f'{len(hits)}/{len(runs)}',
+            'converged_wr2': wr2, 'target_wr2': 1.05 * wr2,
+            'final_wr2': [1.0 - r.best_cc for r in runs], 'cpu_check_delta': [r.cpu_check.get('delta') for r in runs],
+            'note': 'chunks of 250 generations; plain FP32 search (SFU cosine) + quench'}
+
+
+def run_reference_batch(args, world, rank):
+    """The FP64 oracle port of the trial evaluation on a bounded sample of the
+    batch (all host threads): the reference runs one search per worker."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from powder6_b200.swarm_wyckoff import schedule
+    from powder6_b200.workloads import batched_problems
+    items = batched_problems(64, seed=1)
+    trials, t_used = 0, 0.0
+    for _ in range(args.warmup):
+        it = items[0]
+        O.WyckoffCpuRunner(it.problem, min(it.replicas, 256), seed=3).generation(it.problem.refl.n_groups, 1.0)
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < 2.0 * args.steps and k < len(items):
+        it = items[k]
+        g, pen = schedule(BATCH_GENERATIONS, it.problem.refl.n_groups)
+        r = O.WyckoffCpuRunner(it.problem, it.replicas, seed=3)
+        trials += r.generation(int(g[len(g) // 2]), float(pen[len(g) // 2]))
+        k += 1
+    dt = time.perf_counter() - t0
+    v = trials / dt
+    sample = f'one mid-schedule generation of each of the first {k} searches ({trials} trials, FP64 oracle port, OpenMP)'
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'trial structures evaluated/s', 'value': v, 'unit': 'trials/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000 * dt / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': '64 uneven Wyckoff searches (sampled)'},
+        'cpu_baseline': {'value': v, 'unit': 'trials/s', 'cores': O.num_threads(), 'kind': 'port', 'sample': sample},
+        'e2e': {'value': v, 'unit': 'trials/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
 
 
 def dist_setup(args):
@@ -489,6 +544,111 @@ def main_ct(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+BATCH_GENERATIONS = 2000
+
+
+def main_batch(args, world, rank, local):
+    """One step = all 64 uneven searches (space groups P-1, P2_1/c, C2/c, Pnma,
+    P6_3/m, Fm-3m; 1-24 sites; 256-2048 replicas) through BATCH_GENERATIONS
+    generations each, in one persistent launch replayed from a CUDA graph,
+    with the launch shape the autotuner picked.  value: replica-generations
+    per second (CUDA events); the same searches launched one after another
+    are timed beside it ('sequential')."""
+    import torch
+    from powder6_b200.batch import WyckoffBatch, autotune, reset, setup_searches
+    from powder6_b200.swarm_wyckoff import SW_DEFAULTS, schedule
+    from powder6_b200.workloads import batched_problems
+    torch.cuda.set_device(local)
+    items = batched_problems(64, seed=1 + rank)
+    setup = setup_searches(items, BATCH_GENERATIONS, seed=1 + rank)
+    n = len(setup.sessions)
+    swap = int(SW_DEFAULTS['swapEvery'])
+    try:
+        with WyckoffBatch(setup.sessions) as b:
+            tuning = autotune(b, setup)
+            for _ in range(args.warmup):
+                reset(setup)
+                b.run([0] * n, setup.generations, swap, True, use_graph=True)
+                b.synchronize()
+            barrier(world)
+            l0 = b.query()['launches']
+            times = []
+            with ClockSampler(local) as clk:
+                for _ in range(args.steps):
+                    reset(setup)
+                    torch.cuda.synchronize()
+                    b.run([0] * n, setup.generations, swap, True, use_graph=True)
+                    b.synchronize()
+                    times.append(b.last_ms())
+            launches = b.query()['launches'] - l0
+            q = b.query()
+        # the same searches, one launch each
+        reset(setup)
+        seq = 0.0
+        for s_ in setup.sessions:
+            s_.run(0, BATCH_GENERATIONS, swap, True)
+            s_.synchronize(600)
+            seq += s_.last_kernel_ms()
+        # end to end: host states in, one batched run, states out
+        e2e = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            reset(setup)
+            b2 = WyckoffBatch(setup.sessions)
+            b2.set_launch(tuning['ctas_per_sm'], tuning['order'])
+            b2.run([0] * n, setup.generations, swap, True, use_graph=False)
+            b2.synchronize()
+            for s_ in setup.sessions:
+                s_.read_state()
+            e2e.append(time.perf_counter() - t0)
+            b2.close()
+        trials = int(sum(s_.num_particles * g for s_, g in zip(setup.sessions, setup.generations)))
+        cos_total = 0
+        for it, s_ in zip(items, setup.sessions):
+            g, _ = schedule(BATCH_GENERATIONS, it.problem.refl.n_groups)
+            cos_total += algorithmic_cos(it.problem, g, s_.num_particles)[0]
+        h2d = sum(s_.num_particles * (s_.coords_per_particle * 4 + 48) for s_ in setup.sessions)
+        d2h = sum(s_.num_particles * (2 * s_.coords_per_particle * 4 + 48) for s_ in setup.sessions)
+    finally:
+        for s_ in setup.sessions:
+            s_.close()
+    total_ms = max_over_ranks(float(sum(times)), world)
+    value = world * trials * args.steps / (total_ms / 1000.0)
+    e2e_total = max_over_ranks(float(sum(e2e)), world)
+    if rank == 0:
+        clocks = clk.summary()
+        ms = float(np.mean(times))
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clocks['sm_mhz'] or 1965.0
+        peak = MUFU_PER_CLK_PER_SM * nsm * mhz * 1e6 / 1e9
+        achieved = cos_total / (ms / 1000.0) / 1e9
+        refl = [it.problem.refl.n_refl for it in items]
+        line = {
+            'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp32', 'data': 'synthetic',
+            'config': {'workload': f'{n} uneven Wyckoff searches in one persistent launch (CUDA graph): space groups '
+                                   f'P-1, P2_1/c, C2/c, Pnma, P6_3/m, Fm-3m; 1-24 sites; {min(refl)}-{max(refl)} '
+                                   f'reflections; 256-2048 replicas; {BATCH_GENERATIONS} generations each',
+                       'replicas_total': int(sum(s_ for s_ in [it.replicas for it in items])),
+                       'step': 'every search through all its generations, one launch',
+                       'l2': 'per-search tables are re-staged by each CTA; states re-uploaded before each step',
+                       'tuning': {k: tuning[k] for k in ('ctas_per_sm', 'order', 'probe_ms')},
+                       'smem_bytes': q['smem_bytes'], 'items': q['items'],
+                       'sequential_ms': seq, 'batched_speedup': seq / ms,
+                       'parallelism': f'replicas only x{world}'},
+            'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak, 'unit': 'Gcos/s', 'frac': achieved / peak,
+                         'traffic': None,
+                         'note': f'{cos_total:.4g} algorithmic cosines per step; peak = {MUFU_PER_CLK_PER_SM} SFU '
+                                 f'ops/clk/SM x {nsm} SMs x {mhz:.0f} MHz'},
+            'e2e': {'value': world * trials * args.steps / e2e_total, 'unit': 'trials/s', 'h2d_bytes_per_step': h2d,
+                    'd2h_bytes_per_step': d2h},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def measured_peak(key):
     f = ROOT / 'MEASURED_PEAKS.json'
     if f.exists():
@@ -510,11 +670,13 @@ def main():
             run_reference_pt(args, world, rank)
         elif args.workload == 'contract':
             run_reference_ct(args, world, rank)
+        elif args.workload == 'batch':
+            run_reference_batch(args, world, rank)
         else:
             run_reference(args, world, rank)
         return
-    if args.workload in ('pt', 'contract'):
-        (main_pt if args.workload == 'pt' else main_ct)(args, world, rank, local)
+    if args.workload in ('pt', 'contract', 'batch'):
+        {'pt': main_pt, 'contract': main_ct, 'batch': main_batch}[args.workload](args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -610,6 +772,8 @@ def main():
         }
         if not args.no_cpu_baseline and world == 1:
             line['cpu_baseline'] = cpu_baseline(P, groups, pen, n)
+        if world == 1 and G == GENERATIONS:
+            line['time_to_target_wr2'] = wyckoff_time_to_target(P, n, sess)
         print(json.dumps(line), flush=True)
     sess.close()
     if world > 1:
