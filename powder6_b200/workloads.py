@@ -224,13 +224,17 @@ def _cell_volume(cell) -> float:
             + 2 * math.cos(al) * math.cos(be) * math.cos(ga)))
 
 
-def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelength: float = 1.5406):
+def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelength: float = 1.5406,
+                     max_refl: int = 2400):
     """Seeded uneven problems: space groups from BATCH_GROUPS, 1-24 sites and
     50-3000 reflections and 2000-12000 points and 256-2048 replicas (all
     log-uniform), cells uniform in 4-20 A, at most ``max_atoms`` atoms per
     cell (resampled otherwise).  The reflection count sets d_min through the
-    volume of the reciprocal sphere; the point count is recorded only (the
-    search's fitness works on integrated intensities)."""
+    volume of the reciprocal sphere, capped at ``max_refl`` -- the tables of
+    a search are staged in the shared memory of each CTA, and beyond ~2400
+    reflections they no longer fit next to eight replica slices; the point
+    count is recorded only (the search's fitness works on integrated
+    intensities)."""
     from .symmetry import space_group
     rng = np.random.default_rng(seed)
     out: List[BatchItem] = []
@@ -258,10 +262,15 @@ def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelengt
         vol = _cell_volume(cell)
         dmin = (4 * math.pi * vol / (3 * 2 * n_pg * n_c * target)) ** (1.0 / 3.0)
         dmin = max(dmin, wavelength / 2 * 1.0001)
-        prob = wyckoff_problem(seed=int(rng.integers(1 << 30)), group_number=g.number, cell=cell,
-                               composition=tuple(comp.items()), sites=tuple(labels), dmin=dmin,
-                               wavelength=wavelength, true_min_contact=1.0, contact_attempts=40)
-        if prob.refl.n_refl < 8:
+        pseed = int(rng.integers(1 << 30))
+        for _retry in range(6):
+            prob = wyckoff_problem(seed=pseed, group_number=g.number, cell=cell,
+                                   composition=tuple(comp.items()), sites=tuple(labels), dmin=dmin,
+                                   wavelength=wavelength, true_min_contact=1.0, contact_attempts=40)
+            if prob.refl.n_refl <= max_refl:
+                break
+            dmin *= 1.02 * (prob.refl.n_refl / max_refl) ** (1.0 / 3.0)
+        if prob.refl.n_refl < 8 or prob.refl.n_refl > max_refl:
             continue
         replicas = int(round(_log_uniform(rng, 256, 2048) / 8)) * 8
         points = int(round(_log_uniform(rng, 2000, 12000)))
