@@ -332,6 +332,41 @@ p6_status p6_wy_batch_synchronize(p6_wy_batch *b, double timeout_seconds);
 p6_status p6_wy_batch_last_ms(p6_wy_batch *b, float *ms);
 
 /* ======================================================================== */
+/* Proposal network (learned search)                                         */
+/* ======================================================================== */
+
+/* A 3-layer MLP, d_in -> width -> width -> d_out with ReLU, trained on the
+ * GPU (FP32 master weights, Adam, masked mean-squared error with 0/1 masks)
+ * and evaluated with bf16 copies of its weights.  No reference counterpart:
+ * the reference's proposals are all random (swarm_reflection.wgsl:657-725).
+ * Parameters flatten as W1 (d_in x width, row-major), b1, W2, b2, W3
+ * (width x d_out), b3.  Host arrays: X rows x d_in, T and mask rows x d_out. */
+typedef struct p6_mlp p6_mlp;
+p6_status p6_mlp_create(int d_in, int width, int d_out, uint32_t seed, int device, p6_mlp **out);
+p6_status p6_mlp_destroy(p6_mlp *n);
+/* One generation of a learned search on session s: K candidate proposals
+ * per replica (the plain search's move distribution, with a 64-feature
+ * description each), the network's first output as the predicted fitness
+ * gain, the best-ranked candidate evaluated with the exact fitness and the
+ * usual Metropolis test (K = 1, net = NULL: the plain move, no network).
+ * Optional host outputs per replica: the chosen candidate's features
+ * (num_particles x 64), the evaluated fitness change f_new - f_old, whether
+ * it was accepted (0/1), and the predicted gain.  The network's scratch is
+ * used on the session's stream: do not train it meanwhile. */
+p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, int gen, int swap_every, int reeval_first,
+                             float *features, float *gains, float *accepted, float *scores);
+/* Copies the FP32 parameters out (get) and/or in (set); count receives their number. */
+p6_status p6_mlp_params(p6_mlp *n, float *get, const float *set, long long *count);
+/* Gradient of the loss over the given rows (flat, like the parameters) and the loss. */
+p6_status p6_mlp_gradients(p6_mlp *n, const float *X, const float *T, const float *mask, int rows, float *grad,
+                           float *loss);
+/* `epochs` passes of Adam over shuffled minibatches; epoch_loss (may be NULL) gets the mean loss of each. */
+p6_status p6_mlp_train(p6_mlp *n, const float *X, const float *T, const float *mask, int rows, int epochs, int batch,
+                       float lr, uint32_t seed, float *epoch_loss);
+/* Inference with the bf16 weights: Y (rows x d_out). */
+p6_status p6_mlp_predict(p6_mlp *n, const float *X, int rows, float *Y);
+
+/* ======================================================================== */
 /* Profile contraction with the cell and profile fixed                       */
 /* ======================================================================== */
 

@@ -394,3 +394,44 @@ def contract_fp64(intensities, profile_t, yobs, w):
     r = np.asarray(yobs, dtype=np.float64)[None, :] - Y
     chi2 = (w[None, m] * r[:, m] ** 2).sum(axis=1)
     return Y, chi2
+
+
+def mlp_unflatten(w, d_in, width, d_out):
+    """W1 (d_in x width), b1, W2, b2, W3 (width x d_out), b3 from the flat FP32 block."""
+    w = np.asarray(w, dtype=np.float64)
+    sizes = [d_in * width, width, width * width, width, width * d_out, d_out]
+    parts, o = [], 0
+    for n in sizes:
+        parts.append(w[o:o + n]); o += n
+    W1, b1, W2, b2, W3, b3 = parts
+    return W1.reshape(d_in, width), b1, W2.reshape(width, width), b2, W3.reshape(width, d_out), b3
+
+
+def mlp_forward_fp64(w, X, d_in, width, d_out):
+    """FP64 restatement of the proposal network: ReLU(X W1 + b1) -> ReLU(. W2 + b2) -> . W3 + b3."""
+    W1, b1, W2, b2, W3, b3 = mlp_unflatten(w, d_in, width, d_out)
+    H1 = np.maximum(np.asarray(X, np.float64) @ W1 + b1, 0)
+    H2 = np.maximum(H1 @ W2 + b2, 0)
+    return H2 @ W3 + b3, H1, H2
+
+
+def mlp_grads_fp64(w, X, T, mask, d_in, width, d_out):
+    """Gradient of the masked mean-squared error (1/n) sum mask (Y - T)^2 (0/1 masks), flat like w, and the loss."""
+    X = np.asarray(X, np.float64)
+    n = len(X)
+    T = np.asarray(T, np.float64).reshape(n, d_out)
+    M = np.ones_like(T) if mask is None else np.asarray(mask, np.float64).reshape(n, d_out)
+    W1, b1, W2, b2, W3, b3 = mlp_unflatten(w, d_in, width, d_out)
+    Y, H1, H2 = mlp_forward_fp64(w, X, d_in, width, d_out)
+    E = (Y - T) * M
+    loss = float((E * E).sum() / n)
+    dY = 2 * E / n
+    dW3 = H2.T @ dY
+    db3 = dY.sum(0)
+    dH2 = (dY @ W3.T) * (H2 > 0)
+    dW2 = H1.T @ dH2
+    db2 = dH2.sum(0)
+    dH1 = (dH2 @ W2.T) * (H1 > 0)
+    dW1 = X.T @ dH1
+    db1 = dH1.sum(0)
+    return np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dW3.ravel(), db3]), loss

@@ -33,6 +33,7 @@
 #include <thread>
 #include <vector>
 
+#include "mlp_internal.h"
 #include "p6_common.cuh"
 
 namespace p6 {
@@ -106,6 +107,7 @@ struct Params {
   const int *schedGroups;  // per generation; null: use ngaArg/penArg
   const float *schedPen;
   const float *quenchSd;   // per generation: greedy quench with this step; null: Metropolis with adapted steps
+  const uint32_t *extProp; // per particle: the proposal to evaluate (learned search); null: the kernel proposes
   int ngaArg;
   float penArg;
   uint32_t *tracePos;
@@ -860,7 +862,15 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
         if (mcmc) {
           float uMetro;
           const float sd = P.quenchSd ? P.quenchSd[g] : __shfl_sync(0xffffffffu, step, 0);
-          propose(P, ws, proj, g, p, lane, sd, seed, &uMetro);
+          if (P.extProp) {
+            // a proposal chosen outside (the learned search): the Metropolis draw stays ours
+            for (int j = lane; j < (int)curStride; j += 32) ws.prop[j] = P.extProp[(size_t)p * curStride + j];
+            const uint4 u = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xFFFEu, 3u), make_uint2(seed, P.runKey));
+            uMetro = u01(u.x);
+            __syncwarp();
+          } else {
+            propose(P, ws, proj, g, p, lane, sd, seed, &uMetro);
+          }
           double sums[3];
           uint32_t moved = 0;
           const uint4 *evalAtoms;
@@ -1061,6 +1071,105 @@ __global__ void __launch_bounds__(256, 4) wy_batch_kernel(const Params *probs, c
   }
 }
 
+// ---------------------------------------------------------------------------
+// Learned search: K candidate proposals per replica with their features, and
+// the choice among them by the proposal network's predicted gain.
+// ---------------------------------------------------------------------------
+constexpr int kFeat = 64;   // feature vector of one candidate
+
+// One thread per (particle, candidate): the plain search's move (one free
+// site with probability 0.75, else every site; Gaussian steps of the
+// replica's width, projected onto the Wyckoff subspace) and its features:
+// one-hot moved site, collective flag, the site's position and its
+// candidate (sin, cos of 2 pi x), the step in units of the width, and the
+// replica's cc, penalty, fitness, log width and temperature.
+__global__ void wy_candidates_kernel(const Params P, int g, int K, uint32_t *cand, float *feat) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)P.numParticles * K) return;
+  const int p = (int)(t / K), c = (int)(t % K);
+  const size_t stride = (size_t)P.maxSites * 3;
+  const uint32_t *cur = P.pos + (size_t)p * stride;
+  uint32_t *out = cand + (size_t)t * stride;
+  float *f = feat + (size_t)t * kFeat;
+  for (int i = 0; i < kFeat; ++i) f[i] = 0.f;
+  const PState st = P.st[p];
+  const int A = (int)P.assign[p];
+  const uint32_t free = P.freeMask[A];
+  const int nFree = __popc(free);
+  const uint2 key = make_uint2(st.seed, P.runKey);
+  const uint4 r0 = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, (uint32_t)c, 9u), key);
+  int pick = -1;
+  if (u01(r0.x) < 0.75f && nFree > 0) {
+    const int kth = min(nFree - 1, (int)(u01(r0.y) * (float)nFree));
+    pick = __fns(free, 0, kth + 1);
+  }
+  const float sd = st.step;
+  const float scale = sd * 4294967296.0f;
+  constexpr float kTwoPiTurn = 6.28318530717958647f / 4294967296.0f;
+  for (size_t j = 0; j < stride; ++j) out[j] = cur[j];
+  for (int s = 0; s < P.maxSites; ++s) {
+    if (!(pick < 0 || pick == s)) continue;
+    if (!((free >> s) & 1u) && pick < 0) continue;   // fixed sites do not move
+    const uint4 r = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, ((uint32_t)c << 8) | (uint32_t)s, 10u), key);
+    const float2 n01 = gauss2(r.x, r.y), n23 = gauss2(r.z, r.w);
+    const float gz[3] = {n01.x, n01.y, n23.x};
+    int64_t pos[3];
+    for (int i = 0; i < 3; ++i) pos[i] = (int64_t)cur[s * 3 + i] + __float2ll_rn(gz[i] * scale);
+    const ProjFix &pr = P.proj[(size_t)A * P.maxSites + s];
+    uint32_t nw[3];
+    if (pr.pad[0]) {
+      for (int i = 0; i < 3; ++i) nw[i] = (pr.num[4 * i] ? (uint32_t)pos[i] : 0u) + pr.t[i];
+    } else {
+      for (int i = 0; i < 3; ++i) {
+        int64_t acc = (int64_t)pr.num[3 * i] * pos[0] + (int64_t)pr.num[3 * i + 1] * pos[1] +
+                      (int64_t)pr.num[3 * i + 2] * pos[2];
+        if (pr.den != 1) acc = floor_div(acc, pr.den);
+        nw[i] = (uint32_t)(acc + (int64_t)pr.t[i]);
+      }
+    }
+    for (int i = 0; i < 3; ++i) out[s * 3 + i] = nw[i];
+    if (pick == s) {
+      if (s < 32) f[s] = 1.f;
+      for (int i = 0; i < 3; ++i) {
+        float sv, cv;
+        __sincosf((float)(int)cur[s * 3 + i] * kTwoPiTurn, &sv, &cv);
+        f[33 + 2 * i] = sv;
+        f[34 + 2 * i] = cv;
+        f[39 + i] = gz[i];
+        __sincosf((float)(int)nw[i] * kTwoPiTurn, &sv, &cv);
+        f[42 + 2 * i] = sv;
+        f[43 + 2 * i] = cv;
+      }
+    }
+  }
+  f[32] = pick < 0 ? 1.f : 0.f;
+  f[48] = isfinite(st.cc) ? st.cc : 0.f;
+  f[49] = isfinite(st.pen) ? st.pen : 0.f;
+  f[50] = isfinite(st.fit) && st.fit > -1e29f ? st.fit : 0.f;
+  f[51] = __logf(fmaxf(sd, 1e-6f));
+  f[52] = st.temp * 100.f;
+}
+
+// Per particle: the candidate with the largest predicted gain (score column 0
+// of d_out), or candidate 0 without a network; its proposal and features.
+__global__ void wy_select_kernel(const Params P, int K, const float *score, int dOut, const uint32_t *cand,
+                                 const float *feat, uint32_t *ext, float *chosenFeat, float *chosenScore) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.numParticles) return;
+  int best = 0;
+  float bs = score ? score[(size_t)p * K * dOut] : 0.f;
+  if (score)
+    for (int c = 1; c < K; ++c) {
+      const float v = score[((size_t)p * K + c) * dOut];
+      if (v > bs) { bs = v; best = c; }
+    }
+  const size_t stride = (size_t)P.maxSites * 3;
+  const size_t src = (size_t)p * K + best;
+  for (size_t j = 0; j < stride; ++j) ext[(size_t)p * stride + j] = cand[src * stride + j];
+  for (int i = 0; i < kFeat; ++i) chosenFeat[(size_t)p * kFeat + i] = feat[src * kFeat + i];
+  chosenScore[p] = bs;
+}
+
 // Generated cell of one particle in genPack order (parity support).
 __global__ void wy_expand_one(const Params P, const uint32_t *genOrig, int particle, uint32_t *out) {
   const int i = threadIdx.x + blockIdx.x * blockDim.x;
@@ -1099,6 +1208,10 @@ struct p6_wy_session {
   int *dNRuns = nullptr, *dNF = nullptr, *dLadders = nullptr, *dSchedG = nullptr, *dErr = nullptr;
   float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr, *dQuench = nullptr;
   int quenchLen = 0;
+  // learned search: candidates, features, scores, the chosen proposal
+  uint32_t *dCand = nullptr, *dExt = nullptr;
+  float *dFeat = nullptr, *dScore = nullptr, *dChosenFeat = nullptr, *dChosenScore = nullptr;
+  int learnK = 0, learnOut = 0;
   uint32_t *dTracePos = nullptr;
   OpFix *dOps = nullptr;
   ProjFix *dProj = nullptr;
@@ -1207,7 +1320,8 @@ static void free_session(p6_wy_session *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
                   s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTracePos, s->dOps,
-                  s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap};
+                  s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap, s->dCand, s->dExt, s->dFeat, s->dScore,
+                  s->dChosenFeat, s->dChosenScore};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
@@ -1944,6 +2058,93 @@ p6_status p6_wy_launch_count(p6_wy_session *s, long long *count) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Learned search: one generation whose proposals the network pre-ranks.
+// ===========================================================================
+extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, int gen, int swap_every,
+                                        int reeval_first, float *features, float *gains, float *accepted,
+                                        float *scores) {
+  P6_ENTRY();
+  if (!s || K < 1 || (K > 1 && !net)) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
+  if (!s->dLadders) return set_error(P6_ERR_INVALID_ARG, "no ladders set (p6_wy_set_ladders)");
+  if (!s->dSchedG || gen < 0 || gen >= s->schedLen) return set_error(P6_ERR_INVALID_ARG, "generation outside the schedule");
+  if (net && (mlp::input_dim(net) != kFeat || mlp::output_dim(net) < 1))
+    return set_error(P6_ERR_INVALID_ARG, "the network must take 64 features");
+  if (s->incremental) return set_error(P6_ERR_INVALID_ARG, "the learned search uses the full evaluation");
+  P6_CUDA(cudaSetDevice(s->device));
+  Params &P = s->P;
+  const size_t n = P.numParticles, stride = (size_t)P.maxSites * 3;
+  const int dOut = net ? mlp::output_dim(net) : 1;
+  if (K > s->learnK || dOut > s->learnOut) {
+    for (void **q : {(void **)&s->dCand, (void **)&s->dExt, (void **)&s->dFeat, (void **)&s->dScore,
+                     (void **)&s->dChosenFeat, (void **)&s->dChosenScore}) {
+      if (*q) cudaFree(*q);
+      *q = nullptr;
+    }
+    s->learnK = 0;
+    P6_CUDA(cudaMalloc(&s->dCand, n * K * stride * sizeof(uint32_t)));
+    P6_CUDA(cudaMalloc(&s->dExt, n * stride * sizeof(uint32_t)));
+    P6_CUDA(cudaMalloc(&s->dFeat, n * K * kFeat * sizeof(float)));
+    P6_CUDA(cudaMalloc(&s->dScore, n * K * dOut * sizeof(float)));
+    P6_CUDA(cudaMalloc(&s->dChosenFeat, n * kFeat * sizeof(float)));
+    P6_CUDA(cudaMalloc(&s->dChosenScore, n * sizeof(float)));
+    s->learnK = K;
+    s->learnOut = dOut;
+  }
+  const long long threads = (long long)n * K;
+  wy_candidates_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s->stream>>>(P, gen, K, s->dCand, s->dFeat);
+  P6_CUDA(cudaGetLastError());
+  s->launches++;
+  const float *score = nullptr;
+  if (net && K > 1) {
+    p6_status st = mlp::predict_device(net, s->dFeat, (int)threads, s->dScore, s->stream);
+    if (st != P6_OK) return st;
+    score = s->dScore;
+  }
+  wy_select_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(P, K, score, dOut, s->dCand, s->dFeat, s->dExt,
+                                                                      s->dChosenFeat, s->dChosenScore);
+  P6_CUDA(cudaGetLastError());
+  s->launches++;
+  const bool wantTrace = gains || accepted;
+  if (wantTrace && !s->dTraceRec) {
+    p6_status st = p6_wy_set_trace(s, 1);
+    if (st != P6_OK) return st;
+    s->trace = false;
+  }
+  Params saved = P;
+  P.ladders = s->dLadders;
+  P.rungs = s->rungs;
+  P.nLadders = s->nLadders;
+  P.schedGroups = s->dSchedG;
+  P.schedPen = s->dSchedP;
+  P.quenchSd = nullptr;
+  P.extProp = s->dExt;
+  P.tracePos = nullptr;
+  P.traceRec = wantTrace ? s->dTraceRec : nullptr;
+  P.traceIc = nullptr;
+  P6_CUDA(cudaEventRecord(s->ev0, s->stream));
+  cudaError_t e = launch(s, gen, 1, 1, swap_every, reeval_first ? 1 : 0);
+  P = saved;
+  if (e != cudaSuccess) return cuda_error(e, "wy_kernel launch");
+  P6_CUDA(cudaEventRecord(s->ev1, s->stream));
+  std::vector<float> rec;
+  if (wantTrace) {
+    rec.resize(n * 8);
+    P6_CUDA(cudaMemcpyAsync(rec.data(), s->dTraceRec, n * 8 * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  }
+  if (features)
+    P6_CUDA(cudaMemcpyAsync(features, s->dChosenFeat, n * kFeat * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  if (scores) P6_CUDA(cudaMemcpyAsync(scores, s->dChosenScore, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  if (wantTrace || features || scores) {
+    P6_CUDA(cudaStreamSynchronize(s->stream));
+    for (size_t p = 0; p < n && wantTrace; ++p) {
+      if (gains) gains[p] = rec[p * 8] - rec[p * 8 + 5];
+      if (accepted) accepted[p] = rec[p * 8 + 4];
+    }
+  }
+  return P6_OK;
+}
 
 // ===========================================================================
 // Batched searches: many sessions' ladders in one persistent launch.

@@ -144,3 +144,21 @@ def test_penalty_clash_closed_form(oracle, pbso4):
     assert abs(pen - 2.0 * 0.05 * (1 + 9 * (1.2 - 0.8) / 1.2)) < 1e-6
     proj = np.array([0.1, 0.1, 0.1, 0.95, 0.1, 0.1])              # 1.5 A through the cell face
     assert oracle.wy_penalty(proj, T.gen_pack, pack_sym_ops(g.ops), 1, R.tables, R.r_min_off, R.rule_off, 0, 64, 1, geom) == 0
+
+
+def test_mlp_oracle_gradient_is_the_loss_derivative(oracle):
+    """The FP64 network oracle's gradient against central differences of its loss."""
+    rng = np.random.default_rng(2)
+    d_in, width, d_out = 5, 7, 2
+    n_par = d_in * width + width + width * width + width + width * d_out + d_out
+    w = rng.normal(size=n_par) * 0.5
+    X = rng.normal(size=(9, d_in))
+    T = rng.normal(size=(9, d_out))
+    M = (rng.random((9, d_out)) < 0.6).astype(float)
+    g, loss = oracle.mlp_grads_fp64(w, X, T, M, d_in, width, d_out)
+    for i in rng.choice(n_par, 12, replace=False):
+        e = np.zeros(n_par)
+        e[i] = 1e-6
+        lp = oracle.mlp_grads_fp64(w + e, X, T, M, d_in, width, d_out)[1]
+        lm = oracle.mlp_grads_fp64(w - e, X, T, M, d_in, width, d_out)[1]
+        assert abs((lp - lm) / 2e-6 - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
