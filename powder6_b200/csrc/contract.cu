@@ -39,9 +39,12 @@
 #include <vector>
 
 #include "p6_common.cuh"
+#include "tc_common.cuh"
 
 namespace p6 {
 namespace ct {
+
+using namespace p6::tc;
 
 constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
 constexpr int A_TILE = BM * BK * 2;                       // 16 KB per bf16 operand tile
@@ -52,10 +55,11 @@ constexpr int kEpiWarps = 16;                             // four per TMEM lane 
 constexpr int kEpiSpan = BN / (kEpiWarps / 4);              // columns per epilogue warp (64)
 constexpr int kThreads = 64 + 32 * kEpiWarps;               // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
 constexpr uint32_t TMEM_COLS = 2 * BN;                    // two accumulator buffers
-constexpr unsigned long long kWaitNs = 2000000000ull;     // 2 s per wait
 
 // SIMT comparison kernel tiles
 constexpr int FM = 128, FN = 128, FK = 16;
+
+constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
 
 enum CtError : int { CT_OK = 0, CT_WAIT_FULL = 11, CT_WAIT_EMPTY = 12, CT_WAIT_ACC = 13, CT_WAIT_DRAIN = 14 };
 
@@ -67,104 +71,6 @@ struct Params {
   double *chiPart;        // M x nTilesN x (epilogue warps per lane quarter)
   int *errFlag;
 };
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Wait for phase `parity` of `bar` for at most kWaitNs.
-__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity) {
-  const unsigned long long t0 = global_ns();
-  while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > kWaitNs) return false;
-  return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// Shared-memory matrix descriptor of a K-major, 128B-swizzled bf16 tile:
-// 8-row x 128-byte swizzle atoms stacked every 1024 bytes (SBO), LBO unused (1),
-// descriptor version 1, layout SWIZZLE_128B (2).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;
-  d |= (uint64_t)(1024u >> 4) << 32;
-  d |= (uint64_t)1u << 46;
-  d |= (uint64_t)2u << 61;
-  return d;
-}
-
-// Instruction descriptor, kind::f16: FP32 accumulator, bf16 A and B, both
-// K-major, N = BN, M = BM.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// 32 lanes x 32 columns of FP32 from TMEM: thread t gets row t of its warp's lane quarter.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 32 lanes x 64 columns: one load, one wait.
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v) {
-  uint32_t r[64];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, "
-      "%38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, "
-      "%60, %61, %62, %63}, [%64];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
-        "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
-        "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]),
-        "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
-        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
-}
 
 __global__ void __launch_bounds__(kThreads, 1)
     contract_tc_kernel(const __grid_constant__ CUtensorMap tmAhi, const __grid_constant__ CUtensorMap tmAlo,
@@ -259,9 +165,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t off = k * 32;   // 16 bf16 along K inside the 128-byte swizzle row
             const uint64_t aHi = smem_desc(base + off), aLo = smem_desc(base + A_TILE + off);
             const uint64_t bHi = smem_desc(base + 2 * A_TILE + off), bLo = smem_desc(base + 2 * A_TILE + B_TILE + off);
-            umma_bf16(d, aHi, bHi, (done > 0 || k > 0) ? 1u : 0u);
-            umma_bf16(d, aHi, bLo, 1u);
-            umma_bf16(d, aLo, bHi, 1u);
+            umma_bf16(d, aHi, bHi, kIdesc, (done > 0 || k > 0) ? 1u : 0u);
+            umma_bf16(d, aHi, bLo, kIdesc, 1u);
+            umma_bf16(d, aLo, bHi, kIdesc, 1u);
           }
           umma_commit(&emptyBar[s]);
           ++done;
@@ -459,40 +365,9 @@ __global__ void chi_reduce_kernel(const double *part, int M, int nTiles, double 
 // ===========================================================================
 using namespace p6;
 using namespace p6::ct;
+using namespace p6::tc;
 
 namespace {
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
-
-// 2-D bf16 tensor map: rows x Kp elements, K contiguous, box 64 x boxRows, 128B swizzle.
-p6_status make_map(CUtensorMap *m, void *base, int rows, int Kp, int boxRows) {
-  EncodeTiledFn fn = encode_fn();
-  if (!fn) return set_error(P6_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)boxRows};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return set_error(P6_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-  return P6_OK;
-}
-
 // K-ranges of each column tile of width `tile`: the smallest and largest
 // reflection with a nonzero profile value in the tile, rounded out to `align`.
 std::vector<int2> bands(const float *PT, int N, int K, int tile, int align, int Kp) {

@@ -4,11 +4,15 @@
 // writes, and used to pre-rank batched proposals.  The exact structure-factor
 // fitness still decides every acceptance.
 //
-// Training keeps FP32 master weights with Adam; inference runs on bf16 copies
-// of the weights with FP32 accumulation.  All products are one strided,
-// tiled SIMT GEMM (64 x 64 tiles, 4 x 4 per thread) with a bias / ReLU /
-// accumulate epilogue, so forward, backward (A^T B and A B^T) and the
-// masked-MSE gradient share one kernel.
+// Training keeps FP32 master weights with Adam; its products are one
+// strided, tiled SIMT GEMM (64 x 64 tiles, 4 x 4 per thread) with a bias /
+// ReLU / accumulate epilogue, so forward, backward (A^T B and A B^T) and the
+// masked-MSE gradient share one kernel.  Inference -- tens of thousands of
+// candidate rows per search generation -- runs the two hidden layers on the
+// tensor cores: bf16 activations and weights, tcgen05.mma into a TMEM
+// accumulator (one 128 x 256 tile per CTA, all K-blocks staged by TMA at
+// once), bias and ReLU applied by the epilogue warps, bf16 out; the output
+// layer (width -> d_out) is a warp-per-row dot product.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -21,6 +25,7 @@
 
 #include "mlp_internal.h"
 #include "p6_common.cuh"
+#include "tc_common.cuh"
 
 namespace p6 {
 namespace mlp {
@@ -132,6 +137,121 @@ __global__ void to_bf16_kernel(const float *w, __nv_bfloat16 *wh, size_t n) {
     wh[i] = __float2bfloat16_rn(w[i]);
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the tensor cores.
+// ---------------------------------------------------------------------------
+constexpr int LBM = 128, LBN = 256;                 // one tile: 128 rows x the full width
+constexpr int L_A = LBM * 64 * 2, L_B = LBN * 64 * 2;  // bytes of one K-block of A and of B
+constexpr uint32_t kLayerIdesc = tc::idesc_bf16(LBM, LBN);
+
+// out[r][n] = act(sum_k A[r][k] W[k][n] + bias[n]) for one 128-row tile, with
+// B = W^T (width x K, K-major) in bf16; KB K-blocks of 64, all loaded at once.
+template <int KB>
+__global__ void __launch_bounds__(128, 1) layer_tc_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                          const __grid_constant__ CUtensorMap tmB, const float *bias,
+                                                          __nv_bfloat16 *out, int M, int relu, int *errFlag) {
+  using namespace p6::tc;
+  extern __shared__ unsigned char smemRaw[];
+  __shared__ __align__(8) uint64_t fullBar, accBar;
+  __shared__ uint32_t tmemBase;
+  unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, m0 = blockIdx.x * LBM;
+  if (threadIdx.x == 0) {
+    mbar_init(&fullBar, 1);
+    mbar_init(&accBar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmemBase)),
+                 "r"((uint32_t)LBN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmemBase;
+  bool loaded = true;
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(&fullBar, (uint32_t)KB * (L_A + L_B));
+    for (int kb = 0; kb < KB; ++kb) {
+      tma_load_2d(smem + kb * L_A, &tmA, kb * 64, m0, &fullBar);
+      tma_load_2d(smem + KB * L_A + kb * L_B, &tmB, kb * 64, 0, &fullBar);
+    }
+    loaded = wait_phase(&fullBar, 0);
+    if (!loaded) {
+      raise_flag(errFlag, 21);
+      wait_phase(&fullBar, 0);              // copies in flight land before the CTA moves on
+    } else {
+      fence_after_sync();
+      const uint32_t base = smem_u32(smem);
+      for (int kb = 0; kb < KB; ++kb)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint64_t a = smem_desc(base + kb * L_A + k * 32), b = smem_desc(base + KB * L_A + kb * L_B + k * 32);
+          umma_bf16(tmem, a, b, kLayerIdesc, (kb > 0 || k > 0) ? 1u : 0u);
+        }
+      umma_commit(&accBar);
+    }
+    if (!loaded) mbar_arrive(&accBar);
+  }
+  const bool ok = __all_sync(0xffffffffu, wait_phase(&accBar, 0));
+  if (!ok && lane == 0) raise_flag(errFlag, 22);
+  fence_after_sync();
+  const int row = m0 + warp * 32 + lane;
+  for (int c = 0; c < LBN; c += 64) {
+    float v[64];
+    tmem_ld64(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (row < M && ok) {
+      __align__(16) __nv_bfloat16 h[64];
+#pragma unroll
+      for (int j = 0; j < 64; ++j) {
+        float x = v[j] + bias[c + j];
+        if (relu) x = fmaxf(x, 0.f);
+        h[j] = __float2bfloat16_rn(x);
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(out + (size_t)row * LBN + c);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dst[q] = reinterpret_cast<const uint4 *>(h)[q];
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)LBN) : "memory");
+  }
+}
+
+// y[r][o] = sum_k H[r][k] W3[k][o] + b3[o]: one warp per row.
+__global__ void out_layer_kernel(const __nv_bfloat16 *H, int rows, int width, const float *W3, const float *b3,
+                                 int dOut, float *Y) {
+  const int warpsPerBlock = blockDim.x >> 5;
+  const int r = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  for (int o = 0; o < dOut; ++o) {
+    float acc = 0.f;
+    for (int k = lane; k < width; k += 32) acc = fmaf(__bfloat162float(H[(size_t)r * width + k]), W3[k * dOut + o], acc);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+    if (lane == 0) Y[(size_t)r * dOut + o] = acc + b3[o];
+  }
+}
+
+__global__ void rows_to_bf16_kernel(const float *X, size_t n, __nv_bfloat16 *Xh) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    Xh[i] = __float2bfloat16_rn(X[i]);
+}
+
+// Wt[n][k] = bf16(W[k][n]): the K-major operand copy of a K x N weight matrix.
+__global__ void transpose_bf16_kernel(const float *W, int K, int N, __nv_bfloat16 *Wt) {
+  const size_t total = (size_t)K * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int n = (int)(i / K), k = (int)(i % K);
+    Wt[i] = __float2bfloat16_rn(W[(size_t)k * N + n]);
+  }
+}
+
 template <typename BT>
 void gemm(cudaStream_t st, const float *A, long sa0, long sa1, const BT *B, long sb0, long sb1, float *C, int ldc,
           int M, int N, int K, const float *bias, bool relu, bool accumulate) {
@@ -155,6 +275,11 @@ struct p6_mlp {
   size_t off[6] = {};
   float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;   // master weights, gradients, Adam moments
   __nv_bfloat16 *wh = nullptr;                                    // inference copy
+  __nv_bfloat16 *w1t = nullptr, *w2t = nullptr;                   // K-major copies for the tensor-core layers
+  bool tc = false;                                                // width 256 and d_in a multiple of 64
+  int tcCap = 0;
+  __nv_bfloat16 *Xh = nullptr, *H1h = nullptr, *H2h = nullptr;
+  int *dErr = nullptr;
   long long step = 0;
   // scratch for a batch of cap rows
   int cap = 0;
@@ -166,12 +291,49 @@ static void mlp_free(p6_mlp *n) {
   if (!n) return;
   cudaSetDevice(n->device);
   if (n->stream) cudaStreamSynchronize(n->stream);
+  for (void *p : {(void *)n->w1t, (void *)n->w2t, (void *)n->Xh, (void *)n->H1h, (void *)n->H2h, (void *)n->dErr})
+    if (p) cudaFree(p);
   for (void *p : {(void *)n->w, (void *)n->g, (void *)n->m, (void *)n->v, (void *)n->wh, (void *)n->X, (void *)n->T,
                   (void *)n->Mk, (void *)n->H1, (void *)n->H2, (void *)n->Y, (void *)n->dY, (void *)n->dH1,
                   (void *)n->dH2, (void *)n->loss})
     if (p) cudaFree(p);
   if (n->stream) cudaStreamDestroy(n->stream);
   delete n;
+}
+
+// K-major bf16 copies of W1 and W2 for the tensor-core layers.
+static p6_status mlp_refresh_tc(p6_mlp *n) {
+  if (!n->tc) return P6_OK;
+  transpose_bf16_kernel<<<256, 256, 0, n->stream>>>(n->w + n->off[0], n->dIn, n->width, n->w1t);
+  transpose_bf16_kernel<<<256, 256, 0, n->stream>>>(n->w + n->off[2], n->width, n->width, n->w2t);
+  P6_CUDA(cudaGetLastError());
+  return P6_OK;
+}
+
+static p6_status mlp_ensure_tc(p6_mlp *n, int rows) {
+  if (rows <= n->tcCap) return P6_OK;
+  for (__nv_bfloat16 **p : {&n->Xh, &n->H1h, &n->H2h}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  n->tcCap = 0;
+  const size_t r = ((size_t)rows + LBM - 1) / LBM * LBM;
+  P6_CUDA(cudaMalloc(&n->Xh, r * n->dIn * sizeof(__nv_bfloat16)));
+  P6_CUDA(cudaMalloc(&n->H1h, r * LBN * sizeof(__nv_bfloat16)));
+  P6_CUDA(cudaMalloc(&n->H2h, r * LBN * sizeof(__nv_bfloat16)));
+  n->tcCap = rows;
+  return P6_OK;
+}
+
+template <int KB>
+static cudaError_t layer_launch(const CUtensorMap &a, const CUtensorMap &b, const float *bias, __nv_bfloat16 *out,
+                                int rows, int *err, cudaStream_t st) {
+  // at least 100 KB of shared memory: at most two CTAs (2 x 256 TMEM columns) per SM
+  const int smem = std::max(KB * (L_A + L_B) + 1024, 100 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(layer_tc_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  layer_tc_kernel<KB><<<(rows + LBM - 1) / LBM, 128, smem, st>>>(a, b, bias, out, rows, 1, err);
+  return cudaGetLastError();
 }
 
 static p6_status mlp_ensure(p6_mlp *n, int rows) {
@@ -218,9 +380,30 @@ p6_status forward_device(p6_mlp *n, const float *dX, int rows, float *dY, bool i
 }
 
 p6_status predict_device(p6_mlp *n, const float *dX, int rows, float *dY, cudaStream_t st) {
-  p6_status s = mlp_ensure(n, rows);
+  if (!n->tc) {
+    p6_status s = mlp_ensure(n, rows);
+    if (s != P6_OK) return s;
+    return forward_device(n, dX, rows, dY, true, n->H1, n->H2, st);
+  }
+  p6_status s = mlp_ensure_tc(n, rows);
   if (s != P6_OK) return s;
-  return forward_device(n, dX, rows, dY, true, n->H1, n->H2, st);
+  rows_to_bf16_kernel<<<592, 256, 0, st>>>(dX, (size_t)rows * n->dIn, n->Xh);
+  CUtensorMap a1, b1, a2, b2;
+  if ((s = tc::make_map(&a1, n->Xh, rows, n->dIn, LBM)) != P6_OK || (s = tc::make_map(&b1, n->w1t, LBN, n->dIn, LBN)) != P6_OK ||
+      (s = tc::make_map(&a2, n->H1h, rows, LBN, LBM)) != P6_OK || (s = tc::make_map(&b2, n->w2t, LBN, LBN, LBN)) != P6_OK)
+    return s;
+  cudaError_t e;
+  switch (n->dIn / 64) {
+    case 1: e = layer_launch<1>(a1, b1, n->w + n->off[1], n->H1h, rows, n->dErr, st); break;
+    case 2: e = layer_launch<2>(a1, b1, n->w + n->off[1], n->H1h, rows, n->dErr, st); break;
+    case 3: e = layer_launch<3>(a1, b1, n->w + n->off[1], n->H1h, rows, n->dErr, st); break;
+    default: e = layer_launch<4>(a1, b1, n->w + n->off[1], n->H1h, rows, n->dErr, st); break;
+  }
+  if (e == cudaSuccess) e = layer_launch<4>(a2, b2, n->w + n->off[3], n->H2h, rows, n->dErr, st);
+  if (e != cudaSuccess) return cuda_error(e, "mlp tensor-core layers");
+  out_layer_kernel<<<(rows + 7) / 8, 256, 0, st>>>(n->H2h, rows, LBN, n->w + n->off[4], n->w + n->off[5], n->dOut, dY);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? P6_OK : cuda_error(e, "mlp output layer");
 }
 
 int input_dim(const p6_mlp *n) { return n->dIn; }
@@ -302,6 +485,11 @@ p6_status p6_mlp_create(int d_in, int width, int d_out, uint32_t seed, int devic
   if (e == cudaSuccess) e = cudaMalloc(&n->v, o * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&n->wh, o * sizeof(__nv_bfloat16));
   if (e == cudaSuccess) e = cudaMalloc(&n->loss, sizeof(float));
+  n->tc = width == LBN && d_in % 64 == 0 && d_in <= 256;
+  if (e == cudaSuccess && n->tc) e = cudaMalloc(&n->w1t, (size_t)d_in * width * sizeof(__nv_bfloat16));
+  if (e == cudaSuccess && n->tc) e = cudaMalloc(&n->w2t, (size_t)width * width * sizeof(__nv_bfloat16));
+  if (e == cudaSuccess) e = cudaMalloc(&n->dErr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(n->dErr, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemcpy(n->w, h.data(), o * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(n->m, 0, o * sizeof(float));
   if (e == cudaSuccess) e = cudaMemset(n->v, 0, o * sizeof(float));
@@ -309,6 +497,7 @@ p6_status p6_mlp_create(int d_in, int width, int d_out, uint32_t seed, int devic
     to_bf16_kernel<<<256, 256, 0, n->stream>>>(n->w, n->wh, o);
     e = cudaGetLastError();
   }
+  if (e == cudaSuccess && mlp_refresh_tc(n) != P6_OK) e = cudaErrorUnknown;
   if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
   if (e != cudaSuccess) {
     mlp_free(n);
@@ -334,6 +523,8 @@ p6_status p6_mlp_params(p6_mlp *n, float *get, const float *set, long long *coun
     P6_CUDA(cudaMemcpy(n->w, set, n->nParams * sizeof(float), cudaMemcpyHostToDevice));
     to_bf16_kernel<<<256, 256, 0, n->stream>>>(n->w, n->wh, n->nParams);
     P6_CUDA(cudaGetLastError());
+    p6_status s = mlp_refresh_tc(n);
+    if (s != P6_OK) return s;
     P6_CUDA(cudaStreamSynchronize(n->stream));
   }
   if (get) P6_CUDA(cudaMemcpy(get, n->w, n->nParams * sizeof(float), cudaMemcpyDeviceToHost));
@@ -395,6 +586,9 @@ p6_status p6_mlp_train(p6_mlp *n, const float *X, const float *T, const float *m
       epoch_loss[ep] = nb ? l / nb : 0.f;
     }
   }
+  s = mlp_refresh_tc(n);
+  if (s != P6_OK) return s;
+  P6_CUDA(cudaStreamSynchronize(n->stream));
   return P6_OK;
 }
 
@@ -405,9 +599,15 @@ p6_status p6_mlp_predict(p6_mlp *n, const float *X, int rows, float *Y) {
   p6_status s = mlp_ensure(n, rows);
   if (s != P6_OK) return s;
   if ((s = mlp_upload_rows(n, X, nullptr, nullptr, rows)) != P6_OK) return s;
-  if ((s = forward_device(n, n->X, rows, n->Y, true, n->H1, n->H2, n->stream)) != P6_OK) return s;
+  if ((s = predict_device(n, n->X, rows, n->Y, n->stream)) != P6_OK) return s;
   P6_CUDA(cudaMemcpyAsync(Y, n->Y, (size_t)rows * n->dOut * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  int flag = 0;
+  P6_CUDA(cudaMemcpyAsync(&flag, n->dErr, sizeof(int), cudaMemcpyDeviceToHost, n->stream));
   P6_CUDA(cudaStreamSynchronize(n->stream));
+  if (flag) {
+    cudaMemset(n->dErr, 0, sizeof(int));
+    return set_error(P6_ERR_TIMEOUT, "a tensor-core layer wait did not complete in time");
+  }
   return P6_OK;
 }
 

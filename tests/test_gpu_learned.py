@@ -1,8 +1,9 @@
 """Proposal network and learned search.
 
 Parity: the network's gradients (FP32 master weights) against the FP64
-oracle within 1e-5 of the largest gradient; bf16 inference within 2e-2 of
-the FP64 forward pass (bf16 weights carry ~3 significant digits).  Gain:
+oracle within 1e-5 of the largest gradient; inference (bf16 weights and
+activations on the tensor cores) within 5e-2 of the largest FP64 output
+(bf16 carries ~3 significant digits at each of two hidden layers).  Gain:
 trained on the plain search's own moves, ranking 8 candidates raises the
 acceptance rate and the mean exact fitness change of the evaluated
 proposals over the plain move, from the same search state."""
@@ -29,7 +30,12 @@ def test_gradients_and_inference_match_oracle(oracle):
             assert abs(loss - l64) <= 1e-5 * l64
         Y = net.predict(X)
         Y64 = oracle.mlp_forward_fp64(w, X, 64, 256, 1)[0]
-        assert np.max(np.abs(Y - Y64)) <= 2e-2 * np.max(np.abs(Y64))
+        assert np.max(np.abs(Y - Y64)) <= 5e-2 * np.max(np.abs(Y64))
+        # more rows than one tile, a partial last tile
+        X3 = rng.normal(size=(1000, 64)).astype(np.float32)
+        Y3 = net.predict(X3)
+        Y3_64 = oracle.mlp_forward_fp64(w, X3, 64, 256, 1)[0]
+        assert np.max(np.abs(Y3 - Y3_64)) <= 5e-2 * np.max(np.abs(Y3_64))
 
 
 def test_training_fits_a_smooth_target():
