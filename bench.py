@@ -50,10 +50,11 @@ def parse():
     ap.add_argument('--generations', type=int, default=GENERATIONS)
     ap.add_argument('--cos-mode', type=int, default=0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt', 'contract', 'batch'],
+    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt', 'contract', 'batch', 'learned'],
                     help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit; '
                          'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000); '
-                         'batch: 64 uneven Wyckoff searches in one persistent launch')
+                         'batch: 64 uneven Wyckoff searches in one persistent launch; '
+                         'learned: the learned-proposal search (P2_1/c, 17 sites, 8192 replicas)')
     ap.add_argument('--method', default='split', choices=['split', 'fp32'],
                     help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
     ap.add_argument('--chains', type=int, default=64)
@@ -649,6 +650,98 @@ def main_batch(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+LEARNED_GENERATIONS = 1000
+
+
+def main_learned(args, world, rank, local):
+    """One step = one learned-proposal search (P2_1/c, 17 independent C/N/S
+    sites, 575 reflections, 8192 replicas, LEARNED_GENERATIONS generations; 8
+    candidates per replica ranked by the network, the best evaluated with the
+    exact fitness).  The network is trained beforehand (outside the timed
+    region) on 819k moves of the plain search.  value: replica-generations
+    per second over the device span of the search loop; time_to_target:
+    wall seconds to a best wR2 within 1.05x the quenched wR2 of a 2000-
+    generation plain search, for the learned search and for the plain fused
+    search from the same starts."""
+    import torch
+    from powder6_b200.learned import ProposalNet, collect_records, gain_targets, learned_problem, run as lrun
+    from powder6_b200.swarm_wyckoff import WyckoffSession, run_wyckoff_search, schedule
+    torch.cuda.set_device(local)
+    P = learned_problem()
+    n, G = 8192, LEARNED_GENERATIONS
+    with WyckoffSession(P, n, run_key=77 + rank, incremental=0, device=local) as s:
+        X, gains, _ = collect_records(s, P, 200, seed=4 + rank, every=2)
+        T, _ = gain_targets(gains)
+        net = ProposalNet(64, 256, 1, seed=7, device=local)
+        t0 = time.perf_counter()
+        losses = net.train(X, T, epochs=8, batch=2048, lr=1e-3)
+        train_s = time.perf_counter() - t0
+        conv = run_wyckoff_search(P, num_particles=n, generations=2 * G, seed=31, session=s)
+        target = 1.0 - 1.05 * (1.0 - conv.best_cc)
+        for i in range(args.warmup):
+            lrun(s, P, 200, seed=50 + i, net=net, K=8, check_every=100)
+        barrier(world)
+        dev_ms, ttt_l, ttt_p, best_l, best_p, e2e = [], [], [], [], [], []
+        l0 = s.launch_count()
+        with ClockSampler(local) as clk:
+            for i in range(args.steps):
+                t0 = time.perf_counter()
+                tr = lrun(s, P, G, seed=100 + i, net=net, K=8, check_every=100, target_cc=target)
+                s.read_state()
+                e2e.append(time.perf_counter() - t0)
+                dev_ms.append(tr.device_ms)
+                ttt_l.append(tr.time_to_target)
+                best_l.append(tr.best_cc[-1])
+        launches = s.launch_count() - l0
+        for i in range(args.steps):
+            r = run_wyckoff_search(P, num_particles=n, generations=G, seed=100 + i, chunk=100, session=s,
+                                   do_quench=False, target_cc=target)
+            ttt_p.append(r.time_to_target)
+            best_p.append(r.best_cc)
+        net.close()
+    total_ms = max_over_ranks(float(sum(dev_ms)), world)
+    value = world * n * G * args.steps / (total_ms / 1000.0)
+    if rank == 0:
+        clocks = clk.summary()
+        groups, _ = schedule(G, P.refl.n_groups)
+        cos_total = algorithmic_cos(P, groups, n)[0]
+        ms = float(np.mean(dev_ms))
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clocks['sm_mhz'] or 1965.0
+        peak = MUFU_PER_CLK_PER_SM * nsm * mhz * 1e6 / 1e9
+        achieved = cos_total / (ms / 1000.0) / 1e9
+
+        def med(v):
+            v = [x for x in v if x is not None]
+            return float(np.median(v)) if v else None
+        line = {
+            'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp32 fitness, bf16 network', 'data': 'synthetic',
+            'config': {'workload': f'learned-proposal Wyckoff search: P2_1/c a=10.2 b=12.1 c=15.3 beta=100, 17 C/N/S '
+                                   f'sites (68 atoms), {P.refl.n_refl} reflections to d_min 1.5 A, {n} replicas x {G} '
+                                   f'generations, 8 candidates ranked per replica by a 64-256-256-1 MLP',
+                       'training': {'records': int(len(X)), 'epochs': 8, 'seconds': train_s,
+                                    'loss_first_last': [float(losses[0]), float(losses[-1])]},
+                       'step': 'one learned search, one launch of each kernel per generation',
+                       'parallelism': f'replicas only x{world}'},
+            'time_to_target_wr2': {'target_wr2': 1.0 - target, 'converged_wr2_plain_2000': 1.0 - conv.best_cc,
+                                   'learned_median_s': med(ttt_l), 'plain_median_s': med(ttt_p),
+                                   'learned_reached': f'{sum(t is not None for t in ttt_l)}/{len(ttt_l)}',
+                                   'plain_reached': f'{sum(t is not None for t in ttt_p)}/{len(ttt_p)}',
+                                   'best_wr2_learned': [1.0 - b for b in best_l],
+                                   'best_wr2_plain': [1.0 - b for b in best_p]},
+            'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak, 'unit': 'Gcos/s', 'frac': achieved / peak,
+                         'traffic': None,
+                         'note': f'{cos_total:.4g} algorithmic cosines per step (exact evaluations only)'},
+            'e2e': {'value': world * n * G * args.steps / max_over_ranks(float(sum(e2e)), world), 'unit': 'trials/s',
+                    'h2d_bytes_per_step': n * (51 * 4 + 48), 'd2h_bytes_per_step': n * (2 * 51 * 4 + 48)},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def measured_peak(key):
     f = ROOT / 'MEASURED_PEAKS.json'
     if f.exists():
@@ -675,8 +768,9 @@ def main():
         else:
             run_reference(args, world, rank)
         return
-    if args.workload in ('pt', 'contract', 'batch'):
-        {'pt': main_pt, 'contract': main_ct, 'batch': main_batch}[args.workload](args, world, rank, local)
+    if args.workload in ('pt', 'contract', 'batch', 'learned'):
+        {'pt': main_pt, 'contract': main_ct, 'batch': main_batch, 'learned': main_learned}[args.workload](
+            args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

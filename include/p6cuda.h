@@ -355,6 +355,9 @@ p6_status p6_mlp_destroy(p6_mlp *n);
  * used on the session's stream: do not train it meanwhile. */
 p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, int gen, int swap_every, int reeval_first,
                              float *features, float *gains, float *accepted, float *scores);
+/* Marks the start (end = 0) or the end (end = 1) of a span on the session's
+ * stream, for p6_wy_last_kernel_ms (the device time of a multi-launch loop). */
+p6_status p6_wy_time_mark(p6_wy_session *s, int end);
 /* Copies the FP32 parameters out (get) and/or in (set); count receives their number. */
 p6_status p6_mlp_params(p6_mlp *n, float *get, const float *set, long long *count);
 /* Gradient of the loss over the given rows (flat, like the parameters) and the loss. */

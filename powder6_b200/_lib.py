@@ -126,6 +126,7 @@ _SIGS = {
     'p6_mlp_train': (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, _P]),
     'p6_mlp_predict': (C.c_int, [_P, _P, C.c_int, _P]),
     'p6_wy_learned_step': (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P]),
+    'p6_wy_time_mark': (C.c_int, [_P, C.c_int]),
     'p6_ct_create': (C.c_int, [C.POINTER(P6CtProblem), C.c_int, C.POINTER(C.c_void_p)]),
     'p6_ct_destroy': (C.c_int, [_P]),
     'p6_ct_set_intensities': (C.c_int, [_P, _P, C.c_int]),

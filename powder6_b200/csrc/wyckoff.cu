@@ -2123,11 +2123,9 @@ extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, in
   P.tracePos = nullptr;
   P.traceRec = wantTrace ? s->dTraceRec : nullptr;
   P.traceIc = nullptr;
-  P6_CUDA(cudaEventRecord(s->ev0, s->stream));
   cudaError_t e = launch(s, gen, 1, 1, swap_every, reeval_first ? 1 : 0);
   P = saved;
   if (e != cudaSuccess) return cuda_error(e, "wy_kernel launch");
-  P6_CUDA(cudaEventRecord(s->ev1, s->stream));
   std::vector<float> rec;
   if (wantTrace) {
     rec.resize(n * 8);
@@ -2143,6 +2141,16 @@ extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, in
       if (accepted) accepted[p] = rec[p * 8 + 4];
     }
   }
+  return P6_OK;
+}
+
+// Marks the start (end = 0) or end (end = 1) of a timed span on the session's
+// stream; p6_wy_last_kernel_ms then reports the span.
+extern "C" p6_status p6_wy_time_mark(p6_wy_session *s, int end) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaEventRecord(end ? s->ev1 : s->ev0, s->stream));
   return P6_OK;
 }
 

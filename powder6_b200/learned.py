@@ -171,6 +171,7 @@ class SearchTrace:
     best_cc: List[float] = field(default_factory=list)
     generations: int = 0
     time_to_target: Optional[float] = None
+    device_ms: float = 0.0
 
 
 def run(sess: WyckoffSession, problem: WyckoffProblem, generations: int, seed: int, net: Optional[ProposalNet] = None,
@@ -181,6 +182,7 @@ def run(sess: WyckoffSession, problem: WyckoffProblem, generations: int, seed: i
     tr = SearchTrace()
     sess.synchronize(60)
     t0 = time.perf_counter()
+    check(sess.lib.p6_wy_time_mark(sess.h, 0))
     k = K if net is not None else 1
     for g in range(generations):
         reeval = g == 0 or groups[g] != groups[g - 1]
@@ -193,5 +195,8 @@ def run(sess: WyckoffSession, problem: WyckoffProblem, generations: int, seed: i
             tr.best_cc.append(b)
             if target_cc is not None and tr.time_to_target is None and b >= target_cc:
                 tr.time_to_target = tr.seconds[-1]
+    check(sess.lib.p6_wy_time_mark(sess.h, 1))
+    sess.synchronize(600)
+    tr.device_ms = sess.last_kernel_ms()
     tr.generations = generations
     return tr
