@@ -295,6 +295,43 @@ __device__ __forceinline__ void group_sums(const Params &P, const float *ic, con
   __syncwarp();
 }
 
+// Cosine and sine sums of one run for two reflections.  The run's first
+// nPair = run.w >> 8 atoms lead inversion pairs whose partners (the run's last
+// nPair atoms) are not read: a leader's cosine counts twice and its sine
+// cancels.  The singles follow the leaders.
+template <int COSMODE>
+__device__ __forceinline__ void run_sums(const int4 run, const uint4 *atoms, bool centro, uint32_t h0, uint32_t k0,
+                                         uint32_t l0, uint32_t h1, uint32_t k1, uint32_t l1, float &c0, float &s0,
+                                         float &c1, float &s1) {
+  const int nPair = run.w >> 8;
+  const int lead = run.x + nPair, end = run.y - nPair;
+  float p0 = 0.f, p1 = 0.f;
+  for (int a = run.x; a < lead; ++a) {
+    const uint4 at = atoms[a];
+    p0 += cos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z);
+    p1 += cos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z);
+  }
+  c0 = 2.f * p0;
+  c1 = 2.f * p1;
+  s0 = 0.f;
+  s1 = 0.f;
+  if (centro) {
+    for (int a = lead; a < end; ++a) {
+      const uint4 at = atoms[a];
+      c0 += cos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z);
+      c1 += cos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z);
+    }
+  } else {
+    for (int a = lead; a < end; ++a) {
+      const uint4 at = atoms[a];
+      float sa, ca, sb, cb;
+      sincos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z, &sa, &ca);
+      sincos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z, &sb, &cb);
+      c0 += ca; s0 += sa; c1 += cb; s1 += sb;
+    }
+  }
+}
+
 // C_s for the sites in `mask`, written to physical slot ws.slot[s], except
 // site `spareSite` (if >= 0), written to the spare slot ws.slot[maxSites].
 template <int COSMODE>
@@ -313,24 +350,10 @@ __device__ __forceinline__ void site_sums(const Params &P, const WarpView &ws, c
     const uint32_t h1 = (uint32_t)(int)a1.h, k1 = (uint32_t)(int)a1.k, l1 = (uint32_t)(int)a1.l;
     for (int q = 0; q < nRuns; ++q) {
       const int4 run = ws.runs[q];
-      const int site = run.w;
+      const int site = run.w & 0xFF;
       if (!((mask >> site) & 1u)) continue;
-      float c0 = 0.f, s0 = 0.f, c1 = 0.f, s1 = 0.f;
-      if (centro) {
-        for (int a = run.x; a < run.y; ++a) {
-          const uint4 at = atoms[a];
-          c0 += cos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z);
-          c1 += cos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z);
-        }
-      } else {
-        for (int a = run.x; a < run.y; ++a) {
-          const uint4 at = atoms[a];
-          float sa, ca, sb, cb;
-          sincos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z, &sa, &ca);
-          sincos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z, &sb, &cb);
-          c0 += ca; s0 += sa; c1 += cb; s1 += sb;
-        }
-      }
+      float c0, s0, c1, s1;
+      run_sums<COSMODE>(run, atoms, centro, h0, k0, l0, h1, k1, l1, c0, s0, c1, s1);
       const int phys = site == spareSite ? ws.slot[P.maxSites] : ws.slot[site];
       float *dst = Cb + (size_t)phys * pad * comp;
       dst[r0 * comp] = c0;
@@ -361,7 +384,7 @@ __device__ __forceinline__ void fitness_from_banks(const Params &P, const WarpVi
     float fr = 0.f, fi = 0.f;
     for (int q = 0; q < nRuns; ++q) {
       const int4 run = ws.runs[q];
-      const int site = run.w;
+      const int site = run.w & 0xFF;
       const int phys = site == spareSite ? ws.slot[P.maxSites] : ws.slot[site];
       const float *src = Cb + ((size_t)phys * pad + r) * comp;
       const float w = ftab[r * nElem + run.z];
@@ -398,22 +421,8 @@ __device__ __forceinline__ void fitness_direct(const Params &P, const WarpView &
     float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
     for (int q = 0; q < nRuns; ++q) {
       const int4 run = ws.runs[q];
-      float c0 = 0.f, s0 = 0.f, c1 = 0.f, s1 = 0.f;
-      if (centro) {
-        for (int a = run.x; a < run.y; ++a) {
-          const uint4 at = atoms[a];
-          c0 += cos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z);
-          c1 += cos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z);
-        }
-      } else {
-        for (int a = run.x; a < run.y; ++a) {
-          const uint4 at = atoms[a];
-          float sa, ca, sb, cb;
-          sincos_turn<COSMODE>(h0 * at.x + k0 * at.y + l0 * at.z, &sa, &ca);
-          sincos_turn<COSMODE>(h1 * at.x + k1 * at.y + l1 * at.z, &sb, &cb);
-          c0 += ca; s0 += sa; c1 += cb; s1 += sb;
-        }
-      }
+      float c0, s0, c1, s1;
+      run_sums<COSMODE>(run, atoms, centro, h0, k0, l0, h1, k1, l1, c0, s0, c1, s1);
       const float w0 = ftab[r0 * nElem + run.z];
       const float w1 = ftab[(has1 ? r1 : r0) * nElem + run.z];
       fr0 = fmaf(w0, c0, fr0);
@@ -1450,6 +1459,66 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
     }
     nRuns[A] = nr;
     nF[A] = nf;
+    // Inversion pairs: two images of one site whose positions sum to a lattice
+    // vector at every point of the site's subspace have equal cosines and
+    // opposite sines for every integer hkl.  Each run is reordered as
+    // [leaders | singles | partners] and the number of pairs goes to bits 8+
+    // of run.w; the |F|^2 sums read only the leaders (cosine counted twice,
+    // sine cancelled) and the singles.  The test uses two generic points of
+    // the subspace in FP64, so a pair holds wherever the site sits.
+    for (int q = 0; q < nr; ++q) {
+      int4 &run = runs[(size_t)A * kMaxSites + q];
+      const int site = run.w, len = run.y - run.x;
+      const float *pj = pr->site_proj + ((size_t)A * ms + site) * 12;
+      double img[2][64][3];
+      if (len > 64) continue;
+      for (int p = 0; p < 2; ++p) {
+        const double u[3] = {p ? 0.2718281 : 0.1234567, p ? 0.5772156 : 0.3456789, p ? 0.6931471 : 0.7654321};
+        double x[3];
+        for (int k = 0; k < 3; ++k)
+          x[k] = (double)pj[3 * k] * u[0] + (double)pj[3 * k + 1] * u[1] + (double)pj[3 * k + 2] * u[2] + pj[9 + k];
+        for (int i = 0; i < len; ++i) {
+          const int op = (genR[(size_t)A * nTot + run.x + i] >> 8) & 0xFFF;
+          const float *b = pr->sym_packed + op * 12;
+          for (int k = 0; k < 3; ++k)
+            img[p][i][k] = (double)b[3 * k] * x[0] + (double)b[3 * k + 1] * x[1] + (double)b[3 * k + 2] * x[2] + b[9 + k];
+        }
+      }
+      auto inverse = [&](int i, int j) {
+        for (int p = 0; p < 2; ++p)
+          for (int k = 0; k < 3; ++k) {
+            const double v = img[p][i][k] + img[p][j][k];
+            if (std::fabs(v - std::floor(v + 0.5)) > 1e-7) return false;
+          }
+        return true;
+      };
+      int partner[64];
+      for (int i = 0; i < len; ++i) partner[i] = -2;  // -2 unassigned, -1 single
+      for (int i = 0; i < len; ++i) {
+        if (partner[i] != -2) continue;
+        partner[i] = -1;
+        if (inverse(i, i)) continue;  // an image on an inversion centre stands alone
+        for (int j = i + 1; j < len; ++j)
+          if (partner[j] == -2 && inverse(i, j)) {
+            partner[i] = j;
+            partner[j] = i;
+            break;
+          }
+      }
+      std::vector<uint32_t> lead, single, part;
+      for (int i = 0; i < len; ++i) {
+        const uint32_t word = genR[(size_t)A * nTot + run.x + i];
+        if (partner[i] < 0) single.push_back(word);
+        else if (partner[i] > i) lead.push_back(word);
+      }
+      for (int i = 0; i < len; ++i)
+        if (partner[i] >= 0 && partner[i] < i) part.push_back(genR[(size_t)A * nTot + run.x + i]);
+      int w = run.x;
+      for (uint32_t v : lead) genR[(size_t)A * nTot + w++] = v;
+      for (uint32_t v : single) genR[(size_t)A * nTot + w++] = v;
+      for (uint32_t v : part) genR[(size_t)A * nTot + w++] = v;
+      run.w = site | ((int)lead.size() << 8);
+    }
   }
   std::vector<OpFix> ops(pr->n_ops);
   for (int o = 0; o < pr->n_ops; ++o) {

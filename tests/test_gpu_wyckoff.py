@@ -4,6 +4,7 @@ Tolerances (stated per test): the fitness cc = 1 - wR2 and the per-reflection
 mult |F|^2 are FP32 arithmetic on exactly reduced integer phases; the oracle
 is FP64.  Orbit expansion and proposals on the Wyckoff subspace are integer
 arithmetic and are compared bit for bit."""
+import dataclasses
 import math
 
 import numpy as np
@@ -142,6 +143,54 @@ def test_evaluation_parity(prob, oracle, cos_mode, cc_tol, ic_tol):
         assert worst_ic <= ic_tol
         assert worst_pen <= 1e-5
         assert float(st['cc'][0]) > 0.95
+
+
+def _pair_cases():
+    hexa = {'a': 5.0, 'b': 5.0, 'c': 14.0, 'alpha': 90.0, 'beta': 90.0, 'gamma': 120.0}
+    mono = {'a': 9.0, 'b': 6.0, 'c': 8.0, 'alpha': 90.0, 'beta': 105.0, 'gamma': 90.0}
+    return {
+        # Pnma evaluated with the complex sums: the pairs' sines must cancel
+        'pnma-complex': lambda: dataclasses.replace(wyckoff_problem(seed=1), centro=False),
+        # R-3m (hexagonal axes): translations of 1/3 and 2/3 and rhombohedral centring
+        'r-3m': lambda: wyckoff_problem(seed=3, group_number=166, cell=hexa, composition=(('Ti', 6), ('O', 18)),
+                                        sites=(('Ti', '6c'), ('O', '18h')), dmin=1.3, true_min_contact=1.2,
+                                        contact_attempts=200),
+        # C2/c: C centring, a general and a special position
+        'c2/c': lambda: wyckoff_problem(seed=3, group_number=15, cell=mono, composition=(('S', 8), ('O', 4)),
+                                        sites=(('S', '8f'), ('O', '4e')), dmin=1.3, true_min_contact=1.2,
+                                        contact_attempts=200),
+    }
+
+
+@pytest.mark.parametrize('case', ['pnma-complex', 'r-3m', 'c2/c'])
+def test_inversion_pair_evaluation_parity(oracle, case):
+    """Images related by the inversion centre are summed once with weight 2
+    (sines cancelled); the fitness still matches the FP64 oracle's sum over
+    every image: |dcc| <= 2e-6 and mult |F|^2 within 2e-4 of the largest
+    reflection (SFU cosines), on centred cells, fractional translations of
+    1/3 and the complex-sum path."""
+    P = _pair_cases()[case]()
+    n = 128
+    X, _ = random_positions(P, n, 21)
+    with WyckoffSession(P, n, cos_mode=0) as s:
+        s.write_positions_fixed(X)
+        s.set_trace(True)
+        s.set_params(P.refl.n_groups, 1.0)
+        s.dispatch(None, mcmc=False)
+        s.synchronize(60)
+        _, _, st = s.read_state()
+        ic = s.read_trace_ic()
+    worst_cc = worst_ic = 0.0
+    for p in range(n):
+        sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
+        cc, _, _ = oracle_cc_pen(oracle, P, sites, P.refl.n_groups, 1.0)
+        worst_cc = max(worst_cc, abs(float(st['cc'][p]) - cc))
+        if p < 32:
+            ref = icalc_fp64(P, sites)
+            worst_ic = max(worst_ic, float(np.max(np.abs(ic[p] - ref)) / ref.max()))
+    print(f'{case}: max |dcc| {worst_cc:.3e}, max rel |d mult F^2| {worst_ic:.3e}')
+    assert worst_cc <= 2e-6
+    assert worst_ic <= 2e-4
 
 
 def test_mcmc_step_parity_and_proposals(prob, oracle):
