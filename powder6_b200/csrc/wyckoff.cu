@@ -90,6 +90,7 @@ struct Params {
   const ProjFix *proj;     // per (assignment, site)
   const unsigned char *blob;  // staged static tables
   int blobBytes, offRefl, offF, offGroup, offRmin, offSoo, offOps, offPairs, nPairs;
+  const int2 *pairRange;   // per assignment {offset, count} of its site-representative pairs; null: all pairs
   const RuleDev *rules;
   int nRules;
   int numParticles, nTot, maxSites, nRefl, nGroups, nElem, nAssign;
@@ -507,14 +508,26 @@ __device__ __forceinline__ float clash_term(const Params &P, float d, float dmin
   return P.penClash * (1.0f + 9.0f * ((dmin - d) / fmaxf(dmin, 1e-3f)));
 }
 
-// Clash penalty only (no distance rules): sum over pairs i < j.  Small cells
-// walk a precomputed, balanced pair list; large ones stripe j over the lanes.
+// Clash penalty only (no distance rules): sum over pairs i < j.  With
+// site-representative pairs (P.pairRange) the list holds (rep_s, j, m_s) for
+// each site s and every other atom j: every image of a site has the same
+// neighbours, so sum_{i<j} f(d_ij) = 1/2 sum_s m_s sum_{j != rep_s} f(d_{rep_s,j}).
+// Otherwise small cells walk the balanced list of all pairs and large ones
+// stripe j over the lanes.
 __device__ __forceinline__ float clash_penalty(const Params &P, const uint4 *atoms, const float *rmin,
-                                               const uint32_t *pairs, int lane) {
+                                               const uint32_t *pairs, int nPairs, int lane) {
   float pen = 0.f;
   const int n = P.nTot, ne = P.nElem;
-  if (pairs && P.minImageShell == 0) {
-    for (int idx = lane; idx < P.nPairs; idx += 32) {
+  if (pairs && P.pairRange) {
+    for (int idx = lane; idx < nPairs; idx += 32) {
+      const uint32_t e = pairs[idx];
+      const uint4 ai = atoms[e & 0xFFF], aj = atoms[(e >> 12) & 0xFFF];
+      const float dmin = rmin[ai.w * ne + aj.w];
+      const float d = P.minImageShell ? cart_dist(P, ai, aj) : sqrtf(dist2_near(P, ai, aj));
+      if (d < dmin) pen += (0.5f * (float)(e >> 24)) * clash_term(P, d, dmin);
+    }
+  } else if (pairs && P.minImageShell == 0) {
+    for (int idx = lane; idx < nPairs; idx += 32) {
       const uint32_t pr = pairs[idx];
       const uint4 ai = atoms[pr & 0xFFFF], aj = atoms[pr >> 16];
       const float dmin = rmin[ai.w * ne + aj.w];
@@ -665,8 +678,8 @@ __device__ float rule_penalty(const Params &P, const uint4 *atoms, const float *
 
 template <int SLOTS>
 __device__ __forceinline__ float penalty(const Params &P, const uint4 *atoms, const float *rmin,
-                                         const float *shellLen, const uint32_t *pairs, int lane) {
-  if (SLOTS == 0) return clash_penalty(P, atoms, rmin, pairs, lane);
+                                         const float *shellLen, const uint32_t *pairs, int nPairs, int lane) {
+  if (SLOTS == 0) return clash_penalty(P, atoms, rmin, pairs, nPairs, lane);
   return rule_penalty<(SLOTS > 0 ? SLOTS : 1)>(P, atoms, rmin, shellLen, lane);
 }
 
@@ -772,7 +785,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   const float *rmin = reinterpret_cast<const float *>(stat + P.offRmin);
   const double *sooPrefix = reinterpret_cast<const double *>(stat + P.offSoo);
   const OpFix *ops = reinterpret_cast<const OpFix *>(stat + P.offOps);
-  const uint32_t *pairs = P.nPairs > 0 ? reinterpret_cast<const uint32_t *>(stat + P.offPairs) : nullptr;
+  const uint32_t *pairs =
+      (P.nPairs > 0 || P.pairRange) ? reinterpret_cast<const uint32_t *>(stat + P.offPairs) : nullptr;
 
   unsigned char *wbase = smem + blobPad + (size_t)warp * P.warpSmemBytes;
   WarpView ws = warp_view(wbase, P);
@@ -800,11 +814,18 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
       }
     }
     const bool active = p >= 0;
+    const uint32_t *myPairs = pairs;
+    int myNPairs = P.nPairs;
     // chain state in registers (meaningful on lane 0)
     float fit = 0.f, cc0 = 0.f, pen0 = 0.f, step = 0.f, temp = 0.f, bestFit = -1e30f, bestCC = 0.f, bestPen = 0.f;
     uint32_t seed = 0, accepted = 0;
     if (active) {
       const int A = (int)P.assign[p];
+      if (pairs && P.pairRange) {
+        const int2 pr = P.pairRange[A];
+        myPairs = pairs + pr.x;
+        myNPairs = pr.y;
+      }
       if (lane == 0) {
         ws.meta[0] = A;
         ws.meta[1] = P.nRuns[A];
@@ -849,7 +870,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             double sums[3];
             fitness_from_banks(P, ws, Cb, -1, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
             const float cc = cc_of(sums);
-            const float pen = penalty<SLOTS>(P, atomsB[cb], rmin, shellLen, pairs, lane) * penScale;
+            const float pen = penalty<SLOTS>(P, atomsB[cb], rmin, shellLen, myPairs, myNPairs, lane) * penScale;
             fit = cc - pen;
             cc0 = cc;
             pen0 = pen / fmaxf(penScale, 1e-9f);
@@ -862,7 +883,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             double sums[3];
             fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
             const float cc = cc_of(sums);
-            const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, pairs, lane) * penScale;
+            const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
             fit = cc - pen;
             cc0 = cc;
             pen0 = pen / fmaxf(penScale, 1e-9f);
@@ -908,7 +929,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             evalAtoms = atoms;
           }
           const float cc = cc_of(sums);
-          const float pen = penalty<SLOTS>(P, evalAtoms, rmin, shellLen, pairs, lane) * penScale;
+          const float pen = penalty<SLOTS>(P, evalAtoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
           int acc = 0, best = 0;
           if (lane == 0) {
             const float fNew = cc - pen;
@@ -1214,6 +1235,7 @@ struct p6_wy_session {
   int incremental = 0;  // site sums cached per replica (two banks) in shared memory
   uint32_t *dGen = nullptr, *dGenOrig = nullptr, *dFree = nullptr, *dPos = nullptr, *dAssign = nullptr;
   int4 *dRuns = nullptr;
+  int2 *dPairRange = nullptr;
   int *dNRuns = nullptr, *dNF = nullptr, *dLadders = nullptr, *dSchedG = nullptr, *dErr = nullptr;
   float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr, *dQuench = nullptr;
   int quenchLen = 0;
@@ -1330,7 +1352,7 @@ static void free_session(p6_wy_session *s) {
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
                   s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTracePos, s->dOps,
                   s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap, s->dCand, s->dExt, s->dFeat, s->dScore,
-                  s->dChosenFeat, s->dChosenScore};
+                  s->dChosenFeat, s->dChosenScore, s->dPairRange};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
@@ -1553,14 +1575,42 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
     }
   // --- static blob: reflections | f table | groups | rMin | soo prefix | ops | pairs ---
   auto pad16 = [](size_t n) { return (n + 15) & ~(size_t)15; };
-  const int nPairs = nTot <= 96 ? nTot * (nTot - 1) / 2 : 0;
+  // Clash pairs.  The space group maps the cell's atoms onto themselves, and
+  // rounding in the reduced basis is the nearest image out to every
+  // threshold (otherwise the minimum-image shell search is on), so all the
+  // images of one site see the same neighbours: the pairs (rep_s, j), j != rep_s,
+  // with weight m_s / 2 (m_s = the site's atoms in the cell) give the sum over
+  // all pairs i < j from nSites x (nTot - 1) distances instead of nTot^2 / 2.
+  std::vector<uint32_t> repPairs;
+  std::vector<int2> pairRange(nA);
+  bool useRep = true;
+  for (int A = 0; A < nA && useRep; ++A) {
+    std::vector<int> first(ms, -1), mult(ms, 0);
+    for (int i = 0; i < nTot; ++i) {
+      const int s = genR[(size_t)A * nTot + i] & 0xFF;
+      if (first[s] < 0) first[s] = i;
+      ++mult[s];
+    }
+    pairRange[A].x = (int)repPairs.size();
+    for (int s = 0; s < ms && useRep; ++s) {
+      if (!mult[s]) continue;
+      if (mult[s] > 255) useRep = false;
+      for (int j = 0; j < nTot && useRep; ++j)
+        if (j != first[s]) repPairs.push_back((uint32_t)first[s] | ((uint32_t)j << 12) | ((uint32_t)mult[s] << 24));
+    }
+    pairRange[A].y = (int)repPairs.size() - pairRange[A].x;
+    if (repPairs.size() > 4608) useRep = false;
+  }
+  if (!useRep) repPairs.clear();
+  const int nPairs = useRep ? 0 : (nTot <= 96 ? nTot * (nTot - 1) / 2 : 0);
+  const size_t pairWords = useRep ? repPairs.size() : (size_t)nPairs;
   const size_t offRefl = 0, szRefl = pad16((size_t)pr->n_refl * sizeof(ReflRec));
   const size_t offF = offRefl + szRefl, szF = pad16((size_t)pr->n_refl * nE * sizeof(float));
   const size_t offG = offF + szF, szG = pad16((size_t)pr->n_groups * sizeof(float4));
   const size_t offR = offG + szG, szR = pad16((size_t)nE * nE * sizeof(float));
   const size_t offS = offR + szR, szS = pad16((size_t)(pr->n_groups + 1) * sizeof(double));
   const size_t offO = offS + szS, szO = pad16((size_t)pr->n_ops * sizeof(OpFix));
-  const size_t offP = offO + szO, szP = pad16((size_t)nPairs * sizeof(uint32_t));
+  const size_t offP = offO + szO, szP = pad16(pairWords * sizeof(uint32_t));
   const size_t blobBytes = offP + szP;
   std::vector<unsigned char> blob(blobBytes, 0);
   for (int r = 0; r < pr->n_refl; ++r) {
@@ -1598,6 +1648,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   std::memcpy(&blob[offO], ops.data(), ops.size() * sizeof(OpFix));
   {
     int q = 0;
+    if (useRep && !repPairs.empty()) std::memcpy(&blob[offP], repPairs.data(), repPairs.size() * sizeof(uint32_t));
     for (int i = 0; i < nTot && nPairs; ++i)
       for (int j = i + 1; j < nTot; ++j) {
         const uint32_t v = (uint32_t)i | ((uint32_t)j << 16);
@@ -1673,6 +1724,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P6_TRY(upload(&s->dGen, genR.data(), genR.size(), s->stream));
   P6_TRY(upload(&s->dGenOrig, pr->gen_pack, (size_t)nA * nTot, s->stream));
   P6_TRY(upload(&s->dRuns, runs.data(), runs.size(), s->stream));
+  if (useRep) P6_TRY(upload(&s->dPairRange, pairRange.data(), pairRange.size(), s->stream));
   P6_TRY(upload(&s->dNRuns, nRuns.data(), nRuns.size(), s->stream));
   P6_TRY(upload(&s->dNF, nF.data(), nF.size(), s->stream));
   P6_TRY(upload(&s->dFree, freeMask.data(), freeMask.size(), s->stream));
@@ -1715,6 +1767,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.offOps = (int)offO;
   P.offPairs = (int)offP;
   P.nPairs = nPairs;
+  P.pairRange = useRep ? s->dPairRange : nullptr;
   P.rules = s->dRules;
   P.nRules = pr->n_rules;
   P.numParticles = pr->num_particles;

@@ -168,7 +168,9 @@ def test_inversion_pair_evaluation_parity(oracle, case):
     (sines cancelled); the fitness still matches the FP64 oracle's sum over
     every image: |dcc| <= 2e-6 and mult |F|^2 within 2e-4 of the largest
     reflection (SFU cosines), on centred cells, fractional translations of
-    1/3 and the complex-sum path."""
+    1/3 and the complex-sum path.  The clash penalty, summed from each
+    site's representative with weight m_s / 2, matches the oracle's sum over
+    all pairs within 1e-5 relative on random (clashing) structures."""
     P = _pair_cases()[case]()
     n = 128
     X, _ = random_positions(P, n, 21)
@@ -180,17 +182,23 @@ def test_inversion_pair_evaluation_parity(oracle, case):
         s.synchronize(60)
         _, _, st = s.read_state()
         ic = s.read_trace_ic()
-    worst_cc = worst_ic = 0.0
+    worst_cc = worst_ic = worst_pen = 0.0
+    clashing = 0
     for p in range(n):
         sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
-        cc, _, _ = oracle_cc_pen(oracle, P, sites, P.refl.n_groups, 1.0)
+        cc, pen, _ = oracle_cc_pen(oracle, P, sites, P.refl.n_groups, 1.0)
         worst_cc = max(worst_cc, abs(float(st['cc'][p]) - cc))
+        worst_pen = max(worst_pen, abs(float(st['pen'][p]) - pen) / max(1.0, pen))
+        clashing += pen > 0
         if p < 32:
             ref = icalc_fp64(P, sites)
             worst_ic = max(worst_ic, float(np.max(np.abs(ic[p] - ref)) / ref.max()))
-    print(f'{case}: max |dcc| {worst_cc:.3e}, max rel |d mult F^2| {worst_ic:.3e}')
+    print(f'{case}: max |dcc| {worst_cc:.3e}, max rel |d mult F^2| {worst_ic:.3e}, max rel dpen {worst_pen:.3e}, '
+          f'{clashing}/{n} with clashes')
     assert worst_cc <= 2e-6
     assert worst_ic <= 2e-4
+    assert worst_pen <= 1e-5
+    assert clashing >= n // 16
 
 
 def test_mcmc_step_parity_and_proposals(prob, oracle):
