@@ -400,44 +400,106 @@ __device__ __forceinline__ void fitness_from_banks(const Params &P, const WarpVi
   group_sums(P, ic, groups, sooPrefix, nga, lane, sums);
 }
 
-// |F|^2 straight from the atoms with two reflections per lane: the same
-// per-run summation order as site_sums followed by fitness_from_banks (so the
-// result is bit-identical), with fewer live registers than `fitness`.
+// Up to four reflections per lane per pass (rows base + lane + 32 j): each
+// broadcast atom load feeds NR independent cosine chains.  The arithmetic per
+// reflection is the same sequence as run_sums, so |F|^2 is bit-identical to
+// the site-sum path.
+template <int COSMODE, int NR>
+__device__ __forceinline__ void fit_rows(const Params &P, const WarpView &ws, const uint4 *atoms, float *ic,
+                                         const ReflRec *refl, const float *ftab, int base, int nAct, int lane,
+                                         float *traceIc) {
+  const int nRuns = ws.meta[1];
+  const bool centro = P.centro != 0;
+  const int nElem = P.nElem;
+  int r[NR];
+  uint32_t h[NR], k[NR], l[NR];
+  float fr[NR], fi[NR];
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    r[j] = min(base + lane + 32 * j, nAct - 1);
+    const ReflRec a = refl[r[j]];
+    h[j] = (uint32_t)(int)a.h;
+    k[j] = (uint32_t)(int)a.k;
+    l[j] = (uint32_t)(int)a.l;
+    fr[j] = 0.f;
+    fi[j] = 0.f;
+  }
+  for (int q = 0; q < nRuns; ++q) {
+    const int4 run = ws.runs[q];
+    const int nPair = run.w >> 8;
+    const int lead = run.x + nPair, end = run.y - nPair;
+    float c[NR], s[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+      c[j] = 0.f;
+      s[j] = 0.f;
+    }
+    for (int a = run.x; a < lead; ++a) {
+      const uint4 at = atoms[a];
+#pragma unroll
+      for (int j = 0; j < NR; ++j) c[j] += cos_turn<COSMODE>(h[j] * at.x + k[j] * at.y + l[j] * at.z);
+    }
+#pragma unroll
+    for (int j = 0; j < NR; ++j) c[j] = 2.f * c[j];
+    if (centro) {
+      for (int a = lead; a < end; ++a) {
+        const uint4 at = atoms[a];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) c[j] += cos_turn<COSMODE>(h[j] * at.x + k[j] * at.y + l[j] * at.z);
+      }
+    } else {
+      for (int a = lead; a < end; ++a) {
+        const uint4 at = atoms[a];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+          float sa, ca;
+          sincos_turn<COSMODE>(h[j] * at.x + k[j] * at.y + l[j] * at.z, &sa, &ca);
+          c[j] += ca;
+          s[j] += sa;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+      const float w = ftab[r[j] * nElem + run.z];
+      fr[j] = fmaf(w, c[j], fr[j]);
+      fi[j] = fmaf(w, s[j], fi[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    if (base + lane + 32 * j < nAct) {
+      const float v = (float)refl[r[j]].mult * (fr[j] * fr[j] + fi[j] * fi[j]);
+      ic[r[j]] = v;
+      if (traceIc) traceIc[r[j]] = v;
+    }
+  }
+}
+
+// |F|^2 straight from the atoms, in passes of 128, 96, 64 or 32 reflections
+// (fit_rows with NR = 4, 3, 2, 1 as the remaining count needs): the same
+// per-run summation order as site_sums followed by fitness_from_banks, so the
+// result is bit-identical.
 template <int COSMODE>
 __device__ __forceinline__ void fitness_direct(const Params &P, const WarpView &ws, const uint4 *atoms, float *ic,
                                                const ReflRec *refl, const float *ftab, const float4 *groups,
                                                const double *sooPrefix, int nga, int lane, double sums[3],
                                                float *traceIc) {
-  const int nRuns = ws.meta[1];
   const int nAct = nrefl_active(groups, nga);
-  const bool centro = P.centro != 0;
-  const int nElem = P.nElem;
-  for (int r0 = lane; r0 < nAct; r0 += 64) {
-    const int r1 = r0 + 32;
-    const bool has1 = r1 < nAct;
-    const ReflRec a0 = refl[r0];
-    const ReflRec a1 = refl[has1 ? r1 : r0];
-    const uint32_t h0 = (uint32_t)(int)a0.h, k0 = (uint32_t)(int)a0.k, l0 = (uint32_t)(int)a0.l;
-    const uint32_t h1 = (uint32_t)(int)a1.h, k1 = (uint32_t)(int)a1.k, l1 = (uint32_t)(int)a1.l;
-    float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
-    for (int q = 0; q < nRuns; ++q) {
-      const int4 run = ws.runs[q];
-      float c0, s0, c1, s1;
-      run_sums<COSMODE>(run, atoms, centro, h0, k0, l0, h1, k1, l1, c0, s0, c1, s1);
-      const float w0 = ftab[r0 * nElem + run.z];
-      const float w1 = ftab[(has1 ? r1 : r0) * nElem + run.z];
-      fr0 = fmaf(w0, c0, fr0);
-      fi0 = fmaf(w0, s0, fi0);
-      fr1 = fmaf(w1, c1, fr1);
-      fi1 = fmaf(w1, s1, fi1);
-    }
-    const float v0 = (float)a0.mult * (fr0 * fr0 + fi0 * fi0);
-    ic[r0] = v0;
-    if (traceIc) traceIc[r0] = v0;
-    if (has1) {
-      const float v1 = (float)a1.mult * (fr1 * fr1 + fi1 * fi1);
-      ic[r1] = v1;
-      if (traceIc) traceIc[r1] = v1;
+  for (int base = 0; base < nAct;) {
+    const int rem = nAct - base;
+    if (rem > 96) {
+      fit_rows<COSMODE, 4>(P, ws, atoms, ic, refl, ftab, base, nAct, lane, traceIc);
+      base += 128;
+    } else if (rem > 64) {
+      fit_rows<COSMODE, 3>(P, ws, atoms, ic, refl, ftab, base, nAct, lane, traceIc);
+      base += 96;
+    } else if (rem > 32) {
+      fit_rows<COSMODE, 2>(P, ws, atoms, ic, refl, ftab, base, nAct, lane, traceIc);
+      base += 64;
+    } else {
+      fit_rows<COSMODE, 1>(P, ws, atoms, ic, refl, ftab, base, nAct, lane, traceIc);
+      base += 32;
     }
   }
   __syncwarp();
