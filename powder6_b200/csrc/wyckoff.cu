@@ -463,7 +463,7 @@ __device__ __forceinline__ void fit_rows(const Params &P, const WarpView &ws, co
     for (int j = 0; j < NR; ++j) {
       const float w = ftab[r[j] * nElem + run.z];
       fr[j] = fmaf(w, c[j], fr[j]);
-      fi[j] = fmaf(w, s[j], fi[j]);
+      if (!centro) fi[j] = fmaf(w, s[j], fi[j]);
     }
   }
 #pragma unroll
@@ -585,8 +585,13 @@ __device__ __forceinline__ float clash_penalty(const Params &P, const uint4 *ato
       const uint32_t e = pairs[idx];
       const uint4 ai = atoms[e & 0xFFF], aj = atoms[(e >> 12) & 0xFFF];
       const float dmin = rmin[ai.w * ne + aj.w];
-      const float d = P.minImageShell ? cart_dist(P, ai, aj) : sqrtf(dist2_near(P, ai, aj));
-      if (d < dmin) pen += (0.5f * (float)(e >> 24)) * clash_term(P, d, dmin);
+      if (P.minImageShell) {
+        const float d = cart_dist(P, ai, aj);
+        if (d < dmin) pen += (0.5f * (float)(e >> 24)) * clash_term(P, d, dmin);
+      } else {
+        const float d2 = dist2_near(P, ai, aj);
+        if (d2 < dmin * dmin) pen += (0.5f * (float)(e >> 24)) * clash_term(P, sqrtf(d2), dmin);
+      }
     }
   } else if (pairs && P.minImageShell == 0) {
     for (int idx = lane; idx < nPairs; idx += 32) {
