@@ -137,7 +137,7 @@ def algorithmic_cos(P, groups, n_particles):
 def cpu_baseline(P, groups, pen, n_particles, seconds=10.0):
     from oracle import oracle as O
     r = O.WyckoffCpuRunner(P, n_particles, seed=7)
-    gens = np.linspace(0, len(groups) - 1, 64).astype(int)
+    gens = np.linspace(0, len(groups) - 1, 1000).astype(int)
     t0 = time.perf_counter()
     trials = 0
     used = 0

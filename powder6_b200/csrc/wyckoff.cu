@@ -234,11 +234,12 @@ __device__ __forceinline__ int64_t floor_div(int64_t a, int d) {
 //
 // Work is issue-bound (every replica generation is a few thousand warp
 // instructions for a hundred or so warp-wide cosines), so the layout below
-// is chosen to minimise instructions per cosine: two reflections per lane
-// share each broadcast atom load, the phase is three integer multiply-adds,
-// the clash loop walks a balanced pair list on squared distances, the
-// constant sum of w Iobs^2 comes from a prefix table, and the chain state
-// lives in registers of lane 0.
+// is chosen to minimise instructions per cosine: up to four reflections per
+// lane share each broadcast atom load, the phase is three integer
+// multiply-adds, inversion partners are summed once, the clash loop walks the
+// site representatives' pairs on squared distances, the constant sum of
+// w Iobs^2 comes from a prefix table, and the chain state lives in registers
+// of lane 0.
 // ---------------------------------------------------------------------------
 
 // Per-warp shared-memory slice, sized by the session's max_sites (pointers into the slice).
