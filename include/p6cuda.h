@@ -233,6 +233,18 @@ typedef struct {
   int chains;
   double max_temp;
   uint32_t seed;
+  /* March-Dollase preferred orientation (js/rietveld_core.js:824-853, GPU
+   * js/pt_gpu.js:159-160).  has_po = 0: off (factor 1).  Otherwise the March
+   * parameter r is full_values[n_bkg + 14] (the entry after the background),
+   * the direction po_dir is a reciprocal-lattice vector, and the factor of
+   * reflection k averages (r^2 cos^2 a + sin^2 a / r)^(-3/2) over its
+   * equivalents eq_hkl[3 * eq_start[k] .. 3 * eq_start[k + 1]), a = the angle
+   * between the equivalent and po_dir in the current reciprocal metric
+   * (r <= 0 or |r - 1| < 1e-12: factor 1). */
+  int has_po;
+  const int32_t *eq_start; /* n_refl + 1 */
+  const int32_t *eq_hkl;   /* 3 per equivalent */
+  double po_dir[3];
 } p6_pt_problem;
 
 typedef struct p6_pt_session p6_pt_session;

@@ -214,7 +214,8 @@ class PtProblem(C.Structure):
                 ('ffA', C.c_void_p), ('ffB', C.c_void_p), ('ffC', C.c_void_p),
                 ('n', C.c_int), ('tth', C.c_void_p), ('y', C.c_void_p), ('w', C.c_void_p),
                 ('lambda1', C.c_double), ('lambda2', C.c_double), ('ratio', C.c_double), ('polK', C.c_double),
-                ('minFwhm', C.c_double), ('nBkg', C.c_int), ('dmin', C.c_double)]
+                ('minFwhm', C.c_double), ('nBkg', C.c_int), ('dmin', C.c_double),
+                ('hasPo', C.c_int), ('poDir', C.c_double * 3)]
 
 
 class PtSetup(C.Structure):
@@ -267,6 +268,11 @@ class PtModel:
         p.minFwhm = prob.min_fwhm
         p.nBkg = prob.n_bkg
         p.dmin = 0.0 if dmin is None else float(dmin)
+        po_dir = getattr(prob, 'po_dir', None)
+        p.hasPo = 1 if po_dir is not None else 0
+        if po_dir is not None:
+            for i in range(3):
+                p.poDir[i] = float(po_dir[i])
         self.p = p
 
     def cost_full(self, v, with_pattern=False):

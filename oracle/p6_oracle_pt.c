@@ -65,6 +65,9 @@ typedef struct {
     double lambda1, lambda2, ratio, polK, minFwhm;
     int nBkg;
     double dmin;           /* > 0: use this; <= 0: reflectionDmin of the parameters */
+    /* March-Dollase preferred orientation: r = v[PT_BKG0 + nBkg], direction poDir (reciprocal lattice) */
+    int hasPo;
+    double poDir[3];
 } p6o_pt_problem;
 
 static const double GCONV = 0.023548200450309493;   /* sqrt(8 ln 2) / 100 */
@@ -194,6 +197,54 @@ static double inv_dsq_cell(const double *c6, double h, double k, double l, int *
            k * l * (2 * bs * cs * cAs) + h * l * (2 * as * cs * cBs);
 }
 
+/* Coefficients of the 1/d^2 form: aa, bb, cc, ab, bc, ac (the hk, kl, hl terms). */
+static void cell_form(const double *c6, double f[6])
+{
+    int ok;
+    f[0] = inv_dsq_cell(c6, 1, 0, 0, &ok);
+    f[1] = inv_dsq_cell(c6, 0, 1, 0, &ok);
+    f[2] = inv_dsq_cell(c6, 0, 0, 1, &ok);
+    f[3] = inv_dsq_cell(c6, 1, 1, 0, &ok) - f[0] - f[1];
+    f[4] = inv_dsq_cell(c6, 0, 1, 1, &ok) - f[1] - f[2];
+    f[5] = inv_dsq_cell(c6, 1, 0, 1, &ok) - f[0] - f[2];
+}
+
+static double form_g(const double f[6], const double *a, const double *b)
+{
+    return a[0] * b[0] * f[0] + a[1] * b[1] * f[1] + a[2] * b[2] * f[2] + (a[0] * b[1] + a[1] * b[0]) * f[3] / 2 +
+           (a[1] * b[2] + a[2] * b[1]) * f[4] / 2 + (a[0] * b[2] + a[2] * b[0]) * f[5] / 2;
+}
+
+/*
+ * preferredOrientation (js/rietveld_core.js:824-853): the March-Dollase
+ * factor of (h, k, l), averaged over its distinct equivalents h R under the
+ * phase's operators.
+ */
+double p6o_po_factor(const p6o_pt_problem *P, const double *c6, double r, int h, int k, int l)
+{
+    if (!(r > 0) || fabs(r - 1) < 1e-12) return 1;
+    double f[6];
+    cell_form(c6, f);
+    const double *H = P->poDir, HH = form_g(f, H, H), r2 = r * r, ir = 1 / r;
+    if (!(HH > 0)) return 1;
+    int seen[192 * 3], m = 0;
+    double sum = 0;
+    for (int o = 0; o < P->nOps && m < 192; o++) {
+        const int *R = P->rot + 9 * o;
+        int e[3] = {h * R[0] + k * R[3] + l * R[6], h * R[1] + k * R[4] + l * R[7], h * R[2] + k * R[5] + l * R[8]};
+        int dup = 0;
+        for (int q = 0; q < m && !dup; q++)
+            dup = seen[3 * q] == e[0] && seen[3 * q + 1] == e[1] && seen[3 * q + 2] == e[2];
+        if (dup) continue;
+        seen[3 * m] = e[0]; seen[3 * m + 1] = e[1]; seen[3 * m + 2] = e[2];
+        m++;
+        double hv[3] = {e[0], e[1], e[2]};
+        double hh = form_g(f, hv, hv), c = form_g(f, hv, H) / sqrt(hh * HH), c2 = fmin(1, c * c);
+        sum += pow(r2 * c2 + (1 - c2) * ir, -1.5);
+    }
+    return m ? sum / m : 1;
+}
+
 /*
  * chi^2 of the full parameter vector v.  ycalc (may be NULL) receives the
  * calculated pattern; nRefl (may be NULL) the reflection count used.
@@ -256,6 +307,7 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
             }
         }
         F2[r] = Ar * Ar + Br * Br;
+        if (P->hasPo && isfinite(tth)) F2[r] *= p6o_po_factor(P, c6, v[PT_BKG0 + P->nBkg], h[r], k[r], l[r]);
     }
     /* contributions: all K-alpha-1, then all K-alpha-2 */
     for (int r = 0; r < nr; r++) {
@@ -477,10 +529,11 @@ double p6o_voigt_raw(double delta, double inv, double cL, double cG)
 /* (fdStep :526-538, defaultLimits :486-508, stepCap :511-524), Cholesky and */
 /* solveSPD (:1304-1335).  Parameters are identified by their full index.    */
 /* ------------------------------------------------------------------------ */
-enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG };
+enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO };
 
-static int kind_of(int fi)
+static int kind_of(const p6o_pt_problem *P, int fi)
 {
+    if (P->hasPo && fi == PT_BKG0 + P->nBkg) return K_PO;
     if (fi == PT_SCALE) return K_SCALE;
     if (fi >= PT_A && fi <= PT_C) return K_CELL;
     if (fi >= PT_AL && fi <= PT_GA) return K_ANGLE;
@@ -499,6 +552,7 @@ static double fd_step(int kind, double v)
     case K_CELL: return fmax(1e-6 * a, 1e-6);
     case K_ANGLE: return 1e-4;
     case K_ZERO: return 1e-4;
+    case K_PO: return 1e-4;
     default: return fmax(1e-4 * a, 1e-5);
     }
 }
@@ -513,6 +567,7 @@ static void default_limits(int kind, double v, double *lo, double *hi)
     case K_BISO: *lo = -2; *hi = 30; return;
     case K_ZERO: *lo = -2; *hi = 2; return;
     case K_LORENTZ: *lo = 0; *hi = INFINITY; return;
+    case K_PO: *lo = 0.1; *hi = 5; return;
     default: *lo = -INFINITY; *hi = INFINITY; return;
     }
 }
@@ -525,6 +580,7 @@ static double step_cap(int kind, double v)
     case K_ANGLE: return 1;
     case K_BISO: return 2;
     case K_ZERO: return 0.1;
+    case K_PO: return 0.25;
     case K_PROFILE: case K_LORENTZ: return 0.5 * fmax(fabs(v), 5);
     default: return INFINITY;
     }
@@ -615,7 +671,7 @@ int p6o_pt_normal(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *
     double chi = p6o_pt_cost(P, v, y0, NULL);
     if (!isfinite(chi)) { free(v); free(vp); free(y0); free(ya); free(yb); free(J); free(r); return 0; }
     for (int j = 0; j < nv; j++) {
-        const int fi = S->index[j], kind = kind_of(fi);
+        const int fi = S->index[j], kind = kind_of(P, fi);
         double *col = J + (size_t)j * n;
         if (kind == K_SCALE) {
             memcpy(vp, v, sizeof(double) * nFull);
@@ -639,7 +695,8 @@ int p6o_pt_normal(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *
             const double val = x[j], h = fd_step(kind, val);
             double llo, lhi;
             default_limits(kind, val, &llo, &lhi);
-            const int plus = val + h <= lhi, minus = val - h >= llo;
+            /* the March-Dollase column is a forward difference (js/rietveld_core.js:1271-1275) */
+            const int plus = kind == K_PO || val + h <= lhi, minus = kind != K_PO && val - h >= llo;
             double xp[64], xm[64];
             memcpy(xp, x, sizeof(double) * nv);
             memcpy(xm, x, sizeof(double) * nv);
@@ -746,7 +803,7 @@ int p6o_pt_lm(const p6o_pt_problem *P, const p6o_pt_setup *S, const double *base
         memset(step, 0, sizeof(double) * nv);
         for (int a = 0; a < nF; a++) {
             const int q = F[a];
-            const double cap = step_cap(kind_of(S->index[q]), x[q]);
+            const double cap = step_cap(kind_of(P, S->index[q]), x[q]);
             const double sh = fmax(-cap, fmin(cap, dx[a] * sc[a]));
             xn[q] = fmin(S->hi[q], fmax(S->lo[q], x[q] + sh));
             step[q] = xn[q] - x[q];

@@ -93,6 +93,10 @@ struct Params {
   uint32_t seed;
   int stageObs;          // observed pattern staged in shared memory
   int *errFlag;
+  int hasPo;             // March-Dollase factor on; r = v[PBKG0 + nBkg]
+  const int *eqStart;    // nRefl + 1
+  const int *eqHkl;      // 3 per equivalent
+  double poDir[3];       // reciprocal-lattice direction
 };
 
 // ---------------------------------------------------------------------------
@@ -206,6 +210,33 @@ __device__ bool inv_dsq_form(const double *v, double f[6]) {
   return true;
 }
 
+// March-Dollase factor of reflection k (js/rietveld_core.js:824-853): the
+// mean of (r^2 cos^2 a + sin^2 a / r)^(-3/2) over the reflection's
+// equivalents, a the angle to poDir in the reciprocal metric f (the 1/d^2
+// form).  Warp-collective (lanes over the equivalents); every lane returns it.
+__device__ double po_factor(const Params &P, const double f[6], double r, int k, int lane) {
+  if (!(r > 0) || fabs(r - 1) < 1e-12) return 1.0;
+  auto g = [&](double a0, double a1, double a2, double b0, double b1, double b2) {
+    return a0 * b0 * f[0] + a1 * b1 * f[1] + a2 * b2 * f[2] + (a0 * b1 + a1 * b0) * f[3] / 2 +
+           (a1 * b2 + a2 * b1) * f[4] / 2 + (a0 * b2 + a2 * b0) * f[5] / 2;
+  };
+  const double d0 = P.poDir[0], d1 = P.poDir[1], d2 = P.poDir[2];
+  const double HH = g(d0, d1, d2, d0, d1, d2);
+  if (!(HH > 0)) return 1.0;
+  const int e0 = P.eqStart[k], e1 = P.eqStart[k + 1];
+  const double r2 = r * r, ir = 1 / r;
+  double sum = 0;
+  for (int e = e0 + lane; e < e1; e += 32) {
+    const double h0 = P.eqHkl[3 * e], h1 = P.eqHkl[3 * e + 1], h2 = P.eqHkl[3 * e + 2];
+    const double hh = g(h0, h1, h2, h0, h1, h2), c = g(h0, h1, h2, d0, d1, d2) / sqrt(hh * HH);
+    const double c2 = fmin(1.0, c * c), x = r2 * c2 + (1 - c2) * ir;
+    sum += 1.0 / (x * sqrt(x));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  return e1 > e0 ? sum / (e1 - e0) : 1.0;
+}
+
 // ---------------------------------------------------------------------------
 // One full cost evaluation of the parameter vector in shared memory `v`.
 // All threads call it; returns chi^2 on every thread (INF if invalid).
@@ -271,7 +302,8 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
         B += (A_t)wj * sn;
       }
     }
-    if (lane == 0) h1[k] = (H)((double)A * A + (double)B * B);   // F^2, parked until the heights
+    const double po = (P.hasPo && live) ? po_factor(P, sh.f, v[PBKG0 + P.nBkg], k, lane) : 1.0;
+    if (lane == 0) h1[k] = (H)(((double)A * A + (double)B * B) * po);   // F^2 (x March-Dollase), parked until the heights
   }
   __syncwarp();
   // Peaks: lane pairs over this warp's reflections, the even lane preparing
@@ -891,6 +923,15 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
     if (pr->index[j] < 0 || pr->index[j] >= pr->n_full) return set_error(P6_ERR_INVALID_ARG, "parameter index out of range");
   for (int i = 1; i < pr->n_points; ++i)
     if (!(pr->tth[i] > pr->tth[i - 1])) return set_error(P6_ERR_INVALID_ARG, "the 2-theta axis must be ascending");
+  if (pr->has_po) {
+    if (!pr->eq_start || !pr->eq_hkl) return set_error(P6_ERR_INVALID_ARG, "preferred orientation without equivalents");
+    if (pr->n_full < PBKG0 + pr->n_bkg + 1)
+      return set_error(P6_ERR_INVALID_ARG, "preferred orientation: the full vector has no entry after the background");
+    if (pr->eq_start[0] != 0) return set_error(P6_ERR_INVALID_ARG, "eq_start[0] must be 0");
+    for (int k = 0; k < pr->n_refl; ++k)
+      if (pr->eq_start[k + 1] < pr->eq_start[k] || pr->eq_start[k + 1] - pr->eq_start[k] > 192)
+        return set_error(P6_ERR_INVALID_ARG, "eq_start must be ascending with at most 192 equivalents per reflection");
+  }
   p6_pt_session *s = new p6_pt_session();
   s->device = device;
   cudaError_t e = cudaSetDevice(device);
@@ -930,6 +971,12 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
   PT_TRY(pt_upload(s, pr->lo, (size_t)pr->nv, &P.lo));
   PT_TRY(pt_upload(s, pr->hi, (size_t)pr->nv, &P.hi));
   PT_TRY(pt_upload(s, pr->scales, (size_t)pr->nv, &P.scales));
+  P.hasPo = pr->has_po ? 1 : 0;
+  if (P.hasPo) {
+    PT_TRY(pt_upload(s, pr->eq_start, (size_t)pr->n_refl + 1, &P.eqStart));
+    PT_TRY(pt_upload(s, pr->eq_hkl, (size_t)3 * pr->eq_start[pr->n_refl], &P.eqHkl));
+    for (int i = 0; i < 3; ++i) P.poDir[i] = pr->po_dir[i];
+  }
   int smemOptin = 0;
   cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   const int staticBytes = 4096;
@@ -1113,9 +1160,10 @@ p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
 // the scalar control of lm() on the host.
 // ===========================================================================
 namespace {
-enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG };
+enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO };
 
-int lm_kind(int fi) {
+int lm_kind(const Params &P, int fi) {
+  if (P.hasPo && fi == PBKG0 + P.nBkg) return K_PO;
   if (fi == SCALE) return K_SCALE;
   if (fi >= PA && fi <= PC) return K_CELL;
   if (fi >= PAL && fi <= PGA) return K_ANGLE;
@@ -1130,7 +1178,7 @@ double lm_fd_step(int kind, double v) {
   const double a = std::fabs(v);
   switch (kind) {
     case K_CELL: return std::max(1e-6 * a, 1e-6);
-    case K_ANGLE: case K_ZERO: return 1e-4;
+    case K_ANGLE: case K_ZERO: case K_PO: return 1e-4;
     default: return std::max(1e-4 * a, 1e-5);
   }
 }
@@ -1144,6 +1192,7 @@ void lm_limits(int kind, double v, double *lo, double *hi) {
     case K_BISO: *lo = -2; *hi = 30; return;
     case K_ZERO: *lo = -2; *hi = 2; return;
     case K_LORENTZ: *lo = 0; *hi = inf; return;
+    case K_PO: *lo = 0.1; *hi = 5; return;
     default: *lo = -inf; *hi = inf; return;
   }
 }
@@ -1154,6 +1203,7 @@ double lm_step_cap(int kind, double v) {
     case K_ANGLE: return 1;
     case K_BISO: return 2;
     case K_ZERO: return 0.1;
+    case K_PO: return 0.25;
     case K_PROFILE: case K_LORENTZ: return 0.5 * std::max(std::fabs(v), 5.0);
     default: return std::numeric_limits<double>::infinity();
   }
@@ -1216,7 +1266,7 @@ p6_status lm_normal(p6_pt_session *s, const double *x, double *A, double *g, dou
   LmCols L{};
   int m = 1;
   for (int j = 0; j < nv; ++j) {
-    const int fi = s->indexHost[j], kind = lm_kind(fi);
+    const int fi = s->indexHost[j], kind = lm_kind(s->P, fi);
     L.plus[j] = L.minus[j] = 0;
     L.step[j] = 1;
     if (kind == K_SCALE) { L.kind[j] = 0; continue; }
@@ -1224,7 +1274,8 @@ p6_status lm_normal(p6_pt_session *s, const double *x, double *A, double *g, dou
     const double val = x[j], h = lm_fd_step(kind, val);
     double llo, lhi;
     lm_limits(kind, val, &llo, &lhi);
-    const bool plus = val + h <= lhi, minus = val - h >= llo;
+    // the March-Dollase column is a forward difference (js/rietveld_core.js:1271-1275)
+    const bool plus = kind == K_PO || val + h <= lhi, minus = kind != K_PO && val - h >= llo;
     const double vp = plus ? val + h : val, vm = minus ? val - h : val, d = vp - vm;
     if (!(d != 0)) { L.kind[j] = 3; continue; }
     L.kind[j] = 2;
@@ -1306,7 +1357,7 @@ extern "C" p6_status p6_pt_linear_start(p6_pt_session *s, double *x, double *chi
   const int nv = s->P.nv;
   std::vector<int> lin;
   for (int j = 0; j < nv; ++j) {
-    const int k = lm_kind(s->indexHost[j]);
+    const int k = lm_kind(s->P, s->indexHost[j]);
     if (k == K_SCALE || k == K_BKG) lin.push_back(j);
   }
   std::vector<double> A((size_t)nv * nv), g(nv), d(nv + 1), xt(x, x + nv);
@@ -1383,7 +1434,7 @@ extern "C" p6_status p6_pt_lm(p6_pt_session *s, double *x, int max_iter, double 
     std::fill(step.begin(), step.end(), 0.0);
     for (int a = 0; a < nF; ++a) {
       const int q = F[a];
-      const double cap = lm_step_cap(lm_kind(s->indexHost[q]), x[q]);
+      const double cap = lm_step_cap(lm_kind(s->P, s->indexHost[q]), x[q]);
       const double sh = std::max(-cap, std::min(cap, dx[a]));
       xn[q] = std::min(s->hiHost[q], std::max(s->loHost[q], x[q] + sh));
       step[q] = xn[q] - x[q];

@@ -59,6 +59,10 @@ class PTProblem:
     refined: List[str]                # names of the refined parameters
     lo: np.ndarray
     hi: np.ndarray
+    # March-Dollase preferred orientation (js/rietveld_core.js:824-853): the
+    # reciprocal-lattice direction, or None (off).  Its parameter 'po' (r) is
+    # the entry of the full vector after the background.
+    po_dir: Optional[Sequence[float]] = None
 
     @property
     def index(self) -> np.ndarray:
@@ -67,6 +71,10 @@ class PTProblem:
     def full_index(self, name: str) -> int:
         if name.startswith('bkg'):
             return len(FULL_NAMES) + int(name[3:])
+        if name == 'po':
+            if self.po_dir is None:
+                raise KeyError('po: the problem has no preferred-orientation direction')
+            return len(FULL_NAMES) + self.n_bkg
         return FULL_NAMES.index(name)
 
     def apply(self, x: Sequence[float]) -> np.ndarray:
@@ -116,6 +124,8 @@ class Plan:
     stride: int
     point_count: int
     reflection_count: int
+    eq_start: Optional[np.ndarray] = None   # March-Dollase: equivalents of each reflection
+    eq_hkl: Optional[np.ndarray] = None
 
 
 def compile(ctx: PTContext) -> Plan:
@@ -131,7 +141,7 @@ def compile(ctx: PTContext) -> Plan:
     if P.system == 'cubic':
         v[2] = v[3] = v[1]
     cell = {'a': v[1], 'b': v[2], 'c': v[3], 'alpha': v[4], 'beta': v[5], 'gamma': v[6]}
-    refl = generate_reflections(cell, g.ops, dmin, with_eq=False)
+    refl = generate_reflections(cell, g.ops, dmin, with_eq=P.po_dir is not None)
     if not refl:
         raise RuntimeError('No reflections for the PT backend.')
     reps, _nc = cosets(g.ops)
@@ -140,7 +150,13 @@ def compile(ctx: PTContext) -> Plan:
     rep_rot = np.array([o.r for o in reps], dtype=np.int32)
     rep_trans = np.array([o.t_frac for o in reps], dtype=np.float64)
     nv = len(P.refined)
-    return Plan(hkl, mult, rep_rot, rep_trans, dmin, nv, int(ctx.setup['chains']), 3 * nv + 12, len(P.tth), len(refl))
+    eq_start = eq_hkl = None
+    if P.po_dir is not None:
+        counts = np.array([len(r.eq) for r in refl], dtype=np.int32)
+        eq_start = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+        eq_hkl = np.concatenate([np.asarray(r.eq, dtype=np.int32).reshape(-1, 3) for r in refl]).astype(np.int32)
+    return Plan(hkl, mult, rep_rot, rep_trans, dmin, nv, int(ctx.setup['chains']), 3 * nv + 12, len(P.tth), len(refl),
+                eq_start, eq_hkl)
 
 
 class PTSession:
@@ -192,6 +208,12 @@ class PTSession:
         pr.chains = self.plan.chains
         pr.max_temp = float(ctx.setup['maxTemp'])
         pr.seed = int(ctx.setup['seed']) & 0xFFFFFFFF
+        if P.po_dir is not None:
+            pr.has_po = 1
+            pr.eq_start = a(self.plan.eq_start, np.int32)
+            pr.eq_hkl = a(self.plan.eq_hkl, np.int32)
+            for i in range(3):
+                pr.po_dir[i] = float(P.po_dir[i])
         h = C.c_void_p()
         check(self.lib.p6_pt_create(C.byref(pr), int(device), C.byref(h)))
         self.h = h
@@ -477,6 +499,23 @@ def nacl_problem(seed: int = 1, tth0: float = 10.0, tth1: float = 120.0, step: f
     return prob
 
 
+def with_preferred_orientation(prob: PTProblem, direction: Sequence[float], r: float = 1.0, refine: bool = True,
+                               lo: float = 0.5, hi: float = 2.0) -> PTProblem:
+    """A copy of ``prob`` with March-Dollase preferred orientation along the
+    reciprocal-lattice ``direction`` (js/rietveld_core.js:824-853): the March
+    parameter r is appended to the full vector after the background and, with
+    ``refine``, to the refined parameters with the bounds [lo, hi]."""
+    import copy
+    out = copy.copy(prob)
+    out.po_dir = tuple(float(v) for v in direction)
+    out.values = np.concatenate([np.asarray(prob.values, dtype=np.float64)[:len(FULL_NAMES) + prob.n_bkg], [r]])
+    if refine:
+        out.refined = list(prob.refined) + ['po']
+        out.lo = np.concatenate([np.asarray(prob.lo, dtype=np.float64), [lo]])
+        out.hi = np.concatenate([np.asarray(prob.hi, dtype=np.float64), [hi]])
+    return out
+
+
 def set_bounds(prob: PTProblem, truth: np.ndarray):
     t = {n: truth[prob.full_index(n)] for n in prob.refined}
     lo = {'scale': 0.5 * t['scale'], 'a': 0.98 * t['a'], 'Biso': 0.0, 'U': 0.0, 'V': -20.0, 'W': 0.0, 'zero': -0.1}
@@ -518,7 +557,8 @@ def start_vectors(prob: PTProblem, truth_x: np.ndarray, n: int, seed: int = 1) -
     return out
 
 
-STEP_CAP = {'scale': None, 'a': 'cell', 'Biso': 2.0, 'U': 'profile', 'V': 'profile', 'W': 'profile', 'zero': 0.1}
+STEP_CAP = {'scale': None, 'a': 'cell', 'Biso': 2.0, 'U': 'profile', 'V': 'profile', 'W': 'profile', 'zero': 0.1,
+            'po': 0.25}
 
 
 def natural_scales(prob: PTProblem, x: np.ndarray) -> np.ndarray:

@@ -185,3 +185,48 @@ def test_refine_reaches_the_target_rwp(nacl):
     assert r['rwp'] <= target
     assert r['time_to_target'] is not None and r['time_to_target'] <= r['seconds']['lm']
     assert abs(M.cost(r['x']) - r['chi2']) <= 1e-9 * r['chi2']
+
+
+# ---------------------------------------------------------------------------
+# March-Dollase preferred orientation (js/rietveld_core.js:824-853), refined
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope='module')
+def nacl_po(nacl, oracle):
+    from powder6_b200.pt_gpu import with_preferred_orientation
+    P, M, truth = nacl
+    Pp = with_preferred_orientation(P, (1, 1, 0), 1.0, lo=0.5, hi=2.0)
+    return Pp, oracle.PtModel(Pp, dmin=reflection_dmin(Pp)), np.append(truth, 0.8)
+
+
+def test_preferred_orientation_costs_match_oracle(nacl_po):
+    """chi^2 with the March-Dollase factor (lanes over the equivalents, FP64)
+    within the tempering cost's 2e-6, at r = 0.6 .. 1.6 along [110]."""
+    P, M, x0 = nacl_po
+    xs = [x0] + [np.append(v[:-1], r) for v, r in zip(start_vectors(P, x0, 4, seed=21), (0.6, 1.0, 1.25, 1.6))]
+    with PTSession(ctx_of(P, x0, chains=len(xs))) as s:
+        g = s.costs(xs)
+        c64 = s.model_costs(xs)
+    for x, gc, gm in zip(xs, g, c64):
+        c = M.cost(x)
+        assert abs(gc - c) <= CHI2_RTOL * c, (gc, c)
+        assert abs(gm - c) <= 1e-10 * c, (gm, c)
+
+
+def test_preferred_orientation_normal_equations_and_lm_match_oracle(nacl_po):
+    """The r column is the reference's forward difference; A, g, f and an LM
+    run from r = 0.8 match the oracle as the other parameters do."""
+    P, M, x0 = nacl_po
+    x = near_truth(x0)
+    with PTSession(ctx_of(P, x0, chains=2)) as s:
+        A, g, f = s.normal(x)
+        xg, ig = s.lm(x, 30)
+    Ao, go, fo = M.normal(x)
+    assert abs(f - fo) <= 1e-10 * fo
+    d = np.sqrt(np.diag(Ao))
+    assert d[-1] > 0
+    assert np.max(np.abs(A - Ao) / np.outer(d, d)) < 1e-7
+    assert np.max(np.abs(g - go) / (d * math.sqrt(fo))) < 1e-7
+    xo, io = M.lm(x, 30)
+    assert ig['code'] == io['code'] and ig['accepted'] == io['accepted']
+    assert abs(ig['chi2'] - io['chi2']) <= 1e-9 * io['chi2']
+    assert np.allclose(xg, xo, rtol=1e-7, atol=1e-9)

@@ -150,3 +150,68 @@ def test_linear_start_solves_the_scale(nacl):
     x, f = M.linear_start(x0)
     assert abs(x[0] - truth[0]) < 1e-3 * truth[0]
     assert f < M.cost(x0)
+
+
+# ---------------------------------------------------------------------------
+# March-Dollase preferred orientation (js/rietveld_core.js:824-853)
+# ---------------------------------------------------------------------------
+def _po_lib(oracle):
+    lib = oracle.load()
+    lib.p6o_po_factor.restype = C.c_double
+    lib.p6o_po_factor.argtypes = [C.POINTER(oracle.PtProblem), C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+    return lib
+
+
+def _po_restated(cell, rots, h, d, r):
+    """Independent restatement: the reciprocal metric as the inverse of the
+    direct metric, equivalents h R without duplicates, the mean of
+    (r^2 c^2 + (1 - c^2) / r)^(-3/2)."""
+    a, b, c, al, be, ga = cell
+    ca, cb, cg = (math.cos(math.radians(t)) for t in (al, be, ga))
+    G = np.array([[a * a, a * b * cg, a * c * cb], [a * b * cg, b * b, b * c * ca], [a * c * cb, b * c * ca, c * c]])
+    Gs = np.linalg.inv(G)
+    eqs = {tuple(int(v) for v in np.asarray(h) @ np.asarray(R).reshape(3, 3)) for R in rots}
+    d = np.asarray(d, dtype=np.float64)
+    vals = []
+    for e in eqs:
+        e = np.asarray(e, dtype=np.float64)
+        cos = (e @ Gs @ d) / math.sqrt((e @ Gs @ e) * (d @ Gs @ d))
+        c2 = min(1.0, cos * cos)
+        vals.append((r * r * c2 + (1 - c2) / r) ** -1.5)
+    return float(np.mean(vals))
+
+
+def test_march_dollase_factor_closed_form_and_restatement(oracle):
+    """Cubic (002) along [001]: two equivalents parallel, four perpendicular,
+    so the factor is (2 r^-3 + 4 r^1.5) / 6; r = 1 gives 1; a monoclinic cell
+    (P2_1/c, beta = 104 deg) against the restatement with the inverse metric."""
+    from powder6_b200.pt_gpu import with_preferred_orientation
+    from powder6_b200.symmetry import space_group
+    lib = _po_lib(oracle)
+    P = with_preferred_orientation(nacl_problem(seed=1), (0, 0, 1), 0.7)
+    M = oracle.PtModel(P)
+    cub = np.array([5.64, 5.64, 5.64, 90.0, 90.0, 90.0])
+    for r in (0.6, 0.85, 1.0, 1.4):
+        got = lib.p6o_po_factor(C.byref(M.p), cub.ctypes.data, r, 0, 0, 2)
+        assert abs(got - (2 * r ** -3 + 4 * r ** 1.5) / 6) < 1e-13
+    assert lib.p6o_po_factor(C.byref(M.p), cub.ctypes.data, 1.0, 1, 1, 1) == 1.0
+    P14 = with_preferred_orientation(nacl_problem(seed=1), (1, 0, 2), 0.8)
+    P14.group_number = 14
+    M14 = oracle.PtModel(P14)
+    rots = [o.r for o in space_group(14).ops]
+    mono = np.array([7.1, 9.3, 11.2, 90.0, 104.0, 90.0])
+    for hkl in ((1, 0, 0), (1, 2, 3), (-2, 1, 1), (0, 4, 1)):
+        for r in (0.55, 0.8, 1.3):
+            got = lib.p6o_po_factor(C.byref(M14.p), mono.ctypes.data, r, *hkl)
+            want = _po_restated(mono, rots, hkl, (1, 0, 2), r)
+            assert abs(got - want) < 1e-12 * want, (hkl, r, got, want)
+
+
+def test_march_dollase_cost_reduces_to_plain_at_r_one(nacl, oracle):
+    """r = 1 multiplies every height by exactly 1; r != 1 changes chi^2."""
+    from powder6_b200.pt_gpu import with_preferred_orientation
+    P, M, truth = nacl
+    Pp = with_preferred_orientation(P, (0, 0, 1), 1.0)
+    Mp = oracle.PtModel(Pp, dmin=reflection_dmin(P))
+    assert Mp.cost(np.append(truth, 1.0)) == M.cost(truth)
+    assert Mp.cost(np.append(truth, 0.8)) > 1.1 * M.cost(truth)
