@@ -245,6 +245,12 @@ typedef struct {
   const int32_t *eq_start; /* n_refl + 1 */
   const int32_t *eq_hkl;   /* 3 per equivalent */
   double po_dir[3];
+  /* SL/HL axial-divergence asymmetry of the TCH profile (js/profile.js:608-617,
+   * :686-722, :737-740, area correction :799-826; GPU js/pt_gpu.js:332-353).
+   * has_asym = 0: symmetric.  Otherwise SL and HL are the two full-vector
+   * entries after the background (and after r when has_po); each peak gets
+   * asym = SL / tan(theta) + HL, a doubled window and the area correction. */
+  int has_asym;
 } p6_pt_problem;
 
 typedef struct p6_pt_session p6_pt_session;

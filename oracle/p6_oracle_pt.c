@@ -68,6 +68,8 @@ typedef struct {
     /* March-Dollase preferred orientation: r = v[PT_BKG0 + nBkg], direction poDir (reciprocal lattice) */
     int hasPo;
     double poDir[3];
+    /* SL/HL asymmetry: SL = v[PT_BKG0 + nBkg + hasPo], HL the next entry */
+    int hasAsym;
 } p6o_pt_problem;
 
 static const double GCONV = 0.023548200450309493;   /* sqrt(8 ln 2) / 100 */
@@ -104,13 +106,18 @@ static double peak_fwhm(double gG0, double gL0)
 }
 
 typedef struct {
-    double x0, inv, cL, cG, pedestal, maxd, area;
+    double x0, inv, cL, cG, pedestal, maxd, area, asym;
 } voigt_t;
 
+/* evalVoigt (profile.js:731-759), TCH: the asymmetry stretches one flank. */
 static double eval_voigt(double x, const voigt_t *p, double maxd, double pedestal)
 {
     double delta = x - p->x0;
     if (delta > maxd || delta < -maxd) return 0.0;
+    if (p->asym != 0 && fabs(delta) >= 1e-9) {
+        double t = fmax(-0.95, fmin(0.95, p->asym * delta));
+        delta /= (1.0 - t);
+    }
     double dg = (delta * p->inv) * (delta * p->inv);
     double g = exp(-CG * dg);
     double l = 1.0 / (1.0 + 4.0 * dg);
@@ -118,9 +125,75 @@ static double eval_voigt(double x, const voigt_t *p, double maxd, double pedesta
     return v > 0 ? v : 0.0;
 }
 
-/* prepareVoigt, TCH branch (profile.js:603-722), no asymmetry. */
-static void prepare_tch(double tthPeak, double x0, const double *v, double fwhmMin, voigt_t *p)
+/* sharkoErfc (profile.js:791-797): Numerical Recipes' erfcc, fractional error below 1.2e-7. */
+static double erfcc(double x)
 {
+    double z = fabs(x), t = 1 / (1 + 0.5 * z);
+    double ans = t * exp(-z * z - 1.26551223 + t * (1.00002368 + t * (0.37409196 + t * (0.09678418 +
+                 t * (-0.18628806 + t * (0.27886807 + t * (-1.13520398 + t * (1.48851587 +
+                 t * (-0.82215223 + t * 0.17087277)))))))));
+    return x >= 0 ? ans : 2 - ans;
+}
+
+/* asymmetryAreaCorrection (profile.js:799-826): the area the asymmetry adds to
+ * the unit-height peak; H is the TCH fwhm, R the truncation radius. */
+static double asym_area_correction(const voigt_t *prep, double H, double R)
+{
+    static const double X[4] = {0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363};
+    static const double W[4] = {0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763};
+    if (!(prep->asym != 0) || !(R > 0)) return 0;
+    voigt_t as = *prep, sy = *prep;
+    as.x0 = 0; as.pedestal = 0;
+    sy.x0 = 0; sy.pedestal = 0; sy.asym = 0;
+    const double a = prep->asym, w = fmax(1e-6, fmax(1e-6, H));
+    const double clampAt = 0.95 / fabs(a), D = fmax(R, fmin(clampAt, 4096 * w));
+    double total = 0;
+    for (int sd = 0; sd < 2; sd++) {
+        const double side = sd ? 1 : -1;
+        double lo = 0, e = 0.25 * w;
+        for (;;) {
+            double hi = fmin(e, D);
+            for (int pass = 0; pass < 2; pass++) {
+                double plo = lo, phi = hi;
+                if (pass == 0) {
+                    if (!(clampAt > lo && clampAt < hi)) continue;
+                    phi = clampAt;
+                }
+                double m = 0.5 * (plo + phi), h = 0.5 * (phi - plo), sum = 0;
+                for (int i = 0; i < 4; i++)
+                    for (int sg = -1; sg <= 1; sg += 2) {
+                        double d = side * (m + sg * h * X[i]);
+                        sum += W[i] * (eval_voigt(d, &as, INFINITY, 0) - eval_voigt(d, &sy, INFINITY, 0));
+                    }
+                total += sum * h;
+                if (pass == 0) lo = clampAt;
+            }
+            lo = hi;
+            if (hi >= D) break;
+            e *= 2;
+        }
+        const double k = 1 - fmax(-0.95, fmin(0.95, a * side * D));
+        const double xs[2] = {D / k, D};
+        double tl[2];
+        for (int q = 0; q < 2; q++)
+            tl[q] = prep->cL * 0.5 * H * (0.5 * PI_ - atan(2 * xs[q] / H)) +
+                    prep->cG * 0.5 * H * sqrt(PI_ / CG) * erfcc(sqrt(CG) * xs[q] / H);
+        total += k * tl[0] - tl[1];
+    }
+    return total;
+}
+
+/* prepareVoigt, TCH branch (profile.js:603-722); asymIdx >= 0: v[asymIdx] = SL, v[asymIdx + 1] = HL. */
+static void prepare_tch_asym(double tthPeak, double x0, const double *v, double fwhmMin, int asymIdx, voigt_t *p)
+{
+    double asym = 0;
+    if (asymIdx >= 0) {
+        double SL = v[asymIdx], HL = v[asymIdx + 1];
+        if ((SL != 0 || HL != 0) && tthPeak >= 0.1 && tthPeak < 180) {
+            double th = fmax(1e-6, fmin(PI_ / 2.0 - 1e-6, tthPeak * (PI_ / 180) / 2.0)), t = tan(th);
+            if (fabs(t) >= 1e-9) asym = SL / t + HL;
+        }
+    }
     double gG = fwhmMin, gL = fwhmMin;
     double thetaRad = tthPeak * (PI_ / 180) / 2;
     double safe = fmin(thetaRad, PI_ / 2.0 - 1e-6);
@@ -150,13 +223,20 @@ static void prepare_tch(double tthPeak, double x0, const double *v, double fwhmM
     p->inv = 1 / fwhm;
     p->cL = cL;
     p->cG = cG;
+    p->asym = asym;
     p->area = (cL * (1 / pv_l0()) + cG * (1 / pv_g0())) * fwhm;
     double winFwhm = fmax(1e-6, fwhm);
     double etaWin = fmax(0, fmin(1, eta));
     double mult = WIN_G + (WIN_L - WIN_G) * etaWin;
-    double R = fmin(WIN_MAX, mult * fmax(0.01, winFwhm));
+    double R = fmin(WIN_MAX, mult * fmax(0.01, winFwhm) * (asym != 0 ? 2.0 : 1.0));
     p->pedestal = fmax(eval_voigt(x0 + R, p, INFINITY, 0.0), eval_voigt(x0 - R, p, INFINITY, 0.0));
     p->maxd = R;
+    p->area += asym_area_correction(p, fwhm, R);
+}
+
+static void prepare_tch(double tthPeak, double x0, const double *v, double fwhmMin, voigt_t *p)
+{
+    prepare_tch_asym(tthPeak, x0, v, fwhmMin, -1, p);
 }
 
 static double lp_factor(double tth, double K)
@@ -196,6 +276,8 @@ static double inv_dsq_cell(const double *c6, double h, double k, double l, int *
     return h * h * (as * as) + k * k * (bs * bs) + l * l * (cs * cs) + h * k * (2 * as * bs * cGs) +
            k * l * (2 * bs * cs * cAs) + h * l * (2 * as * cs * cBs);
 }
+
+#define AIDX(P) ((P)->hasAsym ? PT_BKG0 + (P)->nBkg + ((P)->hasPo ? 1 : 0) : -1)
 
 /* Coefficients of the 1/d^2 form: aa, bb, cc, ab, bc, ac (the hk, kl, hl terms). */
 static void cell_form(const double *c6, double f[6])
@@ -314,7 +396,7 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
         double bragg = tthR[r];
         if (!(isfinite(bragg) && bragg > 0 && bragg < 180)) continue;
         double base = bragg + v[PT_ZERO];
-        prepare_tch(base, base, v, P->minFwhm, &p1[r]);
+        prepare_tch_asym(base, base, v, P->minFwhm, AIDX(P), &p1[r]);
         double lo = base - p1[r].maxd, hi = base + p1[r].maxd;
         int start = lower_bound(P->tth, n, lo), stop = start;
         if (start >= n) continue;
@@ -332,10 +414,10 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
             if (fabs(sin2) >= 1) continue;
             double tth2 = 2 * asin(sin2) / DEG2RAD;
             double base2 = tth2 + v[PT_ZERO];
-            prepare_tch(base2, base2, v, P->minFwhm, &p2[r]);
+            prepare_tch_asym(base2, base2, v, P->minFwhm, AIDX(P), &p2[r]);
             /* prep1 of this reflection (built in the first pass even if its window missed the axis) */
             voigt_t ref1;
-            prepare_tch(bragg + v[PT_ZERO], bragg + v[PT_ZERO], v, P->minFwhm, &ref1);
+            prepare_tch_asym(bragg + v[PT_ZERO], bragg + v[PT_ZERO], v, P->minFwhm, AIDX(P), &ref1);
             double lpr = lp_factor(base2, P->polK) / lp_factor(ref1.x0, P->polK);
             w2[r] = P->ratio * ref1.area / p2[r].area * lpr;
             double lo = base2 - p2[r].maxd, hi = base2 + p2[r].maxd;
@@ -356,7 +438,7 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
         if (!isfinite(tthR[r])) continue;
         double tc = tthR[r] + v[PT_ZERO];
         voigt_t ref1;
-        prepare_tch(tc, tc, v, P->minFwhm, &ref1);
+        prepare_tch_asym(tc, tc, v, P->minFwhm, AIDX(P), &ref1);
         double K = ref1.area;
         if (!(K > 0)) continue;
         double lp = lp_factor(tc, P->polK);
@@ -516,6 +598,18 @@ void p6o_prepare_tch(const double *v, double minFwhm, double tthPeak, double *ou
     prepare_tch(tthPeak, tthPeak, v, minFwhm, &p);
     out[0] = p.x0; out[1] = p.inv; out[2] = p.cL; out[3] = p.cG; out[4] = p.pedestal; out[5] = p.maxd; out[6] = p.area;
 }
+/* prepareVoigt with SL, HL: out = x0, inv, cL, cG, pedestal, maxd, area (with the asymmetry's correction), asym */
+void p6o_prepare_tch_asym(const double *v, double minFwhm, double tthPeak, double SL, double HL, double *out)
+{
+    double vv[16];
+    memcpy(vv, v, sizeof(double) * 14);
+    vv[14] = SL;
+    vv[15] = HL;
+    voigt_t p;
+    prepare_tch_asym(tthPeak, tthPeak, vv, minFwhm, 14, &p);
+    out[0] = p.x0; out[1] = p.inv; out[2] = p.cL; out[3] = p.cG; out[4] = p.pedestal; out[5] = p.maxd; out[6] = p.area;
+    out[7] = p.asym;
+}
 /* evalVoigt without truncation or pedestal, for area checks */
 double p6o_voigt_raw(double delta, double inv, double cL, double cG)
 {
@@ -529,11 +623,13 @@ double p6o_voigt_raw(double delta, double inv, double cL, double cG)
 /* (fdStep :526-538, defaultLimits :486-508, stepCap :511-524), Cholesky and */
 /* solveSPD (:1304-1335).  Parameters are identified by their full index.    */
 /* ------------------------------------------------------------------------ */
-enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO };
+enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO, K_SL, K_HL };
 
 static int kind_of(const p6o_pt_problem *P, int fi)
 {
     if (P->hasPo && fi == PT_BKG0 + P->nBkg) return K_PO;
+    if (P->hasAsym && fi == AIDX(P)) return K_SL;
+    if (P->hasAsym && fi == AIDX(P) + 1) return K_HL;
     if (fi == PT_SCALE) return K_SCALE;
     if (fi >= PT_A && fi <= PT_C) return K_CELL;
     if (fi >= PT_AL && fi <= PT_GA) return K_ANGLE;
@@ -568,6 +664,7 @@ static void default_limits(int kind, double v, double *lo, double *hi)
     case K_ZERO: *lo = -2; *hi = 2; return;
     case K_LORENTZ: *lo = 0; *hi = INFINITY; return;
     case K_PO: *lo = 0.1; *hi = 5; return;
+    case K_SL: *lo = 0; *hi = INFINITY; return;
     default: *lo = -INFINITY; *hi = INFINITY; return;
     }
 }
@@ -581,6 +678,7 @@ static double step_cap(int kind, double v)
     case K_BISO: return 2;
     case K_ZERO: return 0.1;
     case K_PO: return 0.25;
+    case K_SL: case K_HL: return 0.01;
     case K_PROFILE: case K_LORENTZ: return 0.5 * fmax(fabs(v), 5);
     default: return INFINITY;
     }

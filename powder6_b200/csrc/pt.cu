@@ -66,12 +66,14 @@ struct Chain {
 struct Peak {            // one contribution (K-alpha-1 or K-alpha-2) of a reflection
   double x0, maxd;       // centre and truncation radius, degrees
   float inv, cL, cG, pedestal;
+  float asym;            // SL / tan(theta) + HL (0: symmetric)
   int lo, hi;            // window [lo, hi) in point indices
 };
 
 struct PeakD {           // the same in FP64 throughout (least-squares finish)
   double x0, maxd;
   double inv, cL, cG, pedestal;
+  double asym;
   int lo, hi;
 };
 
@@ -94,6 +96,7 @@ struct Params {
   int stageObs;          // observed pattern staged in shared memory
   int *errFlag;
   int hasPo;             // March-Dollase factor on; r = v[PBKG0 + nBkg]
+  int asymIdx;           // full index of SL (HL follows); -1: no asymmetry
   const int *eqStart;    // nRefl + 1
   const int *eqHkl;      // 3 per equivalent
   double poDir[3];       // reciprocal-lattice direction
@@ -128,9 +131,76 @@ __device__ __forceinline__ double voigt64(double delta, double inv, double cL, d
   const double v = cL * (1.0 / (1.0 + 4.0 * dg)) + cG * exp(-kCg * dg) - pedestal;
   return v > 0 ? v : 0.0;
 }
-// prepareVoigt, TCH branch: widths at tthPeak, centre x0.  Returns the analytic area.
+// SL/HL axial-divergence asymmetry (js/profile.js:737-740): one flank is
+// stretched and the other compressed, delta / (1 - t), t = asym delta
+// clamped at +-0.95.  asym = 0 returns delta unchanged.
+__device__ __forceinline__ double asym_delta(double delta, double asym) {
+  if (asym != 0 && fabs(delta) >= 1e-9) delta /= 1.0 - fmax(-0.95, fmin(0.95, asym * delta));
+  return delta;
+}
+__device__ __forceinline__ float asym_deltaf(float delta, float asym) {
+  if (asym != 0.f && fabsf(delta) >= 1e-9f) delta /= 1.0f - fmaxf(-0.95f, fminf(0.95f, asym * delta));
+  return delta;
+}
+// asymmetryAreaCorrection (js/profile.js:799-826): the area the asymmetry adds
+// to a unit-height peak of width H, mixing (cL, cG), window R.  The
+// (asymmetric - symmetric) difference is integrated with 8-point
+// Gauss-Legendre panels that double in width from 0.25 H out to
+// D = max(R, min(0.95 / |a|, 4096 H)), split at the clamp point; beyond D the
+// stretch is a constant k and both tails are closed-form.
+__device__ double asym_area(double a, double H, double cL, double cG, double R) {
+  if (a == 0 || !(R > 0)) return 0.0;
+  const double inv = 1 / H, w = fmax(1e-6, H);
+  const double clampAt = 0.95 / fabs(a), D = fmax(R, fmin(clampAt, 4096 * w));
+  const double gx[4] = {0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363};
+  const double gw[4] = {0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763};
+  auto panel = [&](double lo, double hi, double side) {
+    const double m = 0.5 * (lo + hi), h = 0.5 * (hi - lo);
+    double s = 0;
+    for (int i = 0; i < 4; ++i)
+      for (int sg = -1; sg <= 1; sg += 2) {
+        const double d = side * (m + sg * h * gx[i]);
+        s += gw[i] * (voigt64(asym_delta(d, a), inv, cL, cG, 0.0) - voigt64(d, inv, cL, cG, 0.0));
+      }
+    return s * h;
+  };
+  auto tail = [&](double x) {
+    return cL * 0.5 * H * (0.5 * kPi - atan(2 * x / H)) + cG * 0.5 * H * sqrt(kPi / kCg) * erfc(sqrt(kCg) * x / H);
+  };
+  double total = 0;
+  for (int sd = 0; sd < 2; ++sd) {
+    const double side = sd ? 1.0 : -1.0;
+    double lo = 0, e = 0.25 * w;
+    for (int it = 0; it < 64; ++it) {
+      const double hi = fmin(e, D);
+      if (clampAt > lo && clampAt < hi) {
+        total += panel(lo, clampAt, side);
+        lo = clampAt;
+      }
+      total += panel(lo, hi, side);
+      lo = hi;
+      if (hi >= D) break;
+      e *= 2;
+    }
+    const double k = 1 - fmax(-0.95, fmin(0.95, a * side * D));
+    total += k * tail(D / k) - tail(D);
+  }
+  return total;
+}
+// prepareVoigt, TCH branch (js/profile.js:603-722): widths at tthPeak, centre
+// x0, the SL/HL asymmetry when asymIdx >= 0 (v[asymIdx] = SL, v[asymIdx + 1]
+// = HL).  Returns the area of the unit-height peak (analytic, plus the
+// asymmetry's correction).
 template <class PK>
-__device__ double prepare(const double *v, double minFwhm, double tthPeak, double x0, PK &p) {
+__device__ double prepare(const double *v, double minFwhm, double tthPeak, double x0, int asymIdx, PK &p) {
+  double asym = 0;
+  if (asymIdx >= 0) {
+    const double SL = v[asymIdx], HL = v[asymIdx + 1];
+    if ((SL != 0 || HL != 0) && tthPeak >= 0.1 && tthPeak < 180) {
+      const double th = fmax(1e-6, fmin(kPi / 2.0 - 1e-6, tthPeak * (kPi / 180) / 2.0)), t = tan(th);
+      if (fabs(t) >= 1e-9) asym = SL / t + HL;
+    }
+  }
   double gG = minFwhm, gL = minFwhm;
   const double theta = tthPeak * (kPi / 180) / 2;
   const double safe = fmin(theta, kPi / 2.0 - 1e-6);
@@ -157,8 +227,9 @@ __device__ double prepare(const double *v, double minFwhm, double tthPeak, doubl
   if (s > 0 && isfinite(s)) { cL = wL / s; cG = wG / s; }
   const double inv = 1 / fwhm;
   const double mult = kWinG + (kWinL - kWinG) * fmax(0.0, fmin(1.0, eta));
-  const double R = fmin(kWinMax, mult * fmax(0.01, fmax(1e-6, fwhm)));
-  const double ped = fmax(voigt64(R, inv, cL, cG, 0.0), voigt64(-R, inv, cL, cG, 0.0));
+  const double R = fmin(kWinMax, mult * fmax(0.01, fmax(1e-6, fwhm)) * (asym != 0 ? 2.0 : 1.0));
+  const double ped =
+      fmax(voigt64(asym_delta(R, asym), inv, cL, cG, 0.0), voigt64(asym_delta(-R, asym), inv, cL, cG, 0.0));
   p.x0 = x0;
   p.maxd = R;
   using T = decltype(p.inv);
@@ -166,7 +237,8 @@ __device__ double prepare(const double *v, double minFwhm, double tthPeak, doubl
   p.cL = (T)cL;
   p.cG = (T)cG;
   p.pedestal = (T)ped;
-  return (cL * (1 / l0) + cG * (1 / g0)) * fwhm;
+  p.asym = (T)asym;
+  return (cL * (1 / l0) + cG * (1 / g0)) * fwhm + asym_area(asym, fwhm, cL, cG, R);
 }
 __device__ __forceinline__ double lp_factor(double tth, double K) {
   if (!isfinite(tth) || tth <= 0 || tth >= 180) return 1;
@@ -326,7 +398,7 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
         const double bragg = 2 * asin(sinT) * kR2D;
         if (line == 0) {
           const double base = bragg + v[PZERO];
-          area = prepare(v, P.minFwhm, base, base, pk1[k]);
+          area = prepare(v, P.minFwhm, base, base, P.asymIdx, pk1[k]);
           lp = lp_factor(base, P.polK);
           const int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = upper_bound(tth, P.n, base + pk1[k].maxd, lo);
           pk1[k].lo = lo;
@@ -338,7 +410,7 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
             const double sin2 = sin(bragg * kD2R / 2.0) * (P.lambda2 / P.lambda1);
             if (fabs(sin2) < 1) {
               const double base2 = 2 * asin(sin2) / kD2R + v[PZERO];
-              area = prepare(v, P.minFwhm, base2, base2, pk2[k]);
+              area = prepare(v, P.minFwhm, base2, base2, P.asymIdx, pk2[k]);
               lp = lp_factor(base2, P.polK);
               const int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd),
                         hi2 = upper_bound(tth, P.n, base2 + pk2[k].maxd, lo2);
@@ -395,13 +467,13 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
       float col = 0.f;
       if (o1 && in && i >= pk1[k].lo && i < pk1[k].hi) {
         const Peak &p = pk1[k];
-        const float d = (float)(x - p.x0) * p.inv, dg = d * d;
+        const float d = asym_deltaf((float)(x - p.x0), p.asym) * p.inv, dg = d * d;
         const float val = p.cL * (1.0f / (1.0f + 4.0f * dg)) + p.cG * expf(-(float)kCg * dg) - p.pedestal;
         col += val > 0.f ? val : 0.f;
       }
       if (o2 && in && i >= pk2[k].lo && i < pk2[k].hi) {
         const Peak &p = pk2[k];
-        const float d = (float)(x - p.x0) * p.inv, dg = d * d;
+        const float d = asym_deltaf((float)(x - p.x0), p.asym) * p.inv, dg = d * d;
         const float val = p.cL * (1.0f / (1.0f + 4.0f * dg)) + p.cG * expf(-(float)kCg * dg) - p.pedestal;
         col += w2[k] * (val > 0.f ? val : 0.f);
       }
@@ -658,11 +730,11 @@ __global__ void __launch_bounds__(kThreads) pt_pattern64_kernel(const Params P, 
       double col = 0.0;
       if (o1 && in && i >= pk1[k].lo && i < pk1[k].hi) {
         const PeakD &p = pk1[k];
-        col += voigt64(x - p.x0, p.inv, p.cL, p.cG, p.pedestal);
+        col += voigt64(asym_delta(x - p.x0, p.asym), p.inv, p.cL, p.cG, p.pedestal);
       }
       if (o2 && in && i >= pk2[k].lo && i < pk2[k].hi) {
         const PeakD &p = pk2[k];
-        col += w2[k] * voigt64(x - p.x0, p.inv, p.cL, p.cG, p.pedestal);
+        col += w2[k] * voigt64(asym_delta(x - p.x0, p.asym), p.inv, p.cL, p.cG, p.pedestal);
       }
       yp += h1[k] * col;
       yu1 += u1[k] * col;
@@ -923,6 +995,8 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
     if (pr->index[j] < 0 || pr->index[j] >= pr->n_full) return set_error(P6_ERR_INVALID_ARG, "parameter index out of range");
   for (int i = 1; i < pr->n_points; ++i)
     if (!(pr->tth[i] > pr->tth[i - 1])) return set_error(P6_ERR_INVALID_ARG, "the 2-theta axis must be ascending");
+  if (pr->has_asym && pr->n_full < PBKG0 + pr->n_bkg + (pr->has_po ? 1 : 0) + 2)
+    return set_error(P6_ERR_INVALID_ARG, "asymmetry: the full vector has no SL, HL entries");
   if (pr->has_po) {
     if (!pr->eq_start || !pr->eq_hkl) return set_error(P6_ERR_INVALID_ARG, "preferred orientation without equivalents");
     if (pr->n_full < PBKG0 + pr->n_bkg + 1)
@@ -972,6 +1046,7 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
   PT_TRY(pt_upload(s, pr->hi, (size_t)pr->nv, &P.hi));
   PT_TRY(pt_upload(s, pr->scales, (size_t)pr->nv, &P.scales));
   P.hasPo = pr->has_po ? 1 : 0;
+  P.asymIdx = pr->has_asym ? PBKG0 + pr->n_bkg + P.hasPo : -1;
   if (P.hasPo) {
     PT_TRY(pt_upload(s, pr->eq_start, (size_t)pr->n_refl + 1, &P.eqStart));
     PT_TRY(pt_upload(s, pr->eq_hkl, (size_t)3 * pr->eq_start[pr->n_refl], &P.eqHkl));
@@ -1160,10 +1235,12 @@ p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
 // the scalar control of lm() on the host.
 // ===========================================================================
 namespace {
-enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO };
+enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO, K_SL, K_HL };
 
 int lm_kind(const Params &P, int fi) {
   if (P.hasPo && fi == PBKG0 + P.nBkg) return K_PO;
+  if (P.asymIdx >= 0 && fi == P.asymIdx) return K_SL;
+  if (P.asymIdx >= 0 && fi == P.asymIdx + 1) return K_HL;
   if (fi == SCALE) return K_SCALE;
   if (fi >= PA && fi <= PC) return K_CELL;
   if (fi >= PAL && fi <= PGA) return K_ANGLE;
@@ -1193,6 +1270,7 @@ void lm_limits(int kind, double v, double *lo, double *hi) {
     case K_ZERO: *lo = -2; *hi = 2; return;
     case K_LORENTZ: *lo = 0; *hi = inf; return;
     case K_PO: *lo = 0.1; *hi = 5; return;
+    case K_SL: *lo = 0; *hi = inf; return;
     default: *lo = -inf; *hi = inf; return;
   }
 }
@@ -1204,6 +1282,7 @@ double lm_step_cap(int kind, double v) {
     case K_BISO: return 2;
     case K_ZERO: return 0.1;
     case K_PO: return 0.25;
+    case K_SL: case K_HL: return 0.01;
     case K_PROFILE: case K_LORENTZ: return 0.5 * std::max(std::fabs(v), 5.0);
     default: return std::numeric_limits<double>::infinity();
   }

@@ -63,6 +63,10 @@ class PTProblem:
     # reciprocal-lattice direction, or None (off).  Its parameter 'po' (r) is
     # the entry of the full vector after the background.
     po_dir: Optional[Sequence[float]] = None
+    # SL/HL axial-divergence asymmetry of the TCH profile (js/profile.js:608-617):
+    # when True, 'SL' and 'HL' are the full-vector entries after the background
+    # (and after 'po').
+    asym: bool = False
 
     @property
     def index(self) -> np.ndarray:
@@ -75,6 +79,10 @@ class PTProblem:
             if self.po_dir is None:
                 raise KeyError('po: the problem has no preferred-orientation direction')
             return len(FULL_NAMES) + self.n_bkg
+        if name in ('SL', 'HL'):
+            if not self.asym:
+                raise KeyError(f'{name}: the problem has no asymmetry')
+            return len(FULL_NAMES) + self.n_bkg + (1 if self.po_dir is not None else 0) + (name == 'HL')
         return FULL_NAMES.index(name)
 
     def apply(self, x: Sequence[float]) -> np.ndarray:
@@ -214,6 +222,7 @@ class PTSession:
             pr.eq_hkl = a(self.plan.eq_hkl, np.int32)
             for i in range(3):
                 pr.po_dir[i] = float(P.po_dir[i])
+        pr.has_asym = 1 if P.asym else 0
         h = C.c_void_p()
         check(self.lib.p6_pt_create(C.byref(pr), int(device), C.byref(h)))
         self.h = h
@@ -516,6 +525,25 @@ def with_preferred_orientation(prob: PTProblem, direction: Sequence[float], r: f
     return out
 
 
+def with_asymmetry(prob: PTProblem, SL: float = 0.0, HL: float = 0.0, refine: Sequence[str] = ('SL', 'HL'),
+                   bounds: Optional[Dict[str, tuple]] = None) -> PTProblem:
+    """A copy of ``prob`` with the SL/HL asymmetry (js/profile.js:608-617):
+    SL and HL are appended to the full vector (after the background and any
+    'po') and the names in ``refine`` to the refined parameters, with
+    ``bounds`` (default SL [0, 0.05], HL [-0.05, 0.05])."""
+    import copy
+    b = {'SL': (0.0, 0.05), 'HL': (-0.05, 0.05)}
+    b.update(bounds or {})
+    out = copy.copy(prob)
+    out.asym = True
+    n0 = len(FULL_NAMES) + prob.n_bkg + (1 if prob.po_dir is not None else 0)
+    out.values = np.concatenate([np.asarray(prob.values, dtype=np.float64)[:n0], [SL, HL]])
+    out.refined = list(prob.refined) + list(refine)
+    out.lo = np.concatenate([np.asarray(prob.lo, dtype=np.float64), [b[n][0] for n in refine]])
+    out.hi = np.concatenate([np.asarray(prob.hi, dtype=np.float64), [b[n][1] for n in refine]])
+    return out
+
+
 def set_bounds(prob: PTProblem, truth: np.ndarray):
     t = {n: truth[prob.full_index(n)] for n in prob.refined}
     lo = {'scale': 0.5 * t['scale'], 'a': 0.98 * t['a'], 'Biso': 0.0, 'U': 0.0, 'V': -20.0, 'W': 0.0, 'zero': -0.1}
@@ -558,7 +586,7 @@ def start_vectors(prob: PTProblem, truth_x: np.ndarray, n: int, seed: int = 1) -
 
 
 STEP_CAP = {'scale': None, 'a': 'cell', 'Biso': 2.0, 'U': 'profile', 'V': 'profile', 'W': 'profile', 'zero': 0.1,
-            'po': 0.25}
+            'po': 0.25, 'SL': 0.01, 'HL': 0.01}
 
 
 def natural_scales(prob: PTProblem, x: np.ndarray) -> np.ndarray:

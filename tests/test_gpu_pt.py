@@ -230,3 +230,49 @@ def test_preferred_orientation_normal_equations_and_lm_match_oracle(nacl_po):
     assert ig['code'] == io['code'] and ig['accepted'] == io['accepted']
     assert abs(ig['chi2'] - io['chi2']) <= 1e-9 * io['chi2']
     assert np.allclose(xg, xo, rtol=1e-7, atol=1e-9)
+
+
+# ---------------------------------------------------------------------------
+# SL/HL asymmetry (js/profile.js:608-617, :737-740, :799-826), refined
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope='module')
+def nacl_asym(nacl, oracle):
+    from powder6_b200.pt_gpu import with_asymmetry
+    P, M, truth = nacl
+    Pa = with_asymmetry(P, 0.0, 0.0, bounds={'SL': (0.0, 0.5), 'HL': (-0.2, 0.2)})
+    return Pa, oracle.PtModel(Pa, dmin=reflection_dmin(Pa)), np.append(truth, [0.2, 0.05])
+
+
+def test_asymmetry_costs_and_patterns_match_oracle(nacl_asym):
+    """Stretched flanks in the FP32 profile (chi^2 within 2e-6, pattern within
+    2e-5 of its maximum), the doubled window and the Gauss-Legendre area
+    correction in FP64, over SL 0 .. 0.4 and HL -0.1 .. 0.1."""
+    P, M, x0 = nacl_asym
+    xs = [x0] + [np.append(v[:-2], a) for v, a in
+                 zip(start_vectors(P, x0, 4, seed=31), ([0.0, 0.0], [0.4, -0.1], [0.05, 0.1], [0.0, -0.05]))]
+    with PTSession(ctx_of(P, x0, chains=len(xs))) as s:
+        g, ys = s.costs(xs, with_pattern=True)
+        c64 = s.model_costs(xs)
+    for x, gc, gm, y in zip(xs, g, c64, ys):
+        c, yo, _ = M.cost_full(P.apply(x), True)
+        assert abs(gc - c) <= CHI2_RTOL * c, (gc, c)
+        assert abs(gm - c) <= 1e-10 * c, (gm, c)
+        assert np.max(np.abs(y - yo)) <= PATTERN_ATOL_FRAC * np.max(np.abs(yo))
+
+
+def test_asymmetry_normal_equations_and_lm_match_oracle(nacl_asym):
+    P, M, x0 = nacl_asym
+    x = near_truth(x0)
+    with PTSession(ctx_of(P, x0, chains=2)) as s:
+        A, g, f = s.normal(x)
+        xg, ig = s.lm(x, 30)
+    Ao, go, fo = M.normal(x)
+    assert abs(f - fo) <= 1e-10 * fo
+    d = np.sqrt(np.diag(Ao))
+    assert d[-1] > 0 and d[-2] > 0
+    assert np.max(np.abs(A - Ao) / np.outer(d, d)) < 1e-7
+    assert np.max(np.abs(g - go) / (d * math.sqrt(fo))) < 1e-7
+    xo, io = M.lm(x, 30)
+    assert ig['code'] == io['code'] and ig['accepted'] == io['accepted']
+    assert abs(ig['chi2'] - io['chi2']) <= 1e-9 * io['chi2']
+    assert np.allclose(xg, xo, rtol=1e-7, atol=1e-9)

@@ -215,3 +215,56 @@ def test_march_dollase_cost_reduces_to_plain_at_r_one(nacl, oracle):
     Mp = oracle.PtModel(Pp, dmin=reflection_dmin(P))
     assert Mp.cost(np.append(truth, 1.0)) == M.cost(truth)
     assert Mp.cost(np.append(truth, 0.8)) > 1.1 * M.cost(truth)
+
+
+# ---------------------------------------------------------------------------
+# SL/HL asymmetry (js/profile.js:608-617, :737-740, :799-826)
+# ---------------------------------------------------------------------------
+def _raw_asym(delta, inv, cL, cG, asym):
+    """evalVoigt of the TCH shape, untruncated and without pedestal, restated."""
+    d = np.asarray(delta, dtype=np.float64)
+    if asym != 0:
+        t = np.clip(asym * d, -0.95, 0.95)
+        d = np.where(np.abs(d) >= 1e-9, d / (1.0 - t), d)
+    dg = (d * inv) ** 2
+    return cL / (1 + 4 * dg) + cG * np.exp(-2.772588722239781 * dg)
+
+
+def test_asymmetry_area_matches_the_brute_force_integral(oracle):
+    """The regressions.test.cjs:1583-1592 check: U = V = 0, W = X = 5, Y = 0,
+    SL = 0.05, HL = 0.02, minFwhm 0.005 at 2theta = 10: the area with the
+    asymmetry's correction equals the analytic area plus the brute-force
+    integral of (asymmetric - symmetric) within 2e-4, and differs from the
+    analytic area by more than 1 %."""
+    lib = oracle.load()
+    lib.p6o_prepare_tch_asym.restype = None
+    lib.p6o_prepare_tch_asym.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p]
+    lib.p6o_prepare_tch.restype = None
+    lib.p6o_prepare_tch.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    v = np.zeros(14)
+    v[7:12] = [0.0, 0.0, 5.0, 5.0, 0.0]
+    out = np.zeros(8)
+    lib.p6o_prepare_tch_asym(v.ctypes.data, 0.005, 10.0, 0.05, 0.02, out.ctypes.data)
+    sym = np.zeros(7)
+    lib.p6o_prepare_tch(v.ctypes.data, 0.005, 10.0, sym.ctypes.data)
+    inv, cL, cG, area, asym = out[1], out[2], out[3], out[6], out[7]
+    assert abs(asym - (0.05 / math.tan(math.radians(5.0)) + 0.02)) < 1e-12
+    assert abs(out[5] - min(10.0, 2 * sym[5])) < 1e-12 or out[5] == 10.0       # the window doubles
+    analytic = sym[6]
+    L, n = 3000 / inv, 200000
+    u = -1 + (np.arange(n) + 0.5) * 2 / n
+    x = L * u ** 3
+    dx = 3 * L * u * u * 2 / n
+    diff = float(((_raw_asym(x, inv, cL, cG, asym) - _raw_asym(x, inv, cL, cG, 0.0)) * dx).sum())
+    assert abs(area - (analytic + diff)) < 2e-4 * (analytic + diff), (area, analytic + diff)
+    assert area > 1.01 * analytic
+
+
+def test_asymmetry_cost_reduces_to_symmetric_at_zero(nacl, oracle):
+    """SL = HL = 0 leaves every peak symmetric: the same chi^2 bit for bit."""
+    from powder6_b200.pt_gpu import with_asymmetry
+    P, M, truth = nacl
+    Pa = with_asymmetry(P, 0.0, 0.0)
+    Ma = oracle.PtModel(Pa, dmin=reflection_dmin(P))
+    assert Ma.cost(np.append(truth, [0.0, 0.0])) == M.cost(truth)
+    assert Ma.cost(np.append(truth, [0.2, 0.05])) > 1.05 * M.cost(truth)
