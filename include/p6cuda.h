@@ -176,6 +176,11 @@ p6_status p6_wy_synchronize(p6_wy_session *s, double timeout_seconds);
 /* Exact coordinate access in the kernel's 32-bit fixed point (x * 2^32). */
 p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current);
 p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best);
+/* syncStateToGPU after a prune (js/swarm_wyckoff.js:2303-2336): current and
+ * best coordinates in fixed point and the particle states, written together
+ * so the chains that keep their assignment keep their best structure exactly. */
+p6_status p6_wy_write_state_fixed(p6_wy_session *s, const uint32_t *current, const uint32_t *best,
+                                  const p6_wy_particle_state *state);
 /* Parity support: record, for the next dispatch, each particle's proposal
  * (max_sites * 3 fixed-point words) and a record of 8 floats
  * {f_new, cc, pen_scaled, u, accepted, f_old, temp, step_before}. */

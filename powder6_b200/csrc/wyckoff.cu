@@ -1989,6 +1989,20 @@ p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current)
   return P6_OK;
 }
 
+p6_status p6_wy_write_state_fixed(p6_wy_session *s, const uint32_t *current, const uint32_t *best,
+                                  const p6_wy_particle_state *state) {
+  P6_ENTRY();
+  if (!s || !current || !best || !state) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t n = (size_t)s->P.numParticles * s->P.maxSites * 3;
+  P6_CUDA(cudaMemcpyAsync(s->dPos, current, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaMemcpyAsync(s->dPos + n, best, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaMemcpyAsync(s->dSt, state, (size_t)s->P.numParticles * sizeof(PState), cudaMemcpyHostToDevice,
+                          s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
 p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best) {
   P6_ENTRY();
   if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");

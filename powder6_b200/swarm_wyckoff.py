@@ -32,6 +32,7 @@ SW_DEFAULTS = dict(
     tempHot=0.05, tempCold=5e-4, rungs=8, swapEvery=10, stepInit=0.08, stepMin=2e-4, stepMax=0.5,
     targetAccept=0.3, stepAdapt=0.08, rampSteps=24, rampStart=0.25, rampFull=0.6,
     quenchSteps=600, quenchStep0=0.02, quenchStep1=5e-5, topN=20, numParticles=512, generations=2000,
+    minParticlesPerAssignment=24,
 )
 
 STATE_DTYPE = np.dtype([('fit', '<f4'), ('cc', '<f4'), ('pen', '<f4'), ('step_size', '<f4'), ('temp', '<f4'),
@@ -219,6 +220,12 @@ class WyckoffSession:
         a = np.ascontiguousarray(x, dtype=np.uint32)
         check(self.lib.p6_wy_write_positions_fixed(self.h, ptr(a)))
 
+    def write_state_fixed(self, current: np.ndarray, best: np.ndarray, state: np.ndarray):
+        c = np.ascontiguousarray(current, dtype=np.uint32)
+        b = np.ascontiguousarray(best, dtype=np.uint32)
+        st = np.ascontiguousarray(state, dtype=STATE_DTYPE)
+        check(self.lib.p6_wy_write_state_fixed(self.h, ptr(c), ptr(b), ptr(st)))
+
     def read_positions_fixed(self):
         n = self.num_particles * self.coords_per_particle
         cur = np.zeros(n, dtype=np.uint32)
@@ -318,6 +325,87 @@ def project_all(problem: WyckoffProblem, positions: np.ndarray, assign_of: np.nd
     return out.reshape(-1).astype(np.float32)
 
 
+def to_fixed(x: np.ndarray) -> np.ndarray:
+    """Fractional coordinates to the kernel's 32-bit fixed point (x mod 1) * 2^32."""
+    f = np.asarray(x, dtype=np.float64)
+    f = f - np.floor(f)
+    v = np.floor(f * 4294967296.0 + 0.5)
+    v[v >= 4294967296.0] -= 4294967296.0
+    return v.astype(np.uint64).astype(np.uint32)
+
+
+# ---------------------------------------------------------------------------
+# Particle budget over assignments: waves, weighting by dimension, pruning
+# (js/wyckoff_assign.js:1188-1278, js/swarm_wyckoff.js:1240-1290, :2291-2337).
+# ---------------------------------------------------------------------------
+def assignment_dims(problem: WyckoffProblem) -> List[int]:
+    """Free parameters of each assignment (at least 1): the particle weights."""
+    return [max(1, sum(int(st.w.n_free) for st in A.sites)) for A in problem.assignments]
+
+
+def weighted_assign(ids: Sequence[int], n: int, min_per: int, weights: Optional[Sequence[float]] = None) -> np.ndarray:
+    """weightedAssign (js/wyckoff_assign.js:1188-1229): a floor of
+    min(min_per, n // len(ids)) particles each, the surplus in proportion to
+    the weights, the rounding remainder to the largest weights; particles of
+    one assignment are contiguous, in the order of ``ids``."""
+    out = np.zeros(n, dtype=np.uint32)
+    ids = list(ids)
+    if not ids:
+        return out
+    floor_each = min(min_per, n // len(ids))
+    w = [max(1e-6, float(weights[a]) if weights is not None and weights[a] else 1.0) for a in ids]
+    total = sum(w)
+    surplus = max(0, n - floor_each * len(ids))
+    counts = [floor_each + int(math.floor(surplus * x / total)) for x in w]
+    order = sorted(range(len(ids)), key=lambda k: -w[k])
+    assigned, oi = sum(counts), 0
+    while assigned < n:
+        counts[order[oi % len(order)]] += 1
+        oi += 1
+        assigned += 1
+    guard = len(order) * 4 + 8
+    while assigned > n and guard > 0:
+        guard -= 1
+        k = order[len(order) - 1 - (oi % len(order))]
+        oi += 1
+        if counts[k] > 1:
+            counts[k] -= 1
+            assigned -= 1
+    p = 0
+    for a, c in zip(ids, counts):
+        for _ in range(c):
+            if p < n:
+                out[p] = a
+                p += 1
+    while p < n:
+        out[p] = ids[p % len(ids)]
+        p += 1
+    return out
+
+
+def prune_assignments(ids: Sequence[int], best: Dict[int, float], keep_fraction: float = 0.5,
+                      min_keep: int = 4) -> List[int]:
+    """pruneAssignments (js/wyckoff_assign.js:1274-1278): the best
+    max(min_keep, ceil(len * keep_fraction)) assignments by best fitness
+    (stable for ties; an assignment without a best ranks last)."""
+    ranked = sorted(ids, key=lambda a: -best.get(a, -math.inf))
+    keep = max(min_keep, math.ceil(len(ranked) * keep_fraction))
+    return ranked[:min(keep, len(ranked))]
+
+
+def assignments_per_wave(n: int, min_per: int = 24, weighted: bool = True) -> int:
+    """assignmentsPerWave (js/wyckoff_assign.js:1251-1253)."""
+    return max(1, n // (min_per * (2 if weighted else 1)))
+
+
+def allocate_waves(ids: Sequence[int], n: int, min_per: int = 24,
+                   weights: Optional[Sequence[float]] = None) -> List[List[int]]:
+    """allocateWaves (js/wyckoff_assign.js:1255-1265): the assignment ids of each wave, in order."""
+    per = assignments_per_wave(n, min_per, weights is not None)
+    ids = list(ids)
+    return [ids[i:i + per] for i in range(0, len(ids), per)]
+
+
 def initial_state(n: int, temps: np.ndarray, rnd: Callable[[], float], settings: Optional[dict] = None):
     d = dict(SW_DEFAULTS)
     d.update(settings or {})
@@ -391,6 +479,10 @@ class SearchResult:
     quench: Dict[str, float] = field(default_factory=dict)
     time_to_target: Optional[float] = None
     wall_s: float = 0.0
+    assignments: List[int] = field(default_factory=list)     # the wave's assignments
+    kept: List[int] = field(default_factory=list)            # still in contention after the prune
+    best_assignment: int = 0
+    per_assignment: Dict[int, float] = field(default_factory=dict)   # best cc of each assignment
 
 
 def quench_schedule(settings: Optional[dict] = None) -> np.ndarray:
@@ -454,10 +546,17 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                        settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
                        on_progress: Optional[Callable[[dict], None]] = None,
                        should_stop: Optional[Callable[[], bool]] = None, do_quench: bool = True,
-                       target_cc: Optional[float] = None) -> SearchResult:
-    """One assignment list, ``restarts`` independent restarts, all generations on
-    the device, then the quench of the per-assignment bests.  The winner is
-    re-scored at full resolution and the final penalty weight and
+                       target_cc: Optional[float] = None, assignment_ids: Optional[Sequence[int]] = None,
+                       prune: bool = True) -> SearchResult:
+    """One wave of assignments (``assignment_ids``, default all of the
+    problem's), ``restarts`` independent restarts, all generations on the
+    device, then the quench of the per-assignment bests.  Particles are shared
+    out in proportion to each assignment's free parameters (weightedAssign);
+    in the first restart, at generation max(20, 0.45 G), a wave of more than
+    four assignments keeps the better half (at least four) by best fitness
+    and hands the retired assignments' particles to the survivors with fresh
+    coordinates and fresh ladders (js/swarm_wyckoff.js:2291-2337).  The
+    winner is re-scored at full resolution and the final penalty weight and
     cross-checked on the CPU, as the reference reports.  With ``target_cc``,
     ``time_to_target`` is the wall time from the start to the first chunk
     boundary (or the end of the quench) at which the best cc reached it."""
@@ -470,8 +569,15 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     sess = session or WyckoffSession(problem, num_particles, run_key=seed, cos_mode=cos_mode, settings=settings)
     n = sess.num_particles
     nA = len(problem.assignments)
-    assign_of = (np.arange(n) % nA).astype(np.uint32) if nA > 1 else np.zeros(n, dtype=np.uint32)
-    assign_of.sort()
+    ids = list(range(nA)) if assignment_ids is None else [int(a) for a in assignment_ids]
+    if not ids or min(ids) < 0 or max(ids) >= nA:
+        raise ValueError('assignment ids out of range')
+    wave_ids = list(ids)
+    dims = assignment_dims(problem)
+    min_per = int(d['minParticlesPerAssignment'])
+    assign_of = weighted_assign(ids, n, min_per, dims)
+    prune_at = max(20, int(round(generations * 0.45)))
+    do_prune = prune and len(ids) > 4 and prune_at < generations
     sess.set_assign(assign_of)
     ladders, temps = build_ladders(assign_of, int(d['rungs']), d['tempCold'], d['tempHot'])
     sess.set_ladders(ladders, max(2, int(d['rungs'])))
@@ -484,17 +590,33 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     acc_total = 0
     hit = None
     cpp = sess.coords_per_particle
+
+    def record(st, bestpos):
+        for i in range(n):
+            if not st['best_fit'][i] > -1e29:
+                continue
+            A = int(assign_of[i])
+            f = float(st['best_cc'][i] - st['best_pen'][i] * scale)
+            if A not in per_a or f > per_a[A]['cc'] - per_a[A]['pen'] * scale:
+                per_a[A] = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
+                            'coords': bestpos[i * cpp:(i + 1) * cpp].copy()}
+
     for restart in range(restarts):
         pos = np.array([rnd() for _ in range(n * cpp)], dtype=np.float32)
         pos = project_all(problem, pos, assign_of)
         st = initial_state(n, temps, rnd, d)
         sess.sync_state(pos, st)
         g0 = 0
+        force_eval = False
         while g0 < generations:
             if should_stop and should_stop():
                 break
-            ng = min(chunk, generations - g0)
-            reeval = g0 == 0 or groups[g0] != groups[g0 - 1]
+            end = min(g0 + chunk, generations)
+            if restart == 0 and do_prune and g0 < prune_at:
+                end = min(end, prune_at)
+            ng = end - g0
+            reeval = g0 == 0 or groups[g0] != groups[g0 - 1] or force_eval
+            force_eval = False
             sess.run(g0, ng, int(d['swapEvery']), reeval)
             sess.synchronize(600.0)
             total_ms += sess.last_kernel_ms()
@@ -504,19 +626,48 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                 ok = stc['best_fit'] > -1e29
                 if np.any(ok) and float(np.max(stc['best_cc'][ok])) >= target_cc:
                     hit = time.perf_counter() - t_start
+            if restart == 0 and do_prune and g0 == prune_at:
+                # successive halving on the bests so far, at the current penalty weight
+                _, bestpos, stp = sess.read_state()
+                record(stp, bestpos)
+                now = float(pen[prune_at - 1])
+                gbest: Dict[int, float] = {}
+                for i in range(n):
+                    if stp['best_fit'][i] > -1e29:
+                        A = int(assign_of[i])
+                        gbest[A] = max(gbest.get(A, -math.inf), float(stp['best_cc'][i] - stp['best_pen'][i] * now))
+                keep = prune_assignments(ids, gbest, 0.5, 4)
+                if len(keep) < len(ids):
+                    ids = keep
+                    fresh = weighted_assign(ids, n, min_per, dims)
+                    moved = fresh != assign_of
+                    assign_of = fresh
+                    cur_fx, best_fx = sess.read_positions_fixed()
+                    rand = np.array([rnd() for _ in range(n * cpp)], dtype=np.float32)
+                    newpos = to_fixed(project_all(problem, rand, assign_of)).reshape(n, cpp)
+                    cur_fx = cur_fx.reshape(n, cpp)
+                    best_fx = best_fx.reshape(n, cpp)
+                    cur_fx[moved] = newpos[moved]
+                    best_fx[moved] = newpos[moved]
+                    stp['fit'][moved] = -np.inf
+                    stp['cc'][moved] = np.nan
+                    stp['pen'][moved] = 0
+                    stp['step_size'][moved] = d['stepInit']
+                    stp['best_fit'][moved] = -1e30
+                    stp['best_cc'][moved] = 0
+                    stp['best_pen'][moved] = 0
+                    ladders, temps = build_ladders(assign_of, int(d['rungs']), d['tempCold'], d['tempHot'])
+                    stp['temp'] = temps
+                    sess.set_assign(assign_of)
+                    sess.set_ladders(ladders, max(2, int(d['rungs'])))
+                    sess.write_state_fixed(cur_fx.reshape(-1), best_fx.reshape(-1), stp)
+                    force_eval = True
             if on_progress:
                 on_progress({'restart': restart + 1, 'restarts': restarts, 'generation': g0 - 1,
                              'generations': generations})
         cur, bestpos, st = sess.read_state()
         acc_total += int(st['accepted'].sum())
-        for i in range(n):
-            if not st['best_fit'][i] > -1e29:
-                continue
-            A = int(assign_of[i])
-            f = float(st['best_cc'][i] - st['best_pen'][i] * scale)
-            if A not in per_a or f > per_a[A]['cc'] - per_a[A]['pen'] * scale:
-                per_a[A] = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
-                            'coords': bestpos[i * cpp:(i + 1) * cpp].copy()}
+        record(st, bestpos)
     qinfo = {}
     if do_quench and per_a and not (should_stop and should_stop()):
         before = {A: v['cc'] for A, v in per_a.items()}
@@ -538,10 +689,46 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     trials = n * generations * restarts
     res = SearchResult(best['cc'], best['pen'], best['coords'], trials, total_ms,
                        acc_total / max(1, trials), float('nan'), sess.launch_count(), seed, quench=qinfo,
-                       time_to_target=hit, wall_s=time.perf_counter() - t_start)
+                       time_to_target=hit, wall_s=time.perf_counter() - t_start, assignments=wave_ids,
+                       kept=list(ids), best_assignment=int(best['A']),
+                       per_assignment={int(A): float(v['cc']) for A, v in per_a.items()})
     if best['coords'] is not None:
         cpu = cpu_cross_check(problem, best['coords'], best['A'])
         res.cpu_check = {'gpu': best['cc'], 'cpu': cpu, 'delta': abs(best['cc'] - cpu)}
     if own:
         sess.close()
     return res
+
+
+def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
+                      restarts: int = 1, seed: int = 20261026, cos_mode: int = 0,
+                      settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
+                      **kwargs) -> SearchResult:
+    """Every assignment of the problem, in waves of assignmentsPerWave in their
+    prior order (allocateWaves, js/wyckoff_assign.js:1255-1265;
+    js/swarm_wyckoff.js:1271-1290), each wave one ``run_wyckoff_search`` with
+    its own prune; the result is the best wave's, with the per-assignment
+    bests, trials and device time of all waves."""
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    own = session is None
+    sess = session or WyckoffSession(problem, num_particles, run_key=seed, cos_mode=cos_mode, settings=settings)
+    try:
+        waves = allocate_waves(range(len(problem.assignments)), sess.num_particles,
+                               int(d['minParticlesPerAssignment']), assignment_dims(problem))
+        scale = float(schedule(generations, problem.refl.n_groups, d)[1][-1])
+        results = [run_wyckoff_search(problem, sess.num_particles, generations, restarts, seed + 7919 * k, cos_mode,
+                                      settings=settings, session=sess, assignment_ids=w, **kwargs)
+                   for k, w in enumerate(waves)]
+    finally:
+        if own:
+            sess.close()
+    best = max(results, key=lambda r: r.best_cc - r.best_pen * scale if r.best_coords is not None else -math.inf)
+    out = SearchResult(**{f: getattr(best, f) for f in best.__dataclass_fields__})
+    out.trials = sum(r.trials for r in results)
+    out.kernel_ms = sum(r.kernel_ms for r in results)
+    out.wall_s = sum(r.wall_s for r in results)
+    out.assignments = [a for r in results for a in r.assignments]
+    out.kept = [a for r in results for a in r.kept]
+    out.per_assignment = {A: cc for r in results for A, cc in r.per_assignment.items()}
+    return out

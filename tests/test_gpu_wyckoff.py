@@ -439,3 +439,39 @@ def test_incremental_site_sums_are_bit_identical_to_full_evaluation(prob, cos_mo
     b = _fused(P, 512, 400, 0, cos_mode)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     assert np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32))
+
+
+PBSO4_ALTERNATIVES = (
+    (('Pb', '4c'), ('S', '4c'), ('O', '8d'), ('O', '8d')),
+    (('Pb', '4a'), ('S', '4c'), ('O', '4c'), ('O', '4c'), ('O', '8d')),
+    (('Pb', '4b'), ('S', '4c'), ('O', '4c'), ('O', '4c'), ('O', '8d')),
+    (('Pb', '4c'), ('S', '4a'), ('O', '4c'), ('O', '4c'), ('O', '8d')),
+    (('Pb', '4c'), ('S', '4b'), ('O', '8d'), ('O', '8d')),
+)
+
+
+def test_prune_keeps_the_better_half_and_finds_the_true_assignment():
+    """Six assignments of PbSO4 in Pnma (the true one first), replicas shared
+    by free-parameter count: at generation 0.45 G the better four stay, the
+    other two's replicas move to them with fresh coordinates and ladders,
+    the retired assignments keep the bests they had, and the true assignment
+    wins, cross-checked on the CPU."""
+    from powder6_b200.swarm_wyckoff import run_wyckoff_search
+    P = wyckoff_problem(seed=1, extra_assignments=PBSO4_ALTERNATIVES)
+    res = run_wyckoff_search(P, num_particles=4096, generations=4000, seed=5)
+    assert res.assignments == list(range(6))
+    assert len(res.kept) == 4 and 0 in res.kept
+    assert set(res.per_assignment) == set(range(6))
+    assert res.best_assignment == 0 and res.best_cc > 0.9, (res.best_assignment, res.best_cc, res.per_assignment)
+    assert res.cpu_check['delta'] < 1e-5
+
+
+def test_waves_cover_every_assignment():
+    """256 replicas hold five assignments per wave: two waves, every
+    assignment searched, the best over both reported."""
+    from powder6_b200.swarm_wyckoff import run_wyckoff_waves
+    P = wyckoff_problem(seed=1, extra_assignments=PBSO4_ALTERNATIVES)
+    res = run_wyckoff_waves(P, num_particles=256, generations=300, seed=9, do_quench=False)
+    assert sorted(res.assignments) == list(range(6))
+    assert set(res.per_assignment) == set(range(6))
+    assert res.best_cc == max(res.per_assignment.values()) or res.best_pen > 0
