@@ -82,6 +82,7 @@ static_assert(sizeof(PState) == 48, "state stride");
 
 struct Params {
   const uint32_t *gen;     // reordered genPack per assignment: F atoms (site runs) first
+  const uint32_t *genOrig; // genPack in the caller's order (polyhedron moves walk it)
   const int4 *runs;        // per assignment, kMaxSites runs {start, end, type, site}
   const int *nRuns;        // per assignment
   const int *nF;           // per assignment: atoms entering |F|^2
@@ -116,6 +117,8 @@ struct Params {
   float *traceIc;          // per particle, nRefl: mult |F|^2 of the last evaluation
   unsigned long long *swapStats;  // [tried, taken]
   int *errFlag;
+  float polyProb;          // share of proposals that try a polyhedron move (0 without counted rules)
+  float invOrth[9];        // Cartesian -> fractional of the cell's own basis
   int warpSmemBytes;       // per-warp shared-memory slice
   int genOff, projOff, atomsOff, icOff;  // offsets inside the slice
   int cbOff, atoms2Off, nReflPad;          // incremental site sums and the second atom bank
@@ -755,9 +758,307 @@ __device__ __forceinline__ float penalty(const Params &P, const uint4 *atoms, co
 // lanes < maxSites turn theirs into three normal deviates for their site; the
 // move choice and the Metropolis deviate come from the block of lane 31
 // (a lane no site uses when maxSites <= 31), or from a second block.
-__device__ __forceinline__ void propose(const Params &P, WarpView &ws, const ProjFix *proj, int g, int p,
-                                        int lane, float sd, uint32_t seed, float *uMetro) {
+// ---------------------------------------------------------------------------
+// Polyhedron moves (swarm_reflection.wgsl:425-576).  A counted rule is picked
+// uniformly, then a centre (an independent site of the rule's first element)
+// uniformly, then the centre's nn nearest partners: every image of every
+// other site of the rule's second element, nearest image.  One of three moves
+// follows with probability 1/3 each: translate the centre and its partners by
+// one fractional Gaussian step, rotate the shell about the centre, or snap
+// the shell to one distance (the rule's ideal shape, aligned on the two
+// partners that fit it best, when the rule has one).  Each moved partner site
+// is the preimage, under the operator that made its image, of the image's new
+// position.  Lane 0 only, with a Philox stream of its own; the new positions
+// (before projection onto the Wyckoff subspaces) go to ws.prop in fixed point
+// and the mask of moved sites is returned (0: no move applies).
+// ---------------------------------------------------------------------------
+constexpr int kMaxPoly = 12;
+
+struct PolyRng {
+  uint2 key;
+  uint32_t g, p, blk;
+  uint4 buf;
+  int pos;
+  __device__ uint32_t word() {
+    if (pos == 4) {
+      buf = philox4x32_10(make_uint4(g, p, 0x7000u + blk, 6u), key);
+      ++blk;
+      pos = 0;
+    }
+    const uint32_t w = pos == 0 ? buf.x : pos == 1 ? buf.y : pos == 2 ? buf.z : buf.w;
+    ++pos;
+    return w;
+  }
+  __device__ float uniform() { return u01(word()); }
+  __device__ float gaussian() {
+    const uint32_t a = word(), b = word();
+    return sqrtf(-2.0f * __logf(u01_open(a))) * __cosf(6.28318530717958647f * u01(b));
+  }
+};
+
+// Ideal directions of the shapes (rule geometry codes 1-5): linear,
+// trigonal planar, tetrahedral, square planar, octahedral.
+__device__ __forceinline__ int shape_count(int code) {
+  switch (code) {
+    case 1: return 2;
+    case 2: return 3;
+    case 3: case 4: return 4;
+    case 5: return 6;
+    default: return 0;
+  }
+}
+__device__ __forceinline__ void shape_vertex(int code, int k, float v[3]) {
+  const float s3 = 0.57735026918962576f, h3 = 0.86602540378443865f;
+  float x = 0, y = 0, z = 0;
+  switch (code) {
+    case 1: x = k == 0 ? 1.f : -1.f; break;
+    case 2:
+      if (k == 0) x = 1.f;
+      else { x = -0.5f; y = k == 1 ? h3 : -h3; }
+      break;
+    case 3: {
+      const float sx[4] = {1, 1, -1, -1}, sy[4] = {1, -1, 1, -1}, sz[4] = {1, -1, -1, 1};
+      x = s3 * sx[k]; y = s3 * sy[k]; z = s3 * sz[k];
+      break;
+    }
+    case 4: {
+      const float cx[4] = {1, 0, -1, 0}, cy[4] = {0, 1, 0, -1};
+      x = cx[k]; y = cy[k];
+      break;
+    }
+    default: {
+      const float cx[6] = {1, 0, -1, 0, 0, 0}, cy[6] = {0, 1, 0, -1, 0, 0}, cz[6] = {0, 0, 0, 0, 1, -1};
+      x = cx[k]; y = cy[k]; z = cz[k];
+    }
+  }
+  v[0] = x; v[1] = y; v[2] = z;
+}
+__device__ __forceinline__ float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+// Orthonormal frame (columns F[.][c]): e1 along a, e2 in the plane of a and b, e3 = e1 x e2.
+__device__ void frame_of(const float a[3], const float b[3], float F[3][3]) {
+  float e1[3], pv[3], e2[3];
+  const float la = rsqrtf(fmaxf(dot3(a, a), 1e-30f));
+  for (int i = 0; i < 3; ++i) e1[i] = a[i] * la;
+  const float bd = dot3(b, e1);
+  for (int i = 0; i < 3; ++i) pv[i] = b[i] - bd * e1[i];
+  if (sqrtf(dot3(pv, pv)) < 1e-4f) {   // b along a: any perpendicular
+    float hv[3] = {0, 0, 0};
+    hv[fabsf(e1[0]) > 0.9f ? 1 : 0] = 1.f;
+    const float hd = dot3(hv, e1);
+    for (int i = 0; i < 3; ++i) pv[i] = hv[i] - hd * e1[i];
+  }
+  const float lp = rsqrtf(fmaxf(dot3(pv, pv), 1e-30f));
+  for (int i = 0; i < 3; ++i) e2[i] = pv[i] * lp;
+  const float e3[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+  for (int i = 0; i < 3; ++i) { F[i][0] = e1[i]; F[i][1] = e2[i]; F[i][2] = e3[i]; }
+}
+// The ideal vertex e carried from the ideal frame Fi into the actual frame Fa.
+__device__ __forceinline__ void carry(const float Fa[3][3], const float Fi[3][3], const float e[3], float w[3]) {
+  const float c0 = Fi[0][0] * e[0] + Fi[1][0] * e[1] + Fi[2][0] * e[2];
+  const float c1 = Fi[0][1] * e[0] + Fi[1][1] * e[1] + Fi[2][1] * e[2];
+  const float c2 = Fi[0][2] * e[0] + Fi[1][2] * e[1] + Fi[2][2] * e[2];
+  for (int i = 0; i < 3; ++i) w[i] = Fa[i][0] * c0 + Fa[i][1] * c1 + Fa[i][2] * c2;
+}
+__device__ __forceinline__ uint32_t frac_to_fixed(float v) {
+  const double f = (double)v - floor((double)v);
+  double x = floor(f * 4294967296.0 + 0.5);
+  if (x >= 4294967296.0) x -= 4294967296.0;
+  return (uint32_t)(unsigned long long)x;
+}
+
+__device__ __noinline__ uint32_t poly_propose(const Params &P, WarpView &ws, const OpFix *ops, float sd, PolyRng &rng) {
+  const int nRules = min(P.nRules, kMaxRules);
+  int nCounted = 0, k = 0;
+  for (int r = 0; r < nRules; ++r)
+    if (P.rules[r].mode != 0) {
+      ++nCounted;
+      if (rng.uniform() < 1.0f / (float)nCounted) k = r;
+    }
+  if (nCounted == 0) return 0u;
+  const RuleDev R = P.rules[k];
+  const int ta = R.a, tb = R.b, geom = R.geom;
+  const float rMin = fmaxf(R.dmin, 0.f), rMax = R.dmax;
+  const int nn = min((int)R.count, kMaxPoly);
+  const int ms = P.maxSites, A = ws.meta[0];
+  const uint32_t *gen = P.genOrig + (size_t)A * P.nTot;
+  // the centre
+  int nCentre = 0, sc = ms;
+  uint32_t seen = 0;
+  for (int g = 0; g < P.nTot; ++g) {
+    const uint32_t w = __ldg(gen + g);
+    const int s = w & 0xFF;
+    if (s >= ms || (int)((w >> 20) & 0xF) != ta || ((seen >> s) & 1u)) continue;
+    seen |= 1u << s;
+    ++nCentre;
+    if (rng.uniform() < 1.0f / (float)nCentre) sc = s;
+  }
+  if (sc >= ms || nn == 0) return 0u;
+  const uint4 cF = make_uint4(ws.cur[sc * 3], ws.cur[sc * 3 + 1], ws.cur[sc * 3 + 2], 0u);
+  // its nn nearest partners
+  float ld[kMaxPoly], lv[kMaxPoly][3];
+  int ls[kMaxPoly], lo[kMaxPoly];
+  for (int m = 0; m < kMaxPoly; ++m) ld[m] = kNoNeighbour;
+  for (int g = 0; g < P.nTot; ++g) {
+    const uint32_t w = __ldg(gen + g);
+    const int s = w & 0xFF;
+    if (s >= ms || s == sc || (int)((w >> 20) & 0xF) != tb) continue;
+    const int o = (w >> 8) & 0xFFF;
+    const OpFix &op = ops[o];
+    const uint32_t x = ws.cur[s * 3], y = ws.cur[s * 3 + 1], z = ws.cur[s * 3 + 2];
+    uint4 img;
+    img.x = (uint32_t)op.r[0] * x + (uint32_t)op.r[1] * y + (uint32_t)op.r[2] * z + op.t[0];
+    img.y = (uint32_t)op.r[3] * x + (uint32_t)op.r[4] * y + (uint32_t)op.r[5] * z + op.t[1];
+    img.z = (uint32_t)op.r[6] * x + (uint32_t)op.r[7] * y + (uint32_t)op.r[8] * z + op.t[2];
+    img.w = 0;
+    float q[3], dv[3];
+    frac_delta(P, img, cF, q);
+    cart_vec(P, q, dv);
+    const float d = sqrtf(dot3(dv, dv));
+    if (d < 1e-4f || d >= ld[nn - 1]) continue;
+    int m = nn - 1;
+    while (m > 0 && ld[m - 1] > d) {
+      ld[m] = ld[m - 1];
+      lv[m][0] = lv[m - 1][0]; lv[m][1] = lv[m - 1][1]; lv[m][2] = lv[m - 1][2];
+      ls[m] = ls[m - 1];
+      lo[m] = lo[m - 1];
+      --m;
+    }
+    ld[m] = d;
+    lv[m][0] = dv[0]; lv[m][1] = dv[1]; lv[m][2] = dv[2];
+    ls[m] = s;
+    lo[m] = o;
+  }
+  int nf = 0;
+  for (int m = 0; m < nn; ++m)
+    if (ld[m] < kNoNeighbour) ++nf;
+  if (nf == 0) return 0u;
+
+  const float kind = rng.uniform();
+  float shift[3] = {0, 0, 0};
+  float nv[kMaxPoly][3];
+  for (int m = 0; m < nf; ++m) { nv[m][0] = lv[m][0]; nv[m][1] = lv[m][1]; nv[m][2] = lv[m][2]; }
+  if (kind < 0.3333333f) {
+    // translate: one fractional step for the whole unit
+    for (int i = 0; i < 3; ++i) shift[i] = rng.gaussian() * sd;
+  } else if (kind < 0.6666667f) {
+    // rotate the shell about its centre (Rodrigues)
+    float ax[3] = {rng.gaussian(), rng.gaussian(), rng.gaussian()};
+    const float la = sqrtf(dot3(ax, ax));
+    if (la < 1e-6f) { ax[0] = 0; ax[1] = 0; ax[2] = 1; }
+    else for (int i = 0; i < 3; ++i) ax[i] /= la;
+    const float ang = rng.gaussian() * fminf(fmaxf(sd * 20.0f, 0.05f), 0.8f);
+    const float c = cosf(ang), sn = sinf(ang);
+    for (int m = 0; m < nf; ++m) {
+      const float *v = lv[m];
+      const float kv = dot3(ax, v);
+      const float cr[3] = {ax[1] * v[2] - ax[2] * v[1], ax[2] * v[0] - ax[0] * v[2], ax[0] * v[1] - ax[1] * v[0]};
+      for (int i = 0; i < 3; ++i) nv[m][i] = v[i] * c + cr[i] * sn + ax[i] * kv * (1.0f - c);
+    }
+  } else {
+    // snap: one distance for the shell, and the ideal shape when the rule has one
+    float mean = 0;
+    for (int m = 0; m < nf; ++m) mean += ld[m];
+    mean = mean / (float)nf * (1.0f + 0.03f * rng.gaussian());
+    const float dT = fminf(fmaxf(mean, fmaxf(rMin, 0.3f)), rMax < 1.0e6f ? rMax : mean);
+    const int nShape = shape_count(geom);
+    if (nShape >= 2 && nf >= 2) {
+      float u0[3] = {lv[0][0] / ld[0], lv[0][1] / ld[0], lv[0][2] / ld[0]};
+      float v0[3], v1[3];
+      shape_vertex(geom, 0, v0);
+      shape_vertex(geom, 1, v1);
+      const float cIdeal = dot3(v0, v1);
+      int j1 = 1;
+      float bestErr = 1.0e9f;
+      for (int m = 1; m < nf; ++m) {
+        const float um[3] = {lv[m][0] / ld[m], lv[m][1] / ld[m], lv[m][2] / ld[m]};
+        const float e = fabsf(dot3(u0, um) - cIdeal);
+        if (e < bestErr) { bestErr = e; j1 = m; }
+      }
+      float Fa[3][3], Fi[3][3];
+      frame_of(u0, lv[j1], Fa);
+      frame_of(v0, v1, Fi);
+      uint32_t usedV = 3u;
+      for (int m = 0; m < nf; ++m) {
+        int vk;
+        if (m == 0) vk = 0;
+        else if (m == j1) vk = 1;
+        else {
+          float bestDot = -2.0f;
+          vk = nShape;
+          const float um[3] = {lv[m][0] / ld[m], lv[m][1] / ld[m], lv[m][2] / ld[m]};
+          for (int qv = 2; qv < nShape; ++qv) {
+            if ((usedV >> qv) & 1u) continue;
+            float e[3], wv[3];
+            shape_vertex(geom, qv, e);
+            carry(Fa, Fi, e, wv);
+            const float dd = dot3(wv, um);
+            if (dd > bestDot) { bestDot = dd; vk = qv; }
+          }
+          if (vk < nShape) usedV |= 1u << vk;
+        }
+        if (vk < nShape) {
+          float e[3], wv[3];
+          shape_vertex(geom, vk, e);
+          carry(Fa, Fi, e, wv);
+          for (int i = 0; i < 3; ++i) nv[m][i] = wv[i] * dT;
+        } else {
+          for (int i = 0; i < 3; ++i) nv[m][i] = lv[m][i] / ld[m] * dT;
+        }
+      }
+    } else {
+      for (int m = 0; m < nf; ++m)
+        for (int i = 0; i < 3; ++i) nv[m][i] = lv[m][i] / ld[m] * dT;
+    }
+  }
+
+  // back to the independent sites: the nearest image of each site carries it
+  const float cf[3] = {(float)((double)cF.x * (1.0 / 4294967296.0)), (float)((double)cF.y * (1.0 / 4294967296.0)),
+                       (float)((double)cF.z * (1.0 / 4294967296.0))};
+  uint32_t mask = 0;
+  if (kind < 0.3333333f) {
+    for (int i = 0; i < 3; ++i) ws.prop[sc * 3 + i] = frac_to_fixed(cf[i] + shift[i]);
+    mask = 1u << sc;
+  }
+  for (int m = 0; m < nf; ++m) {
+    const int s = ls[m];
+    if ((mask >> s) & 1u) continue;
+    float dest[3];
+    for (int i = 0; i < 3; ++i)
+      dest[i] = cf[i] + (P.invOrth[3 * i] * nv[m][0] + P.invOrth[3 * i + 1] * nv[m][1] + P.invOrth[3 * i + 2] * nv[m][2]) +
+                shift[i];
+    // R^-1 (dest - t) by the adjugate
+    const OpFix &op = ops[lo[m]];
+    const float m0 = op.r[0], m1 = op.r[1], m2 = op.r[2], m3 = op.r[3], m4 = op.r[4], m5 = op.r[5], m6 = op.r[6],
+                m7 = op.r[7], m8 = op.r[8];
+    const float c00 = m4 * m8 - m5 * m7, c01 = m5 * m6 - m3 * m8, c02 = m3 * m7 - m4 * m6;
+    const float det = m0 * c00 + m1 * c01 + m2 * c02;
+    const float dn = fabsf(det) < 1e-6f ? 1.0f : det;
+    float wv[3];
+    for (int i = 0; i < 3; ++i) wv[i] = (dest[i] - (float)((double)op.t[i] * (1.0 / 4294967296.0))) / dn;
+    const float out[3] = {c00 * wv[0] + (m2 * m7 - m1 * m8) * wv[1] + (m1 * m5 - m2 * m4) * wv[2],
+                          c01 * wv[0] + (m0 * m8 - m2 * m6) * wv[1] + (m2 * m3 - m0 * m5) * wv[2],
+                          c02 * wv[0] + (m1 * m6 - m0 * m7) * wv[1] + (m0 * m4 - m1 * m3) * wv[2]};
+    for (int i = 0; i < 3; ++i) ws.prop[s * 3 + i] = frac_to_fixed(out[i]);
+    mask |= 1u << s;
+  }
+  return mask;
+}
+
+// SLOTS > 0: the distance-rule variants, the only ones whose problems can
+// have counted rules and so polyhedron moves.
+template <int SLOTS>
+__device__ __forceinline__ void propose(const Params &P, WarpView &ws, const ProjFix *proj, const OpFix *ops, int g,
+                                        int p, int lane, float sd, uint32_t seed, float *uMetro) {
   const uint2 key = make_uint2(seed, P.runKey);
+  uint32_t polyMask = 0;
+  if (SLOTS > 0 && P.polyProb > 0.f) {
+    if (lane == 0) {
+      PolyRng rng{key, (uint32_t)g, (uint32_t)p, 0u, make_uint4(0, 0, 0, 0), 4};
+      if (rng.uniform() < P.polyProb) polyMask = poly_propose(P, ws, ops, sd, rng);
+    }
+    polyMask = __shfl_sync(0xffffffffu, polyMask, 0);
+    __syncwarp();
+  }
   const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, (uint32_t)lane, 2u), key);
   uint4 cc = make_uint4(__shfl_sync(0xffffffffu, c.x, 31), __shfl_sync(0xffffffffu, c.y, 31),
                         __shfl_sync(0xffffffffu, c.z, 31), __shfl_sync(0xffffffffu, c.w, 31));
@@ -765,14 +1066,14 @@ __device__ __forceinline__ void propose(const Params &P, WarpView &ws, const Pro
   const uint32_t free = (uint32_t)ws.meta[4];
   const int nFree = __popc(free);
   int pick = -1;
-  if (u01(cc.x) < 0.75f && nFree > 0) {
+  if (!polyMask && u01(cc.x) < 0.75f && nFree > 0) {
     const int kth = min(nFree - 1, (int)(u01(cc.y) * (float)nFree));
     pick = __fns(free, 0, kth + 1);
   }
   *uMetro = u01(cc.z);
   if (lane < P.maxSites) {
     const int s = lane;
-    const bool moving = (pick < 0) || (pick == s);
+    const bool moving = polyMask ? ((polyMask >> s) & 1u) != 0 : (pick < 0) || (pick == s);
     if (moving) {
       const float2 n01 = gauss2(c.x, c.y);
       const float2 n23 = gauss2(c.z, c.w);
@@ -780,7 +1081,8 @@ __device__ __forceinline__ void propose(const Params &P, WarpView &ws, const Pro
       const float scale = sd * 4294967296.0f;
       int64_t pos[3];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) pos[i] = (int64_t)ws.cur[s * 3 + i] + __float2ll_rn(gz[i] * scale);
+      for (int i = 0; i < 3; ++i)
+        pos[i] = polyMask ? (int64_t)ws.prop[s * 3 + i] : (int64_t)ws.cur[s * 3 + i] + __float2ll_rn(gz[i] * scale);
       const ProjFix &pr = proj[s];
       if (pr.pad[0]) {  // diagonal 0/1 projector: keep or drop each coordinate
 #pragma unroll
@@ -967,7 +1269,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             uMetro = u01(u.x);
             __syncwarp();
           } else {
-            propose(P, ws, proj, g, p, lane, sd, seed, &uMetro);
+            propose<SLOTS>(P, ws, proj, ops, g, p, lane, sd, seed, &uMetro);
           }
           double sums[3];
           uint32_t moved = 0;
@@ -1510,8 +1812,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   if (pr->n_rules > kMaxRules) return set_error(P6_ERR_CAPACITY, "more than 32 distance rules");
   if (pr->max_coord_slots > 256) return set_error(P6_ERR_CAPACITY, "more than 256 neighbour slots");
   if (pr->group_stride != 3 && pr->group_stride != 4) return set_error(P6_ERR_INVALID_ARG, "group stride must be 3 or 4");
-  if (pr->poly_prob > 0.f)
-    return set_error(P6_ERR_INVALID_ARG, "polyhedron moves are not available in this build (poly_prob must be 0)");
+  if (!(pr->poly_prob >= 0.f && pr->poly_prob <= 1.f)) return set_error(P6_ERR_INVALID_ARG, "poly_prob must lie in [0, 1]");
   if (pr->n_tot > 4096) return set_error(P6_ERR_CAPACITY, "more than 4096 generated atoms");
   if (pr->cos_mode != 0 && pr->cos_mode != 1) return set_error(P6_ERR_INVALID_ARG, "cos_mode must be 0 or 1");
   if (pr->incremental < -1 || pr->incremental > 1)
@@ -1819,6 +2120,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
 
   Params &P = s->P;
   P.gen = s->dGen;
+  P.genOrig = s->dGenOrig;
   P.runs = s->dRuns;
   P.nRuns = s->dNRuns;
   P.nF = s->dNF;
@@ -1845,7 +2147,11 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.nGroups = pr->n_groups;
   P.nElem = nE;
   P.nAssign = nA;
+  bool counted = false;
+  for (int k = 0; k < pr->n_rules; ++k) counted |= (int)pr->restraint_tables[pr->rule_off + 7 * k + 5] != 0;
+  P.polyProb = counted ? pr->poly_prob : 0.f;   // no counted rule: nothing to move as a unit
   for (int i = 0; i < 9; ++i) {
+    P.invOrth[i] = (float)pr->inv_orth[i];
     P.orth[i] = (float)pr->orth[i];
     const double x = pr->xform[i];
     if (std::fabs(x - std::floor(x + 0.5)) > 1e-9) {

@@ -116,7 +116,7 @@ class WyckoffSession:
         pr.pen_bond = problem.pen_bond
         pr.pen_coord = problem.pen_coord
         pr.pen_geom = problem.pen_geom
-        pr.poly_prob = 0.0
+        pr.poly_prob = float(min(1.0, max(0.0, (settings or {}).get('polyProb', SW_DEFAULTS['polyProb']))))
         pr.step_up, pr.step_down = ad['STEP_UP'], ad['STEP_DOWN']
         pr.step_min, pr.step_max = ad['STEP_MIN'], ad['STEP_MAX']
         pr.cos_mode = int(cos_mode)

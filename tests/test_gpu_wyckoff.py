@@ -475,3 +475,211 @@ def test_waves_cover_every_assignment():
     assert sorted(res.assignments) == list(range(6))
     assert set(res.per_assignment) == set(range(6))
     assert res.best_cc == max(res.per_assignment.values()) or res.best_pen > 0
+
+
+# ---------------------------------------------------------------------------
+# Polyhedron moves (swarm_reflection.wgsl:425-576) against an FP64 restatement
+# ---------------------------------------------------------------------------
+def _philox_stream(oracle, seed, run_key, g, p):
+    """The lane-0 Philox stream of the polyhedron move: counter (g, p, 0x7000 + block, 6)."""
+    import ctypes as C
+    lib = oracle.load()
+    blk = 0
+    while True:
+        ctr = np.array([g, p, 0x7000 + blk, 6], dtype=np.uint32)
+        key = np.array([seed, run_key], dtype=np.uint32)
+        out = np.zeros(4, dtype=np.uint32)
+        lib.p6o_philox(ctr.ctypes.data_as(C.c_void_p), key.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+        for w in out:
+            yield int(w)
+        blk += 1
+
+
+class _Stream:
+    def __init__(self, gen):
+        self.gen = gen
+
+    def uniform(self):
+        return np.float32((next(self.gen) >> 8) * (1.0 / 16777216.0))
+
+    def gaussian(self):
+        a, b = next(self.gen), next(self.gen)
+        u_open = ((a >> 8) + 1) / 16777216.0
+        return math.sqrt(-2.0 * math.log(u_open)) * math.cos(2 * math.pi * ((b >> 8) / 16777216.0))
+
+
+_SHAPES = {1: [(1, 0, 0), (-1, 0, 0)],
+           2: [(1, 0, 0), (-0.5, math.sqrt(3) / 2, 0), (-0.5, -math.sqrt(3) / 2, 0)],
+           3: [tuple(v / math.sqrt(3) for v in t) for t in ((1, 1, 1), (1, -1, -1), (-1, 1, -1), (-1, -1, 1))],
+           4: [(1, 0, 0), (0, 1, 0), (-1, 0, 0), (0, -1, 0)],
+           5: [(1, 0, 0), (0, 1, 0), (-1, 0, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]}
+
+
+def _frame(a, b):
+    e1 = a / np.linalg.norm(a)
+    pv = b - np.dot(b, e1) * e1
+    if np.linalg.norm(pv) < 1e-4:
+        h = np.array([0.0, 1.0, 0.0]) if abs(e1[0]) > 0.9 else np.array([1.0, 0.0, 0.0])
+        pv = h - np.dot(h, e1) * e1
+    e2 = pv / np.linalg.norm(pv)
+    return np.stack([e1, e2, np.cross(e1, e2)], axis=1)       # columns
+
+
+def _poly_restated(P, sites_fx, rng, sd):
+    """polyPropose in FP64: returns ({site: new fraction (3,)}, kind); empty when no move applies."""
+    T = P.tables
+    ms, nT = T.max_sites, T.n_tot
+    gp = [int(w) for w in T.gen_pack[:nT]]
+    sym = P.sym_packed.astype(np.float64).reshape(-1, 12)
+    tb = P.restraints.tables
+    rules = [tb[P.restraints.rule_off + 7 * k:P.restraints.rule_off + 7 * k + 7] for k in range(P.restraints.n_rules)]
+    n_counted, k = 0, 0
+    for r, rb in enumerate(rules):
+        if int(rb[5]) != 0:
+            n_counted += 1
+            if rng.uniform() < np.float32(1.0) / np.float32(n_counted):
+                k = r
+    if n_counted == 0:
+        return {}, None
+    rb = rules[k]
+    ta, tbt, rmin, rmax, nn, geom = int(rb[0]), int(rb[1]), max(float(rb[2]), 0.0), float(rb[3]), min(int(rb[4]), 12), int(rb[6])
+    n_c, sc, seen = 0, ms, set()
+    for w in gp:
+        s = w & 0xFF
+        if s >= ms or ((w >> 20) & 0xF) != ta or s in seen:
+            continue
+        seen.add(s)
+        n_c += 1
+        if rng.uniform() < np.float32(1.0) / np.float32(n_c):
+            sc = s
+    if sc >= ms or nn == 0:
+        return {}, None
+    X = sites_fx.reshape(ms, 3).astype(np.int64)
+    xf = np.asarray(P.xform, dtype=np.float64).reshape(3, 3).round().astype(np.int64)
+    orth = np.asarray(P.orth, dtype=np.float64).reshape(3, 3)
+    inv = np.asarray(P.inv_orth, dtype=np.float64).reshape(3, 3)
+    cands = []
+    for w in gp:
+        s = w & 0xFF
+        if s >= ms or s == sc or ((w >> 20) & 0xF) != tbt:
+            continue
+        o = (w >> 8) & 0xFFF
+        R = sym[o, :9].round().astype(np.int64).reshape(3, 3)
+        t = np.array([trans_fixed(float(v)) for v in sym[o, 9:]], dtype=np.int64)
+        img = (R @ X[s] + t) % 2 ** 32
+        d = (img - X[sc]) % 2 ** 32
+        d = np.where(d >= 2 ** 31, d - 2 ** 32, d)
+        q = (xf @ d) % 2 ** 32
+        q = np.where(q >= 2 ** 31, q - 2 ** 32, q) / 2.0 ** 32
+        dv = orth @ q
+        dist = float(np.linalg.norm(dv))
+        if dist < 1e-4:
+            continue
+        cands.append((dist, len(cands), dv, s, o))
+    cands.sort(key=lambda c: (c[0], c[1]))            # stable: the first found wins a tie
+    shell = cands[:nn]
+    if not shell:
+        return {}, None
+    kind = rng.uniform()
+    shift = np.zeros(3)
+    lv = [c[2] for c in shell]
+    ld = [c[0] for c in shell]
+    nv = [v.copy() for v in lv]
+    if kind < np.float32(0.3333333):
+        shift = np.array([rng.gaussian(), rng.gaussian(), rng.gaussian()]) * sd
+    elif kind < np.float32(0.6666667):
+        ax = np.array([rng.gaussian(), rng.gaussian(), rng.gaussian()])
+        ax = ax / np.linalg.norm(ax) if np.linalg.norm(ax) >= 1e-6 else np.array([0.0, 0.0, 1.0])
+        ang = rng.gaussian() * min(max(sd * 20.0, 0.05), 0.8)
+        c, sn = math.cos(ang), math.sin(ang)
+        nv = [v * c + np.cross(ax, v) * sn + ax * np.dot(ax, v) * (1 - c) for v in lv]
+    else:
+        mean = sum(ld) / len(ld) * (1 + 0.03 * rng.gaussian())
+        dT = min(max(mean, max(rmin, 0.3)), rmax if rmax < 1e6 else mean)
+        shape = [np.array(v) for v in _SHAPES.get(geom, [])]
+        if len(shape) >= 2 and len(shell) >= 2:
+            u0 = lv[0] / ld[0]
+            c_ideal = float(np.dot(shape[0], shape[1]))
+            errs = [abs(float(np.dot(u0, lv[m] / ld[m])) - c_ideal) for m in range(1, len(shell))]
+            j1 = 1 + int(np.argmin(errs))
+            Fa, Fi = _frame(u0, lv[j1]), _frame(shape[0], shape[1])
+            used = {0, 1}
+            for m in range(len(shell)):
+                if m == 0:
+                    vk = 0
+                elif m == j1:
+                    vk = 1
+                else:
+                    best, vk = -2.0, len(shape)
+                    for qv in range(2, len(shape)):
+                        if qv in used:
+                            continue
+                        dd = float(np.dot(Fa @ (Fi.T @ shape[qv]), lv[m] / ld[m]))
+                        if dd > best:
+                            best, vk = dd, qv
+                    if vk < len(shape):
+                        used.add(vk)
+                nv[m] = (Fa @ (Fi.T @ shape[vk])) * dT if vk < len(shape) else lv[m] / ld[m] * dT
+        else:
+            nv = [v / d * dT for v, d in zip(lv, ld)]
+    cf = X[sc] / 2.0 ** 32
+    out = {}
+    if kind < np.float32(0.3333333):
+        out[sc] = cf + shift
+    for (dist, _, _, s, o), v in zip(shell, nv):
+        if s in out:
+            continue
+        dest = cf + inv @ v + shift
+        R = sym[o, :9].reshape(3, 3)
+        t = np.array([trans_fixed(float(x)) for x in sym[o, 9:]], dtype=np.float64) / 2.0 ** 32
+        out[s] = np.linalg.solve(R, dest - t)
+    label = 'translate' if kind < np.float32(0.3333333) else 'rotate' if kind < np.float32(0.6666667) else 'snap'
+    return out, label
+
+
+def test_polyhedron_moves_match_the_restatement(oracle):
+    """polyProb = 1 on a P2_1/c problem (S and four O on general positions, a
+    counted S-O rule with a tetrahedron): every replica's proposal, as traced,
+    equals the FP64 restatement of the move with the same random stream --
+    the moved sites within 2e-5 (fractional, mod 1), the others bit for bit --
+    and all three kinds of move occur."""
+    cell = {'a': 7.2, 'b': 8.9, 'c': 10.4, 'alpha': 90.0, 'beta': 103.0, 'gamma': 90.0}
+    P = wyckoff_problem(seed=4, group_number=14, cell=cell, composition=(('S', 4), ('O', 16)),
+                        sites=(('S', '4e'), ('O', '4e'), ('O', '4e'), ('O', '4e'), ('O', '4e')), dmin=1.4,
+                        windows=[{'a': 'S', 'b': 'O', 'count': 4, 'dmin': 1.35, 'dmax': 1.65,
+                                  'geometry': 'tetrahedron'}], true_min_contact=1.2, contact_attempts=200)
+    n, run_key = 192, 4242
+    X, _ = random_positions(P, n, 77)
+    rnd = mulberry32(5)
+    st0 = initial_state(n, np.full(n, 0.01, dtype=np.float32), rnd)
+    ms3 = P.max_sites * 3
+    with WyckoffSession(P, n, run_key=run_key, settings={'polyProb': 1.0}) as s:
+        s.sync_state(np.zeros(n * ms3, dtype=np.float32), st0)
+        s.write_positions_fixed(X)
+        s.set_trace(True)
+        s.set_params(P.refl.n_groups, 1.0)
+        s.dispatch(None, mcmc=True)
+        s.synchronize(60)
+        props, rec = s.read_trace()
+    kinds = set()
+    worst = 0.0
+    for p in range(n):
+        x0 = X[p * ms3:(p + 1) * ms3]
+        got = props[p * ms3:(p + 1) * ms3].reshape(-1, 3)
+        gen = _philox_stream(oracle, int(st0['seed'][p]), run_key, 0, p)
+        rng = _Stream(gen)
+        assert rng.uniform() < 1.0
+        sd = float(st0['step_size'][p])
+        want, kind = _poly_restated(P, x0, rng, sd)
+        assert want, p                                    # a counted rule and partners always exist here
+        for si in range(P.max_sites):
+            if si in want:
+                d = got[si] / 2.0 ** 32 - want[si]
+                d -= np.round(d)
+                worst = max(worst, float(np.max(np.abs(d))))
+            else:
+                assert np.array_equal(got[si], x0.reshape(-1, 3)[si]), (p, si)
+        kinds.add(kind)
+    print(f'polyhedron moves: worst fractional difference {worst:.2e}, kinds {sorted(kinds)}')
+    assert worst < 2e-5
+    assert kinds == {'translate', 'rotate', 'snap'}
