@@ -483,6 +483,8 @@ class SearchResult:
     kept: List[int] = field(default_factory=list)            # still in contention after the prune
     best_assignment: int = 0
     per_assignment: Dict[int, float] = field(default_factory=dict)   # best cc of each assignment
+    bests: Dict[int, dict] = field(default_factory=dict)             # {cc, pen, coords} of each assignment
+    screened: Dict[int, float] = field(default_factory=dict)         # screening score (cc - raw pen), if screened
 
 
 def quench_schedule(settings: Optional[dict] = None) -> np.ndarray:
@@ -691,7 +693,9 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                        acc_total / max(1, trials), float('nan'), sess.launch_count(), seed, quench=qinfo,
                        time_to_target=hit, wall_s=time.perf_counter() - t_start, assignments=wave_ids,
                        kept=list(ids), best_assignment=int(best['A']),
-                       per_assignment={int(A): float(v['cc']) for A, v in per_a.items()})
+                       per_assignment={int(A): float(v['cc']) for A, v in per_a.items()},
+                       bests={int(A): {'cc': float(v['cc']), 'pen': float(v['pen']), 'coords': v['coords']}
+                              for A, v in per_a.items()})
     if best['coords'] is not None:
         cpu = cpu_cross_check(problem, best['coords'], best['A'])
         res.cpu_check = {'gpu': best['cc'], 'cpu': cpu, 'delta': abs(best['cc'] - cpu)}
@@ -700,24 +704,81 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     return res
 
 
+# The screening stage (WY_LIMITS, js/wyckoff_limits.js:48-53): when the
+# assignments need more than FULL_WAVES waves, each is first searched for
+# SCREEN_FRACTION of the generations (at least SCREEN_MIN_GENERATIONS, one
+# restart), and only the best FULL_WAVES waves' worth get the full search.
+FULL_WAVES = 2
+SCREEN_FRACTION = 0.1
+SCREEN_MIN_GENERATIONS = 60
+
+
+def rescore_full_resolution(problem: WyckoffProblem, sess: WyckoffSession, bests: Dict[int, dict],
+                            seed: int = 1, settings: Optional[dict] = None) -> Dict[int, dict]:
+    """rescoreAtFullResolution: each assignment's best structure measured with
+    every reflection group and the penalty at weight 1 (one replica per
+    assignment, one evaluation launch); returns {A: {cc, pen, coords}}."""
+    live = sorted(A for A, b in bests.items() if b.get('coords') is not None)
+    if not live:
+        return {}
+    n = sess.num_particles
+    if len(live) > n:
+        raise ValueError('more assignments than replicas to re-score them')
+    assign_of = np.array([live[i] if i < len(live) else live[0] for i in range(n)], dtype=np.uint32)
+    sess.set_assign(assign_of)
+    pos = np.concatenate([bests[int(A)]['coords'] for A in assign_of]).astype(np.float32)
+    st = initial_state(n, np.full(n, SW_DEFAULTS['tempCold'], dtype=np.float32), mulberry32(seed), settings)
+    sess.sync_state(pos, st)
+    sess.set_params(problem.refl.n_groups, 1.0)
+    sess.dispatch(None, mcmc=False)
+    sess.synchronize(60.0)
+    _, _, st = sess.read_state()
+    return {A: {'cc': float(st['cc'][i]), 'pen': float(st['pen'][i]), 'coords': bests[A]['coords']}
+            for i, A in enumerate(live) if np.isfinite(st['cc'][i])}
+
+
 def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
                       restarts: int = 1, seed: int = 20261026, cos_mode: int = 0,
                       settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
                       **kwargs) -> SearchResult:
     """Every assignment of the problem, in waves of assignmentsPerWave in their
     prior order (allocateWaves, js/wyckoff_assign.js:1255-1265;
-    js/swarm_wyckoff.js:1271-1290), each wave one ``run_wyckoff_search`` with
-    its own prune; the result is the best wave's, with the per-assignment
-    bests, trials and device time of all waves."""
+    js/swarm_wyckoff.js:1262-1290, :2393-2425), each wave one
+    ``run_wyckoff_search`` with its own prune.  When they need more than
+    FULL_WAVES waves, a screening stage runs first: every assignment for a
+    tenth of the generations (at least 60, one restart, no quench), its best
+    re-scored at full resolution and penalty weight 1, and only the best
+    FULL_WAVES waves' worth, in the order of their scores, get the full
+    search.  The result is the best full-search wave's, with the
+    per-assignment bests, trials and device time of all waves."""
     d = dict(SW_DEFAULTS)
     d.update(settings or {})
     own = session is None
     sess = session or WyckoffSession(problem, num_particles, run_key=seed, cos_mode=cos_mode, settings=settings)
+    n, min_per, dims = sess.num_particles, int(d['minParticlesPerAssignment']), assignment_dims(problem)
+    all_ids = list(range(len(problem.assignments)))
+    screen_results, screened = [], {}
     try:
-        waves = allocate_waves(range(len(problem.assignments)), sess.num_particles,
-                               int(d['minParticlesPerAssignment']), assignment_dims(problem))
+        kept = all_ids
+        if math.ceil(len(all_ids) / assignments_per_wave(n, min_per, True)) > FULL_WAVES:
+            g_screen = min(generations, max(SCREEN_MIN_GENERATIONS, int(round(generations * SCREEN_FRACTION))))
+            skw = dict(kwargs)
+            skw['do_quench'] = False
+            skw.pop('target_cc', None)
+            bests: Dict[int, dict] = {}
+            for k, w in enumerate(allocate_waves(all_ids, n, min_per, dims)):
+                r = run_wyckoff_search(problem, n, g_screen, 1, seed + 104729 * k, cos_mode, settings=settings,
+                                       session=sess, assignment_ids=w, **skw)
+                screen_results.append(r)
+                bests.update(r.bests)
+            scored = rescore_full_resolution(problem, sess, bests, seed, settings)
+            screened = {A: v['cc'] - v['pen'] for A, v in scored.items()}
+            kept = sorted(screened, key=lambda A: -screened[A])[:assignments_per_wave(n, min_per, True) * FULL_WAVES]
+            if not kept:
+                raise RuntimeError('The screening produced no finite score for any assignment.')
+        waves = allocate_waves(kept, n, min_per, dims)
         scale = float(schedule(generations, problem.refl.n_groups, d)[1][-1])
-        results = [run_wyckoff_search(problem, sess.num_particles, generations, restarts, seed + 7919 * k, cos_mode,
+        results = [run_wyckoff_search(problem, n, generations, restarts, seed + 7919 * k, cos_mode,
                                       settings=settings, session=sess, assignment_ids=w, **kwargs)
                    for k, w in enumerate(waves)]
     finally:
@@ -725,10 +786,12 @@ def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, genera
             sess.close()
     best = max(results, key=lambda r: r.best_cc - r.best_pen * scale if r.best_coords is not None else -math.inf)
     out = SearchResult(**{f: getattr(best, f) for f in best.__dataclass_fields__})
-    out.trials = sum(r.trials for r in results)
-    out.kernel_ms = sum(r.kernel_ms for r in results)
-    out.wall_s = sum(r.wall_s for r in results)
+    out.trials = sum(r.trials for r in screen_results + results)
+    out.kernel_ms = sum(r.kernel_ms for r in screen_results + results)
+    out.wall_s = sum(r.wall_s for r in screen_results + results)
     out.assignments = [a for r in results for a in r.assignments]
     out.kept = [a for r in results for a in r.kept]
     out.per_assignment = {A: cc for r in results for A, cc in r.per_assignment.items()}
+    out.bests = {A: b for r in results for A, b in r.bests.items()}
+    out.screened = screened
     return out

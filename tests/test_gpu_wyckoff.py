@@ -683,3 +683,29 @@ def test_polyhedron_moves_match_the_restatement(oracle):
     print(f'polyhedron moves: worst fractional difference {worst:.2e}, kinds {sorted(kinds)}')
     assert worst < 2e-5
     assert kinds == {'translate', 'rotate', 'snap'}
+
+
+PBSO4_MANY = PBSO4_ALTERNATIVES + (
+    (('Pb', '4c'), ('S', '4c'), ('O', '4c'), ('O', '4c'), ('O', '4c'), ('O', '4c')),
+    (('Pb', '4a'), ('S', '4b'), ('O', '8d'), ('O', '8d')),
+    (('Pb', '4b'), ('S', '4a'), ('O', '8d'), ('O', '8d')),
+    (('Pb', '4c'), ('S', '4c'), ('O', '4a'), ('O', '4c'), ('O', '8d')),
+    (('Pb', '4c'), ('S', '4c'), ('O', '4b'), ('O', '4c'), ('O', '8d')),
+    (('Pb', '4a'), ('S', '4c'), ('O', '8d'), ('O', '8d')),
+)
+
+
+def test_screening_stage_keeps_the_best_two_waves():
+    """Twelve assignments, 256 replicas (five per wave): three waves exceed the
+    two full-search waves, so every assignment is screened for a tenth of the
+    generations, re-scored at full resolution, and only the best ten (two
+    waves) are searched in full, in the order of their scores; the true
+    assignment is among them and wins."""
+    from powder6_b200.swarm_wyckoff import run_wyckoff_waves
+    P = wyckoff_problem(seed=1, extra_assignments=PBSO4_MANY)
+    res = run_wyckoff_waves(P, num_particles=256, generations=2000, seed=3)
+    assert set(res.screened) == set(range(12))
+    order = sorted(res.screened, key=lambda A: -res.screened[A])
+    assert res.assignments == order[:10]
+    assert 0 in res.assignments
+    assert res.best_assignment == 0, (res.best_assignment, res.per_assignment)
