@@ -118,6 +118,7 @@ struct Params {
   unsigned long long *swapStats;  // [tried, taken]
   int *errFlag;
   float polyProb;          // share of proposals that try a polyhedron move (0 without counted rules)
+  int blobGlobal;          // the static tables are read from global memory (too large to stage)
   float invOrth[9];        // Cartesian -> fractional of the cell's own basis
   int warpSmemBytes;       // per-warp shared-memory slice
   int genOff, projOff, atomsOff, icOff;  // offsets inside the slice
@@ -1123,19 +1124,22 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nWarps = blockDim.x >> 5;
 
-  // Stage the static tables once per CTA with the bulk-copy engine.
-  unsigned char *stat = smem;
-  const int blobPad = (P.blobBytes + 127) & ~127;
-  if (threadIdx.x == 0) {
+  // Stage the static tables once per CTA with the bulk-copy engine, unless
+  // they are too large to share the CTA's shared memory with the replica
+  // slices: then every table read goes to global memory (through L1).
+  const bool stage = !P.blobGlobal;
+  const unsigned char *stat = stage ? smem : P.blob;
+  const int blobPad = stage ? (P.blobBytes + 127) & ~127 : 0;
+  if (stage && threadIdx.x == 0) {
     mbar_init(&stageBar, 1);
     fence_mbar_init();
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (stage && threadIdx.x == 0) {
     mbar_arrive_expect_tx(&stageBar, (uint32_t)P.blobBytes);
     for (int off = 0; off < P.blobBytes; off += 65536) {
       const int n = min(65536, P.blobBytes - off);
-      bulk_g2s(stat + off, P.blob + off, (uint32_t)n, &stageBar);
+      bulk_g2s(smem + off, P.blob + off, (uint32_t)n, &stageBar);
     }
   }
   if (threadIdx.x < 27) {
@@ -1143,7 +1147,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
                         (float)((int)threadIdx.x % 3 - 1)};
     shellLen[threadIdx.x] = cart_len(P, t);
   }
-  const bool staged = __syncthreads_and(mbar_wait_bounded(&stageBar, 0, kStageWaitLimit) ? 1 : 0) != 0;
+  const bool staged = !stage || __syncthreads_and(mbar_wait_bounded(&stageBar, 0, kStageWaitLimit) ? 1 : 0) != 0;
+  if (!stage) __syncthreads();
   if (!staged) {
     if (threadIdx.x == 0) raise_flag(P.errFlag, DEV_STAGE_TIMEOUT);
     mbar_wait_bounded(&stageBar, 0, kStageWaitLimit);   // copies still in flight land before the CTA moves on
@@ -1429,7 +1434,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
     __syncthreads();
   }
   // the staging barrier is set up afresh by the next call on this CTA
-  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&stageBar)) : "memory");
+  if (stage && threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&stageBar)) : "memory");
   __syncthreads();
   return true;
 }
@@ -2058,7 +2063,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   if (useIncr && !incrFits4 && smemIncr > (size_t)200 * 1024)
     return set_error(P6_ERR_CAPACITY, "incremental site sums do not fit in shared memory");
   const size_t warpBytes = ((useIncr ? incrEnd : baseEnd) + 127) & ~(size_t)127;
-  const size_t smem = useIncr ? smemIncr : smemFull;
+  size_t smem = useIncr ? smemIncr : smemFull;
 
   p6_wy_session *s = new p6_wy_session();
   s->device = device;
@@ -2071,7 +2076,13 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   int smemOptin = 0, nSM = 0;
   cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, device);
-  // Shared memory: the staged tables once, plus one slice per rung (8 warps).
+  // Shared memory: the staged tables once, plus one slice per rung (8 warps);
+  // when both do not fit, the tables stay in global memory.
+  int blobGlobal = 0;
+  if (!useIncr && (int)smem > smemOptin - 1024 && (int)(warpBytes * rungs) <= smemOptin - 1024) {
+    blobGlobal = 1;
+    smem = warpBytes * rungs;
+  }
   if ((int)smem > smemOptin - 1024) {
     free_session(s);
     return set_error(P6_ERR_CAPACITY, "the reflection table and generated cell do not fit in shared memory");
@@ -2187,6 +2198,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.swapStats = s->dSwap;
   P.errFlag = s->dErr;
   P.warpSmemBytes = (int)warpBytes;
+  P.blobGlobal = blobGlobal;
   P.genOff = (int)genOff;
   P.projOff = (int)projOff;
   P.atomsOff = (int)atomsOff;

@@ -225,16 +225,15 @@ def _cell_volume(cell) -> float:
 
 
 def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelength: float = 1.5406,
-                     max_refl: int = 2400):
+                     max_refl: int = 3000):
     """Seeded uneven problems: space groups from BATCH_GROUPS, 1-24 sites and
     50-3000 reflections and 2000-12000 points and 256-2048 replicas (all
     log-uniform), cells uniform in 4-20 A, at most ``max_atoms`` atoms per
     cell (resampled otherwise).  The reflection count sets d_min through the
-    volume of the reciprocal sphere, capped at ``max_refl`` -- the tables of
-    a search are staged in the shared memory of each CTA, and beyond ~2400
-    reflections they no longer fit next to eight replica slices; the point
-    count is recorded only (the search's fitness works on integrated
-    intensities)."""
+    volume of the reciprocal sphere, capped at ``max_refl`` (a search whose
+    tables do not fit in shared memory next to its eight replica slices reads
+    them from global memory); the point count is recorded only (the search's
+    fitness works on integrated intensities)."""
     from .symmetry import space_group
     rng = np.random.default_rng(seed)
     out: List[BatchItem] = []

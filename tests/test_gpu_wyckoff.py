@@ -709,3 +709,34 @@ def test_screening_stage_keeps_the_best_two_waves():
     assert res.assignments == order[:10]
     assert 0 in res.assignments
     assert res.best_assignment == 0, (res.best_assignment, res.per_assignment)
+
+
+def test_tables_too_large_to_stage_are_read_from_global_memory(oracle):
+    """6432 reflections in 632 groups: the staged tables and eight replica
+    slices exceed a CTA's shared memory, so the tables are read from global
+    memory; the fitness and penalty match the oracle as on the staged path
+    (cc within 2e-6, penalty within 1e-5), and a short fused search runs."""
+    cell = {'a': 16.96, 'b': 10.80, 'c': 13.92, 'alpha': 90.0, 'beta': 90.0, 'gamma': 90.0}
+    P = wyckoff_problem(seed=1, cell=cell, dmin=0.6, true_min_contact=1.2, contact_attempts=200)
+    assert P.refl.n_refl > 6000
+    n = 64
+    X, _ = random_positions(P, n, 31)
+    X[:P.max_sites * 3] = to_fixed(P.true_coords)
+    with WyckoffSession(P, n) as s:
+        q = s.query()
+        assert q['smem_bytes'] < P.refl.n_refl * 4 * 8 + 8 * 1024 * 8   # slices only, no staged tables
+        s.write_positions_fixed(X)
+        s.set_params(P.refl.n_groups, 1.0)
+        s.dispatch(None, mcmc=False)
+        s.synchronize(60)
+        _, _, st = s.read_state()
+        worst_cc = worst_pen = 0.0
+        for p in range(n):
+            sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
+            cc, pen, _ = oracle_cc_pen(oracle, P, sites, P.refl.n_groups, 1.0)
+            worst_cc = max(worst_cc, abs(float(st['cc'][p]) - cc))
+            worst_pen = max(worst_pen, abs(float(st['pen'][p]) - pen) / max(1.0, pen))
+        assert worst_cc <= 2e-6 and worst_pen <= 1e-5, (worst_cc, worst_pen)
+        assert float(st['cc'][0]) > 0.9
+    res = run_wyckoff_search(P, num_particles=256, generations=100, seed=2, do_quench=False)
+    assert np.isfinite(res.best_cc) and res.cpu_check['delta'] < 1e-5

@@ -154,4 +154,4 @@ def test_batched_problem_generator():
         assert sum(d['count'] for d in P.demand) <= 512
         assert 256 <= it.replicas <= 2048 and it.replicas % 8 == 0
         assert 2000 <= it.points <= 12000
-        assert P.refl.n_refl >= 8
+        assert 8 <= P.refl.n_refl <= 3000
