@@ -176,6 +176,12 @@ p6_status p6_wy_synchronize(p6_wy_session *s, double timeout_seconds);
 /* Exact coordinate access in the kernel's 32-bit fixed point (x * 2^32). */
 p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current);
 p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best);
+/* Launch shape of the fused search (p6_wy_run): each replica ladder of 8 on
+ * one CTA of 8 warps (1) or on a thread-block cluster of two 4-warp CTAs (2,
+ * the default; clash-penalty problems only, others use 1).  Two CTAs per
+ * ladder spread the ladders evenly over the SMs; the results are the same
+ * bit for bit.  The reference runs one workgroup per replica. */
+p6_status p6_wy_set_ladder_split(p6_wy_session *s, int ctas_per_ladder);
 /* syncStateToGPU after a prune (js/swarm_wyckoff.js:2303-2336): current and
  * best coordinates in fixed point and the particle states, written together
  * so the chains that keep their assignment keep their best structure exactly. */

@@ -22,6 +22,7 @@
 //  * the group sums scc, soo, sco are accumulated and reduced in FP64;
 //  * random numbers are Philox4x32-10 keyed by (chain seed, session key) and
 //    counted by (generation, replica, lane, purpose): no generator state.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1109,10 +1110,31 @@ __device__ __forceinline__ void propose(const Params &P, WarpView &ws, const Pro
 // ---------------------------------------------------------------------------
 // The kernel.
 // ---------------------------------------------------------------------------
+// A ladder held by RANKS CTAs of one thread-block cluster (RANKS = 2: four
+// rungs each, so 512 ladders become 1024 CTAs that spread evenly over 148
+// SMs).  The exchange energies live in rank 0's shared memory and a swap
+// across the two CTAs moves coordinates through distributed shared memory;
+// with RANKS = 1 these are the CTA's own arrays and the syncs are
+// __syncthreads.
+template <int RANKS>
+__device__ __forceinline__ void ladder_sync() {
+  if constexpr (RANKS > 1)
+    cooperative_groups::this_cluster().sync();
+  else
+    __syncthreads();
+}
+template <int RANKS, class T>
+__device__ __forceinline__ T *ladder_peer(T *p, int rank) {
+  if constexpr (RANKS > 1)
+    return cooperative_groups::this_cluster().map_shared_rank(p, rank);
+  else
+    return p;
+}
+
 // One CTA's share of a search: ladders L0, L0 + Lstep, ... of the problem P,
 // generations [gen0, gen0 + nGen).  Returns false (on every thread) when the
 // static tables could not be staged in time.
-template <int COSMODE, int SLOTS, int INCR>
+template <int COSMODE, int SLOTS, int INCR, int RANKS = 1>
 __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int gen0, int nGen, int mcmc,
                                        int swapEvery, int reevalFirst) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1120,9 +1142,12 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   __shared__ float shellLen[27];
   __shared__ float exFit[kMaxRungs], exCC[kMaxRungs], exPen[kMaxRungs], exTemp[kMaxRungs], exE[kMaxRungs];
   __shared__ int exSwap[kMaxRungs];
+  __shared__ int stagedFlag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nWarps = blockDim.x >> 5;
+  const int rank = RANKS > 1 ? (int)cooperative_groups::this_cluster().block_rank() : 0;
+  const int rung = warp + rank * nWarps;   // this warp's rung of the ladder
 
   // Stage the static tables once per CTA with the bulk-copy engine, unless
   // they are too large to share the CTA's shared memory with the replica
@@ -1147,8 +1172,15 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
                         (float)((int)threadIdx.x % 3 - 1)};
     shellLen[threadIdx.x] = cart_len(P, t);
   }
-  const bool staged = !stage || __syncthreads_and(mbar_wait_bounded(&stageBar, 0, kStageWaitLimit) ? 1 : 0) != 0;
+  bool staged = !stage || __syncthreads_and(mbar_wait_bounded(&stageBar, 0, kStageWaitLimit) ? 1 : 0) != 0;
   if (!stage) __syncthreads();
+  if constexpr (RANKS > 1) {
+    // both CTAs of the ladder go on, or both return
+    if (threadIdx.x == 0) stagedFlag = staged ? 1 : 0;
+    ladder_sync<RANKS>();
+    staged = staged && *ladder_peer<RANKS>(&stagedFlag, rank ^ 1) != 0;
+    ladder_sync<RANKS>();
+  }
   if (!staged) {
     if (threadIdx.x == 0) raise_flag(P.errFlag, DEV_STAGE_TIMEOUT);
     mbar_wait_bounded(&stageBar, 0, kStageWaitLimit);   // copies still in flight land before the CTA moves on
@@ -1180,11 +1212,11 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
 
   for (int L = L0; L < nLadders; L += Lstep) {
     int p = -1;
-    if (warp < rungs) {
+    if (rung < rungs) {
       if (P.ladders)
-        p = P.ladders[(size_t)L * rungs + warp];
+        p = P.ladders[(size_t)L * rungs + rung];
       else {
-        const int q = L * rungs + warp;
+        const int q = L * rungs + rung;
         p = q < P.numParticles ? q : -1;
       }
     }
@@ -1368,13 +1400,16 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
       prevNga = nga;
       // replica exchange inside the ladder (js/swarm_wyckoff.js:1825-1851)
       if (swapEvery > 0 && mcmc && P.ladders && ((g + 1) % swapEvery) == 0) {
+        float *eFit = ladder_peer<RANKS>(exFit, 0), *eCC = ladder_peer<RANKS>(exCC, 0);
+        float *ePen = ladder_peer<RANKS>(exPen, 0);
+        const int *eSwap = ladder_peer<RANKS>(exSwap, 0);
         if (active && lane == 0) {
-          exFit[warp] = fit; exCC[warp] = cc0; exPen[warp] = pen0; exTemp[warp] = temp;
-          exE[warp] = isfinite(cc0) ? cc0 - pen0 * penScale : fit;
+          eFit[rung] = fit; eCC[rung] = cc0; ePen[rung] = pen0; ladder_peer<RANKS>(exTemp, 0)[rung] = temp;
+          ladder_peer<RANKS>(exE, 0)[rung] = isfinite(cc0) ? cc0 - pen0 * penScale : fit;
         }
-        if (threadIdx.x < kMaxRungs) exSwap[threadIdx.x] = -1;
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        if (rank == 0 && threadIdx.x < kMaxRungs) exSwap[threadIdx.x] = -1;
+        ladder_sync<RANKS>();
+        if (rank == 0 && threadIdx.x == 0) {
           const int parity = ((g + 1) / swapEvery) & 1;
           unsigned long long tried = 0, taken = 0;
           for (int r = parity; r + 1 < rungs; r += 2) {
@@ -1400,25 +1435,29 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             atomicAdd(P.swapStats + 1, taken);
           }
         }
-        __syncthreads();
-        // each pair (r, r+1) swaps coordinates and energies; rungs keep temp and step
-        for (int r = warp; r < rungs; r += nWarps) {
-          if (exSwap[r] < 0) continue;
-          const WarpView wa = warp_view(smem + blobPad + (size_t)r * P.warpSmemBytes, P);
-          const WarpView wb = warp_view(smem + blobPad + (size_t)(r + 1) * P.warpSmemBytes, P);
+        ladder_sync<RANKS>();
+        // the energies after the decisions; a rung that received other
+        // coordinates refills its site sums
+        if (active) {
+          if (lane == 0) { fit = eFit[rung]; cc0 = eCC[rung]; pen0 = ePen[rung]; }
+          const bool swapped = eSwap[rung] >= 0 || (rung > 0 && eSwap[rung - 1] == rung);
+          if (swapped) cachedAct = -1;
+        }
+        // each pair (r, r+1) swaps coordinates, by rung r's warp; rungs keep temp and step
+        if (rung < rungs && eSwap[rung] >= 0) {
+          const int r1 = rung + 1;
+          unsigned char *mine = smem + blobPad + (size_t)warp * P.warpSmemBytes;
+          unsigned char *other =
+              ladder_peer<RANKS>(smem + blobPad + (size_t)(r1 % nWarps) * P.warpSmemBytes, r1 / nWarps);
+          const WarpView wa = warp_view(mine, P);
+          const WarpView wb = warp_view(other, P);
           for (int j = lane; j < (int)curStride; j += 32) {
             const uint32_t t = wa.cur[j];
             wa.cur[j] = wb.cur[j];
             wb.cur[j] = t;
           }
         }
-        __syncthreads();
-        if (active) {
-          if (lane == 0) { fit = exFit[warp]; cc0 = exCC[warp]; pen0 = exPen[warp]; }
-          // a rung that received other coordinates refills its site sums
-          const bool swapped = exSwap[warp] >= 0 || (warp > 0 && exSwap[warp - 1] == warp);
-          if (swapped) cachedAct = -1;
-        }
+        ladder_sync<RANKS>();
       }
     }
     if (active) {
@@ -1435,7 +1474,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   }
   // the staging barrier is set up afresh by the next call on this CTA
   if (stage && threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&stageBar)) : "memory");
-  __syncthreads();
+  ladder_sync<RANKS>();   // no CTA leaves while its partner may still reach its shared memory
   return true;
 }
 
@@ -1443,6 +1482,14 @@ template <int COSMODE, int SLOTS, int INCR>
 __global__ void __launch_bounds__(256, 4) wy_kernel(const __grid_constant__ Params P, int gen0, int nGen, int mcmc,
                                                     int swapEvery, int reevalFirst) {
   wy_cta<COSMODE, SLOTS, INCR>(P, blockIdx.x, gridDim.x, gen0, nGen, mcmc, swapEvery, reevalFirst);
+}
+
+// The same search with each ladder of 8 on a cluster of two 4-warp CTAs
+// (launched with cluster dimension 2): ladder = cluster index.
+template <int COSMODE, int SLOTS, int INCR>
+__global__ void __launch_bounds__(128, 8) wy_kernel_pair(const __grid_constant__ Params P, int gen0, int nGen,
+                                                         int mcmc, int swapEvery, int reevalFirst) {
+  wy_cta<COSMODE, SLOTS, INCR, 2>(P, blockIdx.x >> 1, gridDim.x >> 1, gen0, nGen, mcmc, swapEvery, reevalFirst);
 }
 
 // Per-problem generation range of a batched launch.
@@ -1634,6 +1681,8 @@ struct p6_wy_session {
   std::vector<uint32_t> siteCountOfAssign;
   int smemBytes = 0;
   int maxGrid = 0;
+  int smemPair = 0;      // per CTA when a ladder spans a cluster of two CTAs
+  int ladderSplit = 2;   // CTAs per ladder of 8 in the fused search (1 or 2)
 };
 
 namespace {
@@ -1746,6 +1795,28 @@ static cudaError_t launch_variant(p6_wy_session *s, int grid, int block, int gen
   return cudaGetLastError();
 }
 
+// A ladder of 8 on a cluster of two 4-warp CTAs, one cluster per ladder.
+template <int C, int I>
+static cudaError_t launch_pair(p6_wy_session *s, int gen0, int nGen, int mcmc, int swapEvery, int reevalFirst) {
+  auto k = wy_kernel_pair<C, 0, I>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemPair);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * s->P.nLadders, 1, 1);
+  cfg.blockDim = dim3(128, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)s->smemPair;
+  cfg.stream = s->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, k, s->P, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
 template <int C, int S>
 static cudaError_t launch_incr(p6_wy_session *s, int grid, int block, int gen0, int nGen, int mcmc, int swapEvery,
                                int reevalFirst) {
@@ -1761,6 +1832,16 @@ static cudaError_t launch(p6_wy_session *s, int gen0, int nGen, int mcmc, int sw
   grid = std::max(grid, 1);
   cudaError_t e;
   const int C = s->cosMode, S = s->slots;
+  if (s->ladderSplit == 2 && P.ladders && rungs == 8 && S == 0 && s->smemPair > 0) {
+    if (C == 0)
+      e = s->incremental ? launch_pair<0, 1>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
+                         : launch_pair<0, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
+    else
+      e = s->incremental ? launch_pair<1, 1>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
+                         : launch_pair<1, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
+    if (e == cudaSuccess) s->launches++;
+    return e;
+  }
   if (C == 0 && S == 0) e = launch_incr<0, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
   else if (C == 1 && S == 0) e = launch_incr<1, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
   else if (C == 0 && S == 64) e = launch_incr<0, 64>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
@@ -2088,6 +2169,7 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
     return set_error(P6_ERR_CAPACITY, "the reflection table and generated cell do not fit in shared memory");
   }
   s->smemBytes = (int)smem;
+  s->smemPair = (int)((blobGlobal ? 0 : blobPadded) + warpBytes * (rungs / 2));
   p6_status st;
 #define P6_TRY(x)                   \
   do {                              \
@@ -2304,6 +2386,14 @@ p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current)
   P6_CUDA(cudaMemcpyAsync(s->dPos, current, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
   P6_CUDA(cudaMemcpyAsync(s->dPos + n, current, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
   P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_set_ladder_split(p6_wy_session *s, int ctas_per_ladder) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  if (ctas_per_ladder != 1 && ctas_per_ladder != 2) return set_error(P6_ERR_INVALID_ARG, "ctas_per_ladder must be 1 or 2");
+  s->ladderSplit = ctas_per_ladder;
   return P6_OK;
 }
 

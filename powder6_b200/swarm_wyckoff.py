@@ -220,6 +220,10 @@ class WyckoffSession:
         a = np.ascontiguousarray(x, dtype=np.uint32)
         check(self.lib.p6_wy_write_positions_fixed(self.h, ptr(a)))
 
+    def set_ladder_split(self, ctas_per_ladder: int):
+        """Each ladder of 8 on one 8-warp CTA (1) or a cluster of two 4-warp CTAs (2, default)."""
+        check(self.lib.p6_wy_set_ladder_split(self.h, int(ctas_per_ladder)))
+
     def write_state_fixed(self, current: np.ndarray, best: np.ndarray, state: np.ndarray):
         c = np.ascontiguousarray(current, dtype=np.uint32)
         b = np.ascontiguousarray(best, dtype=np.uint32)

@@ -740,3 +740,35 @@ def test_tables_too_large_to_stage_are_read_from_global_memory(oracle):
         assert float(st['cc'][0]) > 0.9
     res = run_wyckoff_search(P, num_particles=256, generations=100, seed=2, do_quench=False)
     assert np.isfinite(res.best_cc) and res.cpu_check['delta'] < 1e-5
+
+
+def test_ladders_on_two_cta_clusters_are_bit_identical(prob):
+    """The fused search with each ladder of 8 on a cluster of two 4-warp CTAs
+    (exchange energies in rank 0's shared memory, cross-CTA swaps through
+    distributed shared memory) gives the same coordinates, bests and states,
+    bit for bit, as the one-CTA ladder, with exchanges taking place."""
+    P = prob
+    n, G = 1024, 300
+    outs = []
+    for split in (1, 2):
+        with WyckoffSession(P, n, run_key=91) as s:
+            s.set_ladder_split(split)
+            assign = np.zeros(n, dtype=np.uint32)
+            s.set_assign(assign)
+            ladders, temps = build_ladders(assign)
+            s.set_ladders(ladders, 8)
+            groups, pen = schedule(G, P.refl.n_groups)
+            s.set_schedule(groups, pen)
+            rnd = mulberry32(17)
+            pos = project_all(P, np.array([rnd() for _ in range(n * s.coords_per_particle)], dtype=np.float32), assign)
+            s.sync_state(pos, initial_state(n, temps, rnd))
+            s.run(0, G, 10, True)
+            s.synchronize(120)
+            cur, best = s.read_positions_fixed()
+            _, _, st = s.read_state()
+            outs.append((cur, best, st.tobytes()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+    st = np.frombuffer(outs[1][2], dtype=STATE_DTYPE)
+    assert np.max(st['best_cc']) > 0.5
