@@ -178,7 +178,8 @@ p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current)
 p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best);
 /* Launch shape of the fused search (p6_wy_run): each replica ladder of 8 on
  * one CTA of 8 warps (1) or on a thread-block cluster of two 4-warp CTAs (2,
- * the default; clash-penalty problems only, others use 1).  Two CTAs per
+ * the default; clash-penalty problems with staged tables and the full
+ * evaluation only, others use 1).  Two CTAs per
  * ladder spread the ladders evenly over the SMs; the results are the same
  * bit for bit.  The reference runs one workgroup per replica. */
 p6_status p6_wy_set_ladder_split(p6_wy_session *s, int ctas_per_ladder);

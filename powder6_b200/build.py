@@ -41,19 +41,37 @@ def needs_build() -> bool:
 
 
 def build(verbose: bool = False, force: bool = False) -> Path:
+    """Each source compiled to an object in parallel (objects in _build/),
+    then linked into the shared library."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc_path(), *ARCH, '-O3', '-lineinfo', '-std=c++17', '--use_fast_math',
-           '-Xcompiler', '-fPIC', '-shared', '-I', str(ROOT / 'include'),
-           '-o', str(LIB) + '.tmp', *map(str, sources())]
+    from concurrent.futures import ThreadPoolExecutor
+    obj_dir = ROOT / '_build'
+    obj_dir.mkdir(exist_ok=True)
+    nvcc = nvcc_path()
+    flags = [*ARCH, '-O3', '-lineinfo', '-std=c++17', '--use_fast_math', '-Xcompiler', '-fPIC',
+             '-I', str(ROOT / 'include')]
     if verbose:
-        cmd.insert(1, '-Xptxas=-v')
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError('nvcc failed building libp6cuda.so')
-    if verbose:
-        sys.stderr.write(res.stderr)
+        flags.insert(0, '-Xptxas=-v')
+
+    def compile_one(src: Path):
+        obj = obj_dir / (src.stem + '.o')
+        return src, obj, subprocess.run([nvcc, *flags, '-c', str(src), '-o', str(obj)], capture_output=True, text=True)
+
+    srcs = sorted(sources(), key=lambda q: -q.stat().st_size)   # the largest first
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, srcs))
+    for src, obj, res in results:
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError(f'nvcc failed on {src.name}')
+        if verbose:
+            sys.stderr.write(res.stderr)
+    link = subprocess.run([nvcc, *ARCH, '-shared', '-o', str(LIB) + '.tmp', *[str(o) for _, o, _ in results]],
+                          capture_output=True, text=True)
+    if link.returncode != 0:
+        sys.stderr.write(link.stdout + link.stderr)
+        raise RuntimeError('nvcc failed linking libp6cuda.so')
     os.replace(str(LIB) + '.tmp', LIB)
     return LIB
 

@@ -1134,7 +1134,9 @@ __device__ __forceinline__ T *ladder_peer(T *p, int rank) {
 // One CTA's share of a search: ladders L0, L0 + Lstep, ... of the problem P,
 // generations [gen0, gen0 + nGen).  Returns false (on every thread) when the
 // static tables could not be staged in time.
-template <int COSMODE, int SLOTS, int INCR, int RANKS = 1>
+// GT = 1: the static tables are read from global memory (too large to stage);
+// a template parameter so that the staged path keeps shared-memory loads.
+template <int COSMODE, int SLOTS, int INCR, int RANKS = 1, int GT = 0>
 __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int gen0, int nGen, int mcmc,
                                        int swapEvery, int reevalFirst) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1152,8 +1154,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   // Stage the static tables once per CTA with the bulk-copy engine, unless
   // they are too large to share the CTA's shared memory with the replica
   // slices: then every table read goes to global memory (through L1).
-  const bool stage = !P.blobGlobal;
-  const unsigned char *stat = stage ? smem : P.blob;
+  constexpr bool stage = GT == 0;
+  const unsigned char *stat = GT ? P.blob : smem;
   const int blobPad = stage ? (P.blobBytes + 127) & ~127 : 0;
   if (stage && threadIdx.x == 0) {
     mbar_init(&stageBar, 1);
@@ -1478,10 +1480,10 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   return true;
 }
 
-template <int COSMODE, int SLOTS, int INCR>
+template <int COSMODE, int SLOTS, int INCR, int GT = 0>
 __global__ void __launch_bounds__(256, 4) wy_kernel(const __grid_constant__ Params P, int gen0, int nGen, int mcmc,
                                                     int swapEvery, int reevalFirst) {
-  wy_cta<COSMODE, SLOTS, INCR>(P, blockIdx.x, gridDim.x, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  wy_cta<COSMODE, SLOTS, INCR, 1, GT>(P, blockIdx.x, gridDim.x, gen0, nGen, mcmc, swapEvery, reevalFirst);
 }
 
 // The same search with each ladder of 8 on a cluster of two 4-warp CTAs
@@ -1518,7 +1520,12 @@ __global__ void __launch_bounds__(256, 4) wy_batch_kernel(const Params *probs, c
     __syncthreads();
     const RunArgs a = args[w.x];
     // Lstep = nLadders: this ladder only
-    if (!wy_cta<COSMODE, SLOTS, INCR>(Ps, w.y, Ps.nLadders, a.gen0, a.nGen, a.mcmc, a.swapEvery, a.reevalFirst)) break;
+    const bool ok = Ps.blobGlobal
+                        ? wy_cta<COSMODE, SLOTS, INCR, 1, 1>(Ps, w.y, Ps.nLadders, a.gen0, a.nGen, a.mcmc, a.swapEvery,
+                                                             a.reevalFirst)
+                        : wy_cta<COSMODE, SLOTS, INCR, 1, 0>(Ps, w.y, Ps.nLadders, a.gen0, a.nGen, a.mcmc, a.swapEvery,
+                                                             a.reevalFirst);
+    if (!ok) break;
     __syncthreads();
   }
 }
@@ -1788,7 +1795,10 @@ static void free_session(p6_wy_session *s) {
 template <int C, int S, int I>
 static cudaError_t launch_variant(p6_wy_session *s, int grid, int block, int gen0, int nGen, int mcmc,
                                   int swapEvery, int reevalFirst) {
-  auto k = wy_kernel<C, S, I>;
+  // global tables only without incremental sums (those need the shared memory anyway)
+  auto k = wy_kernel<C, S, I, 0>;
+  if constexpr (I == 0)
+    if (s->P.blobGlobal) k = wy_kernel<C, S, I, 1>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemBytes);
   if (e != cudaSuccess) return e;
   k<<<grid, block, s->smemBytes, s->stream>>>(s->P, gen0, nGen, mcmc, swapEvery, reevalFirst);
@@ -1832,13 +1842,10 @@ static cudaError_t launch(p6_wy_session *s, int gen0, int nGen, int mcmc, int sw
   grid = std::max(grid, 1);
   cudaError_t e;
   const int C = s->cosMode, S = s->slots;
-  if (s->ladderSplit == 2 && P.ladders && rungs == 8 && S == 0 && s->smemPair > 0) {
-    if (C == 0)
-      e = s->incremental ? launch_pair<0, 1>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
-                         : launch_pair<0, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
-    else
-      e = s->incremental ? launch_pair<1, 1>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
-                         : launch_pair<1, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  if (s->ladderSplit == 2 && P.ladders && rungs == 8 && S == 0 && !s->incremental && s->smemPair > 0 &&
+      !P.blobGlobal) {
+    e = C == 0 ? launch_pair<0, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
+               : launch_pair<1, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
     if (e == cudaSuccess) s->launches++;
     return e;
   }
