@@ -1,5 +1,5 @@
-"""The oracle itself: known answers and identities it must satisfy before it is
-trusted as the checker of the kernels."""
+"""The oracle itself: known answers and identities it must satisfy before the
+kernels are compared against it."""
 import ctypes as C
 import math
 
