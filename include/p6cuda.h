@@ -176,6 +176,26 @@ p6_status p6_wy_synchronize(p6_wy_session *s, double timeout_seconds);
 /* Exact coordinate access in the kernel's 32-bit fixed point (x * 2^32). */
 p6_status p6_wy_write_positions_fixed(p6_wy_session *s, const uint32_t *current);
 p6_status p6_wy_read_positions_fixed(p6_wy_session *s, uint32_t *current, uint32_t *best);
+/* Wyckoff-constrained least-squares refinement of coordinates against the
+ * grouped |F|^2 of the session's tables (refineCoordinatesAgainstWppf,
+ * js/coord_refine.js:266-627): per structure, the closed-form intensity
+ * scale, the analytic Jacobian in the constrained space (P^T), Marquardt
+ * damping scaled by the diagonal, a trust region of max_step (fractional,
+ * infinity norm) and projection back onto the Wyckoff subspaces after each
+ * step.  The group intensities, derivatives and normal equations are FP64 on
+ * the device (one CTA per structure); the damping control runs on the host
+ * for all structures in lock step.  coords (n * max_sites * 3, fractional) are
+ * refined in place; r_start / r_final are the weighted wR(F^2), chi2 the
+ * final weighted residual, iterations the accepted steps.  NULL opts: the
+ * reference's defaults (60 iterations, lambda 1e-3 x10 / x0.4 up to 1e8,
+ * tol_step 1e-6, tol_chi 1e-9, max_step 0.05).  Any output may be NULL. */
+typedef struct {
+  int max_iter;
+  double lambda0, lambda_up, lambda_down, lambda_max, tol_step, tol_chi, max_step;
+} p6_wy_refine_opts;
+p6_status p6_wy_refine(p6_wy_session *s, int n, const uint32_t *assign, double *coords,
+                       const p6_wy_refine_opts *opts, double *r_start, double *r_final, double *chi2,
+                       int *iterations, int *converged);
 /* Launch shape of the fused search (p6_wy_run): each replica ladder of 8 on
  * one CTA of 8 warps (1) or on a thread-block cluster of two 4-warp CTAs (2,
  * the default; clash-penalty problems with staged tables and the full

@@ -8,6 +8,7 @@ baseline leg import this module; the product path never does.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import subprocess
 from pathlib import Path
 
@@ -442,3 +443,150 @@ def mlp_grads_fp64(w, X, T, mask, d_in, width, d_out):
     dW1 = X.T @ dH1
     db1 = dH1.sum(0)
     return np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dW3.ravel(), db3]), loss
+
+
+# ---------------------------------------------------------------------------
+# Wyckoff-constrained coordinate refinement (js/coord_refine.js:266-627), FP64
+# ---------------------------------------------------------------------------
+def _refine_tables(problem, A):
+    """The images entering |F|^2 (site, R, t) of assignment A, the exact
+    projectors, and the grouped observations, from the packed tables."""
+    from fractions import Fraction
+    T = problem.tables
+    ms, nT = T.max_sites, T.n_tot
+    gp = T.gen_pack[A * nT:(A + 1) * nT].astype(np.int64)
+    sym = problem.sym_packed.astype(np.float64).reshape(-1, 12)
+
+    def tfix(v):
+        s = v * 24.0
+        r = math.floor(s + 0.5)
+        if abs(s - r) < 1e-4:
+            return ((int(r) % 24) * 2 ** 32 + 12) // 24 / 2.0 ** 32
+        f = v - math.floor(v)
+        return (math.floor(f * 2 ** 32 + 0.5) % 2 ** 32) / 2.0 ** 32
+
+    atoms = []
+    for w in gp:
+        if (w >> 24) & 1:
+            continue
+        site, op, ty = int(w & 0xFF), int((w >> 8) & 0xFFF), int(min((w >> 20) & 0xF, problem.n_elem - 1))
+        R = sym[op, :9].round().reshape(3, 3)
+        t = np.array([tfix(float(v)) for v in sym[op, 9:]])
+        atoms.append((site, R, t, ty))
+    projs = []
+    sites = problem.assignments[A].sites
+    for si in range(ms):
+        if si < len(sites):
+            Pm = np.array([float(Fraction(v)) for v in sites[si].w.P], dtype=np.float64).reshape(3, 3)
+            Tv = np.array([tfix(float(Fraction(v))) for v in sites[si].w.T])
+        else:
+            Pm, Tv = np.zeros((3, 3)), np.zeros(3)
+        projs.append((Pm, Tv))
+    gm = problem.refl.group_meta.astype(np.float64).reshape(-1, 4)
+    pk = problem.refl.refl_pack[0::2].astype(np.int64)
+    hkl = np.stack([(pk & 0x3FF) - 512, ((pk >> 10) & 0x3FF) - 512, ((pk >> 20) & 0x3FF) - 512], 1).astype(np.float64)
+    mult = problem.refl.refl_pack[1::2].astype(np.float64)
+    ftab = problem.f_tab.astype(np.float64).reshape(-1, problem.n_elem)
+    return atoms, projs, gm, hkl, mult, ftab
+
+
+def wy_refine_intensities(problem, A, x, jac=False):
+    """Ical per group (sum mult |F|^2) and, with jac, dIcal/du in the constrained space (P^T)."""
+    atoms, projs, gm, hkl, mult, ftab = _refine_tables(problem, A)
+    ms = problem.tables.max_sites
+    x = np.asarray(x, dtype=np.float64).reshape(ms, 3)
+    pos = np.array([(R @ x[s] + t) % 1.0 for s, R, t, _ in atoms])
+    ty = np.array([a[3] for a in atoms])
+    ical = np.zeros(len(gm))
+    J = np.zeros((len(gm), ms * 3)) if jac else None
+    for g, (r0, cnt, _, _) in enumerate(gm):
+        grow = np.zeros(ms * 3)
+        for r in range(int(r0), int(r0) + int(cnt)):
+            ph = 2 * np.pi * (pos @ hkl[r])
+            f = ftab[r, ty]
+            c, s = np.cos(ph), np.sin(ph)
+            a_, b_ = float((f * c).sum()), float((f * s).sum())
+            ical[g] += mult[r] * (a_ * a_ + b_ * b_)
+            if jac:
+                w = mult[r] * 2 * 2 * np.pi * f * (b_ * c - a_ * s)
+                for j, (site, R, _, _) in enumerate(atoms):
+                    grow[3 * site:3 * site + 3] += w[j] * (R.T @ hkl[r])
+        if jac:
+            for si, (Pm, _) in enumerate(projs):
+                J[g, 3 * si:3 * si + 3] = Pm.T @ grow[3 * si:3 * si + 3]
+    return ical, J
+
+
+def wy_refine(problem, A, x0, max_iter=60, lambda0=1e-3, lambda_up=10.0, lambda_down=0.4, lambda_max=1e8,
+              tol_step=1e-6, tol_chi=1e-9, max_step=0.05):
+    """refineCoordinatesAgainstWppf restated in FP64 on the packed tables:
+    returns (coords, r_start, r_final, chi2, steps, converged)."""
+    atoms, projs, gm, _, _, _ = _refine_tables(problem, A)
+    ms = problem.tables.max_sites
+    wt = np.where(gm[:, 3] > 0, gm[:, 3], 0.0)
+    io = gm[:, 2]
+
+    def project(x):
+        x = x.reshape(ms, 3).copy()
+        for si, (Pm, Tv) in enumerate(projs):
+            x[si] = (Pm @ x[si] + Tv) % 1.0
+        return x.reshape(-1)
+
+    def scale_chi(ical):
+        den = float((wt * ical * ical).sum())
+        s = float((wt * io * ical).sum()) / den if den > 0 else 0.0
+        return s, float((wt * (io - s * ical) ** 2).sum())
+
+    oo = float((wt * io * io).sum())
+    cur = project(np.asarray(x0, dtype=np.float64))
+    ical, _ = wy_refine_intensities(problem, A, cur)
+    s, chi = scale_chi(ical)
+    r_start = math.sqrt(chi / oo)
+    lam, steps, conv = lambda0, 0, False
+    for _ in range(max_iter):
+        ical, J = wy_refine_intensities(problem, A, cur, jac=True)
+        s, chi = scale_chi(ical)
+        Js = s * J
+        res = io - s * ical
+        JTr = (wt[:, None] * Js * res[:, None]).sum(0)
+        JTJ = (Js * wt[:, None]).T @ Js
+        stepped = False
+        while lam < lambda_max:
+            aug = JTJ.copy()
+            dmax = float(np.max(np.diag(aug)))
+            if not dmax > 0:
+                conv = True
+                break
+            d = np.diag(aug).copy()
+            aug[np.diag_indices_from(aug)] += lam * np.maximum(d, 1e-6 * dmax)
+            try:
+                L = np.linalg.cholesky(aug)
+                dx = np.linalg.solve(L.T, np.linalg.solve(L, JTr))
+            except np.linalg.LinAlgError:
+                lam *= lambda_up
+                continue
+            dx = dx.reshape(ms, 3)
+            for si, (Pm, _) in enumerate(projs):
+                dx[si] = Pm @ dx[si]
+            dx = dx.reshape(-1)
+            big = float(np.max(np.abs(dx)))
+            cap = max_step / big if big > max_step else 1.0
+            trial = project(cur + cap * dx)
+            itr, _ = wy_refine_intensities(problem, A, trial)
+            s_tr, chi_tr = scale_chi(itr)
+            if chi_tr < chi:
+                moved = float(np.max(np.abs(trial - cur)))
+                rel = (chi - chi_tr) / max(chi, 1e-300)
+                cur, s, chi = trial, s_tr, chi_tr
+                lam = max(lam * lambda_down, 1e-12)
+                stepped, steps = True, steps + 1
+                if moved < tol_step or rel < tol_chi:
+                    conv = True
+                break
+            lam *= lambda_up
+        if conv or not stepped:
+            break
+    ical, _ = wy_refine_intensities(problem, A, cur)
+    s, chi = scale_chi(ical)
+    return cur, r_start, math.sqrt(chi / oo), chi, steps, conv
+

@@ -94,6 +94,7 @@ _SIGS = {
     'p6_wy_read_positions_fixed': (C.c_int, [_P, _P, _P]),
     'p6_wy_write_state_fixed': (C.c_int, [_P, _P, _P, _P]),
     'p6_wy_set_ladder_split': (C.c_int, [_P, C.c_int]),
+    'p6_wy_refine': (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P]),
     'p6_wy_set_trace': (C.c_int, [_P, C.c_int]),
     'p6_wy_read_trace': (C.c_int, [_P, _P, _P]),
     'p6_wy_read_trace_ic': (C.c_int, [_P, _P]),

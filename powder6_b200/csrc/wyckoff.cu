@@ -1686,6 +1686,8 @@ struct p6_wy_session {
   long long launches = 0;
   std::vector<uint32_t> hostAssign;
   std::vector<uint32_t> siteCountOfAssign;
+  std::vector<ProjFix> projHost;     // Wyckoff projectors per (assignment, site), for the refinement
+  std::vector<float4> groupsHost;    // {start, count, Iobs, weight} per reflection group
   int smemBytes = 0;
   int maxGrid = 0;
   int smemPair = 0;      // per CTA when a ladder spans a cluster of two CTAs
@@ -2199,6 +2201,12 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P6_TRY(upload(&s->dFree, freeMask.data(), freeMask.size(), s->stream));
   P6_TRY(upload(&s->dOps, ops.data(), ops.size(), s->stream));
   P6_TRY(upload(&s->dProj, proj.data(), proj.size(), s->stream));
+  s->projHost = proj;
+  s->groupsHost.resize(pr->n_groups);
+  for (int gI = 0; gI < pr->n_groups; ++gI) {
+    const float *gm = pr->group_meta + (size_t)gI * pr->group_stride;
+    s->groupsHost[gI] = make_float4(gm[0], gm[1], gm[2], pr->group_stride >= 4 ? gm[3] : 1.0f);
+  }
   P6_TRY(upload(&s->dBlob, blob.data(), blob.size(), s->stream));
   P6_TRY(upload(&s->dRules, rules.data(), rules.size(), s->stream));
   const size_t posWords = (size_t)2 * pr->num_particles * ms * 3;
@@ -3026,3 +3034,387 @@ p6_status p6_wy_batch_last_ms(p6_wy_batch *b, float *ms) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Wyckoff-constrained least-squares refinement of coordinates against the
+// grouped |F|^2 (refineCoordinatesAgainstWppf, js/coord_refine.js:266-627).
+// The device computes, per structure (one CTA each), the group intensities
+// Ical_g = sum mult |F|^2 over the group's reflections and their analytic
+// derivatives with respect to the site coordinates (the chain rule through
+// R^T h, js/coord_refine.js:216-247, projected into each site's Wyckoff
+// subspace by P^T), then the closed-form scale, chi^2 and the normal
+// equations J'WJ, J'W r in FP64; the host runs the Levenberg-Marquardt
+// control of every structure in lock step.
+// ===========================================================================
+namespace p6 {
+namespace wy {
+
+struct RefineArgs {
+  int nP;                   // maxSites * 3
+  const uint32_t *assign;   // per structure
+  const double *coords;     // structures * nP, fractional
+  double *ical;             // structures * nGroups
+  double *jac;              // structures * nGroups * nP, or null
+  double *out;              // structures * (4 + nP + nP * nP): scale, chi2, sum w Io^2, -, J'Wr, J'WJ
+};
+
+constexpr int kRefineThreads = 128;
+constexpr int kRefineMaxAtoms = 1024;
+
+__global__ void __launch_bounds__(kRefineThreads) wy_refine_eval_kernel(const Params P, const RefineArgs R) {
+  __shared__ double ax[kRefineMaxAtoms * 3];
+  __shared__ short asite[kRefineMaxAtoms], aop[kRefineMaxAtoms], atype[kRefineMaxAtoms];
+  __shared__ int nAt;
+  const int st = blockIdx.x, nP = R.nP, ms = P.maxSites;
+  const int A = (int)R.assign[st];
+  const uint32_t *gen = P.genOrig + (size_t)A * P.nTot;
+  const OpFix *ops = P.ops;
+  const double *u = R.coords + (size_t)st * nP;
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int g = 0; g < P.nTot && n < kRefineMaxAtoms; ++g) {
+      const uint32_t w = gen[g];
+      if ((w >> 24) & 1u) continue;   // centring translates scale |F|^2 only; the scale absorbs it
+      asite[n] = (short)(w & 0xFF);
+      aop[n] = (short)((w >> 8) & 0xFFF);
+      atype[n] = (short)min((int)((w >> 20) & 0xF), P.nElem - 1);
+      ++n;
+    }
+    nAt = n;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nAt; j += blockDim.x) {
+    const OpFix &op = ops[aop[j]];
+    const double *x = u + 3 * asite[j];
+    for (int i = 0; i < 3; ++i) {
+      const double v = op.r[3 * i] * x[0] + op.r[3 * i + 1] * x[1] + op.r[3 * i + 2] * x[2] +
+                       (double)op.t[i] * (1.0 / 4294967296.0);
+      ax[3 * j + i] = v - floor(v);
+    }
+  }
+  __syncthreads();
+  const ReflRec *refl = reinterpret_cast<const ReflRec *>(P.blob + P.offRefl);
+  const float *ftab = reinterpret_cast<const float *>(P.blob + P.offF);
+  const float4 *groups = reinterpret_cast<const float4 *>(P.blob + P.offGroup);
+  const bool jac = R.jac != nullptr;
+  for (int gI = threadIdx.x; gI < P.nGroups; gI += blockDim.x) {
+    const float4 gm = groups[gI];
+    const int r0 = (int)gm.x, cnt = (int)gm.y;
+    double acc = 0.0;
+    double grow[kMaxSites * 3];
+    if (jac)
+      for (int p = 0; p < nP; ++p) grow[p] = 0.0;
+    for (int r = r0; r < r0 + cnt; ++r) {
+      const ReflRec rr = refl[r];
+      const double h = rr.h, k = rr.k, l = rr.l;
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < nAt; ++j) {
+        const double f = ftab[(size_t)r * P.nElem + atype[j]];
+        double sn, cs;
+        sincospi(2.0 * (h * ax[3 * j] + k * ax[3 * j + 1] + l * ax[3 * j + 2]), &sn, &cs);
+        a += f * cs;
+        b += f * sn;
+      }
+      acc += (double)rr.mult * (a * a + b * b);
+      if (!jac) continue;
+      // d|F|^2/du = 2 (A dA/du + B dB/du), dA/du = -2 pi f (R^T h) sin, dB/du = 2 pi f (R^T h) cos
+      for (int j = 0; j < nAt; ++j) {
+        const double f = ftab[(size_t)r * P.nElem + atype[j]];
+        double sn, cs;
+        sincospi(2.0 * (h * ax[3 * j] + k * ax[3 * j + 1] + l * ax[3 * j + 2]), &sn, &cs);
+        const double w = (double)rr.mult * 2.0 * 2.0 * 3.14159265358979323846 * f * (b * cs - a * sn);
+        const int *Rm = ops[aop[j]].r;
+        const int base = 3 * asite[j];
+        grow[base] += w * (Rm[0] * h + Rm[3] * k + Rm[6] * l);
+        grow[base + 1] += w * (Rm[1] * h + Rm[4] * k + Rm[7] * l);
+        grow[base + 2] += w * (Rm[2] * h + Rm[5] * k + Rm[8] * l);
+      }
+    }
+    R.ical[(size_t)st * P.nGroups + gI] = acc;
+    if (jac) {
+      // into each site's Wyckoff subspace: P^T g
+      double *J = R.jac + ((size_t)st * P.nGroups + gI) * nP;
+      for (int si = 0; si < ms; ++si) {
+        const ProjFix &pf = P.proj[(size_t)A * ms + si];
+        const double inv = 1.0 / (double)pf.den;
+        const double g0 = grow[3 * si], g1 = grow[3 * si + 1], g2 = grow[3 * si + 2];
+        for (int c = 0; c < 3; ++c)
+          J[3 * si + c] = (pf.num[c] * g0 + pf.num[3 + c] * g1 + pf.num[6 + c] * g2) * inv;
+      }
+    }
+  }
+}
+
+// Scale, chi^2 and (with J) the normal equations of one structure per CTA.
+__global__ void __launch_bounds__(kRefineThreads) wy_refine_normal_kernel(const Params P, const RefineArgs R) {
+  __shared__ double red[3][kRefineThreads];
+  __shared__ double sScale;
+  const int st = blockIdx.x, nP = R.nP, nG = P.nGroups, tid = threadIdx.x;
+  const float4 *groups = reinterpret_cast<const float4 *>(P.blob + P.offGroup);
+  const double *ic = R.ical + (size_t)st * nG;
+  double *out = R.out + (size_t)st * (4 + nP + (size_t)nP * nP);
+  double num = 0, den = 0, oo = 0;
+  for (int g = tid; g < nG; g += blockDim.x) {
+    const float4 gm = groups[g];
+    const double w = gm.w > 0.f ? (double)gm.w : 0.0, io = gm.z;
+    num += w * io * ic[g];
+    den += w * ic[g] * ic[g];
+    oo += w * io * io;
+  }
+  red[0][tid] = num; red[1][tid] = den; red[2][tid] = oo;
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0, b = 0, c = 0;
+    for (int i = 0; i < blockDim.x; ++i) { a += red[0][i]; b += red[1][i]; c += red[2][i]; }
+    sScale = b > 0 ? a / b : 0.0;
+    out[0] = sScale;
+    out[2] = c;
+  }
+  __syncthreads();
+  const double sc = sScale;
+  double chi = 0;
+  for (int g = tid; g < nG; g += blockDim.x) {
+    const float4 gm = groups[g];
+    const double w = gm.w > 0.f ? (double)gm.w : 0.0, d = (double)gm.z - sc * ic[g];
+    chi += w * d * d;
+  }
+  __syncthreads();
+  red[0][tid] = chi;
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0;
+    for (int i = 0; i < blockDim.x; ++i) a += red[0][i];
+    out[1] = a;
+  }
+  if (!R.jac) return;
+  const double *J = R.jac + (size_t)st * nG * nP;
+  for (int p = tid; p < nP; p += blockDim.x) {
+    double t = 0;
+    for (int g = 0; g < nG; ++g) {
+      const float4 gm = groups[g];
+      const double w = gm.w > 0.f ? (double)gm.w : 0.0;
+      t += w * (sc * J[(size_t)g * nP + p]) * ((double)gm.z - sc * ic[g]);
+    }
+    out[4 + p] = t;
+  }
+  for (int pq = tid; pq < nP * nP; pq += blockDim.x) {
+    const int pp = pq / nP, qq = pq % nP;
+    if (qq < pp) continue;
+    double t = 0;
+    for (int g = 0; g < nG; ++g) {
+      const float4 gm = groups[g];
+      const double w = gm.w > 0.f ? (double)gm.w : 0.0;
+      t += w * (sc * J[(size_t)g * nP + pp]) * (sc * J[(size_t)g * nP + qq]);
+    }
+    out[4 + nP + (size_t)pp * nP + qq] = t;
+    out[4 + nP + (size_t)qq * nP + pp] = t;
+  }
+}
+
+}  // namespace wy
+}  // namespace p6
+
+namespace {
+// crSolve (js/coord_refine.js:629-662): Cholesky of the damped normal matrix; false if not positive definite.
+bool refine_solve(const std::vector<double> &A, const std::vector<double> &b, int n, std::vector<double> &x) {
+  std::vector<double> L((size_t)n * n, 0.0), y(n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = A[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+      if (i == j) {
+        if (!(s > 0)) return false;
+        L[(size_t)i * n + i] = std::sqrt(s);
+      } else {
+        L[(size_t)i * n + j] = s / L[(size_t)j * n + j];
+      }
+    }
+  for (int i = 0; i < n; ++i) {
+    double s = b[i];
+    for (int k = 0; k < i; ++k) s -= L[(size_t)i * n + k] * y[k];
+    y[i] = s / L[(size_t)i * n + i];
+  }
+  x.assign(n, 0.0);
+  for (int i = n - 1; i >= 0; --i) {
+    double s = y[i];
+    for (int k = i + 1; k < n; ++k) s -= L[(size_t)k * n + i] * x[k];
+    x[i] = s / L[(size_t)i * n + i];
+  }
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
+}
+}  // namespace
+
+extern "C" p6_status p6_wy_refine(p6_wy_session *s, int n, const uint32_t *assign, double *coords,
+                                  const p6_wy_refine_opts *opts, double *r_start, double *r_final, double *chi2,
+                                  int *iterations, int *converged) {
+  P6_ENTRY();
+  if (!s || n <= 0 || !assign || !coords) return set_error(P6_ERR_INVALID_ARG, "null argument or no structures");
+  p6_wy_refine_opts o{60, 1e-3, 10.0, 0.4, 1e8, 1e-6, 1e-9, 0.05};
+  if (opts) o = *opts;
+  if (o.max_iter < 0 || !(o.lambda0 > 0) || !(o.lambda_up > 1) || !(o.lambda_down > 0) ||
+      !(o.lambda_max > o.lambda0) || !(o.max_step > 0))
+    return set_error(P6_ERR_INVALID_ARG, "refinement options out of range");
+  Params &P = s->P;
+  const int ms = P.maxSites, nP = ms * 3, nG = P.nGroups;
+  for (int i = 0; i < n; ++i)
+    if ((int)assign[i] >= P.nAssign) return set_error(P6_ERR_INVALID_ARG, "assignment index out of range");
+  if (P.nTot > kRefineMaxAtoms) return set_error(P6_ERR_CAPACITY, "more than 1024 generated atoms for the refinement");
+  // free parameters (trace of each projector) against the weighted groups
+  int nObs = 0;
+  for (const float4 &g : s->groupsHost) nObs += g.w > 0.f ? 1 : 0;
+  for (int i = 0; i < n; ++i) {
+    int nFree = 0;
+    for (int si = 0; si < ms; ++si) {
+      const ProjFix &pf = s->projHost[(size_t)assign[i] * ms + si];
+      nFree += (int)std::lround((double)(pf.num[0] + pf.num[4] + pf.num[8]) / pf.den);
+    }
+    if (nObs <= nFree + 1)
+      return set_error(P6_ERR_INVALID_ARG, "the refinement is underdetermined: too few weighted groups for the free coordinates");
+  }
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t outStride = 4 + nP + (size_t)nP * nP;
+  uint32_t *dA = nullptr;
+  double *dX = nullptr, *dI = nullptr, *dJ = nullptr, *dOut = nullptr;
+  auto release = [&]() {
+    for (void *q : {(void *)dA, (void *)dX, (void *)dI, (void *)dJ, (void *)dOut})
+      if (q) cudaFree(q);
+  };
+  cudaError_t e = cudaMalloc(&dA, (size_t)n * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&dX, (size_t)n * nP * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dI, (size_t)n * nG * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dJ, (size_t)n * nG * nP * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dOut, (size_t)n * outStride * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dA, assign, (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) { release(); return cuda_error(e, "refinement buffers"); }
+
+  // projection onto each site's Wyckoff subspace, x mod 1 (js/coord_refine.js:311-327)
+  auto project = [&](int i, double *x) {
+    for (int si = 0; si < ms; ++si) {
+      const ProjFix &pf = s->projHost[(size_t)assign[i] * ms + si];
+      double v[3];
+      for (int c = 0; c < 3; ++c) {
+        v[c] = (pf.num[3 * c] * x[3 * si] + pf.num[3 * c + 1] * x[3 * si + 1] + pf.num[3 * c + 2] * x[3 * si + 2]) /
+                   (double)pf.den +
+               (double)pf.t[c] * (1.0 / 4294967296.0);
+        v[c] -= std::floor(v[c]);
+      }
+      for (int c = 0; c < 3; ++c) x[3 * si + c] = v[c];
+    }
+  };
+  std::vector<double> outH((size_t)n * outStride);
+  auto evaluate = [&](const std::vector<double> &x, bool jac) -> cudaError_t {
+    cudaError_t err = cudaMemcpyAsync(dX, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    if (err != cudaSuccess) return err;
+    RefineArgs a{nP, dA, dX, dI, jac ? dJ : nullptr, dOut};
+    wy_refine_eval_kernel<<<n, kRefineThreads, 0, s->stream>>>(P, a);
+    wy_refine_normal_kernel<<<n, kRefineThreads, 0, s->stream>>>(P, a);
+    s->launches += 2;
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    const size_t cnt = jac ? (size_t)n * outStride : (size_t)n * outStride;
+    err = cudaMemcpyAsync(outH.data(), dOut, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (err != cudaSuccess) return err;
+    return cudaStreamSynchronize(s->stream);
+  };
+  std::vector<double> cur(coords, coords + (size_t)n * nP), start;
+  for (int i = 0; i < n; ++i) project(i, cur.data() + (size_t)i * nP);
+  start = cur;
+  if ((e = evaluate(cur, false)) != cudaSuccess) { release(); return cuda_error(e, "refinement evaluation"); }
+  std::vector<double> scale(n), chi(n), oo(n), lambda(n, o.lambda0);
+  std::vector<int> steps(n, 0), conv(n, 0), done(n, 0);
+  for (int i = 0; i < n; ++i) {
+    scale[i] = outH[(size_t)i * outStride];
+    chi[i] = outH[(size_t)i * outStride + 1];
+    oo[i] = outH[(size_t)i * outStride + 2];
+    if (r_start) r_start[i] = oo[i] > 0 ? std::sqrt(chi[i] / oo[i]) : NAN;
+  }
+  std::vector<double> JTJ((size_t)n * nP * nP), JTr((size_t)n * nP), trial(cur);
+  for (int iter = 0; iter < o.max_iter; ++iter) {
+    bool any = false;
+    for (int i = 0; i < n; ++i) any |= !done[i];
+    if (!any) break;
+    if ((e = evaluate(cur, true)) != cudaSuccess) { release(); return cuda_error(e, "refinement normal equations"); }
+    std::vector<int> searching(n, 0), stepped(n, 0);
+    for (int i = 0; i < n; ++i) {
+      if (done[i]) continue;
+      const double *oh = outH.data() + (size_t)i * outStride;
+      scale[i] = oh[0];
+      chi[i] = oh[1];
+      std::copy(oh + 4, oh + 4 + nP, JTr.begin() + (size_t)i * nP);
+      std::copy(oh + 4 + nP, oh + 4 + nP + (size_t)nP * nP, JTJ.begin() + (size_t)i * nP * nP);
+      searching[i] = 1;
+    }
+    for (;;) {
+      std::vector<int> hasTrial(n, 0);
+      bool anySearch = false, anyTrial = false;
+      for (int i = 0; i < n; ++i) {
+        if (!searching[i]) continue;
+        if (!(lambda[i] < o.lambda_max)) { searching[i] = 0; continue; }
+        anySearch = true;
+        std::vector<double> aug(JTJ.begin() + (size_t)i * nP * nP, JTJ.begin() + (size_t)(i + 1) * nP * nP);
+        double dmax = 0;
+        for (int q = 0; q < nP; ++q) dmax = std::max(dmax, aug[(size_t)q * nP + q]);
+        if (!(dmax > 0)) { conv[i] = 1; searching[i] = 0; continue; }
+        for (int q = 0; q < nP; ++q) aug[(size_t)q * nP + q] += lambda[i] * std::max(aug[(size_t)q * nP + q], 1e-6 * dmax);
+        std::vector<double> rhs(JTr.begin() + (size_t)i * nP, JTr.begin() + (size_t)(i + 1) * nP), dx;
+        if (!refine_solve(aug, rhs, nP, dx)) { lambda[i] *= o.lambda_up; continue; }
+        // back from the constrained space: the position moves by P du
+        for (int si = 0; si < ms; ++si) {
+          const ProjFix &pf = s->projHost[(size_t)assign[i] * ms + si];
+          const double d0 = dx[3 * si], d1 = dx[3 * si + 1], d2 = dx[3 * si + 2];
+          for (int c = 0; c < 3; ++c)
+            dx[3 * si + c] = (pf.num[3 * c] * d0 + pf.num[3 * c + 1] * d1 + pf.num[3 * c + 2] * d2) / (double)pf.den;
+        }
+        double big = 0;
+        for (int q = 0; q < nP; ++q) big = std::max(big, std::fabs(dx[q]));
+        const double cap = big > o.max_step ? o.max_step / big : 1.0;
+        double *t = trial.data() + (size_t)i * nP;
+        const double *c0 = cur.data() + (size_t)i * nP;
+        for (int q = 0; q < nP; ++q) t[q] = c0[q] + cap * dx[q];
+        project(i, t);
+        hasTrial[i] = 1;
+        anyTrial = true;
+      }
+      if (!anySearch) break;
+      if (!anyTrial) continue;
+      for (int i = 0; i < n; ++i)
+        if (!hasTrial[i]) std::copy(cur.begin() + (size_t)i * nP, cur.begin() + (size_t)(i + 1) * nP, trial.begin() + (size_t)i * nP);
+      if ((e = evaluate(trial, false)) != cudaSuccess) { release(); return cuda_error(e, "refinement trial"); }
+      for (int i = 0; i < n; ++i) {
+        if (!hasTrial[i]) continue;
+        const double sTr = outH[(size_t)i * outStride], chiTr = outH[(size_t)i * outStride + 1];
+        if (chiTr < chi[i]) {
+          double moved = 0;
+          for (int q = 0; q < nP; ++q)
+            moved = std::max(moved, std::fabs(trial[(size_t)i * nP + q] - cur[(size_t)i * nP + q]));
+          const double rel = (chi[i] - chiTr) / std::max(chi[i], 1e-300);
+          std::copy(trial.begin() + (size_t)i * nP, trial.begin() + (size_t)(i + 1) * nP, cur.begin() + (size_t)i * nP);
+          scale[i] = sTr;
+          chi[i] = chiTr;
+          lambda[i] = std::max(lambda[i] * o.lambda_down, 1e-12);
+          stepped[i] = 1;
+          steps[i]++;
+          if (moved < o.tol_step || rel < o.tol_chi) conv[i] = 1;
+          searching[i] = 0;
+        } else {
+          lambda[i] *= o.lambda_up;
+        }
+      }
+    }
+    for (int i = 0; i < n; ++i)
+      if (!done[i] && (conv[i] || !stepped[i])) done[i] = 1;
+  }
+  if ((e = evaluate(cur, false)) != cudaSuccess) { release(); return cuda_error(e, "refinement evaluation"); }
+  for (int i = 0; i < n; ++i) {
+    const double c = outH[(size_t)i * outStride + 1], w = outH[(size_t)i * outStride + 2];
+    if (r_final) r_final[i] = w > 0 ? std::sqrt(c / w) : NAN;
+    if (chi2) chi2[i] = c;
+    if (iterations) iterations[i] = steps[i];
+    if (converged) converged[i] = conv[i];
+  }
+  std::copy(cur.begin(), cur.end(), coords);
+  release();
+  return P6_OK;
+}

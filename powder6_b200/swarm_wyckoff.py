@@ -489,6 +489,7 @@ class SearchResult:
     per_assignment: Dict[int, float] = field(default_factory=dict)   # best cc of each assignment
     bests: Dict[int, dict] = field(default_factory=dict)             # {cc, pen, coords} of each assignment
     screened: Dict[int, float] = field(default_factory=dict)         # screening score (cc - raw pen), if screened
+    refined: Dict[int, dict] = field(default_factory=dict)           # {coords, r_start, r, converged} per assignment
 
 
 def quench_schedule(settings: Optional[dict] = None) -> np.ndarray:
@@ -553,7 +554,7 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                        on_progress: Optional[Callable[[dict], None]] = None,
                        should_stop: Optional[Callable[[], bool]] = None, do_quench: bool = True,
                        target_cc: Optional[float] = None, assignment_ids: Optional[Sequence[int]] = None,
-                       prune: bool = True) -> SearchResult:
+                       prune: bool = True, refine: bool = False) -> SearchResult:
     """One wave of assignments (``assignment_ids``, default all of the
     problem's), ``restarts`` independent restarts, all generations on the
     device, then the quench of the per-assignment bests.  Particles are shared
@@ -565,7 +566,10 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     winner is re-scored at full resolution and the final penalty weight and
     cross-checked on the CPU, as the reference reports.  With ``target_cc``,
     ``time_to_target`` is the wall time from the start to the first chunk
-    boundary (or the end of the quench) at which the best cc reached it."""
+    boundary (or the end of the quench) at which the best cc reached it.
+    With ``refine``, the best structure of every assignment is then refined
+    by least squares against the grouped |F|^2 (``refine_coordinates``) and
+    the result carries the refined coordinates and wR(F^2) in ``refined``."""
     import time
     t_start = time.perf_counter()
     d = dict(SW_DEFAULTS)
@@ -703,6 +707,15 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     if best['coords'] is not None:
         cpu = cpu_cross_check(problem, best['coords'], best['A'])
         res.cpu_check = {'gpu': best['cc'], 'cpu': cpu, 'delta': abs(best['cc'] - cpu)}
+    if refine and per_a:
+        for A in sorted(A for A, v in per_a.items() if v.get('coords') is not None):
+            try:
+                ref = refine_coordinates(sess, np.asarray(per_a[A]['coords'], dtype=np.float64)[None, :], [A])
+            except _lib.P6Error as e:        # e.g. more free coordinates than weighted groups
+                res.refined[A] = {'error': str(e)}
+                continue
+            res.refined[A] = {'coords': ref['coords'][0], 'r_start': float(ref['r_start'][0]),
+                              'r': float(ref['r'][0]), 'converged': bool(ref['converged'][0])}
     if own:
         sess.close()
     return res
@@ -739,6 +752,36 @@ def rescore_full_resolution(problem: WyckoffProblem, sess: WyckoffSession, bests
     _, _, st = sess.read_state()
     return {A: {'cc': float(st['cc'][i]), 'pen': float(st['pen'][i]), 'coords': bests[A]['coords']}
             for i, A in enumerate(live) if np.isfinite(st['cc'][i])}
+
+
+class P6WyRefineOpts(C.Structure):
+    _fields_ = [('max_iter', C.c_int), ('lambda0', C.c_double), ('lambda_up', C.c_double),
+                ('lambda_down', C.c_double), ('lambda_max', C.c_double), ('tol_step', C.c_double),
+                ('tol_chi', C.c_double), ('max_step', C.c_double)]
+
+
+REFINE_DEFAULTS = dict(max_iter=60, lambda0=1e-3, lambda_up=10.0, lambda_down=0.4, lambda_max=1e8, tol_step=1e-6,
+                       tol_chi=1e-9, max_step=0.05)
+
+
+def refine_coordinates(sess: WyckoffSession, coords: np.ndarray, assign: Sequence[int],
+                       **opts) -> Dict[str, np.ndarray]:
+    """refineCoordinatesAgainstWppf (js/coord_refine.js:266-627) on the device for
+    a batch of structures: ``coords`` (n x max_sites*3, fractional) against the
+    session's grouped |F|^2, each with its assignment.  Returns the refined
+    coordinates, the weighted wR(F^2) before and after, chi^2, accepted steps
+    and convergence per structure."""
+    o = dict(REFINE_DEFAULTS)
+    o.update(opts)
+    x = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(len(assign), -1)).copy()
+    a = np.ascontiguousarray(assign, dtype=np.uint32)
+    n = len(a)
+    r0, r1, chi = np.zeros(n), np.zeros(n), np.zeros(n)
+    it, cv = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+    ro = P6WyRefineOpts(**o)
+    check(sess.lib.p6_wy_refine(sess.h, n, ptr(a), ptr(x), C.cast(C.pointer(ro), C.c_void_p), ptr(r0), ptr(r1),
+                                ptr(chi), ptr(it), ptr(cv)))
+    return {'coords': x, 'r_start': r0, 'r': r1, 'chi2': chi, 'iterations': it, 'converged': cv.astype(bool)}
 
 
 def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,

@@ -772,3 +772,38 @@ def test_ladders_on_two_cta_clusters_are_bit_identical(prob):
     assert outs[0][2] == outs[1][2]
     st = np.frombuffer(outs[1][2], dtype=STATE_DTYPE)
     assert np.max(st['best_cc']) > 0.5
+
+
+def test_coordinate_refinement_matches_the_restatement(oracle):
+    """Three perturbed PbSO4 structures refined together on the device (FP64
+    intensities, analytic constrained Jacobian, normal equations; damping on
+    the host) reach the FP64 restatement's coordinates within 1e-9 and its wR
+    within 1e-10 relative, with the same convergence and accepted steps."""
+    from powder6_b200.swarm_wyckoff import refine_coordinates
+    P = wyckoff_problem(seed=1)
+    x_true = P.true_coords.copy()
+    starts = [x_true + np.random.default_rng(s).uniform(-0.003, 0.003, x_true.shape) for s in (3, 4, 5)]
+    with WyckoffSession(P, 64) as s:
+        out = refine_coordinates(s, np.stack(starts), [0, 0, 0])
+    for i, x0 in enumerate(starts):
+        xr, r0, r1, chi, steps, conv = oracle.wy_refine(P, 0, x0)
+        d = out['coords'][i] - xr
+        d -= np.round(d)
+        print(f'structure {i}: max |dx| {float(np.max(np.abs(d))):.2e}, r {out["r"][i]:.10f} vs {r1:.10f}, '
+              f'steps {out["iterations"][i]} vs {steps}')
+        assert np.max(np.abs(d)) < 1e-9, (i, float(np.max(np.abs(d))))
+        assert abs(out['r_start'][i] - r0) <= 1e-10 * r0
+        assert abs(out['r'][i] - r1) <= 1e-10 * r1, (out['r'][i], r1)
+        assert int(out['iterations'][i]) == steps and bool(out['converged'][i]) == conv
+        assert out['r'][i] < 0.02
+
+
+def test_search_then_refinement(prob):
+    """A short search followed by the least-squares refinement of its best
+    structure: the refined wR(F^2) is at most the search's and reaches the
+    true structure's."""
+    from powder6_b200.swarm_wyckoff import run_wyckoff_search
+    res = run_wyckoff_search(prob, num_particles=2048, generations=2000, seed=21, refine=True)
+    ref = res.refined[0]
+    assert ref['converged'] and ref['r'] <= ref['r_start'] + 1e-12
+    assert ref['r'] < 0.02
