@@ -54,8 +54,15 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if verbose:
         flags.insert(0, '-Xptxas=-v')
 
+    headers = [q for q in list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h')) + [ROOT / 'include' / 'p6cuda.h']
+               if q.is_file()]
+    newest_header = max((q.stat().st_mtime for q in headers), default=0.0)
+
     def compile_one(src: Path):
         obj = obj_dir / (src.stem + '.o')
+        if (not force and not verbose and obj.exists() and obj.stat().st_mtime > src.stat().st_mtime
+                and obj.stat().st_mtime > newest_header):
+            return src, obj, subprocess.CompletedProcess([], 0, '', '')   # object up to date
         return src, obj, subprocess.run([nvcc, *flags, '-c', str(src), '-o', str(obj)], capture_output=True, text=True)
 
     srcs = sorted(sources(), key=lambda q: -q.stat().st_size)   # the largest first

@@ -41,7 +41,7 @@
 namespace p6 {
 namespace pt {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 1024;   // one CTA per chain: 32 warps hide the latency of the evaluation
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxNv = 32;
 constexpr int kMaxFull = 64;
