@@ -52,11 +52,13 @@ def parse():
     ap.add_argument('--generations', type=int, default=GENERATIONS)
     ap.add_argument('--cos-mode', type=int, default=0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--workload', default='wyckoff', choices=['wyckoff', 'pt', 'contract', 'batch', 'learned'],
+    ap.add_argument('--workload', default='wyckoff',
+                    choices=['wyckoff', 'pt', 'contract', 'batch', 'learned', 'refine'],
                     help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit; '
                          'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000); '
                          'batch: 64 uneven Wyckoff searches in one persistent launch; '
-                         'learned: the learned-proposal search (P2_1/c, 17 sites, 8192 replicas)')
+                         'learned: the learned-proposal search (P2_1/c, 17 sites, 8192 replicas); '
+                         'refine: least-squares refinement of 512 perturbed PbSO4 structures')
     ap.add_argument('--method', default='split', choices=['split', 'fp32'],
                     help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
     ap.add_argument('--chains', type=int, default=64)
@@ -639,6 +641,127 @@ def main_batch(args, world, rank, local):
 LEARNED_GENERATIONS = 1000
 
 
+REFINE_STRUCTURES = 512
+REFINE_WORKLOAD = ('Wyckoff-constrained least-squares refinement (coord_refine) of 512 PbSO4-like Pnma structures '
+                   '(true coordinates + U(-0.003, 0.003) on every coordinate, seeded), 87 groups of 112 '
+                   'reflections, to convergence (at most 60 iterations)')
+
+
+def refine_starts(P, n, seed):
+    rng = np.random.default_rng(seed)
+    return np.stack([P.true_coords + rng.uniform(-0.003, 0.003, P.true_coords.shape) for _ in range(n)])
+
+
+def main_refine(args, world, rank, local):
+    """One step = the refinement of REFINE_STRUCTURES perturbed structures to
+    convergence in one p6_wy_refine call (FP64 group intensities, analytic
+    constrained Jacobians and normal equations on the device, the damping
+    control of all structures in lock step on the host).  value: structures
+    per second, wall time of the C call (it takes and returns host arrays by
+    design: the damping control runs on the host); e2e: the same through the
+    Python wrapper (array packing included); cpu_baseline: the FP64
+    restatement of the algorithm on one host thread, on a sample."""
+    import ctypes as C
+    import torch
+    from powder6_b200 import _lib
+    from powder6_b200.swarm_wyckoff import (P6WyRefineOpts, REFINE_DEFAULTS, WyckoffSession, refine_coordinates)
+    from powder6_b200.workloads import wyckoff_problem
+    torch.cuda.set_device(local)
+    P = wyckoff_problem(seed=1)
+    n = REFINE_STRUCTURES
+    steps_in = [refine_starts(P, n, 100 + 10 * rank + i) for i in range(args.warmup + args.steps)]
+    assign = np.zeros(n, dtype=np.uint32)
+    walls, e2e, iters, rs, conv = [], [], [], [], []
+    with WyckoffSession(P, 64, device=local) as s:
+        ro = P6WyRefineOpts(**REFINE_DEFAULTS)
+        l0 = 0
+        with ClockSampler(local) as clk:
+            for i, x0 in enumerate(steps_in):
+                x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+                r1 = np.zeros(n)
+                it = np.zeros(n, dtype=np.int32)
+                cv = np.zeros(n, dtype=np.int32)
+                if i == args.warmup:
+                    l0 = s.launch_count()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                _lib.check(s.lib.p6_wy_refine(s.h, n, _lib.ptr(assign), _lib.ptr(x), C.cast(C.pointer(ro), C.c_void_p),
+                                              None, _lib.ptr(r1), None, _lib.ptr(it), _lib.ptr(cv)))
+                dt = time.perf_counter() - t0
+                if i >= args.warmup:
+                    walls.append(dt)
+                    iters.append(float(np.mean(it)))
+                    rs.append(float(np.median(r1)))
+                    conv.append(int(cv.sum()))
+        launches = s.launch_count() - l0
+        for i in range(args.steps):
+            t0 = time.perf_counter()
+            refine_coordinates(s, steps_in[args.warmup + i], assign)
+            e2e.append(time.perf_counter() - t0)
+    total = max_over_ranks(float(sum(walls)), world)
+    value = world * n * args.steps / total
+    e2e_value = world * n * args.steps / max_over_ranks(float(sum(e2e)), world)
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            'metric': 'structures refined/s', 'value': value, 'unit': 'structures/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000.0 * total / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': REFINE_WORKLOAD, 'structures': n, 'mean_accepted_steps': float(np.mean(iters)),
+                       'median_final_wr': float(np.median(rs)), 'converged_per_step': conv,
+                       'step': f'one p6_wy_refine call on {n} structures',
+                       'parallelism': f'structures only x{world}'},
+            'e2e': {'value': e2e_value, 'unit': 'structures/s', 'h2d_bytes_per_step': n * P.max_sites * 3 * 8 + n * 4,
+                    'd2h_bytes_per_step': n * P.max_sites * 3 * 8 + n * 24},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import oracle as O
+            sample = refine_starts(P, 64, 7)
+            t0 = time.perf_counter()
+            done = 0
+            for x0 in sample:
+                O.wy_refine(P, 0, x0)
+                done += 1
+                if time.perf_counter() - t0 > 10.0:
+                    break
+            dt = time.perf_counter() - t0
+            line['cpu_baseline'] = {'value': done / dt, 'unit': 'structures/s', 'cores': 1, 'kind': 'port',
+                                    'sample': f'{done} structures refined by the FP64 restatement (numpy, one host '
+                                              f'thread), {dt:.1f} s'}
+        print(json.dumps(line), flush=True)
+
+
+def run_reference_refine(args, world, rank):
+    """The reference arm of the refinement workload: the FP64 restatement of
+    refineCoordinatesAgainstWppf on one host thread; each step refines a
+    bounded sample of the workload's structures."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from powder6_b200.workloads import wyckoff_problem
+    P = wyckoff_problem(seed=1)
+    per_step = 4
+    times = []
+    for i in range(args.warmup + args.steps):
+        sample = refine_starts(P, per_step, 100 + i)
+        t0 = time.perf_counter()
+        for x0 in sample:
+            O.wy_refine(P, 0, x0)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    v = per_step * args.steps / sum(times)
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'structures refined/s', 'value': v, 'unit': 'structures/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000.0 * sum(times) / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': REFINE_WORKLOAD, 'sample': f'{per_step} structures per step'},
+        'cpu_baseline': {'value': v, 'unit': 'structures/s', 'cores': 1, 'kind': 'port',
+                         'sample': f'{per_step} structures per step, FP64 restatement (numpy), one host thread'},
+        'e2e': {'value': v, 'unit': 'structures/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}), flush=True)
+
+
 def main_learned(args, world, rank, local):
     """One step = one learned-proposal search (P2_1/c, 17 independent C/N/S
     sites, 575 reflections, 8192 replicas, LEARNED_GENERATIONS generations; 8
@@ -751,11 +874,14 @@ def main():
             run_reference_ct(args, world, rank)
         elif args.workload == 'batch':
             run_reference_batch(args, world, rank)
+        elif args.workload == 'refine':
+            run_reference_refine(args, world, rank)
         else:
             run_reference(args, world, rank)
         return
-    if args.workload in ('pt', 'contract', 'batch', 'learned'):
-        {'pt': main_pt, 'contract': main_ct, 'batch': main_batch, 'learned': main_learned}[args.workload](
+    if args.workload in ('pt', 'contract', 'batch', 'learned', 'refine'):
+        {'pt': main_pt, 'contract': main_ct, 'batch': main_batch, 'learned': main_learned,
+         'refine': main_refine}[args.workload](
             args, world, rank, local)
         if world > 1:
             import torch.distributed as dist

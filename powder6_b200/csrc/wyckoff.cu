@@ -3313,8 +3313,11 @@ extern "C" p6_status p6_wy_refine(p6_wy_session *s, int n, const uint32_t *assig
     s->launches += 2;
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
-    const size_t cnt = jac ? (size_t)n * outStride : (size_t)n * outStride;
-    err = cudaMemcpyAsync(outH.data(), dOut, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    // with J, everything; without, only scale, chi^2 and sum w Io^2 of each structure
+    err = jac ? cudaMemcpyAsync(outH.data(), dOut, (size_t)n * outStride * sizeof(double), cudaMemcpyDeviceToHost,
+                                s->stream)
+              : cudaMemcpy2DAsync(outH.data(), outStride * sizeof(double), dOut, outStride * sizeof(double),
+                                  4 * sizeof(double), (size_t)n, cudaMemcpyDeviceToHost, s->stream);
     if (err != cudaSuccess) return err;
     return cudaStreamSynchronize(s->stream);
   };
