@@ -283,6 +283,12 @@ typedef struct {
    * entries after the background (and after r when has_po); each peak gets
    * asym = SL / tan(theta) + HL, a doubled window and the area correction. */
   int has_asym;
+  /* Fit method (js/pt_gpu.js:259-297): 0 Rietveld (heights from the
+   * structure); 1 WPPF / Le Bail: every reflection's height is free and
+   * non-negative, solved in every evaluation by NNLS against the observed
+   * pattern minus the background (atoms unused, n_atoms may be 0; at most 64
+   * envelope reflections). */
+  int method;
 } p6_pt_problem;
 
 typedef struct p6_pt_session p6_pt_session;

@@ -70,6 +70,10 @@ typedef struct {
     double poDir[3];
     /* SL/HL asymmetry: SL = v[PT_BKG0 + nBkg + hasPo], HL the next entry */
     int hasAsym;
+    /* 0 Rietveld; 1 WPPF / Le Bail (js/pt_gpu.js:259-297): every active
+     * reflection's height is free and non-negative, solved by NNLS against
+     * y - background (atoms unused) */
+    int method;
 } p6o_pt_problem;
 
 static const double GCONV = 0.023548200450309493;   /* sqrt(8 ln 2) / 100 */
@@ -331,6 +335,83 @@ double p6o_po_factor(const p6o_pt_problem *P, const double *c6, double r, int h,
  * chi^2 of the full parameter vector v.  ycalc (may be NULL) receives the
  * calculated pattern; nRefl (may be NULL) the reflection count used.
  */
+int p6o_solve_spd(const double *A, const double *b, int n, double *x);
+
+/* Lawson-Hanson active-set NNLS on the normal equations: minimise
+ * 1/2 x^T H x - rhs^T x subject to x >= 0 (H symmetric positive semi-definite,
+ * m x m, row-major).  It is the exact solution the free-intensity fit of
+ * js/pt_gpu.js:259-297 (coordinate descent, then an active-set polish)
+ * converges to.  Returns the number of outer iterations, -1 if a passive
+ * block could not be factored. */
+int p6o_nnls_normal(const double *H, const double *rhs, int m, double *x)
+{
+    int *passive = calloc(m + 1, sizeof(int)), *blocked = calloc(m + 1, sizeof(int)), *idx = malloc(sizeof(int) * (m + 1));
+    double *z = malloc(sizeof(double) * (m + 1)), *Hp = malloc(sizeof(double) * (m * m + 1)),
+           *bp = malloc(sizeof(double) * (m + 1)), *zp = malloc(sizeof(double) * (m + 1));
+    double mag = 1.0;
+    for (int j = 0; j < m; j++) { x[j] = 0.0; mag = fmax(mag, fabs(rhs[j])); }
+    const double tol = 1e-12 * mag;
+    int outer = 0, status = 0;
+    for (; outer < 3 * m + 10; outer++) {
+        int enter = -1;
+        double best = tol;
+        for (int j = 0; j < m; j++) {
+            double g = rhs[j];
+            for (int k = 0; k < m; k++) g -= H[j * m + k] * x[k];
+            if (!passive[j] && !blocked[j] && g > best) { best = g; enter = j; }
+        }
+        if (enter < 0) break;
+        passive[enter] = 1;
+        for (int inner = 0; inner < 3 * m + 10; inner++) {
+            int np = 0;
+            for (int j = 0; j < m; j++)
+                if (passive[j]) idx[np++] = j;
+            for (int a = 0; a < np; a++) {
+                bp[a] = rhs[idx[a]];
+                for (int b = 0; b < np; b++) Hp[a * np + b] = H[idx[a] * m + idx[b]];
+            }
+            if (!p6o_solve_spd(Hp, bp, np, zp)) { status = -1; break; }
+            for (int j = 0; j < m; j++) z[j] = 0.0;
+            int allpos = 1;
+            for (int a = 0; a < np; a++) { z[idx[a]] = zp[a]; if (!(zp[a] > 0)) allpos = 0; }
+            if (allpos) { for (int j = 0; j < m; j++) x[j] = z[j]; break; }
+            double alpha = INFINITY;
+            int hit = -1;
+            for (int a = 0; a < np; a++) {
+                const int j = idx[a];
+                if (z[j] <= 0) {
+                    const double t = x[j] / (x[j] - z[j]);
+                    if (t < alpha) { alpha = t; hit = j; }
+                }
+            }
+            for (int a = 0; a < np; a++) { const int j = idx[a]; x[j] += alpha * (z[j] - x[j]); }
+            x[hit] = 0.0;
+            for (int a = 0; a < np; a++) { const int j = idx[a]; if (x[j] <= 0) { x[j] = 0.0; passive[j] = 0; } }
+        }
+        if (status < 0) break;
+        /* an entering column that could not stay positive is not offered again until x moves */
+        if (!passive[enter]) blocked[enter] = 1;
+        else for (int j = 0; j < m; j++) blocked[j] = 0;
+    }
+    free(passive); free(blocked); free(idx); free(z); free(Hp); free(bp); free(zp);
+    return status < 0 ? -1 : outer;
+}
+
+static double chebyshev_background(const p6o_pt_problem *P, const double *v, int i)
+{
+    const int n = P->n;
+    double lo = P->tth[0], hi = P->tth[n - 1];
+    double x = hi > lo ? 2 * (P->tth[i] - lo) / (hi - lo) - 1 : 0;
+    double Tm2 = 1, Tm1 = x, bk = 0;
+    for (int kk = 0; kk < P->nBkg; kk++) {
+        double T = kk == 0 ? 1 : kk == 1 ? x : 2 * x * Tm1 - Tm2;
+        if (kk >= 2) { Tm2 = Tm1; Tm1 = T; }
+        double b = v[PT_BKG0 + kk];
+        if (b) bk += b * T;
+    }
+    return bk;
+}
+
 double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int *nReflOut)
 {
     const int n = P->n;
@@ -433,6 +514,15 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
     /* heights and the pattern (evalPhase + render): column = Ka1 + w2 Ka2 */
     double *y = calloc(n, sizeof(double));
     double *col = malloc(sizeof(double) * n);
+    /* WPPF / Le Bail: the columns are kept, with their windows, for the NNLS */
+    int nFree = 0, capFree = 0;
+    double *fcol = NULL;
+    int *fwin = NULL;
+    if (P->method == 1) {
+        for (int r = 0; r < nr; r++) capFree += (has1[r] || has2[r]) ? 1 : 0;
+        fcol = calloc((size_t)(capFree + 1) * n, sizeof(double));
+        fwin = malloc(sizeof(int) * 2 * (capFree + 1));
+    }
     for (int r = 0; r < nr; r++) {
         if (!has1[r] && !has2[r]) continue;
         if (!isfinite(tthR[r])) continue;
@@ -453,21 +543,59 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
         if (has2[r])
             for (int i = st1[4 * r + 2]; i < st1[4 * r + 3]; i++)
                 col[i] += w2[r] * eval_voigt(P->tth[i], &p2[r], p2[r].maxd, p2[r].pedestal);
+        if (P->method == 1) {
+            for (int i = s0; i < s1; i++) fcol[(size_t)nFree * n + i] = col[i];
+            fwin[2 * nFree] = s0;
+            fwin[2 * nFree + 1] = s1;
+            nFree++;
+            continue;
+        }
         if (!height) continue;
         for (int i = s0; i < s1; i++) y[i] += height * col[i];
     }
-    /* background (Chebyshev over the fitted range) and chi^2 */
-    double lo = P->tth[0], hi = P->tth[n - 1], chi2 = 0;
-    for (int i = 0; i < n; i++) {
-        double x = hi > lo ? 2 * (P->tth[i] - lo) / (hi - lo) - 1 : 0;
-        double Tm2 = 1, Tm1 = x, bk = 0;
-        for (int kk = 0; kk < P->nBkg; kk++) {
-            double T = kk == 0 ? 1 : kk == 1 ? x : 2 * x * Tm1 - Tm2;
-            if (kk >= 2) { Tm2 = Tm1; Tm1 = T; }
-            double b = v[PT_BKG0 + kk];
-            if (b) bk += b * T;
+    if (P->method == 1 && nFree > 0) {
+        /* scaled normal equations: s_j = |W^1/2 c_j|, H = (C S^-1)^T W (C S^-1), rhs = (C S^-1)^T W (y - bkg) */
+        double *sc = calloc(nFree, sizeof(double)), *rhs = calloc(nFree, sizeof(double)),
+               *H = calloc((size_t)nFree * nFree, sizeof(double)), *x = calloc(nFree, sizeof(double));
+        for (int j = 0; j < nFree; j++) {
+            double a = 0, b = 0;
+            for (int i = fwin[2 * j]; i < fwin[2 * j + 1]; i++) {
+                if (!(P->w[i] > 0)) continue;
+                const double c = fcol[(size_t)j * n + i];
+                a += P->w[i] * c * c;
+                b += P->w[i] * c * (P->y[i] - chebyshev_background(P, v, i));
+            }
+            sc[j] = sqrt(fmax(0.0, a));
+            rhs[j] = sc[j] > 0 ? b / sc[j] : 0.0;
         }
-        double yc = bk + y[i];
+        for (int j = 0; j < nFree; j++)
+            for (int k = j; k < nFree; k++) {
+                double h = 0;
+                if (sc[j] > 0 && sc[k] > 0) {
+                    const int lo = fwin[2 * j] > fwin[2 * k] ? fwin[2 * j] : fwin[2 * k];
+                    const int hi = fwin[2 * j + 1] < fwin[2 * k + 1] ? fwin[2 * j + 1] : fwin[2 * k + 1];
+                    for (int i = lo; i < hi; i++)
+                        if (P->w[i] > 0) h += P->w[i] * fcol[(size_t)j * n + i] * fcol[(size_t)k * n + i];
+                    h /= sc[j] * sc[k];
+                }
+                H[j * nFree + k] = H[k * nFree + j] = h;
+            }
+        /* a column with no weighted points stays at zero height */
+        for (int j = 0; j < nFree; j++)
+            if (!(sc[j] > 0)) H[j * nFree + j] = 1.0;
+        p6o_nnls_normal(H, rhs, nFree, x);
+        for (int j = 0; j < nFree; j++) {
+            const double height = sc[j] > 0 ? x[j] / sc[j] : 0.0;
+            if (!height) continue;
+            for (int i = fwin[2 * j]; i < fwin[2 * j + 1]; i++) y[i] += height * fcol[(size_t)j * n + i];
+        }
+        free(sc); free(rhs); free(H); free(x);
+    }
+    free(fcol); free(fwin);
+    /* background (Chebyshev over the fitted range) and chi^2 */
+    double chi2 = 0;
+    for (int i = 0; i < n; i++) {
+        double yc = chebyshev_background(P, v, i) + y[i];
         if (ycalc) ycalc[i] = yc;
         if (!(P->w[i] > 0)) continue;
         double res = P->y[i] - yc;

@@ -97,6 +97,7 @@ struct Params {
   int *errFlag;
   int hasPo;             // March-Dollase factor on; r = v[PBKG0 + nBkg]
   int asymIdx;           // full index of SL (HL follows); -1: no asymmetry
+  int method;            // 0 Rietveld; 1 WPPF / Le Bail: heights free, solved per evaluation by NNLS
   const int *eqStart;    // nRefl + 1
   const int *eqHkl;      // 3 per equivalent
   double poDir[3];       // reciprocal-lattice direction
@@ -439,8 +440,220 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
   }
 }
 
+// ---------------------------------------------------------------------------
+// WPPF / Le Bail intensities (js/pt_gpu.js:259-297): every reflection's height
+// is free and non-negative, solved per evaluation by NNLS against the
+// observed pattern minus the background.  Column k is reflection k's unit
+// height profile (K-alpha-1 plus the weighted K-alpha-2), scaled to unit
+// weighted norm s_k; H = C'WC and rhs = C'W(y - bkg) in that scaling.  The
+// solve follows the reference: eight rounds of {eight cycles of projected
+// coordinate descent, then the KKT error; an active-set polish with a
+// Cholesky factor of the passive block}, converged when the KKT error is at
+// most 1e-5 of max(1, |rhs|).  Heights h_k = x_k / s_k.  Scratch: 2 m^2 + 8 m
+// doubles of shared memory.  Whole-CTA; the solve itself runs on warp 0.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int nnls_bytes(int m) { return (2 * m * m + 8 * m) * 8; }
+constexpr int kMaxFreeRefl = 64;
+
+template <class PK, class HT>
+__device__ __forceinline__ double free_column(const PK *pk1, const PK *pk2, const HT *w2, const int *act, int k,
+                                              int i, double t) {
+  double c = 0;
+  const int a = act[k];
+  if ((a & 1) && i >= pk1[k].lo && i < pk1[k].hi) {
+    const PK &p = pk1[k];
+    c += voigt64(asym_delta(t - p.x0, (double)p.asym), (double)p.inv, (double)p.cL, (double)p.cG, (double)p.pedestal);
+  }
+  if ((a & 2) && i >= pk2[k].lo && i < pk2[k].hi) {
+    const PK &p = pk2[k];
+    c += (double)w2[k] *
+         voigt64(asym_delta(t - p.x0, (double)p.asym), (double)p.inv, (double)p.cL, (double)p.cG, (double)p.pedestal);
+  }
+  return c;
+}
+
+template <class PK, class HT, class WT>
+__device__ void solve_free_heights(const Params &P, const Shared &sh, const PK *pk1, const PK *pk2, HT *h1,
+                                   const HT *w2, const int *act, const double *tth, const double *yobs,
+                                   const WT *wobs, double *nn) {
+  const int m = P.nRefl, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  double *H = nn, *Fc = H + m * m, *rhs = Fc + m * m, *sc = rhs + m, *x = sc + m, *grad = x + m, *sol = grad + m,
+         *mask = sol + m, *tmp = mask + m, *pidx = tmp + m;
+  const double *v = sh.v;
+  const double t0 = tth[0], t1 = tth[P.n - 1], zs = t1 > t0 ? 2.0 / (t1 - t0) : 0.0;
+  auto window = [&](int k, int &lo, int &hi) {
+    lo = P.n;
+    hi = 0;
+    if (act[k] & 1) { lo = min(lo, pk1[k].lo); hi = max(hi, pk1[k].hi); }
+    if (act[k] & 2) { lo = min(lo, pk2[k].lo); hi = max(hi, pk2[k].hi); }
+  };
+  // norms and right-hand sides: warp per reflection
+  for (int k = warp; k < m; k += nw) {
+    int lo, hi;
+    window(k, lo, hi);
+    double a = 0, r = 0;
+    for (int i = lo + lane; i < hi; i += 32) {
+      const double w = (double)wobs[i];
+      if (!(w > 0)) continue;
+      const double t = tth[i], c = free_column(pk1, pk2, w2, act, k, i, t);
+      const double z = t1 > t0 ? (t - t0) * zs - 1 : 0;
+      double Tm2 = 1, Tm1 = z, bk = 0;
+      for (int q = 0; q < P.nBkg; ++q) {
+        const double T = q == 0 ? 1 : q == 1 ? z : 2 * z * Tm1 - Tm2;
+        if (q >= 2) { Tm2 = Tm1; Tm1 = T; }
+        bk += v[PBKG0 + q] * T;
+      }
+      a += w * c * c;
+      r += w * c * (yobs[i] - bk);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    if (lane == 0) {
+      const double sk = sqrt(fmax(0.0, a));
+      sc[k] = sk;
+      rhs[k] = sk > 0 ? r / sk : 0.0;
+    }
+  }
+  __syncthreads();
+  // H in the scaled columns: warp per pair j <= k, over the windows' overlap
+  for (int pq = warp; pq < m * m; pq += nw) {
+    const int j = pq / m, k = pq % m;
+    if (k < j) continue;
+    double hv = 0;
+    if (sc[j] > 0 && sc[k] > 0) {
+      int lj, hj, lk, hk;
+      window(j, lj, hj);
+      window(k, lk, hk);
+      for (int i = max(lj, lk) + lane; i < min(hj, hk); i += 32) {
+        const double w = (double)wobs[i];
+        if (!(w > 0)) continue;
+        const double t = tth[i];
+        hv += w * free_column(pk1, pk2, w2, act, j, i, t) * free_column(pk1, pk2, w2, act, k, i, t);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) hv += __shfl_xor_sync(0xffffffffu, hv, o);
+      hv /= sc[j] * sc[k];
+    }
+    if (lane == 0) {
+      H[j * m + k] = hv;
+      H[k * m + j] = hv;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int j = lane; j < m; j += 32) { x[j] = 0.0; grad[j] = rhs[j]; }
+    double magnitude = 1.0;
+    for (int j = lane; j < m; j += 32) magnitude = fmax(magnitude, fabs(rhs[j]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) magnitude = fmax(magnitude, __shfl_xor_sync(0xffffffffu, magnitude, o));
+    const double tol = 1e-5 * magnitude;
+    __syncwarp();
+    // KKT error of x, with grad = rhs - H x refreshed (warp-collective)
+    auto kkt = [&]() {
+      double err = 0;
+      for (int j = lane; j < m; j += 32) {
+        double g = rhs[j];
+        for (int k = 0; k < m; ++k) g -= H[j * m + k] * x[k];
+        grad[j] = g;
+        err = fmax(err, x[j] > 0 ? fabs(g) : fmax(0.0, g));
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+      __syncwarp();
+      return err;
+    };
+    bool conv = false;
+    for (int round = 0; round < 8 && !conv; ++round) {
+      // projected coordinate descent, eight cycles
+      for (int cyc = 0; cyc < 8; ++cyc)
+        for (int j = 0; j < m; ++j) {
+          const double diag = H[j * m + j];
+          if (!(diag > 0)) continue;
+          const double old = x[j], next = fmax(0.0, old + grad[j] / diag), delta = next - old;
+          __syncwarp();
+          if (lane == 0) x[j] = next;
+          if (delta != 0)
+            for (int k = lane; k < m; k += 32) grad[k] -= H[k * m + j] * delta;
+          __syncwarp();
+        }
+      if (kkt() <= tol) { conv = true; break; }
+      // active-set polish (lane 0; the passive block is small)
+      if (lane == 0) {
+        for (int j = 0; j < m; ++j) mask[j] = x[j] > 0 ? 1.0 : 0.0;
+        for (int it = 0; it < 8; ++it) {
+          int np = 0;
+          for (int j = 0; j < m; ++j) {
+            sol[j] = 0.0;
+            if (mask[j] > 0.5) pidx[np++] = (double)j;
+          }
+          for (int i = 0; i < np; ++i) {
+            const int ri = (int)pidx[i];
+            for (int j = 0; j <= i; ++j) {
+              const int rj = (int)pidx[j];
+              double a = H[ri * m + rj];
+              for (int q = 0; q < j; ++q) a -= Fc[i * m + q] * Fc[j * m + q];
+              if (i == j) Fc[i * m + j] = sqrt(fmax(1e-7, a));
+              else Fc[i * m + j] = a / Fc[j * m + j];
+            }
+            double a = rhs[ri];
+            for (int q = 0; q < i; ++q) a -= Fc[i * m + q] * tmp[q];
+            tmp[i] = a / Fc[i * m + i];
+          }
+          for (int c = 0; c < np; ++c) {
+            const int i = np - 1 - c;
+            double a = tmp[i];
+            for (int q = i + 1; q < np; ++q) a -= Fc[q * m + i] * tmp[q];
+            tmp[i] = a / Fc[i * m + i];
+          }
+          for (int i = 0; i < np; ++i) sol[(int)pidx[i]] = tmp[i];
+          double alpha = 1.0;
+          int hit = -1;
+          for (int j = 0; j < m; ++j)
+            if (mask[j] > 0.5 && sol[j] <= 0.0) {
+              const double old = x[j], den = old - sol[j];
+              const double t = den > 0 ? old / fmax(1e-30, den) : 0.0;
+              if (hit < 0 || t < alpha) { alpha = t; hit = j; }
+            }
+          if (hit >= 0) {
+            for (int j = 0; j < m; ++j)
+              if (mask[j] > 0.5) {
+                const double next = fmax(0.0, x[j] + alpha * (sol[j] - x[j]));
+                x[j] = next;
+                if (next == 0.0 && sol[j] <= 0.0) mask[j] = 0.0;
+              }
+            x[hit] = 0.0;
+            mask[hit] = 0.0;
+            continue;
+          }
+          for (int j = 0; j < m; ++j) x[j] = mask[j] > 0.5 ? sol[j] : 0.0;
+          double err = 0, violation = tol;
+          int enter = -1;
+          for (int j = 0; j < m; ++j) {
+            double g = rhs[j];
+            for (int k = 0; k < m; ++k) g -= H[j * m + k] * x[k];
+            grad[j] = g;
+            err = fmax(err, x[j] > 0 ? fabs(g) : fmax(0.0, g));
+            if (mask[j] < 0.5 && g > violation) { violation = g; enter = j; }
+          }
+          if (err <= tol || enter < 0) break;
+          mask[enter] = 1.0;
+        }
+      }
+      __syncwarp();
+      if (kkt() <= tol) conv = true;
+    }
+  }
+  __syncthreads();
+  for (int k = tid; k < m; k += blockDim.x) h1[k] = (HT)(sc[k] > 0 ? x[k] / sc[k] : 0.0);
+  __syncthreads();
+}
+
 __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, float *h1, float *w2, int *act,
-                           const double *tth, const double *yobs, const float *wobs, float *ycalc) {
+                           const double *tth, const double *yobs, const float *wobs, float *ycalc,
+                           double *nn = nullptr) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
   __syncthreads();
@@ -449,6 +662,7 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
   const int nR = P.nRefl;
   reflection_stage<false>(P, sh, pk1, pk2, h1, w2, nullptr, act, tth);
   __syncthreads();
+  if (P.method == 1) solve_free_heights(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nn);
   // --- pattern in warp tiles of 32 points, then chi^2 (FP64)
   double chi = 0.0;
   const double x0 = tth[0], x1 = tth[P.n - 1], zs = x1 > x0 ? 2.0 / (x1 - x0) : 0.0;
@@ -563,10 +777,11 @@ __global__ void __launch_bounds__(kThreads) pt_cost_kernel(const Params P, const
   const int c = blockIdx.x;
   if (threadIdx.x == 0) apply(P, vectors + (size_t)c * P.nv, sh.v);
   __syncthreads();
+  double *nn = P.method == 1 ? reinterpret_cast<double *>(smem + L.total) : nullptr;
   const double chi = evaluate(P, sh, reinterpret_cast<Peak *>(smem + L.pk1), reinterpret_cast<Peak *>(smem + L.pk2),
                               reinterpret_cast<float *>(smem + L.h1), reinterpret_cast<float *>(smem + L.w2),
                               reinterpret_cast<int *>(smem + L.act), P.tth, P.y, P.w,
-                              ycalc ? ycalc + (size_t)c * P.n : nullptr);
+                              ycalc ? ycalc + (size_t)c * P.n : nullptr, nn);
   if (threadIdx.x == 0) costs[c] = chi;
 }
 
@@ -631,7 +846,8 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
       apply(P, xs, sh.v);
     }
     __syncthreads();
-    const double cost = evaluate(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nullptr);
+    const double cost = evaluate(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nullptr,
+                                 P.method == 1 ? reinterpret_cast<double *>(smem + L.total) : nullptr);
     if (threadIdx.x == 0) {
       st.proposalCost = cost;
       if (bootstrap) {
@@ -711,6 +927,12 @@ __global__ void __launch_bounds__(kThreads) pt_pattern64_kernel(const Params P, 
   }
   reflection_stage<true>(P, sh, pk1, pk2, h1, w2, u1, act, P.tth);
   __syncthreads();
+  if (P.method == 1) {
+    // free heights; no scale column (u1 = 0)
+    solve_free_heights(P, sh, pk1, pk2, h1, w2, act, P.tth, P.y, P.wd, reinterpret_cast<double *>(smem + L.total));
+    for (int k = tid; k < P.nRefl; k += kThreads) u1[k] = 0.0;
+    __syncthreads();
+  }
   const double *v = sh.v;
   const int nR = P.nRefl;
   const double x0 = P.tth[0], x1 = P.tth[P.n - 1], zs = x1 > x0 ? 2.0 / (x1 - x0) : 0.0;
@@ -980,16 +1202,20 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
   clear_error();
   if (!pr || !out) return set_error(P6_ERR_INVALID_ARG, "null problem or output pointer");
   *out = nullptr;
-  if (pr->n_refl <= 0 || pr->n_reps <= 0 || pr->n_atoms <= 0 || pr->n_points < 2)
+  if (pr->n_refl <= 0 || pr->n_reps <= 0 || (pr->n_atoms <= 0 && pr->method == 0) || pr->n_atoms < 0 ||
+      pr->n_points < 2)
     return set_error(P6_ERR_INVALID_ARG, "empty problem");
+  if (pr->method != 0 && pr->method != 1) return set_error(P6_ERR_INVALID_ARG, "method must be 0 (Rietveld) or 1 (WPPF / Le Bail)");
+  if (pr->method == 1 && pr->n_refl > kMaxFreeRefl)
+    return set_error(P6_ERR_CAPACITY, "free-intensity fits hold at most 64 envelope reflections on the device");
   if (pr->nv < 1 || pr->nv > kMaxNv) return set_error(P6_ERR_CAPACITY, "1 to 32 refined parameters");
   if (pr->n_full < PBKG0 + pr->n_bkg || pr->n_full > kMaxFull)
     return set_error(P6_ERR_INVALID_ARG, "full parameter vector too short or too long");
   if (pr->chains < 2 || pr->chains > 65535) return set_error(P6_ERR_INVALID_ARG, "at least 2 chains");
   if (!(pr->max_temp > 1)) return set_error(P6_ERR_INVALID_ARG, "max_temp must exceed 1");
-  if (!pr->hkl || !pr->mult || !pr->rep_rot || !pr->rep_trans || !pr->atom_pos || !pr->atom_wmult ||
-      !pr->atom_occ || !pr->ff_a || !pr->ff_b || !pr->ff_c || !pr->tth || !pr->y || !pr->w || !pr->full_values ||
-      !pr->index || !pr->lo || !pr->hi || !pr->scales)
+  if (!pr->hkl || !pr->mult || !pr->rep_rot || !pr->rep_trans || !pr->tth || !pr->y || !pr->w || !pr->full_values ||
+      !pr->index || !pr->lo || !pr->hi || !pr->scales ||
+      (pr->n_atoms > 0 && (!pr->atom_pos || !pr->atom_wmult || !pr->atom_occ || !pr->ff_a || !pr->ff_b || !pr->ff_c)))
     return set_error(P6_ERR_INVALID_ARG, "null table pointer");
   for (int j = 0; j < pr->nv; ++j)
     if (pr->index[j] < 0 || pr->index[j] >= pr->n_full) return set_error(P6_ERR_INVALID_ARG, "parameter index out of range");
@@ -1055,15 +1281,17 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
   int smemOptin = 0;
   cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   const int staticBytes = 4096;
-  P.stageObs = smem_layout(P.nRefl, P.n, 1).total + staticBytes <= smemOptin ? 1 : 0;
-  s->smemSweep = smem_layout(P.nRefl, P.n, P.stageObs).total;
-  s->smemCost = smem_layout(P.nRefl, P.n, 0).total;
+  P.method = pr->method;
+  const int nnB = P.method == 1 ? nnls_bytes(P.nRefl) : 0;   // free-intensity scratch after each layout
+  P.stageObs = smem_layout(P.nRefl, P.n, 1).total + nnB + staticBytes <= smemOptin ? 1 : 0;
+  s->smemSweep = smem_layout(P.nRefl, P.n, P.stageObs).total + nnB;
+  s->smemCost = smem_layout(P.nRefl, P.n, 0).total + nnB;
   if (s->smemCost + staticBytes > smemOptin) {
     pt_free(s);
     return set_error(P6_ERR_CAPACITY, "too many reflections for the shared-memory peak table");
   }
   // the FP64 peak table of the least-squares finish; 0 when it does not fit (the finish then reports CAPACITY)
-  s->smem64 = smem64_layout(P.nRefl).total + staticBytes <= smemOptin ? smem64_layout(P.nRefl).total : 0;
+  s->smem64 = smem64_layout(P.nRefl).total + nnB + staticBytes <= smemOptin ? smem64_layout(P.nRefl).total + nnB : 0;
   s->fullHost.assign(pr->full_values, pr->full_values + pr->n_full);
   s->indexHost.assign(pr->index, pr->index + pr->nv);
   s->loHost.assign(pr->lo, pr->lo + pr->nv);

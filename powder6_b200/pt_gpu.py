@@ -67,6 +67,20 @@ class PTProblem:
     # when True, 'SL' and 'HL' are the full-vector entries after the background
     # (and after 'po').
     asym: bool = False
+    # Phase method (js/rietveld_core.js:110, js/pt_gpu.js:259-297): 'rietveld'
+    # takes the heights from the structure; 'lebail' and 'wppf' leave every
+    # reflection's height free and non-negative, solved per evaluation by NNLS
+    # against the observed pattern minus the background (atoms unused; at most
+    # 64 reflections in the envelope).
+    method: str = 'rietveld'
+
+    @property
+    def method_code(self) -> int:
+        if self.method == 'rietveld':
+            return 0
+        if self.method in ('lebail', 'wppf'):
+            return 1
+        raise ValueError(f"method must be 'rietveld', 'lebail' or 'wppf', not {self.method!r}")
 
     @property
     def index(self) -> np.ndarray:
@@ -223,6 +237,7 @@ class PTSession:
             for i in range(3):
                 pr.po_dir[i] = float(P.po_dir[i])
         pr.has_asym = 1 if P.asym else 0
+        pr.method = P.method_code
         h = C.c_void_p()
         check(self.lib.p6_pt_create(C.byref(pr), int(device), C.byref(h)))
         self.h = h

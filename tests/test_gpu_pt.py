@@ -276,3 +276,70 @@ def test_asymmetry_normal_equations_and_lm_match_oracle(nacl_asym):
     assert ig['code'] == io['code'] and ig['accepted'] == io['accepted']
     assert abs(ig['chi2'] - io['chi2']) <= 1e-9 * io['chi2']
     assert np.allclose(xg, xo, rtol=1e-7, atol=1e-9)
+
+
+# ---------------------------------------------------------------------------
+# WPPF / Le Bail free intensities (js/pt_gpu.js:259-297): per evaluation, the
+# non-negative heights of every reflection solved against y - background.
+# The kernel's solve (coordinate descent, then an active-set polish, to a KKT
+# error of 1e-5 of the largest right-hand side) and the oracle's exact
+# Lawson-Hanson solve reach the same optimum; the chi^2 tolerances add, to
+# the FP32 / FP64 bars above, 1e-9 of sum w y^2 for the solve's stopping rule.
+# ---------------------------------------------------------------------------
+FREE_SOLVE_ATOL_FRAC = 1e-9
+
+
+@pytest.fixture(scope='module')
+def nacl_wppf(nacl, oracle):
+    import copy
+    P, M, truth = nacl
+    Pw = copy.copy(P)
+    Pw.method = 'wppf'
+    return Pw, oracle.PtModel(Pw, dmin=reflection_dmin(Pw)), truth
+
+
+def test_free_intensity_costs_and_patterns_match_oracle(nacl_wppf):
+    P, M, truth = nacl_wppf
+    xs = [truth] + start_vectors(P, truth, 7, seed=41)
+    slack = FREE_SOLVE_ATOL_FRAC * float(np.sum(P.w * P.y ** 2))
+    with PTSession(ctx_of(P, truth, chains=len(xs))) as s:
+        g, ys = s.costs(xs, with_pattern=True)
+        c64 = s.model_costs(xs)
+    for x, gc, gm, y in zip(xs, g, c64, ys):
+        c, yo, _ = M.cost_full(P.apply(x), True)
+        assert abs(gm - c) <= 1e-10 * c + slack, (gm, c)
+        assert abs(gc - c) <= 2e-5 * c + slack, (gc, c)
+        assert np.max(np.abs(y - yo)) <= PATTERN_ATOL_FRAC * np.max(np.abs(yo))
+
+
+def test_free_intensity_run_reduces_chi2_and_validates(nacl_wppf):
+    """Tempering with free intensities: the cell and profile move, the heights
+    follow by NNLS in every proposal; the run passes the 1e-3 validation gate
+    against the oracle and reaches the noise level (chi^2 below 1.2 per
+    point) from a start two orders of magnitude above it."""
+    P, M, truth = nacl_wppf
+    x0 = start_vectors(P, truth, 1, seed=8)[0]
+    c0 = M.cost(x0)
+    ctx = ctx_of(P, x0, chains=32, sweeps=60, cost=M.cost)
+    ctx.setup['initialCost'] = c0
+    r = run(ctx)
+    assert r['pt']['validationError'] < 1e-5
+    assert r['pt']['bestChi2'] < 0.1 * c0
+    assert abs(M.cost(r['x']) - r['pt']['bestChi2']) <= 1e-6 * r['pt']['bestChi2']
+
+
+def test_free_intensity_envelope_cap_is_enforced(nacl_wppf):
+    """More than 64 envelope reflections is refused at creation with an error,
+    not truncated."""
+    import copy
+    P, _, truth = nacl_wppf
+    Pb = copy.copy(P)
+    Pb.values = P.values.copy()
+    Pb.values[1:4] = 11.28
+    Pb.lo, Pb.hi = P.lo.copy(), P.hi.copy()
+    ia = P.refined.index('a')
+    Pb.lo[ia], Pb.hi[ia] = 11.2, 11.4
+    x = truth.copy()
+    x[ia] = 11.28
+    with pytest.raises(RuntimeError, match='64'):
+        PTSession(ctx_of(Pb, x, chains=2))

@@ -268,3 +268,96 @@ def test_asymmetry_cost_reduces_to_symmetric_at_zero(nacl, oracle):
     Ma = oracle.PtModel(Pa, dmin=reflection_dmin(P))
     assert Ma.cost(np.append(truth, [0.0, 0.0])) == M.cost(truth)
     assert Ma.cost(np.append(truth, [0.2, 0.05])) > 1.05 * M.cost(truth)
+
+
+# ---------------------------------------------------------------------------
+# WPPF / Le Bail free intensities (js/pt_gpu.js:259-297)
+# ---------------------------------------------------------------------------
+def _nnls_lib(oracle):
+    lib = oracle.load()
+    lib.p6o_nnls_normal.restype = C.c_int
+    lib.p6o_nnls_normal.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    return lib
+
+
+def test_nnls_on_normal_equations_matches_scipy(oracle):
+    """The oracle's Lawson-Hanson solve on H = A^T A, rhs = A^T b reaches
+    scipy's NNLS optimum of |A x - b| (relative excess below 1e-12), on random
+    problems of 1..40 columns, a third of them with two nearly collinear
+    columns, and on the degenerate cases: all-negative rhs (x = 0) and one
+    column."""
+    from scipy.optimize import nnls
+    lib = _nnls_lib(oracle)
+    rng = np.random.default_rng(0)
+    for t in range(120):
+        m = int(rng.integers(1, 41))
+        A = rng.normal(size=(int(rng.integers(m, 3 * m + 5)), m))
+        b = 3 * rng.normal(size=A.shape[0])
+        if t % 3 == 0 and m > 1:
+            A[:, 0] = 0.999 * A[:, 1] + 1e-3 * A[:, 0]
+        xs, _ = nnls(A, b, maxiter=10000)
+        H, r, x = np.ascontiguousarray(A.T @ A), np.ascontiguousarray(A.T @ b), np.zeros(m)
+        assert lib.p6o_nnls_normal(H.ctypes.data, r.ctypes.data, m, x.ctypes.data) >= 0
+        assert np.all(x >= 0)
+        fs, fo = np.sum((A @ xs - b) ** 2), np.sum((A @ x - b) ** 2)
+        assert fo - fs <= 1e-12 * max(fs, 1.0), (t, fo, fs)
+    A = np.abs(rng.normal(size=(12, 5)))
+    H, r, x = np.ascontiguousarray(A.T @ A), np.ascontiguousarray(-A.T @ np.ones(12)), np.ones(5)
+    lib.p6o_nnls_normal(H.ctypes.data, r.ctypes.data, 5, x.ctypes.data)
+    assert np.all(x == 0)
+    H, r, x = np.array([[4.0]]), np.array([2.0]), np.zeros(1)
+    lib.p6o_nnls_normal(H.ctypes.data, r.ctypes.data, 1, x.ctypes.data)
+    assert x[0] == 0.5
+
+
+def _free(P, method='wppf'):
+    import copy
+    out = copy.copy(P)
+    out.method = method
+    return out
+
+
+def test_free_intensity_cost_bounds_and_invariances(nacl, oracle):
+    """A free-intensity fit is never worse than the Rietveld heights, which
+    are one non-negative choice of the same columns: chi^2(wppf) <= chi^2
+    (rietveld) at the truth and at start vectors.  At the truth it sits at the
+    noise level (about one per point).  The scale and Biso do not enter it
+    (bit-identical chi^2), 'lebail' and 'wppf' are the same fit, and any other
+    method name is rejected."""
+    P, M, truth = nacl
+    Pw = _free(P)
+    Mw = oracle.PtModel(Pw, dmin=reflection_dmin(P))
+    for x in [truth] + start_vectors(P, truth, 6, seed=21):
+        assert Mw.cost(x) <= M.cost(x) * (1 + 1e-12)
+    c = Mw.cost(truth)
+    assert 0.8 * len(P.tth) < c < 1.2 * len(P.tth)
+    x = truth.copy()
+    x[P.refined.index('scale')] *= 1.3
+    x[P.refined.index('Biso')] += 0.7
+    assert Mw.cost(x) == c
+    assert oracle.PtModel(_free(P, 'lebail'), dmin=reflection_dmin(P)).cost(truth) == c
+    with pytest.raises(ValueError):
+        _free(P, 'pawley').method_code
+
+
+def test_free_intensity_pattern_is_the_nnls_fit(nacl, oracle):
+    """The free-intensity pattern returned with chi^2 is consistent with it
+    (chi^2 = sum w (y - ycalc)^2 to 1e-9), its peak part (ycalc minus the
+    background) is non-negative everywhere, and it lowers chi^2 below the
+    background alone.  The background is the Rietveld pattern at scale 0."""
+    P, M, truth = nacl
+    Mw = oracle.PtModel(_free(P), dmin=reflection_dmin(P))
+    x = start_vectors(P, truth, 1, seed=5)[0]
+    v = P.apply(x)
+    c, y, _ = Mw.cost_full(v, True)
+    bk_only = v.copy()
+    bk_only[0] = 0.0
+    _, bkg, _ = M.cost_full(bk_only, True)
+    w = P.w
+    r = P.y - y
+    assert abs(c - np.sum(w * r * r)) <= 1e-9 * c
+    # every heights-and-background decomposition: the fitted peaks are y - bkg
+    peaks = y - bkg
+    assert np.min(peaks) >= -1e-9 * np.max(np.abs(peaks))
+    # the fit lowers chi^2 from the background alone
+    assert c < np.sum(w * (P.y - bkg) ** 2)
