@@ -53,12 +53,13 @@ def parse():
     ap.add_argument('--cos-mode', type=int, default=0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--workload', default='wyckoff',
-                    choices=['wyckoff', 'pt', 'contract', 'batch', 'learned', 'refine'],
+                    choices=['wyckoff', 'pt', 'contract', 'batch', 'learned', 'refine', 'cf'],
                     help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit; '
                          'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000); '
                          'batch: 64 uneven Wyckoff searches in one persistent launch; '
                          'learned: the learned-proposal search (P2_1/c, 17 sites, 8192 replicas); '
-                         'refine: least-squares refinement of 512 perturbed PbSO4 structures')
+                         'refine: least-squares refinement of 512 perturbed PbSO4 structures; '
+                         'cf: charge flipping, 128 random starts of the adaptive plan on a 64^3 grid')
     ap.add_argument('--method', default='split', choices=['split', 'fp32'],
                     help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
     ap.add_argument('--chains', type=int, default=64)
@@ -762,6 +763,142 @@ def run_reference_refine(args, world, rank):
         'e2e': {'value': v, 'unit': 'structures/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}), flush=True)
 
 
+CF_GRID = 64
+CF_TRIALS = 128
+CF_CYCLES = 100
+CF_WORKLOAD = (f'charge flipping, synthetic P2_1/c structure (9.1 x 7.3 x 10.4 A, beta 104, d >= 0.8 A), '
+               f'{CF_GRID}^3 grid, {CF_TRIALS} random starts of the adaptive plan (3 settings), {CF_CYCLES} cycles')
+
+
+def cf_setup(rank=0):
+    from powder6_b200.charge_flipping import (build_reflection_model, cf_plan, classify_weak_orbits, synthetic_job)
+    job = synthetic_job(grid=CF_GRID, dmin=0.8, seed=1)
+    m = build_reflection_model(job, CF_GRID)
+    plan = cf_plan(CF_TRIALS)
+    trials = []
+    for i, t in enumerate(plan['trials']):
+        wk = classify_weak_orbits(m, t['weakFraction'], 'cluster')
+        trials.append({'threshold': t['threshold'], 'symLambda': t['symLambda'], 'seed': 1000 * rank + i + 1,
+                       'weak': wk['flags'] if wk['weakOrbits'] else None})
+    return job, m, trials
+
+
+def cf_cpu_rate(m, trials, seconds):
+    """Cycles per second of the FP64 restatement (numpy FFTs, one thread)."""
+    from oracle.oracle_cf import CfState
+    from powder6_b200.charge_flipping import model_initial_grid
+    done, t0 = 0, time.perf_counter()
+    st = None
+    while time.perf_counter() - t0 < seconds:
+        t = trials[done % len(trials)]
+        if st is None or done % 10 == 0:
+            st = CfState(m, model_initial_grid(m, CF_GRID, t['seed']), t['threshold'], t['symLambda'], t['seed'],
+                         t['weak'])
+        st.cycle()
+        done += 1
+    return done / (time.perf_counter() - t0), done
+
+
+def main_cf(args, world, rank, local):
+    """One step = CF_CYCLES cycles of all CF_TRIALS trials (one graph replay
+    per cycle: six transform passes and the reciprocal step, every trial in
+    each launch).  value: trial-cycles per second from CUDA events on the
+    session's stream, grids resident; e2e: the same per step through the
+    public API with the starting grids uploaded (pinned-size host arrays,
+    set_grid), the run, the best R read back and the best trial's density
+    map read back; the grids (128 x 2 MB) exceed L2, so no flush is needed."""
+    import torch
+    from powder6_b200.charge_flipping import CFSession, model_initial_grid
+    torch.cuda.set_device(local)
+    job, m, trials = cf_setup(rank)
+    starts = [model_initial_grid(m, CF_GRID, t['seed']) for t in trials]
+    ms, e2e = [], []
+    with CFSession(m, trials, device=local) as s:
+        for i, g in enumerate(starts):
+            s.set_grid(g, i)
+        for _ in range(args.warmup):
+            s.run(CF_CYCLES)
+        l0 = s.launch_count()
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                s.run(CF_CYCLES)
+                ms.append(s.last_ms())
+        launches = s.launch_count() - l0
+        fft_ms, rec_ms = s.time_kernels(3)
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            for i, g in enumerate(starts):
+                s.set_grid(g, i)
+            s.run(CF_CYCLES)
+            best = s.best_r()
+            s.read(int(np.argmin(best)), 'map')
+            e2e.append(time.perf_counter() - t0)
+    total_ms = max_over_ranks(float(sum(ms)), world)
+    units = world * CF_TRIALS * CF_CYCLES * args.steps
+    value = units / (total_ms / 1000.0)
+    e2e_value = units / max_over_ranks(float(sum(e2e)), world)
+    if rank == 0:
+        cells = CF_GRID ** 3
+        pass_bytes = 2 * cells * 8 * CF_TRIALS            # read + write every trial's grid once
+        achieved = pass_bytes / (fft_ms * 1e-3) / 1e9
+        peak, peak_note = measured_peak('hbm_gbs')
+        clocks = clk.summary()
+        line = {
+            'metric': 'charge-flipping trial-cycles/s', 'value': value, 'unit': 'cycles/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': CF_WORKLOAD, 'grid': CF_GRID, 'trials': CF_TRIALS, 'cycles_per_step': CF_CYCLES,
+                       'orbits': m['nOrbits'], 'clusters': m['nClusters'], 'members': m['nMembers'],
+                       'l2': f'grids {CF_TRIALS * cells * 8 / 1e6:.0f} MB > L2, no flush',
+                       'fft_pass_ms': fft_ms, 'reciprocal_ms': rec_ms,
+                       'parallelism': f'trials only x{world}'},
+            'e2e': {'value': e2e_value, 'unit': 'cycles/s', 'h2d_bytes_per_step': CF_TRIALS * cells * 8,
+                    'd2h_bytes_per_step': CF_TRIALS * 4 + cells * 4 + CF_TRIALS * CF_CYCLES * 4},
+            'roofline': {'kernel': 'cf_fft_kernel<64>', 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                         'unit': 'GB/s', 'frac': achieved / peak if peak else None, 'peak_source': peak_note,
+                         'traffic': None,
+                         'algorithmic_bytes_per_launch': pass_bytes},
+            'gpu_launches': int(launches),
+            'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            rate, done = cf_cpu_rate(m, trials, 10.0)
+            line['cpu_baseline'] = {'value': rate, 'unit': 'cycles/s', 'cores': 1, 'kind': 'port',
+                                    'sample': f'{done} cycles of the FP64 restatement (numpy FFTs, one thread) on '
+                                              f'the same model, trials in turn'}
+        print(json.dumps(line), flush=True)
+
+
+def run_reference_cf(args, world, rank):
+    """The reference arm of the charge-flipping workload: the FP64
+    restatement of the cycle (numpy FFTs, one host thread); each step is a
+    bounded sample of 10 trial-cycles."""
+    if rank != 0:
+        return
+    from oracle.oracle_cf import CfState
+    from powder6_b200.charge_flipping import model_initial_grid
+    job, m, trials = cf_setup(0)
+    times, per_step = [], 10
+    for i in range(args.warmup + args.steps):
+        t = trials[i % len(trials)]
+        st = CfState(m, model_initial_grid(m, CF_GRID, t['seed']), t['threshold'], t['symLambda'], t['seed'],
+                     t['weak'])
+        t0 = time.perf_counter()
+        for _ in range(per_step):
+            st.cycle()
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    v = per_step * args.steps / sum(times)
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'charge-flipping trial-cycles/s', 'value': v, 'unit': 'cycles/s',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000.0 * sum(times) / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': CF_WORKLOAD, 'sample': f'{per_step} cycles of one trial per step'},
+        'cpu_baseline': {'value': v, 'unit': 'cycles/s', 'cores': 1, 'kind': 'port',
+                         'sample': f'{per_step} cycles of one trial per step, FP64 restatement (numpy), one thread'},
+        'e2e': {'value': v, 'unit': 'cycles/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}), flush=True)
+
+
 def main_learned(args, world, rank, local):
     """One step = one learned-proposal search (P2_1/c, 17 independent C/N/S
     sites, 575 reflections, 8192 replicas, LEARNED_GENERATIONS generations; 8
@@ -876,12 +1013,14 @@ def main():
             run_reference_batch(args, world, rank)
         elif args.workload == 'refine':
             run_reference_refine(args, world, rank)
+        elif args.workload == 'cf':
+            run_reference_cf(args, world, rank)
         else:
             run_reference(args, world, rank)
         return
-    if args.workload in ('pt', 'contract', 'batch', 'learned', 'refine'):
+    if args.workload in ('pt', 'contract', 'batch', 'learned', 'refine', 'cf'):
         {'pt': main_pt, 'contract': main_ct, 'batch': main_batch, 'learned': main_learned,
-         'refine': main_refine}[args.workload](
+         'refine': main_refine, 'cf': main_cf}[args.workload](
             args, world, rank, local)
         if world > 1:
             import torch.distributed as dist

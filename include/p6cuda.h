@@ -472,6 +472,70 @@ p6_status p6_ct_last_ms(p6_ct_session *s, float *ms);
 p6_status p6_ct_query(p6_ct_session *s, long long *band_kblocks, long long *band_cols128, int *n_tiles,
                       long long *launches);
 
+/* ======================================================================== */
+/* Dual-space charge flipping on a powder reflection model                   */
+/* ======================================================================== */
+/* The cycle of charge_flipping.wgsl:182-632 in the order
+ * js/charge_flipping_worker.js:2353-2395 dispatches it: F -> rho (inverse
+ * 3-D FFT, 1/n^3), the flip threshold delta = delta_sigma * sigma(Re rho),
+ * the flip (Re rho < delta -> -Re rho, Im rho = 0), rho -> F, the R factor on
+ * cluster totals, the Le Bail repartition of each cluster's observed
+ * intensity, the space-group symmetrisation damped by sym_lambda, the
+ * amplitude constraint (a quarter-turn for weak orbits), hard zeros on the
+ * absent reflections and F(000), and the best iterate kept on the device.
+ * Independent trials (random starts and settings of one model) run in the
+ * same launches.  Grids are interleaved complex floats, index h + k n + l n^2
+ * with the Miller indices wrapped into 0..n-1. */
+typedef struct {
+  int n;                               /* grid edge: 8, 16, 32, 64 or 128 */
+  int n_orbits;
+  const uint32_t *orbit_start;         /* n_orbits: first member of each orbit */
+  const uint32_t *orbit_count;         /* n_orbits: members of each orbit */
+  int n_members;
+  const uint32_t *orbit_idx;           /* n_members: grid index, | 0x80000000 when the member stores the Friedel mate */
+  const float *phase;                  /* 2 n_members: exp(+2 pi i h0.t) of the operator that produced the member */
+  int n_clusters;
+  const uint32_t *cluster_orbit_start; /* n_clusters: first orbit (the orbits of a cluster are consecutive) */
+  const uint32_t *cluster_n_orbits;    /* n_clusters */
+  const float *cluster_obs_i;          /* n_clusters: observed intensity of the cluster */
+  int n_absent;
+  const uint32_t *absent_idx;          /* n_absent: grid indices held at zero */
+} p6_cf_model;
+
+typedef struct {
+  float delta_sigma;                   /* flip threshold in units of the map's sigma */
+  float sym_lambda;                    /* 0: P1 charge flipping .. 1: strict space-group symmetry */
+  uint32_t seed;                       /* phase restarts of reflections whose amplitude collapsed */
+  const uint8_t *weak;                 /* n_orbits flags (quarter-turn instead of the amplitude constraint), or NULL */
+} p6_cf_trial;
+
+typedef struct p6_cf_session p6_cf_session;
+
+/* Replaces the GPU setup of runChargeFlippingGPU (js/charge_flipping_worker.js:1997-2330). */
+p6_status p6_cf_create(const p6_cf_model *model, int n_trials, const p6_cf_trial *trials, int device,
+                       p6_cf_session **out);
+p6_status p6_cf_destroy(p6_cf_session *s);
+/* Uploads the starting F grid (2 n^3 floats) of one trial, or of every trial
+ * when trial < 0, makes it the best iterate and resets the best R to +inf. */
+p6_status p6_cf_set_grid(p6_cf_session *s, int trial, const float *grid);
+/* Runs `cycles` cycles of every trial (the loop of
+ * js/charge_flipping_worker.js:2353-2395); r_history (n_trials x cycles, row
+ * per trial, may be NULL) receives the R factor of each cycle.  Blocking. */
+p6_status p6_cf_run(p6_cf_session *s, int cycles, float *r_history);
+/* Best R of every trial (n_trials floats). */
+p6_status p6_cf_best_r(p6_cf_session *s, float *best_r);
+/* which = 0: the current F grid (2 n^3 floats); 1: the best F grid; 2: the
+ * density of the best grid (n^3 floats, the real part of its inverse
+ * transform with 1/n^3). */
+p6_status p6_cf_read(p6_cf_session *s, int trial, int which, float *out);
+/* Device time of the last p6_cf_run, and the kernels launched so far. */
+p6_status p6_cf_last_ms(p6_cf_session *s, float *ms);
+p6_status p6_cf_launch_count(p6_cf_session *s, long long *count);
+/* Runs `cycles` cycles as separate launches with events between them and
+ * returns the mean device time of one transform pass (one axis, every trial)
+ * and of one reciprocal step; the R factors of these cycles are not kept. */
+p6_status p6_cf_time_kernels(p6_cf_session *s, int cycles, float *fft_pass_ms, float *reciprocal_ms);
+
 /* Philox4x32-10 of one (counter, key) on the device: known-answer check. */
 p6_status p6_philox_device(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

@@ -142,6 +142,15 @@ _SIGS = {
     'p6_ct_last_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_ct_query': (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                               C.POINTER(C.c_longlong)]),
+    'p6_cf_create': (C.c_int, [_P, C.c_int, _P, C.c_int, C.POINTER(C.c_void_p)]),
+    'p6_cf_destroy': (C.c_int, [_P]),
+    'p6_cf_set_grid': (C.c_int, [_P, C.c_int, _P]),
+    'p6_cf_run': (C.c_int, [_P, C.c_int, _P]),
+    'p6_cf_best_r': (C.c_int, [_P, _P]),
+    'p6_cf_read': (C.c_int, [_P, C.c_int, C.c_int, _P]),
+    'p6_cf_last_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
+    'p6_cf_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    'p6_cf_time_kernels': (C.c_int, [_P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }
 
 _lib = None
