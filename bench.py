@@ -62,6 +62,8 @@ def parse():
                          'cf: charge flipping, 128 random starts of the adaptive plan on a 64^3 grid')
     ap.add_argument('--method', default='split', choices=['split', 'fp32'],
                     help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
+    ap.add_argument('--cf-trials', type=int, default=None, help='cf: random starts (default 128)')
+    ap.add_argument('--cf-cycles', type=int, default=None, help='cf: cycles per step (default 100)')
     ap.add_argument('--chains', type=int, default=64)
     ap.add_argument('--sweeps', type=int, default=2000)
     return ap.parse_args()
@@ -770,13 +772,14 @@ CF_WORKLOAD = (f'charge flipping, synthetic P2_1/c structure (9.1 x 7.3 x 10.4 A
                f'{CF_GRID}^3 grid, {CF_TRIALS} random starts of the adaptive plan (3 settings), {CF_CYCLES} cycles')
 
 
-def cf_setup(rank=0):
+def cf_setup(rank=0, n_trials=CF_TRIALS):
     from powder6_b200.charge_flipping import (build_reflection_model, cf_plan, classify_weak_orbits, synthetic_job)
     job = synthetic_job(grid=CF_GRID, dmin=0.8, seed=1)
     m = build_reflection_model(job, CF_GRID)
-    plan = cf_plan(CF_TRIALS)
+    plan = cf_plan(min(128, max(6, n_trials)))
     trials = []
-    for i, t in enumerate(plan['trials']):
+    for i in range(n_trials):
+        t = plan['trials'][i % len(plan['trials'])]
         wk = classify_weak_orbits(m, t['weakFraction'], 'cluster')
         trials.append({'threshold': t['threshold'], 'symLambda': t['symLambda'], 'seed': 1000 * rank + i + 1,
                        'weak': wk['flags'] if wk['weakOrbits'] else None})
@@ -800,7 +803,7 @@ def cf_cpu_rate(m, trials, seconds):
 
 
 def main_cf(args, world, rank, local):
-    """One step = CF_CYCLES cycles of all CF_TRIALS trials (one graph replay
+    """One step = CF_CYCLES cycles of all CF_TRIALS trials (or --cf-cycles, --cf-trials) (one graph replay
     per cycle: six transform passes and the reciprocal step, every trial in
     each launch).  value: trial-cycles per second from CUDA events on the
     session's stream, grids resident; e2e: the same per step through the
@@ -810,18 +813,20 @@ def main_cf(args, world, rank, local):
     import torch
     from powder6_b200.charge_flipping import CFSession, model_initial_grid
     torch.cuda.set_device(local)
-    job, m, trials = cf_setup(rank)
+    n_trials = args.cf_trials or CF_TRIALS
+    cycles = args.cf_cycles or CF_CYCLES
+    job, m, trials = cf_setup(rank, n_trials)
     starts = [model_initial_grid(m, CF_GRID, t['seed']) for t in trials]
     ms, e2e = [], []
     with CFSession(m, trials, device=local) as s:
         for i, g in enumerate(starts):
             s.set_grid(g, i)
         for _ in range(args.warmup):
-            s.run(CF_CYCLES)
+            s.run(cycles)
         l0 = s.launch_count()
         with ClockSampler(local) as clk:
             for _ in range(args.steps):
-                s.run(CF_CYCLES)
+                s.run(cycles)
                 ms.append(s.last_ms())
         launches = s.launch_count() - l0
         fft_ms, rec_ms = s.time_kernels(3)
@@ -829,34 +834,43 @@ def main_cf(args, world, rank, local):
             t0 = time.perf_counter()
             for i, g in enumerate(starts):
                 s.set_grid(g, i)
-            s.run(CF_CYCLES)
+            s.run(cycles)
             best = s.best_r()
             s.read(int(np.argmin(best)), 'map')
             e2e.append(time.perf_counter() - t0)
     total_ms = max_over_ranks(float(sum(ms)), world)
-    units = world * CF_TRIALS * CF_CYCLES * args.steps
+    units = world * n_trials * cycles * args.steps
     value = units / (total_ms / 1000.0)
     e2e_value = units / max_over_ranks(float(sum(e2e)), world)
     if rank == 0:
         cells = CF_GRID ** 3
-        pass_bytes = 2 * cells * 8 * CF_TRIALS            # read + write every trial's grid once
+        pass_bytes = 2 * cells * 8 * n_trials            # read + write every trial's grid once
         achieved = pass_bytes / (fft_ms * 1e-3) / 1e9
         peak, peak_note = measured_peak('hbm_gbs')
         clocks = clk.summary()
+        traffic = None
+        tf = ROOT / 'profiles' / 'cf_fft_traffic.txt'
+        if tf.exists() and n_trials == CF_TRIALS:
+            for ln in tf.read_text().splitlines():
+                if ln.startswith('bytes_per_pass:'):
+                    traffic = int(ln.split(':', 1)[1])
         line = {
             'metric': 'charge-flipping trial-cycles/s', 'value': value, 'unit': 'cycles/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': CF_WORKLOAD, 'grid': CF_GRID, 'trials': CF_TRIALS, 'cycles_per_step': CF_CYCLES,
+            'config': {'workload': CF_WORKLOAD if (n_trials, cycles) == (CF_TRIALS, CF_CYCLES) else
+                       f'{CF_WORKLOAD} (run with {n_trials} starts, {cycles} cycles)',
+                       'grid': CF_GRID, 'trials': n_trials, 'cycles_per_step': cycles,
                        'orbits': m['nOrbits'], 'clusters': m['nClusters'], 'members': m['nMembers'],
-                       'l2': f'grids {CF_TRIALS * cells * 8 / 1e6:.0f} MB > L2, no flush',
+                       'l2': f'grids {n_trials * cells * 8 / 1e6:.0f} MB' + (' > L2, no flush' if n_trials * cells * 8 > 126e6
+                                                                      else ' (in L2)'),
                        'fft_pass_ms': fft_ms, 'reciprocal_ms': rec_ms,
                        'parallelism': f'trials only x{world}'},
-            'e2e': {'value': e2e_value, 'unit': 'cycles/s', 'h2d_bytes_per_step': CF_TRIALS * cells * 8,
-                    'd2h_bytes_per_step': CF_TRIALS * 4 + cells * 4 + CF_TRIALS * CF_CYCLES * 4},
+            'e2e': {'value': e2e_value, 'unit': 'cycles/s', 'h2d_bytes_per_step': n_trials * cells * 8,
+                    'd2h_bytes_per_step': n_trials * 4 + cells * 4 + n_trials * cycles * 4},
             'roofline': {'kernel': 'cf_fft_kernel<64>', 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                          'unit': 'GB/s', 'frac': achieved / peak if peak else None, 'peak_source': peak_note,
-                         'traffic': None,
+                         'traffic': traffic, 'unit_of_launch': f'one pass over all {n_trials} trials',
                          'algorithmic_bytes_per_launch': pass_bytes},
             'gpu_launches': int(launches),
             'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},

@@ -532,8 +532,9 @@ p6_status p6_cf_read(p6_cf_session *s, int trial, int which, float *out);
 p6_status p6_cf_last_ms(p6_cf_session *s, float *ms);
 p6_status p6_cf_launch_count(p6_cf_session *s, long long *count);
 /* Runs `cycles` cycles as separate launches with events between them and
- * returns the mean device time of one transform pass (one axis, every trial)
- * and of one reciprocal step; the R factors of these cycles are not kept. */
+ * returns the mean device time of one transform pass (one axis, every trial,
+ * all chunks) and of one reciprocal step; the R factors of these cycles are
+ * not kept. */
 p6_status p6_cf_time_kernels(p6_cf_session *s, int cycles, float *fft_pass_ms, float *reciprocal_ms);
 
 /* Philox4x32-10 of one (counter, key) on the device: known-answer check. */

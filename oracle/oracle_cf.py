@@ -62,6 +62,8 @@ class CfState:
         self.weak = None if weak is None else np.asarray(weak, bool)
         self.last_rho = None
         self.last_delta = None
+        self.pre_mag = None      # per grid point: |F| just before the amplitude constraint (NaN elsewhere)
+        self.fft_max = 0.0       # max |F| out of the forward transform
 
     def cycle(self) -> float:
         m, n = self.m, self.n
@@ -73,6 +75,8 @@ class CfState:
         self.last_rho, self.last_delta = re.copy(), delta
         flipped = np.where(re < delta, -re, re)
         F = np.fft.fftn(flipped.reshape(n, n, n)).ravel()
+        self.fft_max = float(np.abs(F).max())
+        self.pre_mag = np.full(F.size, np.nan)
         idx_all = m['orbitIdx']
         ph = m['phase'].astype(np.float64)
         num = den = 0.0
@@ -113,6 +117,7 @@ class CfState:
                     amp = math.sqrt(max(0.0, target) / cnt)
                     f = F[idx]
                     mag = np.abs(f)
+                    self.pre_mag[idx] = mag
                     out = np.empty_like(f)
                     live = mag > 1e-20
                     out[live] = f[live] * (amp / mag[live])
@@ -129,6 +134,19 @@ class CfState:
             self.best = F.copy()
         self.F = F
         return R
+
+    def tolerance(self, base: float, fft_rel: float) -> np.ndarray:
+        """Per grid point bound on |F_device - F_oracle| after the last cycle:
+        ``base`` plus, for a constrained member, the phase error the forward
+        transform's error (``fft_rel`` of its largest |F|) causes when the
+        member is rescaled from magnitude |F_pre| to its target: |F| times
+        min(2, 4 fft_rel max|F| / |F_pre|).  Small |F_pre| make the constraint
+        ill-conditioned; everything else is held to ``base``."""
+        amp = np.abs(self.F)
+        pm = self.pre_mag
+        cond = np.where(np.isfinite(pm), amp * np.minimum(2.0, 4 * fft_rel * self.fft_max / np.maximum(
+            np.nan_to_num(pm, nan=1.0), 1e-300)), 0.0)
+        return base + cond
 
     def ambiguous(self, band: float) -> int:
         """Points of the last flip within band * sigma of the threshold: where

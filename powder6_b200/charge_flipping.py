@@ -545,7 +545,13 @@ def run_charge_flipping(job: dict, device: int = 0, trials: Optional[Sequence[di
     base = {'threshold': float(job.get('thresholdSigma', 1.1)),
             'symLambda': min(1.0, max(0.0, float(job.get('symLambda') or 0.0))),
             'weakFraction': float(job.get('weakFraction') or 0.0), 'seed': int(job.get('seed', 1))}
-    specs = [dict(base, **t) for t in trials] if trials else [base]
+    specs = []
+    for t in (trials or [{}]):
+        spec = dict(base, **t)
+        if 'seed' not in t and 'seedSlot' in t:
+            # the seed of an adaptive start (js/rietveld/rv_solve.js:556)
+            spec['seed'] = (base['seed'] + int(t['seedSlot']) * 7919) & 0xFFFFFFFF
+        specs.append(spec)
     grouping = job.get('weakGrouping', 'cluster')
     dev_trials, weak_counts = [], []
     for t in specs:

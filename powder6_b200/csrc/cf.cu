@@ -124,26 +124,69 @@ __device__ __forceinline__ void tile_geometry(int axis, int tile, long long &bas
   }
 }
 
+// Bit reversal of i over log2(R) bits, at compile time.
+template <int R>
+__host__ __device__ constexpr int bitrev(int i) {
+  int r = 0;
+  for (int m = 1, k = R >> 1; m < R; m <<= 1, k >>= 1)
+    if (i & m) r |= k;
+  return r;
+}
+
+// In-register DFT of R points (R = 1, 2, 4, 8, 16): radix-2 decimation in
+// time from the bit-reversed order, fully unrolled.  tw[m] = exp(-+2 pi i m /
+// N); the DFT's own twiddle exp(-+2 pi i k / 2L) is tw[k (R / 2L) (N / R)].
+template <int R, int N>
+__device__ __forceinline__ void dft_regs(float2 (&a)[R], const float2 *tw) {
+  float2 b[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) b[bitrev<R>(i)] = a[i];
+#pragma unroll
+  for (int L = 1; L < R; L <<= 1) {
+#pragma unroll
+    for (int j = 0; j < R / 2; ++j) {
+      const int k = j & (L - 1), i0 = ((j - k) << 1) + k, i1 = i0 + L;
+      const float2 w = tw[k * (R / (2 * L)) * (N / R)];
+      const float2 c = make_float2(b[i1].x * w.x - b[i1].y * w.y, b[i1].x * w.y + b[i1].y * w.x);
+      b[i1] = make_float2(b[i0].x - c.x, b[i0].y - c.y);
+      b[i0] = make_float2(b[i0].x + c.x, b[i0].y + c.y);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) a[i] = b[i];
+}
+
 // One axis of the 3-D transform for every tile of every trial (in place).
 // Forward: F(h) = sum_x rho(x) exp(-2 pi i h x / n); inverse: the + sign, and
 // the 1/n^3 of the whole inverse transform applied by EPI_SCALE*.
+//
+// Each line of n = R1 R2 points (R1 = 8) is a four-step transform: with
+// x index R2 n1 + n2 and X index k1 + R1 k2,
+//   X[k1 + R1 k2] = sum_n2 W_R2^(n2 k2) W_n^(n2 k1) sum_n1 x[R2 n1 + n2] W_R1^(n1 k1).
+// Step 1 (a thread per line and n2) loads its R1 points straight from global
+// memory, transforms them in registers and applies W_n^(n2 k1); one exchange
+// through shared memory (rows padded against bank conflicts); step 2 (a
+// thread per line and k1) transforms over n2 in registers and stores.  Every
+// global access is a coalesced run: consecutive threads take consecutive
+// points of a line along x, and consecutive x (lines) along y and z.
 template <int N>
-__global__ void __launch_bounds__(kThreads) cf_fft_kernel(const Params P, float2 *data, int axis, int inverse,
-                                                          int prologue, int epilogue) {
+__global__ void __launch_bounds__(kThreads, 4) cf_fft_kernel(const Params P, float2 *data, int trialBase, int axis,
+                                                             int inverse, int prologue, int epilogue) {
   constexpr int XT = tile_lines(N);
-  constexpr int LOGN = N == 8 ? 3 : N == 16 ? 4 : N == 32 ? 5 : N == 64 ? 6 : 7;
-  constexpr int LD = N + 1;   // padded line stride
-  __shared__ float2 s[XT * LD];
-  __shared__ float2 tw[N / 2];
+  constexpr int R1 = N < 8 ? N : 8, R2 = N / R1;
+  constexpr int ROW = R1 + 1;          // exchange row of one n2, padded
+  constexpr int LD = R2 * ROW + 1;     // one line, padded
+  __shared__ float2 y[XT * LD];
+  __shared__ float2 tw[N];
   __shared__ double red[2 * kWarps];
   __shared__ float sDelta;
   __shared__ int sKeep;
-  const int tid = threadIdx.x, tile = blockIdx.x, trial = blockIdx.y;
+  const int tid = threadIdx.x, tile = blockIdx.x, trial = trialBase + blockIdx.y;
   float2 *g = data + (long long)trial * P.cells;
   long long base, eS;
   int tS;
   tile_geometry<N>(axis, tile, base, tS, eS);
-  for (int m = tid; m < N / 2; m += kThreads) {
+  for (int m = tid; m < N; m += kThreads) {
     float sn, cs;
     sincospif(2.0f * (float)m / (float)N, &sn, &cs);
     tw[m] = make_float2(cs, inverse ? sn : -sn);
@@ -168,56 +211,49 @@ __global__ void __launch_bounds__(kThreads) cf_fft_kernel(const Params P, float2
   __syncthreads();
   float2 *keep = sKeep ? P.best + (long long)trial * P.cells : nullptr;
   const float delta = sDelta;
-  for (int i = tid; i < XT * N; i += kThreads) {
-    int t, e;
-    if (axis == 0) {
-      t = i / N;
-      e = i % N;
-    } else {
-      t = i % XT;
-      e = i / XT;
+  for (int vt = tid; vt < XT * R2; vt += kThreads) {
+    const int t = axis == 0 ? vt / R2 : vt % XT, n2 = axis == 0 ? vt % R2 : vt / XT;
+    const long long lineBase = base + (long long)t * tS;
+    float2 a[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) a[n1] = g[lineBase + (long long)(R2 * n1 + n2) * eS];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+      if (keep) keep[lineBase + (long long)(R2 * n1 + n2) * eS] = a[n1];
+      if (prologue == PRO_FLIP) {
+        float re = a[n1].x;
+        if (re < delta) re = -re;
+        a[n1] = make_float2(re, 0.f);
+      }
     }
-    const long long off = base + (long long)t * tS + (long long)e * eS;
-    float2 v = g[off];
-    if (keep) keep[off] = v;
-    if (prologue == PRO_FLIP) {
-      float re = v.x;
-      if (re < delta) re = -re;
-      v = make_float2(re, 0.f);
-    }
-    s[t * LD + (int)(__brev((unsigned)e) >> (32 - LOGN))] = v;
-  }
-  for (int L = 1; L < N; L <<= 1) {
-    __syncthreads();
-    for (int b = tid; b < XT * (N / 2); b += kThreads) {
-      const int t = b / (N / 2), j = b % (N / 2), k = j & (L - 1), i0 = ((j - k) << 1) + k, i1 = i0 + L;
-      const float2 w = tw[k * (N / (2 * L))];
-      const float2 a = s[t * LD + i0], c = s[t * LD + i1];
-      const float2 cw = make_float2(c.x * w.x - c.y * w.y, c.x * w.y + c.y * w.x);
-      s[t * LD + i0] = make_float2(a.x + cw.x, a.y + cw.y);
-      s[t * LD + i1] = make_float2(a.x - cw.x, a.y - cw.y);
+    dft_regs<R1, N>(a, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      const float2 w = tw[(n2 * k1) & (N - 1)];
+      y[t * LD + n2 * ROW + k1] = make_float2(a[k1].x * w.x - a[k1].y * w.y, a[k1].x * w.y + a[k1].y * w.x);
     }
   }
   __syncthreads();
   const float scale = epilogue != EPI_NONE ? 1.0f / (float)P.cells : 1.0f;
   double sa = 0, sb = 0;
-  for (int i = tid; i < XT * N; i += kThreads) {
-    int t, e;
-    if (axis == 0) {
-      t = i / N;
-      e = i % N;
-    } else {
-      t = i % XT;
-      e = i / XT;
+  for (int vt = tid; vt < XT * R1; vt += kThreads) {
+    const int t = axis == 0 ? vt / R1 : vt % XT, k1 = axis == 0 ? vt % R1 : vt / XT;
+    const long long lineBase = base + (long long)t * tS;
+    float2 a[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) a[n2] = y[t * LD + n2 * ROW + k1];
+    dft_regs<R2, N>(a, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      float2 x = a[k2];
+      if (epilogue != EPI_NONE) {
+        x.x *= scale;
+        x.y *= scale;
+      }
+      g[lineBase + (long long)(k1 + R1 * k2) * eS] = x;
+      sa += (double)x.x;
+      sb += (double)x.x * (double)x.x;
     }
-    float2 v = s[t * LD + e];
-    if (epilogue != EPI_NONE) {
-      v.x *= scale;
-      v.y *= scale;
-    }
-    g[base + (long long)t * tS + (long long)e * eS] = v;
-    sa += (double)v.x;
-    sb += (double)v.x * (double)v.x;
   }
   if (epilogue == EPI_SCALE_MOMENTS) {
     block_sum2(sa, sb, red);
@@ -225,15 +261,109 @@ __global__ void __launch_bounds__(kThreads) cf_fft_kernel(const Params P, float2
   }
 }
 
+// The common case of the reciprocal step: a cluster whose orbits are
+// consecutive in the member table and hold at most 32 members together.  Each
+// lane keeps one member's F in registers through the R terms, repartition,
+// symmetrisation and constraint (per-orbit sums by shuffles), so the grid is
+// read and written once.  Same arithmetic as the general path below.
+__device__ __forceinline__ bool cluster_in_registers(const Params &P, float2 *g, int c, int o0, int no, double obs,
+                                                     int lane, float lam, bool doSym, uint32_t seed,
+                                                     const uint8_t *weak, double &dSum, double &tSum) {
+  if (no > 32) return false;
+  const int m0 = (int)P.orbitStart[o0];
+  // lane j < no reads orbit o0 + j; the members must be consecutive and few
+  int myStart = 0, myCnt = 0;
+  if (lane < no) {
+    myStart = (int)P.orbitStart[o0 + lane];
+    myCnt = (int)P.orbitCount[o0 + lane];
+  }
+  int end = myStart + myCnt;
+  const int prevEnd = __shfl_up_sync(0xffffffffu, end, 1);
+  const bool chain = lane == 0 || lane >= no || myStart == prevEnd;
+  if (!__all_sync(0xffffffffu, chain)) return false;
+  const int total_m = __shfl_sync(0xffffffffu, end, no - 1) - m0;
+  if (total_m > 32) return false;
+  // this lane's member and its orbit (local index j)
+  const bool live = lane < total_m;
+  const int p = m0 + lane;
+  int j = 0;
+  for (int q = 1; q < no; ++q)
+    if (p >= __shfl_sync(0xffffffffu, myStart, q)) j = q;
+  const int cnt = __shfl_sync(0xffffffffu, myCnt, j);
+  uint32_t word = 0, idx = 0;
+  float2 f = make_float2(0.f, 0.f);
+  float cr = 0.f, ci = 0.f;
+  if (live) {
+    word = P.orbitIdx[p];
+    idx = word & kIdxMask;
+    f = g[idx];
+    cr = P.phase[2 * p];
+    ci = P.phase[2 * p + 1];
+  }
+  const double f2 = live ? (double)f.x * f.x + (double)f.y * f.y : 0.0;
+  const double total = warp_sum(f2);
+  const double tObs = sqrt(fmax(0.0, obs));
+  dSum += fabs(sqrt(fmax(0.0, total)) - tObs);
+  tSum += tObs;
+  // per-orbit |F|^2 and, for the symmetrisation, the reduced sums
+  const float b0 = (word & kConjBit) ? -f.y : f.y;
+  const float rr = live ? f.x * cr + b0 * ci : 0.f, ri = live ? b0 * cr - f.x * ci : 0.f;
+  double so = 0;
+  float sr = 0.f, si = 0.f;
+  for (int q = 0; q < no; ++q) {
+    const bool mine = live && j == q;
+    const double sq = warp_sum(mine ? f2 : 0.0);
+    if (j == q) so = sq;
+    if (doSym) {
+      const float a = warp_sumf(mine ? rr : 0.f), b = warp_sumf(mine ? ri : 0.f);
+      if (j == q) {
+        sr = a;
+        si = b;
+      }
+    }
+  }
+  if (!live) return true;
+  const double members = (double)total_m;
+  const double target = total > 1e-20 ? so * (obs / total) : (members > 0 ? obs * cnt / members : 0.0);
+  if (doSym && cnt >= 2) {
+    const float inv = 1.0f / (float)cnt;
+    sr *= inv;
+    si *= inv;
+    const float a = sr * cr - si * ci;
+    float b = sr * ci + si * cr;
+    if (word & kConjBit) b = -b;
+    f = make_float2(f.x * (1.f - lam) + a * lam, f.y * (1.f - lam) + b * lam);
+  }
+  if (weak && weak[o0 + j]) {
+    const uint32_t n = (uint32_t)P.n, h = idx % n, k = (idx / n) % n, l = idx / (n * n);
+    const uint32_t mate = (n - h) % n + ((n - k) % n) * n + ((n - l) % n) * n * n;
+    f = idx > mate ? make_float2(f.y, -f.x) : make_float2(-f.y, f.x);
+  } else {
+    const float amp = (float)sqrt(fmax(0.0, target) / (double)cnt);
+    const float m = sqrtf(f.x * f.x + f.y * f.y);
+    if (m > 1e-20f) {
+      const float sc = amp / m;
+      f = make_float2(f.x * sc, f.y * sc);
+    } else {
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)p, 0x43465246u, 0u, 0u), make_uint2(seed, 0x52535452u));
+      float sn, cs;
+      sincospif(2.0f * u01(r.x), &sn, &cs);
+      f = make_float2(amp * cs, amp * sn);
+    }
+  }
+  g[idx] = f;
+  return true;
+}
+
 // The reciprocal-space half of a cycle (charge_flipping.wgsl reduce_rfactor,
 // repartition, symmetrize, constrain, zero_absent, zero_dc, finalize_rfactor,
 // keep_best's comparison and commit_best).  The member sets of different
 // clusters, the absent list and F(000) are disjoint, so one warp per cluster
 // applies the reference's global kernel order exactly within its cluster.
-__global__ void __launch_bounds__(kThreads) cf_reciprocal_kernel(const Params P) {
+__global__ void __launch_bounds__(kThreads) cf_reciprocal_kernel(const Params P, int trialBase) {
   __shared__ double red[2 * kWarps];
   __shared__ int sLast;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, trial = blockIdx.y;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, trial = trialBase + blockIdx.y;
   float2 *g = P.grid + (long long)trial * P.cells;
   const float lamRaw = P.symLambda[trial];
   const float lam = fminf(fmaxf(lamRaw, 0.f), 1.f);
@@ -244,6 +374,7 @@ __global__ void __launch_bounds__(kThreads) cf_reciprocal_kernel(const Params P)
   for (int c = blockIdx.x * kWarps + warp; c < P.nClusters; c += gridDim.x * kWarps) {
     const int o0 = (int)P.clusterOrbitStart[c], no = (int)P.clusterNOrbits[c];
     const double obs = (double)P.clusterObs[c];
+    if (cluster_in_registers(P, g, c, o0, no, obs, lane, lam, lamRaw > 0.f, seed, weak, dSum, tSum)) continue;
     double total = 0, members = 0;
     for (int o = o0; o < o0 + no; ++o) {
       const int st = (int)P.orbitStart[o], cnt = (int)P.orbitCount[o];
@@ -333,14 +464,17 @@ __global__ void __launch_bounds__(kThreads) cf_reciprocal_kernel(const Params P)
     sLast = ticket == gridDim.x - 1 ? 1 : 0;
   }
   __syncthreads();
-  if (sLast && tid == 0) {
-    __threadfence();
-    double a = 0, b = 0;
-    for (unsigned i = 0; i < gridDim.x; ++i) {
-      const double2 v = __ldcg(&P.rPartial[(long long)trial * gridDim.x + i]);
-      a += v.x;
-      b += v.y;
-    }
+  if (!sLast) return;
+  // the last CTA of this trial: every partial is visible; sum them in a fixed order
+  __threadfence();
+  double a = 0, b = 0;
+  for (unsigned i = tid; i < gridDim.x; i += kThreads) {
+    const double2 v = __ldcg(&P.rPartial[(long long)trial * gridDim.x + i]);
+    a += v.x;
+    b += v.y;
+  }
+  block_sum2(a, b, red);
+  if (tid == 0) {
     const float R = b > 0 ? (float)(a / b) : NAN;
     const int cyc = P.cycleCount[trial];
     if (cyc < P.historyCap) P.history[(long long)trial * P.historyCap + cyc] = R;
@@ -418,29 +552,48 @@ p6_status cf_upload(p6_cf_session *s, const T **out, const T *src, size_t count)
   return P6_OK;
 }
 
-// Launches one axis of the transform for `trials` trials of `data`.
-void launch_fft(const Params &P, float2 *data, int trials, int axis, int inverse, int prologue, int epilogue,
-                cudaStream_t stream) {
+// Launches one axis of the transform for trials [t0, t0 + trials) of `data`.
+void launch_fft(const Params &P, float2 *data, int t0, int trials, int axis, int inverse, int prologue,
+                int epilogue, cudaStream_t stream) {
   const dim3 grid(P.tiles, trials);
   switch (P.n) {
-    case 8: cf_fft_kernel<8><<<grid, kThreads, 0, stream>>>(P, data, axis, inverse, prologue, epilogue); break;
-    case 16: cf_fft_kernel<16><<<grid, kThreads, 0, stream>>>(P, data, axis, inverse, prologue, epilogue); break;
-    case 32: cf_fft_kernel<32><<<grid, kThreads, 0, stream>>>(P, data, axis, inverse, prologue, epilogue); break;
-    case 64: cf_fft_kernel<64><<<grid, kThreads, 0, stream>>>(P, data, axis, inverse, prologue, epilogue); break;
-    default: cf_fft_kernel<128><<<grid, kThreads, 0, stream>>>(P, data, axis, inverse, prologue, epilogue); break;
+    case 8: cf_fft_kernel<8><<<grid, kThreads, 0, stream>>>(P, data, t0, axis, inverse, prologue, epilogue); break;
+    case 16: cf_fft_kernel<16><<<grid, kThreads, 0, stream>>>(P, data, t0, axis, inverse, prologue, epilogue); break;
+    case 32: cf_fft_kernel<32><<<grid, kThreads, 0, stream>>>(P, data, t0, axis, inverse, prologue, epilogue); break;
+    case 64: cf_fft_kernel<64><<<grid, kThreads, 0, stream>>>(P, data, t0, axis, inverse, prologue, epilogue); break;
+    default:
+      cf_fft_kernel<128><<<grid, kThreads, 0, stream>>>(P, data, t0, axis, inverse, prologue, epilogue);
+      break;
   }
 }
 
-// The seven launches of one cycle, on `stream`.
+// Trials per chunk: a chunk's grids (at most 32 MB, a quarter of L2) stay in
+// L2 through its seven launches, so a cycle reads and writes each grid in
+// HBM about once instead of once per pass.
+int chunk_trials(const Params &P) {
+  const long long bytes = P.cells * (long long)sizeof(float2);
+  return (int)std::max<long long>(1, std::min<long long>(P.nTrials, (32LL << 20) / bytes));
+}
+
+// The seven launches of one cycle for every chunk of trials, on `stream`.
 void enqueue_cycle(const p6_cf_session *s) {
   const Params &P = s->P;
-  launch_fft(P, P.grid, P.nTrials, 0, 1, PRO_KEEP, EPI_NONE, s->stream);
-  launch_fft(P, P.grid, P.nTrials, 1, 1, PRO_NONE, EPI_NONE, s->stream);
-  launch_fft(P, P.grid, P.nTrials, 2, 1, PRO_NONE, EPI_SCALE_MOMENTS, s->stream);
-  launch_fft(P, P.grid, P.nTrials, 2, 0, PRO_FLIP, EPI_NONE, s->stream);
-  launch_fft(P, P.grid, P.nTrials, 1, 0, PRO_NONE, EPI_NONE, s->stream);
-  launch_fft(P, P.grid, P.nTrials, 0, 0, PRO_NONE, EPI_NONE, s->stream);
-  cf_reciprocal_kernel<<<dim3(s->recipCtas, P.nTrials), kThreads, 0, s->stream>>>(P);
+  const int chunk = chunk_trials(P);
+  for (int t0 = 0; t0 < P.nTrials; t0 += chunk) {
+    const int nt = std::min(chunk, P.nTrials - t0);
+    launch_fft(P, P.grid, t0, nt, 0, 1, PRO_KEEP, EPI_NONE, s->stream);
+    launch_fft(P, P.grid, t0, nt, 1, 1, PRO_NONE, EPI_NONE, s->stream);
+    launch_fft(P, P.grid, t0, nt, 2, 1, PRO_NONE, EPI_SCALE_MOMENTS, s->stream);
+    launch_fft(P, P.grid, t0, nt, 2, 0, PRO_FLIP, EPI_NONE, s->stream);
+    launch_fft(P, P.grid, t0, nt, 1, 0, PRO_NONE, EPI_NONE, s->stream);
+    launch_fft(P, P.grid, t0, nt, 0, 0, PRO_NONE, EPI_NONE, s->stream);
+    cf_reciprocal_kernel<<<dim3(s->recipCtas, nt), kThreads, 0, s->stream>>>(P, t0);
+  }
+}
+
+int launches_per_cycle(const Params &P) {
+  const int chunk = chunk_trials(P);
+  return 7 * ((P.nTrials + chunk - 1) / chunk);
 }
 
 p6_status capture_cycle(p6_cf_session *s) {
@@ -644,7 +797,7 @@ p6_status p6_cf_run(p6_cf_session *s, int cycles, float *r_history) {
   P6_CUDA(cudaGetLastError());
   P6_CUDA(cudaMemsetAsync(P.pending, 0, P.nTrials * sizeof(int), s->stream));
   P6_CUDA(cudaEventRecord(s->ev1, s->stream));
-  s->launches += 7LL * cycles + 1;
+  s->launches += (long long)launches_per_cycle(P) * cycles + 1;
   std::vector<float> hist;
   if (r_history && cycles > 0) {
     hist.resize((size_t)P.nTrials * P.historyCap);
@@ -683,9 +836,9 @@ p6_status p6_cf_read(p6_cf_session *s, int trial, int which, float *out) {
     return wait_stream(s, 60.0);
   }
   P6_CUDA(cudaMemcpyAsync(s->scratch, P.best + (size_t)trial * P.cells, bytes, cudaMemcpyDeviceToDevice, s->stream));
-  launch_fft(P, s->scratch, 1, 0, 1, PRO_NONE, EPI_NONE, s->stream);
-  launch_fft(P, s->scratch, 1, 1, 1, PRO_NONE, EPI_NONE, s->stream);
-  launch_fft(P, s->scratch, 1, 2, 1, PRO_NONE, EPI_SCALE, s->stream);
+  launch_fft(P, s->scratch, 0, 1, 0, 1, PRO_NONE, EPI_NONE, s->stream);
+  launch_fft(P, s->scratch, 0, 1, 1, 1, PRO_NONE, EPI_NONE, s->stream);
+  launch_fft(P, s->scratch, 0, 1, 2, 1, PRO_NONE, EPI_SCALE, s->stream);
   P6_CUDA(cudaGetLastError());
   s->launches += 3;
   P6_CUDA(cudaMemcpy2DAsync(out, sizeof(float), s->scratch, sizeof(float2), sizeof(float), (size_t)P.cells,
@@ -711,31 +864,35 @@ p6_status p6_cf_time_kernels(p6_cf_session *s, int cycles, float *fft_pass_ms, f
   P6_CUDA(cudaEventCreate(&ec));
   double fft = 0, rec = 0;
   p6_status st = P6_OK;
-  for (int c = 0; c < cycles && st == P6_OK; ++c) {
-    cudaEventRecord(ea, s->stream);
-    launch_fft(P, P.grid, P.nTrials, 0, 1, PRO_KEEP, EPI_NONE, s->stream);
-    launch_fft(P, P.grid, P.nTrials, 1, 1, PRO_NONE, EPI_NONE, s->stream);
-    launch_fft(P, P.grid, P.nTrials, 2, 1, PRO_NONE, EPI_SCALE_MOMENTS, s->stream);
-    launch_fft(P, P.grid, P.nTrials, 2, 0, PRO_FLIP, EPI_NONE, s->stream);
-    launch_fft(P, P.grid, P.nTrials, 1, 0, PRO_NONE, EPI_NONE, s->stream);
-    launch_fft(P, P.grid, P.nTrials, 0, 0, PRO_NONE, EPI_NONE, s->stream);
-    cudaEventRecord(eb, s->stream);
-    cf_reciprocal_kernel<<<dim3(s->recipCtas, P.nTrials), kThreads, 0, s->stream>>>(P);
-    cudaEventRecord(ec, s->stream);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) { st = cuda_error(e, "kernel launch"); break; }
-    st = wait_stream(s, 60.0);
-    float a = 0, b = 0;
-    cudaEventElapsedTime(&a, ea, eb);
-    cudaEventElapsedTime(&b, eb, ec);
-    fft += a;
-    rec += b;
-    s->launches += 7;
-  }
+  const int chunk = chunk_trials(P);
+  for (int c = 0; c < cycles && st == P6_OK; ++c)
+    for (int t0 = 0; t0 < P.nTrials && st == P6_OK; t0 += chunk) {
+      const int nt = std::min(chunk, P.nTrials - t0);
+      cudaEventRecord(ea, s->stream);
+      launch_fft(P, P.grid, t0, nt, 0, 1, PRO_KEEP, EPI_NONE, s->stream);
+      launch_fft(P, P.grid, t0, nt, 1, 1, PRO_NONE, EPI_NONE, s->stream);
+      launch_fft(P, P.grid, t0, nt, 2, 1, PRO_NONE, EPI_SCALE_MOMENTS, s->stream);
+      launch_fft(P, P.grid, t0, nt, 2, 0, PRO_FLIP, EPI_NONE, s->stream);
+      launch_fft(P, P.grid, t0, nt, 1, 0, PRO_NONE, EPI_NONE, s->stream);
+      launch_fft(P, P.grid, t0, nt, 0, 0, PRO_NONE, EPI_NONE, s->stream);
+      cudaEventRecord(eb, s->stream);
+      cf_reciprocal_kernel<<<dim3(s->recipCtas, nt), kThreads, 0, s->stream>>>(P, t0);
+      cudaEventRecord(ec, s->stream);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) { st = cuda_error(e, "kernel launch"); break; }
+      st = wait_stream(s, 60.0);
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, ea, eb);
+      cudaEventElapsedTime(&b, eb, ec);
+      fft += a;
+      rec += b;
+      s->launches += 7;
+    }
   cudaEventDestroy(ea);
   cudaEventDestroy(eb);
   cudaEventDestroy(ec);
   if (st != P6_OK) return st;
+  // per pass over every trial, and per reciprocal step over every trial
   *fft_pass_ms = (float)(fft / (6.0 * cycles));
   *reciprocal_ms = (float)(rec / cycles);
   return P6_OK;
