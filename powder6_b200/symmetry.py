@@ -225,6 +225,11 @@ _WYCKOFF: Dict[str, List[Tuple[str, int, str]]] = {
                  ('j', 12, '1/2,y,y'), ('i', 12, '0,y,y'), ('h', 12, 'x,1/2,0'), ('g', 8, 'x,x,x'),
                  ('f', 6, 'x,1/2,1/2'), ('e', 6, 'x,0,0'), ('d', 3, '1/2,0,0'), ('c', 3, '0,1/2,1/2'),
                  ('b', 1, '1/2,1/2,1/2'), ('a', 1, '0,0,0')],
+    '-P 4 2': [('u', 16, 'x,y,z'), ('t', 8, 'x,1/2,z'), ('s', 8, 'x,0,z'), ('r', 8, 'x,x,z'), ('q', 8, 'x,y,1/2'),
+               ('p', 8, 'x,y,0'), ('o', 4, 'x,1/2,1/2'), ('n', 4, 'x,1/2,0'), ('m', 4, 'x,0,1/2'),
+               ('l', 4, 'x,0,0'), ('k', 4, 'x,x,1/2'), ('j', 4, 'x,x,0'), ('i', 4, '0,1/2,z'), ('h', 2, '1/2,1/2,z'),
+               ('g', 2, '0,0,z'), ('f', 2, '0,1/2,0'), ('e', 2, '0,1/2,1/2'), ('d', 1, '1/2,1/2,1/2'),
+               ('c', 1, '1/2,1/2,0'), ('b', 1, '0,0,1/2'), ('a', 1, '0,0,0')],
     '-R 3 2"': [('i', 36, 'x,y,z'), ('h', 18, 'x,-x,z'), ('g', 18, 'x,0,1/2'), ('f', 18, 'x,0,0'),
                 ('e', 9, '1/2,0,0'), ('d', 9, '1/2,0,1/2'), ('c', 6, '0,0,z'), ('b', 3, '0,0,1/2'),
                 ('a', 3, '0,0,0')],
@@ -238,6 +243,7 @@ SPACE_GROUPS: Dict[int, Tuple[str, str, str]] = {
     14: ('P2_1/c', '-P 2ybc', 'monoclinic'),
     15: ('C2/c', '-C 2yc', 'monoclinic'),
     62: ('Pnma', '-P 2ac 2n', 'orthorhombic'),
+    123: ('P4/mmm', '-P 4 2', 'tetragonal'),
     166: ('R-3m:H', '-R 3 2"', 'trigonal'),
     176: ('P6_3/m', '-P 6c', 'hexagonal'),
     221: ('Pm-3m', '-P 4 2 3', 'cubic'),

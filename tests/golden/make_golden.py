@@ -26,7 +26,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 # number -> Hall symbol of the setting pinned (International Tables standard settings;
 # monoclinic groups in unique axis b, cell choice 1)
-GROUPS = {1: 'P 1', 2: '-P 1', 12: '-C 2y', 14: '-P 2ybc', 15: '-C 2yc', 62: '-P 2ac 2n',
+GROUPS = {1: 'P 1', 2: '-P 1', 12: '-C 2y', 14: '-P 2ybc', 15: '-C 2yc', 62: '-P 2ac 2n', 123: '-P 4 2',
           166: '-R 3 2"', 176: '-P 6c', 221: '-P 4 2 3', 225: '-F 4 2 3'}
 ELEMENTS = ['H', 'C', 'N', 'O', 'Na', 'S', 'Cl', 'Pb', 'Ti', 'Fe']
 GENERIC = (0.1234, 0.3721, 0.5873)

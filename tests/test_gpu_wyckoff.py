@@ -466,6 +466,20 @@ def test_prune_keeps_the_better_half_and_finds_the_true_assignment():
     assert res.cpu_check['delta'] < 1e-5
 
 
+def test_search_over_the_enumerated_assignments_finds_the_true_one():
+    """Enumeration, then search: the twelve deduplicated PbSO4 assignments
+    (tetrahedral S kept off the inversion centres) share 4096 replicas by
+    free-parameter count, the prune keeps the better half, and the true
+    assignment wins with cc > 0.9."""
+    from powder6_b200.swarm_wyckoff import run_wyckoff_search
+    from test_wyckoff_assign import enumerated_pbso4_alternatives
+    alts, _ = enumerated_pbso4_alternatives()
+    P = wyckoff_problem(seed=1, extra_assignments=alts)
+    res = run_wyckoff_search(P, num_particles=4096, generations=4000, seed=5)
+    assert res.assignments == list(range(12)) and 0 in res.kept
+    assert res.best_assignment == 0 and res.best_cc > 0.9, (res.best_assignment, res.best_cc, res.per_assignment)
+
+
 def test_waves_cover_every_assignment():
     """256 replicas hold five assignments per wave: two waves, every
     assignment searched, the best over both reported."""
