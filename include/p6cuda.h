@@ -315,6 +315,13 @@ p6_status p6_pt_read_state(p6_pt_session *s, float *state, double *x, double *be
 p6_status p6_pt_synchronize(p6_pt_session *s, double timeout_seconds);
 p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms);
 p6_status p6_pt_launch_count(p6_pt_session *s, long long *count);
+/* CTAs per chain in the sweeps: 2 runs each chain on a two-CTA cluster (the
+ * pattern's tiles split between them, chi^2 combined through distributed
+ * shared memory), chosen at creation when twice the chains fit the SMs;
+ * 1 is one CTA per chain.  Trajectories differ between the two only by the
+ * order of the chi^2 sum. */
+p6_status p6_pt_set_split(p6_pt_session *s, int ctas_per_chain);
+p6_status p6_pt_get_split(p6_pt_session *s, int *ctas_per_chain);
 
 /* Least-squares finish after tempering (js/rietveld_core.js:1953-2140), in
  * FP64 on the device: patterns, the finite-difference Jacobian (fdStep

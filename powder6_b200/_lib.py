@@ -111,6 +111,8 @@ _SIGS = {
     'p6_pt_synchronize': (C.c_int, [_P, C.c_double]),
     'p6_pt_last_batch_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_pt_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    'p6_pt_set_split': (C.c_int, [_P, C.c_int]),
+    'p6_pt_get_split': (C.c_int, [_P, C.POINTER(C.c_int)]),
     'p6_pt_costs_static': (C.c_int, [_P, _P, C.c_int, _P, _P]),
     'p6_pt_model_costs': (C.c_int, [_P, _P, C.c_int, _P]),
     'p6_pt_normal': (C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double)]),

@@ -23,6 +23,7 @@
 //  * |F|^2 takes a warp per reflection with the lanes over the coset
 //    representatives; the phase is reduced to one turn in FP64 before the
 //    FP32 sine and cosine.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -319,6 +320,7 @@ struct Shared {
   double f[6];
   int valid;
   double warpChi[kWarps];
+  double chiPart;   // this CTA's share of chi^2 when a chain spans a cluster
   double chi;
 };
 
@@ -651,9 +653,14 @@ __device__ void solve_free_heights(const Params &P, const Shared &sh, const PK *
   __syncthreads();
 }
 
+// split = 2: the chain's evaluation spans a two-CTA cluster.  Both CTAs do
+// the reflection stage (identical inputs, identical results); the 32-point
+// tiles of the pattern alternate between them (rank r takes tiles
+// warp + kWarps (2 i + r)), and chi^2 = part(rank 0) + part(rank 1) in both,
+// through distributed shared memory.
 __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, float *h1, float *w2, int *act,
                            const double *tth, const double *yobs, const float *wobs, float *ycalc,
-                           double *nn = nullptr) {
+                           double *nn = nullptr, int split = 1, int rank = 0) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
   __syncthreads();
@@ -666,7 +673,7 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
   // --- pattern in warp tiles of 32 points, then chi^2 (FP64)
   double chi = 0.0;
   const double x0 = tth[0], x1 = tth[P.n - 1], zs = x1 > x0 ? 2.0 / (x1 - x0) : 0.0;
-  for (int base = warp * 32; base < P.n; base += kThreads) {
+  for (int base = (warp + rank * kWarps) * 32; base < P.n; base += split * kThreads) {
     const int i = base + lane;
     const bool in = i < P.n;
     const double x = in ? tth[i] : 0.0;
@@ -718,7 +725,18 @@ __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, fl
   if (tid == 0) {
     double t = 0;
     for (int w = 0; w < kWarps; ++w) t += sh.warpChi[w];
-    sh.chi = isfinite(t) ? t : INFINITY;
+    sh.chiPart = t;
+    if (split == 1) sh.chi = isfinite(t) ? t : INFINITY;
+  }
+  if (split == 2) {
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    cl.sync();
+    if (tid == 0) {
+      const double a = *cl.map_shared_rank(&sh.chiPart, 0), b = *cl.map_shared_rank(&sh.chiPart, 1);
+      const double t = a + b;
+      sh.chi = isfinite(t) ? t : INFINITY;
+    }
+    cl.sync();   // the peer's part is read before either CTA starts the next evaluation
   }
   __syncthreads();
   return sh.chi;
@@ -787,11 +805,13 @@ __global__ void __launch_bounds__(kThreads) pt_cost_kernel(const Params P, const
 
 // One sweep: the exchange of the previous sweep (if any), then `moves`
 // proposals with Metropolis.  in/out are the double-buffered chain states.
+// split = 2: a chain per two-CTA cluster (launched with cluster dimension
+// 2); both CTAs run the chain's logic identically and rank 0 writes it back.
 __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, const Chain *in, Chain *out, int moves,
-                                                            int exchangeParity, int bootstrap) {
+                                                            int exchangeParity, int bootstrap, int split) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ Shared sh;
-  __shared__ double xs[kMaxNv], cur;
+  __shared__ double xs[kMaxNv];
   __shared__ Chain st;
   const SmemLayout L = smem_layout(P.nRefl, P.n, P.stageObs);
   Peak *pk1 = reinterpret_cast<Peak *>(smem + L.pk1), *pk2 = reinterpret_cast<Peak *>(smem + L.pk2);
@@ -805,7 +825,8 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
     for (int i = threadIdx.x; i < P.n; i += kThreads) { t[i] = P.tth[i]; y[i] = P.y[i]; w[i] = P.w[i]; }
     tth = t; yobs = y; wobs = w;
   }
-  const int c = blockIdx.x, C = P.chains;
+  const int c = blockIdx.x / split, C = P.chains;
+  const int rank = split == 2 ? (int)cooperative_groups::this_cluster().block_rank() : 0;
   const double T = pow(P.maxTemp, (double)c / (double)(C - 1));
   if (threadIdx.x == 0) {
     st = in[c];
@@ -847,7 +868,7 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
     }
     __syncthreads();
     const double cost = evaluate(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nullptr,
-                                 P.method == 1 ? reinterpret_cast<double *>(smem + L.total) : nullptr);
+                                 P.method == 1 ? reinterpret_cast<double *>(smem + L.total) : nullptr, split, rank);
     if (threadIdx.x == 0) {
       st.proposalCost = cost;
       if (bootstrap) {
@@ -869,7 +890,7 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && rank == 0) {
     if (!bootstrap && moves > 0) st.sweep += 1;
     out[c] = st;
   }
@@ -1133,6 +1154,7 @@ struct p6_pt_session {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   Params P{};
   int smemSweep = 0, smemCost = 0;
+  int split = 1;            // CTAs per chain in the sweep (2: a two-CTA cluster)
   Chain *dChain[2] = {nullptr, nullptr};
   int curBuf = 0;
   int pendingParity = -1;   // exchange owed by the last sweep, applied at the start of the next
@@ -1197,6 +1219,8 @@ static p6_status pt_ensure_vectors(p6_pt_session *s, int n) {
 }
 
 extern "C" {
+
+static int pt_cluster_capacity(int smemBytes);
 
 p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out) {
   clear_error();
@@ -1303,6 +1327,13 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
     e = cudaFuncSetAttribute(pt_pattern64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smem64);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(pt_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s->smemCost);
   if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaFuncSetAttribute"); }
+  // chains that leave half the SMs idle span two-CTA clusters when the
+  // device can schedule every chain's cluster at once
+  {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (2 * pr->chains <= sms && pt_cluster_capacity(s->smemSweep) >= pr->chains) s->split = 2;
+  }
   for (int b = 0; b < 2; ++b) {
     e = cudaMalloc(&s->dChain[b], (size_t)pr->chains * sizeof(Chain));
     if (e != cudaSuccess) { pt_free(s); return cuda_error(e, "cudaMalloc chains"); }
@@ -1361,10 +1392,51 @@ p6_status p6_pt_initial(p6_pt_session *s, const double *vectors, int n_vectors) 
   return P6_OK;
 }
 
+// Two-CTA clusters of the sweep kernel the device can hold at once (0 when
+// the cluster launch is not possible with this shared memory).
+static int pt_cluster_capacity(int smemBytes) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smemBytes;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, pt_sweep_kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 // One sweep launch: exchange owed by the previous sweep, then `moves` proposals.
 static cudaError_t pt_launch_sweep(p6_pt_session *s, int moves, int parity, int bootstrap) {
   Chain *in = s->dChain[s->curBuf], *out = s->dChain[s->curBuf ^ 1];
-  pt_sweep_kernel<<<s->P.chains, kThreads, s->smemSweep, s->stream>>>(s->P, in, out, moves, parity, bootstrap);
+  const int split = s->split;
+  if (split == 1) {
+    pt_sweep_kernel<<<s->P.chains, kThreads, s->smemSweep, s->stream>>>(s->P, in, out, moves, parity, bootstrap, 1);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(s->P.chains * split);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = s->smemSweep;
+    cfg.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = split;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, pt_sweep_kernel, s->P, (const Chain *)in, out, moves, parity,
+                                             bootstrap, split);
+    if (e != cudaSuccess) return e;
+  }
   s->curBuf ^= 1;
   s->launches++;
   return cudaGetLastError();
@@ -1421,6 +1493,24 @@ p6_status p6_pt_read_state(p6_pt_session *s, float *state, double *x, double *be
       counters[4 * c + 2] = ch.swaps; counters[4 * c + 3] = ch.swapAttempts;
     }
   }
+  return P6_OK;
+}
+
+p6_status p6_pt_set_split(p6_pt_session *s, int ctas_per_chain) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  if (ctas_per_chain != 1 && ctas_per_chain != 2) return set_error(P6_ERR_INVALID_ARG, "1 or 2 CTAs per chain");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (ctas_per_chain == 2 && pt_cluster_capacity(s->smemSweep) < s->P.chains)
+    return set_error(P6_ERR_CAPACITY, "the device cannot hold every chain's two-CTA cluster at once");
+  s->split = ctas_per_chain;
+  return P6_OK;
+}
+
+p6_status p6_pt_get_split(p6_pt_session *s, int *ctas_per_chain) {
+  clear_error();
+  if (!s || !ctas_per_chain) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  *ctas_per_chain = s->split;
   return P6_OK;
 }
 

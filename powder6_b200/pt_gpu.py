@@ -349,6 +349,17 @@ class PTSession:
         check(self.lib.p6_pt_launch_count(self.h, C.byref(v)))
         return v.value
 
+    @property
+    def split(self) -> int:
+        """CTAs per chain in the sweeps (2: a two-CTA cluster per chain)."""
+        v = C.c_int()
+        check(self.lib.p6_pt_get_split(self.h, C.byref(v)))
+        return v.value
+
+    @split.setter
+    def split(self, ctas_per_chain: int):
+        check(self.lib.p6_pt_set_split(self.h, int(ctas_per_chain)))
+
 
 def create(ctx: PTContext, device: int = 0) -> PTSession:
     return PTSession(ctx, device)

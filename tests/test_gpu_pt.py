@@ -91,6 +91,32 @@ def test_batch_counters_and_monotone_best(nacl):
     assert launches >= sweeps + 1
 
 
+def test_two_cta_clusters_match_one_cta_chains(nacl):
+    """Sixteen chains leave most SMs idle, so the session sweeps each chain on
+    a two-CTA cluster.  The bootstrap chi^2 matches the cost kernel's to 1e-13
+    in both splits, and ten sweeps make the same Metropolis decisions: the
+    splits differ only in the order of the chi^2 sum."""
+    P, M, truth = nacl
+    xs = start_vectors(P, truth, 16, seed=21)
+    runs = {}
+    for split in (2, 1):
+        with PTSession(ctx_of(P, truth, chains=16, seed=4)) as s:
+            if split == 2:
+                assert s.split == 2
+            s.split = split
+            ref = np.array(s.costs(xs))
+            s.initial(xs)
+            s.batch(1, True)
+            _, _, c0, _ = s.exact_state()
+            assert np.max(np.abs(c0[:, 0] - ref) / ref) < 1e-13
+            s.batch(10)
+            runs[split] = s.exact_state()
+    x2, b2, c2, n2 = runs[2]
+    x1, b1, c1, n1 = runs[1]
+    assert np.array_equal(n2, n1)
+    assert np.allclose(x2, x1, rtol=1e-12, atol=0) and np.allclose(c2, c1, rtol=1e-12, atol=0)
+
+
 def test_determinism(nacl):
     P, M, truth = nacl
     x0 = start_vectors(P, truth, 1, seed=6)[0]
