@@ -289,6 +289,12 @@ typedef struct {
    * pattern minus the background (atoms unused, n_atoms may be 0; at most 64
    * envelope reflections). */
   int method;
+  /* Sample displacement and transparency (js/pt_gpu.js:169-171, :355): when
+   * set, the two full-vector entries after SL, HL (or after 'po', or after
+   * the background) are disp and transp, and every peak moves by
+   * (-disp 1e-3 cos(theta) + transp sin(2 theta)) degrees before the zero
+   * point. */
+  int has_shift;
 } p6_pt_problem;
 
 typedef struct p6_pt_session p6_pt_session;

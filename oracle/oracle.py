@@ -216,7 +216,8 @@ class PtProblem(C.Structure):
                 ('n', C.c_int), ('tth', C.c_void_p), ('y', C.c_void_p), ('w', C.c_void_p),
                 ('lambda1', C.c_double), ('lambda2', C.c_double), ('ratio', C.c_double), ('polK', C.c_double),
                 ('minFwhm', C.c_double), ('nBkg', C.c_int), ('dmin', C.c_double),
-                ('hasPo', C.c_int), ('poDir', C.c_double * 3), ('hasAsym', C.c_int), ('method', C.c_int)]
+                ('hasPo', C.c_int), ('poDir', C.c_double * 3), ('hasAsym', C.c_int), ('method', C.c_int),
+                ('hasShift', C.c_int)]
 
 
 class PtSetup(C.Structure):
@@ -276,6 +277,7 @@ class PtModel:
                 p.poDir[i] = float(po_dir[i])
         p.hasAsym = 1 if getattr(prob, 'asym', False) else 0
         p.method = prob.method_code if hasattr(prob, 'method_code') else 0
+        p.hasShift = 1 if getattr(prob, 'shift', False) else 0
         self.p = p
 
     def cost_full(self, v, with_pattern=False):

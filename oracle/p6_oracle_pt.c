@@ -74,6 +74,9 @@ typedef struct {
      * reflection's height is free and non-negative, solved by NNLS against
      * y - background (atoms unused) */
     int method;
+    /* sample displacement and transparency (js/pt_gpu.js:169-171, :355): the
+     * two full-vector entries after SL, HL (or 'po', or the background) */
+    int hasShift;
 } p6o_pt_problem;
 
 static const double GCONV = 0.023548200450309493;   /* sqrt(8 ln 2) / 100 */
@@ -282,6 +285,20 @@ static double inv_dsq_cell(const double *c6, double h, double k, double l, int *
 }
 
 #define AIDX(P) ((P)->hasAsym ? PT_BKG0 + (P)->nBkg + ((P)->hasPo ? 1 : 0) : -1)
+#define SIDX(P) ((P)->hasShift ? PT_BKG0 + (P)->nBkg + ((P)->hasPo ? 1 : 0) + ((P)->hasAsym ? 2 : 0) : -1)
+
+/* shift(t, disp, transp) of js/pt_gpu.js:355 in degrees: displacement
+ * -disp 1e-3 cos(theta), transparency transp sin(2 theta); 0 at theta = 90
+ * and wherever it is not finite (profile.js calculatePeakShift) */
+static double sample_shift(const p6o_pt_problem *P, const double *v, double t)
+{
+    if (!P->hasShift) return 0.0;
+    const double disp = v[SIDX(P)], transp = v[SIDX(P) + 1];
+    const double th = t * DEG2RAD / 2;
+    if (fabs(th - PI_ / 2) < 1e-6) return 0.0;
+    const double d = (-disp * 0.001 * cos(th) + transp * sin(2 * th)) / DEG2RAD;
+    return isfinite(d) ? d : 0.0;
+}
 
 /* Coefficients of the 1/d^2 form: aa, bb, cc, ab, bc, ac (the hk, kl, hl terms). */
 static void cell_form(const double *c6, double f[6])
@@ -423,7 +440,8 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
     if (!(dmin > 0)) {
         double lambda = P->lambda1;
         if (P->ratio > 1e-6 && P->lambda2 > 0) lambda = fmin(lambda, P->lambda2);
-        double margin = WIN_MAX + fabs(v[PT_ZERO]);
+        double margin = WIN_MAX + fabs(v[PT_ZERO]) +
+                        (P->hasShift ? (fabs(v[SIDX(P)]) * 0.001 + fabs(v[SIDX(P) + 1])) * R2D : 0.0);
         double upper = fmin(179.999999, P->tth[n - 1] + margin + .001);
         dmin = lambda / (2 * sin(upper * DEG2RAD / 2));
     }
@@ -476,7 +494,7 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
     for (int r = 0; r < nr; r++) {
         double bragg = tthR[r];
         if (!(isfinite(bragg) && bragg > 0 && bragg < 180)) continue;
-        double base = bragg + v[PT_ZERO];
+        double base = bragg + sample_shift(P, v, bragg) + v[PT_ZERO];
         prepare_tch_asym(base, base, v, P->minFwhm, AIDX(P), &p1[r]);
         double lo = base - p1[r].maxd, hi = base + p1[r].maxd;
         int start = lower_bound(P->tth, n, lo), stop = start;
@@ -494,11 +512,12 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
             double sin2 = sin(bragg * DEG2RAD / 2.0) * (P->lambda2 / P->lambda1);
             if (fabs(sin2) >= 1) continue;
             double tth2 = 2 * asin(sin2) / DEG2RAD;
-            double base2 = tth2 + v[PT_ZERO];
+            double base2 = tth2 + sample_shift(P, v, tth2) + v[PT_ZERO];
             prepare_tch_asym(base2, base2, v, P->minFwhm, AIDX(P), &p2[r]);
             /* prep1 of this reflection (built in the first pass even if its window missed the axis) */
             voigt_t ref1;
-            prepare_tch_asym(bragg + v[PT_ZERO], bragg + v[PT_ZERO], v, P->minFwhm, AIDX(P), &ref1);
+            const double base1 = bragg + sample_shift(P, v, bragg) + v[PT_ZERO];
+            prepare_tch_asym(base1, base1, v, P->minFwhm, AIDX(P), &ref1);
             double lpr = lp_factor(base2, P->polK) / lp_factor(ref1.x0, P->polK);
             w2[r] = P->ratio * ref1.area / p2[r].area * lpr;
             double lo = base2 - p2[r].maxd, hi = base2 + p2[r].maxd;
@@ -526,7 +545,7 @@ double p6o_pt_cost(const p6o_pt_problem *P, const double *v, double *ycalc, int 
     for (int r = 0; r < nr; r++) {
         if (!has1[r] && !has2[r]) continue;
         if (!isfinite(tthR[r])) continue;
-        double tc = tthR[r] + v[PT_ZERO];
+        double tc = tthR[r] + sample_shift(P, v, tthR[r]) + v[PT_ZERO];
         voigt_t ref1;
         prepare_tch_asym(tc, tc, v, P->minFwhm, AIDX(P), &ref1);
         double K = ref1.area;
@@ -751,11 +770,13 @@ double p6o_voigt_raw(double delta, double inv, double cL, double cG)
 /* (fdStep :526-538, defaultLimits :486-508, stepCap :511-524), Cholesky and */
 /* solveSPD (:1304-1335).  Parameters are identified by their full index.    */
 /* ------------------------------------------------------------------------ */
-enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO, K_SL, K_HL };
+enum { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO, K_SL, K_HL, K_DISP, K_TRANSP };
 
 static int kind_of(const p6o_pt_problem *P, int fi)
 {
     if (P->hasPo && fi == PT_BKG0 + P->nBkg) return K_PO;
+    if (P->hasShift && fi == SIDX(P)) return K_DISP;
+    if (P->hasShift && fi == SIDX(P) + 1) return K_TRANSP;
     if (P->hasAsym && fi == AIDX(P)) return K_SL;
     if (P->hasAsym && fi == AIDX(P) + 1) return K_HL;
     if (fi == PT_SCALE) return K_SCALE;
@@ -777,6 +798,8 @@ static double fd_step(int kind, double v)
     case K_ANGLE: return 1e-4;
     case K_ZERO: return 1e-4;
     case K_PO: return 1e-4;
+    case K_DISP: return 1e-2;
+    case K_TRANSP: return 1e-6;
     default: return fmax(1e-4 * a, 1e-5);
     }
 }
@@ -807,6 +830,8 @@ static double step_cap(int kind, double v)
     case K_ZERO: return 0.1;
     case K_PO: return 0.25;
     case K_SL: case K_HL: return 0.01;
+    case K_DISP: return 2;
+    case K_TRANSP: return 0.01;
     case K_PROFILE: case K_LORENTZ: return 0.5 * fmax(fabs(v), 5);
     default: return INFINITY;
     }

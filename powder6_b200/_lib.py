@@ -62,7 +62,7 @@ class P6PtProblem(C.Structure):
                 ('nv', C.c_int), ('index', C.c_void_p), ('lo', C.c_void_p), ('hi', C.c_void_p), ('scales', C.c_void_p),
                 ('cubic', C.c_int), ('chains', C.c_int), ('max_temp', C.c_double), ('seed', C.c_uint32),
                 ('has_po', C.c_int), ('eq_start', C.c_void_p), ('eq_hkl', C.c_void_p), ('po_dir', C.c_double * 3),
-                ('has_asym', C.c_int), ('method', C.c_int)]
+                ('has_asym', C.c_int), ('method', C.c_int), ('has_shift', C.c_int)]
 
 
 _P = C.c_void_p

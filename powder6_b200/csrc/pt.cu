@@ -98,6 +98,7 @@ struct Params {
   int *errFlag;
   int hasPo;             // March-Dollase factor on; r = v[PBKG0 + nBkg]
   int asymIdx;           // full index of SL (HL follows); -1: no asymmetry
+  int shiftIdx;          // full index of the displacement (transparency follows); -1: none
   int method;            // 0 Rietveld; 1 WPPF / Le Bail: heights free, solved per evaluation by NNLS
   const int *eqStart;    // nRefl + 1
   const int *eqHkl;      // 3 per equivalent
@@ -189,6 +190,16 @@ __device__ double asym_area(double a, double H, double cL, double cG, double R) 
   }
   return total;
 }
+// Sample displacement and transparency shift of a peak at 2-theta t
+// (js/pt_gpu.js:355, :169-171): (-disp 1e-3 cos(theta) + transp sin(2 theta))
+// in degrees, 0 at theta = 90 degrees and wherever it is not finite.
+__host__ __device__ inline double sample_shift(double t, double disp, double transp) {
+  const double th = t * kD2R * 0.5;
+  if (fabs(th - 0.5 * kPi) < 1e-6) return 0.0;
+  const double d = (-disp * 0.001 * cos(th) + transp * sin(2.0 * th)) / kD2R;
+  return isfinite(d) ? d : 0.0;
+}
+
 // prepareVoigt, TCH branch (js/profile.js:603-722): widths at tthPeak, centre
 // x0, the SL/HL asymmetry when asymIdx >= 0 (v[asymIdx] = SL, v[asymIdx + 1]
 // = HL).  Returns the area of the unit-height peak (analytic, plus the
@@ -400,7 +411,8 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
       if (live) {
         const double bragg = 2 * asin(sinT) * kR2D;
         if (line == 0) {
-          const double base = bragg + v[PZERO];
+          const double base =
+              bragg + (P.shiftIdx >= 0 ? sample_shift(bragg, v[P.shiftIdx], v[P.shiftIdx + 1]) : 0.0) + v[PZERO];
           area = prepare(v, P.minFwhm, base, base, P.asymIdx, pk1[k]);
           lp = lp_factor(base, P.polK);
           const int lo = lower_bound(tth, P.n, base - pk1[k].maxd), hi = upper_bound(tth, P.n, base + pk1[k].maxd, lo);
@@ -412,7 +424,9 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
           if (doublet) {
             const double sin2 = sin(bragg * kD2R / 2.0) * (P.lambda2 / P.lambda1);
             if (fabs(sin2) < 1) {
-              const double base2 = 2 * asin(sin2) / kD2R + v[PZERO];
+              const double b2 = 2 * asin(sin2) / kD2R;
+              const double base2 =
+                  b2 + (P.shiftIdx >= 0 ? sample_shift(b2, v[P.shiftIdx], v[P.shiftIdx + 1]) : 0.0) + v[PZERO];
               area = prepare(v, P.minFwhm, base2, base2, P.asymIdx, pk2[k]);
               lp = lp_factor(base2, P.polK);
               const int lo2 = lower_bound(tth, P.n, base2 - pk2[k].maxd),
@@ -1247,6 +1261,8 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
     if (!(pr->tth[i] > pr->tth[i - 1])) return set_error(P6_ERR_INVALID_ARG, "the 2-theta axis must be ascending");
   if (pr->has_asym && pr->n_full < PBKG0 + pr->n_bkg + (pr->has_po ? 1 : 0) + 2)
     return set_error(P6_ERR_INVALID_ARG, "asymmetry: the full vector has no SL, HL entries");
+  if (pr->has_shift && pr->n_full < PBKG0 + pr->n_bkg + (pr->has_po ? 1 : 0) + (pr->has_asym ? 2 : 0) + 2)
+    return set_error(P6_ERR_INVALID_ARG, "sample shift: the full vector has no displacement, transparency entries");
   if (pr->has_po) {
     if (!pr->eq_start || !pr->eq_hkl) return set_error(P6_ERR_INVALID_ARG, "preferred orientation without equivalents");
     if (pr->n_full < PBKG0 + pr->n_bkg + 1)
@@ -1297,6 +1313,7 @@ p6_status p6_pt_create(const p6_pt_problem *pr, int device, p6_pt_session **out)
   PT_TRY(pt_upload(s, pr->scales, (size_t)pr->nv, &P.scales));
   P.hasPo = pr->has_po ? 1 : 0;
   P.asymIdx = pr->has_asym ? PBKG0 + pr->n_bkg + P.hasPo : -1;
+  P.shiftIdx = pr->has_shift ? PBKG0 + pr->n_bkg + P.hasPo + (pr->has_asym ? 2 : 0) : -1;
   if (P.hasPo) {
     PT_TRY(pt_upload(s, pr->eq_start, (size_t)pr->n_refl + 1, &P.eqStart));
     PT_TRY(pt_upload(s, pr->eq_hkl, (size_t)3 * pr->eq_start[pr->n_refl], &P.eqHkl));
@@ -1553,10 +1570,12 @@ p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
 // the scalar control of lm() on the host.
 // ===========================================================================
 namespace {
-enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO, K_SL, K_HL };
+enum LmKind { K_SCALE, K_CELL, K_ANGLE, K_PROFILE, K_LORENTZ, K_ZERO, K_BISO, K_BKG, K_PO, K_SL, K_HL, K_DISP, K_TRANSP };
 
 int lm_kind(const Params &P, int fi) {
   if (P.hasPo && fi == PBKG0 + P.nBkg) return K_PO;
+  if (P.shiftIdx >= 0 && fi == P.shiftIdx) return K_DISP;
+  if (P.shiftIdx >= 0 && fi == P.shiftIdx + 1) return K_TRANSP;
   if (P.asymIdx >= 0 && fi == P.asymIdx) return K_SL;
   if (P.asymIdx >= 0 && fi == P.asymIdx + 1) return K_HL;
   if (fi == SCALE) return K_SCALE;
@@ -1574,6 +1593,8 @@ double lm_fd_step(int kind, double v) {
   switch (kind) {
     case K_CELL: return std::max(1e-6 * a, 1e-6);
     case K_ANGLE: case K_ZERO: case K_PO: return 1e-4;
+    case K_DISP: return 1e-2;
+    case K_TRANSP: return 1e-6;
     default: return std::max(1e-4 * a, 1e-5);
   }
 }
@@ -1601,6 +1622,8 @@ double lm_step_cap(int kind, double v) {
     case K_ZERO: return 0.1;
     case K_PO: return 0.25;
     case K_SL: case K_HL: return 0.01;
+    case K_DISP: return 2;
+    case K_TRANSP: return 0.01;
     case K_PROFILE: case K_LORENTZ: return 0.5 * std::max(std::fabs(v), 5.0);
     default: return std::numeric_limits<double>::infinity();
   }

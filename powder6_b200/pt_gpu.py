@@ -73,6 +73,10 @@ class PTProblem:
     # against the observed pattern minus the background (atoms unused; at most
     # 64 reflections in the envelope).
     method: str = 'rietveld'
+    # Sample displacement and transparency (js/pt_gpu.js:169-171, :355): when
+    # True, 'disp' and 'transp' are the full-vector entries after SL, HL (or
+    # after 'po', or after the background).
+    shift: bool = False
 
     @property
     def method_code(self) -> int:
@@ -97,6 +101,11 @@ class PTProblem:
             if not self.asym:
                 raise KeyError(f'{name}: the problem has no asymmetry')
             return len(FULL_NAMES) + self.n_bkg + (1 if self.po_dir is not None else 0) + (name == 'HL')
+        if name in ('disp', 'transp'):
+            if not self.shift:
+                raise KeyError(f'{name}: the problem has no sample shift')
+            return (len(FULL_NAMES) + self.n_bkg + (1 if self.po_dir is not None else 0) + (2 if self.asym else 0) +
+                    (name == 'transp'))
         return FULL_NAMES.index(name)
 
     def apply(self, x: Sequence[float]) -> np.ndarray:
@@ -125,12 +134,16 @@ def reflection_dmin(problem: PTProblem) -> float:
     lam = problem.lambda1
     if problem.ratio > 1e-6 and problem.lambda2 > 0:
         lam = min(lam, problem.lambda2)
-    zi = problem.full_index('zero')
-    zmax = abs(problem.values[zi])
-    if 'zero' in problem.refined:
-        j = problem.refined.index('zero')
-        zmax = max(abs(problem.lo[j]), abs(problem.hi[j]))
-    upper = min(179.999999, float(problem.tth[-1]) + PROFILE_WINDOW_MAX_DEG + zmax + .001)
+    def magnitude(name):
+        v = abs(problem.values[problem.full_index(name)])
+        if name in problem.refined:
+            j = problem.refined.index(name)
+            v = max(abs(problem.lo[j]), abs(problem.hi[j]))
+        return v
+    margin = PROFILE_WINDOW_MAX_DEG + magnitude('zero')
+    if problem.shift:
+        margin += (magnitude('disp') * 0.001 + magnitude('transp')) * 180.0 / math.pi
+    upper = min(179.999999, float(problem.tth[-1]) + margin + .001)
     return lam / (2 * math.sin(math.radians(upper) / 2))
 
 
@@ -238,6 +251,7 @@ class PTSession:
                 pr.po_dir[i] = float(P.po_dir[i])
         pr.has_asym = 1 if P.asym else 0
         pr.method = P.method_code
+        pr.has_shift = 1 if P.shift else 0
         h = C.c_void_p()
         check(self.lib.p6_pt_create(C.byref(pr), int(device), C.byref(h)))
         self.h = h
@@ -570,6 +584,26 @@ def with_asymmetry(prob: PTProblem, SL: float = 0.0, HL: float = 0.0, refine: Se
     return out
 
 
+def with_sample_shift(prob: PTProblem, disp: float = 0.0, transp: float = 0.0,
+                      refine: Sequence[str] = ('disp', 'transp'), bounds: Optional[Dict[str, tuple]] = None) -> PTProblem:
+    """A copy of ``prob`` with sample displacement and transparency
+    (js/pt_gpu.js:169-171, :355): 'disp' and 'transp' appended to the full
+    vector (after the background, 'po', SL and HL) and the names in
+    ``refine`` to the refined parameters, with ``bounds`` (default disp
+    [-100, 100], transp [-0.01, 0.01])."""
+    import copy
+    b = {'disp': (-100.0, 100.0), 'transp': (-0.01, 0.01)}
+    b.update(bounds or {})
+    out = copy.copy(prob)
+    out.shift = True
+    n0 = (len(FULL_NAMES) + prob.n_bkg + (1 if prob.po_dir is not None else 0) + (2 if prob.asym else 0))
+    out.values = np.concatenate([np.asarray(prob.values, dtype=np.float64)[:n0], [disp, transp]])
+    out.refined = list(prob.refined) + list(refine)
+    out.lo = np.concatenate([np.asarray(prob.lo, dtype=np.float64), [b[n][0] for n in refine]])
+    out.hi = np.concatenate([np.asarray(prob.hi, dtype=np.float64), [b[n][1] for n in refine]])
+    return out
+
+
 def set_bounds(prob: PTProblem, truth: np.ndarray):
     t = {n: truth[prob.full_index(n)] for n in prob.refined}
     lo = {'scale': 0.5 * t['scale'], 'a': 0.98 * t['a'], 'Biso': 0.0, 'U': 0.0, 'V': -20.0, 'W': 0.0, 'zero': -0.1}
@@ -612,7 +646,7 @@ def start_vectors(prob: PTProblem, truth_x: np.ndarray, n: int, seed: int = 1) -
 
 
 STEP_CAP = {'scale': None, 'a': 'cell', 'Biso': 2.0, 'U': 'profile', 'V': 'profile', 'W': 'profile', 'zero': 0.1,
-            'po': 0.25, 'SL': 0.01, 'HL': 0.01}
+            'po': 0.25, 'SL': 0.01, 'HL': 0.01, 'disp': 2.0, 'transp': 0.01}
 
 
 def natural_scales(prob: PTProblem, x: np.ndarray) -> np.ndarray:

@@ -369,3 +369,53 @@ def test_free_intensity_envelope_cap_is_enforced(nacl_wppf):
     x[ia] = 11.28
     with pytest.raises(RuntimeError, match='64'):
         PTSession(ctx_of(Pb, x, chains=2))
+
+
+# ---------------------------------------------------------------------------
+# Sample displacement and transparency (js/pt_gpu.js:169-171, :355), refined
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope='module')
+def nacl_shift(nacl, oracle):
+    from powder6_b200.pt_gpu import with_sample_shift
+    P, M, truth = nacl
+    Ps = with_sample_shift(P, 0.0, 0.0)
+    return Ps, oracle.PtModel(Ps, dmin=reflection_dmin(Ps)), np.append(truth, [30.0, 0.002])
+
+
+def test_sample_shift_costs_and_patterns_match_oracle(nacl_shift):
+    """Every peak (both lines) moved by the displacement and transparency
+    before the zero point: chi^2 within 2e-6 (FP32 profile) and 1e-10 (FP64
+    model), pattern within 2e-5 of its maximum, over disp -80 .. 80 and
+    transp -0.008 .. 0.008."""
+    P, M, x0 = nacl_shift
+    xs = [x0] + [np.append(v[:-2], a) for v, a in
+                 zip(start_vectors(P, x0, 4, seed=33), ([0.0, 0.0], [80.0, -0.008], [-80.0, 0.008], [10.0, 0.0]))]
+    with PTSession(ctx_of(P, x0, chains=len(xs))) as s:
+        g, ys = s.costs(xs, with_pattern=True)
+        c64 = s.model_costs(xs)
+    for x, gc, gm, y in zip(xs, g, c64, ys):
+        c, yo, _ = M.cost_full(P.apply(x), True)
+        assert abs(gc - c) <= CHI2_RTOL * c, (gc, c)
+        assert abs(gm - c) <= 1e-10 * c, (gm, c)
+        assert np.max(np.abs(y - yo)) <= PATTERN_ATOL_FRAC * np.max(np.abs(yo))
+
+
+def test_sample_shift_normal_equations_and_lm_match_oracle(nacl_shift):
+    """The displacement and transparency columns of J'WJ (forward
+    differences of 1e-2 and 1e-6) and the LM finish with their step caps (2
+    and 0.01) agree with the oracle."""
+    P, M, x0 = nacl_shift
+    x = near_truth(x0)
+    with PTSession(ctx_of(P, x0, chains=2)) as s:
+        A, g, f = s.normal(x)
+        xg, ig = s.lm(x, 30)
+    Ao, go, fo = M.normal(x)
+    assert abs(f - fo) <= 1e-10 * fo
+    d = np.sqrt(np.diag(Ao))
+    assert d[-1] > 0 and d[-2] > 0
+    assert np.max(np.abs(A - Ao) / np.outer(d, d)) < 1e-7
+    assert np.max(np.abs(g - go) / (d * math.sqrt(fo))) < 1e-7
+    xo, io = M.lm(x, 30)
+    assert ig['code'] == io['code'] and ig['accepted'] == io['accepted']
+    assert abs(ig['chi2'] - io['chi2']) <= 1e-9 * io['chi2']
+    assert np.allclose(xg, xo, rtol=1e-7, atol=1e-9)

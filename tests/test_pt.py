@@ -361,3 +361,44 @@ def test_free_intensity_pattern_is_the_nnls_fit(nacl, oracle):
     assert np.min(peaks) >= -1e-9 * np.max(np.abs(peaks))
     # the fit lowers chi^2 from the background alone
     assert c < np.sum(w * (P.y - bkg) ** 2)
+
+
+# ---------------------------------------------------------------------------
+# Sample displacement and transparency (js/pt_gpu.js:169-171, :355)
+# ---------------------------------------------------------------------------
+def test_sample_shift_reduces_to_plain_at_zero(nacl, oracle):
+    """disp = transp = 0 leaves every peak where it was: the same chi^2 bit
+    for bit; a displacement of 100 moves them."""
+    from powder6_b200.pt_gpu import with_sample_shift
+    P, M, truth = nacl
+    Ps = with_sample_shift(P, 0.0, 0.0)
+    Ms = oracle.PtModel(Ps, dmin=reflection_dmin(P))
+    assert Ms.cost(np.append(truth, [0.0, 0.0])) == M.cost(truth)
+    assert Ms.cost(np.append(truth, [100.0, 0.0])) > 1.05 * M.cost(truth)
+
+
+def test_sample_shift_is_a_local_zero_point(nacl, oracle):
+    """Near one isolated peak, displacement and transparency act as the zero
+    point (-disp 1e-3 cos(theta) + transp sin(2 theta)) in degrees at that
+    peak's Bragg angle: with the doublet off, the (200) peak of the shifted
+    pattern matches the unshifted one with that zero point to 2e-3 of its
+    height within +-0.3 degrees."""
+    import copy
+    from powder6_b200.pt_gpu import with_sample_shift
+    P, _, truth = nacl
+    P1 = copy.copy(P)
+    P1.ratio = 0.0
+    disp, transp = 60.0, 0.003
+    Ps = with_sample_shift(P1, disp, transp)
+    v = P1.apply(truth)
+    a = v[1]
+    bragg = 2 * math.degrees(math.asin(P1.lambda1 * 2 / (2 * a)))       # (200): d = a / 2
+    th = math.radians(bragg / 2)
+    dz = (-disp * 1e-3 * math.cos(th) + transp * math.sin(2 * th)) * 180 / math.pi
+    ys = oracle.PtModel(Ps, dmin=reflection_dmin(Ps)).cost_full(np.append(v, [disp, transp]), True)[1]
+    vz = v.copy()
+    vz[P1.full_index('zero')] += dz
+    yz = oracle.PtModel(P1, dmin=reflection_dmin(Ps)).cost_full(vz, True)[1]
+    sel = np.abs(P1.tth - (bragg + dz)) < 0.3
+    assert abs(dz) > 0.05
+    assert np.max(np.abs(ys[sel] - yz[sel])) <= 2e-3 * np.max(yz[sel])
