@@ -64,6 +64,8 @@ def parse():
                     help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
     ap.add_argument('--cf-trials', type=int, default=None, help='cf: random starts (default 128)')
     ap.add_argument('--cf-cycles', type=int, default=None, help='cf: cycles per step (default 100)')
+    ap.add_argument('--pt-method', default='rietveld', choices=['rietveld', 'wppf'],
+                    help='pt: heights from the structure (default) or free and solved by NNLS in every evaluation')
     ap.add_argument('--chains', type=int, default=64)
     ap.add_argument('--sweeps', type=int, default=2000)
     return ap.parse_args()
@@ -268,11 +270,14 @@ PT_WORKLOAD = ('pt-rietveld NaCl Fm-3m a=5.640 (Na 4a, Cl 4b, Biso 1.0), Cu Ka1/
                'from +/-5 % starts')
 
 
-def pt_setup(seed):
+def pt_setup(seed, method='rietveld'):
+    """The NaCl problem (observations synthesised from the structure), fitted
+    with the structure's heights ('rietveld') or free ones ('wppf')."""
     from oracle import oracle as O
     from powder6_b200.pt_gpu import nacl_problem, start_vectors, synthesise
     P = nacl_problem(seed=1)
     truth = synthesise(P, O.PtModel(P).pattern, seed=1)
+    P.method = method
     x0 = start_vectors(P, truth, 1, seed=seed)[0]
     return P, truth, x0
 
@@ -292,7 +297,7 @@ def run_reference_pt(args, world, rank):
         return
     from oracle import oracle as O
     from powder6_b200.pt_gpu import pt_scales, reflection_dmin
-    P, truth, x0 = pt_setup(5)
+    P, truth, x0 = pt_setup(5, args.pt_method)
     M = O.PtModel(P, dmin=reflection_dmin(P))
     sc = pt_scales(P, x0)
     chains, per_step = 16, 2
@@ -312,7 +317,7 @@ def run_reference_pt(args, world, rank):
         'impl': 'reference', 'metric': 'trial structures evaluated/s', 'value': v, 'unit': 'trials/s',
         'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000 * dt / args.steps,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-        'config': {'workload': PT_WORKLOAD + ' (sampled)'},
+        'config': {'workload': PT_WORKLOAD + ' (sampled)', 'method': args.pt_method},
         'cpu_baseline': {'value': v, 'unit': 'trials/s', 'cores': 1, 'kind': 'port', 'sample': sample},
         'e2e': {'value': v, 'unit': 'trials/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }), flush=True)
@@ -347,9 +352,9 @@ def main_pt(args, world, rank, local):
     import torch
     from powder6_b200.pt_gpu import PTContext, PTSession, pt_scales, refine
     torch.cuda.set_device(local)
-    P, truth, _ = pt_setup(5)
+    P, truth, _ = pt_setup(5, args.pt_method)
     target_rwp, target_chi2 = pt_target(P, truth)
-    starts = [pt_setup(10 + i + 100 * rank)[2] for i in range(args.warmup + args.steps)]
+    starts = [pt_setup(10 + i + 100 * rank, args.pt_method)[2] for i in range(args.warmup + args.steps)]
 
     def ctx_for(x0, seed):
         return PTContext(P, x0, {'chains': args.chains, 'sweeps': args.sweeps, 'maxTemp': 100.0, 'seed': seed,
@@ -392,7 +397,7 @@ def main_pt(args, world, rank, local):
             'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp32 profile, fp64 peaks and chi2', 'data': 'synthetic',
-            'config': {'workload': PT_WORKLOAD, 'chains': args.chains, 'sweeps': args.sweeps,
+            'config': {'workload': PT_WORKLOAD, 'method': args.pt_method, 'chains': args.chains, 'sweeps': args.sweeps,
                        'step': 'one tempering run (all sweeps) for value; one refine() for e2e',
                        'l2': 'flushed before every step (256 MB write)', 'parallelism': f'replicas only x{world}'},
             'time_to_target_rwp': {'median_s': float(np.median(reached)) if reached else None,

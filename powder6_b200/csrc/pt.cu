@@ -471,11 +471,26 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
 __host__ __device__ inline int nnls_bytes(int m) { return (2 * m * m + 8 * m) * 8; }
 constexpr int kMaxFreeRefl = 64;
 
+// Column k of the free-intensity design matrix at point i: the unit-height
+// K-alpha-1 peak plus w2 times the K-alpha-2 one.  FP32 peaks (the tempering
+// path) evaluate the shape exactly as the pattern does; FP64 peaks (the
+// least-squares path) in FP64.
+__device__ __forceinline__ float shape32(const Peak &p, double t) {
+  const float d = asym_deltaf((float)(t - p.x0), p.asym) * p.inv, dg = d * d;
+  const float val = p.cL * (1.0f / (1.0f + 4.0f * dg)) + p.cG * expf(-(float)kCg * dg) - p.pedestal;
+  return val > 0.f ? val : 0.f;
+}
+
 template <class PK, class HT>
 __device__ __forceinline__ double free_column(const PK *pk1, const PK *pk2, const HT *w2, const int *act, int k,
                                               int i, double t) {
   double c = 0;
   const int a = act[k];
+  if constexpr (std::is_same<PK, Peak>::value) {
+    if ((a & 1) && i >= pk1[k].lo && i < pk1[k].hi) c += (double)shape32(pk1[k], t);
+    if ((a & 2) && i >= pk2[k].lo && i < pk2[k].hi) c += (double)w2[k] * (double)shape32(pk2[k], t);
+    return c;
+  }
   if ((a & 1) && i >= pk1[k].lo && i < pk1[k].hi) {
     const PK &p = pk1[k];
     c += voigt64(asym_delta(t - p.x0, (double)p.asym), (double)p.inv, (double)p.cL, (double)p.cG, (double)p.pedestal);
@@ -531,13 +546,14 @@ __device__ void solve_free_heights(const Params &P, const Shared &sh, const PK *
       const double sk = sqrt(fmax(0.0, a));
       sc[k] = sk;
       rhs[k] = sk > 0 ? r / sk : 0.0;
+      H[k * m + k] = sk > 0 ? 1.0 : 0.0;   // a scaled column has unit norm
     }
   }
   __syncthreads();
   // H in the scaled columns: warp per pair j <= k, over the windows' overlap
   for (int pq = warp; pq < m * m; pq += nw) {
     const int j = pq / m, k = pq % m;
-    if (k < j) continue;
+    if (k <= j) continue;
     double hv = 0;
     if (sc[j] > 0 && sc[k] > 0) {
       int lj, hj, lk, hk;
