@@ -175,8 +175,13 @@ __global__ void __launch_bounds__(kThreads, 4) cf_fft_kernel(const Params P, flo
   constexpr int XT = tile_lines(N);
   constexpr int R1 = N < 8 ? N : 8, R2 = N / R1;
   constexpr int ROW = R1 + 1;          // exchange row of one n2, padded
-  constexpr int LD = R2 * ROW + 1;     // one line, padded
-  __shared__ float2 y[XT * LD];
+  constexpr int LDMAX = R2 * ROW + 1;
+  __shared__ float2 y[XT * LDMAX];
+  // line stride of the exchange: along x consecutive lanes walk n2 (or k1)
+  // within a line, and the unpadded stride R2 ROW keeps the lines a half-warp
+  // touches on disjoint 8-byte banks; along y and z consecutive lanes walk the
+  // lines, and R2 ROW + 1 does
+  const int ld = axis == 0 ? LDMAX - 1 : LDMAX;
   __shared__ float2 tw[N];
   __shared__ double red[2 * kWarps];
   __shared__ float sDelta;
@@ -230,7 +235,7 @@ __global__ void __launch_bounds__(kThreads, 4) cf_fft_kernel(const Params P, flo
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) {
       const float2 w = tw[(n2 * k1) & (N - 1)];
-      y[t * LD + n2 * ROW + k1] = make_float2(a[k1].x * w.x - a[k1].y * w.y, a[k1].x * w.y + a[k1].y * w.x);
+      y[t * ld + n2 * ROW + k1] = make_float2(a[k1].x * w.x - a[k1].y * w.y, a[k1].x * w.y + a[k1].y * w.x);
     }
   }
   __syncthreads();
@@ -241,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 4) cf_fft_kernel(const Params P, flo
     const long long lineBase = base + (long long)t * tS;
     float2 a[R2];
 #pragma unroll
-    for (int n2 = 0; n2 < R2; ++n2) a[n2] = y[t * LD + n2 * ROW + k1];
+    for (int n2 = 0; n2 < R2; ++n2) a[n2] = y[t * ld + n2 * ROW + k1];
     dft_regs<R2, N>(a, tw);
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) {
