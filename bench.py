@@ -812,8 +812,8 @@ def main_cf(args, world, rank, local):
     per cycle: six transform passes and the reciprocal step, every trial in
     each launch).  value: trial-cycles per second from CUDA events on the
     session's stream, grids resident; e2e: the same per step through the
-    public API with the starting grids uploaded (pinned-size host arrays,
-    set_grid), the run, the best R read back and the best trial's density
+    public API with the starting grids uploaded from pinned host memory
+    (set_grid), the run, the best R read back and the best trial's density
     map read back; the grids (128 x 2 MB) exceed L2, so no flush is needed."""
     import torch
     from powder6_b200.charge_flipping import CFSession, model_initial_grid
@@ -821,7 +821,12 @@ def main_cf(args, world, rank, local):
     n_trials = args.cf_trials or CF_TRIALS
     cycles = args.cf_cycles or CF_CYCLES
     job, m, trials = cf_setup(rank, n_trials)
-    starts = [model_initial_grid(m, CF_GRID, t['seed']) for t in trials]
+    # the starting grids in pinned host memory, as an application streaming
+    # starts would hold them (the e2e leg uploads them every step)
+    pinned = torch.empty((n_trials, 2 * CF_GRID ** 3), dtype=torch.float32).pin_memory()
+    for i, t in enumerate(trials):
+        pinned[i] = torch.from_numpy(model_initial_grid(m, CF_GRID, t['seed']))
+    starts = [pinned[i].numpy() for i in range(n_trials)]
     ms, e2e = [], []
     with CFSession(m, trials, device=local) as s:
         for i, g in enumerate(starts):
