@@ -371,9 +371,20 @@ p6_status p6_pt_lm(p6_pt_session *s, double *x, int max_iter, double tol, double
  * single thread never overlaps itself because the call returns only after its
  * stream has finished.  The first call on each device looks up the array's
  * address (cudaGetSymbolAddress); make that first call outside any stream
- * capture. */
+ * capture.  The address is looked up again when the device's context has
+ * changed since (cudaDeviceReset replaces the context and reloads the
+ * module), so the first call after a reset must also come outside a capture.
+ * The call waits for its stream at most P6_PT_STATIC_WAIT_SECONDS and then
+ * returns P6_ERR_TIMEOUT with its copies possibly still in flight: call
+ * p6_pt_synchronize before reusing or freeing `costs` and `ycalc`. */
 #define P6_PT_STATIC_SCRATCH_BYTES (4u << 20)
+#define P6_PT_STATIC_WAIT_SECONDS 60.0
 p6_status p6_pt_costs_static(p6_pt_session *s, const double *vectors, int n_vectors, double *costs, float *ycalc);
+
+/* How many vectors the session's allocating scratch (grown by p6_pt_costs
+ * with cudaMalloc) holds now; 0 until p6_pt_costs first runs.  Lets a caller
+ * check that it only ever used the allocation-free call. */
+p6_status p6_pt_vector_capacity(p6_pt_session *s, int *n_vectors);
 
 /* Many searches in one persistent launch.  The sessions (same device and
  * cos_mode, incremental evaluation off, at most 8 rungs, ladders and

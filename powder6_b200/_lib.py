@@ -114,6 +114,7 @@ _SIGS = {
     'p6_pt_set_split': (C.c_int, [_P, C.c_int]),
     'p6_pt_get_split': (C.c_int, [_P, C.POINTER(C.c_int)]),
     'p6_pt_costs_static': (C.c_int, [_P, _P, C.c_int, _P, _P]),
+    'p6_pt_vector_capacity': (C.c_int, [_P, C.POINTER(C.c_int)]),
     'p6_pt_model_costs': (C.c_int, [_P, _P, C.c_int, _P]),
     'p6_pt_normal': (C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double)]),
     'p6_pt_linear_start': (C.c_int, [_P, _P, C.POINTER(C.c_double)]),

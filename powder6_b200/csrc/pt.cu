@@ -1570,6 +1570,13 @@ p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms) {
   return P6_OK;
 }
 
+p6_status p6_pt_vector_capacity(p6_pt_session *s, int *n_vectors) {
+  clear_error();
+  if (!s || !n_vectors) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  *n_vectors = s->vecCap;
+  return P6_OK;
+}
+
 p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
   clear_error();
   if (!s || !count) return set_error(P6_ERR_INVALID_ARG, "null argument");
@@ -1939,21 +1946,68 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_static_scratch_mu;
 unsigned char *g_static_scratch_addr[kMaxDevices] = {};
+unsigned long long g_static_scratch_ctx[kMaxDevices] = {};
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// Address of the scratch array on `device` (the current device), looked up once.
+// Unique id of the current device's context (the driver's cuCtxGetId, reached
+// through the runtime's entry-point table so the library links no driver
+// stub); 0 when the driver cannot say.  A device reset replaces the primary
+// context, and with it the id and the module that holds the scratch array.
+unsigned long long current_context_id() {
+  typedef int (*GetCurrentFn)(void **);
+  typedef int (*GetIdFn)(void *, unsigned long long *);
+  static GetCurrentFn getCurrent = nullptr;
+  static GetIdFn getId = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      getCurrent = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      getId = reinterpret_cast<GetIdFn>(f);
+  }
+  void *ctx = nullptr;
+  unsigned long long id = 0;
+  if (!getCurrent || !getId || getCurrent(&ctx) != 0 || !ctx || getId(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Address of the scratch array on `device` (the current device): looked up
+// with cudaGetSymbolAddress at the first call on the device, and again only
+// when the device's context has changed since (cudaDeviceReset).
 p6_status static_scratch(int device, unsigned char **out) {
   if (device < 0 || device >= kMaxDevices) return set_error(P6_ERR_INVALID_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_static_scratch_mu);
-  if (!g_static_scratch_addr[device]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_static_scratch_addr[device] || ctx != g_static_scratch_ctx[device]) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_pt_static_scratch);
     if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_pt_static_scratch)");
     g_static_scratch_addr[device] = static_cast<unsigned char *>(p);
+    g_static_scratch_ctx[device] = ctx;
   }
   *out = g_static_scratch_addr[device];
   return P6_OK;
+}
+
+// Waits for the session's stream for at most P6_PT_STATIC_WAIT_SECONDS.
+p6_status static_wait(p6_pt_session *s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaStreamQuery(s->stream);
+    if (e == cudaSuccess) return P6_OK;
+    if (e != cudaErrorNotReady) return cuda_error(e, "cudaStreamQuery");
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > P6_PT_STATIC_WAIT_SECONDS)
+      return set_error(P6_ERR_TIMEOUT, "p6_pt_costs_static: the device did not finish within the deadline; "
+                                       "call p6_pt_synchronize before reusing the output buffers");
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
 }
 }  // namespace
 
@@ -1986,6 +2040,5 @@ extern "C" p6_status p6_pt_costs_static(p6_pt_session *s, const double *vectors,
   if (ycalc)
     P6_CUDA(cudaMemcpyAsync(ycalc, dY, (size_t)n_vectors * s->P.n * sizeof(float), cudaMemcpyDeviceToHost,
                             s->stream));
-  P6_CUDA(cudaStreamSynchronize(s->stream));
-  return P6_OK;
+  return static_wait(s);
 }

@@ -291,6 +291,12 @@ class PTSession:
                                           None if y is None else y.ctypes.data))
         return (out, y) if with_pattern else out
 
+    def vector_capacity(self) -> int:
+        """Vectors the allocating scratch of costs() holds (0 until costs() first runs)."""
+        n = C.c_int(0)
+        check(self.lib.p6_pt_vector_capacity(self.h, C.byref(n)))
+        return int(n.value)
+
     def initial(self, vectors: Sequence[Sequence[float]]):
         v = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(-1, self.plan.nv))
         check(self.lib.p6_pt_initial(self.h, v.ctypes.data, len(v)))

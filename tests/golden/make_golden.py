@@ -1,8 +1,8 @@
 """Generate the committed golden fixtures from the reference's own data files.
 
-Run in a container where the reference tree is mounted:
+Run where the reference tree is available, giving its path:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference tree>
 
 It reads, read-only:
   * sg/all.json (the cctbx-generated space-group database the reference ships):
@@ -78,11 +78,13 @@ def main(ref_root):
         ff[e] = {'Z': rec['Z'], 'a': rec['a'], 'b': rec['b'], 'c': rec['c']}
     text = json.dumps({'source': 'Waasmaier & Kirfel (1995), five-Gaussian f0, via the reference scattering table',
                        'table': ff}, indent=1)
-    (HERE / 'xray_wk1995_subset.json').write_text(text)
-    # the package reads the same coefficients for its synthetic workloads
-    (HERE.parent.parent / 'powder6_b200' / 'data' / 'xray_wk1995_subset.json').write_text(text)
-    print('wrote', HERE / 'sg_fixture.json', HERE / 'xray_wk1995_subset.json')
+    # the package reads the coefficients for its synthetic workloads (one copy, package data)
+    ff_path = HERE.parent.parent / 'powder6_b200' / 'data' / 'xray_wk1995_subset.json'
+    ff_path.write_text(text)
+    print('wrote', HERE / 'sg_fixture.json', ff_path)
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) != 2:
+        sys.exit('usage: python tests/golden/make_golden.py <path of the reference tree>')
+    main(sys.argv[1])

@@ -2,7 +2,9 @@
 
 Collected last so that it also runs after every other GPU test has used the
 device; it passes alone as well.  Two calls in a row with different vectors
-check that nothing carries over in the shared static scratch."""
+check that nothing carries over in the shared static scratch, and a fresh
+session that only ever makes static calls must leave the device's free memory
+and its own allocating scratch untouched."""
 import numpy as np
 import pytest
 
@@ -43,3 +45,22 @@ def test_static_costs_reject_oversize_requests(session):
     # the same count without patterns fits, and the session still works
     c = s.costs_static([truth] * n)
     assert np.all(c == c[0]) and np.isfinite(c[0])
+
+
+def test_static_costs_allocate_no_device_memory(oracle):
+    torch = pytest.importorskip('torch')
+    P = nacl_problem(seed=1)
+    truth = synthesise(P, oracle.PtModel(P).pattern, seed=1)
+    ctx = PTContext(P, truth, {'chains': 8, 'sweeps': 1, 'maxTemp': 10.0, 'seed': 1, 'scales': pt_scales(P, truth)})
+    with PTSession(ctx) as s:
+        s.costs_static([truth])                      # first call on the device: address look-up
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(0)[0]
+        for n in (1, 7, 64, 300):                    # growing, the last larger than any costs() call here
+            c = s.costs_static(start_vectors(P, truth, n, seed=30 + n))
+            assert c.shape == (n,) and np.all(np.isfinite(c))
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info(0)[0] == free0
+        assert s.vector_capacity() == 0              # the allocating scratch was never grown
+        s.costs([truth])                             # the allocating call does grow it
+        assert s.vector_capacity() >= 1
