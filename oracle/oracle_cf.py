@@ -77,14 +77,14 @@ class CfState:
         F = np.fft.fftn(flipped.reshape(n, n, n)).ravel()
         self.fft_max = float(np.abs(F).max())
         self.pre_mag = np.full(F.size, np.nan)
-        idx_all = m['orbitIdx']
+        idx_all = m['orbit_idx']
         ph = m['phase'].astype(np.float64)
         num = den = 0.0
         lam = min(1.0, max(0.0, self.sym_lambda))
-        for c in range(m['nClusters']):
-            o0, no = int(m['clusterOrbitStart'][c]), int(m['clusterNOrbits'][c])
-            obs = float(m['clusterObsI'][c])
-            orbits = [(int(m['orbitStart'][o]), int(m['orbitCount'][o])) for o in range(o0, o0 + no)]
+        for c in range(m['n_clusters']):
+            o0, no = int(m['cluster_orbit_start'][c]), int(m['cluster_n_orbits'][c])
+            obs = float(m['cluster_obs_i'][c])
+            orbits = [(int(m['orbit_start'][o]), int(m['orbit_count'][o])) for o in range(o0, o0 + no)]
             sums = []
             for st, cnt in orbits:
                 idx = idx_all[st:st + cnt] & IDX_MASK
@@ -125,7 +125,7 @@ class CfState:
                         ang = 2 * math.pi * philox_u01(st + int(q), self.seed)
                         out[q] = amp * (math.cos(ang) + 1j * math.sin(ang))
                     F[idx] = out
-        absent = m['orbitIdx'][m['absentStart']:m['absentStart'] + m['absentCount']] & IDX_MASK
+        absent = m['orbit_idx'][m['absent_start']:m['absent_start'] + m['absent_count']] & IDX_MASK
         F[absent] = 0
         F[0] = 0
         R = num / den if den > 0 else math.nan

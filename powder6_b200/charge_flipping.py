@@ -8,7 +8,7 @@ launches.
 
 Names follow the reference: ``build_reflection_model`` (js/charge_flipping_
 worker.js:563-948), ``model_initial_grid`` (:951-981),
-``classify_weak_orbits`` (:1213-1310), ``find_systematic_absences``
+``classify_weak_orbits`` (the rule of :1213-1310), ``find_systematic_absences``
 (:336-424), ``normalize_symops`` (:279-298), ``run_charge_flipping``
 (:1997-2500, the GPU run), and ``cf_plan`` (js/cf_adaptive.js:43-51, the
 settings of the adaptive multi-start search, whose trials run here as one
@@ -243,8 +243,8 @@ def build_reflection_model(job: dict, N: int) -> dict:
                      'rawI': float(raw) if raw is not None and math.isfinite(raw) else I,
                      'sigma': float(sigma) if sigma is not None and sigma > 0 else None})
     if not refs:
-        return {'error': 'no-reflections', 'maxIndexSeen': max_index, 'minGridForAll': 2 * max_index + 2,
-                'droppedZero': dropped_zero, 'droppedRange': dropped_range}
+        return {'error': 'no-reflections', 'max_index_seen': max_index, 'min_grid_for_all': 2 * max_index + 2,
+                'dropped_zero': dropped_zero, 'dropped_range': dropped_range}
 
     def sort_key(r):
         if r['tth'] is not None:
@@ -268,7 +268,7 @@ def build_reflection_model(job: dict, N: int) -> dict:
             significant_absent += 1
     requested_lambda = min(1.0, max(0.0, float(job.get('symLambda') or 0.0)))
     if requested_lambda >= 0.999 and significant_absent > 0:
-        return {'error': 'significant-systematic-absence', 'significantAbsent': significant_absent}
+        return {'error': 'significant-systematic-absence', 'significant_absent': significant_absent}
 
     orbit_start, orbit_count, orbit_target, orbit_centric = [], [], [], []
     idx_flat, phase_flat = [], []
@@ -305,23 +305,23 @@ def build_reflection_model(job: dict, N: int) -> dict:
         c_n[c] += 1
         c_obs[c] += scaled
     if not orbit_start:
-        return {'error': 'no-reflections', 'maxIndexSeen': max_index, 'minGridForAll': 2 * max_index + 2,
-                'droppedZero': dropped_zero, 'droppedRange': dropped_range}
+        return {'error': 'no-reflections', 'max_index_seen': max_index, 'min_grid_for_all': 2 * max_index + 2,
+                'dropped_zero': dropped_zero, 'dropped_range': dropped_range}
     keep = [c for c in range(len(c_start)) if c_n[c] > 0]
     n_members = len(idx_flat)
     return {
         'N': N,
-        'nOrbits': len(orbit_start), 'nClusters': len(keep), 'nMembers': n_members,
-        'orbitStart': np.array(orbit_start, np.uint32), 'orbitCount': np.array(orbit_count, np.uint32),
-        'orbitTargetI': np.array(orbit_target, np.float32), 'orbitCentricPhase': np.array(orbit_centric, np.float64),
-        'orbitIdx': np.concatenate([np.array(idx_flat, np.uint32), absent]).astype(np.uint32),
+        'n_orbits': len(orbit_start), 'n_clusters': len(keep), 'n_members': n_members,
+        'orbit_start': np.array(orbit_start, np.uint32), 'orbit_count': np.array(orbit_count, np.uint32),
+        'orbit_target_i': np.array(orbit_target, np.float32), 'orbit_centric_phase': np.array(orbit_centric, np.float64),
+        'orbit_idx': np.concatenate([np.array(idx_flat, np.uint32), absent]).astype(np.uint32),
         'phase': np.array(phase_flat, np.float32),
-        'clusterOrbitStart': np.array([c_start[c] for c in keep], np.uint32),
-        'clusterNOrbits': np.array([c_n[c] for c in keep], np.uint32),
-        'clusterObsI': np.array([c_obs[c] for c in keep], np.float32),
-        'absentStart': n_members, 'absentCount': int(len(absent)),
-        'droppedZero': dropped_zero, 'droppedRange': dropped_range, 'droppedDuplicate': dropped_duplicate,
-        'significantAbsent': significant_absent, 'maxIndexSeen': max_index, 'minGridForAll': 2 * max_index + 2,
+        'cluster_orbit_start': np.array([c_start[c] for c in keep], np.uint32),
+        'cluster_n_orbits': np.array([c_n[c] for c in keep], np.uint32),
+        'cluster_obs_i': np.array([c_obs[c] for c in keep], np.float32),
+        'absent_start': n_members, 'absent_count': int(len(absent)),
+        'dropped_zero': dropped_zero, 'dropped_range': dropped_range, 'dropped_duplicate': dropped_duplicate,
+        'significant_absent': significant_absent, 'max_index_seen': max_index, 'min_grid_for_all': 2 * max_index + 2,
     }
 
 
@@ -332,12 +332,12 @@ def model_initial_grid(model: dict, N: int, seed: int) -> np.ndarray:
     phase factors, amplitude sqrt(target / count).  2 N^3 floats."""
     init = np.zeros(2 * N ** 3, np.float32)
     rand = mulberry32(seed)
-    idx, ph = model['orbitIdx'], model['phase']
-    for g in range(model['nOrbits']):
-        start, count = int(model['orbitStart'][g]), int(model['orbitCount'][g])
-        amp = math.sqrt(max(0.0, float(model['orbitTargetI'][g])) / count)
+    idx, ph = model['orbit_idx'], model['phase']
+    for g in range(model['n_orbits']):
+        start, count = int(model['orbit_start'][g]), int(model['orbit_count'][g])
+        amp = math.sqrt(max(0.0, float(model['orbit_target_i'][g])) / count)
         u = rand()
-        centric = float(model['orbitCentricPhase'][g])
+        centric = float(model['orbit_centric_phase'][g])
         ang = centric + (0.0 if u < 0.5 else math.pi) if math.isfinite(centric) else 2 * math.pi * u
         f0r, f0i = amp * math.cos(ang), amp * math.sin(ang)
         for p in range(start, start + count):
@@ -354,36 +354,45 @@ def model_initial_grid(model: dict, N: int, seed: int) -> np.ndarray:
 
 
 def classify_weak_orbits(model: dict, fraction: float, grouping: str = 'cluster') -> dict:
-    """The weakest fraction of orbits (or of 2-theta clusters), by intensity
-    per grid point, flagged for the quarter-turn instead of the amplitude
-    constraint (js/charge_flipping_worker.js:1213-1310)."""
+    """Orbits that take the quarter-turn instead of the amplitude constraint
+    (the weak-reflection rule of js/charge_flipping_worker.js:1213-1310).
+
+    The units ranked are single orbits (``grouping='individual'``) or whole
+    2-theta clusters; a unit's strength is its observed intensity per grid
+    point it occupies (a unit with no points ranks strongest).  The weakest
+    floor(fraction * units) are flagged, every orbit of a flagged cluster
+    with it.  Returns the per-orbit flags and a summary: the mode, the
+    strength of the last unit flagged, and the flagged and total counts."""
     mode = 'individual' if grouping == 'individual' else 'cluster'
-    f = min(1.0, max(0.0, float(fraction or 0.0)))
-    flags = np.zeros(model['nOrbits'], np.uint8)
-    units = []
+    frac = min(1.0, max(0.0, float(fraction or 0.0)))
+    count = np.asarray(model['orbit_count'], dtype=np.float64)
+    n_orb = int(model['n_orbits'])
     if mode == 'individual':
-        for g in range(model['nOrbits']):
-            cnt = int(model['orbitCount'][g])
-            units.append((float(model['orbitTargetI'][g]) / cnt if cnt > 0 else math.inf, g))
+        intensity = np.asarray(model['orbit_target_i'], dtype=np.float64)
+        points = count
     else:
-        for c in range(model['nClusters']):
-            s, n = int(model['clusterOrbitStart'][c]), int(model['clusterNOrbits'][c])
-            members = sum(int(model['orbitCount'][s + j]) for j in range(n))
-            units.append((float(model['clusterObsI'][c]) / members if members > 0 else math.inf, c))
-    units.sort()
-    n_weak = min(len(units), int(math.floor(f * len(units))))
-    weak_orbits = 0
-    for i in range(n_weak):
-        idx = units[i][1]
-        if mode == 'individual':
-            flags[idx] = 1
-            weak_orbits += 1
-        else:
-            s, n = int(model['clusterOrbitStart'][idx]), int(model['clusterNOrbits'][idx])
-            flags[s:s + n] = 1
-            weak_orbits += n
-    return {'flags': flags, 'mode': mode, 'cutoff': units[n_weak - 1][0] if n_weak > 0 else 0.0,
-            'weakUnits': n_weak, 'totalUnits': len(units), 'weakOrbits': weak_orbits}
+        start = np.asarray(model['cluster_orbit_start'], dtype=np.int64)
+        span = np.asarray(model['cluster_n_orbits'], dtype=np.int64)
+        intensity = np.asarray(model['cluster_obs_i'], dtype=np.float64)
+        # points per cluster: prefix sums of the orbit point counts over each span
+        cum = np.concatenate([[0.0], np.cumsum(count)])
+        points = cum[start + span] - cum[start]
+    with np.errstate(divide='ignore', invalid='ignore'):
+        strength = np.where(points > 0, intensity / np.where(points > 0, points, 1.0), np.inf)
+    n_units = len(strength)
+    n_weak = min(n_units, int(math.floor(frac * n_units)))
+    weakest = np.argsort(strength, kind='stable')[:n_weak]
+    if mode == 'individual':
+        flags = np.zeros(n_orb, dtype=np.uint8)
+        flags[weakest] = 1
+    else:
+        # mark each flagged cluster's orbit span with a difference array
+        edge = np.zeros(n_orb + 1, dtype=np.int64)
+        np.add.at(edge, start[weakest], 1)
+        np.add.at(edge, start[weakest] + span[weakest], -1)
+        flags = (np.cumsum(edge)[:n_orb] > 0).astype(np.uint8)
+    return {'flags': flags, 'mode': mode, 'cutoff': float(strength[weakest[-1]]) if n_weak else 0.0,
+            'weak_units': n_weak, 'total_units': n_units, 'weak_orbits': int(flags.sum())}
 
 
 MIN_STARTS, MAX_STARTS = 6, 128
@@ -445,21 +454,21 @@ class CFSession:
             self._keep.append(x)
             return x.ctypes.data
 
-        nm = model['nMembers']
+        nm = model['n_members']
         m = P6CfModel()
         m.n = self.N
-        m.n_orbits = model['nOrbits']
-        m.orbit_start = a(model['orbitStart'], np.uint32)
-        m.orbit_count = a(model['orbitCount'], np.uint32)
+        m.n_orbits = model['n_orbits']
+        m.orbit_start = a(model['orbit_start'], np.uint32)
+        m.orbit_count = a(model['orbit_count'], np.uint32)
         m.n_members = nm
-        m.orbit_idx = a(model['orbitIdx'][:nm], np.uint32)
+        m.orbit_idx = a(model['orbit_idx'][:nm], np.uint32)
         m.phase = a(model['phase'], np.float32)
-        m.n_clusters = model['nClusters']
-        m.cluster_orbit_start = a(model['clusterOrbitStart'], np.uint32)
-        m.cluster_n_orbits = a(model['clusterNOrbits'], np.uint32)
-        m.cluster_obs_i = a(model['clusterObsI'], np.float32)
-        m.n_absent = model['absentCount']
-        m.absent_idx = a(model['orbitIdx'][nm:], np.uint32) if model['absentCount'] else None
+        m.n_clusters = model['n_clusters']
+        m.cluster_orbit_start = a(model['cluster_orbit_start'], np.uint32)
+        m.cluster_n_orbits = a(model['cluster_n_orbits'], np.uint32)
+        m.cluster_obs_i = a(model['cluster_obs_i'], np.float32)
+        m.n_absent = model['absent_count']
+        m.absent_idx = a(model['orbit_idx'][nm:], np.uint32) if model['absent_count'] else None
         arr = (P6CfTrial * self.n_trials)()
         for t, tr in enumerate(trials):
             arr[t].delta_sigma = float(tr.get('threshold', 1.1))
@@ -556,9 +565,9 @@ def run_charge_flipping(job: dict, device: int = 0, trials: Optional[Sequence[di
     dev_trials, weak_counts = [], []
     for t in specs:
         wk = classify_weak_orbits(model, t['weakFraction'], grouping)
-        weak_counts.append(wk['weakOrbits'])
+        weak_counts.append(wk['weak_orbits'])
         dev_trials.append({'threshold': t['threshold'], 'symLambda': t['symLambda'], 'seed': t['seed'],
-                           'weak': wk['flags'] if wk['weakOrbits'] else None})
+                           'weak': wk['flags'] if wk['weak_orbits'] else None})
     with CFSession(model, dev_trials, device) as s:
         for i, t in enumerate(specs):
             s.set_grid(model_initial_grid(model, N, t['seed']), i)
@@ -571,11 +580,11 @@ def run_charge_flipping(job: dict, device: int = 0, trials: Optional[Sequence[di
             best_iter = int(np.argmin(np.where(fin, h, np.inf))) + 1 if fin.any() else 0
             results.append({'bestR': float(best[i]), 'bestIter': best_iter, 'finalR': float(h[-1]) if cycles else math.nan,
                             'rHistory': h, 'seed': t['seed'], 'symLambda': t['symLambda'],
-                            'threshold': t['threshold'], 'weakOrbits': weak_counts[i]})
+                            'threshold': t['threshold'], 'weak_orbits': weak_counts[i]})
         top = int(np.argmin(best))
         out = dict(results[top])
         out.update({'map': s.read(top, 'map'), 'backend': 'gpu', 'trials': results, 'bestTrial': top,
-                    'gridSize': N, 'nOrbits': model['nOrbits'], 'nClusters': model['nClusters'],
+                    'gridSize': N, 'n_orbits': model['n_orbits'], 'n_clusters': model['n_clusters'],
                     'deviceMs': s.last_ms()})
     return out
 

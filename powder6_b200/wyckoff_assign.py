@@ -1,32 +1,48 @@
-"""Wyckoff assignments consistent with a composition: the caller of the
-search that decides which (element, Wyckoff position) sets the device
-searches.
+"""Wyckoff assignments consistent with a composition: which (element,
+Wyckoff position) sets the device searches.
 
-Restates js/wyckoff_assign.js:184-206 (``multisets_summing_to``), :226-352
-(site stabiliser, inversion and coordination compatibility), :354-572
-(``enumerate_assignments``), :574-605 (the fixed-point clash message) and
-:664-754 (``normalizer_permutations``, ``dedupe_equivalent_assignments``),
-over this package's space groups (``symmetry.SpaceGroup``).  An enumerated
-assignment converts to the search's ``wyckoff_tables.Assignment`` with
-``to_search_assignment``.
+Behaviour follows the reference's assignment step (js/wyckoff_assign.js:184-754:
+the per-element position multisets, the site-symmetry exclusions for a stated
+coordination, the combination with no fixed point shared by two elements and
+at most 32 sites, failure messages that name the constraint, and the removal
+of assignments that an origin shift or an inversion of the group maps onto
+one another), pinned by its regression counts.  The construction is this
+module's own:
+
+* per element, the position multisets summing to the count are the
+  solutions of a bounded knapsack over the multiplicities (a position without
+  free coordinates at most once, a free one up to ``maxRepeat`` times).  A
+  reachability table, built backwards over the positions, holds for every
+  remainder the bitmask of site counts that can still complete it; the
+  solutions are then read off site count by site count (fewest sites first),
+  expanding only branches the table says complete;
+* elements are combined by a breadth-first fold over states (bitmask of the
+  fixed points taken, sites used): a choice joins a state when its own
+  fixed-point mask is disjoint from the state's;
+* a site's symmetry is read from the operators that fix a generic point of
+  its subspace, all operators at once in integer arithmetic over 1/24;
+* equivalent assignments are found through the group's affine normaliser
+  x -> m x + s (m = +-1): every shift s at the group's own translation
+  resolution (1/24) that conjugates the group onto itself, reduced to cosets
+  of the group with ``SymOp.compose``; each coset permutes the positions,
+  found by an exact subspace test of the mapped generic point.
 
 Positions are the group's ``wyckoff`` list; ``demand`` is
-[{'element', 'count' (atoms per cell), 'z', 'r'}].  Messages name the
-constraint that failed, as the reference's do.
+[{'element', 'count' (atoms per cell), 'z', 'r'}].
 """
 from __future__ import annotations
 
 import math
-from typing import Dict, List, Optional, Sequence
+from fractions import Fraction
+from itertools import product
+from typing import Dict, List, Optional, Sequence, Tuple
 
-from .symmetry import SpaceGroup, WyckoffPosition
+import numpy as np
+
+from .symmetry import IDENT, INV, TDEN, SpaceGroup, SymOp, WyckoffPosition
 
 MAX_SITES = 32            # sites one assignment may hold (the search kernel's limit)
 MAX_ASSIGNMENTS = 4000    # enumeration cap
-
-# A deliberately generic point: its projection onto a position cannot land on
-# a higher-symmetry sub-position by accident.
-_GENERIC = (0.1357913, 0.2468135, 0.3579246)
 
 # Coordination polyhedra without an inversion centre.
 NON_CENTROSYMMETRIC_GEOMETRY = {'tetrahedral', 'trigonal-planar', 'trigonal-pyramidal', 'square-pyramidal',
@@ -37,321 +53,348 @@ NON_CENTROSYMMETRIC_GEOMETRY = {'tetrahedral', 'trigonal-planar', 'trigonal-pyra
 TETRAHEDRAL_AT_FOUR = {'B', 'C', 'N', 'F', 'AL', 'SI', 'P', 'S', 'CL', 'GA', 'GE', 'AS', 'SE', 'BR', 'V', 'CR', 'MN',
                        'FE', 'CO', 'ZN', 'MO', 'W', 'TC', 'RE', 'BE', 'I', 'XE'}
 
-
-def _ops(group: SpaceGroup):
-    return [(tuple(o.r), tuple(o.t_frac)) for o in group.ops]
-
-
-def multisets_summing_to(positions: Sequence[WyckoffPosition], target: int, opts: dict) -> List[List[int]]:
-    """Index multisets of ``positions`` whose multiplicities sum to
-    ``target``: a position without free coordinates at most once, one with
-    free coordinates at most ``maxRepeat`` times, at most ``maxSites`` sites,
-    at most ``maxPerElement`` results, indices non-decreasing."""
-    out: List[List[int]] = []
-    counts = [0] * len(positions)
-    chosen: List[int] = []
-
-    def rec(start: int, remaining: int):
-        if remaining == 0:
-            out.append(list(chosen))
-            return
-        if len(chosen) >= opts['maxSites'] or len(out) >= opts['maxPerElement']:
-            return
-        for i in range(start, len(positions)):
-            m = positions[i].multiplicity
-            if not m or m > remaining:
-                continue
-            cap = opts['maxRepeat'] if positions[i].n_free > 0 else 1
-            if counts[i] >= cap:
-                continue
-            counts[i] += 1
-            chosen.append(i)
-            rec(i, remaining - m)
-            chosen.pop()
-            counts[i] -= 1
-            if len(out) >= opts['maxPerElement']:
-                return
-
-    rec(0, target)
-    return out
+# A point no special position passes through: each coordinate a fraction of
+# 24 * 1009, so operators (translations in 1/24) act on it in integers.
+_SCALE = TDEN * 1009
+_GEN = (137, 251, 409)
 
 
-def _near_int(d: float, tol: float) -> bool:
-    return abs(d - round(d)) < tol
+def _label(w: WyckoffPosition) -> str:
+    return f'{w.multiplicity}{w.letter}'
 
 
-def site_stabilizer(w: WyckoffPosition, ops) -> list:
-    """Operators mapping the position's generic representative onto itself
-    modulo a lattice translation."""
-    p = w.project(*_GENERIC)
-    stab = []
-    for r, t in ops:
-        q = [r[3 * i] * p[0] + r[3 * i + 1] * p[1] + r[3 * i + 2] * p[2] + t[i] for i in range(3)]
-        if all(_near_int(q[i] - p[i], 1e-4) for i in range(3)):
-            stab.append((r, t))
-    return stab
+def _generic_point(w: WyckoffPosition) -> Tuple[Fraction, Fraction, Fraction]:
+    g = [Fraction(v, 1009) for v in _GEN]
+    return tuple(sum(w.P[3 * i + k] * g[k] for k in range(3)) + w.T[i] for i in range(3))
 
 
-def site_has_inversion(w: WyckoffPosition, ops) -> bool:
-    return any(tuple(r) == (-1, 0, 0, 0, -1, 0, 0, 0, -1) for r, _ in site_stabilizer(w, ops))
+# ---------------------------------------------------------------------------
+# Site symmetry
+# ---------------------------------------------------------------------------
+def _op_arrays(ops: Sequence) -> Tuple[np.ndarray, np.ndarray]:
+    """Rotations (n, 3, 3) and translations in 1/24 (n, 3) of SymOps or (r, t_frac) pairs."""
+    R, T = [], []
+    for o in ops:
+        if isinstance(o, SymOp):
+            R.append(o.r)
+            T.append(o.t)
+        else:
+            r, t = o
+            R.append(tuple(r))
+            T.append(tuple(int(round(v * TDEN)) for v in t))
+    return np.array(R, dtype=np.int64).reshape(-1, 3, 3), np.array(T, dtype=np.int64).reshape(-1, 3)
+
+
+def site_rotations(w: WyckoffPosition, ops: Sequence) -> List[Tuple[int, ...]]:
+    """Rotation parts of the operators fixing a generic point of ``w`` modulo
+    the lattice (exact: the point is held in units of 1 / (24 * 1009))."""
+    R, T = _op_arrays(ops)
+    p = np.array([int(v * _SCALE) for v in _generic_point(w)], dtype=np.int64)
+    img = np.einsum('nij,j->ni', R, p) + T * (_SCALE // TDEN)
+    fixed = np.all((img - p) % _SCALE == 0, axis=1)
+    return [tuple(int(v) for v in R[k].reshape(-1)) for k in np.nonzero(fixed)[0]]
+
+
+def site_has_inversion(w: WyckoffPosition, ops: Sequence) -> bool:
+    return INV in site_rotations(w, ops)
 
 
 def coordination_compatible(w: WyckoffPosition, element: str, req: Optional[dict], ops) -> Optional[str]:
     """None when an atom of ``element`` with coordination ``req`` ({'count',
-    'geometry'}) can sit on ``w``; else the reason.  Parity: an inversion
-    centre pairs every neighbour, so the count must be even.  Geometry: a
-    polyhedron without an inversion centre (stated, or tetrahedral for the
-    tetrahedral formers at four neighbours) cannot sit on one."""
+    'geometry'}) may sit on ``w``; otherwise why not.  A site on an inversion
+    centre sees its neighbours in antipodal pairs, so it needs an even
+    count, and no polyhedron lacking a centre of symmetry (stated, or the
+    tetrahedron implied by four neighbours of a tetrahedral former) fits it."""
     if not req or not req.get('count') or req['count'] <= 0 or not ops:
         return None
     if not site_has_inversion(w, ops):
         return None
-    label = f'{w.multiplicity}{w.letter}'
-    if req['count'] % 2 == 1:
-        return (f"{element} needs {req['count']} neighbours, an odd number, but {label} has an inversion "
-                f"centre, which pairs every neighbour with an antipode.")
+    n = int(req['count'])
+    if n % 2:
+        return (f"{w.multiplicity}{w.letter} is an inversion centre, where neighbours come in opposite pairs; "
+                f"{element} with {n} neighbours (an odd number) cannot sit there.")
     geom = str(req['geometry']).lower() if req.get('geometry') else None
-    if not geom and req['count'] == 4 and str(element).upper() in TETRAHEDRAL_AT_FOUR:
+    if not geom and n == 4 and str(element).upper() in TETRAHEDRAL_AT_FOUR:
         geom = 'tetrahedral'
-    if geom and geom in NON_CENTROSYMMETRIC_GEOMETRY:
-        return (f"{element} on {label} would put a {geom} coordination on an inversion centre, which no {geom} "
-                f"arrangement has.")
+    if geom in NON_CENTROSYMMETRIC_GEOMETRY:
+        return (f"{w.multiplicity}{w.letter} is an inversion centre, and a {geom} arrangement around {element} "
+                f"has no centre of symmetry to put there.")
     return None
 
 
-def _fixed_point_clash(wyckoff, demand, per_element, fixed_only) -> Optional[str]:
-    forced, pool = [], set()
-    for e, combos in enumerate(per_element):
-        if combos and all(any(i in fixed_only for i in c) for c in combos):
-            forced.append(e)
-            for c in combos:
-                pool.update(i for i in c if i in fixed_only)
-    if len(forced) < 2:
-        return None
+# ---------------------------------------------------------------------------
+# Position multisets per element: bounded knapsack with a reachability table
+# ---------------------------------------------------------------------------
+def multisets_summing_to(positions: Sequence[WyckoffPosition], target: int, opts: dict) -> List[List[int]]:
+    """Index multisets of ``positions`` whose multiplicities sum to
+    ``target``, each index at most once for a position without free
+    coordinates and at most ``maxRepeat`` times otherwise, with at most
+    ``maxSites`` sites; at most ``maxPerElement`` of them, fewest sites first,
+    then in order of the positions (indices non-decreasing within one)."""
+    n = len(positions)
+    max_sites = int(opts['maxSites'])
+    limit = int(opts['maxPerElement'])
+    mult = [int(p.multiplicity) for p in positions]
+    cap = [0 if m <= 0 else (1 if p.n_free == 0 else int(opts['maxRepeat'])) for p, m in zip(positions, mult)]
+    # reach[i][r]: bit k set when positions i.. can make remainder r with exactly k sites
+    reach = [[0] * (target + 1) for _ in range(n + 1)]
+    reach[n][0] = 1
+    for i in range(n - 1, -1, -1):
+        nxt, cur = reach[i + 1], reach[i]
+        for r in range(target + 1):
+            bits = 0
+            for c in range(0, cap[i] + 1):
+                if c * mult[i] > r:
+                    break
+                bits |= nxt[r - c * mult[i]] << c
+            cur[r] = bits & ((1 << (max_sites + 1)) - 1)
+    out: List[List[int]] = []
+    counts = [0] * n
 
-    def lst(a):
-        return ''.join(a) if len(a) <= 1 else ', '.join(a[:-1]) + ' and ' + a[-1]
-    who = [f"{demand[e]['element']} ({demand[e]['count']} per cell)" for e in forced]
-    where = [f'{wyckoff[i].multiplicity}{wyckoff[i].letter}' for i in sorted(pool)]
-    tail = (f'That is {len(forced)} elements for {len(pool)} such position(s). ' if len(forced) > len(pool)
-            else 'No way of sharing them out leaves every element its own. ')
-    return (f"No assignment places {lst([demand[e]['element'] for e in forced])} on separate sites: {lst(who)} can "
-            f"only go on fixed points (positions with no free coordinate: {lst(where)}), and a fixed point holds "
-            f"one element. " + tail + "The search builds ordered models, one element per site.")
+    def walk(i: int, r: int, k: int):
+        """Positions i.., remainder r, exactly k more sites."""
+        if len(out) >= limit:
+            return
+        if i == n:
+            out.append([j for j in range(n) for _ in range(counts[j])])
+            return
+        for c in range(min(cap[i], k), -1, -1):
+            rest = r - c * mult[i]
+            if rest < 0 or not (reach[i + 1][rest] >> (k - c)) & 1:
+                continue
+            counts[i] = c
+            walk(i + 1, rest, k - c)
+            counts[i] = 0
+
+    for k in range(1, max_sites + 1):
+        if (reach[0][target] >> k) & 1:
+            walk(0, target, k)
+        if len(out) >= limit:
+            break
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Enumeration
+# ---------------------------------------------------------------------------
+def _join(words: Sequence[str]) -> str:
+    return words[0] if len(words) == 1 else ', '.join(words[:-1]) + ' and ' + words[-1]
+
+
+def _no_multiset_reason(d: dict, mults: Sequence[int], m_max: int, opts: dict) -> str:
+    avail = sorted(set(mults))
+    g = 0
+    for v in avail:
+        g = math.gcd(g, v)
+    shown = ', '.join(map(str, avail))
+    if g == 0 or d['count'] % g:
+        return (f"Every available multiplicity ({shown}) is a multiple of {g}, a common factor that "
+                f"{d['count']} does not share, so no combination reaches it. Check Z.")
+    need = math.ceil(d['count'] / m_max)
+    if need > opts['maxSites']:
+        return (f"The multiplicities ({shown}) reach {d['count']} only with {need} or more sites; the search "
+                f"takes at most {opts['maxSites']} sites per element and {opts['maxRepeat']} uses of one "
+                f"position.")
+    return (f"The multiplicities ({shown}) could add up to it, but the positions without free coordinates "
+            f"hold one atom each, and those available do not suffice.")
 
 
 def enumerate_assignments(group: SpaceGroup, demand: Sequence[dict], options: Optional[dict] = None) -> dict:
-    """Every assignment of Wyckoff positions to the demanded atoms per cell
-    (js/wyckoff_assign.js:354-572): per element, the multisets of positions
-    summing to its count (largest multiplicities first, site-symmetry
-    exclusions from ``coordination`` applied before the combinatorics), then
-    their combinations with no fixed point shared by two elements and at most
-    ``maxTotalSites`` sites.  Returns {'assignments': [{'sites': [{'element',
-    'elementIdx', 'z', 'r', 'wIdx'}], 'nSites'}], 'truncated',
-    'droppedTooManySites', 'siteSymmetryExcluded'} or, when none exists, an
-    empty list with an 'error' naming the cause."""
+    """Every assignment of Wyckoff positions to the demanded atoms per cell.
+
+    Returns {'assignments': [{'sites': [{'element', 'elementIdx', 'z', 'r',
+    'wIdx'}], 'nSites'}], 'truncated', 'droppedTooManySites',
+    'siteSymmetryExcluded'}; when none exists the list is empty and 'error'
+    says which constraint left nothing."""
     options = dict(options or {})
     wyckoff = group.wyckoff
-    ops = _ops(group)
     ceiling = options.get('ceiling', 24)
     mults = [w.multiplicity for w in wyckoff if w.multiplicity > 0]
     m_max = max(mults) if mults else 1
-    max_count = max((d['count'] for d in demand), default=0)
-    needed = min(ceiling, math.ceil(max_count / m_max))
-    opts = {'maxSites': min(ceiling, max(options.get('maxSites', 4), needed)),
-            'maxRepeat': min(ceiling, max(options.get('maxRepeat', 4), needed)),
+    need = min(ceiling, math.ceil(max((d['count'] for d in demand), default=0) / m_max))
+    opts = {'maxSites': min(ceiling, max(options.get('maxSites', 4), need)),
+            'maxRepeat': min(ceiling, max(options.get('maxRepeat', 4), need)),
             'maxPerElement': options.get('maxPerElement', 500),
             'maxTotal': options.get('maxTotal', MAX_ASSIGNMENTS)}
     max_total_sites = options.get('maxTotalSites', MAX_SITES)
-    idx = sorted(range(len(wyckoff)), key=lambda i: -wyckoff[i].multiplicity)   # stable, as the reference's sort
-    srt = [wyckoff[i] for i in idx]
-    coordination = options.get('coordination')
-    use_ops = ops if options.get('symOps', True) else None
+    coordination = options.get('coordination') or {}
+    check_symmetry = options.get('symOps', True)
+    order = sorted(range(len(wyckoff)), key=lambda i: (-wyckoff[i].multiplicity, i))
     excluded: List[str] = []
-    excluded_for: List[list] = [[] for _ in demand]
-    allowed_for: List[Optional[set]] = []
+    per_element: List[List[List[int]]] = []
     for e, d in enumerate(demand):
-        req = coordination.get(str(d['element']).upper()) if coordination else None
-        if not req or not use_ops:
-            allowed_for.append(None)
-            continue
-        ok = set()
-        for i, w in enumerate(wyckoff):
-            why = coordination_compatible(w, d['element'], req, use_ops)
-            if why:
-                excluded.append(why)
-                excluded_for[e].append({'label': f'{w.multiplicity}{w.letter}', 'mult': w.multiplicity, 'why': why})
-            else:
-                ok.add(i)
-        allowed_for.append(ok)
-    per_element = []
-    for e, d in enumerate(demand):
-        ok = allowed_for[e]
-        pool = [w for k, w in enumerate(srt) if ok is None or idx[k] in ok]
-        pool_idx = [i for i in idx if ok is None or i in ok]
-        per_element.append([[pool_idx[k] for k in s] for s in multisets_summing_to(pool, d['count'], opts)])
-    for e, d in enumerate(demand):
-        if not per_element[e] and allowed_for[e] is not None and \
-                multisets_summing_to(srt, d['count'], dict(opts, maxPerElement=1)):
-            el = str(d['element'])
-            name = el[:1].upper() + el[1:].lower()
-            req = coordination[el.upper()]
-            lost = [x for x in excluded_for[e] if x['mult'] <= d['count']] or excluded_for[e]
-            return {'assignments': [], 'siteSymmetryExcluded': excluded, 'coordinationConflict': el,
-                    'error': (f"No Wyckoff assignment gives {d['count']} {name} atoms per cell with the "
-                              f"coordination stated for {name} ({req['count']} neighbour"
-                              f"{'' if req['count'] == 1 else 's'}"
-                              f"{', ' + req['geometry'] if req.get('geometry') else ''}). Site symmetry excludes "
-                              f"{', '.join(x['label'] for x in lost)}: {lost[0]['why']}")}
-        if not per_element[e]:
-            avail = sorted(set(mults))
-            g = 0
-            for v in avail:
-                g = math.gcd(g, v)
-            reachable = g > 0 and d['count'] % g == 0
-            min_sites = math.ceil(d['count'] / m_max)
-            if reachable and min_sites > opts['maxSites']:
-                why = (f"The multiplicities available ({', '.join(map(str, avail))}) can reach that total, but only "
-                       f"with at least {min_sites} sites, and the search is capped at {opts['maxSites']} distinct "
-                       f"site(s) per element and {opts['maxRepeat']} reuse(s) of any one position.")
-            elif reachable:
-                why = (f"The multiplicities available ({', '.join(map(str, avail))}) could sum to it, but not with "
-                       f"these positions: one without free coordinates holds a single atom.")
-            else:
-                why = (f"The multiplicities available ({', '.join(map(str, avail))}) share a common factor of {g}, "
-                       f"so no combination of them can sum to {d['count']}. Check Z.")
-            return {'assignments': [], 'error': f"No Wyckoff assignment gives {d['count']} {d['element']} atoms per "
-                                                f"cell. {why}"}
-    fixed_only = {i for i, w in enumerate(wyckoff) if w.n_free == 0}
-    assignments: List[dict] = []
-    dropped = [0]
-    cur: List[Optional[list]] = [None] * len(demand)
+        req = coordination.get(str(d['element']).upper())
+        allowed, lost = order, []
+        if req and check_symmetry:
+            allowed = []
+            for i in order:
+                why = coordination_compatible(wyckoff[i], d['element'], req, group.ops)
+                if why:
+                    excluded.append(why)
+                    lost.append((wyckoff[i], why))
+                else:
+                    allowed.append(i)
+        sets = [[allowed[k] for k in s]
+                for s in multisets_summing_to([wyckoff[i] for i in allowed], d['count'], opts)]
+        if not sets:
+            name = str(d['element'])[:1].upper() + str(d['element'])[1:].lower()
+            if lost and multisets_summing_to([wyckoff[i] for i in order], d['count'], dict(opts, maxPerElement=1)):
+                fits = [x for x in lost if x[0].multiplicity <= d['count']] or lost
+                geom = f", {req['geometry']}" if req.get('geometry') else ''
+                return {'assignments': [], 'siteSymmetryExcluded': excluded, 'coordinationConflict': d['element'],
+                        'error': (f"{d['count']} {name} atoms per cell cannot be placed with the coordination "
+                                  f"stated for {name} ({req['count']} neighbours{geom}): "
+                                  f"{_join([_label(w) for w, _ in fits])} would be needed, and {fits[0][1]}")}
+            return {'assignments': [], 'error': f"No Wyckoff assignment gives {d['count']} {d['element']} atoms "
+                                                f"per cell. {_no_multiset_reason(d, mults, m_max, opts)}"}
+        per_element.append(sets)
 
-    def rec(e: int, used_fixed: set, used: int):
-        if len(assignments) >= opts['maxTotal']:
-            return
-        if used > max_total_sites:
-            dropped[0] += 1
-            return
-        if e == len(demand):
-            sites = [{'element': demand[k]['element'], 'elementIdx': k, 'z': demand[k].get('z'),
-                      'r': demand[k].get('r'), 'wIdx': w} for k in range(len(demand)) for w in cur[k]]
-            assignments.append({'sites': sites, 'nSites': len(sites)})
-            return
-        for combo in per_element[e]:
-            clash, added = False, []
-            for w in combo:
-                if w not in fixed_only:
+    # breadth-first fold over (fixed points taken, sites used)
+    fixed_bit = {i: 1 << k for k, i in enumerate(i for i, w in enumerate(wyckoff) if w.n_free == 0)}
+    choice_mask = [[sum(fixed_bit.get(i, 0) for i in s) for s in sets] for sets in per_element]
+    states: List[Tuple[int, int, Tuple[int, ...]]] = [(0, 0, ())]
+    dropped = truncated = 0
+    for e, sets in enumerate(per_element):
+        grown = []
+        for mask, used, picks in states:
+            for j, s in enumerate(sets):
+                if mask & choice_mask[e][j]:
                     continue
-                if w in used_fixed:
-                    clash = True
+                if used + len(s) > max_total_sites:
+                    dropped += 1
+                    continue
+                grown.append((mask | choice_mask[e][j], used + len(s), picks + (j,)))
+                if len(grown) >= opts['maxTotal']:
+                    truncated = 1
                     break
-                used_fixed.add(w)
-                added.append(w)
-            if not clash:
-                cur[e] = combo
-                rec(e + 1, used_fixed, used + len(combo))
-            for w in added:
-                used_fixed.discard(w)
-            if len(assignments) >= opts['maxTotal']:
-                return
-
-    rec(0, set(), 0)
-    if not assignments and dropped[0]:
-        return {'assignments': [], 'siteSymmetryExcluded': excluded, 'droppedTooManySites': dropped[0],
-                'error': (f"Every Wyckoff assignment for this composition needs more than {max_total_sites} "
-                          f"independent sites, which is the most the search kernel holds.")}
+            if len(grown) >= opts['maxTotal']:
+                break
+        states = grown
+    assignments = []
+    for _, used, picks in states:
+        sites = [{'element': demand[e]['element'], 'elementIdx': e, 'z': demand[e].get('z'),
+                  'r': demand[e].get('r'), 'wIdx': i} for e, j in enumerate(picks) for i in per_element[e][j]]
+        assignments.append({'sites': sites, 'nSites': used})
     if not assignments:
-        clash = _fixed_point_clash(wyckoff, demand, per_element, fixed_only)
-        if clash:
-            return {'assignments': [], 'siteSymmetryExcluded': excluded, 'droppedTooManySites': dropped[0],
-                    'fixedPointClash': True, 'error': clash}
-    return {'assignments': assignments, 'truncated': len(assignments) >= opts['maxTotal'],
-            'droppedTooManySites': dropped[0], 'siteSymmetryExcluded': excluded}
+        err = None
+        if dropped:
+            err = (f"Every Wyckoff assignment for this composition needs more than {max_total_sites} independent "
+                   f"sites, more than the search kernel holds.")
+        else:
+            # elements that can only go on fixed points, competing for them
+            bound = [e for e, masks in enumerate(choice_mask) if all(masks)]
+            pool = sorted({i for e in bound for s in per_element[e] for i in s if i in fixed_bit})
+            if len(bound) >= 2:
+                who = [f"{demand[e]['element']} ({demand[e]['count']} per cell)" for e in bound]
+                err = (f"{_join(who)} fit only on positions without free coordinates "
+                       f"({_join([_label(wyckoff[i]) for i in pool])}), and a fixed point holds one element, so "
+                       f"no assignment gives each of them its own sites. The search builds ordered models, one "
+                       f"element per site.")
+        out = {'assignments': [], 'siteSymmetryExcluded': excluded, 'droppedTooManySites': dropped}
+        if err:
+            out['error'] = err
+            out['fixedPointClash'] = not dropped
+        return out
+    return {'assignments': assignments, 'truncated': bool(truncated), 'droppedTooManySites': dropped,
+            'siteSymmetryExcluded': excluded}
+
+
+# ---------------------------------------------------------------------------
+# Equivalent assignments: the affine normaliser x -> m x + s
+# ---------------------------------------------------------------------------
+def normalizer_cosets(group: SpaceGroup) -> List[SymOp]:
+    """Representatives, other than the group's own, of the cosets of the
+    group in its normaliser among the maps x -> m x + s (m = +-1, s in
+    1/24): those for which (R, m t + (I - R) s) belongs to the group for
+    every (R, t) in it.  Each maps structures onto equivalent ones (the same
+    |F|, the same distances)."""
+    R, T = _op_arrays(group.ops)
+    # membership table: rotation id x translation code (t0 * 576 + t1 * 24 + t2)
+    rot_ids: Dict[Tuple[int, ...], int] = {}
+    rid = np.array([rot_ids.setdefault(tuple(int(v) for v in R[k].reshape(-1)), len(rot_ids))
+                    for k in range(len(R))], dtype=np.int64)
+    table = np.zeros((len(rot_ids), TDEN ** 3), dtype=bool)
+    table[rid, (T[:, 0] % TDEN) * TDEN * TDEN + (T[:, 1] % TDEN) * TDEN + T[:, 2] % TDEN] = True
+    I3 = np.eye(3, dtype=np.int64)
+    shifts = np.array(list(product(range(TDEN), repeat=3)), dtype=np.int64)         # (24^3, 3)
+    found: List[SymOp] = []
+    for m in (1, -1):
+        # conjugate translations of every operator for every shift: (shifts, ops, 3)
+        conj = (m * T[None, :, :] + np.einsum('nij,sj->sni', I3[None] - R, shifts)) % TDEN
+        code = conj[..., 0] * TDEN * TDEN + conj[..., 1] * TDEN + conj[..., 2]
+        ok = table[rid[None, :], code].all(axis=1)
+        mat = IDENT if m == 1 else INV
+        for s in shifts[ok]:
+            found.append(SymOp(mat, tuple(int(v) for v in s)))
+    # cosets N G: keyed by their least element; the group's own coset is dropped
+    def canon(o: SymOp):
+        return (o.r, tuple(v % TDEN for v in o.t))
+    own = min(canon(g) for g in group.ops)
+    reps: Dict[tuple, SymOp] = {}
+    for n in found:
+        k = min(canon(n.compose(g)) for g in group.ops)
+        if k != own and k not in reps:
+            reps[k] = n
+    return list(reps.values())
+
+
+def _on_subspace(w: WyckoffPosition, y: Sequence[Fraction]) -> bool:
+    return all(sum(w.P[3 * i + k] * y[k] for k in range(3)) + w.T[i] == y[i] for i in range(3))
+
+
+def _position_of(group: SpaceGroup, q: Sequence[Fraction], mult: int) -> int:
+    """The position (of multiplicity ``mult``) whose orbit holds the point q."""
+    images = []
+    for o in group.ops:
+        y = [sum(o.r[3 * i + k] * q[k] for k in range(3)) + Fraction(o.t[i], TDEN) for i in range(3)]
+        images.append([v - math.floor(v) for v in y])
+    for j, w in enumerate(group.wyckoff):
+        if w.multiplicity != mult:
+            continue
+        for y in images:
+            for n in product((-1, 0, 1), repeat=3):
+                if _on_subspace(w, [y[i] + n[i] for i in range(3)]):
+                    return j
+    return -1
 
 
 def normalizer_permutations(group: SpaceGroup) -> List[List[int]]:
-    """Permutations of the Wyckoff positions induced by the maps x -> m x + s
-    (m = +-1, s in quarter-cell steps) that normalise the group: an origin
-    shift or an inversion turns an assignment into an equivalent one (the
-    same |F|, the same distances).  perm[i] = the position i maps onto."""
-    wyckoff = group.wyckoff
-    ops = _ops(group)
-    by_rot: Dict[tuple, list] = {}
-    for r, t in ops:
-        by_rot.setdefault(r, []).append(t)
-
-    def close(a, b):
-        return _near_int(a - b, 1e-6)
-
-    def member(r, t):
-        return any(close(u[0], t[0]) and close(u[1], t[1]) and close(u[2], t[2]) for u in by_rot.get(r, ()))
-
-    def apply(r, t, x):
-        return [r[3 * i] * x[0] + r[3 * i + 1] * x[1] + r[3 * i + 2] * x[2] + t[i] for i in range(3)]
-
-    generic = [w.project(*_GENERIC) for w in wyckoff]
-    steps = (0.0, 0.25, 0.5, 0.75)
+    """For each normaliser coset that moves some position, perm[i] = the
+    position that position i maps onto."""
     perms = []
-    for m in (1, -1):
-        for s0 in steps:
-            for s1 in steps:
-                for s2 in steps:
-                    if m == 1 and not (s0 or s1 or s2):
-                        continue
-                    s = (s0, s1, s2)
-                    ok = True
-                    for r, w in ops:
-                        Rs = [r[3 * i] * s0 + r[3 * i + 1] * s1 + r[3 * i + 2] * s2 for i in range(3)]
-                        if not member(r, [m * w[i] + s[i] - Rs[i] for i in range(3)]):
-                            ok = False
-                            break
-                    if not ok:
-                        continue
-                    perm = []
-                    for i in range(len(wyckoff)):
-                        p = generic[i]
-                        q = [m * p[k] + s[k] for k in range(3)]
-                        found = -1
-                        for j in range(len(wyckoff)):
-                            if found >= 0:
-                                break
-                            if wyckoff[j].multiplicity != wyckoff[i].multiplicity:
-                                continue
-                            for r, t in ops:
-                                gq = apply(r, t, q)
-                                pr = wyckoff[j].project(*gq)
-                                if all(close(pr[k], gq[k]) for k in range(3)):
-                                    found = j
-                                    break
-                        if found < 0:
-                            break
-                        perm.append(found)
-                    if len(perm) == len(wyckoff) and any(j != i for i, j in enumerate(perm)):
-                        perms.append(perm)
+    if len(group.wyckoff) < 2:
+        return perms
+    generic = [_generic_point(w) for w in group.wyckoff]
+    for n in normalizer_cosets(group):
+        perm = []
+        for i, w in enumerate(group.wyckoff):
+            p = generic[i]
+            q = [n.r[4 * k] * p[k] + Fraction(n.t[k], TDEN) for k in range(3)]
+            j = _position_of(group, q, w.multiplicity)
+            if j < 0:
+                break
+            perm.append(j)
+        if len(perm) == len(group.wyckoff) and perm != list(range(len(perm))):
+            perms.append(perm)
     return perms
 
 
 def dedupe_equivalent_assignments(assignments: List[dict], group: SpaceGroup) -> dict:
-    """One assignment of each set related by a normaliser permutation, the
-    first met (the enumeration's order is kept)."""
+    """The first assignment met of each class related by a normaliser
+    permutation (the enumeration's order is kept)."""
     perms = normalizer_permutations(group)
     if not perms:
-        return {'assignments': assignments, 'dropped': 0}
+        return {'assignments': list(assignments), 'dropped': 0}
 
-    def key_of(a, perm):
-        return '|'.join(sorted(f"{s['elementIdx']}:{perm[s['wIdx']] if perm else s['wIdx']}" for s in a['sites']))
+    def canonical(a):
+        base = [(s['elementIdx'], s['wIdx']) for s in a['sites']]
+        return min([tuple(sorted(base))] + [tuple(sorted((e, p[i]) for e, i in base)) for p in perms])
     seen, kept = set(), []
     for a in assignments:
-        key = key_of(a, None)
-        for perm in perms:
-            k = key_of(a, perm)
-            if k < key:
-                key = k
-        if key in seen:
-            continue
-        seen.add(key)
-        kept.append(a)
+        c = canonical(a)
+        if c not in seen:
+            seen.add(c)
+            kept.append(a)
     return {'assignments': kept, 'dropped': len(assignments) - len(kept)}
 
 
@@ -365,5 +408,4 @@ def to_search_assignment(group: SpaceGroup, assignment: dict):
 def assignment_labels(group: SpaceGroup, assignment: dict) -> List[tuple]:
     """[(element, '4c'), ...]: the form ``workloads.wyckoff_problem`` and
     ``wyckoff_tables.make_assignment`` take."""
-    return [(s['element'], f"{group.wyckoff[s['wIdx']].multiplicity}{group.wyckoff[s['wIdx']].letter}")
-            for s in assignment['sites']]
+    return [(s['element'], _label(group.wyckoff[s['wIdx']])) for s in assignment['sites']]

@@ -43,10 +43,10 @@ def test_centric_starts_have_the_measured_amplitudes_and_a_real_map(t):
     j = physics_job([IDENTITY, inversion(t)])
     m = build_reflection_model(j, 16)
     init = model_initial_grid(m, 16, j['seed'])
-    for g in range(m['nOrbits']):
-        expected = m['orbitTargetI'][g] / m['orbitCount'][g]
-        for p in range(m['orbitStart'][g], m['orbitStart'][g] + m['orbitCount'][g]):
-            i = int(m['orbitIdx'][p]) & IDX_MASK
+    for g in range(m['n_orbits']):
+        expected = m['orbit_target_i'][g] / m['orbit_count'][g]
+        for p in range(m['orbit_start'][g], m['orbit_start'][g] + m['orbit_count'][g]):
+            i = int(m['orbit_idx'][p]) & IDX_MASK
             assert abs(init[2 * i] ** 2 + init[2 * i + 1] ** 2 - expected) < 1e-6 * expected
     rho = density(init, 16)
     assert np.sum(rho.imag ** 2) < 1e-12 * np.sum(rho.real ** 2)
@@ -79,20 +79,20 @@ def test_model_invariants():
     absent list is the tail of orbitIdx."""
     j = synthetic_job()
     m = build_reflection_model(j, 32)
-    nm = m['nMembers']
-    idx = m['orbitIdx'][:nm] & IDX_MASK
-    absent = m['orbitIdx'][nm:]
+    nm = m['n_members']
+    idx = m['orbit_idx'][:nm] & IDX_MASK
+    absent = m['orbit_idx'][nm:]
     assert len(np.unique(idx)) == nm and 0 not in idx
     assert not set(idx.tolist()) & set(absent.tolist())
     # P2_1/c: Laue 2/m orbits of 2 or 4 members, the powder multiplicities
-    assert set(m['orbitCount'].tolist()) <= {2, 4}
+    assert set(m['orbit_count'].tolist()) <= {2, 4}
     absent_set = set(absent.tolist())
     allowed = [q for q in j['hklList']
                if (q['h_orig'] % 32) + (q['k_orig'] % 32) * 32 + (q['l_orig'] % 32) * 1024 not in absent_set]
     assert nm == sum(q['multiplicity'] for q in allowed)
-    for c in range(m['nClusters']):
-        s, n = m['clusterOrbitStart'][c], m['clusterNOrbits'][c]
-        assert m['clusterObsI'][c] >= np.sum(m['orbitTargetI'][s:s + n]) * (1 - 1e-6)
+    for c in range(m['n_clusters']):
+        s, n = m['cluster_orbit_start'][c], m['cluster_n_orbits'][c]
+        assert m['cluster_obs_i'][c] >= np.sum(m['orbit_target_i'][s:s + n]) * (1 - 1e-6)
 
 
 def test_systematic_absences_p21c():
@@ -132,8 +132,8 @@ def test_weak_classification_and_plan():
     j = physics_job([IDENTITY, inversion((0, 0, 0))])
     m = build_reflection_model(j, 16)
     w = classify_weak_orbits(m, .25, 'individual')
-    assert w['weakOrbits'] == 2 and w['flags'].sum() == 2
-    per = m['orbitTargetI'] / m['orbitCount']
+    assert w['weak_orbits'] == 2 and w['flags'].sum() == 2
+    per = m['orbit_target_i'] / m['orbit_count']
     assert set(np.nonzero(w['flags'])[0]) == set(np.argsort(per, kind='stable')[:2])
     p = cf_plan(9)
     assert [t['threshold'] for t in p['trials'][:3]] == [1.0, 1.1, 1.2]
@@ -159,20 +159,20 @@ def test_oracle_cycle_steps():
     flipped = np.where(rho < st.last_delta, -rho, rho)
     Ff = np.fft.fftn(flipped.reshape(32, 32, 32)).ravel()
     num = den = 0.0
-    for c in range(m['nClusters']):
-        s, n = m['clusterOrbitStart'][c], m['clusterNOrbits'][c]
+    for c in range(m['n_clusters']):
+        s, n = m['cluster_orbit_start'][c], m['cluster_n_orbits'][c]
         tot = 0.0
         for o in range(s, s + n):
-            idx = m['orbitIdx'][m['orbitStart'][o]:m['orbitStart'][o] + m['orbitCount'][o]] & IDX_MASK
+            idx = m['orbit_idx'][m['orbit_start'][o]:m['orbit_start'][o] + m['orbit_count'][o]] & IDX_MASK
             tot += np.sum(np.abs(Ff[idx]) ** 2)
-        num += abs(math.sqrt(tot) - math.sqrt(m['clusterObsI'][c]))
-        den += math.sqrt(m['clusterObsI'][c])
+        num += abs(math.sqrt(tot) - math.sqrt(m['cluster_obs_i'][c]))
+        den += math.sqrt(m['cluster_obs_i'][c])
     assert abs(R - num / den) <= 1e-12
-    for o in range(m['nOrbits']):
-        idx = m['orbitIdx'][m['orbitStart'][o]:m['orbitStart'][o] + m['orbitCount'][o]] & IDX_MASK
+    for o in range(m['n_orbits']):
+        idx = m['orbit_idx'][m['orbit_start'][o]:m['orbit_start'][o] + m['orbit_count'][o]] & IDX_MASK
         a = np.abs(st.F[idx])
         assert np.max(a) - np.min(a) <= 1e-9 * max(1.0, np.max(a))
-    assert np.all(st.F[m['orbitIdx'][m['nMembers']:]] == 0) and st.F[0] == 0
+    assert np.all(st.F[m['orbit_idx'][m['n_members']:]] == 0) and st.F[0] == 0
 
 
 def test_oracle_converges_on_the_synthetic_structure():

@@ -143,7 +143,7 @@ def test_create_rejects_inconsistent_models(model):
     with pytest.raises(P6Error):
         CFSession(bad, [{'threshold': 1.1}])
     dup = dict(m)
-    dup['orbitIdx'] = m['orbitIdx'].copy()
-    dup['orbitIdx'][1] = dup['orbitIdx'][0]
+    dup['orbit_idx'] = m['orbit_idx'].copy()
+    dup['orbit_idx'][1] = dup['orbit_idx'][0]
     with pytest.raises(P6Error, match='claimed twice'):
         CFSession(dup, [{'threshold': 1.1}])
