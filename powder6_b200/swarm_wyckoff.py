@@ -554,7 +554,7 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                        on_progress: Optional[Callable[[dict], None]] = None,
                        should_stop: Optional[Callable[[], bool]] = None, do_quench: bool = True,
                        target_cc: Optional[float] = None, assignment_ids: Optional[Sequence[int]] = None,
-                       prune: bool = True, refine: bool = False) -> SearchResult:
+                       prune: bool = True, refine: bool = False, world: int = 1) -> SearchResult:
     """One wave of assignments (``assignment_ids``, default all of the
     problem's), ``restarts`` independent restarts, all generations on the
     device, then the quench of the per-assignment bests.  Particles are shared
@@ -569,8 +569,16 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
     boundary (or the end of the quench) at which the best cc reached it.
     With ``refine``, the best structure of every assignment is then refined
     by least squares against the grouped |F|^2 (``refine_coordinates``) and
-    the result carries the refined coordinates and wR(F^2) in ``refined``."""
+    the result carries the refined coordinates and wR(F^2) in ``refined``.
+
+    Sharded over ``world`` ranks (one process per GPU, each with its own
+    replicas, ladders and seed), every rank calls this with the same problem,
+    schedule and chunking; at every chunk boundary the per-assignment bests
+    are merged over the ranks (``dist.bests_over_ranks``), the prune decides
+    on the global bests, a stop request on any rank stops all of them, and
+    every rank returns the same per-assignment winners."""
     import time
+    from .dist import any_over_ranks, bests_over_ranks, max_per_assignment
     t_start = time.perf_counter()
     d = dict(SW_DEFAULTS)
     d.update(settings or {})
@@ -611,7 +619,16 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                 per_a[A] = {'cc': float(st['best_cc'][i]), 'pen': float(st['best_pen'][i]),
                             'coords': bestpos[i * cpp:(i + 1) * cpp].copy()}
 
+    stop = False
+
+    def merge():
+        nonlocal per_a
+        if world > 1:
+            per_a = bests_over_ranks(per_a, nA, cpp, scale, world)
+
     for restart in range(restarts):
+        if stop:
+            break
         pos = np.array([rnd() for _ in range(n * cpp)], dtype=np.float32)
         pos = project_all(problem, pos, assign_of)
         st = initial_state(n, temps, rnd, d)
@@ -619,7 +636,10 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
         g0 = 0
         force_eval = False
         while g0 < generations:
-            if should_stop and should_stop():
+            stop = bool(should_stop and should_stop())
+            if world > 1:
+                stop = any_over_ranks(stop, world)
+            if stop:
                 break
             end = min(g0 + chunk, generations)
             if restart == 0 and do_prune and g0 < prune_at:
@@ -631,10 +651,18 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
             sess.synchronize(600.0)
             total_ms += sess.last_kernel_ms()
             g0 += ng
+            if world > 1:
+                _, bp_sync, st_sync = sess.read_state()
+                record(st_sync, bp_sync)
+                merge()
             if target_cc is not None and hit is None and g0 < generations:
-                _, _, stc = sess.read_state()
-                ok = stc['best_fit'] > -1e29
-                if np.any(ok) and float(np.max(stc['best_cc'][ok])) >= target_cc:
+                if world > 1:
+                    reached = any(v['cc'] >= target_cc for v in per_a.values())
+                else:
+                    _, _, stc = sess.read_state()
+                    ok = stc['best_fit'] > -1e29
+                    reached = bool(np.any(ok) and float(np.max(stc['best_cc'][ok])) >= target_cc)
+                if reached:
                     hit = time.perf_counter() - t_start
             if restart == 0 and do_prune and g0 == prune_at:
                 # successive halving on the bests so far, at the current penalty weight
@@ -646,6 +674,7 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                     if stp['best_fit'][i] > -1e29:
                         A = int(assign_of[i])
                         gbest[A] = max(gbest.get(A, -math.inf), float(stp['best_cc'][i] - stp['best_pen'][i] * now))
+                gbest = max_per_assignment(gbest, nA, world)
                 keep = prune_assignments(ids, gbest, 0.5, 4)
                 if len(keep) < len(ids):
                     ids = keep
@@ -673,19 +702,30 @@ def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, gener
                     sess.write_state_fixed(cur_fx.reshape(-1), best_fx.reshape(-1), stp)
                     force_eval = True
             if on_progress:
-                on_progress({'restart': restart + 1, 'restarts': restarts, 'generation': g0 - 1,
-                             'generations': generations})
+                info = {'restart': restart + 1, 'restarts': restarts, 'generation': g0,
+                        'generations': generations,
+                        'fraction': (restart + g0 / generations) / restarts}
+                _, bp, sp = sess.read_state()
+                ok = np.nonzero(sp['best_fit'] > -1e29)[0]
+                if len(ok):
+                    now = float(pen[g0 - 1])
+                    i = int(ok[np.argmax(sp['best_cc'][ok] - sp['best_pen'][ok] * now)])
+                    info.update(best=float(sp['best_cc'][i] - sp['best_pen'][i] * now), cc=float(sp['best_cc'][i]),
+                                assignment=int(assign_of[i]), coords=bp[i * cpp:(i + 1) * cpp].copy())
+                on_progress(info)
         cur, bestpos, st = sess.read_state()
         acc_total += int(st['accepted'].sum())
         record(st, bestpos)
+        merge()
     qinfo = {}
-    if do_quench and per_a and not (should_stop and should_stop()):
+    if do_quench and per_a and not stop:
         before = {A: v['cc'] for A, v in per_a.items()}
         q = quench(problem, sess, per_a, rnd, d)
         qinfo = {'ms': q.pop('_ms'), 'improved': int(sum(1 for A in q if q[A].get('improved'))),
                  'best_before': max(before.values())}
         total_ms += qinfo['ms']
         per_a = q
+        merge()
         sess.set_assign(assign_of)
         sess.set_schedule(groups, pen)
     best = {'cc': -np.inf, 'pen': 0.0, 'coords': None, 'A': 0}
@@ -784,6 +824,15 @@ def refine_coordinates(sess: WyckoffSession, coords: np.ndarray, assign: Sequenc
     return {'coords': x, 'r_start': r0, 'r': r1, 'chi2': chi, 'iterations': it, 'converged': cv.astype(bool)}
 
 
+def _wave_progress(on_progress: Callable[[dict], None], k: int, waves: int, stage: str):
+    """A progress callback that adds the wave and the stage to each report."""
+    def report(p: dict):
+        q = dict(p, wave=k + 1, waves=waves, stage=stage)
+        q['fraction'] = (k + p.get('fraction', 0.0)) / waves
+        on_progress(q)
+    return report
+
+
 def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
                       restarts: int = 1, seed: int = 20261026, cos_mode: int = 0,
                       settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
@@ -800,6 +849,8 @@ def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, genera
     per-assignment bests, trials and device time of all waves."""
     d = dict(SW_DEFAULTS)
     d.update(settings or {})
+    on_progress = kwargs.pop('on_progress', None)
+    should_stop = kwargs.get('should_stop')
     own = session is None
     sess = session or WyckoffSession(problem, num_particles, run_key=seed, cos_mode=cos_mode, settings=settings)
     n, min_per, dims = sess.num_particles, int(d['minParticlesPerAssignment']), assignment_dims(problem)
@@ -813,7 +864,10 @@ def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, genera
             skw['do_quench'] = False
             skw.pop('target_cc', None)
             bests: Dict[int, dict] = {}
-            for k, w in enumerate(allocate_waves(all_ids, n, min_per, dims)):
+            screen_waves = allocate_waves(all_ids, n, min_per, dims)
+            for k, w in enumerate(screen_waves):
+                if on_progress is not None:
+                    skw['on_progress'] = _wave_progress(on_progress, k, len(screen_waves), 'screen')
                 r = run_wyckoff_search(problem, n, g_screen, 1, seed + 104729 * k, cos_mode, settings=settings,
                                        session=sess, assignment_ids=w, **skw)
                 screen_results.append(r)
@@ -825,9 +879,15 @@ def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, genera
                 raise RuntimeError('The screening produced no finite score for any assignment.')
         waves = allocate_waves(kept, n, min_per, dims)
         scale = float(schedule(generations, problem.refl.n_groups, d)[1][-1])
-        results = [run_wyckoff_search(problem, n, generations, restarts, seed + 7919 * k, cos_mode,
-                                      settings=settings, session=sess, assignment_ids=w, **kwargs)
-                   for k, w in enumerate(waves)]
+        results = []
+        for k, w in enumerate(waves):
+            kw = dict(kwargs)
+            if on_progress is not None:
+                kw['on_progress'] = _wave_progress(on_progress, k, len(waves), 'search')
+            results.append(run_wyckoff_search(problem, n, generations, restarts, seed + 7919 * k, cos_mode,
+                                              settings=settings, session=sess, assignment_ids=w, **kw))
+            if should_stop is not None and should_stop():
+                break
     finally:
         if own:
             sess.close()

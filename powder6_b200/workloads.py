@@ -156,14 +156,36 @@ def wyckoff_problem(seed: int = 1, group_number: int = 62,
         fo2 = i_true + rng.normal() * sigma
         tth = 2 * math.degrees(math.asin(min(1.0, wavelength / (2 * r.d0))))
         rows.append({'h': r.h, 'k': r.k, 'l': r.l, 'mult': r.m, 'Fo2': fo2, 'sigma': sigma, 'd': r.d0, 'tth': tth})
+    return build_problem(group, cell, demand, [sites, *extra_assignments], rows, windows, min_contact, true)
+
+
+def build_problem(group: SpaceGroup, cell: Dict[str, float], demand: List[dict],
+                  label_sets: Sequence[Sequence[Tuple[str, str]]], rows: Sequence[dict],
+                  windows: Sequence[dict] = (), min_contact: Optional[float] = None,
+                  true_coords: Optional[np.ndarray] = None, overall_b: float = 0.0) -> WyckoffProblem:
+    """A search problem from observation rows ({h, k, l, mult, Fo2, sigma, d,
+    tth}: |F|^2 per reflection with multiplicity and Lp removed) and one or
+    more site assignments ([(element, '4c'), ...] each): the packed reflection
+    groups, the scattering table, the assignment and restraint tables and the
+    cell's reduced basis."""
+    ff_table = load_form_factor_table()
+    missing = sorted({d['element'] for d in demand if d['element'] not in ff_table})
+    if missing:
+        raise ValueError(f'No X-ray scattering factor for {", ".join(missing)}.')
+    assignments = [make_assignment(group, demand, a) for a in label_sets]
+    tables = build_assignment_tables(assignments, group, demand)
     refl = pack_reflections(rows)
-    f_tab, n_elem, _missing = scattering_table(refl, demand, ff, 0.0)
+    f_tab, n_elem, _missing = scattering_table(refl, demand, gaussian_form_factor(ff_table), overall_b)
     restraints = build_restraint_tables(demand, list(windows), min_contact)
     red = reduced_cell(cell)
     orth0 = orth_matrix(cell).astype(np.float64)
+    true = None
+    if true_coords is not None:
+        true = np.zeros(tables.max_sites * 3)
+        true[:len(true_coords)] = true_coords[:tables.max_sites * 3]
     prob = WyckoffProblem(group, cell, demand, assignments, tables, refl, f_tab, n_elem, restraints,
                           pack_sym_ops(group.ops), has_inversion_at_origin(group.ops), red.orth, red.xform,
-                          inverse3(orth0), 1 if restraints.max_distance > red.safe_radius else 0, true, rows)
+                          inverse3(orth0), 1 if restraints.max_distance > red.safe_radius else 0, true, list(rows))
     # penBond / penCoord per charged slot (js/swarm_wyckoff.js:1482-1506)
     n_of = {d['element'].upper(): d['count'] for d in demand}
     bond_slots, coord_centres = 0, 0
@@ -275,3 +297,35 @@ def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelengt
         points = int(round(_log_uniform(rng, 2000, 12000)))
         out.append(BatchItem(prob, replicas, points, target))
     return out
+
+
+def wyckoff_job(problem: WyckoffProblem, wavelength: float = 1.5406, polarisation_k: float = 1.0,
+                **fields) -> dict:
+    """A 'wyckoff-search' job message (js/rietveld/rv_solve.js:800-803) for a
+    synthetic problem: the group's operators and Wyckoff table, the cell, the
+    composition per formula unit with Z, and its reflections as the WPPF
+    extraction hands them over (intensity = |F|^2 m Lp, sigma on the same
+    scale, 2-theta, d, multiplicity and Lp)."""
+    from math import gcd
+    g = problem.group
+    counts = [d['count'] for d in problem.demand]
+    Z = 0
+    for c in counts:
+        Z = gcd(Z, c)
+    formula = ''.join(f"{d['element']}{d['count'] // Z if d['count'] // Z > 1 else ''}" for d in problem.demand)
+    hkl = []
+    for r in problem.rows:
+        th = math.radians(0.5 * r['tth'])
+        lp = (1.0 / (math.sin(th) ** 2 * math.cos(th))) * (1 + polarisation_k * math.cos(2 * th) ** 2) / \
+            (1 + polarisation_k)
+        k = r['mult'] * lp
+        hkl.append({'h_orig': r['h'], 'k_orig': r['k'], 'l_orig': r['l'], 'intensity': r['Fo2'] * k,
+                    'sigma': r['sigma'] * k, 'multiplicity': r['mult'], 'tth': r['tth'], 'd': r['d'], 'lp': lp})
+    job = {'type': 'wyckoff-search', 'cell': dict(problem.cell),
+           'symops': [{'xyz': None, 'r': list(o.r), 't_num': list(o.t), 't_den': 24} for o in g.ops],
+           'wyckoffTable': [{'letter': w.letter, 'multiplicity': w.multiplicity, 'special_op': w.triplet,
+                             'n_free': w.n_free} for w in g.wyckoff],
+           'targetComposition': formula, 'wyckoffZ': Z, 'hklList': hkl, 'wavelength': wavelength,
+           'polarization': {'K': polarisation_k}, 'applyLP': True, 'seed': 1}
+    job.update(fields)
+    return job

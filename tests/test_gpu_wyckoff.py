@@ -821,3 +821,27 @@ def test_search_then_refinement(prob):
     ref = res.refined[0]
     assert ref['converged'] and ref['r'] <= ref['r_start'] + 1e-12
     assert ref['r'] < 0.02
+
+
+def test_worker_job_runs_on_the_device():
+    """A 'wyckoff-search' job message through the worker protocol to the
+    device search and back: the enumerated PbSO4 assignments are searched,
+    the progress stream carries the best so far, the winner is re-scored on
+    the CPU and refined, and the final message is wy-structure."""
+    from powder6_b200.workloads import wyckoff_job
+    from powder6_b200.wyckoff_worker import WyckoffWorker
+    P = wyckoff_problem(seed=1)
+    out = []
+    w = WyckoffWorker(out.append, threaded=False)
+    w.on_message(wyckoff_job(P, swarmParticles=4096, swarmIterations=4000, seed=5))
+    kinds = [m['type'] for m in out]
+    assert kinds[0] == 'wy-start' and kinds[-1] == 'wy-structure', [m.get('message') for m in out]
+    prog = [m for m in out if m['type'] == 'wy-progress']
+    assert len(prog) >= 10 and all(m['bestSites'] for m in prog)
+    assert prog[-1]['generation'] == 4000 and prog[-1]['fraction'] == pytest.approx(1.0)
+    res = out[-1]['results']
+    sol = res['wyckoffResult']
+    assert sol['cpuCheck']['delta'] < 1e-5
+    assert res['refinement']['R'] <= res['refinement']['RStart'] + 1e-12
+    assert sum(s['multiplicity'] for s in res['sites']) == 24
+    print('worker found', sol['assignment'], 'cc', sol['searchCC'], 'R', res['refinement'])
