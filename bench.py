@@ -50,7 +50,8 @@ def parse():
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--particles', type=int, default=PARTICLES)
     ap.add_argument('--generations', type=int, default=GENERATIONS)
-    ap.add_argument('--cos-mode', type=int, default=0)
+    ap.add_argument('--cos-mode', type=int, default=-1,
+                    help='0 SFU cosine, 1 FMA polynomial, 2 factored FP64; -1 (default): 2 where the group allows it')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--workload', default='wyckoff',
                     choices=['wyckoff', 'pt', 'contract', 'batch', 'learned', 'refine', 'cf'],
@@ -166,7 +167,7 @@ def wyckoff_time_to_target(P, n, sess):
     start, generations in chunks of 250 so the best can be read between
     launches) to the first chunk boundary, or the end of the quench, at
     which the best wR2 is within the target."""
-    from powder6_b200.swarm_wyckoff import run_wyckoff_search
+    from powder6_b200.swarm_wyckoff import COS_NAMES, run_wyckoff_search
     conv = run_wyckoff_search(P, num_particles=n, generations=GENERATIONS, seed=11, session=sess)
     wr2 = 1.0 - conv.best_cc
     target = 1.0 - 1.05 * wr2
@@ -176,7 +177,7 @@ def wyckoff_time_to_target(P, n, sess):
     return {'median_s': float(np.median(hits)) if hits else None, 'reached': f'{len(hits)}/{len(runs)}',
             'converged_wr2': wr2, 'target_wr2': 1.05 * wr2,
             'final_wr2': [1.0 - r.best_cc for r in runs], 'cpu_check_delta': [r.cpu_check.get('delta') for r in runs],
-            'note': 'chunks of 250 generations; plain FP32 search (SFU cosine) + quench'}
+            'note': f'chunks of 250 generations; plain search ({COS_NAMES[sess.cos_mode]}) + quench'}
 
 
 def run_reference_batch(args, world, rank):
@@ -1051,14 +1052,16 @@ def main():
             dist.destroy_process_group()
         return
     import torch
-    from powder6_b200.swarm_wyckoff import (WyckoffSession, build_ladders, initial_state, project_all,
-                                            schedule)
+    from powder6_b200.swarm_wyckoff import (COS_FACTORED, COS_NAMES, WyckoffSession, build_ladders,
+                                            default_cos_mode, initial_state, project_all, schedule)
     from powder6_b200.workloads import mulberry32, wyckoff_problem
     torch.cuda.set_device(local)
     P = wyckoff_problem(seed=1)
     n = args.particles
     G = args.generations
     groups, pen = schedule(G, P.refl.n_groups)
+    if args.cos_mode < 0:
+        args.cos_mode = default_cos_mode(P)
     sess = WyckoffSession(P, n, run_key=1000 + rank, cos_mode=args.cos_mode, device=local)
     assign = np.zeros(n, dtype=np.uint32)
     sess.set_assign(assign)
@@ -1115,26 +1118,41 @@ def main():
         nsm = torch.cuda.get_device_properties(local).multi_processor_count
         mhz = clocks['sm_mhz'] or 1965.0
         peak = MUFU_PER_CLK_PER_SM * nsm * mhz * 1e6 / 1e9
-        traffic = None
+        traffic, inst_per_trial = None, None
         tf = ROOT / 'profiles' / 'wy_kernel_traffic.txt'
         if tf.exists():
             for ln in tf.read_text().splitlines():
                 if ln.startswith('bytes_per_launch:'):
                     traffic = int(ln.split(':', 1)[1])
+                if ln.startswith('warp_instructions_per_trial:'):
+                    inst_per_trial = float(ln.split(':', 1)[1])
+        sfu = {'bound': 'sfu', 'achieved': achieved, 'peak': peak, 'unit': 'Gcos/s', 'frac': achieved / peak,
+               'traffic': traffic,
+               'note': f'{cos_total:.4g} algorithmic cosines per launch (the reference\'s count); peak = '
+                       f'{MUFU_PER_CLK_PER_SM} SFU ops/clk/SM x {nsm} SMs x {mhz:.0f} MHz (median SM clock under load)'}
+        if args.cos_mode == COS_FACTORED and inst_per_trial:
+            # the factored evaluation issues no cosine per term: the bound is instruction issue
+            issue_peak = 4 * nsm * mhz * 1e6 / 1e9
+            issued = inst_per_trial * trials_per_step / (ms / 1000.0) / 1e9
+            roofline = {'bound': 'issue', 'achieved': issued, 'peak': issue_peak, 'unit': 'Gwarp-inst/s',
+                        'frac': issued / issue_peak, 'traffic': traffic,
+                        'note': f'{inst_per_trial:.0f} warp instructions per trial (ncu, small case of the same '
+                                f'search) x trials/s; peak = 4 warp instructions/clk/SM x {nsm} SMs x {mhz:.0f} MHz',
+                        'sfu_equivalent': sfu}
+        else:
+            roofline = sfu
         line = {
             'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp32', 'data': 'synthetic',
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'fp64' if args.cos_mode == COS_FACTORED else 'fp32',
+            'data': 'synthetic',
             'config': {'workload': f'wyckoff-search Pnma PbSO4-like (Pb 4c, S 4c, O 4c, O 4c, O 8d; 24 atoms/cell), '
                                    f'{n} replicas x {G} generations per GPU, d_min 1.2 A '
                                    f'({P.refl.n_refl} reflections, {P.refl.n_groups} groups)',
                        'replicas_per_gpu': n, 'generations': G, 'step': 'one full search, one launch',
-                       'l2': 'flushed before every step (256 MB write)', 'cos': ['sfu', 'poly'][args.cos_mode],
+                       'l2': 'flushed before every step (256 MB write)', 'cos': COS_NAMES[args.cos_mode],
                        'parallelism': f'replicas only x{world}'},
-            'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak, 'unit': 'Gcos/s',
-                         'frac': achieved / peak, 'traffic': traffic,
-                         'note': f'{cos_total:.4g} algorithmic cosines per launch; peak = {MUFU_PER_CLK_PER_SM} '
-                                 f'SFU ops/clk/SM x {nsm} SMs x {mhz:.0f} MHz (median SM clock under load)'},
+            'roofline': roofline,
             'e2e': {'value': e2e_value, 'unit': 'trials/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
             'gpu_launches': int(launches),
             'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},

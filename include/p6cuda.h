@@ -112,7 +112,11 @@ typedef struct {
   /* Robbins-Monro step adaptation (exp(a(1-t)), exp(-a t)) and bounds */
   float step_up, step_down, step_min, step_max;
   /* fitness arithmetic: 0 = SFU cosine on the integer-reduced phase,
-   * 1 = FMA-pipe polynomial (slower, closer to FP64) */
+   * 1 = FMA-pipe polynomial (slower, closer to FP64), 2 = factored FP64:
+   * per site and axis cos/sin tables of 2 pi n x built in FP64 from the exact
+   * 32-bit turn, |F| as per-reflection monomials of three table entries,
+   * FP64 |F|^2 and sums (groups whose rotations are all diagonal: triclinic,
+   * monoclinic, orthorhombic; no incremental form; not in batched launches) */
   int cos_mode;
   uint32_t run_key; /* key of the counter-based generator for this session */
   /* per-replica site sums of |F| kept in shared memory so a proposal
@@ -216,6 +220,11 @@ p6_status p6_wy_read_trace(p6_wy_session *s, uint32_t *proposals, float *records
 /* mult * |F|^2 of every reflection of each particle's last traced evaluation
  * (num_particles * n_refl floats; reflections past the active groups untouched). */
 p6_status p6_wy_read_trace_ic(p6_wy_session *s, float *ic);
+/* The FP64 fitness sums {sum w Ic^2, sum w Io^2, sum w Ic Io} over the active
+ * groups of each particle's last traced evaluation (num_particles * 3
+ * doubles); cc = sco / sqrt(scc soo), the grouped wR2^2 after the best scale
+ * is 1 - cc^2 (js/swarm_wyckoff.js:679-766). */
+p6_status p6_wy_read_trace_sums(p6_wy_session *s, double *sums);
 /* The generated cell of one particle's current coordinates, in genPack order,
  * fixed point (n_tot * 3 words). */
 p6_status p6_wy_debug_expand(p6_wy_session *s, int particle, uint32_t *atoms);
@@ -320,6 +329,13 @@ p6_status p6_pt_batch(p6_pt_session *s, int count, int bootstrap);
 p6_status p6_pt_read_state(p6_pt_session *s, float *state, double *x, double *best, double *costs, double *counters);
 p6_status p6_pt_synchronize(p6_pt_session *s, double timeout_seconds);
 p6_status p6_pt_last_batch_ms(p6_pt_session *s, float *ms);
+/* Parity support: record, for every chain, the decisions of the last sweep
+ * of each p6_pt_batch: {exchange tried, swapped, la, log u} and then per
+ * move {parameter index, proposed value, log u, cost before, proposal cost,
+ * accepted} (chains * (4 + 6 nv) doubles), for replaying the Metropolis and
+ * exchange rules of temper (js/rietveld_core.js:2171-2241) on the host. */
+p6_status p6_pt_set_trace(p6_pt_session *s, int enable);
+p6_status p6_pt_read_trace(p6_pt_session *s, double *out);
 p6_status p6_pt_launch_count(p6_pt_session *s, long long *count);
 /* CTAs per chain in the sweeps: 2 runs each chain on a two-CTA cluster (the
  * pattern's tiles split between them, chi^2 combined through distributed

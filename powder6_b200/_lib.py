@@ -14,6 +14,7 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / 'libp6cuda.so'
 
 P6_OK = 0
+P6_ERR_CAPACITY = 2
 STATUS_NAMES = {0: 'OK', 1: 'INVALID_ARG', 2: 'CAPACITY', 3: 'DEVICE_LOST', 4: 'TIMEOUT', 5: 'NOT_CONVERGED',
                 6: 'VALIDATION', 7: 'CUDA'}
 
@@ -98,6 +99,7 @@ _SIGS = {
     'p6_wy_set_trace': (C.c_int, [_P, C.c_int]),
     'p6_wy_read_trace': (C.c_int, [_P, _P, _P]),
     'p6_wy_read_trace_ic': (C.c_int, [_P, _P]),
+    'p6_wy_read_trace_sums': (C.c_int, [_P, _P]),
     'p6_wy_debug_expand': (C.c_int, [_P, C.c_int, _P]),
     'p6_wy_last_kernel_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_wy_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
@@ -111,6 +113,8 @@ _SIGS = {
     'p6_pt_synchronize': (C.c_int, [_P, C.c_double]),
     'p6_pt_last_batch_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_pt_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    'p6_pt_set_trace': (C.c_int, [_P, C.c_int]),
+    'p6_pt_read_trace': (C.c_int, [_P, _P]),
     'p6_pt_set_split': (C.c_int, [_P, C.c_int]),
     'p6_pt_get_split': (C.c_int, [_P, C.POINTER(C.c_int)]),
     'p6_pt_costs_static': (C.c_int, [_P, _P, C.c_int, _P, _P]),

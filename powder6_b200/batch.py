@@ -92,7 +92,8 @@ def setup_searches(items: Sequence[BatchItem], generations: int = 2000, seed: in
     sessions, starts, gens = [], [], []
     for k, it in enumerate(items):
         P = it.problem
-        s = WyckoffSession(P, it.replicas, run_key=seed * 1000 + k, settings=settings, incremental=0)
+        s = WyckoffSession(P, it.replicas, run_key=seed * 1000 + k, cos_mode=0, settings=settings,
+                               incremental=0)
         n = s.num_particles
         assign = np.zeros(n, dtype=np.uint32)
         s.set_assign(assign)

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -125,6 +126,15 @@ struct Params {
   int genOff, projOff, atomsOff, icOff;  // offsets inside the slice
   int cbOff, atoms2Off, nReflPad;          // incremental site sums and the second atom bank
   int curOff, propOff, runsOff, slotOff;   // WarpView offsets
+  // factored FP64 structure factors (cos mode 2): blob offsets of the monomial
+  // coefficients (real, imaginary or -1 when every one is real), their table
+  // indices and the FP64 scattering factors; the per-axis table shape; the
+  // per-warp offsets of the site tables and their coordinate tags
+  int offK, offKi, offIdx, offF64;
+  int nMono, tabLen, tabE;
+  int axE[3], axOff[3];
+  int tabOff, tagOff;
+  double *traceSums;       // per particle {scc, soo, sco} of the last traced evaluation (FP64)
 };
 
 // ---------------------------------------------------------------------------
@@ -510,6 +520,195 @@ __device__ __forceinline__ void fitness_direct(const Params &P, const WarpView &
   }
   __syncwarp();
   group_sums(P, ic, groups, sooPrefix, nga, lane, sums);
+}
+
+// ---------------------------------------------------------------------------
+// Factored FP64 structure factors (cos mode 2), for groups whose rotations are
+// all diagonal (triclinic, monoclinic, orthorhombic).  With R_j = diag(sigma_j)
+// the image phase separates by axis, e^{2 pi i h.(R_j x + t_j)} = e^{2 pi i h.t_j}
+// prod_a (c_a + i sigma_ja sgn(h_a) s_a), c_a = cos 2 pi |h_a| x_a,
+// s_a = sin 2 pi |h_a| x_a.  Summed over the N_p operators modulo centring, a
+// site with n_s images entering |F|^2 contributes
+//   S_s(h) = n_s sum_m K_m(h) prod_a (bit a of m ? s_a : c_a),
+//   K_m(h) = (1/N_p) sum_j e^{2 pi i h.t_j} prod_{a in m} i sigma_ja sgn(h_a),
+// because each image is reached by |stabiliser| = N_p / n_s operators.  K
+// depends on the reflection alone (host-side, exact phases); an mmm group
+// leaves one monomial per reflection, 2/m two.  Per site and evaluation the
+// warp builds cos and sin of 2 pi n x_a for n = 0..max |h_a| from the exact
+// 32-bit turn n x_a, in FP64; n_s is folded into the x table.  A table is
+// rebuilt only when its site's coordinates differ from the ones it was built
+// for (the tag), so a single-site move rebuilds one table.  |F|^2, the group
+// sums and the fitness sums are FP64 throughout.
+// ---------------------------------------------------------------------------
+// sin and cos of 2 pi t for a 32-bit turn t: quarter-turn reduction in
+// integers, then the Taylor series of sin and cos of phi = x pi / 2 with
+// |x| <= 1/2 through x^15 and x^16 (truncation below 1e-17).
+__device__ __forceinline__ void sincos_turn_f64(uint32_t ph, double *s_out, double *c_out) {
+  const uint32_t q = (ph + 0x20000000u) >> 30;
+  const int r = (int)(ph - (q << 30));
+  const double x = (double)r * (kHalfPi / 1073741824.0);
+  const double x2 = x * x;
+  const double sp = x * fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, -1.0 / 1307674368000.0,
+                                                                             1.0 / 6227020800.0),
+                                                                     -1.0 / 39916800.0),
+                                                             1.0 / 362880.0),
+                                                     -1.0 / 5040.0),
+                                             1.0 / 120.0),
+                                     -1.0 / 6.0),
+                             1.0);
+  const double cp =
+      fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, fma(x2, 1.0 / 20922789888000.0,
+                                                                  -1.0 / 87178291200.0),
+                                                          1.0 / 479001600.0),
+                                                  -1.0 / 3628800.0),
+                                          1.0 / 40320.0),
+                                  -1.0 / 720.0),
+                          1.0 / 24.0),
+                  -0.5),
+          1.0);
+  double cs = (q & 1u) ? sp : cp;
+  double sn = (q & 1u) ? cp : sp;
+  if ((q + 1u) & 2u) cs = -cs;   // q = 1, 2
+  if (q & 2u) sn = -sn;          // q = 2, 3
+  *s_out = sn;
+  *c_out = cs;
+}
+
+// Rebuild the per-axis tables of the sites whose coordinates (in `sites`)
+// differ from their tags.  Table of site s: per axis a, cos(2 pi n x_a) for
+// n < axE[a] then sin, starting at axOff[a]; the x table is scaled by n_s.
+// One stale site at a time, its entries over the lanes.
+__device__ __forceinline__ void factor_tables(const Params &P, const WarpView &ws, const uint32_t *sites,
+                                              double *tab, uint4 *tag, int lane) {
+  const int nRuns = ws.meta[1];
+  bool need = false;
+  if (lane < nRuns) {
+    const int s = ws.runs[lane].w & 0xFF;
+    const uint4 t = tag[s];
+    need = !(t.w != 0u && t.x == sites[3 * s] && t.y == sites[3 * s + 1] && t.z == sites[3 * s + 2]);
+  }
+  uint32_t mask = __ballot_sync(0xffffffffu, need);
+  const int e0 = P.axE[0], e01 = P.axE[0] + P.axE[1];
+  while (mask) {
+    const int q = __ffs(mask) - 1;
+    mask &= mask - 1u;
+    const int4 run = ws.runs[q];
+    const int s = run.w & 0xFF;
+    const double ns = (double)(run.y - run.x);
+    double *t = tab + (size_t)s * P.tabLen;
+    for (int j = lane; j < P.tabE; j += 32) {
+      const int a = j < e0 ? 0 : (j < e01 ? 1 : 2);
+      const int n = j - (a == 0 ? 0 : (a == 1 ? e0 : e01));
+      double sn, cs;
+      sincos_turn_f64((uint32_t)n * sites[3 * s + a], &sn, &cs);
+      if (a == 0) {
+        sn *= ns;
+        cs *= ns;
+      }
+      t[P.axOff[a] + n] = cs;
+      t[P.axOff[a] + P.axE[a] + n] = sn;
+    }
+  }
+  if (need) {
+    const int s = ws.runs[lane].w & 0xFF;
+    tag[s] = make_uint4(sites[3 * s], sites[3 * s + 1], sites[3 * s + 2], 1u);
+  }
+  __syncwarp();
+}
+
+// Group sums scc, sco (FP64) from FP64 mult |F|^2; soo from the prefix table.
+__device__ __forceinline__ void group_sums_f64(const double *ic, const float4 *groups, const double *sooPrefix,
+                                               int nga, int lane, double sums[3]) {
+  double dcc = 0.0, dco = 0.0;
+  for (int g = lane; g < nga; g += 32) {
+    const float4 gm = groups[g];
+    if (!(gm.w > 0.f)) continue;
+    const int start = (int)gm.x, cnt = (int)gm.y;
+    double iCalc = 0.0;
+    for (int m = 0; m < cnt; ++m) iCalc += ic[start + m];
+    const double wc = (double)gm.w * iCalc;
+    dcc = fma(wc, iCalc, dcc);
+    dco = fma(wc, (double)gm.z, dco);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dcc += __shfl_xor_sync(0xffffffffu, dcc, o);
+    dco += __shfl_xor_sync(0xffffffffu, dco, o);
+  }
+  sums[0] = dcc;
+  sums[1] = sooPrefix[nga];
+  sums[2] = dco;
+  __syncwarp();
+}
+
+// mult |F|^2 of reflections base + lane and base + lane + 32 from the site
+// tables: F(h) = sum_k K_k(h) sum_s f_s(h) T_{s,k}(h), T a product of three
+// table entries whose indices (10 bits each) the host packed per (k, h).  The
+// two reflections of a lane share each run's loads; their table offsets are
+// unpacked once per monomial, outside the loop over sites.
+__device__ __forceinline__ void factored_rows(const Params &P, const WarpView &ws, const double *tab, double *ic,
+                                              const ReflRec *refl, const unsigned char *stat, int base, int nAct,
+                                              int lane, float *traceIc) {
+  constexpr int NR = 2;
+  const int nRuns = ws.meta[1];
+  const int nM = P.nMono, pad = P.nReflPad, tl = P.tabLen;
+  const double *kre = reinterpret_cast<const double *>(stat + P.offK);
+  const double *kim = P.offKi >= 0 ? reinterpret_cast<const double *>(stat + P.offKi) : nullptr;
+  const uint32_t *idx = reinterpret_cast<const uint32_t *>(stat + P.offIdx);
+  const double *f64 = reinterpret_cast<const double *>(stat + P.offF64);
+  int r[NR];
+  double fr[NR], fi[NR];
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    r[j] = min(base + lane + 32 * j, nAct - 1);
+    fr[j] = 0.0;
+    fi[j] = 0.0;
+  }
+  for (int k = 0; k < nM; ++k) {
+    int o0[NR], o1[NR], o2[NR];
+    double acc[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+      const uint32_t w = idx[k * pad + r[j]];
+      o0[j] = (int)(w & 0x3FFu);
+      o1[j] = (int)((w >> 10) & 0x3FFu);
+      o2[j] = (int)(w >> 20);
+      acc[j] = 0.0;
+    }
+    for (int q = 0; q < nRuns; ++q) {
+      const int4 run = ws.runs[q];
+      const double *t = tab + (size_t)(run.w & 0xFF) * tl;
+      const double *fq = f64 + (size_t)run.z * pad;
+#pragma unroll
+      for (int j = 0; j < NR; ++j) acc[j] = fma(fq[r[j]], t[o0[j]] * t[o1[j]] * t[o2[j]], acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+      fr[j] = fma(kre[k * pad + r[j]], acc[j], fr[j]);
+      if (kim) fi[j] = fma(kim[k * pad + r[j]], acc[j], fi[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NR; ++j)
+    if (base + lane + 32 * j < nAct) {
+      const double v = (double)refl[r[j]].mult * (fr[j] * fr[j] + fi[j] * fi[j]);
+      ic[r[j]] = v;
+      if (traceIc) traceIc[r[j]] = (float)v;
+    }
+}
+
+// The factored evaluation of the coordinates in `sites`: stale site tables
+// rebuilt, then |F|^2 in passes of 64 reflections, then the FP64 group sums.
+__device__ __forceinline__ void fitness_factored(const Params &P, const WarpView &ws, const uint32_t *sites,
+                                                 double *tab, uint4 *tag, double *ic, const ReflRec *refl,
+                                                 const unsigned char *stat, const float4 *groups,
+                                                 const double *sooPrefix, int nga, int lane, double sums[3],
+                                                 float *traceIc) {
+  factor_tables(P, ws, sites, tab, tag, lane);
+  const int nAct = nrefl_active(groups, nga);
+  for (int base = 0; base < nAct; base += 64) factored_rows(P, ws, tab, ic, refl, stat, base, nAct, lane, traceIc);
+  __syncwarp();
+  group_sums_f64(ic, groups, sooPrefix, nga, lane, sums);
 }
 
 // Expand the images of the sites in `mask` from `sites` into dst; copy the others from src.
@@ -1210,6 +1409,9 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   uint32_t *bestBase = P.pos + (size_t)P.numParticles * curStride;
 
   float *Cb = INCR ? reinterpret_cast<float *>(wbase + P.cbOff) : nullptr;
+  double *ftabs = COSMODE == 2 ? reinterpret_cast<double *>(wbase + P.tabOff) : nullptr;
+  uint4 *ftags = COSMODE == 2 ? reinterpret_cast<uint4 *>(wbase + P.tagOff) : nullptr;
+  double *ic64 = reinterpret_cast<double *>(wbase + P.icOff);
   uint4 *atomsB[2] = {atoms, INCR ? reinterpret_cast<uint4 *>(wbase + P.atoms2Off) : atoms};
 
   for (int L = L0; L < nLadders; L += Lstep) {
@@ -1252,6 +1454,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
       for (int j = lane; j < (int)curStride; j += 32) ws.cur[j] = P.pos[(size_t)p * curStride + j];
       for (int j = lane; j < P.nTot; j += 32) gen[j] = __ldg(P.gen + (size_t)A * P.nTot + j);
       for (int j = lane; j < P.maxSites; j += 32) proj[j] = P.proj[(size_t)A * P.maxSites + j];
+      if constexpr (COSMODE == 2)
+        for (int j = lane; j < P.maxSites; j += 32) ftags[j] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncwarp();
     const uint32_t allSites = P.maxSites >= 32 ? 0xffffffffu : ((1u << P.maxSites) - 1u);
@@ -1290,7 +1494,13 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             expand(P, gen, ops, ws.cur, atoms, lane);
             __syncwarp();
             double sums[3];
-            fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
+            if constexpr (COSMODE == 2)
+              fitness_factored(P, ws, ws.cur, ftabs, ftags, ic64, refl, stat, groups, sooPrefix, ngaC, lane, sums,
+                               tIc);
+            else
+              fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
+            if (P.traceSums && lane == 0)
+              for (int k = 0; k < 3; ++k) P.traceSums[(size_t)p * 3 + k] = sums[k];
             const float cc = cc_of(sums);
             const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
             fit = cc - pen;
@@ -1334,9 +1544,15 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
           } else {
             expand(P, gen, ops, ws.prop, atoms, lane);
             __syncwarp();
-            fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
+            if constexpr (COSMODE == 2)
+              fitness_factored(P, ws, ws.prop, ftabs, ftags, ic64, refl, stat, groups, sooPrefix, ngaC, lane, sums,
+                               tIc);
+            else
+              fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
             evalAtoms = atoms;
           }
+          if (P.traceSums && lane == 0)
+            for (int k = 0; k < 3; ++k) P.traceSums[(size_t)p * 3 + k] = sums[k];
           const float cc = cc_of(sums);
           const float pen = penalty<SLOTS>(P, evalAtoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
           int acc = 0, best = 0;
@@ -1667,6 +1883,7 @@ struct p6_wy_session {
   int2 *dPairRange = nullptr;
   int *dNRuns = nullptr, *dNF = nullptr, *dLadders = nullptr, *dSchedG = nullptr, *dErr = nullptr;
   float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr, *dQuench = nullptr;
+  double *dTraceSums = nullptr;   // per particle {scc, soo, sco} of the last traced evaluation
   int quenchLen = 0;
   // learned search: candidates, features, scores, the chosen proposal
   uint32_t *dCand = nullptr, *dExt = nullptr;
@@ -1783,7 +2000,7 @@ static void free_session(p6_wy_session *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
-                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTracePos, s->dOps,
+                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTraceSums, s->dTracePos, s->dOps,
                   s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap, s->dCand, s->dExt, s->dFeat, s->dScore,
                   s->dChosenFeat, s->dChosenScore, s->dPairRange};
   for (void *p : ptrs)
@@ -1846,12 +2063,17 @@ static cudaError_t launch(p6_wy_session *s, int gen0, int nGen, int mcmc, int sw
   const int C = s->cosMode, S = s->slots;
   if (s->ladderSplit == 2 && P.ladders && rungs == 8 && S == 0 && !s->incremental && s->smemPair > 0 &&
       !P.blobGlobal) {
-    e = C == 0 ? launch_pair<0, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
-               : launch_pair<1, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
+    e = C == 0   ? launch_pair<0, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
+        : C == 1 ? launch_pair<1, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst)
+                 : launch_pair<2, 0>(s, gen0, nGen, mcmc, swapEvery, reevalFirst);
     if (e == cudaSuccess) s->launches++;
     return e;
   }
-  if (C == 0 && S == 0) e = launch_incr<0, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  if (C == 2)   // the factored evaluation has no incremental form
+    e = S == 0    ? launch_variant<2, 0, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst)
+        : S == 64 ? launch_variant<2, 64, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst)
+                  : launch_variant<2, 256, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
+  else if (C == 0 && S == 0) e = launch_incr<0, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
   else if (C == 1 && S == 0) e = launch_incr<1, 0>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
   else if (C == 0 && S == 64) e = launch_incr<0, 64>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
   else if (C == 1 && S == 64) e = launch_incr<1, 64>(s, grid, block, gen0, nGen, mcmc, swapEvery, reevalFirst);
@@ -1909,7 +2131,9 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   if (pr->group_stride != 3 && pr->group_stride != 4) return set_error(P6_ERR_INVALID_ARG, "group stride must be 3 or 4");
   if (!(pr->poly_prob >= 0.f && pr->poly_prob <= 1.f)) return set_error(P6_ERR_INVALID_ARG, "poly_prob must lie in [0, 1]");
   if (pr->n_tot > 4096) return set_error(P6_ERR_CAPACITY, "more than 4096 generated atoms");
-  if (pr->cos_mode != 0 && pr->cos_mode != 1) return set_error(P6_ERR_INVALID_ARG, "cos_mode must be 0 or 1");
+  if (pr->cos_mode < 0 || pr->cos_mode > 2) return set_error(P6_ERR_INVALID_ARG, "cos_mode must be 0, 1 or 2");
+  if (pr->cos_mode == 2 && pr->incremental == 1)
+    return set_error(P6_ERR_INVALID_ARG, "the factored evaluation (cos_mode 2) has no incremental form");
   if (pr->incremental < -1 || pr->incremental > 1)
     return set_error(P6_ERR_INVALID_ARG, "incremental must be -1 (auto), 0 or 1");
 
@@ -2037,7 +2261,117 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
       for (int k = 0; k < 9; ++k) norm += std::fabs(b[k]);
       if (norm > 1e-6) freeMask[A] |= 1u << si;
     }
-  // --- static blob: reflections | f table | groups | rMin | soo prefix | ops | pairs ---
+  // --- factored FP64 structure factors (cos mode 2) ---------------------------
+  const bool factored = pr->cos_mode == 2;
+  const int nReflPad = (pr->n_refl + 3) & ~3;
+  int nMono = 0, axE[3] = {1, 1, 1}, axOff[3] = {0, 0, 0}, tabLen = 0, tabE = 0;
+  bool complexK = false;
+  std::vector<double> monoRe, monoIm, f64;
+  std::vector<uint32_t> monoIdx;
+  if (factored) {
+    for (int o = 0; o < pr->n_ops; ++o)
+      for (int k = 0; k < 9; ++k)
+        if (k % 4 != 0 && ops[o].r[k] != 0)
+          return set_error(P6_ERR_INVALID_ARG,
+                           "the factored evaluation (cos_mode 2) needs a group whose rotations are all diagonal");
+    for (int A = 0; A < nA; ++A) {
+      uint32_t seen = 0;
+      for (int q = 0; q < nRuns[A]; ++q) {
+        const int site = runs[(size_t)A * kMaxSites + q].w & 0xFF;
+        if (seen & (1u << site))
+          return set_error(P6_ERR_INVALID_ARG, "factored evaluation: a site's images are not contiguous");
+        seen |= 1u << site;
+      }
+    }
+    // operators modulo the centring translations (translations in 1/24, exact)
+    std::vector<std::array<int, 3>> tn(pr->n_ops);
+    for (int o = 0; o < pr->n_ops; ++o)
+      for (int k = 0; k < 3; ++k) {
+        const double v = (double)pr->sym_packed[o * 12 + 9 + k] * 24.0;
+        tn[o][k] = (((int)std::floor(v + 0.5)) % 24 + 24) % 24;
+      }
+    std::vector<int> cen, reps;
+    for (int o = 0; o < pr->n_ops; ++o)
+      if (ops[o].r[0] == 1 && ops[o].r[4] == 1 && ops[o].r[8] == 1) cen.push_back(o);
+    for (int o = 0; o < pr->n_ops; ++o) {
+      bool dup = false;
+      for (int j : reps) {
+        if (ops[j].r[0] != ops[o].r[0] || ops[j].r[4] != ops[o].r[4] || ops[j].r[8] != ops[o].r[8]) continue;
+        for (int c : cen) {
+          bool same = true;
+          for (int k = 0; k < 3; ++k) same &= ((tn[o][k] - tn[j][k] - tn[c][k]) % 24 + 48) % 24 == 0;
+          if (same) { dup = true; break; }
+        }
+        if (dup) break;
+      }
+      if (!dup) reps.push_back(o);
+    }
+    std::vector<std::array<int, 3>> hkl(pr->n_refl);
+    for (int r = 0; r < pr->n_refl; ++r) {
+      const uint32_t pk = pr->refl_pack[2 * r];
+      hkl[r] = {(int)(pk & 0x3FF) - 512, (int)((pk >> 10) & 0x3FF) - 512, (int)((pk >> 20) & 0x3FF) - 512};
+      for (int a = 0; a < 3; ++a) axE[a] = std::max(axE[a], std::abs(hkl[r][a]) + 1);
+    }
+    axOff[0] = 0;
+    axOff[1] = 2 * axE[0];
+    axOff[2] = axOff[1] + 2 * axE[1];
+    tabLen = axOff[2] + 2 * axE[2];
+    tabE = axE[0] + axE[1] + axE[2];
+    if (tabLen > 1024) return set_error(P6_ERR_CAPACITY, "factored evaluation: Miller indices too large for the site tables");
+    // K_m(h) = (1/N_p) sum_j e^{2 pi i h.t_j} prod_{a in m} (i sigma_ja sgn h_a)
+    const double kTwoPi = 6.283185307179586476925286766559;
+    std::vector<std::vector<std::pair<int, std::pair<double, double>>>> mono(pr->n_refl);
+    for (int r = 0; r < pr->n_refl; ++r) {
+      const int *h = hkl[r].data();
+      for (int m = 0; m < 8; ++m) {
+        bool zero = false;
+        for (int a = 0; a < 3; ++a) zero |= ((m >> a) & 1) && h[a] == 0;
+        if (zero) continue;
+        double re = 0.0, im = 0.0;
+        for (int j : reps) {
+          const int ph = ((h[0] * tn[j][0] + h[1] * tn[j][1] + h[2] * tn[j][2]) % 24 + 24) % 24;
+          double cr = std::cos(kTwoPi * ph / 24.0), ci = std::sin(kTwoPi * ph / 24.0);
+          for (int a = 0; a < 3; ++a)
+            if ((m >> a) & 1) {   // times i sigma sgn(h): (cr + i ci) i g = -ci g + i cr g
+              const double g = (double)ops[j].r[4 * a] * (h[a] > 0 ? 1.0 : -1.0);
+              const double nr = -ci * g, ni = cr * g;
+              cr = nr;
+              ci = ni;
+            }
+          re += cr;
+          im += ci;
+        }
+        re /= (double)reps.size();
+        im /= (double)reps.size();
+        if (std::fabs(re) < 1e-9) re = 0.0;
+        if (std::fabs(im) < 1e-9) im = 0.0;
+        if (re != 0.0 || im != 0.0) mono[r].push_back({m, {re, im}});
+        complexK |= im != 0.0;
+      }
+      nMono = std::max(nMono, (int)mono[r].size());
+    }
+    nMono = std::max(nMono, 1);
+    if (nMono > 4)
+      return set_error(P6_ERR_INVALID_ARG, "factored evaluation: more than four monomials per reflection "
+                                           "(use cos_mode 0 or 1 for this group)");
+    monoRe.assign((size_t)nMono * nReflPad, 0.0);
+    monoIm.assign(complexK ? (size_t)nMono * nReflPad : 0, 0.0);
+    monoIdx.assign((size_t)nMono * nReflPad, 0u);
+    for (int r = 0; r < pr->n_refl; ++r)
+      for (size_t k = 0; k < mono[r].size(); ++k) {
+        const int m = mono[r][k].first;
+        uint32_t word = 0;
+        for (int a = 0; a < 3; ++a)
+          word |= (uint32_t)(axOff[a] + ((m >> a) & 1) * axE[a] + std::abs(hkl[r][a])) << (10 * a);
+        monoRe[k * nReflPad + r] = mono[r][k].second.first;
+        if (complexK) monoIm[k * nReflPad + r] = mono[r][k].second.second;
+        monoIdx[k * nReflPad + r] = word;
+      }
+    f64.assign((size_t)nE * nReflPad, 0.0);
+    for (int r = 0; r < pr->n_refl; ++r)
+      for (int t = 0; t < nE; ++t) f64[(size_t)t * nReflPad + r] = (double)pr->f_tab[(size_t)r * nE + t];
+  }
+  // --- static blob: reflections | f table | groups | rMin | soo prefix | ops | pairs [| factored] ---
   auto pad16 = [](size_t n) { return (n + 15) & ~(size_t)15; };
   // Clash pairs.  The space group maps the cell's atoms onto themselves, and
   // rounding in the reduced basis is the nearest image out to every
@@ -2075,7 +2409,11 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   const size_t offS = offR + szR, szS = pad16((size_t)(pr->n_groups + 1) * sizeof(double));
   const size_t offO = offS + szS, szO = pad16((size_t)pr->n_ops * sizeof(OpFix));
   const size_t offP = offO + szO, szP = pad16(pairWords * sizeof(uint32_t));
-  const size_t blobBytes = offP + szP;
+  const size_t offK = offP + szP, szK = pad16(monoRe.size() * sizeof(double));
+  const size_t offKi = offK + szK, szKi = pad16(monoIm.size() * sizeof(double));
+  const size_t offIdx = offKi + szKi, szIdx = pad16(monoIdx.size() * sizeof(uint32_t));
+  const size_t offF64 = offIdx + szIdx, szF64 = pad16(f64.size() * sizeof(double));
+  const size_t blobBytes = offF64 + szF64;
   std::vector<unsigned char> blob(blobBytes, 0);
   for (int r = 0; r < pr->n_refl; ++r) {
     const uint32_t pk = pr->refl_pack[2 * r];
@@ -2119,6 +2457,12 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
         std::memcpy(&blob[offP + (size_t)(q++) * sizeof(uint32_t)], &v, sizeof(v));
       }
   }
+  if (factored) {
+    std::memcpy(&blob[offK], monoRe.data(), monoRe.size() * sizeof(double));
+    if (complexK) std::memcpy(&blob[offKi], monoIm.data(), monoIm.size() * sizeof(double));
+    std::memcpy(&blob[offIdx], monoIdx.data(), monoIdx.size() * sizeof(uint32_t));
+    std::memcpy(&blob[offF64], f64.data(), f64.size() * sizeof(double));
+  }
   std::vector<RuleDev> rules(std::max(pr->n_rules, 1));
   for (int k = 0; k < pr->n_rules; ++k) {
     const float *rb = pr->restraint_tables + pr->rule_off + 7 * k;
@@ -2130,7 +2474,6 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   // site sums (only when the caller asks for incremental evaluation).
   const int rungs = 8;
   const int comp = pr->centro ? 1 : 2;
-  const int nReflPad = (pr->n_refl + 3) & ~3;
   const size_t curOff = 32;
   const size_t propOff = curOff + (((size_t)ms * 3 * sizeof(uint32_t) + 15) & ~(size_t)15);
   const size_t runsOff = propOff + (((size_t)ms * 3 * sizeof(uint32_t) + 15) & ~(size_t)15);
@@ -2139,7 +2482,11 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   const size_t projOff = (genOff + (size_t)nTot * sizeof(uint32_t) + 15) & ~(size_t)15;
   const size_t atomsOff = (projOff + (size_t)ms * sizeof(ProjFix) + 15) & ~(size_t)15;
   const size_t icOff = atomsOff + (size_t)nTot * sizeof(uint4);
-  const size_t baseEnd = icOff + (size_t)nReflPad * sizeof(float);
+  // the factored evaluation keeps FP64 |F|^2 and, per site, its axis tables and their coordinate tags
+  const size_t icEnd = icOff + (size_t)nReflPad * (factored ? sizeof(double) : sizeof(float));
+  const size_t tabOff = (icEnd + 15) & ~(size_t)15;
+  const size_t tagOff = tabOff + (factored ? (size_t)ms * tabLen * sizeof(double) : 0);
+  const size_t baseEnd = factored ? tagOff + (size_t)ms * sizeof(uint4) : icEnd;
   const size_t atoms2Off = (baseEnd + 15) & ~(size_t)15;
   const size_t cbOff = atoms2Off + (size_t)nTot * sizeof(uint4);
   const size_t incrEnd = cbOff + (size_t)(ms + 1) * nReflPad * comp * sizeof(float);
@@ -2296,6 +2643,20 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.errFlag = s->dErr;
   P.warpSmemBytes = (int)warpBytes;
   P.blobGlobal = blobGlobal;
+  P.offK = (int)offK;
+  P.offKi = complexK ? (int)offKi : -1;
+  P.offIdx = (int)offIdx;
+  P.offF64 = (int)offF64;
+  P.nMono = nMono;
+  P.tabLen = tabLen;
+  P.tabE = tabE;
+  for (int a = 0; a < 3; ++a) {
+    P.axE[a] = axE[a];
+    P.axOff[a] = axOff[a];
+  }
+  P.tabOff = (int)tabOff;
+  P.tagOff = (int)tagOff;
+  P.traceSums = nullptr;
   P.genOff = (int)genOff;
   P.projOff = (int)projOff;
   P.atomsOff = (int)atomsOff;
@@ -2446,6 +2807,8 @@ p6_status p6_wy_set_trace(p6_wy_session *s, int enable) {
     P6_CUDA(cudaMalloc(&s->dTraceIc, (size_t)s->P.numParticles * std::max(s->P.nRefl, 1) * sizeof(float)));
     P6_CUDA(cudaMemsetAsync(s->dTraceIc, 0, (size_t)s->P.numParticles * std::max(s->P.nRefl, 1) * sizeof(float),
                             s->stream));
+    P6_CUDA(cudaMalloc(&s->dTraceSums, (size_t)s->P.numParticles * 3 * sizeof(double)));
+    P6_CUDA(cudaMemsetAsync(s->dTraceSums, 0, (size_t)s->P.numParticles * 3 * sizeof(double), s->stream));
   }
   s->trace = enable != 0;
   return P6_OK;
@@ -2478,6 +2841,7 @@ static p6_status dispatch_impl(p6_wy_session *s, int mcmc) {
   P.tracePos = s->trace ? s->dTracePos : nullptr;
   P.traceRec = s->trace ? s->dTraceRec : nullptr;
   P.traceIc = s->trace ? s->dTraceIc : nullptr;
+  P.traceSums = s->trace ? s->dTraceSums : nullptr;
   P6_CUDA(cudaEventRecord(s->ev0, s->stream));
   cudaError_t e = launch(s, 0, 1, mcmc, 0, 0);
   P = saved;
@@ -2595,6 +2959,7 @@ p6_status p6_wy_run(p6_wy_session *s, int gen0, int n_gen, int swap_every, int r
   P.tracePos = s->trace ? s->dTracePos : nullptr;
   P.traceRec = s->trace ? s->dTraceRec : nullptr;
   P.traceIc = s->trace ? s->dTraceIc : nullptr;
+  P.traceSums = s->trace ? s->dTraceSums : nullptr;
   P6_CUDA(cudaEventRecord(s->ev0, s->stream));
   cudaError_t e = launch(s, gen0, n_gen, 1, swap_every, reeval_first ? 1 : 0);
   P = saved;
@@ -2638,6 +3003,16 @@ p6_status p6_wy_read_trace_ic(p6_wy_session *s, float *ic) {
   if (!s || !s->dTraceIc || !ic) return set_error(P6_ERR_INVALID_ARG, "tracing was not enabled");
   P6_CUDA(cudaSetDevice(s->device));
   P6_CUDA(cudaMemcpyAsync(ic, s->dTraceIc, (size_t)s->P.numParticles * s->P.nRefl * sizeof(float),
+                          cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_read_trace_sums(p6_wy_session *s, double *sums) {
+  P6_ENTRY();
+  if (!s || !s->dTraceSums || !sums) return set_error(P6_ERR_INVALID_ARG, "tracing was not enabled");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaMemcpyAsync(sums, s->dTraceSums, (size_t)s->P.numParticles * 3 * sizeof(double),
                           cudaMemcpyDeviceToHost, s->stream));
   P6_CUDA(cudaStreamSynchronize(s->stream));
   return P6_OK;
@@ -2860,6 +3235,8 @@ p6_status p6_wy_batch_create(p6_wy_session *const *sessions, int n_sessions, p6_
     if (!s) return set_error(P6_ERR_INVALID_ARG, "null session in the batch");
     if (s->device != sessions[0]->device) return set_error(P6_ERR_INVALID_ARG, "sessions on different devices");
     if (s->cosMode != sessions[0]->cosMode) return set_error(P6_ERR_INVALID_ARG, "sessions with different cos_mode");
+    if (s->cosMode == 2)
+      return set_error(P6_ERR_INVALID_ARG, "the batched launch takes cos_mode 0 or 1 (the groups of a batch differ)");
     if (s->incremental) return set_error(P6_ERR_INVALID_ARG, "batched searches use the full evaluation (incremental = 0)");
     if (s->P.rungs > 8) return set_error(P6_ERR_CAPACITY, "batched ladders hold at most 8 rungs");
   }

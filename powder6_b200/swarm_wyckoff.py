@@ -62,13 +62,33 @@ def adaptation(settings: Optional[dict] = None) -> Dict[str, float]:
     return out
 
 
-class WyckoffSession:
-    """One device session: the buffers and kernel of one search (swarm_wyckoff.js:1293-1720)."""
+COS_SFU, COS_POLY, COS_FACTORED = 0, 1, 2
+COS_NAMES = {COS_SFU: 'sfu', COS_POLY: 'poly', COS_FACTORED: 'factored-fp64'}
 
-    def __init__(self, problem: WyckoffProblem, num_particles: int, run_key: int = 1, cos_mode: int = 0,
-                 device: int = 0, settings: Optional[dict] = None, max_coord_slots: Optional[int] = None,
-                 incremental: int = -1):
+
+def factored_ok(problem: WyckoffProblem) -> bool:
+    """The factored FP64 evaluation applies: every rotation of the group is
+    diagonal (triclinic, monoclinic and orthorhombic groups)."""
+    return all(all(o.r[k] == 0 for k in (1, 2, 3, 5, 6, 7)) for o in problem.group.ops)
+
+
+def default_cos_mode(problem: WyckoffProblem) -> int:
+    """Factored FP64 where the group allows it, else the SFU cosine."""
+    return COS_FACTORED if factored_ok(problem) else COS_SFU
+
+
+class WyckoffSession:
+    """One device session: the buffers and kernel of one search (swarm_wyckoff.js:1293-1720).
+    ``cos_mode`` None picks ``default_cos_mode``."""
+
+    def __init__(self, problem: WyckoffProblem, num_particles: int, run_key: int = 1,
+                 cos_mode: Optional[int] = None, device: int = 0, settings: Optional[dict] = None,
+                 max_coord_slots: Optional[int] = None, incremental: int = -1):
         self.lib = _lib.load()
+        auto = cos_mode is None
+        if auto:
+            cos_mode = default_cos_mode(problem) if incremental != 1 else COS_SFU
+        self.cos_mode = int(cos_mode)
         self.problem = problem
         self.num_particles = int(num_particles)
         T = problem.tables
@@ -124,7 +144,15 @@ class WyckoffSession:
         pr.incremental = int(incremental)
         self.adapt = ad
         h = C.c_void_p()
-        check(self.lib.p6_wy_create(C.byref(pr), int(device), C.byref(h)))
+        st = self.lib.p6_wy_create(C.byref(pr), int(device), C.byref(h))
+        if st == _lib.P6_ERR_CAPACITY and auto and cos_mode == COS_FACTORED:
+            # the factored tables do not fit next to the replica slices: the SFU cosine reads its tables
+            # from global memory instead
+            cos_mode = COS_SFU
+            self.cos_mode = cos_mode
+            pr.cos_mode = cos_mode
+            st = self.lib.p6_wy_create(C.byref(pr), int(device), C.byref(h))
+        check(st)
         self.h = h
         self.coords_per_particle = T.max_sites * 3
 
@@ -250,6 +278,12 @@ class WyckoffSession:
         ic = np.zeros(self.num_particles * self.problem.refl.n_refl, dtype=np.float32)
         check(self.lib.p6_wy_read_trace_ic(self.h, ptr(ic)))
         return ic.reshape(self.num_particles, -1)
+
+    def read_trace_sums(self):
+        """FP64 (scc, soo, sco) of each particle's last traced evaluation."""
+        out = np.zeros(self.num_particles * 3, dtype=np.float64)
+        check(self.lib.p6_wy_read_trace_sums(self.h, ptr(out)))
+        return out.reshape(self.num_particles, 3)
 
     def debug_expand(self, particle: int):
         out = np.zeros(self.problem.n_tot * 3, dtype=np.uint32)
@@ -549,7 +583,8 @@ def quench(problem: WyckoffProblem, sess: 'WyckoffSession', best: Dict[int, dict
 
 
 def run_wyckoff_search(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
-                       restarts: int = 1, seed: int = 20261026, cos_mode: int = 0, chunk: Optional[int] = None,
+                       restarts: int = 1, seed: int = 20261026, cos_mode: Optional[int] = None,
+                       chunk: Optional[int] = None,
                        settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
                        on_progress: Optional[Callable[[dict], None]] = None,
                        should_stop: Optional[Callable[[], bool]] = None, do_quench: bool = True,
@@ -834,7 +869,7 @@ def _wave_progress(on_progress: Callable[[dict], None], k: int, waves: int, stag
 
 
 def run_wyckoff_waves(problem: WyckoffProblem, num_particles: int = 4096, generations: int = 5000,
-                      restarts: int = 1, seed: int = 20261026, cos_mode: int = 0,
+                      restarts: int = 1, seed: int = 20261026, cos_mode: Optional[int] = None,
                       settings: Optional[dict] = None, session: Optional[WyckoffSession] = None,
                       **kwargs) -> SearchResult:
     """Every assignment of the problem, in waves of assignmentsPerWave in their

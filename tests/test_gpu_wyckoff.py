@@ -107,11 +107,19 @@ def test_orbit_expansion_bit_exact(prob, oracle):
             assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize('cos_mode,cc_tol,ic_tol', [(0, 2e-6, 2e-4), (1, 5e-7, 5e-6)])
-def test_evaluation_parity(prob, oracle, cos_mode, cc_tol, ic_tol):
+CHI2 = lambda sums: 1.0 - sums[2] ** 2 / (sums[0] * sums[1])   # grouped wR2^2 after the best scale
+
+
+@pytest.mark.parametrize('cos_mode,cc_tol,ic_tol,chi2_tol', [(0, 2e-6, 2e-4, None), (1, 5e-7, 5e-6, None),
+                                                              (2, 1e-7, 1e-5, 1e-6)])
+def test_evaluation_parity(prob, oracle, cos_mode, cc_tol, ic_tol, chi2_tol):
     """cc within cc_tol (absolute, on a [0, 1] fitness), penalty within 1e-5
     relative, and mult |F|^2 within ic_tol relative to the largest reflection
-    of each structure (FP32 sum of FP32 cosines vs FP64)."""
+    of each structure (FP32 sum of FP32 cosines for modes 0 and 1, the
+    factored FP64 evaluation for mode 2, vs FP64).  For the factored mode the
+    device's FP64 fitness sums give the chi^2-like 1 - cc^2 (wR2^2 after the
+    best scale) of every replica, random and true structures alike, within
+    chi2_tol relative of the FP64 oracle's."""
     P = prob
     n = 256
     X, assign = random_positions(P, n, 5 + cos_mode)
@@ -121,16 +129,18 @@ def test_evaluation_parity(prob, oracle, cos_mode, cc_tol, ic_tol):
     with WyckoffSession(P, n, cos_mode=cos_mode) as s:
         s.write_positions_fixed(X)
         s.set_trace(True)
-        worst_cc = worst_ic = worst_pen = 0.0
+        worst_cc = worst_ic = worst_pen = worst_chi = 0.0
         for nga, scale in ((P.refl.n_groups, 1.0), (max(8, P.refl.n_groups // 4), 2.5)):
             s.set_params(nga, scale)
             s.dispatch(None, mcmc=False)
             s.synchronize(60)
             _, _, st = s.read_state()
             ic = s.read_trace_ic()
+            dsums = s.read_trace_sums()
             for p in range(n):
                 sites = X[p * P.max_sites * 3:(p + 1) * P.max_sites * 3]
-                cc, pen, _ = oracle_cc_pen(oracle, P, sites, nga, scale)
+                cc, pen, sums = oracle_cc_pen(oracle, P, sites, nga, scale)
+                worst_chi = max(worst_chi, abs(CHI2(dsums[p]) - CHI2(sums)) / CHI2(sums))
                 worst_cc = max(worst_cc, abs(float(st['cc'][p]) - cc))
                 worst_pen = max(worst_pen, abs(float(st['pen'][p]) * scale - pen) / max(1.0, pen))
                 assert abs(float(st['fit'][p]) - (cc - pen)) < cc_tol + 1e-5 * max(1.0, pen)
@@ -138,8 +148,10 @@ def test_evaluation_parity(prob, oracle, cos_mode, cc_tol, ic_tol):
                     ref = icalc_fp64(P, sites)
                     worst_ic = max(worst_ic, float(np.max(np.abs(ic[p] - ref)) / ref.max()))
         print(f'cos_mode {cos_mode}: max |dcc| {worst_cc:.3e}, max rel |d mult F^2| {worst_ic:.3e}, '
-              f'max rel dpen {worst_pen:.3e}')
+              f'max rel dpen {worst_pen:.3e}, max rel d(1 - cc^2) {worst_chi:.3e}')
         assert worst_cc <= cc_tol
+        if chi2_tol is not None:
+            assert worst_chi <= chi2_tol
         assert worst_ic <= ic_tol
         assert worst_pen <= 1e-5
         assert float(st['cc'][0]) > 0.95
