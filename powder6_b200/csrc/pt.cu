@@ -103,7 +103,11 @@ struct Params {
   const int *eqStart;    // nRefl + 1
   const int *eqHkl;      // 3 per equivalent
   double poDir[3];       // reciprocal-lattice direction
+  // per chain, the decisions of the last sweep: {exchange tried, swapped, la,
+  // log u} then per move {j, proposed x_j, log u, cost before, cost, accepted}
+  double *trace;
 };
+constexpr int kTraceHead = 4, kTraceMove = 6;
 
 // ---------------------------------------------------------------------------
 // Profile model (FP64 per peak).
@@ -843,6 +847,7 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
   __shared__ Shared sh;
   __shared__ double xs[kMaxNv];
   __shared__ Chain st;
+  __shared__ int drawnJ;
   const SmemLayout L = smem_layout(P.nRefl, P.n, P.stageObs);
   Peak *pk1 = reinterpret_cast<Peak *>(smem + L.pk1), *pk2 = reinterpret_cast<Peak *>(smem + L.pk2);
   float *h1 = reinterpret_cast<float *>(smem + L.h1), *w2 = reinterpret_cast<float *>(smem + L.w2);
@@ -860,6 +865,8 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
   const double T = pow(P.maxTemp, (double)c / (double)(C - 1));
   if (threadIdx.x == 0) {
     st = in[c];
+    if (P.trace && rank == 0 && !bootstrap)
+      for (int k = 0; k < kTraceHead; ++k) P.trace[(size_t)c * (kTraceHead + kTraceMove * P.nv) + k] = 0.0;
     // adjacent exchange of the previous sweep, even/odd pairs alternating
     if (exchangeParity >= 0) {
       const int left = ((c - exchangeParity) % 2 == 0) ? c : c - 1;
@@ -870,7 +877,15 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
         const double la = 0.5 * (1 / Ta - 1 / Tb) * (a.cost - b.cost);
         const uint4 r = philox4x32_10(make_uint4((uint32_t)a.sweep, (uint32_t)left, 0x45584348u, 3u),
                                       make_uint2(P.seed, 0x9E3779B9u));
-        const bool swap = la >= 0 || log(uniform_open(r.x)) < la;
+        const double lu = log(uniform_open(r.x));
+        const bool swap = la >= 0 || lu < la;
+        if (P.trace && rank == 0 && !bootstrap) {
+          double *tr = P.trace + (size_t)c * (kTraceHead + kTraceMove * P.nv);
+          tr[0] = 1.0;
+          tr[1] = swap ? 1.0 : 0.0;
+          tr[2] = la;
+          tr[3] = lu;
+        }
         if (c == left) st.swapAttempts += 1;
         if (swap) {
           const Chain &o = (c == left) ? b : a;
@@ -890,6 +905,7 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
         const uint4 r = philox4x32_10(make_uint4((uint32_t)st.sweep, (uint32_t)c, (uint32_t)m, 1u),
                                       make_uint2(P.seed, 0x2545F491u));
         const int j = min(P.nv - 1, (int)(uniform_open(r.x) * P.nv));
+        drawnJ = j;
         const double z = sqrt(-2.0 * log(uniform_open(r.y))) * cos(2.0 * kPi * uniform_open(r.z));
         xs[j] = reflect(st.x[j] + z * P.scales[j] * sqrt(T), P.lo[j], P.hi[j]);
         st.logu = log(uniform_open(r.w));
@@ -907,7 +923,19 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
         for (int j = 0; j < P.nv; ++j) st.best[j] = st.x[j];
       } else {
         st.proposals += 1;
-        if (isfinite(cost) && (cost <= st.cost || st.logu < (st.cost - cost) / (2 * T))) {
+        const double before = st.cost;
+        const bool acc = isfinite(cost) && (cost <= st.cost || st.logu < (st.cost - cost) / (2 * T));
+        if (P.trace && rank == 0 && m < P.nv) {
+          double *tr = P.trace + (size_t)c * (kTraceHead + kTraceMove * P.nv) + kTraceHead + kTraceMove * m;
+          const int jm = drawnJ;
+          tr[0] = (double)jm;
+          tr[1] = xs[jm];
+          tr[2] = st.logu;
+          tr[3] = before;
+          tr[4] = cost;
+          tr[5] = acc ? 1.0 : 0.0;
+        }
+        if (acc) {
           for (int j = 0; j < P.nv; ++j) st.x[j] = xs[j];
           st.cost = cost;
           st.accepted += 1;
@@ -1206,6 +1234,7 @@ struct p6_pt_session {
   double *dLmVec = nullptr, *dLmY = nullptr, *dLmYu = nullptr, *dLmChi = nullptr, *dLmOut = nullptr;
   int *dLmF = nullptr;
   int lmCap = 0;
+  double *dTrace = nullptr;   // per chain, the last sweep's decisions (p6_pt_set_trace)
 };
 
 template <typename T>
@@ -1227,7 +1256,7 @@ static void pt_free(p6_pt_session *s) {
   for (int i = 0; i < s->nAlloc; ++i) cudaFree(s->dAlloc[i]);
   for (void *p : {(void *)s->dChain[0], (void *)s->dChain[1], (void *)s->dVec, (void *)s->dCost, (void *)s->dY,
                   (void *)s->dLmVec, (void *)s->dLmY, (void *)s->dLmYu, (void *)s->dLmChi, (void *)s->dLmOut,
-                  (void *)s->dLmF})
+                  (void *)s->dLmF, (void *)s->dTrace})
     if (p) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -1577,6 +1606,29 @@ p6_status p6_pt_vector_capacity(p6_pt_session *s, int *n_vectors) {
   return P6_OK;
 }
 
+p6_status p6_pt_set_trace(p6_pt_session *s, int enable) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t n = (size_t)s->P.chains * (kTraceHead + kTraceMove * s->P.nv);
+  if (enable && !s->dTrace) {
+    P6_CUDA(cudaMalloc(&s->dTrace, n * sizeof(double)));
+    P6_CUDA(cudaMemsetAsync(s->dTrace, 0, n * sizeof(double), s->stream));
+  }
+  s->P.trace = enable ? s->dTrace : nullptr;
+  return P6_OK;
+}
+
+p6_status p6_pt_read_trace(p6_pt_session *s, double *out) {
+  clear_error();
+  if (!s || !out || !s->dTrace) return set_error(P6_ERR_INVALID_ARG, "tracing was not enabled");
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t n = (size_t)s->P.chains * (kTraceHead + kTraceMove * s->P.nv);
+  P6_CUDA(cudaMemcpyAsync(out, s->dTrace, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
 p6_status p6_pt_launch_count(p6_pt_session *s, long long *count) {
   clear_error();
   if (!s || !count) return set_error(P6_ERR_INVALID_ARG, "null argument");
@@ -1671,7 +1723,7 @@ p6_status lm_ensure(p6_pt_session *s, int m) {
     return set_error(P6_ERR_CAPACITY, "too many reflections for the FP64 peak table of the least-squares finish");
   if (m <= s->lmCap) return P6_OK;
   for (void *p : {(void *)s->dLmVec, (void *)s->dLmY, (void *)s->dLmYu, (void *)s->dLmChi, (void *)s->dLmOut,
-                  (void *)s->dLmF})
+                  (void *)s->dLmF, (void *)s->dTrace})
     if (p) cudaFree(p);
   s->dLmVec = s->dLmY = s->dLmYu = s->dLmChi = s->dLmOut = nullptr;
   s->dLmF = nullptr;

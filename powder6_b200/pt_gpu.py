@@ -323,6 +323,18 @@ class PTSession:
                                         counters.ctypes.data))
         return x, best, costs, counters
 
+    def set_trace(self, on: bool):
+        check(self.lib.p6_pt_set_trace(self.h, 1 if on else 0))
+
+    def read_trace(self):
+        """Per chain, the last sweep's exchange {tried, swapped, la, log u} and
+        moves (nv x {j, proposed x_j, log u, cost before, cost, accepted})."""
+        c, nv = self.plan.chains, self.plan.nv
+        out = np.zeros(c * (4 + 6 * nv), dtype=np.float64)
+        check(self.lib.p6_pt_read_trace(self.h, out.ctypes.data))
+        out = out.reshape(c, 4 + 6 * nv)
+        return out[:, :4], out[:, 4:].reshape(c, nv, 6)
+
     def synchronize(self, timeout: float = 60.0):
         check(self.lib.p6_pt_synchronize(self.h, float(timeout)))
 
