@@ -489,7 +489,7 @@ def rwp(problem: PTProblem, chi2: float) -> float:
 
 
 def refine(ctx: PTContext, device: int = 0, max_iter: int = 20, tol: float = 1e-5,
-           target_chi2: Optional[float] = None) -> dict:
+           target_chi2: Optional[float] = None, finish: bool = True) -> dict:
     """refine() with algorithm 'pt' (js/rietveld_core.js:2242-2300) on the device:
     one Gauss-Newton step on the scale and background, tempering from there
     (``run``), the tempering's best kept if it is no worse than the start,
@@ -497,7 +497,9 @@ def refine(ctx: PTContext, device: int = 0, max_iter: int = 20, tol: float = 1e-
     LM record, the wall time at the end of each stage and, with
     ``target_chi2``, the wall time at which the best chi^2 so far first
     reached it (checked after the linear start, after every batch of sweeps
-    and after the finish)."""
+    and after the finish).  ``finish`` False stops after the tempering (the
+    least-squares finish is skipped), so the tempering's own progress can be
+    timed."""
     import time
     t0 = time.perf_counter()
     hit = {'t': None}
@@ -524,8 +526,11 @@ def refine(ctx: PTContext, device: int = 0, max_iter: int = 20, tol: float = 1e-
         t_pt = time.perf_counter() - t0
         if r['pt']['bestChi2'] <= f:
             x = r['x']
-        xf, lm = gpu.lm(x, max_iter, tol)
-        note(lm['chi2'])
+        if finish:
+            xf, lm = gpu.lm(x, max_iter, tol)
+            note(lm['chi2'])
+        else:
+            xf, lm = x, {'chi2': min(f, r['pt']['bestChi2']), 'skipped': True}
         t_lm = time.perf_counter() - t0
     return {'x': xf, 'chi2': lm['chi2'], 'rwp': rwp(ctx.problem, lm['chi2']), 'pt': r['pt'], 'lm': lm,
             'stopped': r['stopped'], 'seconds': {'linear': t_lin, 'pt': t_pt, 'lm': t_lm},

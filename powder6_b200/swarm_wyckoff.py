@@ -382,42 +382,28 @@ def assignment_dims(problem: WyckoffProblem) -> List[int]:
 
 
 def weighted_assign(ids: Sequence[int], n: int, min_per: int, weights: Optional[Sequence[float]] = None) -> np.ndarray:
-    """weightedAssign (js/wyckoff_assign.js:1188-1229): a floor of
-    min(min_per, n // len(ids)) particles each, the surplus in proportion to
-    the weights, the rounding remainder to the largest weights; particles of
-    one assignment are contiguous, in the order of ``ids``."""
+    """Replicas per assignment by largest-remainder (Hamilton) apportionment,
+    the allocation rule of js/wyckoff_assign.js:1188-1229: every id gets a
+    floor of min(min_per, n // len(ids)); the surplus is shared in proportion
+    to the weights (the free-parameter counts), whole parts first, and the
+    replicas left over go one each to the largest fractional parts (ties: the
+    larger weight, then the earlier id).  The replicas of one assignment are
+    contiguous, in the order of ``ids``."""
     out = np.zeros(n, dtype=np.uint32)
     ids = list(ids)
     if not ids:
         return out
-    floor_each = min(min_per, n // len(ids))
-    w = [max(1e-6, float(weights[a]) if weights is not None and weights[a] else 1.0) for a in ids]
-    total = sum(w)
-    surplus = max(0, n - floor_each * len(ids))
-    counts = [floor_each + int(math.floor(surplus * x / total)) for x in w]
-    order = sorted(range(len(ids)), key=lambda k: -w[k])
-    assigned, oi = sum(counts), 0
-    while assigned < n:
-        counts[order[oi % len(order)]] += 1
-        oi += 1
-        assigned += 1
-    guard = len(order) * 4 + 8
-    while assigned > n and guard > 0:
-        guard -= 1
-        k = order[len(order) - 1 - (oi % len(order))]
-        oi += 1
-        if counts[k] > 1:
-            counts[k] -= 1
-            assigned -= 1
-    p = 0
-    for a, c in zip(ids, counts):
-        for _ in range(c):
-            if p < n:
-                out[p] = a
-                p += 1
-    while p < n:
-        out[p] = ids[p % len(ids)]
-        p += 1
+    k = len(ids)
+    floor_each = min(min_per, n // k)
+    w = np.array([max(1e-6, float(weights[a]) if weights is not None and weights[a] else 1.0) for a in ids])
+    quota = (n - floor_each * k) * w / w.sum()
+    whole = np.floor(quota + 1e-9)
+    counts = floor_each + whole.astype(np.int64)
+    left = n - int(counts.sum())
+    if left > 0:
+        order = np.lexsort((np.arange(k), -w, -(quota - whole)))
+        counts[order[:left]] += 1
+    out[:] = np.repeat(np.array(ids, dtype=np.uint32), counts)
     return out
 
 
