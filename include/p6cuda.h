@@ -220,6 +220,36 @@ p6_status p6_wy_read_trace(p6_wy_session *s, uint32_t *proposals, float *records
 /* mult * |F|^2 of every reflection of each particle's last traced evaluation
  * (num_particles * n_refl floats; reflections past the active groups untouched). */
 p6_status p6_wy_read_trace_ic(p6_wy_session *s, float *ic);
+/* A rigid fragment with torsions (the config-5 molecule): the sites of the
+ * session's single assignment are the fragment's atoms in order, and each
+ * replica searches a translation t (fractional), a unit quaternion q and the
+ * torsion angles instead of the sites' coordinates.  Atom i = t + to_frac .
+ * R(q) . (ref_i after the torsions, applied in order, each turning the atoms of
+ * `moving[k]` about the bond axis_b[k] -> axis_c[k] by its angle).  A
+ * proposal moves every parameter (p = 1/4) or one group: the translation
+ * (steps of width x trans_step), the orientation (a turn of width x
+ * angle_step radians about a random axis) or one torsion (width x
+ * angle_step); the structure-factor fitness, penalty and acceptance are the
+ * search's own.  The reference searches molecules as sites held by distance
+ * rules (js/molecule_rules.js:1-18, swarm_reflection.wgsl:893-1130); this is
+ * the direct-space parametrisation of the same molecule.  NULL turns it off. */
+typedef struct {
+  int n_atoms;          /* <= 32 and <= max_sites */
+  int n_tors;           /* <= 8 */
+  int axis_b[8], axis_c[8];
+  uint32_t moving[8];   /* bit i: atom i turns with torsion k */
+  double ref_xyz[96];   /* reference geometry, Cartesian A about its centroid */
+  double to_frac[9];    /* Cartesian -> fractional of the cell, row-major */
+  double trans_step, angle_step;
+} p6_wy_fragment;
+p6_status p6_wy_set_fragment(p6_wy_session *s, const p6_wy_fragment *fragment);
+/* Per particle 16 floats: t[3], q[4] (w, x, y, z), the torsion angles; the
+ * write sets the current and the best parameters, the read returns both. */
+p6_status p6_wy_write_fragment_state(p6_wy_session *s, const float *current);
+p6_status p6_wy_read_fragment_state(p6_wy_session *s, float *current, float *best);
+/* Parity support: the fixed-point coordinates (n_atoms * 3 words per vector)
+ * of n parameter vectors, mapped on the device as the search maps them. */
+p6_status p6_wy_debug_fragment(p6_wy_session *s, const float *params, int n, uint32_t *coords);
 /* The FP64 fitness sums {sum w Ic^2, sum w Io^2, sum w Ic Io} over the active
  * groups of each particle's last traced evaluation (num_particles * 3
  * doubles); cc = sco / sqrt(scc soo), the grouped wR2^2 after the best scale

@@ -593,3 +593,36 @@ def wy_refine(problem, A, x0, max_iter=60, lambda0=1e-3, lambda_up=10.0, lambda_
     s, chi = scale_chi(ical)
     return cur, r_start, math.sqrt(chi / oo), chi, steps, conv
 
+
+
+# ---------------------------------------------------------------------------
+# Rigid fragment with torsions -> fractional coordinates (FP64)
+# ---------------------------------------------------------------------------
+def _axis_angle_matrix(u, ang):
+    """Rotation by ang about the unit axis u (Rodrigues' formula in matrix form)."""
+    K = np.array([[0.0, -u[2], u[1]], [u[2], 0.0, -u[0]], [-u[1], u[0], 0.0]])
+    return np.eye(3) + math.sin(ang) * K + (1.0 - math.cos(ang)) * (K @ K)
+
+
+def fragment_coords_fp64(ref, axis_b, axis_c, moving, to_frac, params):
+    """Fractional coordinates of a rigid fragment at parameters (t[3], q[4]
+    = (w, x, y, z), torsion angles): torsion k turns the atoms in the bit mask
+    moving[k] about the bond axis_b[k] -> axis_c[k] as the earlier torsions
+    left it; then the rotation of the unit quaternion, the change of basis
+    and the translation, wrapped into [0, 1).  The map the search uses for a
+    molecule (direct-space parametrisation of js/molecule_rules.js)."""
+    x = np.array(ref, dtype=np.float64).reshape(-1, 3).copy()
+    p = np.asarray(params, dtype=np.float64)
+    for k in range(len(axis_b)):
+        b, c = x[axis_b[k]].copy(), x[axis_c[k]].copy()
+        u = (c - b) / np.linalg.norm(c - b)
+        Rk = _axis_angle_matrix(u, float(p[7 + k]))
+        for i in range(len(x)):
+            if (int(moving[k]) >> i) & 1:
+                x[i] = b + Rk @ (x[i] - b)
+    w, qx, qy, qz = p[3:7] / np.linalg.norm(p[3:7])
+    # the quaternion's rotation as the composition of a turn by 2 acos(w) about (qx, qy, qz)
+    s = math.sqrt(max(0.0, 1.0 - w * w))
+    Rq = np.eye(3) if s < 1e-15 else _axis_angle_matrix(np.array([qx, qy, qz]) / s, 2.0 * math.atan2(s, w))
+    f = (x @ Rq.T) @ np.asarray(to_frac, dtype=np.float64).reshape(3, 3).T + p[:3]
+    return f - np.floor(f)

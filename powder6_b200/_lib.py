@@ -100,6 +100,10 @@ _SIGS = {
     'p6_wy_read_trace': (C.c_int, [_P, _P, _P]),
     'p6_wy_read_trace_ic': (C.c_int, [_P, _P]),
     'p6_wy_read_trace_sums': (C.c_int, [_P, _P]),
+    'p6_wy_set_fragment': (C.c_int, [_P, _P]),
+    'p6_wy_write_fragment_state': (C.c_int, [_P, _P]),
+    'p6_wy_read_fragment_state': (C.c_int, [_P, _P, _P]),
+    'p6_wy_debug_fragment': (C.c_int, [_P, _P, C.c_int, _P]),
     'p6_wy_debug_expand': (C.c_int, [_P, C.c_int, _P]),
     'p6_wy_last_kernel_ms': (C.c_int, [_P, C.POINTER(C.c_float)]),
     'p6_wy_launch_count': (C.c_int, [_P, C.POINTER(C.c_longlong)]),

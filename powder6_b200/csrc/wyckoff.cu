@@ -75,6 +75,20 @@ struct ReflRec {  // 8 bytes
   unsigned short mult;
 };
 
+// A rigid fragment with torsions (a molecule whose atoms are the sites of the
+// assignment, in order): per replica, a translation (fractional), an
+// orientation quaternion and the torsion angles replace the sites' free
+// coordinates as the searched parameters.
+constexpr int kFragMaxAtoms = 32, kFragMaxTors = 8, kFragParams = 16;
+struct FragDev {
+  int nAtoms, nTors;
+  int axisB[kFragMaxTors], axisC[kFragMaxTors];  // each torsion turns about the bond b -> c
+  uint32_t moving[kFragMaxTors];                  // the atoms it turns (bit i = atom i)
+  float ref[kFragMaxAtoms * 3];                   // Cartesian reference geometry (A), about its centroid
+  float toFrac[9];                                // Cartesian -> fractional of the cell, row-major
+  float transStep, angleStep;                     // per unit of the replica's step width
+};
+
 struct PState {  // mirror of p6_wy_particle_state
   float fit, cc, pen, step, temp;
   uint32_t seed, accepted, pad;
@@ -135,6 +149,10 @@ struct Params {
   int axE[3], axOff[3];
   int tabOff, tagOff;
   double *traceSums;       // per particle {scc, soo, sco} of the last traced evaluation (FP64)
+  const FragDev *frag;     // rigid-fragment search: the fragment; null: the sites move independently
+  float *fragState;        // per particle the current fragment parameters (kFragParams floats)
+  float *fragBest;         // per particle the parameters of its best structure
+  int fragOff;             // per-warp slice offset of the current and proposed parameters
 };
 
 // ---------------------------------------------------------------------------
@@ -574,33 +592,50 @@ __device__ __forceinline__ void sincos_turn_f64(uint32_t ph, double *s_out, doub
   *c_out = cs;
 }
 
-// Rebuild the per-axis tables of the sites whose coordinates (in `sites`)
-// differ from their tags.  Table of site s: per axis a, cos(2 pi n x_a) for
-// n < axE[a] then sin, starting at axOff[a]; the x table is scaled by n_s.
-// One stale site at a time, its entries over the lanes.
+// Two banks of per-axis tables per site.  Bank k of site s holds, per axis a,
+// cos(2 pi n x_a) for n < axE[a] then sin, starting at axOff[a], for the
+// coordinates in its tag; the x table is scaled by n_s.  A site whose
+// coordinates (in `sites`) match neither tag is rebuilt, one stale site at a
+// time with its entries over the lanes, into the bank that does not hold the
+// current coordinates' table -- so a rejected proposal leaves the current
+// tables intact and an accepted one finds its own.  sel[q] is the table
+// offset run q reads.
 __device__ __forceinline__ void factor_tables(const Params &P, const WarpView &ws, const uint32_t *sites,
-                                              double *tab, uint4 *tag, int lane) {
+                                              double *tab, uint4 *tag, int *sel, int lane) {
   const int nRuns = ws.meta[1];
+  const int ms = P.maxSites, tl = P.tabLen;
   bool need = false;
+  int s = 0, bank = 0;
   if (lane < nRuns) {
-    const int s = ws.runs[lane].w & 0xFF;
-    const uint4 t = tag[s];
-    need = !(t.w != 0u && t.x == sites[3 * s] && t.y == sites[3 * s + 1] && t.z == sites[3 * s + 2]);
+    s = ws.runs[lane].w & 0xFF;
+    const uint32_t X0 = sites[3 * s], X1 = sites[3 * s + 1], X2 = sites[3 * s + 2];
+    const uint4 t0 = tag[s], t1 = tag[ms + s];
+    if (t0.w != 0u && t0.x == X0 && t0.y == X1 && t0.z == X2) {
+      bank = 0;
+    } else if (t1.w != 0u && t1.x == X0 && t1.y == X1 && t1.z == X2) {
+      bank = 1;
+    } else {
+      need = true;
+      const uint32_t C0 = ws.cur[3 * s], C1 = ws.cur[3 * s + 1], C2 = ws.cur[3 * s + 2];
+      bank = (t0.w != 0u && t0.x == C0 && t0.y == C1 && t0.z == C2) ? 1 : 0;
+    }
+    sel[lane] = (bank * ms + s) * tl;
   }
   uint32_t mask = __ballot_sync(0xffffffffu, need);
+  __syncwarp();
   const int e0 = P.axE[0], e01 = P.axE[0] + P.axE[1];
   while (mask) {
     const int q = __ffs(mask) - 1;
     mask &= mask - 1u;
     const int4 run = ws.runs[q];
-    const int s = run.w & 0xFF;
+    const int sq = run.w & 0xFF;
     const double ns = (double)(run.y - run.x);
-    double *t = tab + (size_t)s * P.tabLen;
+    double *t = tab + sel[q];
     for (int j = lane; j < P.tabE; j += 32) {
       const int a = j < e0 ? 0 : (j < e01 ? 1 : 2);
       const int n = j - (a == 0 ? 0 : (a == 1 ? e0 : e01));
       double sn, cs;
-      sincos_turn_f64((uint32_t)n * sites[3 * s + a], &sn, &cs);
+      sincos_turn_f64((uint32_t)n * sites[3 * sq + a], &sn, &cs);
       if (a == 0) {
         sn *= ns;
         cs *= ns;
@@ -609,10 +644,7 @@ __device__ __forceinline__ void factor_tables(const Params &P, const WarpView &w
       t[P.axOff[a] + P.axE[a] + n] = sn;
     }
   }
-  if (need) {
-    const int s = ws.runs[lane].w & 0xFF;
-    tag[s] = make_uint4(sites[3 * s], sites[3 * s + 1], sites[3 * s + 2], 1u);
-  }
+  if (need) tag[bank * ms + s] = make_uint4(sites[3 * s], sites[3 * s + 1], sites[3 * s + 2], 1u);
   __syncwarp();
 }
 
@@ -646,9 +678,9 @@ __device__ __forceinline__ void group_sums_f64(const double *ic, const float4 *g
 // table entries whose indices (10 bits each) the host packed per (k, h).  The
 // two reflections of a lane share each run's loads; their table offsets are
 // unpacked once per monomial, outside the loop over sites.
-__device__ __forceinline__ void factored_rows(const Params &P, const WarpView &ws, const double *tab, double *ic,
-                                              const ReflRec *refl, const unsigned char *stat, int base, int nAct,
-                                              int lane, float *traceIc) {
+__device__ __forceinline__ void factored_rows(const Params &P, const WarpView &ws, const double *tab, const int *sel,
+                                              double *ic, const ReflRec *refl, const unsigned char *stat, int base,
+                                              int nAct, int lane, float *traceIc) {
   constexpr int NR = 2;
   const int nRuns = ws.meta[1];
   const int nM = P.nMono, pad = P.nReflPad, tl = P.tabLen;
@@ -675,9 +707,10 @@ __device__ __forceinline__ void factored_rows(const Params &P, const WarpView &w
       o2[j] = (int)(w >> 20);
       acc[j] = 0.0;
     }
+#pragma unroll 4
     for (int q = 0; q < nRuns; ++q) {
       const int4 run = ws.runs[q];
-      const double *t = tab + (size_t)(run.w & 0xFF) * tl;
+      const double *t = tab + sel[q];
       const double *fq = f64 + (size_t)run.z * pad;
 #pragma unroll
       for (int j = 0; j < NR; ++j) acc[j] = fma(fq[r[j]], t[o0[j]] * t[o1[j]] * t[o2[j]], acc[j]);
@@ -704,9 +737,11 @@ __device__ __forceinline__ void fitness_factored(const Params &P, const WarpView
                                                  const unsigned char *stat, const float4 *groups,
                                                  const double *sooPrefix, int nga, int lane, double sums[3],
                                                  float *traceIc) {
-  factor_tables(P, ws, sites, tab, tag, lane);
+  int *sel = reinterpret_cast<int *>(tag + 2 * P.maxSites);
+  factor_tables(P, ws, sites, tab, tag, sel, lane);
   const int nAct = nrefl_active(groups, nga);
-  for (int base = 0; base < nAct; base += 64) factored_rows(P, ws, tab, ic, refl, stat, base, nAct, lane, traceIc);
+  for (int base = 0; base < nAct; base += 64)
+    factored_rows(P, ws, tab, sel, ic, refl, stat, base, nAct, lane, traceIc);
   __syncwarp();
   group_sums_f64(ic, groups, sooPrefix, nga, lane, sums);
 }
@@ -1247,10 +1282,108 @@ __device__ __noinline__ uint32_t poly_propose(const Params &P, WarpView &ws, con
 
 // SLOTS > 0: the distance-rule variants, the only ones whose problems can
 // have counted rules and so polyhedron moves.
+// Fragment parameters -> fixed-point site coordinates (lane i: atom i).
+// The torsions are applied from the reference geometry outward in their
+// order, each about its bond as the earlier torsions left it (forward
+// kinematics; the axis atoms are read from their lanes), then the rotation of
+// the unit quaternion q = (w, x, y, z), then Cartesian -> fractional plus the
+// translation.  prm: t[3], q[4], torsion angles.
+__device__ __noinline__ void frag_atoms(const FragDev &F, const float *prm, uint32_t *out, int lane) {
+  const bool mine = lane < F.nAtoms;
+  float x = mine ? F.ref[3 * lane] : 0.f, y = mine ? F.ref[3 * lane + 1] : 0.f, z = mine ? F.ref[3 * lane + 2] : 0.f;
+  for (int t = 0; t < F.nTors; ++t) {
+    const int b = F.axisB[t], c = F.axisC[t];
+    const float bx = __shfl_sync(0xffffffffu, x, b), by = __shfl_sync(0xffffffffu, y, b),
+                bz = __shfl_sync(0xffffffffu, z, b);
+    const float cx = __shfl_sync(0xffffffffu, x, c), cy = __shfl_sync(0xffffffffu, y, c),
+                cz = __shfl_sync(0xffffffffu, z, c);
+    if ((F.moving[t] >> lane) & 1u) {
+      float ux = cx - bx, uy = cy - by, uz = cz - bz;
+      const float inv = rsqrtf(ux * ux + uy * uy + uz * uz);
+      ux *= inv; uy *= inv; uz *= inv;
+      float sn, cs;
+      sincosf(prm[7 + t], &sn, &cs);
+      // Rodrigues: v' = v cos + (u x v) sin + u (u.v)(1 - cos), v about b
+      const float vx = x - bx, vy = y - by, vz = z - bz;
+      const float d = ux * vx + uy * vy + uz * vz;
+      const float wx = uy * vz - uz * vy, wy = uz * vx - ux * vz, wz = ux * vy - uy * vx;
+      x = bx + vx * cs + wx * sn + ux * d * (1.f - cs);
+      y = by + vy * cs + wy * sn + uy * d * (1.f - cs);
+      z = bz + vz * cs + wz * sn + uz * d * (1.f - cs);
+    }
+  }
+  if (!mine) return;
+  const float qw = prm[3], qx = prm[4], qy = prm[5], qz = prm[6];
+  const float r00 = 1.f - 2.f * (qy * qy + qz * qz), r01 = 2.f * (qx * qy - qw * qz), r02 = 2.f * (qx * qz + qw * qy);
+  const float r10 = 2.f * (qx * qy + qw * qz), r11 = 1.f - 2.f * (qx * qx + qz * qz), r12 = 2.f * (qy * qz - qw * qx);
+  const float r20 = 2.f * (qx * qz - qw * qy), r21 = 2.f * (qy * qz + qw * qx), r22 = 1.f - 2.f * (qx * qx + qy * qy);
+  const float X = r00 * x + r01 * y + r02 * z, Y = r10 * x + r11 * y + r12 * z, Z = r20 * x + r21 * y + r22 * z;
+  const float *T = F.toFrac;
+  out[3 * lane] = frac_to_fixed(T[0] * X + T[1] * Y + T[2] * Z + prm[0]);
+  out[3 * lane + 1] = frac_to_fixed(T[3] * X + T[4] * Y + T[5] * Z + prm[1]);
+  out[3 * lane + 2] = frac_to_fixed(T[6] * X + T[7] * Y + T[8] * Z + prm[2]);
+}
+
+// A fragment proposal: with probability 1/4 every parameter moves, otherwise
+// one group -- the translation, the orientation or one torsion -- chosen
+// uniformly.  Gaussian steps of the replica's width sd: translation sd x
+// transStep per axis, orientation a turn of sd x angleStep about a random
+// axis, torsion sd x angleStep.  Lane 0 draws (Philox, its own counters) and
+// writes the proposed parameters; every lane then maps them to coordinates.
+__device__ __noinline__ void frag_propose(const Params &P, float *fcur, float *fprop, uint32_t *prop, int g, int p,
+                                          int lane, float sd, uint2 key, float *uMetro) {
+  const FragDev &F = *P.frag;
+  if (lane == 0) {
+    const uint4 a = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xF7A60000u, 1u), key);
+    const uint4 b = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xF7A60000u, 2u), key);
+    const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xF7A60000u, 3u), key);
+    for (int k = 0; k < kFragParams; ++k) fprop[k] = fcur[k];
+    const bool all = u01(a.x) < 0.25f;
+    const int pick = min(1 + F.nTors, (int)(u01(a.y) * (float)(2 + F.nTors)));
+    const float2 n0 = gauss2(b.x, b.y), n1 = gauss2(b.z, b.w), n2 = gauss2(c.x, c.y), n3 = gauss2(c.z, c.w);
+    if (all || pick == 0) {
+      fprop[0] += n0.x * sd * F.transStep;
+      fprop[1] += n0.y * sd * F.transStep;
+      fprop[2] += n1.x * sd * F.transStep;
+      for (int k = 0; k < 3; ++k) fprop[k] -= floorf(fprop[k]);
+    }
+    if (all || pick == 1) {
+      float ax = n1.y, ay = n2.x, az = n2.y;
+      const float nn = rsqrtf(fmaxf(ax * ax + ay * ay + az * az, 1e-20f));
+      ax *= nn; ay *= nn; az *= nn;
+      float sn, cs;
+      sincosf(0.5f * n3.x * sd * F.angleStep, &sn, &cs);
+      const float dw = cs, dx = ax * sn, dy = ay * sn, dz = az * sn;
+      const float qw = fcur[3], qx = fcur[4], qy = fcur[5], qz = fcur[6];
+      float w = dw * qw - dx * qx - dy * qy - dz * qz, x = dw * qx + dx * qw + dy * qz - dz * qy,
+            y = dw * qy - dx * qz + dy * qw + dz * qx, z = dw * qz + dx * qy - dy * qx + dz * qw;
+      const float qn = rsqrtf(w * w + x * x + y * y + z * z);
+      fprop[3] = w * qn; fprop[4] = x * qn; fprop[5] = y * qn; fprop[6] = z * qn;
+    }
+    for (int t = 0; t < F.nTors; ++t)
+      if (all || pick == 2 + t) {
+        const uint4 d = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)p, 0xF7A60000u, 4u + (uint32_t)t), key);
+        float v = fprop[7 + t] + gauss2(d.x, d.y).x * sd * F.angleStep;
+        v -= 6.28318530717958647f * floorf(v * 0.159154943091895336f + 0.5f);   // into [-pi, pi)
+        fprop[7 + t] = v;
+      }
+    *uMetro = u01(a.z);
+  }
+  *uMetro = __shfl_sync(0xffffffffu, *uMetro, 0);
+  __syncwarp();
+  frag_atoms(F, fprop, prop, lane);
+  __syncwarp();
+}
+
 template <int SLOTS>
 __device__ __forceinline__ void propose(const Params &P, WarpView &ws, const ProjFix *proj, const OpFix *ops, int g,
                                         int p, int lane, float sd, uint32_t seed, float *uMetro) {
   const uint2 key = make_uint2(seed, P.runKey);
+  if (P.frag) {
+    float *fp = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(ws.meta) + P.fragOff);
+    frag_propose(P, fp, fp + kFragParams, ws.prop, g, p, lane, sd, key, uMetro);
+    return;
+  }
   uint32_t polyMask = 0;
   if (SLOTS > 0 && P.polyProb > 0.f) {
     if (lane == 0) {
@@ -1412,6 +1545,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
   double *ftabs = COSMODE == 2 ? reinterpret_cast<double *>(wbase + P.tabOff) : nullptr;
   uint4 *ftags = COSMODE == 2 ? reinterpret_cast<uint4 *>(wbase + P.tagOff) : nullptr;
   double *ic64 = reinterpret_cast<double *>(wbase + P.icOff);
+  float *fcurW = reinterpret_cast<float *>(wbase + P.fragOff);   // fragment parameters: current, then proposed
   uint4 *atomsB[2] = {atoms, INCR ? reinterpret_cast<uint4 *>(wbase + P.atoms2Off) : atoms};
 
   for (int L = L0; L < nLadders; L += Lstep) {
@@ -1455,7 +1589,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
       for (int j = lane; j < P.nTot; j += 32) gen[j] = __ldg(P.gen + (size_t)A * P.nTot + j);
       for (int j = lane; j < P.maxSites; j += 32) proj[j] = P.proj[(size_t)A * P.maxSites + j];
       if constexpr (COSMODE == 2)
-        for (int j = lane; j < P.maxSites; j += 32) ftags[j] = make_uint4(0u, 0u, 0u, 0u);
+        for (int j = lane; j < 2 * P.maxSites; j += 32) ftags[j] = make_uint4(0u, 0u, 0u, 0u);
+      if (P.frag && lane < kFragParams) fcurW[lane] = P.fragState[(size_t)p * kFragParams + lane];
     }
     __syncwarp();
     const uint32_t allSites = P.maxSites >= 32 ? 0xffffffffu : ((1u << P.maxSites) - 1u);
@@ -1594,6 +1729,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             for (int j = lane; j < (int)curStride; j += 32) P.tracePos[(size_t)p * curStride + j] = ws.prop[j];
           if (acc) {
             for (int j = lane; j < (int)curStride; j += 32) ws.cur[j] = ws.prop[j];
+            if (P.frag && lane < kFragParams) fcurW[lane] = fcurW[kFragParams + lane];
             if constexpr (INCR) {
               cb ^= 1;
               if (__popc(moved) == 1) {
@@ -1607,8 +1743,10 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
               }
             }
           }
-          if (best)
+          if (best) {
             for (int j = lane; j < (int)curStride; j += 32) bestBase[(size_t)p * curStride + j] = ws.prop[j];
+            if (P.frag && lane < kFragParams) P.fragBest[(size_t)p * kFragParams + lane] = fcurW[kFragParams + lane];
+          }
           __syncwarp();
         } else if (lane == 0 && P.traceRec) {
           float *rec = P.traceRec + (size_t)p * 8;
@@ -1674,12 +1812,19 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
             wa.cur[j] = wb.cur[j];
             wb.cur[j] = t;
           }
+          if (P.frag && lane < kFragParams) {
+            float *fa = reinterpret_cast<float *>(mine + P.fragOff), *fb = reinterpret_cast<float *>(other + P.fragOff);
+            const float t = fa[lane];
+            fa[lane] = fb[lane];
+            fb[lane] = t;
+          }
         }
         ladder_sync<RANKS>();
       }
     }
     if (active) {
       for (int j = lane; j < (int)curStride; j += 32) P.pos[(size_t)p * curStride + j] = ws.cur[j];
+      if (P.frag && lane < kFragParams) P.fragState[(size_t)p * kFragParams + lane] = fcurW[lane];
       if (lane == 0) {
         PState st;
         st.fit = fit; st.cc = cc0; st.pen = pen0; st.step = step; st.temp = temp;
@@ -1861,6 +2006,17 @@ __global__ void wy_expand_one(const Params P, const uint32_t *genOrig, int parti
 
 __global__ void philox_one(uint4 c, uint2 k, uint4 *out) { *out = philox4x32_10(c, k); }
 
+// One warp per parameter vector: the fragment's fixed-point coordinates.
+__global__ void wy_fragment_atoms_kernel(const FragDev *F, const float *prm, int n, uint32_t *out) {
+  const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (v >= n) return;
+  __shared__ uint32_t buf[8][kFragMaxAtoms * 3];
+  uint32_t *o = buf[threadIdx.x >> 5];
+  frag_atoms(*F, prm + (size_t)v * kFragParams, o, lane);
+  __syncwarp();
+  for (int j = lane; j < F->nAtoms * 3; j += 32) out[(size_t)v * F->nAtoms * 3 + j] = o[j];
+}
+
 }  // namespace wy
 }  // namespace p6
 
@@ -1884,6 +2040,8 @@ struct p6_wy_session {
   int *dNRuns = nullptr, *dNF = nullptr, *dLadders = nullptr, *dSchedG = nullptr, *dErr = nullptr;
   float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr, *dQuench = nullptr;
   double *dTraceSums = nullptr;   // per particle {scc, soo, sco} of the last traced evaluation
+  FragDev *dFrag = nullptr;       // rigid-fragment search (p6_wy_set_fragment)
+  float *dFragState = nullptr, *dFragBest = nullptr;
   int quenchLen = 0;
   // learned search: candidates, features, scores, the chosen proposal
   uint32_t *dCand = nullptr, *dExt = nullptr;
@@ -2000,7 +2158,7 @@ static void free_session(p6_wy_session *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
-                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTraceSums, s->dTracePos, s->dOps,
+                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTraceSums, s->dFrag, s->dFragState, s->dFragBest, s->dTracePos, s->dOps,
                   s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap, s->dCand, s->dExt, s->dFeat, s->dScore,
                   s->dChosenFeat, s->dChosenScore, s->dPairRange};
   for (void *p : ptrs)
@@ -2485,8 +2643,11 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   // the factored evaluation keeps FP64 |F|^2 and, per site, its axis tables and their coordinate tags
   const size_t icEnd = icOff + (size_t)nReflPad * (factored ? sizeof(double) : sizeof(float));
   const size_t tabOff = (icEnd + 15) & ~(size_t)15;
-  const size_t tagOff = tabOff + (factored ? (size_t)ms * tabLen * sizeof(double) : 0);
-  const size_t baseEnd = factored ? tagOff + (size_t)ms * sizeof(uint4) : icEnd;
+  const size_t tagOff = tabOff + (factored ? (size_t)2 * ms * tabLen * sizeof(double) : 0);
+  // two banks of tags, then the table offset each run reads
+  const size_t fragOff =
+      ((factored ? tagOff + (size_t)2 * ms * sizeof(uint4) + (size_t)ms * sizeof(int) : icEnd) + 15) & ~(size_t)15;
+  const size_t baseEnd = fragOff + 2 * kFragParams * sizeof(float);   // fragment parameters: current, proposed
   const size_t atoms2Off = (baseEnd + 15) & ~(size_t)15;
   const size_t cbOff = atoms2Off + (size_t)nTot * sizeof(uint4);
   const size_t incrEnd = cbOff + (size_t)(ms + 1) * nReflPad * comp * sizeof(float);
@@ -2657,6 +2818,10 @@ p6_status p6_wy_create(const p6_wy_problem *pr, int device, p6_wy_session **out)
   P.tabOff = (int)tabOff;
   P.tagOff = (int)tagOff;
   P.traceSums = nullptr;
+  P.frag = nullptr;
+  P.fragState = nullptr;
+  P.fragBest = nullptr;
+  P.fragOff = (int)fragOff;
   P.genOff = (int)genOff;
   P.projOff = (int)projOff;
   P.atomsOff = (int)atomsOff;
@@ -3008,6 +3173,94 @@ p6_status p6_wy_read_trace_ic(p6_wy_session *s, float *ic) {
   return P6_OK;
 }
 
+p6_status p6_wy_set_fragment(p6_wy_session *s, const p6_wy_fragment *f) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (!f) {
+    s->P.frag = nullptr;
+    return P6_OK;
+  }
+  if (s->P.nAssign != 1) return set_error(P6_ERR_INVALID_ARG, "a fragment search takes one assignment");
+  if (f->n_atoms < 1 || f->n_atoms > kFragMaxAtoms || f->n_atoms > s->P.maxSites)
+    return set_error(P6_ERR_CAPACITY, "the fragment has more atoms than the sites (or than 32)");
+  if (f->n_tors < 0 || f->n_tors > kFragMaxTors) return set_error(P6_ERR_CAPACITY, "at most 8 torsions");
+  FragDev h{};
+  h.nAtoms = f->n_atoms;
+  h.nTors = f->n_tors;
+  for (int t = 0; t < f->n_tors; ++t) {
+    if (f->axis_b[t] < 0 || f->axis_b[t] >= f->n_atoms || f->axis_c[t] < 0 || f->axis_c[t] >= f->n_atoms ||
+        f->axis_b[t] == f->axis_c[t])
+      return set_error(P6_ERR_INVALID_ARG, "a torsion axis names an atom outside the fragment");
+    h.axisB[t] = f->axis_b[t];
+    h.axisC[t] = f->axis_c[t];
+    h.moving[t] = f->moving[t] & (f->n_atoms >= 32 ? 0xffffffffu : ((1u << f->n_atoms) - 1u));
+  }
+  for (int i = 0; i < 3 * f->n_atoms; ++i) h.ref[i] = (float)f->ref_xyz[i];
+  for (int i = 0; i < 9; ++i) h.toFrac[i] = (float)f->to_frac[i];
+  h.transStep = (float)f->trans_step;
+  h.angleStep = (float)f->angle_step;
+  if (!s->dFrag) P6_CUDA(cudaMalloc(&s->dFrag, sizeof(FragDev)));
+  if (!s->dFragState) {
+    P6_CUDA(cudaMalloc(&s->dFragState, (size_t)s->P.numParticles * kFragParams * sizeof(float)));
+    P6_CUDA(cudaMalloc(&s->dFragBest, (size_t)s->P.numParticles * kFragParams * sizeof(float)));
+    P6_CUDA(cudaMemsetAsync(s->dFragState, 0, (size_t)s->P.numParticles * kFragParams * sizeof(float), s->stream));
+    P6_CUDA(cudaMemsetAsync(s->dFragBest, 0, (size_t)s->P.numParticles * kFragParams * sizeof(float), s->stream));
+  }
+  P6_CUDA(cudaMemcpyAsync(s->dFrag, &h, sizeof(FragDev), cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  s->P.frag = s->dFrag;
+  s->P.fragState = s->dFragState;
+  s->P.fragBest = s->dFragBest;
+  return P6_OK;
+}
+
+p6_status p6_wy_write_fragment_state(p6_wy_session *s, const float *current) {
+  P6_ENTRY();
+  if (!s || !current || !s->dFragState) return set_error(P6_ERR_INVALID_ARG, "no fragment set");
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t bytes = (size_t)s->P.numParticles * kFragParams * sizeof(float);
+  P6_CUDA(cudaMemcpyAsync(s->dFragState, current, bytes, cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaMemcpyAsync(s->dFragBest, current, bytes, cudaMemcpyHostToDevice, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_read_fragment_state(p6_wy_session *s, float *current, float *best) {
+  P6_ENTRY();
+  if (!s || !s->dFragState) return set_error(P6_ERR_INVALID_ARG, "no fragment set");
+  P6_CUDA(cudaSetDevice(s->device));
+  const size_t bytes = (size_t)s->P.numParticles * kFragParams * sizeof(float);
+  if (current) P6_CUDA(cudaMemcpyAsync(current, s->dFragState, bytes, cudaMemcpyDeviceToHost, s->stream));
+  if (best) P6_CUDA(cudaMemcpyAsync(best, s->dFragBest, bytes, cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return P6_OK;
+}
+
+p6_status p6_wy_debug_fragment(p6_wy_session *s, const float *params, int n, uint32_t *coords) {
+  P6_ENTRY();
+  if (!s || !s->dFrag || !params || !coords || n <= 0) return set_error(P6_ERR_INVALID_ARG, "no fragment or bad arguments");
+  P6_CUDA(cudaSetDevice(s->device));
+  int nAtoms = 0;
+  P6_CUDA(cudaMemcpy(&nAtoms, s->dFrag, sizeof(int), cudaMemcpyDeviceToHost));
+  float *dp = nullptr;
+  uint32_t *dc = nullptr;
+  P6_CUDA(cudaMalloc(&dp, (size_t)n * kFragParams * sizeof(float)));
+  cudaError_t e = cudaMalloc(&dc, (size_t)n * nAtoms * 3 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, params, (size_t)n * kFragParams * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) {
+    wy_fragment_atoms_kernel<<<(n + 7) / 8, 256, 0, s->stream>>>(s->dFrag, dp, n, dc);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(coords, dc, (size_t)n * nAtoms * 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaFree(dp);
+  if (dc) cudaFree(dc);
+  if (e != cudaSuccess) return cuda_error(e, "fragment coordinates");
+  return P6_OK;
+}
+
 p6_status p6_wy_read_trace_sums(p6_wy_session *s, double *sums) {
   P6_ENTRY();
   if (!s || !s->dTraceSums || !sums) return set_error(P6_ERR_INVALID_ARG, "tracing was not enabled");
@@ -3071,6 +3324,7 @@ extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, in
   if (!s || K < 1 || (K > 1 && !net)) return set_error(P6_ERR_INVALID_ARG, "bad arguments");
   if (!s->dLadders) return set_error(P6_ERR_INVALID_ARG, "no ladders set (p6_wy_set_ladders)");
   if (!s->dSchedG || gen < 0 || gen >= s->schedLen) return set_error(P6_ERR_INVALID_ARG, "generation outside the schedule");
+  if (s->P.frag) return set_error(P6_ERR_INVALID_ARG, "the learned step moves sites, not a fragment");
   if (net && (mlp::input_dim(net) != kFeat || mlp::output_dim(net) < 1))
     return set_error(P6_ERR_INVALID_ARG, "the network must take 64 features");
   if (s->incremental) return set_error(P6_ERR_INVALID_ARG, "the learned search uses the full evaluation");

@@ -11,7 +11,9 @@ It reads, read-only:
     parameter count, projector (P, T) and the orbit of a fixed generic point;
   * scatters/xray_wk1995_ions.json: the five-Gaussian coefficients of the few
     elements the tests and benchmarks use (Waasmaier & Kirfel, Acta Cryst. A51
-    (1995) 416, as tabulated by cctbx).
+    (1995) 416, as tabulated by cctbx);
+  * test_files/cimetidine/cime.pdb: cimetidine's 17 non-hydrogen atoms and
+    their bonds, the molecule of the learned-proposal workload.
 
 Only derived, compact records are written (operator sets as integers over 24,
 rational projectors, orbit coordinates); nothing else from the reference tree is
@@ -81,7 +83,26 @@ def main(ref_root):
     # the package reads the coefficients for its synthetic workloads (one copy, package data)
     ff_path = HERE.parent.parent / 'powder6_b200' / 'data' / 'xray_wk1995_subset.json'
     ff_path.write_text(text)
-    print('wrote', HERE / 'sg_fixture.json', ff_path)
+    # the config-5 molecule: cimetidine's non-hydrogen atoms (element, Cartesian A) and their bonds,
+    # from the reference's test file test_files/cimetidine/cime.pdb (ATOM records and CONECT)
+    atoms, serial_of, bonds = [], {}, set()
+    for line in (ref / 'test_files' / 'cimetidine' / 'cime.pdb').read_text().splitlines():
+        if line.startswith(('ATOM', 'HETATM')):
+            el = line[76:78].strip() or line[12:16].strip()[:1]
+            if el.upper() == 'H':
+                continue
+            serial_of[int(line[6:11])] = len(atoms)
+            atoms.append({'element': el.capitalize(), 'xyz': [float(line[30:38]), float(line[38:46]),
+                                                               float(line[46:54])]})
+        elif line.startswith('CONECT'):
+            nums = [int(v) for v in line[6:].split()[:5] if v.isdigit()]
+            for other in nums[1:]:
+                if nums[0] in serial_of and other in serial_of:
+                    bonds.add(tuple(sorted((serial_of[nums[0]], serial_of[other]))))
+    mol_path = HERE.parent.parent / 'powder6_b200' / 'data' / 'cimetidine_heavy.json'
+    mol_path.write_text(json.dumps({'source': 'cimetidine, non-hydrogen atoms of the reference test file',
+                                    'atoms': atoms, 'bonds': sorted(bonds)}, indent=1))
+    print('wrote', HERE / 'sg_fixture.json', ff_path, mol_path)
 
 
 if __name__ == '__main__':
