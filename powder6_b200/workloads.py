@@ -247,12 +247,13 @@ def _cell_volume(cell) -> float:
 
 
 def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelength: float = 1.5406,
-                     max_refl: int = 3000):
+                     max_refl: int = 3000, min_refl: int = 50):
     """Seeded uneven problems: space groups from BATCH_GROUPS, 1-24 sites and
     50-3000 reflections and 2000-12000 points and 256-2048 replicas (all
     log-uniform), cells uniform in 4-20 A, at most ``max_atoms`` atoms per
     cell (resampled otherwise).  The reflection count sets d_min through the
-    volume of the reciprocal sphere, capped at ``max_refl`` (a search whose
+    volume of the reciprocal sphere, kept within [``min_refl``, ``max_refl``]
+    by moving d_min (a search whose
     tables do not fit in shared memory next to its eight replica slices reads
     them from global memory); the point count is recorded only (the search's
     fitness works on integrated intensities)."""
@@ -284,14 +285,17 @@ def batched_problems(n: int = 64, seed: int = 1, max_atoms: int = 512, wavelengt
         dmin = (4 * math.pi * vol / (3 * 2 * n_pg * n_c * target)) ** (1.0 / 3.0)
         dmin = max(dmin, wavelength / 2 * 1.0001)
         pseed = int(rng.integers(1 << 30))
-        for _retry in range(6):
+        for _retry in range(8):
             prob = wyckoff_problem(seed=pseed, group_number=g.number, cell=cell,
                                    composition=tuple(comp.items()), sites=tuple(labels), dmin=dmin,
                                    wavelength=wavelength, true_min_contact=1.0, contact_attempts=40)
-            if prob.refl.n_refl <= max_refl:
+            if prob.refl.n_refl > max_refl:
+                dmin *= 1.02 * (prob.refl.n_refl / max_refl) ** (1.0 / 3.0)
+            elif prob.refl.n_refl < min_refl and dmin > wavelength / 2 * 1.0001:
+                dmin = max(wavelength / 2 * 1.0001, dmin * 0.98 * (prob.refl.n_refl / min_refl) ** (1.0 / 3.0))
+            else:
                 break
-            dmin *= 1.02 * (prob.refl.n_refl / max_refl) ** (1.0 / 3.0)
-        if prob.refl.n_refl < 8 or prob.refl.n_refl > max_refl:
+        if prob.refl.n_refl < min_refl or prob.refl.n_refl > max_refl:
             continue
         replicas = int(round(_log_uniform(rng, 256, 2048) / 8)) * 8
         points = int(round(_log_uniform(rng, 2000, 12000)))
