@@ -346,7 +346,8 @@ struct Shared {
 // unit-scale heights u1 for the scale column of the least-squares finish.
 template <bool F64, class PK, class H>
 __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK *pk2, H *h1, H *w2, double *u1,
-                                 int *act, const double *tth) {
+                                 int *act, const double *tth, const float *f2read = nullptr,
+                                 float *f2write = nullptr) {
   using A_t = typename std::conditional<F64, double, float>::type;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double *v = sh.v;
@@ -354,6 +355,10 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
   const bool doublet = P.ratio > 1e-6 && P.lambda2 > 1e-6 && fabs(P.lambda1 - P.lambda2) > 1e-6;
   // |F|^2: warp per reflection, lanes over the coset representatives
   for (int k = warp; k < nR; k += kWarps) {
+    if (f2read) {   // |F|^2 (x March-Dollase) of these cell, Biso and r values, computed by an earlier move
+      if (lane == 0) h1[k] = (H)f2read[k];
+      continue;
+    }
     const int hh = P.hkl[3 * k], kk = P.hkl[3 * k + 1], ll = P.hkl[3 * k + 2];
     const double q = hh * hh * sh.f[0] + kk * kk * sh.f[1] + ll * ll * sh.f[2] + hh * kk * sh.f[3] +
                      kk * ll * sh.f[4] + hh * ll * sh.f[5];
@@ -393,7 +398,10 @@ __device__ void reflection_stage(const Params &P, const Shared &sh, PK *pk1, PK 
       }
     }
     const double po = (P.hasPo && live) ? po_factor(P, sh.f, v[PBKG0 + P.nBkg], k, lane) : 1.0;
-    if (lane == 0) h1[k] = (H)(((double)A * A + (double)B * B) * po);   // F^2 (x March-Dollase), parked until the heights
+    if (lane == 0) {
+      h1[k] = (H)(((double)A * A + (double)B * B) * po);   // F^2 (x March-Dollase), parked until the heights
+      if (f2write) f2write[k] = (float)h1[k];
+    }
   }
   __syncwarp();
   // Peaks: lane pairs over this warp's reflections, the even lane preparing
@@ -694,14 +702,15 @@ __device__ void solve_free_heights(const Params &P, const Shared &sh, const PK *
 // through distributed shared memory.
 __device__ double evaluate(const Params &P, Shared &sh, Peak *pk1, Peak *pk2, float *h1, float *w2, int *act,
                            const double *tth, const double *yobs, const float *wobs, float *ycalc,
-                           double *nn = nullptr, int split = 1, int rank = 0) {
+                           double *nn = nullptr, int split = 1, int rank = 0, const float *f2read = nullptr,
+                           float *f2write = nullptr) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) sh.valid = inv_dsq_form(sh.v, sh.f) ? 1 : 0;
   __syncthreads();
   if (!sh.valid) return INFINITY;
   const double *v = sh.v;
   const int nR = P.nRefl;
-  reflection_stage<false>(P, sh, pk1, pk2, h1, w2, nullptr, act, tth);
+  reflection_stage<false>(P, sh, pk1, pk2, h1, w2, nullptr, act, tth, f2read, f2write);
   __syncthreads();
   if (P.method == 1) solve_free_heights(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nn);
   // --- pattern in warp tiles of 32 points, then chi^2 (FP64)
@@ -801,7 +810,7 @@ __device__ __forceinline__ double uniform_open(uint32_t x) { return ((double)x +
 // Kernels.
 // ---------------------------------------------------------------------------
 struct SmemLayout {
-  int pk1, pk2, h1, w2, act, tth, y, w, total;
+  int pk1, pk2, h1, w2, act, f2, tth, y, w, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int nRefl, int n, int stage) {
@@ -813,6 +822,7 @@ __host__ __device__ inline SmemLayout smem_layout(int nRefl, int n, int stage) {
   L.h1 = take(nRefl * 4);
   L.w2 = take(nRefl * 4);
   L.act = take(nRefl * 4);
+  L.f2 = take(2 * nRefl * 4);   // two banks of |F|^2 for the sweep's moves that keep the cell, Biso and r
   L.tth = stage ? take(n * 8) : 0;
   L.y = stage ? take(n * 8) : 0;
   L.w = stage ? take(n * 4) : 0;
@@ -848,10 +858,19 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
   __shared__ double xs[kMaxNv];
   __shared__ Chain st;
   __shared__ int drawnJ;
+  // |F|^2 reuse: bank f2cur holds the current state's |F|^2 when f2valid; a move that changes
+  // no parameter |F|^2 depends on (cell, Biso, March-Dollase r) reads it, any other writes the other bank
+  __shared__ int f2cur, f2valid, f2mode, f2bank, f2isF;
   const SmemLayout L = smem_layout(P.nRefl, P.n, P.stageObs);
   Peak *pk1 = reinterpret_cast<Peak *>(smem + L.pk1), *pk2 = reinterpret_cast<Peak *>(smem + L.pk2);
   float *h1 = reinterpret_cast<float *>(smem + L.h1), *w2 = reinterpret_cast<float *>(smem + L.w2);
   int *act = reinterpret_cast<int *>(smem + L.act);
+  float *f2 = reinterpret_cast<float *>(smem + L.f2);
+  const bool reuseF2 = P.method == 0;
+  if (threadIdx.x == 0) {
+    f2cur = 0;
+    f2valid = 0;
+  }
   const double *tth = P.tth, *yobs = P.y;
   const float *wobs = P.w;
   if (P.stageObs) {
@@ -911,13 +930,23 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
         st.logu = log(uniform_open(r.w));
       }
       apply(P, xs, sh.v);
+      const int fi = bootstrap ? -1 : P.index[drawnJ];
+      f2isF = bootstrap || (fi >= PA && fi <= PGA) || fi == PBISO || (P.hasPo && fi == PBKG0 + P.nBkg);
+      f2mode = !reuseF2 ? 0 : (f2valid && !f2isF ? 1 : 2);       // 0 compute only, 1 read, 2 compute and keep
+      f2bank = f2mode == 1 ? f2cur : (f2valid || f2isF ? f2cur ^ 1 : f2cur);
     }
     __syncthreads();
+    const int nR = P.nRefl;
     const double cost = evaluate(P, sh, pk1, pk2, h1, w2, act, tth, yobs, wobs, nullptr,
-                                 P.method == 1 ? reinterpret_cast<double *>(smem + L.total) : nullptr, split, rank);
+                                 P.method == 1 ? reinterpret_cast<double *>(smem + L.total) : nullptr, split, rank,
+                                 f2mode == 1 ? f2 + f2bank * nR : nullptr, f2mode == 2 ? f2 + f2bank * nR : nullptr);
     if (threadIdx.x == 0) {
       st.proposalCost = cost;
       if (bootstrap) {
+        if (f2mode == 2 && sh.valid) {
+          f2cur = f2bank;
+          f2valid = 1;
+        }
         st.cost = cost;
         st.bestCost = cost;
         for (int j = 0; j < P.nv; ++j) st.best[j] = st.x[j];
@@ -925,6 +954,10 @@ __global__ void __launch_bounds__(kThreads) pt_sweep_kernel(const Params P, cons
         st.proposals += 1;
         const double before = st.cost;
         const bool acc = isfinite(cost) && (cost <= st.cost || st.logu < (st.cost - cost) / (2 * T));
+        if (f2mode == 2 && sh.valid && (!f2isF || acc)) {   // the bank now holds the current state's |F|^2
+          f2cur = f2bank;
+          f2valid = 1;
+        }
         if (P.trace && rank == 0 && m < P.nv) {
           double *tr = P.trace + (size_t)c * (kTraceHead + kTraceMove * P.nv) + kTraceHead + kTraceMove * m;
           const int jm = drawnJ;
