@@ -1850,7 +1850,7 @@ __global__ void __launch_bounds__(256, 4) wy_kernel(const __grid_constant__ Para
 // The same search with each ladder of 8 on a cluster of two 4-warp CTAs
 // (launched with cluster dimension 2): ladder = cluster index.
 template <int COSMODE, int SLOTS, int INCR>
-__global__ void __launch_bounds__(128, 8) wy_kernel_pair(const __grid_constant__ Params P, int gen0, int nGen,
+__global__ void __launch_bounds__(128, 7) wy_kernel_pair(const __grid_constant__ Params P, int gen0, int nGen,
                                                          int mcmc, int swapEvery, int reevalFirst) {
   wy_cta<COSMODE, SLOTS, INCR, 2>(P, blockIdx.x >> 1, gridDim.x >> 1, gen0, nGen, mcmc, swapEvery, reevalFirst);
 }
