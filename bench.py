@@ -63,8 +63,9 @@ def parse():
                          'learned: the learned-proposal search (P2_1/c, 17 sites, 8192 replicas); '
                          'refine: least-squares refinement of 512 perturbed PbSO4 structures; '
                          'cf: charge flipping, 128 random starts of the adaptive plan on a 64^3 grid')
-    ap.add_argument('--method', default='split', choices=['split', 'fp32'],
-                    help='contract: split-BF16 tensor cores (default) or plain FP32 CUDA cores')
+    ap.add_argument('--method', default='split', choices=['split', 'split3', 'fp32'],
+                    help='contract: two-part split-BF16 (default), three-part split-BF16 (six products, '
+                         'chi^2 within 4e-6 of FP64, half the rate), or plain FP32 CUDA cores')
     ap.add_argument('--cf-trials', type=int, default=None, help='cf: random starts (default 128)')
     ap.add_argument('--cf-cycles', type=int, default=None, help='cf: cycles per step (default 100)')
     ap.add_argument('--pt-method', default='rietveld', choices=['rietveld', 'wppf'],
@@ -499,10 +500,11 @@ def main_ct(args, world, rank, local, emit=True):
     second from CUDA events, I resident (196 MB, larger than L2); e2e: the
     same through p6_ct_run_host from pinned host memory (I in, chi^2 out)."""
     import torch
-    from powder6_b200.contraction import FP32, SPLIT_BF16, ContractionSession, banded_problem
+    from powder6_b200.contraction import FP32, SPLIT3_BF16, SPLIT_BF16, ContractionSession, banded_problem
     torch.cuda.set_device(local)
     p = banded_problem(seed=1 + rank)
-    method = SPLIT_BF16 if args.method == 'split' else FP32
+    method = {'split': SPLIT_BF16, 'split3': SPLIT3_BF16}.get(args.method, FP32)
+    tensor = method in (SPLIT_BF16, SPLIT3_BF16)
     M, K = p.intensities.shape
     N = p.profile_t.shape[0]
     pinned = torch.empty((M, K), dtype=torch.float32, pin_memory=True)
@@ -541,9 +543,10 @@ def main_ct(args, world, rank, local, emit=True):
         ms = float(np.mean(times))
         ms_eval = ms / reps
         n_mt = (M + 127) // 128
-        if method == SPLIT_BF16:
-            flops = 3 * 2.0 * 128 * 256 * 64 * q['band_kblocks'] * n_mt
-            note = 'executed tcgen05 MMA flops (3 bf16 products per K step over each tile band)'
+        if tensor:
+            products = 3 if method == SPLIT_BF16 else 6
+            flops = products * 2.0 * 128 * 256 * 64 * q['band_kblocks'] * n_mt
+            note = f'executed tcgen05 MMA flops ({products} bf16 products per K step over each tile band)'
             peak = measured_peak('bf16_tflops')
         else:
             flops = 2.0 * 128 * 128 * q['band_cols128'] * n_mt
@@ -555,12 +558,14 @@ def main_ct(args, world, rank, local, emit=True):
             'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None,
-            'dtype': 'bf16x3 split, fp32 accumulate, fp64 chi2' if method == SPLIT_BF16 else 'fp32, fp64 chi2',
+            'dtype': ('bf16x3 split, fp32 accumulate, fp64 chi2' if method == SPLIT_BF16 else
+                      'bf16 three-part split (6 products), fp32 accumulate, fp64 chi2' if method == SPLIT3_BF16 else
+                      'fp32, fp64 chi2'),
             'data': 'synthetic',
             'config': {'workload': CT_WORKLOAD, 'method': args.method, 'replicas': M, 'reflections': K, 'points': N,
                        'step': f'{reps} evaluations of all {M} replicas', 'ms_per_evaluation': ms_eval,
                        'l2': 'inputs larger than L2 (I is 196 MB)', 'parallelism': f'replicas only x{world}'},
-            'roofline': {'bound': 'tensor' if method == SPLIT_BF16 else 'fp32', 'achieved': achieved,
+            'roofline': {'bound': 'tensor' if tensor else 'fp32', 'achieved': achieved,
                          'peak': peak[0], 'unit': 'TFLOP/s',
                          'frac': achieved / peak[0] if peak[0] else None, 'traffic': None,
                          'note': f'{note}: {flops:.4g} per launch; useful banded flops {useful:.4g}; '

