@@ -56,13 +56,15 @@ def parse():
     ap.add_argument('--no-sub-workloads', action='store_true',
                     help='default workload: leave out the PT and contraction sub-results')
     ap.add_argument('--workload', default='wyckoff',
-                    choices=['wyckoff', 'pt', 'contract', 'batch', 'learned', 'refine', 'cf'],
+                    choices=['wyckoff', 'pt', 'contract', 'batch', 'learned', 'refine', 'cf', 'profile'],
                     help='wyckoff: the plain Wyckoff search (default); pt: the NaCl parallel-tempering fit; '
                          'contract: the fixed-profile contraction Y = I . P (16384 x 3000 x 12000); '
                          'batch: 64 uneven Wyckoff searches in one persistent launch; '
                          'learned: the learned-proposal search (P2_1/c, 17 sites, 8192 replicas); '
                          'refine: least-squares refinement of 512 perturbed PbSO4 structures; '
-                         'cf: charge flipping, 128 random starts of the adaptive plan on a 64^3 grid')
+                         'cf: charge flipping, 128 random starts of the adaptive plan on a 64^3 grid; '
+                         'profile: the PbSO4-like search against its powder pattern (fixed cell and profile, '
+                         'split-BF16 contraction), with time to target Rwp, chosen vs plain')
     ap.add_argument('--method', default='split', choices=['split', 'split3', 'fp32'],
                     help='contract: two-part split-BF16 (default), three-part split-BF16 (six products, '
                          'chi^2 within 4e-6 of FP64, half the rate), or plain FP32 CUDA cores')
@@ -1057,6 +1059,214 @@ def main_learned(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_reference_profile(args, world, rank):
+    if rank != 0:
+        return
+    from powder6_b200.profile_search import profile_problem
+    pp = profile_problem()
+    for _ in range(args.warmup):
+        profile_cpu_rate(pp, 0.3)
+    trials, dt = profile_cpu_rate(pp, 2.0 * args.steps)
+    v = trials / dt
+    sample = f'{trials} random structures, FP64 oracle port (per-reflection |F|^2, fitted-scale chi^2), one thread'
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'trial structures evaluated/s', 'value': v, 'unit': 'trials/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1000 * dt / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': PROFILE_WORKLOAD + ' (sampled trials)'},
+        'cpu_baseline': {'value': v, 'unit': 'trials/s', 'cores': 1, 'kind': 'port', 'sample': sample},
+        'e2e': {'value': v, 'unit': 'trials/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+
+
+def main_profile(args, world, rank, local, emit=True):
+    """The fixed-profile Wyckoff search.  One step = PROFILE_CHUNK generations
+    of all 4096 replicas with the chosen method (search kernel, three-part
+    split-BF16 contraction with the fitted scale, acceptance and exchange per
+    generation).  value: trials/s from CUDA events on the search's stream,
+    L2 flushed before each step; e2e: the same through the host API with
+    host buffers (positions and states uploaded, the chunk, positions, bests
+    and states read back).  The roofline is the contraction's (the largest
+    share of a generation), timed alone on the same shapes."""
+    import torch
+    from powder6_b200.contraction import ContractionSession
+    from powder6_b200.profile_search import SPLIT3_BF16, ProfileSearch, _ContractionInput, profile_problem
+    from powder6_b200.swarm_wyckoff import STATE_DTYPE
+    torch.cuda.set_device(local)
+    pp = profile_problem()
+    n = args.particles
+    method = SPLIT3_BF16
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f'cuda:{local}')
+    G = max(PROFILE_GENERATIONS, PROFILE_CHUNK * (args.steps + args.warmup))
+    with ProfileSearch(pp, n, run_key=5 + rank) as ps:
+        ps.start(G, seed=5 + rank, method=method)
+        ps.synchronize()
+        g0 = 0
+        for _ in range(args.warmup):
+            ps.run(g0, PROFILE_CHUNK, method)
+            g0 += PROFILE_CHUNK
+        ps.synchronize()
+        barrier(world)
+        l0 = ps.wy.launch_count() + ps.ct.query()['launches']
+        times = []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                ps.run(g0, PROFILE_CHUNK, method)
+                ps.synchronize()
+                times.append(ps.last_ms())
+                g0 += PROFILE_CHUNK
+        launches = ps.wy.launch_count() + ps.ct.query()['launches'] - l0
+        total_ms = max_over_ranks(float(sum(times)), world)
+        value = world * n * PROFILE_CHUNK * args.steps / (total_ms / 1000.0)
+        # end to end: host positions and states in, the chunk, positions, bests and states out
+        pos, _, st = ps.wy.read_state()
+        pin_pos = torch.empty(len(pos), dtype=torch.float32, pin_memory=True).numpy()
+        pin_pos[:] = pos
+        pin_st = torch.empty(len(st) * STATE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True).numpy().view(
+            STATE_DTYPE)
+        pin_st[:] = st
+        e2e = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ps.wy.sync_state(pin_pos, pin_st)
+            ps.run(g0 % (G - PROFILE_CHUNK), PROFILE_CHUNK, method)
+            ps.synchronize()
+            cur, best, stb = ps.wy.read_state()
+            e2e.append(time.perf_counter() - t0)
+        e2e_value = world * n * PROFILE_CHUNK * args.steps / max_over_ranks(float(sum(e2e)), world)
+        h2d = pin_pos.nbytes + pin_st.nbytes
+        d2h = 2 * pin_pos.nbytes + pin_st.nbytes
+    # the contraction alone on the same shapes (split, product, fitted reduction)
+    rng = np.random.default_rng(3)
+    I = rng.lognormal(0.0, 1.5, (n, pp.n_refl)).astype(np.float32)
+    with ContractionSession(_ContractionInput(pp), max_replicas=n, device=local) as s:
+        s.set_fitted(True)
+        s.set_intensities(I)
+        q = s.query()
+        for _ in range(5):
+            s.evaluate(method)
+        s.synchronize()
+        ct_ms = []
+        for _ in range(20):
+            s.evaluate(method)
+            s.synchronize()
+            ct_ms.append(s.last_ms())
+    if rank != 0:
+        return None
+    clocks = clk.summary()
+    ms = float(np.mean(times))
+    ms_gen = ms / PROFILE_CHUNK
+    ct_eval = float(np.median(ct_ms))
+    n_mt = (n + 127) // 128
+    flops = 6 * 2.0 * 128 * 256 * 64 * q['band_kblocks'] * n_mt
+    peak = measured_peak('bf16_tflops')
+    achieved = flops / (ct_eval / 1000.0) / 1e12
+    line = {
+        'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'fp64 |F|^2, bf16 three-part split (6 products) fp32 accumulate, fp64 chi2',
+        'data': 'synthetic',
+        'config': {'workload': PROFILE_WORKLOAD, 'method': 'split3-bf16', 'replicas': n,
+                   'reflections': pp.n_refl, 'points': pp.n_points,
+                   'step': f'{PROFILE_CHUNK} generations of all {n} replicas', 'us_per_generation': 1000 * ms_gen,
+                   'l2': 'flushed before every step (256 MB write)', 'parallelism': f'replicas only x{world}'},
+        'roofline': {'bound': 'tensor', 'achieved': achieved, 'peak': peak[0], 'unit': 'TFLOP/s',
+                     'frac': achieved / peak[0] if peak[0] else None, 'traffic': None,
+                     'note': f'contraction (split, tcgen05 product, fitted reduction) timed alone on the same '
+                             f'shapes: {ct_eval:.4f} ms per evaluation, {100 * ct_eval / ms_gen:.0f} % of a '
+                             f'generation; executed MMA flops {flops:.4g} (six bf16 products over each tile band); '
+                             f'peak {peak[1]}'},
+        'e2e': {'value': e2e_value, 'unit': 'trials/s', 'h2d_bytes_per_step': int(h2d),
+                'd2h_bytes_per_step': int(d2h)},
+        'gpu_launches': int(launches),
+        'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
+    }
+    if not args.no_cpu_baseline and world == 1:
+        trials, dt = profile_cpu_rate(pp, 10.0)
+        line['cpu_baseline'] = {'value': trials / dt, 'unit': 'trials/s', 'cores': 1, 'kind': 'port',
+                                'sample': f'{trials} random structures through the FP64 oracle (per-reflection '
+                                          f'|F|^2 and the fitted-scale chi^2 over 7680 points), {dt:.1f} s'}
+    if world == 1:
+        line['time_to_target_rwp'] = profile_time_to_target(pp, n)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
+PROFILE_GENERATIONS = 2000
+PROFILE_CHUNK = 100
+PROFILE_TTT_CHUNK = 50
+PROFILE_SEEDS = 8
+PROFILE_WORKLOAD = ('fixed-profile Wyckoff search: the Pnma PbSO4-like structure (Pb 4c, S 4c, O 4c, O 4c, O 8d) '
+                    'against its powder pattern (Cu Ka1/Ka2, 5-81.8 deg at 0.01 deg: 7680 points, 112 reflections, '
+                    'pseudo-Voigt at +/-20 FWHM, Poisson counts, peak 1e4), 4096 replicas, fitness 1 - Rwp at '
+                    'the best scale - penalty')
+
+
+def profile_cpu_rate(pp, seconds):
+    """The FP64 oracle's trial evaluation on the host (one thread): the
+    per-reflection mult |F|^2 of a random structure and the fitted-scale
+    chi^2 over the whole pattern.  Returns (trials, seconds)."""
+    from oracle import oracle as O
+    prob = pp.problem
+    ms = prob.tables.max_sites
+    rng = np.random.default_rng(7)
+    PT = pp.profile_t.astype(np.float64)
+    t0 = time.perf_counter()
+    done = 0
+    while time.perf_counter() - t0 < seconds:
+        x = np.zeros(ms * 3)
+        for si, s in enumerate(prob.assignments[0].sites):
+            x[si * 3:si * 3 + 3] = np.array(s.w.project(*rng.random(3))) % 1.0
+        I = O.wy_reflection_intensities(prob, 0, x)
+        O.profile_fitted_chi2(I[None, :], PT, pp.yobs, pp.w)
+        done += 1
+    return done, time.perf_counter() - t0
+
+
+def profile_time_to_target(pp, n, seeds=PROFILE_SEEDS):
+    """Time to target Rwp, the chosen method against the plain one, on the
+    same search (proposals, ladders, schedule, seeds): the chosen form runs
+    the pattern as the three-part split-BF16 product on the tensor cores
+    (chi^2 within 1e-6 of FP64); the plain form renders every reflection at
+    every point in FP32 on the CUDA cores, the reference's dense
+    `columns`/`targets` stages; the band-limited FP32 product is shown
+    beside them.  The target is 1.05 x the FP64 Rwp of the structure the
+    pattern was made from (the converged value of a search that solves it).
+    Wall time from the first evaluation of the random start (the host's
+    drawing and upload of it excluded) to the first 50-generation boundary
+    at or below the target; median over ``seeds`` seeds."""
+    from powder6_b200.profile_search import FP32, FP32_DENSE, METHOD_NAMES, SPLIT3_BF16, ProfileSearch, \
+        run_profile_search
+    target = 1.05 * pp.rwp_true
+    out = {'target_rwp': target, 'converged_rwp': pp.rwp_true,
+           'target_source': 'FP64 Rwp of the generating structure at its best scale (the noise floor)'}
+    med = {}
+    with ProfileSearch(pp, n, run_key=17) as ps:
+        for m in (SPLIT3_BF16, FP32_DENSE, FP32):
+            runs = [run_profile_search(pp, n, PROFILE_GENERATIONS, seed=301 + k, method=m, chunk=PROFILE_TTT_CHUNK,
+                                       target_rwp=target, search=ps, stop_at_target=True) for k in range(seeds)]
+            hits = [r.time_to_target for r in runs if r.time_to_target is not None]
+            gens = [r.generations_to_target for r in runs if r.generations_to_target is not None]
+            med[m] = float(np.median(hits)) if hits else None
+            out[METHOD_NAMES[m]] = {'median_s': med[m], 'reached': f'{len(hits)}/{len(runs)}',
+                                    'median_generations': float(np.median(gens)) if gens else None,
+                                    'final_rwp': [r.best_rwp for r in runs],
+                                    'cpu_check_delta': [r.cpu_check.get('delta') for r in runs]}
+    out['chosen'] = METHOD_NAMES[SPLIT3_BF16]
+    out['plain'] = METHOD_NAMES[FP32_DENSE]
+    out['chosen_s'] = med[SPLIT3_BF16]
+    out['plain_s'] = med[FP32_DENSE]
+    out['ratio'] = (med[FP32_DENSE] / med[SPLIT3_BF16]) if med[SPLIT3_BF16] and med[FP32_DENSE] else None
+    out['ratio_vs_fp32_banded'] = (med[FP32] / med[SPLIT3_BF16]) if med[SPLIT3_BF16] and med[FP32] else None
+    out['note'] = (f'chunks of {PROFILE_TTT_CHUNK} generations, {n} replicas, stop at the target; '
+                   f'median over {seeds} seeds')
+    return out
+
+
 def measured_peak(key):
     f = ROOT / 'MEASURED_PEAKS.json'
     if f.exists():
@@ -1084,12 +1294,14 @@ def main():
             run_reference_refine(args, world, rank)
         elif args.workload == 'cf':
             run_reference_cf(args, world, rank)
+        elif args.workload == 'profile':
+            run_reference_profile(args, world, rank)
         else:
             run_reference(args, world, rank)
         return
-    if args.workload in ('pt', 'contract', 'batch', 'learned', 'refine', 'cf'):
+    if args.workload in ('pt', 'contract', 'batch', 'learned', 'refine', 'cf', 'profile'):
         {'pt': main_pt, 'contract': main_ct, 'batch': main_batch, 'learned': main_learned,
-         'refine': main_refine, 'cf': main_cf}[args.workload](
+         'refine': main_refine, 'cf': main_cf, 'profile': main_profile}[args.workload](
             args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
@@ -1216,6 +1428,8 @@ def main():
         a = copy.copy(args)
         a.method = 'split'
         sub['contract'] = main_ct(a, world, rank, local, emit=False)
+        a = copy.copy(args)
+        sub['profile'] = main_profile(a, world, rank, local, emit=False)
         if rank == 0:
             line['workloads'] = sub
     if rank == 0:

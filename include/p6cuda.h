@@ -521,7 +521,10 @@ typedef struct {
  * products, so the tensor core's FP32 accumulation is what is left (chi^2
  * within about 4e-6 of FP64 against 1.2e-5 for the two-part split); twice
  * the MMA work of P6_CT_SPLIT_BF16. */
-enum { P6_CT_SPLIT_BF16 = 0, P6_CT_FP32 = 1, P6_CT_SPLIT3_BF16 = 2 };
+/* P6_CT_FP32_DENSE: the FP32 CUDA-core product over every reflection at
+ * every point, the dense render js/pt_gpu.js:249-252 (`columns`, `targets`)
+ * performs; P6_CT_FP32 runs the same product over each tile's band only. */
+enum { P6_CT_SPLIT_BF16 = 0, P6_CT_FP32 = 1, P6_CT_SPLIT3_BF16 = 2, P6_CT_FP32_DENSE = 3 };
 
 typedef struct p6_ct_session p6_ct_session;
 
@@ -543,8 +546,36 @@ p6_status p6_ct_last_ms(p6_ct_session *s, float *ms);
 /* Band statistics: K-blocks (64 reflections) summed over the 256-point tiles
  * the tensor-core path runs, reflections summed over the 128-point tiles of
  * the FP32 path, the number of 256-point tiles, kernels launched. */
+/* Fitted scale (fitted != 0): chi^2 of each replica at its best scale,
+ * min over s >= 0 of sum w (y - s Y)^2 = sum w y^2 - a^2 / b with a = sum
+ * w y Y and b = sum w Y^2 (FP64 sums), as a structure search with the scale
+ * free needs; fitted == 0 (the default) takes the intensities as scaled. */
+p6_status p6_ct_set_fitted(p6_ct_session *s, int fitted);
+/* Waits, then copies the fitted scales of the last evaluation (n_replicas doubles). */
+p6_status p6_ct_read_scale(p6_ct_session *s, double *scale);
 p6_status p6_ct_query(p6_ct_session *s, long long *band_kblocks, long long *band_cols128, int *n_tiles,
                       long long *launches);
+
+/* Fixed-profile Wyckoff search: the search of p6_wy_run with the profile
+ * chi^2 as its energy, for a cell and profile held fixed.  The contraction
+ * session's reflections must be the search session's (same count and order,
+ * profile columns carrying Lp and the peak shape, so a row of intensities is
+ * mult |F|^2 per reflection) and hold at least as many replicas.  Per
+ * generation, on the search session's stream: the search kernel proposes a
+ * move for every replica and writes the proposal's intensities into the
+ * contraction's buffer; Y = I . P runs with `method` (P6_CT_*) and gives the
+ * chi^2 at each replica's best scale over the first n_active_points points
+ * (<= 0: all); an acceptance kernel applies the Metropolis test with the
+ * replica's fitness 1 - Rwp - penalty, keeps the best structures, adapts the
+ * step and exchanges replicas along the ladders every swap_every
+ * generations.  Every reflection is evaluated (the resolution part of the
+ * schedule is not used); the penalty scale and the quench follow the
+ * session's schedules.  init != 0 first evaluates the current structures at
+ * generation gen0 and makes them the chains' energies (n_gen may then be 0).
+ * Asynchronous: p6_wy_synchronize waits and also reports a contraction wait
+ * that ran out.  In the particle states, cc holds 1 - Rwp. */
+p6_status p6_wy_profile_run(p6_wy_session *s, p6_ct_session *ct, int method, int gen0, int n_gen, int swap_every,
+                            int init, int n_active_points);
 
 /* ======================================================================== */
 /* Dual-space charge flipping on a powder reflection model                   */

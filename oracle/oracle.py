@@ -407,6 +407,50 @@ def contract_fp64(intensities, profile_t, yobs, w):
     return Y, chi2
 
 
+def profile_fitted_chi2(intensities, profile_t, yobs, w, n_active=None):
+    """FP64 chi^2 of each row of ``intensities`` at its best scale:
+    y_calc = s sum_k I_k col_k (evalPhase/render, js/rietveld_core.js:855-917)
+    and chi^2(s) = sum over w > 0 of w (y - y_calc)^2 (:1878-1889), minimised
+    over s >= 0 in closed form, s = sum w y Y / sum w Y^2.  Only the first
+    ``n_active`` points count.  Returns (chi2, scale, sum w y^2)."""
+    PT = np.asarray(profile_t, dtype=np.float64)
+    n = PT.shape[0] if n_active is None else int(n_active)
+    I = np.atleast_2d(np.asarray(intensities, dtype=np.float64))
+    Y = I @ PT[:n].T
+    ww = np.asarray(w, dtype=np.float64)[:n]
+    ww = np.where(ww > 0, ww, 0.0)
+    y = np.asarray(yobs, dtype=np.float64)[:n]
+    syy = float((ww * y * y).sum())
+    chi = np.empty(len(I))
+    scale = np.zeros(len(I))
+    for r in range(len(I)):
+        a = float((ww * y * Y[r]).sum())
+        b = float((ww * Y[r] * Y[r]).sum())
+        if a > 0 and b > 0:
+            scale[r] = a / b
+            chi[r] = float((ww * (y - scale[r] * Y[r]) ** 2).sum())
+        else:
+            chi[r] = syy
+    return chi, scale, syy
+
+
+def wy_reflection_intensities(problem, A, x):
+    """mult |F|^2 of every reflection (FP64) for the sites x (max_sites x 3
+    fractional, already on their Wyckoff positions) of assignment A, from the
+    packed tables: the per-reflection sums of swarm_reflection.wgsl's
+    structure-factor pass before grouping."""
+    atoms, _projs, _gm, hkl, mult, ftab = _refine_tables(problem, A)
+    ms = problem.tables.max_sites
+    x = np.asarray(x, dtype=np.float64).reshape(ms, 3)
+    pos = np.array([(R @ x[s] + t) % 1.0 for s, R, t, _ in atoms])
+    ty = np.array([a[3] for a in atoms])
+    ph = 2 * np.pi * (hkl @ pos.T)
+    f = ftab[:, ty]
+    fr = (f * np.cos(ph)).sum(1)
+    fi = (f * np.sin(ph)).sum(1)
+    return mult * (fr * fr + fi * fi)
+
+
 def mlp_unflatten(w, d_in, width, d_out):
     """W1 (d_in x width), b1, W2, b2, W3 (width x d_out), b3 from the flat FP32 block."""
     w = np.asarray(w, dtype=np.float64)

@@ -28,6 +28,8 @@ from ._lib import P6CtProblem, check
 SPLIT_BF16 = 0
 FP32 = 1
 SPLIT3_BF16 = 2   # three bf16 parts, six products: limited by the tensor core's FP32 accumulation
+FP32_DENSE = 3    # every reflection at every point on the CUDA cores (the reference's dense render)
+METHOD_NAMES = {SPLIT_BF16: 'split-bf16', FP32: 'fp32-banded', SPLIT3_BF16: 'split3-bf16', FP32_DENSE: 'fp32-dense'}
 
 
 @dataclass
@@ -139,6 +141,15 @@ class ContractionSession:
         check(self.lib.p6_ct_run_host(self.h, a.ctypes.data, len(a), int(method), chi.ctypes.data))
         self.m = len(a)
         return chi
+
+    def set_fitted(self, on: bool = True):
+        """chi^2 at each replica's best scale instead of the intensities as given."""
+        check(self.lib.p6_ct_set_fitted(self.h, 1 if on else 0))
+
+    def read_scale(self) -> np.ndarray:
+        s = np.zeros(self.m)
+        check(self.lib.p6_ct_read_scale(self.h, s.ctypes.data))
+        return s
 
     def synchronize(self):
         check(self.lib.p6_ct_synchronize(self.h))

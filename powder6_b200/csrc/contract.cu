@@ -30,10 +30,11 @@
 // + I_h P_l + I_l P_h + I_m P_m: every operand exact to 2^-27 and every
 // product down to 2^-24 kept, so the tensor core's FP32 accumulation is the
 // limit (measured: chi^2 within 3.7e-6 of FP64, against 1.2e-5 for the
-// two-part split and 3.4e-7 for the FP32 CUDA-core product).  The same pipeline runs it as three
-// virtual K-blocks per K-block, each staging four operand tiles and issuing
-// its share of the six products (v0: h,m x h,m less m.m; v1: h.l + l.h;
-// v2: m.m).
+// two-part split and 3.4e-7 for the FP32 CUDA-core product).  The same
+// pipeline runs it as two virtual K-blocks per K-block, each staging four
+// operand tiles and issuing its share of the six products (v0: h,m x h,m,
+// four products; v1: h.l + l.h), so each distinct operand tile but the high
+// parts is staged once per K-block.
 // A plain FP32 CUDA-core kernel over the same bands is the comparison
 // method.  Every device wait is bounded; a wait that runs out records an
 // error the host reports as P6_ERR_TIMEOUT.
@@ -50,6 +51,7 @@
 
 #include "p6_common.cuh"
 #include "tc_common.cuh"
+#include "ct_internal.h"
 
 namespace p6 {
 namespace ct {
@@ -75,14 +77,20 @@ enum CtError : int { CT_OK = 0, CT_WAIT_FULL = 11, CT_WAIT_EMPTY = 12, CT_WAIT_A
 
 struct Params {
   int M, N, Kp, nTilesN, nTilesM;
-  int virt;               // virtual K-blocks per K-block: 1 (two-part split) or 3 (three-part split)
+  int virt;               // virtual K-blocks per K-block: 1 (two-part split) or 2 (three-part split)
   const int2 *kRange;     // per BN tile: K-blocks [x, y)
   const float *yobs, *w;  // N
-  float *Y;               // optional, M x N
-  double *chiPart;        // M x nTilesN x (epilogue warps per lane quarter)
+  const double *wy, *w64; // N: w y_obs and w in FP64 (fitted-scale sums)
+  float *Y;               // optional, M x ldY
+  int ldY;
+  double *chiPart;        // M x nTilesN x (epilogue warps per lane quarter), two per slot when fitted
   int *errFlag;
 };
 
+// FITTED: instead of sum w (y - y_calc)^2 the epilogue forms, per replica,
+// a = sum w y y_calc and b = sum w y_calc^2 (FP64 products and sums), from
+// which chi^2 at the best scale s = a / b is sum w y^2 - a^2 / b.
+template <bool FITTED>
 __global__ void __launch_bounds__(kThreads, 1)
     contract_tc_kernel(const __grid_constant__ CUtensorMap tmAhi, const __grid_constant__ CUtensorMap tmAlo,
                        const __grid_constant__ CUtensorMap tmBhi, const __grid_constant__ CUtensorMap tmBlo,
@@ -138,8 +146,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_arrive_expect_tx(&fullBar[s], STAGE_BYTES);
           const int kx = (vi / P.virt) * BK, v = vi % P.virt;
           // the stage's operand slots A1, A2, B1, B2 for this virtual K-block
-          const CUtensorMap *a1 = v == 2 ? &tmAlo : &tmAhi, *a2 = v == 1 ? &tmAlo2 : &tmAlo;
-          const CUtensorMap *b1 = v == 0 ? &tmBhi : (v == 1 ? &tmBlo2 : &tmBlo), *b2 = v == 1 ? &tmBhi : &tmBlo;
+          const CUtensorMap *a1 = &tmAhi, *a2 = v == 1 ? &tmAlo2 : &tmAlo;
+          const CUtensorMap *b1 = v == 1 ? &tmBlo2 : &tmBhi, *b2 = v == 1 ? &tmBhi : &tmBlo;
           tma_load_2d(st, a1, kx, mt * BM, &fullBar[s]);
           tma_load_2d(st + A_TILE, a2, kx, mt * BM, &fullBar[s]);
           tma_load_2d(st + 2 * A_TILE, b1, kx, nt * BN, &fullBar[s]);
@@ -177,7 +185,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
           // products of the slots: bit 0 A1.B1, bit 1 A1.B2, bit 2 A2.B1, bit 3 A2.B2
           const int v = vi % P.virt;
-          const int mask = P.virt == 1 || v == 0 ? 0x7 : (v == 1 ? 0x9 : 0x1);
+          const int mask = P.virt == 1 ? 0x7 : (v == 0 ? 0xF : 0x9);
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
             const uint32_t off = k * 32;   // 16 bf16 along K inside the 128-byte swizzle row
@@ -222,7 +230,40 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int jj = 0; jj < kEpiSpan; ++jj) v[jj] = 0.f;
       }
       double chi0 = 0.0, chi1 = 0.0;
-      if (grow < P.M) {
+      if (FITTED && grow < P.M) {
+        const int col0 = nt * BN + cBeg;
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+        if (col0 + kEpiSpan <= P.N) {
+          const double2 *wy2 = reinterpret_cast<const double2 *>(P.wy + col0);
+          const double2 *ww2 = reinterpret_cast<const double2 *>(P.w64 + col0);
+#pragma unroll
+          for (int g = 0; g < kEpiSpan / 2; ++g) {
+            const double2 wy = __ldg(wy2 + g), ww = __ldg(ww2 + g);
+            const double y0 = (double)v[2 * g], y1 = (double)v[2 * g + 1];
+            a0 = fma(wy.x, y0, a0);
+            a1 = fma(wy.y, y1, a1);
+            b0 = fma(ww.x * y0, y0, b0);
+            b1 = fma(ww.y * y1, y1, b1);
+          }
+        } else {
+#pragma unroll
+          for (int jj = 0; jj < kEpiSpan; ++jj) {
+            if (col0 + jj < P.N) {
+              const double y0 = (double)v[jj];
+              a0 = fma(__ldg(P.wy + col0 + jj), y0, a0);
+              b0 = fma(__ldg(P.w64 + col0 + jj) * y0, y0, b0);
+            }
+          }
+        }
+        double *dst = P.chiPart + (((size_t)grow * P.nTilesN + nt) * slots + part) * 2;
+        dst[0] = a0 + a1;
+        dst[1] = b0 + b1;
+        if (P.Y) {
+#pragma unroll
+          for (int jj = 0; jj < kEpiSpan; ++jj)
+            if (col0 + jj < P.N) P.Y[(size_t)grow * P.ldY + col0 + jj] = v[jj];
+        }
+      } else if (grow < P.M) {
         const int col0 = nt * BN + cBeg;
         if (col0 + kEpiSpan <= P.N) {
           // whole span inside the pattern: vector loads of the observed counts and weights
@@ -235,21 +276,21 @@ __global__ void __launch_bounds__(kThreads, 1)
             chi0 += (double)(ww.x * d0 * d0) + (double)(ww.y * d1 * d1);
             chi1 += (double)(ww.z * d2 * d2) + (double)(ww.w * d3 * d3);
           }
-          if (P.Y && (P.N & 3) == 0) {
-            float4 *dst = reinterpret_cast<float4 *>(P.Y + (size_t)grow * P.N + col0);
+          if (P.Y && (P.ldY & 3) == 0) {
+            float4 *dst = reinterpret_cast<float4 *>(P.Y + (size_t)grow * P.ldY + col0);
 #pragma unroll
             for (int g = 0; g < kEpiSpan / 4; ++g)
               dst[g] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
           } else if (P.Y) {
 #pragma unroll
-            for (int jj = 0; jj < kEpiSpan; ++jj) P.Y[(size_t)grow * P.N + col0 + jj] = v[jj];
+            for (int jj = 0; jj < kEpiSpan; ++jj) P.Y[(size_t)grow * P.ldY + col0 + jj] = v[jj];
           }
         } else {
 #pragma unroll
           for (int jj = 0; jj < kEpiSpan; ++jj) {
             const int col = col0 + jj;
             if (col < P.N) {
-              if (P.Y) P.Y[(size_t)grow * P.N + col] = v[jj];
+              if (P.Y) P.Y[(size_t)grow * P.ldY + col] = v[jj];
               const float dd = __ldg(P.yobs + col) - v[jj];
               chi0 += (double)(__ldg(P.w + col) * dd * dd);
             }
@@ -311,9 +352,13 @@ __global__ void split_kernel(const float *src, int rows, int cols, int ld, int K
 
 // Plain FP32 comparison: 128 x 128 tile, 16 x 16 threads x (8 x 8) outputs, K steps of 16
 // over the tile's band; FP64 chi^2 partials per 128-column tile.
+// FITTED: the partials are a = sum w y y_calc and b = sum w y_calc^2 (two per
+// tile), as in the tensor-core kernel.  ldY: row stride of the stored Y.
+template <bool FITTED>
 __global__ void __launch_bounds__(256) contract_fp32_kernel(const float *I, int ldI, const float *PT, int ldP,
                                                             const int2 *kRange128, int M, int N, int nTiles128,
-                                                            const float *yobs, const float *w, float *Y,
+                                                            const float *yobs, const float *w, const double *wy,
+                                                            const double *w64, float *Y, int ldY,
                                                             double *chiPart) {
   __shared__ float As[FK][FM + 4], Bs[FK][FN + 4];
   __shared__ double rowChi[FM][17];
@@ -347,37 +392,91 @@ __global__ void __launch_bounds__(256) contract_fp32_kernel(const float *I, int 
     }
     __syncthreads();
   }
+  double cb[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int gm = mt * FM + ty * 8 + i;
-    double c = 0.0;
+    double c = 0.0, b = 0.0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int gn = nt * FN + tx * 8 + j;
       if (gm < M && gn < N) {
-        if (Y) Y[(size_t)gm * N + gn] = acc[i][j];
-        const double d = (double)yobs[gn] - (double)acc[i][j];
-        c += (double)w[gn] * d * d;
+        if (Y) Y[(size_t)gm * ldY + gn] = acc[i][j];
+        const double y = (double)acc[i][j];
+        if (FITTED) {
+          c = fma(wy[gn], y, c);
+          b = fma(w64[gn] * y, y, b);
+        } else {
+          const double d = (double)yobs[gn] - y;
+          c += (double)w[gn] * d * d;
+        }
       }
     }
     rowChi[ty * 8 + i][tx] = c;
+    cb[i] = b;
   }
   __syncthreads();
   if (threadIdx.x < FM) {
     const int gm = mt * FM + threadIdx.x;
     double c = 0.0;
     for (int t = 0; t < 16; ++t) c += rowChi[threadIdx.x][t];
-    if (gm < M) chiPart[(size_t)gm * nTiles128 + nt] = c;
+    if (gm < M) chiPart[((size_t)gm * nTiles128 + nt) * (FITTED ? 2 : 1)] = c;
+  }
+  if (FITTED) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) rowChi[ty * 8 + i][tx] = cb[i];
+    __syncthreads();
+    if (threadIdx.x < FM) {
+      const int gm = mt * FM + threadIdx.x;
+      double b = 0.0;
+      for (int t = 0; t < 16; ++t) b += rowChi[threadIdx.x][t];
+      if (gm < M) chiPart[((size_t)gm * nTiles128 + nt) * 2 + 1] = b;
+    }
   }
 }
 
-// chi2[r] = sum of the row's tile partials, in tile order.
+// chi2[r] = sum of the row's tile partials: one warp per row, lane l
+// summing partials l, l + 32, ... in order, then a fixed butterfly across
+// the lanes (the same order every call: bit-reproducible).
 __global__ void chi_reduce_kernel(const double *part, int M, int nTiles, double *chi2) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (r >= M) return;
+  const double *row = part + (size_t)r * nTiles;
   double s = 0.0;
-  for (int t = 0; t < nTiles; ++t) s += part[(size_t)r * nTiles + t];
-  chi2[r] = s;
+  for (int t = lane; t < nTiles; t += 32) s += row[t];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) chi2[r] = s;
+}
+
+// Fitted scale: a and b summed in tile order; chi^2 at s = a / b is
+// syy - a s (syy = sum w y^2 over the active points); s = 0 and chi^2 = syy
+// when no positive scale lowers it.
+__global__ void chi_reduce_fitted_kernel(const double *part, int M, int nTiles, double syy, double *chi2,
+                                         double *scale) {
+  const int r = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (r >= M) return;
+  const double2 *row = reinterpret_cast<const double2 *>(part) + (size_t)r * nTiles;
+  double a = 0.0, b = 0.0;
+  for (int t = lane; t < nTiles; t += 32) {
+    const double2 v = row[t];
+    a += v.x;
+    b += v.y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane != 0) return;
+  double s = 0.0, c = syy;
+  if (a > 0.0 && b > 0.0) {
+    s = a / b;
+    c = fmax(syy - a * s, 0.0);
+  }
+  chi2[r] = c;
+  if (scale) scale[r] = s;
 }
 
 }  // namespace ct
@@ -432,7 +531,10 @@ struct p6_ct_session {
   float *dY = nullptr;                  // maxM x N, allocated on first request
   float *dYobs = nullptr, *dW = nullptr;
   double *dPart = nullptr, *dChi = nullptr;
-  int2 *dRange = nullptr, *dRange128 = nullptr;
+  double *dWy = nullptr, *dW64 = nullptr, *dScale = nullptr;   // fitted-scale mode
+  std::vector<double> syyPrefix;        // sum of w y^2 over the first j points, j = 0..N
+  int fitted = 0;
+  int2 *dRange = nullptr, *dRange128 = nullptr, *dRangeDense = nullptr;
   int *dErr = nullptr;
   long long bandBlocks = 0, bandCols128 = 0;   // sum of K-blocks over BN tiles; sum of K over 128-col tiles
   CUtensorMap mapAhi, mapAlo, mapBhi, mapBlo, mapAlo2, mapBlo2;
@@ -447,6 +549,7 @@ static void ct_free(p6_ct_session *s) {
   for (void *p : {(void *)s->dPT, (void *)s->dBhi, (void *)s->dBlo, (void *)s->dAhi, (void *)s->dAlo, (void *)s->dI,
                   (void *)s->dBlo2, (void *)s->dAlo2,
                   (void *)s->dY, (void *)s->dYobs, (void *)s->dW, (void *)s->dPart, (void *)s->dChi,
+                  (void *)s->dWy, (void *)s->dW64, (void *)s->dScale, (void *)s->dRangeDense,
                   (void *)s->dRange, (void *)s->dRange128, (void *)s->dErr})
     if (p) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
@@ -466,6 +569,83 @@ static p6_status ct_check_flag(p6_ct_session *s) {
   }
   return P6_OK;
 }
+
+// Y = I . P for the first M rows of I (M x K, FP32, row-major) on `st`, over
+// the first nAct points: with `fitted`, chi^2 at each replica's best scale
+// (and the scale), else the plain weighted chi^2; Y kept when given.
+static p6_status ct_enqueue(p6_ct_session *s, cudaStream_t st, const float *I, int M, int method, bool fitted,
+                            int nAct, float *Y) {
+  if (M <= 0 || M > s->maxM) return set_error(P6_ERR_CAPACITY, "replica count outside the session's capacity");
+  nAct = std::max(1, std::min(nAct, s->N));
+  const int slots = kEpiWarps / 4;
+  int nParts;
+  if (method == P6_CT_SPLIT_BF16 || method == P6_CT_SPLIT3_BF16) {
+    const bool three = method == P6_CT_SPLIT3_BF16;
+    split_kernel<<<2368, 256, 0, st>>>(I, M, s->K, s->K, s->Kp, s->dAhi, s->dAlo, three ? s->dAlo2 : nullptr);
+    P6_CUDA(cudaGetLastError());
+    Params P;
+    P.M = M; P.N = nAct; P.Kp = s->Kp; P.nTilesN = (nAct + BN - 1) / BN; P.nTilesM = (M + BM - 1) / BM;
+    P.virt = three ? 2 : 1;
+    P.kRange = s->dRange; P.yobs = s->dYobs; P.w = s->dW; P.wy = s->dWy; P.w64 = s->dW64;
+    P.Y = Y; P.ldY = s->N; P.chiPart = s->dPart; P.errFlag = s->dErr;
+    // persistent: one CTA per SM, tiles handed out round-robin
+    const int grid = std::min(P.nTilesN * P.nTilesM, s->numSMs);
+    if (fitted)
+      contract_tc_kernel<true><<<grid, kThreads, SMEM_BYTES, st>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo,
+                                                                    s->mapAlo2, s->mapBlo2, P);
+    else
+      contract_tc_kernel<false><<<grid, kThreads, SMEM_BYTES, st>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo,
+                                                                     s->mapAlo2, s->mapBlo2, P);
+    P6_CUDA(cudaGetLastError());
+    nParts = P.nTilesN * slots;   // per replica: tiles x epilogue slots, in order
+    s->launches += 2;
+  } else {
+    const int nT = (nAct + FN - 1) / FN;
+    const dim3 grid(nT, (M + FM - 1) / FM);
+    const int2 *range = method == P6_CT_FP32_DENSE ? s->dRangeDense : s->dRange128;
+    if (fitted)
+      contract_fp32_kernel<true><<<grid, 256, 0, st>>>(I, s->K, s->dPT, s->K, range, M, nAct, nT, s->dYobs, s->dW,
+                                                        s->dWy, s->dW64, Y, s->N, s->dPart);
+    else
+      contract_fp32_kernel<false><<<grid, 256, 0, st>>>(I, s->K, s->dPT, s->K, range, M, nAct, nT, s->dYobs, s->dW,
+                                                         s->dWy, s->dW64, Y, s->N, s->dPart);
+    P6_CUDA(cudaGetLastError());
+    nParts = nT;
+    s->launches += 1;
+  }
+  // one warp per replica row, eight rows per block
+  if (fitted)
+    chi_reduce_fitted_kernel<<<(M + 7) / 8, 256, 0, st>>>(s->dPart, M, nParts, s->syyPrefix[nAct], s->dChi,
+                                                           s->dScale);
+  else
+    chi_reduce_kernel<<<(M + 7) / 8, 256, 0, st>>>(s->dPart, M, nParts, s->dChi);
+  P6_CUDA(cudaGetLastError());
+  s->launches += 1;
+  return P6_OK;
+}
+
+namespace p6 {
+namespace ct {
+// The link a fixed-profile search uses (ct_internal.h).
+ProfileLink link(p6_ct_session *s) {
+  ProfileLink L;
+  L.intensities = s->dI;
+  L.chi2 = s->dChi;
+  L.n_refl = s->K;
+  L.n_points = s->N;
+  L.max_replicas = s->maxM;
+  L.device = s->device;
+  return L;
+}
+p6_status enqueue_fitted(p6_ct_session *s, cudaStream_t stream, int n_replicas, int method, int n_active_points) {
+  return ct_enqueue(s, stream, s->dI, n_replicas, method, true, n_active_points, nullptr);
+}
+double syy(p6_ct_session *s, int n_active_points) {
+  return s->syyPrefix[std::max(0, std::min(n_active_points, s->N))];
+}
+p6_status check(p6_ct_session *s) { return ct_check_flag(s); }
+}  // namespace ct
+}  // namespace p6
 
 extern "C" {
 
@@ -515,10 +695,14 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
   CT_ALLOC(s->dI, M * K * sizeof(float));
   CT_ALLOC(s->dYobs, N * sizeof(float));
   CT_ALLOC(s->dW, N * sizeof(float));
-  CT_ALLOC(s->dPart, M * std::max((size_t)s->nTilesN * (kEpiWarps / 4), (size_t)s->nTiles128) * sizeof(double));
+  CT_ALLOC(s->dPart, 2 * M * std::max((size_t)s->nTilesN * (kEpiWarps / 4), (size_t)s->nTiles128) * sizeof(double));
   CT_ALLOC(s->dChi, M * sizeof(double));
+  CT_ALLOC(s->dScale, M * sizeof(double));
+  CT_ALLOC(s->dWy, N * sizeof(double));
+  CT_ALLOC(s->dW64, N * sizeof(double));
   CT_ALLOC(s->dRange, kb.size() * sizeof(int2));
   CT_ALLOC(s->dRange128, r128.size() * sizeof(int2));
+  CT_ALLOC(s->dRangeDense, r128.size() * sizeof(int2));
   CT_ALLOC(s->dErr, sizeof(int));
 #undef CT_ALLOC
   cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
@@ -530,6 +714,19 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
   cudaMemcpyAsync(s->dW, pr->w, N * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dRange, kb.data(), kb.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->dRange128, r128.data(), r128.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
+  // the dense comparison: every 128-point tile runs over all reflections
+  const std::vector<int2> dense(r128.size(), make_int2(0, s->K));
+  cudaMemcpyAsync(s->dRangeDense, dense.data(), dense.size() * sizeof(int2), cudaMemcpyHostToDevice, s->stream);
+  // fitted-scale operands: w (points with w <= 0 excluded) and w y in FP64
+  std::vector<double> w64(N), wy(N);
+  s->syyPrefix.assign(N + 1, 0.0);
+  for (size_t j = 0; j < N; ++j) {
+    w64[j] = pr->w[j] > 0.f ? (double)pr->w[j] : 0.0;
+    wy[j] = w64[j] * (double)pr->yobs[j];
+    s->syyPrefix[j + 1] = s->syyPrefix[j] + wy[j] * (double)pr->yobs[j];
+  }
+  cudaMemcpyAsync(s->dW64, w64.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+  cudaMemcpyAsync(s->dWy, wy.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->stream);
   split_kernel<<<2368, 256, 0, s->stream>>>(s->dPT, s->N, s->K, s->K, s->Kp, s->dBhi, s->dBlo, s->dBlo2);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -544,7 +741,9 @@ p6_status p6_ct_create(const p6_ct_problem *pr, int device, p6_ct_session **out)
     return st;
   }
   cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, device);
-  e = cudaFuncSetAttribute(contract_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  e = cudaFuncSetAttribute(contract_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(contract_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   if (e != cudaSuccess) { ct_free(s); return cuda_error(e, "cudaFuncSetAttribute"); }
   *out = s;
   return P6_OK;
@@ -571,42 +770,32 @@ p6_status p6_ct_set_intensities(p6_ct_session *s, const float *intensities, int 
 p6_status p6_ct_evaluate(p6_ct_session *s, int method, int store_pattern) {
   clear_error();
   if (!s || s->M <= 0) return set_error(P6_ERR_INVALID_ARG, "no intensities set");
-  if (method != P6_CT_SPLIT_BF16 && method != P6_CT_FP32 && method != P6_CT_SPLIT3_BF16)
-    return set_error(P6_ERR_INVALID_ARG, "unknown method");
+  if (method < P6_CT_SPLIT_BF16 || method > P6_CT_FP32_DENSE) return set_error(P6_ERR_INVALID_ARG, "unknown method");
   P6_CUDA(cudaSetDevice(s->device));
   if (store_pattern && !s->dY) P6_CUDA(cudaMalloc(&s->dY, (size_t)s->maxM * s->N * sizeof(float)));
-  float *Y = store_pattern ? s->dY : nullptr;
   P6_CUDA(cudaEventRecord(s->ev0, s->stream));
-  int nTiles;
-  if (method == P6_CT_SPLIT_BF16 || method == P6_CT_SPLIT3_BF16) {
-    const bool three = method == P6_CT_SPLIT3_BF16;
-    split_kernel<<<2368, 256, 0, s->stream>>>(s->dI, s->M, s->K, s->K, s->Kp, s->dAhi, s->dAlo,
-                                              three ? s->dAlo2 : nullptr);
-    P6_CUDA(cudaGetLastError());
-    Params P;
-    P.M = s->M; P.N = s->N; P.Kp = s->Kp; P.nTilesN = s->nTilesN; P.nTilesM = (s->M + BM - 1) / BM;
-    P.virt = three ? 3 : 1;
-    P.kRange = s->dRange; P.yobs = s->dYobs; P.w = s->dW; P.Y = Y; P.chiPart = s->dPart; P.errFlag = s->dErr;
-    // persistent: one CTA per SM, tiles handed out round-robin
-    const int grid = std::min(P.nTilesN * P.nTilesM, s->numSMs);
-    contract_tc_kernel<<<grid, kThreads, SMEM_BYTES, s->stream>>>(s->mapAhi, s->mapAlo, s->mapBhi, s->mapBlo,
-                                                                   s->mapAlo2, s->mapBlo2, P);
-    P6_CUDA(cudaGetLastError());
-    nTiles = s->nTilesN * (kEpiWarps / 4);   // per replica: tiles x epilogue slots, in order
-    s->launches += 2;
-  } else {
-    const dim3 grid(s->nTiles128, (s->M + FM - 1) / FM);
-    contract_fp32_kernel<<<grid, 256, 0, s->stream>>>(s->dI, s->K, s->dPT, s->K, s->dRange128, s->M, s->N,
-                                                       s->nTiles128, s->dYobs, s->dW, Y, s->dPart);
-    P6_CUDA(cudaGetLastError());
-    nTiles = s->nTiles128;
-    s->launches += 1;
-  }
-  chi_reduce_kernel<<<(s->M + 255) / 256, 256, 0, s->stream>>>(s->dPart, s->M, nTiles, s->dChi);
-  P6_CUDA(cudaGetLastError());
-  s->launches += 1;
+  const p6_status st = ct_enqueue(s, s->stream, s->dI, s->M, method, s->fitted != 0, s->N,
+                                  store_pattern ? s->dY : nullptr);
+  if (st != P6_OK) return st;
   P6_CUDA(cudaEventRecord(s->ev1, s->stream));
   return P6_OK;
+}
+
+p6_status p6_ct_set_fitted(p6_ct_session *s, int fitted) {
+  clear_error();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  s->fitted = fitted ? 1 : 0;
+  return P6_OK;
+}
+
+p6_status p6_ct_read_scale(p6_ct_session *s, double *scale) {
+  clear_error();
+  if (!s || !scale) return set_error(P6_ERR_INVALID_ARG, "null argument");
+  if (!s->fitted) return set_error(P6_ERR_INVALID_ARG, "the session is not in fitted-scale mode");
+  P6_CUDA(cudaSetDevice(s->device));
+  P6_CUDA(cudaMemcpyAsync(scale, s->dScale, (size_t)s->M * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  return ct_check_flag(s);
 }
 
 p6_status p6_ct_read(p6_ct_session *s, double *chi2, float *pattern) {

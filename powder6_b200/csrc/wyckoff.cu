@@ -35,6 +35,7 @@
 #include <thread>
 #include <vector>
 
+#include "ct_internal.h"
 #include "mlp_internal.h"
 #include "p6_common.cuh"
 
@@ -153,6 +154,8 @@ struct Params {
   float *fragState;        // per particle the current fragment parameters (kFragParams floats)
   float *fragBest;         // per particle the parameters of its best structure
   int fragOff;             // per-warp slice offset of the current and proposed parameters
+  int deferAccept;         // fixed-profile search: evaluate and record the proposal, leave the decision
+                           // to wy_profile_accept_kernel (the fitness is the profile chi^2)
 };
 
 // ---------------------------------------------------------------------------
@@ -683,7 +686,7 @@ __device__ __forceinline__ void factored_rows(const Params &P, const WarpView &w
                                               int nAct, int lane, float *traceIc) {
   constexpr int NR = 2;
   const int nRuns = ws.meta[1];
-  const int nM = P.nMono, pad = P.nReflPad, tl = P.tabLen;
+  const int nM = P.nMono, pad = P.nReflPad;
   const double *kre = reinterpret_cast<const double *>(stat + P.offK);
   const double *kim = P.offKi >= 0 ? reinterpret_cast<const double *>(stat + P.offKi) : nullptr;
   const uint32_t *idx = reinterpret_cast<const uint32_t *>(stat + P.offIdx);
@@ -1691,7 +1694,15 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
           const float cc = cc_of(sums);
           const float pen = penalty<SLOTS>(P, evalAtoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
           int acc = 0, best = 0;
-          if (lane == 0) {
+          if (P.deferAccept) {
+            // fixed-profile search: the proposal's intensities went to traceIc;
+            // its penalty and Metropolis draw wait for the profile chi^2
+            if (lane == 0 && P.traceRec) {
+              float *rec = P.traceRec + (size_t)p * 8;
+              rec[0] = cc - pen; rec[1] = cc; rec[2] = pen; rec[3] = uMetro;
+              rec[4] = 0.f; rec[5] = 0.f; rec[6] = temp; rec[7] = step;
+            }
+          } else if (lane == 0) {
             const float fNew = cc - pen;
             float fOld = fit;
             if (fOld > -1.0e29f) fOld = cc0 - pen0 * penScale;
@@ -2017,6 +2028,148 @@ __global__ void wy_fragment_atoms_kernel(const FragDev *F, const float *prm, int
   for (int j = lane; j < F->nAtoms * 3; j += 32) out[(size_t)v * F->nAtoms * 3 + j] = o[j];
 }
 
+// Acceptance step of a fixed-profile search: the Metropolis test, best
+// tracking, step adaptation and ladder exchange of the fused search
+// (js/swarm_wyckoff.js:1825-1851 for the exchange) with the profile chi^2 as
+// the energy.  A replica's agreement is 1 - Rwp, Rwp = sqrt(chi^2 / sum w y^2)
+// at its best scale, and its fitness is agreement - penalty, the place cc -
+// penalty holds in the intensity search.  One warp per ladder, lane r on rung
+// r; the proposals and their penalties and uniforms come from the search
+// kernel's deferred generation (tracePos, traceRec).  init != 0: chi^2 is of
+// the current structures, which become the chains' energies.
+constexpr int kAcceptWarps = 4;
+__global__ void __launch_bounds__(32 * kAcceptWarps) wy_profile_accept_kernel(const Params P, const double *chi2,
+                                                                             double syy, int g, int swapEvery,
+                                                                             int init) {
+  __shared__ float sE[kAcceptWarps][kMaxRungs], sT[kAcceptWarps][kMaxRungs];
+  __shared__ int sSwap[kAcceptWarps][kMaxRungs];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int L = blockIdx.x * kAcceptWarps + w;
+  if (L >= P.nLadders) return;   // whole warps leave together
+  const int rungs = P.rungs;
+  const size_t stride = (size_t)P.maxSites * 3;
+  uint32_t *bestBase = P.pos + (size_t)P.numParticles * stride;
+  const float penScale = P.schedGroups ? P.schedPen[g] : P.penArg;
+  const float ps = fmaxf(penScale, 1e-9f);
+  int p = -1;
+  if (lane < rungs) {
+    if (P.ladders) {
+      p = P.ladders[(size_t)L * rungs + lane];
+    } else {
+      const int q = L * rungs + lane;
+      p = q < P.numParticles ? q : -1;
+    }
+  }
+  int acc = 0, best = 0;
+  PState st{};
+  if (p >= 0) {
+    st = P.st[p];
+    float *rec = P.traceRec + (size_t)p * 8;
+    const float pen = rec[2];
+    const float cc = 1.0f - (float)sqrt(fmax(chi2[p], 0.0) / syy);
+    const float fNew = cc - pen;
+    if (init) {
+      st.fit = fNew; st.cc = cc; st.pen = pen / ps;
+      acc = 1;
+    } else {
+      float fOld = st.fit;
+      if (fOld > -1.0e29f) fOld = st.cc - st.pen * penScale;
+      const float u = rec[3];
+      if (P.quenchSd)
+        acc = fNew > fOld ? 1 : 0;
+      else if (fNew >= fOld)
+        acc = 1;
+      else if (u < expf((fNew - fOld) / fmaxf(st.temp, 1e-9f)))
+        acc = 1;
+      if (acc) {
+        st.fit = fNew; st.cc = cc; st.pen = pen / ps;
+        st.accepted += 1u;
+      }
+      if (!P.quenchSd) st.step = fminf(fmaxf(st.step * (acc ? P.stepUp : P.stepDown), P.stepMin), P.stepMax);
+      rec[4] = (float)acc;
+      rec[5] = fOld;
+    }
+    rec[0] = fNew;
+    rec[1] = cc;
+    if (acc) {
+      const float bestR = st.bestFit > -1.0e29f ? st.bestCC - st.bestPen * penScale : -1.0e30f;
+      if (fNew > bestR) {
+        st.bestFit = fNew; st.bestCC = cc; st.bestPen = pen / ps;
+        best = 1;
+      }
+    }
+  }
+  // accepted proposals become current (init keeps the current structures);
+  // new bests are copied from the current bank
+  const unsigned accMask = init ? 0u : __ballot_sync(0xffffffffu, acc);
+  const unsigned bestMask = __ballot_sync(0xffffffffu, best);
+  for (unsigned m = accMask; m; m &= m - 1) {
+    const int q = __shfl_sync(0xffffffffu, p, __ffs(m) - 1);
+    for (int j = lane; j < (int)stride; j += 32) P.pos[(size_t)q * stride + j] = P.tracePos[(size_t)q * stride + j];
+  }
+  __syncwarp();
+  for (unsigned m = bestMask; m; m &= m - 1) {
+    const int q = __shfl_sync(0xffffffffu, p, __ffs(m) - 1);
+    for (int j = lane; j < (int)stride; j += 32) bestBase[(size_t)q * stride + j] = P.pos[(size_t)q * stride + j];
+  }
+  __syncwarp();
+  if (swapEvery > 0 && !init && ((g + 1) % swapEvery) == 0) {
+    if (p >= 0) {
+      sE[w][lane] = isfinite(st.cc) ? st.cc - st.pen * penScale : st.fit;
+      sT[w][lane] = st.temp;
+    }
+    if (lane < kMaxRungs) sSwap[w][lane] = -1;
+    __syncwarp();
+    if (lane == 0) {
+      const int parity = ((g + 1) / swapEvery) & 1;
+      unsigned long long tried = 0, taken = 0;
+      for (int r = parity; r + 1 < rungs; r += 2) {
+        const int a = P.ladders ? P.ladders[(size_t)L * rungs + r] : L * rungs + r;
+        const int b = P.ladders ? P.ladders[(size_t)L * rungs + r + 1] : L * rungs + r + 1;
+        if (a < 0 || b < 0 || a >= P.numParticles || b >= P.numParticles) continue;
+        const float fa = sE[w][r], fb = sE[w][r + 1];
+        if (!isfinite(fa) || !isfinite(fb)) continue;
+        ++tried;
+        const float d = (1.0f / sT[w][r] - 1.0f / sT[w][r + 1]) * (fb - fa);
+        if (d < 0.f) {
+          const uint4 c = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)L, (uint32_t)r, 7u),
+                                        make_uint2(P.runKey, 0x45584348u));
+          if (u01(c.x) >= expf(d)) continue;
+        }
+        ++taken;
+        sSwap[w][r] = r + 1;
+      }
+      if (P.swapStats && tried) {
+        atomicAdd(P.swapStats, tried);
+        atomicAdd(P.swapStats + 1, taken);
+      }
+    }
+    __syncwarp();
+    // energies follow the coordinates; temperature and step stay with the rung
+    int partner = lane;
+    if (lane < rungs) {
+      if (sSwap[w][lane] >= 0) partner = lane + 1;
+      else if (lane > 0 && sSwap[w][lane - 1] == lane) partner = lane - 1;
+    }
+    const float oFit = __shfl_sync(0xffffffffu, st.fit, partner);
+    const float oCC = __shfl_sync(0xffffffffu, st.cc, partner);
+    const float oPen = __shfl_sync(0xffffffffu, st.pen, partner);
+    if (partner != lane && p >= 0) {
+      st.fit = oFit; st.cc = oCC; st.pen = oPen;
+    }
+    for (int r = 0; r + 1 < rungs; ++r) {
+      if (sSwap[w][r] < 0) continue;
+      const int a = __shfl_sync(0xffffffffu, p, r), b = __shfl_sync(0xffffffffu, p, r + 1);
+      for (int j = lane; j < (int)stride; j += 32) {
+        const uint32_t t = P.pos[(size_t)a * stride + j];
+        P.pos[(size_t)a * stride + j] = P.pos[(size_t)b * stride + j];
+        P.pos[(size_t)b * stride + j] = t;
+      }
+    }
+  }
+  if (p >= 0) P.st[p] = st;
+}
+
 }  // namespace wy
 }  // namespace p6
 
@@ -2067,6 +2220,8 @@ struct p6_wy_session {
   int maxGrid = 0;
   int smemPair = 0;      // per CTA when a ladder spans a cluster of two CTAs
   int ladderSplit = 2;   // CTAs per ladder of 8 in the fused search (1 or 2)
+  std::vector<float> schedPenHost;   // the penalty schedule (fixed-profile search)
+  p6_ct_session *linkedCt = nullptr; // contraction of the last fixed-profile run (its waits are checked too)
 };
 
 namespace {
@@ -3079,6 +3234,7 @@ p6_status p6_wy_set_schedule(p6_wy_session *s, const int32_t *sched_groups, cons
   if (st != P6_OK) return st;
   P6_CUDA(cudaStreamSynchronize(s->stream));
   s->schedLen = n_gen;
+  s->schedPenHost.assign(sched_pen, sched_pen + n_gen);
   return P6_OK;
 }
 
@@ -3159,6 +3315,11 @@ p6_status p6_wy_synchronize(p6_wy_session *s, double timeout_seconds) {
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (el > timeout_seconds) return set_error(P6_ERR_TIMEOUT, "the device did not finish within the deadline");
     std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  if (s->linkedCt) {
+    p6_status st = ct::check(s->linkedCt);
+    s->linkedCt = nullptr;
+    if (st != P6_OK) return st;
   }
   return check_device_flag(s);
 }
@@ -3398,6 +3559,87 @@ extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, in
     }
   }
   return P6_OK;
+}
+
+// A Wyckoff search with the cell and profile fixed: each generation the
+// search kernel proposes and evaluates every replica's move with its
+// deferred acceptance, writing the proposal's mult |F|^2 row into the
+// contraction's intensity buffer; the contraction forms Y = I . P and the
+// chi^2 at each replica's best scale; wy_profile_accept_kernel takes the
+// Metropolis decisions and the ladder exchange.  Everything is queued on the
+// search session's stream.
+extern "C" p6_status p6_wy_profile_run(p6_wy_session *s, p6_ct_session *ct, int method, int gen0, int n_gen,
+                                       int swap_every, int init, int n_active_points) {
+  P6_ENTRY();
+  if (!s || !ct) return set_error(P6_ERR_INVALID_ARG, "null session");
+  if (!s->dLadders) return set_error(P6_ERR_INVALID_ARG, "no ladders set (p6_wy_set_ladders)");
+  if (s->schedPenHost.empty() || gen0 < 0 || n_gen < 0 || gen0 + n_gen > s->schedLen ||
+      (n_gen == 0 && !init) || (init && gen0 >= s->schedLen))
+    return set_error(P6_ERR_INVALID_ARG, "generation range outside the schedule");
+  if (s->P.frag) return set_error(P6_ERR_INVALID_ARG, "the fixed-profile search moves sites, not a fragment");
+  if (method < P6_CT_SPLIT_BF16 || method > P6_CT_FP32_DENSE) return set_error(P6_ERR_INVALID_ARG, "unknown method");
+  const ct::ProfileLink L = ct::link(ct);
+  if (L.device != s->device) return set_error(P6_ERR_INVALID_ARG, "the sessions are on different devices");
+  if (L.n_refl != s->P.nRefl)
+    return set_error(P6_ERR_INVALID_ARG, "the profile's reflections are not the search's reflections");
+  if (L.max_replicas < s->P.numParticles)
+    return set_error(P6_ERR_CAPACITY, "the contraction holds fewer replicas than the search");
+  if (s->dQuench && gen0 + n_gen > s->quenchLen)
+    return set_error(P6_ERR_INVALID_ARG, "generation range outside the quench schedule");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (!s->dTracePos) {
+    const bool was = s->trace;
+    p6_status st = p6_wy_set_trace(s, 1);
+    if (st != P6_OK) return st;
+    s->trace = was;
+  }
+  const int nAct = n_active_points > 0 ? std::min(n_active_points, L.n_points) : L.n_points;
+  const double syy = ct::syy(ct, nAct);
+  if (!(syy > 0.0)) return set_error(P6_ERR_INVALID_ARG, "no weighted counts in the active points");
+  Params &P = s->P;
+  const Params saved = P;
+  const int savedIncr = s->incremental;
+  s->incremental = 0;   // one generation per launch: the full evaluation
+  P.ladders = s->dLadders;
+  P.rungs = s->rungs;
+  P.nLadders = s->nLadders;
+  P.schedGroups = nullptr;   // every reflection is evaluated: the pattern needs all of them
+  P.schedPen = nullptr;
+  P.ngaArg = P.nGroups;
+  P.quenchSd = s->dQuench;
+  P.extProp = nullptr;
+  P.deferAccept = 1;
+  P.tracePos = s->dTracePos;
+  P.traceRec = s->dTraceRec;
+  P.traceIc = L.intensities;
+  P.traceSums = nullptr;
+  const int n = P.numParticles;
+  const int acceptGrid = (P.nLadders + kAcceptWarps - 1) / kAcceptWarps;
+  p6_status st = P6_OK;
+  cudaError_t e = cudaEventRecord(s->ev0, s->stream);
+  auto step = [&](int g, int mcmc, int swapEvery, int first) -> p6_status {
+    P.penArg = s->schedPenHost[g];
+    cudaError_t le = launch(s, g, 1, mcmc, 0, 0);
+    if (le != cudaSuccess) return cuda_error(le, "wy_kernel launch");
+    p6_status cs = ct::enqueue_fitted(ct, s->stream, n, method, nAct);
+    if (cs != P6_OK) return cs;
+    wy_profile_accept_kernel<<<acceptGrid, 32 * kAcceptWarps, 0, s->stream>>>(P, L.chi2, syy, g, swapEvery, first);
+    le = cudaGetLastError();
+    if (le != cudaSuccess) return cuda_error(le, "wy_profile_accept_kernel launch");
+    s->launches++;
+    return P6_OK;
+  };
+  if (e != cudaSuccess) st = cuda_error(e, "cudaEventRecord");
+  if (st == P6_OK && init) st = step(gen0, 0, 0, 1);
+  for (int gi = 0; gi < n_gen && st == P6_OK; ++gi) st = step(gen0 + gi, 1, swap_every, 0);
+  if (st == P6_OK) {
+    e = cudaEventRecord(s->ev1, s->stream);
+    if (e != cudaSuccess) st = cuda_error(e, "cudaEventRecord");
+  }
+  P = saved;
+  s->incremental = savedIncr;
+  s->linkedCt = ct;
+  return st;
 }
 
 // Marks the start (end = 0) or end (end = 1) of a timed span on the session's

@@ -444,9 +444,9 @@ def initial_state(n: int, temps: np.ndarray, rnd: Callable[[], float], settings:
     return st
 
 
-def cpu_cross_check(problem: WyckoffProblem, coords: np.ndarray, assign: int = 0) -> float:
-    """FP64 re-score of one structure from the packed arrays (the report's
-    cross-check, js/swarm_wyckoff.js:2524-2563)."""
+def reflection_intensities(problem: WyckoffProblem, coords: np.ndarray, assign: int = 0) -> np.ndarray:
+    """mult |F|^2 of every reflection of one structure in FP64, from the packed
+    arrays (the intensities the search kernel forms)."""
     T = problem.tables
     ms = T.max_sites
     sp = T.site_proj[assign * ms * 12:(assign + 1) * ms * 12].astype(np.float64).reshape(ms, 12)
@@ -470,7 +470,13 @@ def cpu_cross_check(problem: WyckoffProblem, coords: np.ndarray, assign: int = 0
     f = problem.f_tab.astype(np.float64).reshape(-1, problem.n_elem)[:, ty]
     fr = (f * np.cos(ph)).sum(1)
     fi = (f * np.sin(ph)).sum(1)
-    ic = mult * (fr * fr + fi * fi)
+    return mult * (fr * fr + fi * fi)
+
+
+def cpu_cross_check(problem: WyckoffProblem, coords: np.ndarray, assign: int = 0) -> float:
+    """FP64 re-score of one structure from the packed arrays (the report's
+    cross-check, js/swarm_wyckoff.js:2524-2563)."""
+    ic = reflection_intensities(problem, coords, assign)
     gm = problem.refl.group_meta.astype(np.float64).reshape(-1, problem.refl.group_stride)
     scc = soo = sco = 0.0
     for row in gm:
