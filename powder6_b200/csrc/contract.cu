@@ -62,10 +62,11 @@ constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
 constexpr int A_TILE = BM * BK * 2;                       // 16 KB per bf16 operand tile
 constexpr int B_TILE = BN * BK * 2;                       // 32 KB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;      // 96 KB: A_hi, A_lo, B_hi, B_lo
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack (1024-B swizzle atoms)
 constexpr int kEpiWarps = 16;                             // four per TMEM lane quarter
 constexpr int kEpiSpan = BN / (kEpiWarps / 4);              // columns per epilogue warp (64)
 constexpr int kThreads = 64 + 32 * kEpiWarps;               // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
+constexpr int EPI_W_BYTES = kEpiWarps * kEpiSpan * 16;      // fitted epilogue: {w y, w} of each warp's columns
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_W_BYTES + 1024;   // + alignment slack (1024-B swizzle atoms)
 constexpr uint32_t TMEM_COLS = 2 * BN;                    // two accumulator buffers
 
 // SIMT comparison kernel tiles
@@ -211,11 +212,23 @@ __global__ void __launch_bounds__(kThreads, 1)
     // w (y - y_calc)^2 are formed in FP32 and summed in FP64
     const int q = warp & 3, part = (warp - 2) >> 2, cBeg = part * kEpiSpan;
     const int slots = kEpiWarps / 4;
+    // fitted: this warp's weights for the tile's columns, staged in shared
+    // memory before the accumulator wait and read back as broadcasts
+    double2 *wbuf = reinterpret_cast<double2 *>(smem + STAGES * STAGE_BYTES) + (size_t)(warp - 2) * kEpiSpan;
     int j = 0;
     for (int t = blockIdx.x; t < nTiles; t += gridDim.x, ++j) {
       const int nt = t % P.nTilesN, mt = t / P.nTilesN, acc = j & 1;
       const int2 kr = P.kRange[nt];
       const int row = q * 32 + lane, grow = mt * BM + row;
+      if (FITTED) {
+        const int col0 = nt * BN + cBeg;
+        __syncwarp();   // every lane is done with the previous tile's weights
+        for (int c = lane; c < kEpiSpan; c += 32) {
+          const int col = col0 + c;
+          wbuf[c] = col < P.N ? make_double2(__ldg(P.wy + col), __ldg(P.w64 + col)) : make_double2(0.0, 0.0);
+        }
+        __syncwarp();
+      }
       const bool ok = __all_sync(0xffffffffu, wait_phase(&accFull[acc], (j >> 1) & 1));
       if (!ok) {
         if (lane == 0) raise_flag(P.errFlag, CT_WAIT_ACC);
@@ -233,27 +246,15 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (FITTED && grow < P.M) {
         const int col0 = nt * BN + cBeg;
         double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-        if (col0 + kEpiSpan <= P.N) {
-          const double2 *wy2 = reinterpret_cast<const double2 *>(P.wy + col0);
-          const double2 *ww2 = reinterpret_cast<const double2 *>(P.w64 + col0);
+        // columns past the active points carry zero weights
 #pragma unroll
-          for (int g = 0; g < kEpiSpan / 2; ++g) {
-            const double2 wy = __ldg(wy2 + g), ww = __ldg(ww2 + g);
-            const double y0 = (double)v[2 * g], y1 = (double)v[2 * g + 1];
-            a0 = fma(wy.x, y0, a0);
-            a1 = fma(wy.y, y1, a1);
-            b0 = fma(ww.x * y0, y0, b0);
-            b1 = fma(ww.y * y1, y1, b1);
-          }
-        } else {
-#pragma unroll
-          for (int jj = 0; jj < kEpiSpan; ++jj) {
-            if (col0 + jj < P.N) {
-              const double y0 = (double)v[jj];
-              a0 = fma(__ldg(P.wy + col0 + jj), y0, a0);
-              b0 = fma(__ldg(P.w64 + col0 + jj) * y0, y0, b0);
-            }
-          }
+        for (int g = 0; g < kEpiSpan / 2; ++g) {
+          const double2 q0 = wbuf[2 * g], q1 = wbuf[2 * g + 1];
+          const double y0 = (double)v[2 * g], y1 = (double)v[2 * g + 1];
+          a0 = fma(q0.x, y0, a0);
+          a1 = fma(q1.x, y1, a1);
+          b0 = fma(q0.y * y0, y0, b0);
+          b1 = fma(q1.y * y1, y1, b1);
         }
         double *dst = P.chiPart + (((size_t)grow * P.nTilesN + nt) * slots + part) * 2;
         dst[0] = a0 + a1;

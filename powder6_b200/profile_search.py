@@ -312,3 +312,46 @@ def run_profile_search(pp: ProfileProblem, num_particles: int = 4096, generation
     finally:
         if own:
             ps.close()
+
+
+def main(argv=None):
+    """python -m powder6_b200.profile_search: a short fixed-profile search of
+    the PbSO4-like pattern with each method named, or (--contract-evals)
+    only the fitted-scale contraction of random intensity rows; one JSON
+    line per method."""
+    import argparse
+    import json
+    names = {v: k for k, v in METHOD_NAMES.items()}
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument('--replicas', type=int, default=4096)
+    ap.add_argument('--generations', type=int, default=10)
+    ap.add_argument('--methods', default='split3-bf16,fp32-dense', help=', '.join(names))
+    ap.add_argument('--seed', type=int, default=3)
+    ap.add_argument('--contract-evals', type=int, default=0,
+                    help='evaluate the contraction this many times on random rows instead of searching')
+    a = ap.parse_args(argv)
+    methods = [names[m] for m in a.methods.split(',') if m]
+    pp = profile_problem()
+    if a.contract_evals > 0:
+        I = np.random.default_rng(a.seed).lognormal(0.0, 1.5, (a.replicas, pp.n_refl)).astype(np.float32)
+        with ContractionSession(_ContractionInput(pp), max_replicas=a.replicas) as s:
+            s.set_fitted(True)
+            s.set_intensities(I)
+            for m in methods:
+                for _ in range(a.contract_evals):
+                    s.evaluate(m)
+                s.synchronize()
+                print(json.dumps({'method': METHOD_NAMES[m], 'ms_per_evaluation': s.last_ms()}), flush=True)
+        return
+    with ProfileSearch(pp, a.replicas, run_key=a.seed) as ps:
+        for m in methods:
+            ps.start(max(a.generations, 2), seed=a.seed, method=m)
+            ps.run(0, a.generations, m)
+            ps.synchronize()
+            rwp, _, _, _ = ps.best()
+            print(json.dumps({'method': METHOD_NAMES[m], 'generations': a.generations, 'best_rwp': rwp,
+                              'rwp_true': pp.rwp_true, 'ms_last_run': ps.last_ms()}), flush=True)
+
+
+if __name__ == '__main__':
+    main()
