@@ -360,6 +360,36 @@ def pt_cpu_baseline(P, x0, seconds=10.0):
 PT_FP64_FLOPS_PER_POINT = 4 * 6 + 6   # Chebyshev background (6 terms: recurrence + accumulate), residual, w r^2
 
 
+def pt_roofline(fp64_achieved, fp64_peak, flops_eval, nsm, mhz, trials, ms, chains):
+    """The sweep kernel's bound is instruction issue and latency, not a pipe:
+    warp instructions per evaluation (profiles/pt_sweep_traffic.txt, from an
+    ncu capture of one sweep launch) x evaluations/s against 4 warp
+    instructions/clk/SM; the FP64 figure is kept beside it."""
+    fp64 = {'bound': 'fp64', 'achieved': fp64_achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s',
+            'frac': fp64_achieved / fp64_peak, 'traffic': None,
+            'note': f'{flops_eval} FP64 flops per evaluation ({PT_FP64_FLOPS_PER_POINT} per pattern point: '
+                    f'Chebyshev background, residual, w r^2; the FP32 peak shapes and the per-reflection '
+                    f'FP64 stage not counted); peak 64 FP64 FMA/clk/SM x {nsm} SMs x {mhz:.0f} MHz'}
+    inst, traffic = None, None
+    tf = ROOT / 'profiles' / 'pt_sweep_traffic.txt'
+    if tf.exists():
+        for ln in tf.read_text().splitlines():
+            if ln.startswith('warp_instructions_per_evaluation:'):
+                inst = float(ln.split(':', 1)[1])
+            if ln.startswith('bytes_per_launch:'):
+                traffic = int(ln.split(':', 1)[1])
+    if not inst:
+        return fp64
+    peak = 4 * nsm * mhz * 1e6 / 1e9
+    issued = inst * trials / (ms / 1000.0) / 1e9
+    return {'bound': 'issue', 'achieved': issued, 'peak': peak, 'unit': 'Gwarp-inst/s', 'frac': issued / peak,
+            'traffic': traffic,
+            'note': f'{inst:.0f} warp instructions per evaluation (ncu, one sweep launch of the same fit) x '
+                    f'evaluations/s; peak = 4 warp instructions/clk/SM x {nsm} SMs x {mhz:.0f} MHz; '
+                    f'{chains} chains on two-CTA clusters occupy {2 * chains} SMs, one evaluation in flight each',
+            'fp64_equivalent': fp64}
+
+
 def main_pt(args, world, rank, local, emit=True):
     """One step = one tempering run of the NaCl fit: args.sweeps sweeps of
     args.chains chains from a +/-5 % start.  value: proposals per second of
@@ -436,12 +466,7 @@ def main_pt(args, world, rank, local, emit=True):
                                    'tempering_only': {'median_s': float(np.median(reached_pt)) if reached_pt else None,
                                                       'reached': f'{len(reached_pt)}/{len(ttt_pt)}',
                                                       'note': 'linear start + tempering, no least-squares finish'}},
-            'roofline': {'bound': 'fp64', 'achieved': fp64_achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s',
-                         'frac': fp64_achieved / fp64_peak, 'traffic': None,
-                         'note': f'{flops_eval} FP64 flops per evaluation ({PT_FP64_FLOPS_PER_POINT} per pattern point: '
-                                 f'Chebyshev background, residual, w r^2; the FP32 peak shapes and the per-reflection '
-                                 f'FP64 stage not counted); peak 64 FP64 FMA/clk/SM x {nsm} SMs x {mhz:.0f} MHz. '
-                                 f'{args.chains} chains hold one evaluation each in flight: the sweep is latency-bound'},
+            'roofline': pt_roofline(fp64_achieved, fp64_peak, flops_eval, nsm, mhz, trials, ms, args.chains),
             'e2e': {'value': e2e_value, 'unit': 'trials/s', 'h2d_bytes_per_step': len(starts[0]) * 8,
                     'd2h_bytes_per_step': len(starts[0]) * 8},
             'gpu_launches': int(launches),
@@ -540,6 +565,23 @@ def main_ct(args, world, rank, local, emit=True):
             e2e.append(time.perf_counter() - t0)
         e2e_total = max_over_ranks(float(sum(e2e)), world)
         e2e_value = world * M * args.steps / e2e_total
+        # chosen vs plain on this configuration: the time of one evaluation of all
+        # replicas with the chosen product against the FP32 CUDA-core products
+        cvp = {}
+        if world == 1:
+            from powder6_b200.contraction import FP32_DENSE, METHOD_NAMES
+            s.set_intensities(host)
+            for m in (method, FP32_DENSE, FP32):
+                s.evaluate(m)
+                s.synchronize()
+                s.evaluate(m)
+                s.synchronize()
+                cvp[METHOD_NAMES[m]] = s.last_ms()
+            cvp = {'chosen': METHOD_NAMES[method], 'ms_per_evaluation': cvp,
+                   'ratio_vs_fp32_dense': cvp[METHOD_NAMES[FP32_DENSE]] / cvp[METHOD_NAMES[method]],
+                   'ratio_vs_fp32_banded': cvp[METHOD_NAMES[FP32]] / cvp[METHOD_NAMES[method]],
+                   'note': 'one evaluation of all replicas (split, product, chi^2); the plain method is the '
+                           'dense FP32 render of every reflection at every point'}
     if rank == 0:
         clocks = clk.summary()
         ms = float(np.mean(times))
@@ -577,6 +619,8 @@ def main_ct(args, world, rank, local, emit=True):
             'gpu_launches': int(launches),
             'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
         }
+        if cvp:
+            line['chosen_vs_plain'] = cvp
         if not args.no_cpu_baseline and world == 1:
             trials, dt = ct_cpu_rows(p, 10.0)
             line['cpu_baseline'] = {'value': trials / dt, 'unit': 'trials/s', 'cores': os.cpu_count(),

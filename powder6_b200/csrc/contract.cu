@@ -575,7 +575,7 @@ static p6_status ct_check_flag(p6_ct_session *s) {
 // the first nAct points: with `fitted`, chi^2 at each replica's best scale
 // (and the scale), else the plain weighted chi^2; Y kept when given.
 static p6_status ct_enqueue(p6_ct_session *s, cudaStream_t st, const float *I, int M, int method, bool fitted,
-                            int nAct, float *Y) {
+                            int nAct, float *Y, bool reduce = true, int *partsOut = nullptr) {
   if (M <= 0 || M > s->maxM) return set_error(P6_ERR_CAPACITY, "replica count outside the session's capacity");
   nAct = std::max(1, std::min(nAct, s->N));
   const int slots = kEpiWarps / 4;
@@ -614,6 +614,8 @@ static p6_status ct_enqueue(p6_ct_session *s, cudaStream_t st, const float *I, i
     nParts = nT;
     s->launches += 1;
   }
+  if (partsOut) *partsOut = nParts;
+  if (!reduce) return P6_OK;
   // one warp per replica row, eight rows per block
   if (fitted)
     chi_reduce_fitted_kernel<<<(M + 7) / 8, 256, 0, st>>>(s->dPart, M, nParts, s->syyPrefix[nAct], s->dChi,
@@ -640,6 +642,11 @@ ProfileLink link(p6_ct_session *s) {
 }
 p6_status enqueue_fitted(p6_ct_session *s, cudaStream_t stream, int n_replicas, int method, int n_active_points) {
   return ct_enqueue(s, stream, s->dI, n_replicas, method, true, n_active_points, nullptr);
+}
+p6_status enqueue_fitted_partials(p6_ct_session *s, cudaStream_t stream, int n_replicas, int method,
+                                  int n_active_points, const double2 **part, int *n_parts) {
+  *part = reinterpret_cast<const double2 *>(s->dPart);
+  return ct_enqueue(s, stream, s->dI, n_replicas, method, true, n_active_points, nullptr, false, n_parts);
 }
 double syy(p6_ct_session *s, int n_active_points) {
   return s->syyPrefix[std::max(0, std::min(n_active_points, s->N))];

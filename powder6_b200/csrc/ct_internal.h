@@ -18,6 +18,12 @@ ProfileLink link(p6_ct_session *s);
 // Y = I . P over the first n_active_points points and the fitted-scale chi^2
 // of the first n_replicas rows of the intensity buffer, on `stream`.
 p6_status enqueue_fitted(p6_ct_session *s, cudaStream_t stream, int n_replicas, int method, int n_active_points);
+// The same without the per-replica reduction: the fitted-scale partials
+// {a, b} of replica r are part[r * n_parts + t], t < n_parts (summed in
+// order t = l, l + 32, ... per lane l, then across the lanes in a fixed
+// butterfly, by the caller's kernel).
+p6_status enqueue_fitted_partials(p6_ct_session *s, cudaStream_t stream, int n_replicas, int method,
+                                  int n_active_points, const double2 **part, int *n_parts);
 // sum w y^2 over the first n_active_points points (FP64).
 double syy(p6_ct_session *s, int n_active_points);
 // Reports (and clears) a tensor-core pipeline wait that ran out.

@@ -2038,9 +2038,9 @@ __global__ void wy_fragment_atoms_kernel(const FragDev *F, const float *prm, int
 // kernel's deferred generation (tracePos, traceRec).  init != 0: chi^2 is of
 // the current structures, which become the chains' energies.
 constexpr int kAcceptWarps = 4;
-__global__ void __launch_bounds__(32 * kAcceptWarps) wy_profile_accept_kernel(const Params P, const double *chi2,
-                                                                             double syy, int g, int swapEvery,
-                                                                             int init) {
+__global__ void __launch_bounds__(32 * kAcceptWarps) wy_profile_accept_kernel(const Params P, const double2 *part,
+                                                                             int nParts, double syy, int g,
+                                                                             int swapEvery, int init) {
   __shared__ float sE[kAcceptWarps][kMaxRungs], sT[kAcceptWarps][kMaxRungs];
   __shared__ int sSwap[kAcceptWarps][kMaxRungs];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -2060,13 +2060,38 @@ __global__ void __launch_bounds__(32 * kAcceptWarps) wy_profile_accept_kernel(co
       p = q < P.numParticles ? q : -1;
     }
   }
+  // chi^2 of each rung's replica at its best scale from the contraction's
+  // partials {a = sum w y Y, b = sum w Y^2}: the rungs' rows are read at
+  // once, lpr lanes per rung (lane l: rung l / lpr, partials l % lpr, + lpr,
+  // ... in order), then a fixed butterfly inside each group of lpr lanes;
+  // chi^2 = sum w y^2 - a^2 / b (no positive scale: sum w y^2)
+  int lpr = 32;
+  while (lpr > 1 && lpr * rungs > 32) lpr >>= 1;
+  const int myRung = lane / lpr, sub = lane % lpr;
+  const int q = __shfl_sync(0xffffffffu, p, myRung);
+  double a = 0.0, b = 0.0;
+  if (myRung < rungs && q >= 0) {
+    const double2 *row = part + (size_t)q * nParts;
+    for (int t = sub; t < nParts; t += lpr) {
+      const double2 v = row[t];
+      a += v.x;
+      b += v.y;
+    }
+  }
+  for (int o = lpr >> 1; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  double chiGroup = syy;
+  if (a > 0.0 && b > 0.0) chiGroup = fmax(syy - a * (a / b), 0.0);
+  const double chi = __shfl_sync(0xffffffffu, chiGroup, lane < rungs ? lane * lpr : 0);
   int acc = 0, best = 0;
   PState st{};
   if (p >= 0) {
     st = P.st[p];
     float *rec = P.traceRec + (size_t)p * 8;
     const float pen = rec[2];
-    const float cc = 1.0f - (float)sqrt(fmax(chi2[p], 0.0) / syy);
+    const float cc = 1.0f - (float)sqrt(chi / syy);
     const float fNew = cc - pen;
     if (init) {
       st.fit = fNew; st.cc = cc; st.pen = pen / ps;
@@ -3565,8 +3590,9 @@ extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, in
 // search kernel proposes and evaluates every replica's move with its
 // deferred acceptance, writing the proposal's mult |F|^2 row into the
 // contraction's intensity buffer; the contraction forms Y = I . P and the
-// chi^2 at each replica's best scale; wy_profile_accept_kernel takes the
-// Metropolis decisions and the ladder exchange.  Everything is queued on the
+// fitted-scale partials of every replica; wy_profile_accept_kernel reduces
+// them to each replica's chi^2 at its best scale and takes the Metropolis
+// decisions and the ladder exchange.  Everything is queued on the
 // search session's stream.
 extern "C" p6_status p6_wy_profile_run(p6_wy_session *s, p6_ct_session *ct, int method, int gen0, int n_gen,
                                        int swap_every, int init, int n_active_points) {
@@ -3621,9 +3647,12 @@ extern "C" p6_status p6_wy_profile_run(p6_wy_session *s, p6_ct_session *ct, int 
     P.penArg = s->schedPenHost[g];
     cudaError_t le = launch(s, g, 1, mcmc, 0, 0);
     if (le != cudaSuccess) return cuda_error(le, "wy_kernel launch");
-    p6_status cs = ct::enqueue_fitted(ct, s->stream, n, method, nAct);
+    const double2 *part = nullptr;
+    int nParts = 0;
+    p6_status cs = ct::enqueue_fitted_partials(ct, s->stream, n, method, nAct, &part, &nParts);
     if (cs != P6_OK) return cs;
-    wy_profile_accept_kernel<<<acceptGrid, 32 * kAcceptWarps, 0, s->stream>>>(P, L.chi2, syy, g, swapEvery, first);
+    wy_profile_accept_kernel<<<acceptGrid, 32 * kAcceptWarps, 0, s->stream>>>(P, part, nParts, syy, g, swapEvery,
+                                                                             first);
     le = cudaGetLastError();
     if (le != cudaSuccess) return cuda_error(le, "wy_profile_accept_kernel launch");
     s->launches++;
