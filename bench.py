@@ -1278,19 +1278,20 @@ def profile_time_to_target(pp, n, seeds=PROFILE_SEEDS):
     (chi^2 within 1e-6 of FP64); the plain form renders every reflection at
     every point in FP32 on the CUDA cores, the reference's dense
     `columns`/`targets` stages; the band-limited FP32 product is shown
-    beside them.  The target is 1.05 x the FP64 Rwp of the structure the
+    beside them, and the Gram form (chi^2 at the best scale from v . I and
+    I G I^T in FP64 inside the fused search: no pattern formed).  The target is 1.05 x the FP64 Rwp of the structure the
     pattern was made from (the converged value of a search that solves it).
     Wall time from the first evaluation of the random start (the host's
     drawing and upload of it excluded) to the first 50-generation boundary
     at or below the target; median over ``seeds`` seeds."""
-    from powder6_b200.profile_search import FP32, FP32_DENSE, METHOD_NAMES, SPLIT3_BF16, ProfileSearch, \
+    from powder6_b200.profile_search import FP32, FP32_DENSE, GRAM_FP64, METHOD_NAMES, SPLIT3_BF16, ProfileSearch, \
         run_profile_search
     target = 1.05 * pp.rwp_true
     out = {'target_rwp': target, 'converged_rwp': pp.rwp_true,
            'target_source': 'FP64 Rwp of the generating structure at its best scale (the noise floor)'}
     med = {}
     with ProfileSearch(pp, n, run_key=17) as ps:
-        for m in (SPLIT3_BF16, FP32_DENSE, FP32):
+        for m in (SPLIT3_BF16, FP32_DENSE, FP32, GRAM_FP64):
             runs = [run_profile_search(pp, n, PROFILE_GENERATIONS, seed=301 + k, method=m, chunk=PROFILE_TTT_CHUNK,
                                        target_rwp=target, search=ps, stop_at_target=True) for k in range(seeds)]
             hits = [r.time_to_target for r in runs if r.time_to_target is not None]
@@ -1306,6 +1307,9 @@ def profile_time_to_target(pp, n, seeds=PROFILE_SEEDS):
     out['plain_s'] = med[FP32_DENSE]
     out['ratio'] = (med[FP32_DENSE] / med[SPLIT3_BF16]) if med[SPLIT3_BF16] and med[FP32_DENSE] else None
     out['ratio_vs_fp32_banded'] = (med[FP32] / med[SPLIT3_BF16]) if med[SPLIT3_BF16] and med[FP32] else None
+    # the exact reformulation: no pattern formed, the whole search in one fused launch
+    out['gram_s'] = med[GRAM_FP64]
+    out['ratio_gram_vs_plain'] = (med[FP32_DENSE] / med[GRAM_FP64]) if med[GRAM_FP64] and med[FP32_DENSE] else None
     out['note'] = (f'chunks of {PROFILE_TTT_CHUNK} generations, {n} replicas, stop at the target; '
                    f'median over {seeds} seeds')
     return out

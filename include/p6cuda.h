@@ -556,6 +556,21 @@ p6_status p6_ct_read_scale(p6_ct_session *s, double *scale);
 p6_status p6_ct_query(p6_ct_session *s, long long *band_kblocks, long long *band_cols128, int *n_tiles,
                       long long *launches);
 
+/* Fixed-profile fitness in Gram form, for every later evaluation of the
+ * session (p6_wy_run, p6_wy_dispatch, ...): with the cell and profile fixed,
+ * y_calc = s I . P with I = mult |F|^2 per reflection, and the weighted
+ * chi^2 at the best scale is sum w y^2 - a^2 / b with a = v . I and
+ * b = I G I^T, where v = P (w y) and G = P W P^T (banded, symmetric) are
+ * fixed.  The search kernel forms a and b from its FP64 intensities, so the
+ * fitness cc becomes 1 - Rwp (exact in FP64, no pattern formed) and the
+ * whole search stays one launch.  v: n_refl doubles; band: the upper band
+ * of G by diagonal, band[d * n_refl + k] = G[k][k + d] (0 past the end),
+ * d = 0..bw; syy = sum w y^2.  Needs cos mode 2 (the factored FP64
+ * evaluation); every reflection is evaluated (the resolution part of the
+ * schedule is not used).  v == NULL returns to the grouped-intensity
+ * fitness. */
+p6_status p6_wy_set_profile(p6_wy_session *s, const double *v, const double *band, int bw, double syy);
+
 /* Fixed-profile Wyckoff search: the search of p6_wy_run with the profile
  * chi^2 as its energy, for a cell and profile held fixed.  The contraction
  * session's reflections must be the search session's (same count and order,

@@ -156,6 +156,7 @@ _SIGS = {
     'p6_ct_set_fitted': (C.c_int, [_P, C.c_int]),
     'p6_ct_read_scale': (C.c_int, [_P, _P]),
     'p6_wy_profile_run': (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    'p6_wy_set_profile': (C.c_int, [_P, _P, _P, C.c_int, C.c_double]),
     'p6_cf_create': (C.c_int, [_P, C.c_int, _P, C.c_int, C.POINTER(C.c_void_p)]),
     'p6_cf_destroy': (C.c_int, [_P]),
     'p6_cf_set_grid': (C.c_int, [_P, C.c_int, _P]),

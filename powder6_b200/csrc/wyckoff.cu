@@ -156,6 +156,12 @@ struct Params {
   int fragOff;             // per-warp slice offset of the current and proposed parameters
   int deferAccept;         // fixed-profile search: evaluate and record the proposal, leave the decision
                            // to wy_profile_accept_kernel (the fitness is the profile chi^2)
+  // fixed-profile fitness in Gram form (cos mode 2): v = P (w y) per reflection,
+  // G = P W P^T as its upper band by diagonal (profG[d * profK + k] = G[k][k + d]);
+  // null: the grouped-intensity fitness
+  const double *profV, *profG;
+  int profK, profBw;
+  double profSyy;
 };
 
 // ---------------------------------------------------------------------------
@@ -790,6 +796,32 @@ __device__ __forceinline__ void expand(const Params &P, const uint32_t *gen, con
     a.w = (uint32_t)t;
     atoms[i] = a;
   }
+}
+
+// The agreement 1 - Rwp of a structure against a fixed-profile pattern, from
+// its FP64 intensities I (mult |F|^2 per reflection, all reflections): with
+// y_calc = s I . P, the weighted chi^2 at the best scale is
+// sum w y^2 - a^2 / b with a = v . I and b = I G I^T, G banded and symmetric
+// (the diagonal plus twice the upper band).  Exact in FP64 and independent
+// of the number of pattern points.
+__device__ __forceinline__ float profile_cc(const Params &P, const double *I, int lane) {
+  const int K = P.profK, bw = P.profBw;
+  double a = 0.0, b = 0.0;
+  for (int k = lane; k < K; k += 32) {
+    const double Ik = I[k];
+    a = fma(__ldg(P.profV + k), Ik, a);
+    double u = 0.0;
+    for (int d = 1; d <= bw && k + d < K; ++d) u = fma(__ldg(P.profG + (size_t)d * K + k), I[k + d], u);
+    b = fma(Ik, fma(2.0, u, __ldg(P.profG + k) * Ik), b);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  double chi = P.profSyy;
+  if (a > 0.0 && b > 0.0) chi = fmax(P.profSyy - a * (a / b), 0.0);
+  return 1.0f - (float)sqrt(chi / P.profSyy);
 }
 
 __device__ __forceinline__ float cc_of(const double sums[3]) {
@@ -1604,7 +1636,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
       const int g = gen0 + gi;
       const int nga = P.schedGroups ? P.schedGroups[g] : P.ngaArg;
       const float penScale = P.schedGroups ? P.schedPen[g] : P.penArg;
-      const int ngaC = max(0, min(nga, P.nGroups));
+      // the Gram-form profile fitness needs every reflection: no resolution ramp
+      const int ngaC = P.profV ? P.nGroups : max(0, min(nga, P.nGroups));
       if (active) {
         float *tIc = P.traceIc ? P.traceIc + (size_t)p * P.nRefl : nullptr;
         const bool reeval = mcmc && ((gi == 0 && reevalFirst) || (gi > 0 && nga != prevNga));
@@ -1639,7 +1672,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
               fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
             if (P.traceSums && lane == 0)
               for (int k = 0; k < 3; ++k) P.traceSums[(size_t)p * 3 + k] = sums[k];
-            const float cc = cc_of(sums);
+            const float cc = (COSMODE == 2 && P.profV) ? profile_cc(P, ic64, lane) : cc_of(sums);
             const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
             fit = cc - pen;
             cc0 = cc;
@@ -1691,7 +1724,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
           }
           if (P.traceSums && lane == 0)
             for (int k = 0; k < 3; ++k) P.traceSums[(size_t)p * 3 + k] = sums[k];
-          const float cc = cc_of(sums);
+          const float cc = (COSMODE == 2 && P.profV) ? profile_cc(P, ic64, lane) : cc_of(sums);
           const float pen = penalty<SLOTS>(P, evalAtoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
           int acc = 0, best = 0;
           if (P.deferAccept) {
@@ -2246,6 +2279,7 @@ struct p6_wy_session {
   int smemPair = 0;      // per CTA when a ladder spans a cluster of two CTAs
   int ladderSplit = 2;   // CTAs per ladder of 8 in the fused search (1 or 2)
   std::vector<float> schedPenHost;   // the penalty schedule (fixed-profile search)
+  double *dProfV = nullptr, *dProfG = nullptr;   // Gram-form fixed-profile fitness (p6_wy_set_profile)
   p6_ct_session *linkedCt = nullptr; // contraction of the last fixed-profile run (its waits are checked too)
 };
 
@@ -2340,7 +2374,7 @@ static void free_session(p6_wy_session *s) {
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
                   s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTraceSums, s->dFrag, s->dFragState, s->dFragBest, s->dTracePos, s->dOps,
                   s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap, s->dCand, s->dExt, s->dFeat, s->dScore,
-                  s->dChosenFeat, s->dChosenScore, s->dPairRange};
+                  s->dChosenFeat, s->dChosenScore, s->dPairRange, s->dProfV, s->dProfG};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
@@ -3583,6 +3617,41 @@ extern "C" p6_status p6_wy_learned_step(p6_wy_session *s, p6_mlp *net, int K, in
       if (accepted) accepted[p] = rec[p * 8 + 4];
     }
   }
+  return P6_OK;
+}
+
+// The fixed-profile fitness in Gram form for every later evaluation of the
+// session: v (n_refl doubles) and the upper band of G by diagonal (band[d *
+// n_refl + k] = G[k][k + d], d = 0..bw), sum w y^2 = syy.  v == NULL
+// returns to the grouped-intensity fitness.
+extern "C" p6_status p6_wy_set_profile(p6_wy_session *s, const double *v, const double *band, int bw, double syy) {
+  P6_ENTRY();
+  if (!s) return set_error(P6_ERR_INVALID_ARG, "null session");
+  P6_CUDA(cudaSetDevice(s->device));
+  if (!v) {
+    s->P.profV = nullptr;
+    s->P.profG = nullptr;
+    return P6_OK;
+  }
+  if (!band || bw < 0 || !(syy > 0.0)) return set_error(P6_ERR_INVALID_ARG, "empty profile operands");
+  if (s->cosMode != 2)
+    return set_error(P6_ERR_INVALID_ARG, "the Gram-form profile fitness needs the factored FP64 evaluation");
+  const int K = s->P.nRefl;
+  if (bw >= K) bw = K - 1;
+  for (double **q : {&s->dProfV, &s->dProfG}) {
+    if (*q) cudaFree(*q);
+    *q = nullptr;
+  }
+  p6_status st = upload(&s->dProfV, v, (size_t)K, s->stream);
+  if (st != P6_OK) return st;
+  st = upload(&s->dProfG, band, (size_t)K * (bw + 1), s->stream);
+  if (st != P6_OK) return st;
+  P6_CUDA(cudaStreamSynchronize(s->stream));
+  s->P.profV = s->dProfV;
+  s->P.profG = s->dProfG;
+  s->P.profK = K;
+  s->P.profBw = bw;
+  s->P.profSyy = syy;
   return P6_OK;
 }
 

@@ -18,8 +18,13 @@ the ladder exchange.  The fitness is 1 - Rwp - penalty (Rwp on the
 background-subtracted pattern).
 
 The product runs with ``method``:
-  * SPLIT_BF16 -- the tensor cores (tcgen05, split-BF16, FP32 accumulation)
-    over each 256-point tile's band of reflections;
+  * GRAM_FP64 -- no pattern at all: with the profile fixed, chi^2 at the
+    best scale is sum w y^2 - (v . I)^2 / (I G I^T) with v = P (w y) and
+    G = P W P^T fixed and banded, so the fused search kernel forms it from
+    its FP64 intensities (``p6_wy_set_profile``) and every generation stays
+    in one launch; exact in FP64;
+  * SPLIT3_BF16 / SPLIT_BF16 -- the tensor cores (tcgen05, split-BF16, FP32
+    accumulation) over each 256-point tile's band of reflections;
   * FP32_DENSE -- every reflection at every point on the CUDA cores in FP32,
     the dense render of the reference's `columns` and `targets` stages
     (js/pt_gpu.js:249-252);
@@ -46,8 +51,12 @@ from .swarm_wyckoff import (SW_DEFAULTS, WyckoffSession, build_ladders, initial_
                             reflection_intensities, schedule, weighted_assign, assignment_dims)
 from .workloads import WyckoffProblem, mulberry32, wyckoff_problem
 
-__all__ = ['ProfileProblem', 'profile_problem', 'profile_rwp', 'ProfileSearch', 'ProfileResult',
-           'run_profile_search', 'SPLIT_BF16', 'SPLIT3_BF16', 'FP32', 'FP32_DENSE', 'METHOD_NAMES']
+GRAM_FP64 = 4     # the fitted-scale chi^2 in Gram form inside the fused search (no contraction)
+METHOD_NAMES = dict(METHOD_NAMES)
+METHOD_NAMES[GRAM_FP64] = 'gram-fp64'
+
+__all__ = ['ProfileProblem', 'profile_problem', 'profile_rwp', 'gram_operands', 'ProfileSearch', 'ProfileResult',
+           'run_profile_search', 'SPLIT_BF16', 'SPLIT3_BF16', 'FP32', 'FP32_DENSE', 'GRAM_FP64', 'METHOD_NAMES']
 
 
 @dataclass
@@ -155,6 +164,30 @@ def profile_rwp(pp: ProfileProblem, intensities: np.ndarray, n_active_points: Op
     return np.sqrt(np.maximum(chi, 0.0) / syy)
 
 
+def gram_operands(pp: ProfileProblem, n_active_points: Optional[int] = None):
+    """v = P (w y) per reflection, the upper band of G = P W P^T by diagonal
+    (band[d, k] = G[k, k + d]), its width and sum w y^2, in FP64, over the
+    first ``n_active_points`` points: the fixed profile's whole contribution
+    to chi^2 at the best scale."""
+    n = pp.n_points if n_active_points is None else int(n_active_points)
+    PT = pp.profile_t[:n].astype(np.float64)
+    w = np.maximum(pp.w[:n].astype(np.float64), 0.0)
+    y = pp.yobs[:n].astype(np.float64)
+    v = PT.T @ (w * y)
+    G = PT.T @ (w[:, None] * PT)
+    K = G.shape[0]
+    nz = np.abs(G) > 0
+    bw = 0
+    for k in range(K):
+        cols = np.flatnonzero(nz[k, k:])
+        if len(cols):
+            bw = max(bw, int(cols[-1]))
+    band = np.zeros((bw + 1, K))
+    for d in range(bw + 1):
+        band[d, :K - d] = np.diagonal(G, d)
+    return v, band, bw, float(np.sum(w * y * y))
+
+
 @dataclass
 class ProfileResult:
     best_rwp: float
@@ -190,6 +223,21 @@ class ProfileSearch:
         self.num_particles = self.wy.num_particles
         self.assign_of = np.zeros(self.num_particles, dtype=np.uint32)
         self.n_gen = 0
+        self._gram = None
+        self._gram_on = False
+
+    def set_gram(self, on: bool):
+        """The search kernel's own fitness: the Gram form of the profile chi^2
+        (on) or the grouped intensities (off)."""
+        if on and not self._gram_on:
+            if self._gram is None:
+                v, band, bw, syy = gram_operands(self.pp)
+                self._gram = (np.ascontiguousarray(v), np.ascontiguousarray(band), bw, syy)
+            v, band, bw, syy = self._gram
+            check(self.lib.p6_wy_set_profile(self.wy.h, v.ctypes.data, band.ctypes.data, int(bw), float(syy)))
+        elif not on and self._gram_on:
+            check(self.lib.p6_wy_set_profile(self.wy.h, None, None, 0, 0.0))
+        self._gram_on = bool(on)
 
     def close(self):
         self.wy.close()
@@ -221,7 +269,9 @@ class ProfileSearch:
         ladders, temps = build_ladders(self.assign_of, int(d['rungs']), d['tempCold'], d['tempHot'])
         self.wy.set_ladders(ladders, max(2, int(d['rungs'])))
         groups, pen = schedule(generations, prob.refl.n_groups, d)
+        groups[:] = prob.refl.n_groups     # the pattern needs every reflection: no resolution ramp
         self.wy.set_schedule(groups, pen)
+        self.pen0 = float(pen[0])
         self.pen_final = float(pen[-1])
         self.n_gen = generations
         rnd = mulberry32(seed)
@@ -232,6 +282,16 @@ class ProfileSearch:
     def run(self, gen0: int, n_gen: int, method: int = SPLIT_BF16, swap_every: Optional[int] = None,
             init: bool = False, n_active_points: int = 0):
         se = int(self.settings['swapEvery']) if swap_every is None else int(swap_every)
+        if method == GRAM_FP64:
+            # the fused search with the Gram-form fitness: all generations in one launch
+            self.set_gram(True)
+            if init:
+                self.wy.set_params(self.pp.problem.refl.n_groups, self.pen0)
+                self.wy.dispatch(None, mcmc=False)
+            if n_gen > 0:
+                self.wy.run(int(gen0), int(n_gen), se, reeval_first=False)
+            return
+        self.set_gram(False)
         check(self.lib.p6_wy_profile_run(self.wy.h, self.ct.h, int(method), int(gen0), int(n_gen), se,
                                          1 if init else 0, int(n_active_points)))
 

@@ -7,7 +7,8 @@ the fitted scale, which chi^2 does not depend on to first order, to ten
 times those.  Near the true structure, where chi^2 is a
 small difference of large sums, the same bars hold (the structures at and
 around the truth).  In the search, a replica's 1 - Rwp is kept in FP32, so
-Rwp is compared to Rwp * tol / 2 + 2e-7 absolute.  The
+Rwp is compared to Rwp * tol / 2 + 2e-7 absolute; the Gram form inside the
+fused search (exact FP64, no pattern formed) to the same FP32 rounding.  The
 acceptance of one generation is replayed on the host from the recorded
 proposal, penalty and uniform: the same decisions, and the accepted
 proposals become the current structures."""
@@ -15,13 +16,13 @@ import numpy as np
 import pytest
 
 from powder6_b200.contraction import ContractionSession, banded_problem
-from powder6_b200.profile_search import (FP32, FP32_DENSE, SPLIT3_BF16, SPLIT_BF16, ProfileSearch, profile_problem,
-                                         run_profile_search)
+from powder6_b200.profile_search import (FP32, FP32_DENSE, GRAM_FP64, SPLIT3_BF16, SPLIT_BF16, ProfileSearch,
+                                         profile_problem, run_profile_search)
 from powder6_b200.swarm_wyckoff import schedule
 
 pytestmark = pytest.mark.gpu
 
-TOL = {SPLIT_BF16: 3e-5, SPLIT3_BF16: 1e-6, FP32: 5e-7, FP32_DENSE: 5e-7}
+TOL = {SPLIT_BF16: 3e-5, SPLIT3_BF16: 1e-6, FP32: 5e-7, FP32_DENSE: 5e-7, GRAM_FP64: 1e-9}
 
 
 @pytest.fixture(scope='module')
@@ -75,7 +76,7 @@ def oracle_rwp(oracle, pp, fixed, assign_of):
     return np.sqrt(chi / syy)
 
 
-@pytest.mark.parametrize('method', [SPLIT_BF16, FP32_DENSE])
+@pytest.mark.parametrize('method', [SPLIT_BF16, FP32_DENSE, GRAM_FP64])
 def test_first_evaluation_matches_oracle(oracle, pp, method):
     with ProfileSearch(pp, 256, run_key=7) as ps:
         ps.start(200, seed=3, method=method)
@@ -87,8 +88,9 @@ def test_first_evaluation_matches_oracle(oracle, pp, method):
     err = np.abs((1.0 - st['cc'].astype(np.float64)) - r)
     print(f'method {method}: max |Rwp - Rwp64| {err.max():.2e} (Rwp {r.min():.3f}..{r.max():.3f})')
     assert np.all(err <= r * TOL[method] / 2 + 2e-7)
-    np.testing.assert_array_equal(best, cur)
-    np.testing.assert_array_equal(st['best_cc'], st['cc'])
+    if method != GRAM_FP64:   # the fused search's first evaluation leaves the bests to the first move
+        np.testing.assert_array_equal(best, cur)
+        np.testing.assert_array_equal(st['best_cc'], st['cc'])
 
 
 def test_generation_replays_on_oracle(oracle, pp):
@@ -132,7 +134,7 @@ def test_generation_replays_on_oracle(oracle, pp):
     assert np.all(b1 >= b0 - 1e-6)
 
 
-@pytest.mark.parametrize('method', [SPLIT_BF16, FP32_DENSE])
+@pytest.mark.parametrize('method', [SPLIT_BF16, FP32_DENSE, GRAM_FP64])
 def test_search_improves_and_rescore_agrees(pp, method):
     res = run_profile_search(pp, num_particles=1024, generations=400, seed=2, method=method, chunk=100)
     print(f'{res.method}: best Rwp {res.best_rwp:.4f} (true {pp.rwp_true:.4f}), {res.device_ms:.1f} ms, '

@@ -78,3 +78,22 @@ def test_pattern_shape(pp):
     r = profile_rwp(pp, np.array(rnd))
     assert 0.0 < pp.rwp_true < 0.2
     assert np.min(r) > 2.0 * pp.rwp_true
+
+
+def test_gram_form_equals_the_pattern_chi2(pp):
+    from powder6_b200.profile_search import gram_operands
+    v, band, bw, syy = gram_operands(pp)
+    assert band.shape == (bw + 1, pp.n_refl) and 0 < bw < pp.n_refl
+    rng = np.random.default_rng(11)
+    I = rng.lognormal(0, 1.5, (5, pp.n_refl))
+    K = pp.n_refl
+    G = np.zeros((K, K))
+    for d in range(bw + 1):
+        G[np.arange(K - d), np.arange(d, K)] = band[d, :K - d]
+        G[np.arange(d, K), np.arange(K - d)] = band[d, :K - d]
+    a = I @ v
+    b = np.einsum('rk,kl,rl->r', I, G, I)
+    chi = np.where((a > 0) & (b > 0), syy - a * a / b, syy)
+    chi64, _, syy64 = O.profile_fitted_chi2(I, pp.profile_t, pp.yobs, pp.w)
+    assert syy == pytest.approx(syy64, rel=1e-12)
+    np.testing.assert_allclose(chi, chi64, rtol=1e-10)
