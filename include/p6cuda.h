@@ -563,12 +563,13 @@ p6_status p6_ct_query(p6_ct_session *s, long long *band_kblocks, long long *band
  * b = I G I^T, where v = P (w y) and G = P W P^T (banded, symmetric) are
  * fixed.  The search kernel forms a and b from its FP64 intensities, so the
  * fitness cc becomes 1 - Rwp (exact in FP64, no pattern formed) and the
- * whole search stays one launch.  v: n_refl doubles; band: the upper band
- * of G by diagonal, band[d * n_refl + k] = G[k][k + d] (0 past the end),
- * d = 0..bw; syy = sum w y^2.  Needs cos mode 2 (the factored FP64
- * evaluation); every reflection is evaluated (the resolution part of the
- * schedule is not used).  v == NULL returns to the grouped-intensity
- * fitness. */
+ * whole search stays one launch (also in p6_wy_batch_run, each session
+ * with its own pattern).  v: n_refl doubles; band: the upper band of G by
+ * diagonal, band[d * n_refl + k] = G[k][k + d] (0 past the end), d = 0..bw;
+ * syy = sum w y^2.  In cos mode 2 the intensities are FP64, in modes 0 and
+ * 1 FP32; a and b are summed in FP64 either way.  Every reflection is
+ * evaluated (the resolution part of the schedule is not used).  v == NULL
+ * returns to the grouped-intensity fitness. */
 p6_status p6_wy_set_profile(p6_wy_session *s, const double *v, const double *band, int bw, double syy);
 
 /* Fixed-profile Wyckoff search: the search of p6_wy_run with the profile

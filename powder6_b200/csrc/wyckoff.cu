@@ -803,15 +803,17 @@ __device__ __forceinline__ void expand(const Params &P, const uint32_t *gen, con
 // y_calc = s I . P, the weighted chi^2 at the best scale is
 // sum w y^2 - a^2 / b with a = v . I and b = I G I^T, G banded and symmetric
 // (the diagonal plus twice the upper band).  Exact in FP64 and independent
-// of the number of pattern points.
-__device__ __forceinline__ float profile_cc(const Params &P, const double *I, int lane) {
+// of the number of pattern points.  I is FP64 in the factored evaluation,
+// FP32 in the cosine modes.
+template <typename T>
+__device__ __forceinline__ float profile_cc(const Params &P, const T *I, int lane) {
   const int K = P.profK, bw = P.profBw;
   double a = 0.0, b = 0.0;
   for (int k = lane; k < K; k += 32) {
-    const double Ik = I[k];
+    const double Ik = (double)I[k];
     a = fma(__ldg(P.profV + k), Ik, a);
     double u = 0.0;
-    for (int d = 1; d <= bw && k + d < K; ++d) u = fma(__ldg(P.profG + (size_t)d * K + k), I[k + d], u);
+    for (int d = 1; d <= bw && k + d < K; ++d) u = fma(__ldg(P.profG + (size_t)d * K + k), (double)I[k + d], u);
     b = fma(Ik, fma(2.0, u, __ldg(P.profG + k) * Ik), b);
   }
 #pragma unroll
@@ -1653,7 +1655,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
           if (reeval || !mcmc) {
             double sums[3];
             fitness_from_banks(P, ws, Cb, -1, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
-            const float cc = cc_of(sums);
+            const float cc = P.profV ? profile_cc(P, ic, lane) : cc_of(sums);
             const float pen = penalty<SLOTS>(P, atomsB[cb], rmin, shellLen, myPairs, myNPairs, lane) * penScale;
             fit = cc - pen;
             cc0 = cc;
@@ -1672,7 +1674,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
               fitness_direct<COSMODE>(P, ws, atoms, ic, refl, ftab, groups, sooPrefix, ngaC, lane, sums, tIc);
             if (P.traceSums && lane == 0)
               for (int k = 0; k < 3; ++k) P.traceSums[(size_t)p * 3 + k] = sums[k];
-            const float cc = (COSMODE == 2 && P.profV) ? profile_cc(P, ic64, lane) : cc_of(sums);
+            const float cc = P.profV ? (COSMODE == 2 ? profile_cc(P, ic64, lane) : profile_cc(P, ic, lane)) : cc_of(sums);
             const float pen = penalty<SLOTS>(P, atoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
             fit = cc - pen;
             cc0 = cc;
@@ -1724,7 +1726,7 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
           }
           if (P.traceSums && lane == 0)
             for (int k = 0; k < 3; ++k) P.traceSums[(size_t)p * 3 + k] = sums[k];
-          const float cc = (COSMODE == 2 && P.profV) ? profile_cc(P, ic64, lane) : cc_of(sums);
+          const float cc = P.profV ? (COSMODE == 2 ? profile_cc(P, ic64, lane) : profile_cc(P, ic, lane)) : cc_of(sums);
           const float pen = penalty<SLOTS>(P, evalAtoms, rmin, shellLen, myPairs, myNPairs, lane) * penScale;
           int acc = 0, best = 0;
           if (P.deferAccept) {
@@ -3634,8 +3636,6 @@ extern "C" p6_status p6_wy_set_profile(p6_wy_session *s, const double *v, const 
     return P6_OK;
   }
   if (!band || bw < 0 || !(syy > 0.0)) return set_error(P6_ERR_INVALID_ARG, "empty profile operands");
-  if (s->cosMode != 2)
-    return set_error(P6_ERR_INVALID_ARG, "the Gram-form profile fitness needs the factored FP64 evaluation");
   const int K = s->P.nRefl;
   if (bw >= K) bw = K - 1;
   for (double **q : {&s->dProfV, &s->dProfG}) {

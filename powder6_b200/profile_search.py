@@ -55,7 +55,8 @@ GRAM_FP64 = 4     # the fitted-scale chi^2 in Gram form inside the fused search 
 METHOD_NAMES = dict(METHOD_NAMES)
 METHOD_NAMES[GRAM_FP64] = 'gram-fp64'
 
-__all__ = ['ProfileProblem', 'profile_problem', 'profile_rwp', 'gram_operands', 'ProfileSearch', 'ProfileResult',
+__all__ = ['ProfileProblem', 'profile_problem', 'profile_rwp', 'gram_operands', 'PatternGram', 'pattern_gram',
+           'set_session_pattern', 'ProfileSearch', 'ProfileResult',
            'run_profile_search', 'SPLIT_BF16', 'SPLIT3_BF16', 'FP32', 'FP32_DENSE', 'GRAM_FP64', 'METHOD_NAMES']
 
 
@@ -186,6 +187,92 @@ def gram_operands(pp: ProfileProblem, n_active_points: Optional[int] = None):
     for d in range(bw + 1):
         band[d, :K - d] = np.diagonal(G, d)
     return v, band, bw, float(np.sum(w * y * y))
+
+
+@dataclass
+class PatternGram:
+    """A pattern reduced to what the Gram-form fitness reads (``gram_operands``),
+    built without the dense profile matrix."""
+    v: np.ndarray
+    band: np.ndarray
+    bw: int
+    syy: float
+    n_points: int
+    rwp_true: float
+
+
+def pattern_gram(problem: WyckoffProblem, n_points: Optional[int] = None, seed: int = 1, step: float = 0.01,
+                 wavelength: float = 1.5406,
+                 wavelength2: float = 1.5444, ratio: float = 0.5, U: float = 0.004, V: float = -0.002,
+                 W: float = 0.003, eta: float = 0.5, window: float = 20.0, peak_counts: float = 1.0e4,
+                 bkg0: float = 40.0, bkg1: float = 60.0, tth_lo: float = 5.0) -> PatternGram:
+    """The pattern of ``profile_problem`` for ``problem``'s true structure,
+    from ``tth_lo`` to 2 degrees past the last reflection at ``step`` (or
+    ``n_points`` evenly spaced points), kept as a sparse profile matrix: the
+    Gram operands v = P (w y) and the band of G = P W P^T, and the true
+    structure's Rwp (FP64).  The Gram form costs n_refl x (bw + 1) FMAs per
+    trial, so it suits patterns whose reflections overlap little."""
+    from scipy import sparse
+    if problem.true_coords is None:
+        raise ValueError('the problem has no true structure to make a pattern from')
+    rng = np.random.default_rng(seed)
+    t1 = reflection_two_theta(problem, wavelength)
+    t2 = 2.0 * np.degrees(np.arcsin(np.clip(np.sin(np.radians(t1 / 2.0)) * wavelength2 / wavelength, 0.0, 1.0)))
+    th = np.radians(t1 / 2.0)
+    fw = np.sqrt(np.maximum(U * np.tan(th) ** 2 + V * np.tan(th) + W, 1e-6))
+    lp = (1.0 + np.cos(2 * th) ** 2) / (np.sin(th) ** 2 * np.cos(th))
+    tth_hi = float(np.max(t2)) + 2.0
+    if n_points is None:
+        tth = tth_lo + step * np.arange(int(math.floor((tth_hi - tth_lo) / step)) + 1)
+    else:
+        tth = np.linspace(tth_lo, tth_hi, int(n_points))
+    rows, cols, vals = [], [], []
+    for k in range(len(t1)):
+        lo = int(np.searchsorted(tth, min(t1[k], t2[k]) - window * fw[k], 'left'))
+        hi = int(np.searchsorted(tth, max(t1[k], t2[k]) + window * fw[k], 'right'))
+        if hi <= lo:
+            continue
+        x = tth[lo:hi]
+        col = np.zeros(hi - lo)
+        for centre, hgt in ((t1[k], 1.0), (t2[k], ratio)):
+            m = np.abs(x - centre) <= window * fw[k]
+            col[m] += hgt * lp[k] * pseudo_voigt(x[m] - centre, fw[k], eta)
+        nz = col != 0
+        rows.append(np.arange(lo, hi)[nz])
+        cols.append(np.full(int(nz.sum()), k))
+        vals.append(col[nz])
+    K = len(t1)
+    P = sparse.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(len(tth), K))
+    I = reflection_intensities(problem, problem.true_coords, 0)
+    net = P @ I
+    scale = peak_counts / float(np.max(net))
+    bkg = bkg0 + bkg1 * np.exp(-tth / 25.0)
+    counts = rng.poisson(scale * net + bkg).astype(np.float64)
+    w = 1.0 / np.maximum(counts, 1.0)
+    y = counts - bkg
+    v = P.T @ (w * y)
+    G = (P.T @ sparse.diags(w) @ P).tocoo()
+    up = G.col >= G.row
+    d = G.col[up] - G.row[up]
+    bw = int(d.max()) if d.size else 0
+    band = np.zeros((bw + 1, K))
+    band[d, G.row[up]] = G.data[up]
+    syy = float(np.sum(w * y * y))
+    a, b = float(I @ v), float(np.sum((P @ I) ** 2 * w))
+    chi = syy - a * a / b if a > 0 and b > 0 else syy
+    return PatternGram(np.asarray(v, dtype=np.float64), band, bw, syy, len(tth), float(np.sqrt(max(chi, 0.0) / syy)))
+
+
+def set_session_pattern(session: WyckoffSession, pg: Optional[PatternGram]):
+    """The Gram-form profile fitness for a search session (``p6_wy_set_profile``);
+    None returns it to the grouped-intensity fitness."""
+    if pg is None:
+        check(session.lib.p6_wy_set_profile(session.h, None, None, 0, 0.0))
+        return
+    v = np.ascontiguousarray(pg.v, dtype=np.float64)
+    band = np.ascontiguousarray(pg.band, dtype=np.float64)
+    session._pattern_keep = (v, band)
+    check(session.lib.p6_wy_set_profile(session.h, v.ctypes.data, band.ctypes.data, int(pg.bw), float(pg.syy)))
 
 
 @dataclass

@@ -141,3 +141,17 @@ def test_search_improves_and_rescore_agrees(pp, method):
           f'accept {res.accept_rate:.2f}, check {res.cpu_check}')
     assert res.best_rwp < 0.5
     assert res.cpu_check['delta'] <= res.best_rwp * TOL[method] + 1e-6
+
+
+def test_gram_form_in_the_fp32_cosine_mode(oracle, pp):
+    # cos mode 1 (FMA polynomial): FP32 intensities (|F|^2 within 5e-6 relative of the largest), FP64 sums
+    with ProfileSearch(pp, 256, run_key=9, cos_mode=1) as ps:
+        ps.start(200, seed=4, method=GRAM_FP64)
+        ps.synchronize()
+        _, _, st = ps.wy.read_state()
+        cur, _ = ps.wy.read_positions_fixed()
+        assign_of = ps.assign_of.copy()
+    r = oracle_rwp(oracle, pp, cur, assign_of)
+    err = np.abs((1.0 - st['cc'].astype(np.float64)) - r)
+    print(f'cos mode 1, Gram form: max |Rwp - Rwp64| {err.max():.2e}')
+    assert np.all(err <= 2e-5 * r + 2e-7)

@@ -97,3 +97,14 @@ def test_gram_form_equals_the_pattern_chi2(pp):
     chi64, _, syy64 = O.profile_fitted_chi2(I, pp.profile_t, pp.yobs, pp.w)
     assert syy == pytest.approx(syy64, rel=1e-12)
     np.testing.assert_allclose(chi, chi64, rtol=1e-10)
+
+
+def test_sparse_pattern_matches_the_dense_one(pp):
+    from powder6_b200.profile_search import gram_operands, pattern_gram
+    pg = pattern_gram(pp.problem, seed=1)
+    v, band, bw, syy = gram_operands(pp)
+    assert pg.n_points == pp.n_points and pg.bw == bw
+    np.testing.assert_allclose(pg.v, v, rtol=1e-5, atol=1e-6 * np.max(np.abs(v)))
+    np.testing.assert_allclose(pg.band, band, rtol=1e-5, atol=1e-6 * np.max(band))
+    assert pg.syy == pytest.approx(syy, rel=1e-9)
+    assert pg.rwp_true == pytest.approx(pp.rwp_true, rel=1e-5)
