@@ -155,3 +155,34 @@ def test_gram_form_in_the_fp32_cosine_mode(oracle, pp):
     err = np.abs((1.0 - st['cc'].astype(np.float64)) - r)
     print(f'cos mode 1, Gram form: max |Rwp - Rwp64| {err.max():.2e}')
     assert np.all(err <= 2e-5 * r + 2e-7)
+
+
+def test_profile_run_refuses_mismatched_sessions(pp):
+    from powder6_b200._lib import P6Error, check
+    from powder6_b200.profile_search import _ContractionInput
+    with ProfileSearch(pp, 128, run_key=2) as ps:
+        ps.prepare(50, seed=2)
+        lib = ps.lib
+        # a contraction over other reflections
+        other = banded_problem(n_refl=pp.n_refl + 8, n_points=1000, n_replicas=128, seed=3)
+        with ContractionSession(other, max_replicas=128) as ct:
+            with pytest.raises(P6Error) as e:
+                check(lib.p6_wy_profile_run(ps.wy.h, ct.h, SPLIT_BF16, 0, 1, 10, 1, 0))
+            assert e.value.status == 'INVALID_ARG'
+        # a contraction holding fewer replicas than the search
+        with ContractionSession(_ContractionInput(pp), max_replicas=64) as ct:
+            with pytest.raises(P6Error) as e:
+                check(lib.p6_wy_profile_run(ps.wy.h, ct.h, SPLIT_BF16, 0, 1, 10, 1, 0))
+            assert e.value.status == 'CAPACITY'
+        # generations outside the schedule, an unknown method
+        with pytest.raises(P6Error):
+            ps.run(40, 20, SPLIT_BF16)
+        with pytest.raises(P6Error):
+            check(lib.p6_wy_profile_run(ps.wy.h, ps.ct.h, 9, 0, 1, 10, 0, 0))
+        # Gram operands without weighted counts
+        v = np.zeros(pp.n_refl)
+        with pytest.raises(P6Error):
+            check(lib.p6_wy_set_profile(ps.wy.h, v.ctypes.data, v.ctypes.data, 0, 0.0))
+        # the session still runs after the refusals
+        ps.run(0, 5, SPLIT_BF16, init=True)
+        ps.synchronize()
