@@ -65,7 +65,7 @@ constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;      // 96 KB: A_hi, A_lo, 
 constexpr int kEpiWarps = 16;                             // four per TMEM lane quarter
 constexpr int kEpiSpan = BN / (kEpiWarps / 4);              // columns per epilogue warp (64)
 constexpr int kThreads = 64 + 32 * kEpiWarps;               // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
-constexpr int EPI_W_BYTES = kEpiWarps * kEpiSpan * 16;      // fitted epilogue: {w y, w} of each warp's columns
+constexpr int EPI_W_BYTES = 2 * kEpiWarps * kEpiSpan * 16;  // fitted epilogue: {w y, w} of each warp's columns, two tiles
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_W_BYTES + 1024;   // + alignment slack (1024-B swizzle atoms)
 constexpr uint32_t TMEM_COLS = 2 * BN;                    // two accumulator buffers
 
@@ -212,20 +212,40 @@ __global__ void __launch_bounds__(kThreads, 1)
     // w (y - y_calc)^2 are formed in FP32 and summed in FP64
     const int q = warp & 3, part = (warp - 2) >> 2, cBeg = part * kEpiSpan;
     const int slots = kEpiWarps / 4;
-    // fitted: this warp's weights for the tile's columns, staged in shared
-    // memory before the accumulator wait and read back as broadcasts
-    double2 *wbuf = reinterpret_cast<double2 *>(smem + STAGES * STAGE_BYTES) + (size_t)(warp - 2) * kEpiSpan;
+    // fitted: this warp's weights for a tile's columns, copied into shared
+    // memory one tile ahead (cp.async into two buffers) and read back as
+    // broadcasts, so their trip from L2 overlaps the tile before
+    double2 *wbase = reinterpret_cast<double2 *>(smem + STAGES * STAGE_BYTES) + (size_t)(warp - 2) * kEpiSpan;
+    auto prefetch = [&](int tile, double2 *dst) {
+      const int col0 = (tile % P.nTilesN) * BN + cBeg;
+      for (int c = lane; c < kEpiSpan; c += 32) {
+        const int col = col0 + c;
+        if (col < P.N) {
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(&dst[c].x)), "l"(P.wy + col)
+                       : "memory");
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(&dst[c].y)), "l"(P.w64 + col)
+                       : "memory");
+        } else {
+          dst[c] = make_double2(0.0, 0.0);
+        }
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (FITTED && blockIdx.x < nTiles) prefetch(blockIdx.x, wbase);
     int j = 0;
     for (int t = blockIdx.x; t < nTiles; t += gridDim.x, ++j) {
       const int nt = t % P.nTilesN, mt = t / P.nTilesN, acc = j & 1;
       const int2 kr = P.kRange[nt];
       const int row = q * 32 + lane, grow = mt * BM + row;
+      double2 *wbuf = wbase + (size_t)(j & 1) * kEpiWarps * kEpiSpan;
       if (FITTED) {
-        const int col0 = nt * BN + cBeg;
-        __syncwarp();   // every lane is done with the previous tile's weights
-        for (int c = lane; c < kEpiSpan; c += 32) {
-          const int col = col0 + c;
-          wbuf[c] = col < P.N ? make_double2(__ldg(P.wy + col), __ldg(P.w64 + col)) : make_double2(0.0, 0.0);
+        // the next tile's weights go into the other buffer (its last reader,
+        // the tile before this one, finished at its closing __syncwarp)
+        if (t + (int)gridDim.x < nTiles) {
+          prefetch(t + gridDim.x, wbase + (size_t)((j + 1) & 1) * kEpiWarps * kEpiSpan);
+          asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+          asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncwarp();
       }
@@ -304,6 +324,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&accEmpty[acc]);
     }
+    if (FITTED) asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the loop
   }
   fence_before_sync();
   __syncthreads();
