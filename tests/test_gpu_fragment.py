@@ -73,3 +73,25 @@ def test_search_keeps_the_fragment_and_refines_from_near_the_truth(config5):
         assert abs(np.linalg.norm(orth @ e) - np.linalg.norm(frag.ref[u] - frag.ref[v])) < 1e-3
     print(f'fragment refinement from near the truth: best cc {res.best_cc:.4f}, {res.kernel_ms:.0f} ms on the device')
     assert res.best_cc > 0.9
+
+
+def test_fragment_search_scored_on_the_pattern(config5):
+    # the fragment's fitness as the pattern's chi^2 in Gram form: every replica's
+    # 1 - Rwp after a short search equals the oracle's (FP64 intensities of the
+    # device's coordinates, FP64 fitted-scale chi^2 over the dense pattern)
+    from powder6_b200.profile_search import pattern_gram, profile_problem, set_session_pattern
+    P, frag, _ = config5
+    pp = profile_problem(P, seed=1)           # the dense pattern on the grid pattern_gram uses
+    with WyckoffSession(P, 64, run_key=4) as s:
+        set_session_pattern(s, pattern_gram(P, seed=1))
+        run_fragment_search(P, frag, 64, 30, seed=4, chunk=30, session=s, do_quench=False, full_resolution=True)
+        _, _, st = s.read_state()
+        cur, _ = s.read_positions_fixed()
+    cpp = P.tables.max_sites * 3
+    x = cur.astype(np.float64).reshape(-1, cpp) / TWO32
+    I = np.array([O.wy_reflection_intensities(P, 0, xi) for xi in x])
+    chi, _, syy = O.profile_fitted_chi2(I, pp.profile_t, pp.yobs, pp.w)
+    r = np.sqrt(chi / syy)
+    err = np.abs((1.0 - st['cc'].astype(np.float64)) - r)
+    print(f'fragment, Gram form: max |Rwp - Rwp64| {err.max():.2e} (Rwp {r.min():.3f}..{r.max():.3f})')
+    assert np.all(err <= 1e-5 * r + 2e-7)
