@@ -1111,54 +1111,69 @@ FRAGMENT_SEEDS = (11, 12, 13, 14)
 
 def main_fragment(args, world, rank, local):
     """Config 5 as a rigid fragment: cimetidine (17 non-H atoms, 6 torsions)
-    on 4e of P2_1/c, 8192 replicas x FRAGMENT_GENERATIONS generations from
-    random placements, every reflection at the final penalty weight, the
-    fitness the pattern's chi^2 at the best scale in Gram form (5895 points,
-    575 reflections).  One step = one search; value: trials/s from CUDA
-    events; time to target: wall seconds to a best Rwp <= 1.05 x the true
-    structure's, per seed (the quench included)."""
+    on 4e of P2_1/c, 8192 replicas from random placements, every reflection
+    at the final penalty weight, scored on its powder pattern (5895 points,
+    575 reflections): chi^2 at the best scale from the three-part split-BF16
+    contraction (the chosen form), from the dense FP32 render (plain), and
+    in Gram form inside the fused search.  Per seed (the first --steps of
+    FRAGMENT_SEEDS) each method searches up to FRAGMENT_GENERATIONS
+    generations; time to target: wall seconds from the first evaluation to
+    the first 500-generation boundary with a best Rwp <= 1.05 x the true
+    structure's.  value: trials/s of the chosen method from CUDA events."""
     import torch
-    from powder6_b200.fragment import fragment_problem, run_fragment_search
-    from powder6_b200.profile_search import pattern_gram, set_session_pattern
-    from powder6_b200.swarm_wyckoff import WyckoffSession
+    from powder6_b200.contraction import FP32_DENSE, SPLIT3_BF16
+    from powder6_b200.fragment import fragment_problem, run_fragment_pattern_search
+    from powder6_b200.profile_search import GRAM_FP64, METHOD_NAMES, profile_problem
     torch.cuda.set_device(local)
     P, frag, _ = fragment_problem(seed=1)
-    pg = pattern_gram(P, seed=1)
-    target = 1.05 * pg.rwp_true
+    pp = profile_problem(P, seed=1)
+    target = 1.05 * pp.rwp_true
     n = 8192
-    runs = []
+    methods = (SPLIT3_BF16, FP32_DENSE, GRAM_FP64)
+    runs = {m: [] for m in methods}
     with ClockSampler(local) as clk:
         for seed in FRAGMENT_SEEDS[:max(1, args.steps)]:
-            with WyckoffSession(P, n, run_key=seed, device=local) as s:
-                set_session_pattern(s, pg)
-                r = run_fragment_search(P, frag, n, FRAGMENT_GENERATIONS, seed=seed, chunk=500,
-                                        target_cc=1.0 - target, session=s, full_resolution=True)
-                runs.append(r)
+            for m in methods:
+                runs[m].append(run_fragment_pattern_search(P, frag, pp, m, n, FRAGMENT_GENERATIONS, seed=seed,
+                                                           chunk=500, target_rwp=target))
     if rank != 0:
         return
     clocks = clk.summary()
-    ms = float(np.mean([r.kernel_ms for r in runs]))
-    trials = n * FRAGMENT_GENERATIONS
-    hits = [r.time_to_target for r in runs if r.time_to_target is not None]
+
+    def summary(rs):
+        hits = [r['time_to_target'] for r in rs if r['time_to_target'] is not None]
+        us = [1000.0 * r['device_ms'] / max(1, r['generations']) for r in rs]
+        return {'median_s': float(np.median(hits)) if hits else None, 'reached': f'{len(hits)}/{len(rs)}',
+                'final_rwp': [r['best_rwp'] for r in rs],
+                'generations_to_target': [r['generations_to_target'] for r in rs],
+                'us_per_generation': float(np.median(us))}
+    ttt = {METHOD_NAMES[m]: summary(runs[m]) for m in methods}
+    chosen, plain, gram = (ttt[METHOD_NAMES[m]] for m in methods)
+    both = [(a['time_to_target'], b['time_to_target']) for a, b in zip(runs[SPLIT3_BF16], runs[FP32_DENSE])
+            if a['time_to_target'] is not None and b['time_to_target'] is not None]
+    cr = runs[SPLIT3_BF16]
+    value = n * sum(r['generations'] for r in cr) / (sum(r['device_ms'] for r in cr) / 1000.0)
     line = {
-        'metric': 'trial structures evaluated/s', 'value': trials / (ms / 1000.0), 'unit': 'trials/s', 'n_gpus': world,
-        'steps': len(runs), 'warmup': 0, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
-        'vs_baseline': None, 'dtype': 'fp64 |F|^2 and Gram sums', 'data': 'synthetic',
+        'metric': 'trial structures evaluated/s', 'value': value, 'unit': 'trials/s', 'n_gpus': world,
+        'steps': len(cr), 'warmup': 0, 'ms_per_step': float(np.mean([r['device_ms'] for r in cr])),
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'fp64 |F|^2, bf16 three-part split (6 products) fp32 accumulate, fp64 chi2', 'data': 'synthetic',
         'config': {'workload': f'rigid-fragment search, cimetidine (C10N6S, 17 non-H atoms, 6 torsions) on 4e of '
                                f'P2_1/c (10.2 x 12.1 x 15.3 A, beta 100), {P.refl.n_refl} reflections to 1.5 A, '
-                               f'pattern {pg.n_points} points (G bandwidth {pg.bw}), {n} replicas x '
-                               f'{FRAGMENT_GENERATIONS} generations from random placements',
-                   'step': 'one search (plus its quench)', 'parallelism': f'replicas only x{world}'},
+                               f'pattern {pp.n_points} points, {n} replicas from random placements, up to '
+                               f'{FRAGMENT_GENERATIONS} generations per search',
+                   'step': 'one search per seed and method', 'parallelism': f'replicas only x{world}'},
         'roofline': None,
         'e2e': None,
         'gpu_launches': None,
         'clocks': {k: clocks[k] for k in ('sm_mhz', 'sm_max_mhz', 'reasons')},
-        'time_to_target_rwp': {'median_s': float(np.median(hits)) if hits else None,
-                               'reached': f'{len(hits)}/{len(runs)}', 'target_rwp': target,
-                               'converged_rwp': pg.rwp_true,
-                               'final_rwp': [1.0 - r.best_cc for r in runs],
-                               'note': 'target 1.05 x the true structure\'s FP64 Rwp; seeds ' +
-                                       ', '.join(str(x) for x in FRAGMENT_SEEDS[:len(runs)])},
+        'time_to_target_rwp': {'target_rwp': target, 'converged_rwp': pp.rwp_true, 'methods': ttt,
+                               'chosen': METHOD_NAMES[SPLIT3_BF16], 'plain': METHOD_NAMES[FP32_DENSE],
+                               'chosen_s': chosen['median_s'], 'plain_s': plain['median_s'],
+                               'ratio_seeds_both_reached': [b / a for a, b in both],
+                               'gram_s': gram['median_s'],
+                               'note': 'target 1.05 x the true structure\'s FP64 Rwp; chunks of 500 generations; '
+                                       'seeds ' + ', '.join(str(x) for x in FRAGMENT_SEEDS[:len(cr)])},
     }
     print(json.dumps(line), flush=True)
 

@@ -588,6 +588,9 @@ p6_status p6_wy_set_profile(p6_wy_session *s, const double *v, const double *ban
  * schedule is not used); the penalty scale and the quench follow the
  * session's schedules.  init != 0 first evaluates the current structures at
  * generation gen0 and makes them the chains' energies (n_gen may then be 0).
+ * A rigid-fragment session (p6_wy_set_fragment) runs too: a proposal's
+ * fragment parameters follow its coordinates through the acceptance, the
+ * bests and the exchange.
  * Asynchronous: p6_wy_synchronize waits and also reports a contraction wait
  * that ran out.  In the particle states, cc holds 1 - Rwp. */
 p6_status p6_wy_profile_run(p6_wy_session *s, p6_ct_session *ct, int method, int gen0, int n_gen, int swap_every,

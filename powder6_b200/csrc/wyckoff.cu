@@ -153,6 +153,7 @@ struct Params {
   const FragDev *frag;     // rigid-fragment search: the fragment; null: the sites move independently
   float *fragState;        // per particle the current fragment parameters (kFragParams floats)
   float *fragBest;         // per particle the parameters of its best structure
+  float *fragProp;         // per particle the proposed parameters of a deferred generation
   int fragOff;             // per-warp slice offset of the current and proposed parameters
   int deferAccept;         // fixed-profile search: evaluate and record the proposal, leave the decision
                            // to wy_profile_accept_kernel (the fitness is the profile chi^2)
@@ -1737,6 +1738,8 @@ __device__ __forceinline__ bool wy_cta(const Params &P, int L0, int Lstep, int g
               rec[0] = cc - pen; rec[1] = cc; rec[2] = pen; rec[3] = uMetro;
               rec[4] = 0.f; rec[5] = 0.f; rec[6] = temp; rec[7] = step;
             }
+            if (P.frag && P.fragProp && lane < kFragParams)
+              P.fragProp[(size_t)p * kFragParams + lane] = fcurW[kFragParams + lane];
           } else if (lane == 0) {
             const float fNew = cc - pen;
             float fOld = fit;
@@ -2163,14 +2166,20 @@ __global__ void __launch_bounds__(32 * kAcceptWarps) wy_profile_accept_kernel(co
   // new bests are copied from the current bank
   const unsigned accMask = init ? 0u : __ballot_sync(0xffffffffu, acc);
   const unsigned bestMask = __ballot_sync(0xffffffffu, best);
+  // (a rigid fragment's parameters follow its coordinates)
+  const bool frag = P.frag && P.fragState && P.fragBest && P.fragProp;
   for (unsigned m = accMask; m; m &= m - 1) {
     const int q = __shfl_sync(0xffffffffu, p, __ffs(m) - 1);
     for (int j = lane; j < (int)stride; j += 32) P.pos[(size_t)q * stride + j] = P.tracePos[(size_t)q * stride + j];
+    if (frag && lane < kFragParams)
+      P.fragState[(size_t)q * kFragParams + lane] = P.fragProp[(size_t)q * kFragParams + lane];
   }
   __syncwarp();
   for (unsigned m = bestMask; m; m &= m - 1) {
     const int q = __shfl_sync(0xffffffffu, p, __ffs(m) - 1);
     for (int j = lane; j < (int)stride; j += 32) bestBase[(size_t)q * stride + j] = P.pos[(size_t)q * stride + j];
+    if (frag && lane < kFragParams)
+      P.fragBest[(size_t)q * kFragParams + lane] = P.fragState[(size_t)q * kFragParams + lane];
   }
   __syncwarp();
   if (swapEvery > 0 && !init && ((g + 1) % swapEvery) == 0) {
@@ -2225,6 +2234,11 @@ __global__ void __launch_bounds__(32 * kAcceptWarps) wy_profile_accept_kernel(co
         P.pos[(size_t)a * stride + j] = P.pos[(size_t)b * stride + j];
         P.pos[(size_t)b * stride + j] = t;
       }
+      if (frag && lane < kFragParams) {
+        const float t = P.fragState[(size_t)a * kFragParams + lane];
+        P.fragState[(size_t)a * kFragParams + lane] = P.fragState[(size_t)b * kFragParams + lane];
+        P.fragState[(size_t)b * kFragParams + lane] = t;
+      }
     }
   }
   if (p >= 0) P.st[p] = st;
@@ -2254,7 +2268,7 @@ struct p6_wy_session {
   float *dSchedP = nullptr, *dTraceRec = nullptr, *dTraceIc = nullptr, *dQuench = nullptr;
   double *dTraceSums = nullptr;   // per particle {scc, soo, sco} of the last traced evaluation
   FragDev *dFrag = nullptr;       // rigid-fragment search (p6_wy_set_fragment)
-  float *dFragState = nullptr, *dFragBest = nullptr;
+  float *dFragState = nullptr, *dFragBest = nullptr, *dFragProp = nullptr;
   int quenchLen = 0;
   // learned search: candidates, features, scores, the chosen proposal
   uint32_t *dCand = nullptr, *dExt = nullptr;
@@ -2374,7 +2388,7 @@ static void free_session(p6_wy_session *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   void *ptrs[] = {s->dGen, s->dGenOrig, s->dFree, s->dPos, s->dAssign, s->dRuns, s->dNRuns, s->dNF,
-                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTraceSums, s->dFrag, s->dFragState, s->dFragBest, s->dTracePos, s->dOps,
+                  s->dLadders, s->dSchedG, s->dErr, s->dSchedP, s->dQuench, s->dTraceRec, s->dTraceIc, s->dTraceSums, s->dFrag, s->dFragState, s->dFragBest, s->dFragProp, s->dTracePos, s->dOps,
                   s->dProj, s->dBlob, s->dRules, s->dSt, s->dSwap, s->dCand, s->dExt, s->dFeat, s->dScore,
                   s->dChosenFeat, s->dChosenScore, s->dPairRange, s->dProfV, s->dProfG};
   for (void *p : ptrs)
@@ -3426,6 +3440,8 @@ p6_status p6_wy_set_fragment(p6_wy_session *s, const p6_wy_fragment *f) {
   if (!s->dFragState) {
     P6_CUDA(cudaMalloc(&s->dFragState, (size_t)s->P.numParticles * kFragParams * sizeof(float)));
     P6_CUDA(cudaMalloc(&s->dFragBest, (size_t)s->P.numParticles * kFragParams * sizeof(float)));
+    P6_CUDA(cudaMalloc(&s->dFragProp, (size_t)s->P.numParticles * kFragParams * sizeof(float)));
+    P6_CUDA(cudaMemsetAsync(s->dFragProp, 0, (size_t)s->P.numParticles * kFragParams * sizeof(float), s->stream));
     P6_CUDA(cudaMemsetAsync(s->dFragState, 0, (size_t)s->P.numParticles * kFragParams * sizeof(float), s->stream));
     P6_CUDA(cudaMemsetAsync(s->dFragBest, 0, (size_t)s->P.numParticles * kFragParams * sizeof(float), s->stream));
   }
@@ -3434,6 +3450,7 @@ p6_status p6_wy_set_fragment(p6_wy_session *s, const p6_wy_fragment *f) {
   s->P.frag = s->dFrag;
   s->P.fragState = s->dFragState;
   s->P.fragBest = s->dFragBest;
+  s->P.fragProp = s->dFragProp;
   return P6_OK;
 }
 
@@ -3671,7 +3688,6 @@ extern "C" p6_status p6_wy_profile_run(p6_wy_session *s, p6_ct_session *ct, int 
   if (s->schedPenHost.empty() || gen0 < 0 || n_gen < 0 || gen0 + n_gen > s->schedLen ||
       (n_gen == 0 && !init) || (init && gen0 >= s->schedLen))
     return set_error(P6_ERR_INVALID_ARG, "generation range outside the schedule");
-  if (s->P.frag) return set_error(P6_ERR_INVALID_ARG, "the fixed-profile search moves sites, not a fragment");
   if (method < P6_CT_SPLIT_BF16 || method > P6_CT_FP32_DENSE) return set_error(P6_ERR_INVALID_ARG, "unknown method");
   const ct::ProfileLink L = ct::link(ct);
   if (L.device != s->device) return set_error(P6_ERR_INVALID_ARG, "the sessions are on different devices");

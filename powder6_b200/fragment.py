@@ -350,3 +350,82 @@ def run_fragment_search(problem: WyckoffProblem, frag: Fragment, num_particles: 
     if own:
         sess.close()
     return res
+
+
+def run_fragment_pattern_search(problem: WyckoffProblem, frag: Fragment, pp, method: int, num_particles: int = 8192,
+                                generations: int = 15000, seed: int = 1, chunk: int = 500,
+                                target_rwp: Optional[float] = None, settings: Optional[dict] = None) -> dict:
+    """The rigid-fragment search scored on a powder pattern (``pp``, a
+    ProfileProblem of ``problem``): every reflection at the final penalty
+    weight from random placements, with the pattern's chi^2 at the best scale
+    from the split-BF16 or FP32 contraction (``p6_wy_profile_run``) or in
+    Gram form inside the fused search (``GRAM_FP64``).  The clock runs from
+    the first evaluation (the host's drawing and upload of the start
+    excluded) to the first chunk boundary at or below ``target_rwp``.
+    Returns best_rwp, time_to_target, generations_to_target, device_ms."""
+    from .contraction import ContractionSession
+    from .profile_search import GRAM_FP64, METHOD_NAMES, PatternGram, _ContractionInput, gram_operands, \
+        set_session_pattern
+    from .swarm_wyckoff import SW_DEFAULTS, WyckoffSession, build_ladders, initial_state, schedule
+    d = dict(SW_DEFAULTS)
+    d.update(settings or {})
+    swap = int(d['swapEvery'])
+    with WyckoffSession(problem, num_particles, run_key=seed, settings=settings) as sess:
+        n, cpp = sess.num_particles, sess.coords_per_particle
+        set_fragment(sess, frag)
+        assign = np.zeros(n, dtype=np.uint32)
+        sess.set_assign(assign)
+        ladders, temps = build_ladders(assign, int(d['rungs']), d['tempCold'], d['tempHot'])
+        sess.set_ladders(ladders, int(d['rungs']))
+        groups, pen = schedule(generations, problem.refl.n_groups, d)
+        groups[:] = problem.refl.n_groups
+        pen[:] = pen[-1]
+        sess.set_schedule(groups, pen)
+        rng = np.random.default_rng(seed)
+        prm = random_params(rng, n, len(frag.torsions))
+        pos = np.zeros((n, cpp), dtype=np.float32)
+        for i in range(n):
+            pos[i, :frag.n_atoms * 3] = fragment_coords(frag, prm[i]).reshape(-1)
+        sess.sync_state(pos.reshape(-1), initial_state(n, temps, mulberry32(seed), d))
+        write_fragment_state(sess, prm)
+        ct = None
+        if method == GRAM_FP64:
+            v, band, bw, syy = gram_operands(pp)
+            set_session_pattern(sess, PatternGram(v, band, bw, syy, pp.n_points, pp.rwp_true))
+            sess.set_params(problem.refl.n_groups, float(pen[-1]))
+        else:
+            ct = ContractionSession(_ContractionInput(pp), max_replicas=n)
+            ct.set_fitted(True)
+        try:
+            sess.synchronize(600.0)
+            t0 = time.perf_counter()
+            if ct is None:
+                sess.dispatch(None, mcmc=False)
+            else:
+                check(sess.lib.p6_wy_profile_run(sess.h, ct.h, int(method), 0, 0, swap, 1, 0))
+            sess.synchronize(600.0)
+            dev_ms = sess.last_kernel_ms()
+            hit, hit_gen, g0 = None, None, 0
+            while g0 < generations:
+                ng = min(chunk, generations - g0)
+                if ct is None:
+                    sess.run(g0, ng, swap, False)
+                else:
+                    check(sess.lib.p6_wy_profile_run(sess.h, ct.h, int(method), g0, ng, swap, 0, 0))
+                sess.synchronize(600.0)
+                dev_ms += sess.last_kernel_ms()
+                g0 += ng
+                if target_rwp is not None and hit is None:
+                    _, _, st = sess.read_state()
+                    ok = st['best_fit'] > -1e29
+                    if np.any(ok) and 1.0 - float(np.max(st['best_cc'][ok])) <= target_rwp:
+                        hit, hit_gen = time.perf_counter() - t0, g0
+                        break
+            _, _, st = sess.read_state()
+            ok = st['best_fit'] > -1e29
+            best = 1.0 - float(np.max(st['best_cc'][ok])) if np.any(ok) else 1.0
+            return {'method': METHOD_NAMES[method], 'seed': seed, 'best_rwp': best, 'time_to_target': hit,
+                    'generations_to_target': hit_gen, 'generations': g0, 'device_ms': dev_ms}
+        finally:
+            if ct is not None:
+                ct.close()

@@ -95,3 +95,48 @@ def test_fragment_search_scored_on_the_pattern(config5):
     err = np.abs((1.0 - st['cc'].astype(np.float64)) - r)
     print(f'fragment, Gram form: max |Rwp - Rwp64| {err.max():.2e} (Rwp {r.min():.3f}..{r.max():.3f})')
     assert np.all(err <= 1e-5 * r + 2e-7)
+
+
+def test_fragment_parameters_follow_the_contraction_search(config5):
+    # the fragment searched with the pattern's chi^2 from the split-BF16 contraction
+    # (deferred acceptance): after accepted moves, bests and ladder exchanges every
+    # replica's current and best coordinates are the device map of its current and
+    # best parameters, bit for bit
+    from powder6_b200._lib import check
+    from powder6_b200.contraction import SPLIT3_BF16, ContractionSession
+    from powder6_b200.profile_search import _ContractionInput, profile_problem
+    from powder6_b200.swarm_wyckoff import SW_DEFAULTS, build_ladders, initial_state, schedule
+    from powder6_b200.workloads import mulberry32
+    from powder6_b200.fragment import fragment_coords
+    P, frag, _ = config5
+    pp = profile_problem(P, seed=1)
+    n = 256
+    with WyckoffSession(P, n, run_key=6) as s, ContractionSession(_ContractionInput(pp), max_replicas=n) as ct:
+        ct.set_fitted(True)
+        set_fragment(s, frag)
+        cpp = s.coords_per_particle
+        assign = np.zeros(n, dtype=np.uint32)
+        s.set_assign(assign)
+        ladders, temps = build_ladders(assign, 8, SW_DEFAULTS['tempCold'], SW_DEFAULTS['tempHot'])
+        s.set_ladders(ladders, 8)
+        groups, pen = schedule(60, P.refl.n_groups)
+        groups[:] = P.refl.n_groups
+        s.set_schedule(groups, pen)
+        prm = random_params(np.random.default_rng(6), n, len(frag.torsions))
+        pos = np.zeros((n, cpp), dtype=np.float32)
+        for i in range(n):
+            pos[i, :frag.n_atoms * 3] = fragment_coords(frag, prm[i]).reshape(-1)
+        s.sync_state(pos.reshape(-1), initial_state(n, temps, mulberry32(6)))
+        from powder6_b200.fragment import write_fragment_state
+        write_fragment_state(s, prm)
+        check(s.lib.p6_wy_profile_run(s.h, ct.h, SPLIT3_BF16, 0, 0, 10, 1, 0))
+        check(s.lib.p6_wy_profile_run(s.h, ct.h, SPLIT3_BF16, 0, 60, 10, 0, 0))
+        s.synchronize(120)
+        cur_fx, best_fx = s.read_positions_fixed()
+        cur_prm, best_prm = read_fragment_state(s)
+        _, _, st = s.read_state()
+        assert st['accepted'].sum() > 0
+        assert np.any(np.abs(cur_prm - prm.astype(np.float32)) > 0)
+        for fx, pr in ((cur_fx, cur_prm), (best_fx, best_prm)):
+            mapped = device_coords(s, frag, pr).reshape(n, -1)
+            assert np.array_equal(mapped, fx.reshape(n, cpp)[:, :frag.n_atoms * 3])
