@@ -813,9 +813,17 @@ __device__ __forceinline__ float profile_cc(const Params &P, const T *I, int lan
   for (int k = lane; k < K; k += 32) {
     const double Ik = (double)I[k];
     a = fma(__ldg(P.profV + k), Ik, a);
-    double u = 0.0;
-    for (int d = 1; d <= bw && k + d < K; ++d) u = fma(__ldg(P.profG + (size_t)d * K + k), (double)I[k + d], u);
-    b = fma(Ik, fma(2.0, u, __ldg(P.profG + k) * Ik), b);
+    // the band's diagonals in two interleaved chains, so the loads and FMAs overlap
+    const int dEnd = min(bw, K - 1 - k);
+    double u0 = 0.0, u1 = 0.0;
+    int d = 1;
+#pragma unroll 4
+    for (; d + 1 <= dEnd; d += 2) {
+      u0 = fma(__ldg(P.profG + (size_t)d * K + k), (double)I[k + d], u0);
+      u1 = fma(__ldg(P.profG + (size_t)(d + 1) * K + k), (double)I[k + d + 1], u1);
+    }
+    if (d <= dEnd) u0 = fma(__ldg(P.profG + (size_t)d * K + k), (double)I[k + d], u0);
+    b = fma(Ik, fma(2.0, u0 + u1, __ldg(P.profG + k) * Ik), b);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
