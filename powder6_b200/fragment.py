@@ -429,3 +429,29 @@ def run_fragment_pattern_search(problem: WyckoffProblem, frag: Fragment, pp, met
         finally:
             if ct is not None:
                 ct.close()
+
+
+def main(argv=None):
+    """python -m powder6_b200.fragment: a short search of config 5's rigid
+    fragment against its pattern with each method named; one JSON line per
+    method."""
+    import argparse
+    from .profile_search import METHOD_NAMES, profile_problem
+    names = {v: k for k, v in METHOD_NAMES.items()}
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument('--replicas', type=int, default=8192)
+    ap.add_argument('--generations', type=int, default=100)
+    ap.add_argument('--methods', default='split3-bf16,fp32-dense,gram-fp64', help=', '.join(names))
+    ap.add_argument('--seed', type=int, default=11)
+    a = ap.parse_args(argv)
+    P, frag, _ = fragment_problem(seed=1)
+    pp = profile_problem(P, seed=1)
+    for m in a.methods.split(','):
+        r = run_fragment_pattern_search(P, frag, pp, names[m], a.replicas, a.generations, seed=a.seed,
+                                        chunk=a.generations)
+        r['us_per_generation'] = 1000.0 * r['device_ms'] / max(1, r['generations'])
+        print(json.dumps(r), flush=True)
+
+
+if __name__ == '__main__':
+    main()
